@@ -1,0 +1,745 @@
+// Test-infrastructure driver for the reference implementation.
+//
+// Compiled by oracle/Makefile together with the reference's own hot-path
+// sources (read in place from the reference tree) into oracle/_ref/ref_harness.
+// It never enters the product: the tests use it to pin the oracle restatement
+// and to produce golden fixtures, and bench.py's reference arm uses it as the
+// CPU baseline.  It builds the same objects the reference's App builds for a
+// YAML config (src/qmc/app.cpp:432-452 Hamiltonian order, src/builders/
+// jastrow.cpp:48-63 cusps, :339-389 image-summed Padé under Ewald,
+// src/builders/slater.cpp:267 plane-wave shells), but directly, without the
+// YAML/HDF5 layers, the way tests/test_dmc_bench.cpp does.
+//
+// usage: ref_harness MODE key=value...
+//   MODE setup  : print the system description (every setup-time table) as JSON
+//   MODE init   : print the initial walker positions (app.cpp:56-112 semantics)
+//   MODE eval   : evaluate ln|psi|, grad, lap and E_L of the initial walkers
+//   MODE vmc    : run the reference VMC driver and print its trace
+//   MODE dmc    : run the reference DMC driver and print its trace
+//   MODE bench  : time DMC (or VMC, method=vmc) steps with all host threads
+#include <omp.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "hamiltonian/coulomb.h"
+#include "hamiltonian/ewald_term.h"
+#include "hamiltonian/hamiltonian.h"
+#include "hamiltonian/kinetic.h"
+#include "numerics/long_range_breakup.h"
+#include "numerics/pair_radial.h"
+#include "numerics/random.h"
+#include "numerics/xoshiro_random.h"
+#include "population/walker.h"
+#include "population/walker_ensemble.h"
+#include "population/walker_set.h"
+#include "qmc/dmc.h"
+#include "qmc/vmc.h"
+#include "wavefunction/drummond_jastrow.h"
+#include "wavefunction/orbital_set.h"
+#include "wavefunction/pade_jastrow.h"
+#include "wavefunction/slater_determinant.h"
+#include "wavefunction/trial_wavefunction.h"
+
+using namespace alea;
+
+namespace {
+
+// ── tiny JSON writer ────────────────────────────────────────────────────────
+struct Json {
+    std::string s;
+    bool first = true;
+    void sep() {
+        if (!first) s += ",";
+        first = false;
+    }
+    void key(const std::string& k) {
+        sep();
+        s += "\"" + k + "\":";
+        first = true;
+    }
+    void num(double x) {
+        sep();
+        char b[40];
+        if (std::isfinite(x))
+            std::snprintf(b, sizeof b, "%.17g", x);
+        else
+            std::snprintf(b, sizeof b, "null");
+        s += b;
+    }
+    void inum(long long x) {
+        sep();
+        s += std::to_string(x);
+    }
+    void str(const std::string& x) {
+        sep();
+        s += "\"" + x + "\"";
+    }
+    void open(char c) {
+        sep();
+        s += c;
+        first = true;
+    }
+    void close(char c) {
+        s += c;
+        first = false;
+    }
+    template <class V>
+    void arr(const std::string& k, const V& v) {
+        key(k);
+        open('[');
+        for (auto x : v) num(static_cast<double>(x));
+        close(']');
+    }
+    void kv(const std::string& k, double x) {
+        key(k);
+        num(x);
+    }
+    void ki(const std::string& k, long long x) {
+        key(k);
+        inum(x);
+    }
+    void ks(const std::string& k, const std::string& x) {
+        key(k);
+        str(x);
+    }
+};
+
+using Args = std::map<std::string, std::string>;
+
+double getd(const Args& a, const std::string& k, double d) {
+    auto it = a.find(k);
+    return it == a.end() ? d : std::stod(it->second);
+}
+long long geti(const Args& a, const std::string& k, long long d) {
+    auto it = a.find(k);
+    return it == a.end() ? d : std::stoll(it->second);
+}
+std::string gets(const Args& a, const std::string& k, const std::string& d) {
+    auto it = a.find(k);
+    return it == a.end() ? d : it->second;
+}
+
+ParticleGroup make_group(const std::string& name, std::size_t first, std::size_t n,
+                         double charge, std::size_t dim, double mass = 1.0) {
+    ParticleGroup g;
+    g.name = name;
+    g.mass.assign(dim, mass);
+    g.inv_mass.assign(dim, 1.0 / mass);
+    g.charge = charge;
+    g.first = first;
+    g.last = first + n;
+    g.count = n;
+    return g;
+}
+
+// Everything one system needs, plus what the setup dump reports.
+struct System {
+    std::string kind;
+    std::size_t dim = 2, np = 0;
+    std::vector<ParticleGroup> groups;
+    SimulationCell cell;
+    TrialWavefunction psi;
+    Hamiltonian ham;
+    double L_open = 1.0;                 // open-cell initialisation box
+    std::vector<double> anchors;         // [np*dim] crystal sites per particle
+    double jitter = 0.0;
+    Json setup;                          // system description
+};
+
+void dump_cell(Json& j, const SimulationCell& c) {
+    j.key("cell");
+    j.open('{');
+    j.ki("periodic", c.is_periodic() ? 1 : 0);
+    j.ki("dim", static_cast<long long>(c.dim()));
+    if (c.is_periodic()) {
+        j.arr("vectors", c.vectors());
+        j.arr("reciprocal", c.reciprocal());
+        j.ki("orthorhombic", c.orthorhombic() ? 1 : 0);
+        j.kv("volume", c.volume());
+        j.kv("ws_radius", c.ws_radius());
+    }
+    j.close('}');
+}
+
+void dump_groups(Json& j, const std::vector<ParticleGroup>& groups) {
+    j.key("groups");
+    j.open('[');
+    for (const ParticleGroup& g : groups) {
+        j.open('{');
+        j.ks("name", g.name);
+        j.ki("first", static_cast<long long>(g.first));
+        j.ki("last", static_cast<long long>(g.last));
+        j.kv("charge", g.charge);
+        j.arr("inv_mass", g.inv_mass);
+        j.close('}');
+    }
+    j.close(']');
+}
+
+void dump_spline(Json& j, const std::string& k, const numerics::LongRangeSpline& sp) {
+    j.key(k);
+    j.open('{');
+    j.kv("r_cut", sp.r_cut);
+    j.kv("inv_delta", sp.inv_delta);
+    j.ki("n_knots", sp.n_knots);
+    j.arr("scaled", sp.scaled);
+    j.close('}');
+}
+
+// The image-summed Padé tables, rebuilt with exactly the calls and options of
+// PeriodicPairSum's constructor (src/wavefunction/periodic_pair_sum.cpp:21-60),
+// which is deterministic: same inputs, same tables.
+void dump_pade_image_sum(Json& j, const SimulationCell& cell, const std::vector<double>& a,
+                         const std::vector<double>& b) {
+    const double rc = cell.ws_radius();
+    numerics::BreakupOptions opt{};
+    opt.k_continuum = 20.0 * 3.14159265358979323846 / rc;
+    opt.k_max = 300.0 / rc;
+    opt.n_continuum = 150;
+    opt.k_cut = 5.0 * std::min(std::hypot(cell.reciprocal()[0], cell.reciprocal()[1]),
+                               std::hypot(cell.reciprocal()[2], cell.reciprocal()[3]));
+    const numerics::LongRangeBreakup br =
+        numerics::build_long_range_breakup(cell, numerics::pade_radial(a, b, rc), opt);
+    j.key("image_sum");
+    j.open('{');
+    dump_spline(j, "spline", br.spline());
+    j.kv("u_inf", numerics::pade_limit(a, b));
+    j.arr("n1", br.n1());
+    j.arr("n2", br.n2());
+    j.arr("kx", br.kx());
+    j.arr("ky", br.ky());
+    j.arr("weight", br.weight());
+    j.kv("k_cut", br.k_cut());
+    j.close('}');
+}
+
+// ── systems ─────────────────────────────────────────────────────────────────
+
+// 2D homogeneous electron gas: plane-wave determinants per spin, image-summed
+// Padé u = a1 r/(1 + b r) on every spin pair (a1 from the Kato cusp), Ewald.
+std::unique_ptr<System> build_heg(const Args& a) {
+    auto s = std::make_unique<System>();
+    s->kind = "heg";
+    const std::size_t nu = static_cast<std::size_t>(geti(a, "nu", 21));
+    const std::size_t nd = static_cast<std::size_t>(geti(a, "nd", 21));
+    const double rs = getd(a, "rs", 30.0);
+    const double bden = getd(a, "b", 0.3);
+    const double tol = getd(a, "tol", 1e-6);
+    const double pi = 3.14159265358979323846;
+    s->dim = 2;
+    s->np = nu + nd;
+    const double L = std::sqrt(static_cast<double>(s->np) * pi * rs * rs);
+    const std::vector<double> vec{L, 0.0, 0.0, L};
+    s->cell = SimulationCell(2, vec);
+    s->groups.push_back(make_group("up", 0, nu, -1.0, 2));
+    if (nd > 0) s->groups.push_back(make_group("down", nu, nd, -1.0, 2));
+
+    // Hamiltonian: kinetic, then one cell-wide Ewald term (app.cpp:438-445).
+    s->ham.add_component(std::make_unique<Kinetic>(s->groups));
+    auto ewald = std::make_unique<EwaldTerm>(s->groups, 1.0, s->cell, tol);
+    const EwaldTerm& ew = *ewald;
+
+    Json& j = s->setup;
+    j.open('{');
+    j.ks("kind", "heg");
+    j.ki("dim", 2);
+    j.ki("np", static_cast<long long>(s->np));
+    dump_cell(j, s->cell);
+    dump_groups(j, s->groups);
+
+    // Slater: one plane-wave block per spin group (builders/slater.cpp:267).
+    std::vector<SlaterDeterminant::Block> blocks;
+    j.key("slater");
+    j.open('[');
+    for (const ParticleGroup& g : s->groups) {
+        auto orb = make_plane_wave_orbitals(s->cell, g.size());
+        j.open('{');
+        j.ki("first", static_cast<long long>(g.first));
+        j.ki("last", static_cast<long long>(g.last));
+        j.ks("type", "plane_wave");
+        j.arr("k", orb->kvectors());
+        // is_sin is private; recover it from the shell table the factory used.
+        const ReciprocalShellTable t = reciprocal_shell_table(s->cell, g.size());
+        std::vector<double> is_sin(t.is_sin.begin(), t.is_sin.begin() + g.size());
+        j.arr("is_sin", is_sin);
+        j.close('}');
+        blocks.push_back({g.first, g.last, std::move(orb)});
+    }
+    j.close(']');
+    s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
+
+    // Padé on every group pair, a1 = 2 mu R/(2 l + d - 1) (builders/jastrow.cpp:48-63):
+    // same-spin pairs of a determinant group are P-wave (l = 1), opposite spins S-wave.
+    j.key("pade");
+    j.open('[');
+    for (std::size_t ga = 0; ga < s->groups.size(); ++ga)
+        for (std::size_t gb = ga; gb < s->groups.size(); ++gb) {
+            const ParticleGroup& A = s->groups[ga];
+            const ParticleGroup& B = s->groups[gb];
+            if (ga == gb && A.size() < 2) continue;
+            const double R = ew.coulomb_cusp_residue(A, B);
+            const int ell = ga == gb ? 1 : 0;
+            const double a1 = 2.0 * 0.5 * R / static_cast<double>(2 * ell + 2 - 1);
+            std::vector<Parameter> params{Parameter{"a1", a1, true},
+                                          Parameter{"pade_0", bden, false}};
+            auto pj = std::make_unique<PadeJastrow>(1, 1, A, B, params);
+            pj->sum_over_images(s->cell);
+            j.open('{');
+            j.arr("ga", std::vector<double>{double(A.first), double(A.last)});
+            j.arr("gb", std::vector<double>{double(B.first), double(B.last)});
+            j.arr("a", std::vector<double>{a1});
+            j.arr("b", std::vector<double>{bden});
+            dump_pade_image_sum(j, s->cell, {a1}, {bden});
+            j.close('}');
+            s->psi.add_component(std::move(pj));
+        }
+    j.close(']');
+
+    // Ewald tables (numerics/ewald_breakup.h:67-103).
+    const numerics::EwaldSetup& es = ew.setup();
+    j.key("ewald");
+    j.open('{');
+    j.kv("r_cut", es.r_cut);
+    dump_spline(j, "spline", es.long_range);
+    j.arr("n1", es.n1);
+    j.arr("n2", es.n2);
+    j.arr("kx", es.kx);
+    j.arr("ky", es.ky);
+    j.arr("weight", es.weight);
+    j.ki("n1_max", es.n1_max);
+    j.ki("n2_max", es.n2_max);
+    j.kv("inv_eps", 1.0);
+    j.kv("self_energy", ew.self_energy());
+    j.kv("background_energy", ew.background_energy());
+    j.kv("v_long_zero", es.v_long_zero);
+    j.kv("sr_k0", es.sr_k0);
+    j.close('}');
+    j.close('}');
+    s->ham.add_component(std::move(ewald));
+    return s;
+}
+
+// 2D Wigner crystal: Gaussian orbitals at explicit sites (a triangular lattice
+// in a rectangular cell, alternate rows per spin), Drummond Jastrow (C = 3),
+// Ewald.  Initial positions: sites plus Gaussian jitter.
+std::unique_ptr<System> build_crystal(const Args& a) {
+    auto s = std::make_unique<System>();
+    s->kind = "crystal";
+    const int nx = static_cast<int>(geti(a, "nx", 10));
+    const int ny = static_cast<int>(geti(a, "ny", 12));   // even
+    const double rs = getd(a, "rs", 40.0);
+    const double calpha = getd(a, "calpha", 0.1);
+    const double tol = getd(a, "tol", 1e-6);
+    const double alpha0 = getd(a, "alpha0", 0.0);
+    const double pi = 3.14159265358979323846;
+    const std::size_t N = static_cast<std::size_t>(nx * ny);
+    const std::size_t nu = N / 2, nd = N - nu;
+    s->dim = 2;
+    s->np = N;
+    const double alat = rs * std::sqrt(2.0 * pi / std::sqrt(3.0));
+    const double Lx = nx * alat, Ly = ny * alat * std::sqrt(3.0) / 2.0;
+    s->cell = SimulationCell(2, std::vector<double>{Lx, 0.0, 0.0, Ly});
+    s->groups.push_back(make_group("up", 0, nu, -1.0, 2));
+    s->groups.push_back(make_group("down", nu, nd, -1.0, 2));
+    // Sites: row r, column c at ((c + (r%2)/2) a, r a sqrt3/2), shifted to the
+    // centred cell; even rows carry spin up, odd rows spin down.
+    std::vector<double> up_c, dn_c;
+    for (int r = 0; r < ny; ++r)
+        for (int c = 0; c < nx; ++c) {
+            const double x = (c + 0.5 * (r % 2)) * alat - 0.5 * Lx;
+            const double y = r * alat * std::sqrt(3.0) / 2.0 - 0.5 * Ly;
+            auto& dst = (r % 2 == 0) ? up_c : dn_c;
+            dst.push_back(x);
+            dst.push_back(y);
+        }
+    const double alpha = calpha / (rs * rs);
+    s->anchors = up_c;
+    s->anchors.insert(s->anchors.end(), dn_c.begin(), dn_c.end());
+    s->jitter = getd(a, "jitter", 1.0 / std::sqrt(4.0 * alpha));
+
+    s->ham.add_component(std::make_unique<Kinetic>(s->groups));
+    auto ewald = std::make_unique<EwaldTerm>(s->groups, 1.0, s->cell, tol);
+    const EwaldTerm& ew = *ewald;
+
+    Json& j = s->setup;
+    j.open('{');
+    j.ks("kind", "crystal");
+    j.ki("dim", 2);
+    j.ki("np", static_cast<long long>(s->np));
+    dump_cell(j, s->cell);
+    dump_groups(j, s->groups);
+    std::vector<SlaterDeterminant::Block> blocks;
+    j.key("slater");
+    j.open('[');
+    for (std::size_t gi = 0; gi < 2; ++gi) {
+        const ParticleGroup& g = s->groups[gi];
+        const std::vector<double>& cen = gi == 0 ? up_c : dn_c;
+        std::vector<double> al(g.size(), alpha);
+        j.open('{');
+        j.ki("first", static_cast<long long>(g.first));
+        j.ki("last", static_cast<long long>(g.last));
+        j.ks("type", "gaussian");
+        j.arr("centers", cen);
+        j.arr("alphas", al);
+        j.close('}');
+        blocks.push_back({g.first, g.last,
+                          std::make_unique<GaussianOrbitalSet>(2, cen, al, s->cell)});
+    }
+    j.close(']');
+    s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
+
+    // Drummond: same-spin pairs (l = 1) in one item, opposite spins (l = 0) in another.
+    const double Lcut = getd(a, "cutoff", 0.999 * s->cell.ws_radius());
+    j.key("drummond");
+    j.open('[');
+    for (int item = 0; item < 2; ++item) {
+        std::vector<JastrowGroupPair> pairs;
+        if (item == 0) {
+            pairs.push_back({s->groups[0], s->groups[0]});
+            pairs.push_back({s->groups[1], s->groups[1]});
+        } else {
+            pairs.push_back({s->groups[0], s->groups[1]});
+        }
+        const double R = ew.coulomb_cusp_residue(pairs[0].a, pairs[0].b);
+        const double gamma = 2.0 * 0.5 * R / static_cast<double>(2 * (item == 0 ? 1 : 0) + 1);
+        std::vector<Parameter> params{Parameter{"p0", alpha0, true},
+                                      Parameter{"L", Lcut, true, true}};
+        auto dj = std::make_unique<DrummondJastrow>(3, gamma, pairs, params);
+        j.open('{');
+        j.ki("C", 3);
+        j.kv("gamma", gamma);
+        j.kv("L", Lcut);
+        j.arr("coeffs", std::vector<double>{alpha0});
+        j.key("pairs");
+        j.open('[');
+        for (const auto& p : pairs)
+            j.arr("", std::vector<double>{double(p.a.first), double(p.a.last),
+                                          double(p.b.first), double(p.b.last)});
+        j.close(']');
+        j.close('}');
+        s->psi.add_component(std::move(dj));
+    }
+    j.close(']');
+    const numerics::EwaldSetup& es = ew.setup();
+    j.key("ewald");
+    j.open('{');
+    j.kv("r_cut", es.r_cut);
+    dump_spline(j, "spline", es.long_range);
+    j.arr("n1", es.n1);
+    j.arr("n2", es.n2);
+    j.arr("kx", es.kx);
+    j.arr("ky", es.ky);
+    j.arr("weight", es.weight);
+    j.ki("n1_max", es.n1_max);
+    j.ki("n2_max", es.n2_max);
+    j.kv("inv_eps", 1.0);
+    j.kv("self_energy", ew.self_energy());
+    j.kv("background_energy", ew.background_energy());
+    j.kv("v_long_zero", es.v_long_zero);
+    j.kv("sr_k0", es.sr_k0);
+    j.close('}');
+    j.arr("anchors", s->anchors);
+    j.kv("jitter", s->jitter);
+    j.close('}');
+    s->ham.add_component(std::move(ewald));
+    return s;
+}
+
+// Open 2D exciton: one electron, one hole, u = a1 r with a1 = -1 (the exact
+// ground state, tests/configs/exciton_2d_cusp_m1.yaml), open Coulomb.
+std::unique_ptr<System> build_exciton(const Args& a) {
+    auto s = std::make_unique<System>();
+    s->kind = "exciton";
+    s->dim = 2;
+    s->np = 2;
+    s->cell = SimulationCell(2);
+    s->L_open = getd(a, "L", 1.0);
+    s->groups.push_back(make_group("electron_group", 0, 1, -1.0, 2));
+    s->groups.push_back(make_group("hole_group", 1, 1, 1.0, 2));
+    s->ham.add_component(std::make_unique<Kinetic>(s->groups));
+    s->ham.add_component(std::make_unique<CoulombTerm>(s->groups[0], s->groups[1], 1.0));
+    const double a1 = 2.0 * 0.5 * (-1.0) / 1.0;
+    std::vector<Parameter> params{Parameter{"a1", a1, true}};
+    s->psi.add_component(
+        std::make_unique<PadeJastrow>(1, 0, s->groups[0], s->groups[1], params));
+    Json& j = s->setup;
+    j.open('{');
+    j.ks("kind", "exciton");
+    j.ki("dim", 2);
+    j.ki("np", 2);
+    dump_cell(j, s->cell);
+    dump_groups(j, s->groups);
+    j.key("pade");
+    j.open('[');
+    j.open('{');
+    j.arr("ga", std::vector<double>{0, 1});
+    j.arr("gb", std::vector<double>{1, 2});
+    j.arr("a", std::vector<double>{a1});
+    j.arr("b", std::vector<double>{});
+    j.close('}');
+    j.close(']');
+    j.key("coulomb");
+    j.open('[');
+    j.open('{');
+    j.arr("ga", std::vector<double>{0, 1});
+    j.arr("gb", std::vector<double>{1, 2});
+    j.kv("coef", -1.0);
+    j.close('}');
+    j.close(']');
+    j.kv("L_open", s->L_open);
+    j.close('}');
+    return s;
+}
+
+std::unique_ptr<System> build_system(const Args& a) {
+    const std::string k = gets(a, "system", "heg");
+    if (k == "heg") return build_heg(a);
+    if (k == "crystal") return build_crystal(a);
+    if (k == "exciton") return build_exciton(a);
+    throw std::runtime_error("unknown system " + k);
+}
+
+// Initial positions with the reference App's semantics (app.cpp:56-112):
+// numerics::Random (mt19937_64) in walker, particle, dimension order; uniform
+// fractional coordinates in [-1/2, 1/2) mapped through the cell vectors,
+// uniform in [-L/2, L/2) for an open cell, or anchor + jitter * N(0, 1).
+void initialize(WalkerEnsemble& ens, const System& s, std::uint64_t seed) {
+    numerics::Random rng(seed);
+    const std::size_t np = s.np, dim = s.dim;
+    const auto av = s.cell.vectors();
+    std::vector<double> pos(np * dim);
+    for (Walker& w : ens.walkers()) {
+        for (std::size_t p = 0; p < np; ++p) {
+            if (!s.anchors.empty()) {
+                for (std::size_t d = 0; d < dim; ++d)
+                    pos[p * dim + d] = s.anchors[p * dim + d] + s.jitter * rng.gaussian();
+            } else if (s.cell.is_periodic()) {
+                double f[3];
+                for (std::size_t i = 0; i < dim; ++i) f[i] = rng.uniform(-0.5, 0.5);
+                for (std::size_t d = 0; d < dim; ++d) {
+                    double acc = 0.0;
+                    for (std::size_t i = 0; i < dim; ++i) acc += f[i] * av[i * dim + d];
+                    pos[p * dim + d] = acc;
+                }
+            } else {
+                for (std::size_t d = 0; d < dim; ++d)
+                    pos[p * dim + d] = rng.uniform(-0.5 * s.L_open, 0.5 * s.L_open);
+            }
+        }
+        w.set_positions(pos);
+    }
+}
+
+void put_positions(Json& j, const std::string& k, const WalkerEnsemble& ens) {
+    j.key(k);
+    j.open('[');
+    for (const Walker& w : ens.walkers()) j.arr("", w.positions());
+    j.close(']');
+}
+
+// Array with no key (the writer's "arr" with an empty key writes `"":`); used
+// inside lists, so strip that.
+std::string fix_empty_keys(std::string s) {
+    std::string out;
+    out.reserve(s.size());
+    for (std::size_t i = 0; i < s.size(); ++i) {
+        if (s.compare(i, 3, "\"\":") == 0) {
+            i += 2;
+            continue;
+        }
+        out += s[i];
+    }
+    return out;
+}
+
+int run(const std::string& mode, const Args& a) {
+    auto sys = build_system(a);
+    const std::size_t nw = static_cast<std::size_t>(geti(a, "nw", 4));
+    const std::uint64_t seed = static_cast<std::uint64_t>(geti(a, "seed", 12345));
+    const std::uint64_t init_seed = static_cast<std::uint64_t>(geti(a, "init_seed", seed));
+
+    if (mode == "setup") {
+        std::printf("%s\n", fix_empty_keys(sys->setup.s).c_str());
+        return 0;
+    }
+    WalkerEnsemble ens(nw, sys->groups, sys->dim, sys->cell);
+    initialize(ens, *sys, init_seed);
+
+    Json out;
+    out.open('{');
+    out.ks("mode", mode);
+    if (mode == "init") {
+        put_positions(out, "positions", ens);
+    } else if (mode == "eval") {
+        WalkerSet ws(nw, sys->np, sys->dim, sys->cell);
+        for (Walker& w : ens.walkers()) ws.add_walker(w);
+        ws.load_all();
+        TrialWavefunction psi = sys->psi.clone();
+        Hamiltonian ham = sys->ham.clone();
+        psi.evaluate_batch(ws);
+        ham.evaluate_batch(ws);
+        put_positions(out, "positions", ens);
+        out.arr("log_psi", ws.log_psi());
+        out.arr("local_energy", ws.local_energies());
+        out.arr("grad", ws.gradients());
+        out.arr("lap", ws.laplacians());
+        out.key("component_log_psi");
+        out.open('[');
+        for (const auto& c : psi.components()) out.arr("", c->log_psi_c());
+        out.close(']');
+        // Kinetic alone, to separate the potential.
+        Hamiltonian kin;
+        kin.add_component(std::make_unique<Kinetic>(sys->groups));
+        kin.evaluate_batch(ws);
+        out.arr("kinetic", ws.local_energies());
+    } else if (mode == "vmc") {
+        VMCConfig c;
+        c.n_equilibration_blocks = static_cast<int>(geti(a, "eq", 0));
+        c.n_accumulation_blocks = static_cast<int>(geti(a, "acc", 2));
+        c.n_steps = static_cast<int>(geti(a, "steps", 3));
+        c.n_substeps = static_cast<int>(geti(a, "substeps", 1));
+        c.tau = getd(a, "tau", 1.0);
+        c.use_drift = geti(a, "drift", 0) != 0;
+        c.n_threads = static_cast<int>(geti(a, "threads", static_cast<long long>(nw)));
+        c.seed = seed;
+        const int T = std::min<int>(c.n_threads, static_cast<int>(nw));
+        put_positions(out, "initial_positions", ens);
+        VMC vmc(c, ens, sys->psi, sys->ham);
+        std::vector<std::vector<double>> el(static_cast<std::size_t>(T));
+        vmc.set_measure_hook([&](const WalkerSet& ws, const TrialWavefunction&) {
+            auto& v = el[static_cast<std::size_t>(omp_get_thread_num())];
+            for (double e : ws.local_energies()) v.push_back(e);
+        });
+        vmc.run();
+        out.kv("energy", vmc.energy());
+        out.kv("energy_error", vmc.energy_error());
+        out.kv("variance", vmc.energy_variance());
+        out.kv("acceptance", vmc.acceptance_ratio());
+        out.ki("threads", T);
+        out.key("thread_local_energy");
+        out.open('[');
+        for (const auto& v : el) out.arr("", v);
+        out.close(']');
+        out.arr("final_positions", vmc.final_configurations());
+        out.arr("block_energies", vmc.block_energies());
+    } else if (mode == "dmc" || mode == "bench") {
+        const bool bench = mode == "bench";
+        const std::string method = gets(a, "method", "dmc");
+        const int host_threads = omp_get_max_threads();
+        if (bench && method == "vmc") {
+            VMCConfig c;
+            c.n_equilibration_blocks = 0;
+            c.n_accumulation_blocks = 1;
+            c.n_steps = static_cast<int>(geti(a, "steps", 2));
+            c.n_substeps = 1;
+            c.tau = getd(a, "tau", 1.0);
+            c.n_threads = static_cast<int>(geti(a, "threads", host_threads));
+            c.seed = seed;
+            VMC vmc(c, ens, sys->psi, sys->ham);
+            std::vector<double> stamps;
+            vmc.set_measure_hook([&](const WalkerSet&, const TrialWavefunction&) {
+                if (omp_get_thread_num() == 0)
+                    stamps.push_back(std::chrono::duration<double>(
+                        std::chrono::steady_clock::now().time_since_epoch()).count());
+            });
+            vmc.run();
+            out.ki("threads", c.n_threads);
+            out.arr("stamps", stamps);
+            out.kv("acceptance", vmc.acceptance_ratio());
+        } else {
+            DMCConfig c;
+            c.n_equilibration_blocks = static_cast<int>(geti(a, "eq", 0));
+            c.n_accumulation_blocks = static_cast<int>(geti(a, "acc", 1));
+            c.n_steps = static_cast<int>(geti(a, "steps", 3));
+            c.n_substeps = static_cast<int>(geti(a, "substeps", 1));
+            c.tau = getd(a, "tau", 0.5);
+            c.n_threads = static_cast<int>(
+                geti(a, "threads", bench ? host_threads : static_cast<long long>(nw)));
+            c.seed = seed;
+            c.population_generations = getd(a, "generations", 10.0);
+            if (!bench) put_positions(out, "initial_positions", ens);
+            DMC dmc(c, ens, sys->psi, sys->ham);
+            std::vector<double> stamps, wsum, ewsum;
+            std::vector<std::vector<double>> el, wt, ids;
+            dmc.set_measure_hook([&](const WalkerSet& ws, const TrialWavefunction&) {
+                stamps.push_back(std::chrono::duration<double>(
+                    std::chrono::steady_clock::now().time_since_epoch()).count());
+                double sw = 0.0, se = 0.0;
+                for (std::size_t w = 0; w < ws.num_walkers(); ++w) {
+                    sw += ws.weights()[w];
+                    se += ws.weights()[w] * ws.local_energies()[w];
+                }
+                wsum.push_back(sw);
+                ewsum.push_back(se);
+                if (!bench) {
+                    el.emplace_back(ws.local_energies().begin(), ws.local_energies().end());
+                    wt.emplace_back(ws.weights().begin(), ws.weights().end());
+                    ids.emplace_back(ws.ids().begin(), ws.ids().end());
+                }
+            });
+            const auto t0 = std::chrono::steady_clock::now();
+            dmc.run();
+            const double wall =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            out.ki("threads", c.n_threads);
+            out.kv("wall", wall);
+            out.arr("stamps", stamps);
+            out.arr("weight_sum", wsum);
+            out.arr("weighted_energy_sum", ewsum);
+            out.ks("summary_first_line", "");
+            if (!bench) {
+                out.key("local_energy");
+                out.open('[');
+                for (const auto& v : el) out.arr("", v);
+                out.close(']');
+                out.key("weights");
+                out.open('[');
+                for (const auto& v : wt) out.arr("", v);
+                out.close(']');
+                out.key("ids");
+                out.open('[');
+                for (const auto& v : ids) out.arr("", v);
+                out.close(']');
+                out.arr("final_positions", dmc.final_configurations());
+            }
+        }
+    } else {
+        throw std::runtime_error("unknown mode " + mode);
+    }
+    out.close('}');
+    std::printf("%s\n", fix_empty_keys(out.s).c_str());
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: ref_harness MODE key=value...\n");
+        return 2;
+    }
+    Args a;
+    for (int i = 2; i < argc; ++i) {
+        const std::string s = argv[i];
+        const auto eq = s.find('=');
+        if (eq == std::string::npos) {
+            std::fprintf(stderr, "bad argument %s\n", s.c_str());
+            return 2;
+        }
+        a[s.substr(0, eq)] = s.substr(eq + 1);
+    }
+    try {
+        return run(argv[1], a);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_harness: %s\n", e.what());
+        return 1;
+    }
+}
