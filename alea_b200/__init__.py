@@ -1,0 +1,288 @@
+"""alea_b200 — B200-native VMC/DMC walker hot path for Alea.
+
+The walker ensemble lives in HBM; every sweep, local energy and branching
+gather runs in the sm_100a kernels of ``libalea_b200.so`` behind the C ABI of
+``include/alea_gpu.h``.  This module is the thin Python view of that ABI used
+by tests and the benchmark; C/C++ hosts call the ABI directly.
+
+A system is described by a plain dict (the schema of ``setup.describe_*``,
+see ``alea_b200/setup.py``): cell, particle groups, determinant blocks with
+their orbitals, pair Jastrows (Padé with image-sum tables, Drummond), Ewald
+tables and open Coulomb terms.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Any, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import load as _load
+
+__all__ = ["Walkers", "AleaGpuError", "pack_system", "STREAM_VMC", "STREAM_DMC", "STREAM_BRANCH"]
+
+STREAM_VMC = _capi.STREAM_VMC
+STREAM_DMC = _capi.STREAM_DMC
+STREAM_BRANCH = _capi.STREAM_BRANCH
+
+
+class AleaGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"alea_gpu error {code} ({_capi.ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_capi.c_dp)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_capi.c_ip)
+
+
+def pack_system(desc: Dict[str, Any]):
+    """alea_gpu_system from a description dict.  Returns (struct, keepalive)."""
+    keep: List[np.ndarray] = []
+
+    def f64(x):
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+        keep.append(a)
+        return a
+
+    def i32(x):
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.int32))
+        keep.append(a)
+        return a
+
+    s = _capi.System()
+    s.dim = int(desc["dim"])
+    s.n_particles = int(desc["np"])
+    cell = desc["cell"]
+    s.periodic = int(cell["periodic"])
+    if s.periodic:
+        for i, v in enumerate(cell["vectors"]):
+            s.lattice[i] = float(v)
+    groups = desc["groups"]
+    s.n_groups = len(groups)
+    for i, g in enumerate(groups):
+        G = s.groups[i]
+        G.first, G.last, G.charge = int(g["first"]), int(g["last"]), float(g["charge"])
+        for d, v in enumerate(g["inv_mass"]):
+            G.inv_mass[d] = float(v)
+    blocks = desc.get("slater", [])
+    s.n_blocks = len(blocks)
+    for i, b in enumerate(blocks):
+        B = s.blocks[i]
+        B.first, B.last = int(b["first"]), int(b["last"])
+        if b["type"] == "plane_wave":
+            B.type = _capi.ORB_PLANE_WAVE
+            B.k = _dp(f64(b["k"]))
+            B.is_sin = _ip(i32(b["is_sin"]))
+        else:
+            B.type = _capi.ORB_GAUSSIAN
+            B.centers = _dp(f64(b["centers"]))
+            B.alphas = _dp(f64(b["alphas"]))
+    terms = []
+    for p in desc.get("pade", []):
+        terms.append(("pade", p))
+    for d in desc.get("drummond", []):
+        terms.append(("drummond", d))
+    s.n_terms = len(terms)
+    for i, (kind, t) in enumerate(terms):
+        T = s.terms[i]
+        if kind == "pade":
+            T.kind = _capi.PAIR_PADE
+            T.n_pairs = 1
+            pr = [int(t["ga"][0]), int(t["ga"][1]), int(t["gb"][0]), int(t["gb"][1])]
+            for k in range(4):
+                T.pairs[0][k] = pr[k]
+            a, b = list(t["a"]), list(t["b"])
+            T.num_order, T.den_order = len(a), len(b)
+            for k, v in enumerate(a + b):
+                T.coeffs[k] = float(v)
+            im = t.get("image_sum")
+            T.image_sum = 1 if im else 0
+            if im:
+                sp = im["spline"]
+                T.short_range.r_cut = float(sp["r_cut"])
+                T.short_range.inv_delta = float(sp["inv_delta"])
+                T.short_range.n_knots = int(sp["n_knots"])
+                T.short_range.scaled = _dp(f64(sp["scaled"]))
+                T.u_inf = float(im["u_inf"])
+                T.kset.n_k = len(im["weight"])
+                T.kset.n1 = _ip(i32(im["n1"]))
+                T.kset.n2 = _ip(i32(im["n2"]))
+                T.kset.kx = _dp(f64(im["kx"]))
+                T.kset.ky = _dp(f64(im["ky"]))
+                T.kset.weight = _dp(f64(im["weight"]))
+        else:
+            T.kind = _capi.PAIR_DRUMMOND
+            T.n_pairs = len(t["pairs"])
+            for q, pr in enumerate(t["pairs"]):
+                for k in range(4):
+                    T.pairs[q][k] = int(pr[k])
+            T.C = int(t["C"])
+            T.gamma = float(t["gamma"])
+            T.L = float(t["L"])
+            T.n_coeffs = len(t["coeffs"])
+            for k, v in enumerate(t["coeffs"]):
+                T.dcoeffs[k] = float(v)
+    ew = desc.get("ewald")
+    if ew:
+        E = s.ewald
+        E.enabled = 1
+        E.r_cut = float(ew["r_cut"])
+        E.inv_eps = float(ew.get("inv_eps", 1.0))
+        E.constant = float(ew["self_energy"]) + float(ew.get("background_energy", 0.0))
+        sp = ew["spline"]
+        E.long_range.r_cut = float(sp["r_cut"])
+        E.long_range.inv_delta = float(sp["inv_delta"])
+        E.long_range.n_knots = int(sp["n_knots"])
+        E.long_range.scaled = _dp(f64(sp["scaled"]))
+        E.kset.n_k = len(ew["weight"])
+        E.kset.n1 = _ip(i32(ew["n1"]))
+        E.kset.n2 = _ip(i32(ew["n2"]))
+        E.kset.kx = _dp(f64(ew["kx"]))
+        E.kset.ky = _dp(f64(ew["ky"]))
+        E.kset.weight = _dp(f64(ew["weight"]))
+    cl = desc.get("coulomb", [])
+    s.n_coulomb = len(cl)
+    for i, c in enumerate(cl):
+        C = s.coulomb[i]
+        C.a_first, C.a_last = int(c["ga"][0]), int(c["ga"][1])
+        C.b_first, C.b_last = int(c["gb"][0]), int(c["gb"][1])
+        C.coef = float(c["coef"])
+    return s, keep
+
+
+class Walkers:
+    """A context on one device holding up to ``capacity`` walkers of a system."""
+
+    def __init__(self, desc: Dict[str, Any], capacity: int, device: int = 0):
+        self.lib = _load()
+        self.desc = desc
+        self.np = int(desc["np"])
+        self.dim = int(desc["dim"])
+        sysc, keep = pack_system(desc)
+        ctx = ctypes.c_void_p()
+        rc = self.lib.alea_gpu_create(ctypes.byref(sysc), device, int(capacity), ctypes.byref(ctx))
+        if rc != 0:
+            raise AleaGpuError(rc, self.lib.alea_gpu_last_error(None).decode())
+        self.ctx = ctx
+        self.capacity = int(capacity)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.alea_gpu_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise AleaGpuError(rc, self.lib.alea_gpu_last_error(self.ctx).decode())
+
+    @property
+    def nw(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.alea_gpu_num_walkers(self.ctx, ctypes.byref(n)))
+        return n.value
+
+    def upload(self, positions_aos: np.ndarray) -> None:
+        """Walkers from AoS positions [w][p][d]; evaluates ψ and E_L."""
+        pos = np.asarray(positions_aos, dtype=np.float64).reshape(-1, self.np * self.dim)
+        nw = pos.shape[0]
+        soa = np.ascontiguousarray(pos.T)   # [p*dim + d][w]
+        self._check(self.lib.alea_gpu_upload_walkers(self.ctx, _dp(soa), nw))
+
+    def evaluate(self) -> None:
+        self._check(self.lib.alea_gpu_evaluate(self.ctx))
+
+    def measure(self) -> None:
+        self._check(self.lib.alea_gpu_measure(self.ctx))
+
+    def download(self) -> Dict[str, np.ndarray]:
+        nw = self.nw
+        n = self.np * self.dim
+        pos = np.zeros(n * nw)
+        grad = np.zeros(n * nw)
+        lap = np.zeros(n * nw)
+        lp = np.zeros(nw)
+        el = np.zeros(nw)
+        w = np.zeros(nw)
+        self._check(self.lib.alea_gpu_download_walkers(self.ctx, _dp(pos), _dp(lp), _dp(grad),
+                                                       _dp(lap), _dp(el), _dp(w)))
+        return {
+            "positions": pos.reshape(n, nw).T.copy(),
+            "grad": grad.reshape(n, nw).T.copy(),
+            "lap": lap.reshape(n, nw).T.copy(),
+            "log_psi": lp, "local_energy": el, "weights": w,
+        }
+
+    def move(self, p: int, new_pos_aos: np.ndarray, accept: Optional[Sequence[bool]] = None):
+        """Single-particle move of p for every walker; new_pos_aos [w][d]."""
+        nw = self.nw
+        npos = np.ascontiguousarray(np.asarray(new_pos_aos, dtype=np.float64).reshape(nw, self.dim).T)
+        lr = np.zeros(nw)
+        ph = np.zeros(nw)
+        ng = np.zeros(self.dim * nw)
+        nl = np.zeros(self.dim * nw)
+        if accept is not None:
+            mask = np.ascontiguousarray(np.asarray(accept, dtype=np.uint8))
+            mp = mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        else:
+            mp = None
+        self._check(self.lib.alea_gpu_move(self.ctx, int(p), _dp(npos), mp, _dp(lr), _dp(ph),
+                                           _dp(ng), _dp(nl)))
+        return lr, ph, ng.reshape(self.dim, nw).T, nl.reshape(self.dim, nw).T
+
+    def set_streams(self, seed: int, kind: int, n: int) -> None:
+        self._check(self.lib.alea_gpu_set_streams(self.ctx, ctypes.c_uint64(seed),
+                                                  ctypes.c_uint64(kind), int(n)))
+
+    def vmc_step(self, tau: float, n_substeps: int = 1, drift: bool = False) -> _capi.StepStats:
+        prm = _capi.VmcParams(tau, n_substeps, 1 if drift else 0)
+        st = _capi.StepStats()
+        self._check(self.lib.alea_gpu_vmc_step(self.ctx, ctypes.byref(prm), ctypes.byref(st)))
+        return st
+
+    def dmc_advance(self, tau, n_substeps, e_trial, e_ref, e_cut, e_max) -> _capi.StepStats:
+        prm = _capi.DmcParams(tau, n_substeps, e_trial, e_ref, e_cut, e_max)
+        st = _capi.StepStats()
+        self._check(self.lib.alea_gpu_dmc_advance(self.ctx, ctypes.byref(prm), ctypes.byref(st)))
+        return st
+
+    def dmc_branch(self, state: np.ndarray, target: int) -> None:
+        st = np.ascontiguousarray(state, dtype=np.uint64)
+        self._check(self.lib.alea_gpu_dmc_branch(self.ctx, st.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_uint64)), int(target)))
+        state[:] = st
+
+    def last_kernel_ms(self) -> float:
+        v = ctypes.c_double()
+        self._check(self.lib.alea_gpu_last_kernel_ms(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def _run(self, fn, n_eq, n_acc, n_steps, n_substeps, tau, streams, seed, drift=False,
+             target=0, generations=10.0, alpha=2.0, n_blocks_out=0):
+        cfg = _capi.RunConfig(n_eq, n_acc, n_steps, n_substeps, tau, 1 if drift else 0, streams,
+                              ctypes.c_uint64(seed), target, generations, alpha)
+        res = _capi.RunResult()
+        blocks = np.zeros(max(n_blocks_out, 1))
+        self._check(fn(self.ctx, ctypes.byref(cfg), ctypes.byref(res), _dp(blocks)))
+        return res, blocks[:n_blocks_out]
+
+    def vmc_run(self, n_eq, n_acc, n_steps, n_substeps, tau, streams, seed, drift=False):
+        T = min(streams, self.nw)
+        return self._run(self.lib.alea_gpu_vmc_run, n_eq, n_acc, n_steps, n_substeps, tau, streams,
+                         seed, drift=drift, n_blocks_out=T * n_acc)
+
+    def dmc_run(self, n_eq, n_acc, n_steps, n_substeps, tau, streams, seed, target=0,
+                generations=10.0):
+        return self._run(self.lib.alea_gpu_dmc_run, n_eq, n_acc, n_steps, n_substeps, tau,
+                         streams, seed, target=target, generations=generations, n_blocks_out=n_acc)

@@ -1,0 +1,153 @@
+"""ctypes binding of the C ABI in include/alea_gpu.h (libalea_b200.so).
+
+The structures below mirror the header field for field.  The library is
+built in-tree (``python -m alea_b200.build``); importing this module on a
+machine without it raises ImportError rather than falling back to anything.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libalea_b200.so")
+
+ALEA_OK = 0
+ERRORS = {1: "invalid", 2: "cuda", 3: "unsupported", 4: "singular", 5: "timeout", 6: "nomem"}
+ORB_PLANE_WAVE, ORB_GAUSSIAN = 0, 1
+PAIR_PADE, PAIR_DRUMMOND = 0, 1
+STREAM_VMC = 0x766D632D74687264
+STREAM_DMC = 0x646D632D74687264
+STREAM_BRANCH = 0x646D632D62726368
+
+c_dp = ctypes.POINTER(ctypes.c_double)
+c_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Spline(ctypes.Structure):
+    _fields_ = [("r_cut", ctypes.c_double), ("inv_delta", ctypes.c_double),
+                ("n_knots", ctypes.c_int), ("scaled", c_dp)]
+
+
+class KSet(ctypes.Structure):
+    _fields_ = [("n_k", ctypes.c_int), ("n1", c_ip), ("n2", c_ip), ("kx", c_dp),
+                ("ky", c_dp), ("weight", c_dp)]
+
+
+class Group(ctypes.Structure):
+    _fields_ = [("first", ctypes.c_int), ("last", ctypes.c_int), ("charge", ctypes.c_double),
+                ("inv_mass", ctypes.c_double * 3)]
+
+
+class Orbitals(ctypes.Structure):
+    _fields_ = [("first", ctypes.c_int), ("last", ctypes.c_int), ("type", ctypes.c_int),
+                ("k", c_dp), ("is_sin", c_ip), ("centers", c_dp), ("alphas", c_dp)]
+
+
+class PairTerm(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("n_pairs", ctypes.c_int),
+                ("pairs", (ctypes.c_int * 4) * 4), ("num_order", ctypes.c_int),
+                ("den_order", ctypes.c_int), ("coeffs", ctypes.c_double * 16),
+                ("image_sum", ctypes.c_int), ("short_range", Spline), ("u_inf", ctypes.c_double),
+                ("kset", KSet), ("C", ctypes.c_int), ("gamma", ctypes.c_double),
+                ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int),
+                ("dcoeffs", ctypes.c_double * 16)]
+
+
+class Ewald(ctypes.Structure):
+    _fields_ = [("enabled", ctypes.c_int), ("r_cut", ctypes.c_double),
+                ("inv_eps", ctypes.c_double), ("constant", ctypes.c_double),
+                ("long_range", Spline), ("kset", KSet)]
+
+
+class Coulomb(ctypes.Structure):
+    _fields_ = [("a_first", ctypes.c_int), ("a_last", ctypes.c_int), ("b_first", ctypes.c_int),
+                ("b_last", ctypes.c_int), ("coef", ctypes.c_double)]
+
+
+class System(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("n_particles", ctypes.c_int), ("periodic", ctypes.c_int),
+                ("lattice", ctypes.c_double * 9), ("n_groups", ctypes.c_int),
+                ("groups", Group * 8), ("n_blocks", ctypes.c_int), ("blocks", Orbitals * 4),
+                ("n_terms", ctypes.c_int), ("terms", PairTerm * 8), ("ewald", Ewald),
+                ("n_coulomb", ctypes.c_int), ("coulomb", Coulomb * 8)]
+
+
+class VmcParams(ctypes.Structure):
+    _fields_ = [("tau", ctypes.c_double), ("n_substeps", ctypes.c_int), ("use_drift", ctypes.c_int)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("energy_sum", ctypes.c_double), ("energy_sq_sum", ctypes.c_double),
+                ("weight_sum", ctypes.c_double), ("n_accepted", ctypes.c_int64),
+                ("n_proposed", ctypes.c_int64), ("n_cut", ctypes.c_int64),
+                ("n_walkers", ctypes.c_int)]
+
+
+class DmcParams(ctypes.Structure):
+    _fields_ = [("tau", ctypes.c_double), ("n_substeps", ctypes.c_int),
+                ("e_trial", ctypes.c_double), ("e_ref", ctypes.c_double),
+                ("e_cut", ctypes.c_double), ("e_max", ctypes.c_double)]
+
+
+class RunConfig(ctypes.Structure):
+    _fields_ = [("n_equilibration_blocks", ctypes.c_int), ("n_accumulation_blocks", ctypes.c_int),
+                ("n_steps", ctypes.c_int), ("n_substeps", ctypes.c_int), ("tau", ctypes.c_double),
+                ("use_drift", ctypes.c_int), ("n_streams", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("target_walkers", ctypes.c_int), ("population_generations", ctypes.c_double),
+                ("branch_cutoff_alpha", ctypes.c_double)]
+
+
+class RunResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("energy_error", ctypes.c_double),
+                ("variance", ctypes.c_double), ("acceptance", ctypes.c_double),
+                ("walltime_s", ctypes.c_double), ("n_walkers", ctypes.c_int),
+                ("e_trial", ctypes.c_double)]
+
+
+EXPORTS = [
+    "alea_gpu_abi_version", "alea_gpu_create", "alea_gpu_destroy", "alea_gpu_last_error",
+    "alea_gpu_upload_walkers", "alea_gpu_evaluate", "alea_gpu_num_walkers",
+    "alea_gpu_download_walkers", "alea_gpu_move", "alea_gpu_measure", "alea_gpu_set_streams",
+    "alea_gpu_vmc_step", "alea_gpu_dmc_advance", "alea_gpu_dmc_branch", "alea_gpu_vmc_run",
+    "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms",
+]
+
+_LIB = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libalea_b200.so and declare the ABI's signatures."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m alea_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    I, D = ctypes.c_int, ctypes.c_double
+    sig = {
+        "alea_gpu_abi_version": ([], I),
+        "alea_gpu_create": ([ctypes.POINTER(System), I, I, ctypes.POINTER(P)], I),
+        "alea_gpu_destroy": ([P], I),
+        "alea_gpu_last_error": ([P], ctypes.c_char_p),
+        "alea_gpu_upload_walkers": ([P, c_dp, I], I),
+        "alea_gpu_evaluate": ([P], I),
+        "alea_gpu_num_walkers": ([P, c_ip], I),
+        "alea_gpu_download_walkers": ([P, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp], I),
+        "alea_gpu_move": ([P, I, c_dp, ctypes.POINTER(ctypes.c_uint8), c_dp, c_dp, c_dp, c_dp], I),
+        "alea_gpu_measure": ([P], I),
+        "alea_gpu_set_streams": ([P, ctypes.c_uint64, ctypes.c_uint64, I], I),
+        "alea_gpu_vmc_step": ([P, ctypes.POINTER(VmcParams), ctypes.POINTER(StepStats)], I),
+        "alea_gpu_dmc_advance": ([P, ctypes.POINTER(DmcParams), ctypes.POINTER(StepStats)], I),
+        "alea_gpu_dmc_branch": ([P, ctypes.POINTER(ctypes.c_uint64), I], I),
+        "alea_gpu_vmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),
+        "alea_gpu_dmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),
+        "alea_gpu_last_kernel_ms": ([P, c_dp], I),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = lib
+    return lib

@@ -1,0 +1,1149 @@
+// C ABI of the B200 walker hot path (include/alea_gpu.h): context and device
+// buffers, the system description on the device, and the host halves of the
+// VMC/DMC drivers (population control, branching, statistics).
+//
+// Host algorithms restated from the reference (ItaloAlb/alea):
+//   streams        src/numerics/random.h:39-56, src/numerics/xoshiro_random.h:23-49
+//   ziggurat       src/numerics/xoshiro_random.h:110-175 (table construction)
+//   cell           src/population/simulation_cell.cpp:160-270
+//   VMC loop       src/qmc/vmc.cpp:23-62, :189-431
+//   DMC loop       src/qmc/dmc.cpp:525-884, src/qmc/population_control.cpp:37-103
+//   branching      src/population/walker_set.cpp:187-239
+//   spread         src/numerics/statistics.cpp:297-315
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/alea_gpu.h"
+#include "alea_dev.cuh"
+#include "alea_kernels.h"
+
+using namespace alea_gpu;
+
+namespace {
+
+std::string g_create_error;
+
+// ───────────────────────── host random numbers ─────────────────────────
+
+uint64_t splitmix64(uint64_t x) {
+    x += 0x9e3779b97f4a7c15ULL;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+    return x ^ (x >> 31);
+}
+uint64_t stream_seed(uint64_t base, uint64_t stream, uint64_t index) {
+    return splitmix64(splitmix64(splitmix64(base) ^ stream) ^ index);
+}
+struct HostXo {
+    uint64_t s[4];
+    explicit HostXo(uint64_t seed) {
+        for (uint64_t i = 0; i < 4; ++i) s[i] = splitmix64(seed + i * 0x9e3779b97f4a7c15ULL);
+    }
+    HostXo() : s{0, 0, 0, 0} {}
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {
+        const uint64_t result = rotl(s[0] + s[3], 23) + s[0];
+        const uint64_t t = s[1] << 17;
+        s[2] ^= s[0];
+        s[3] ^= s[1];
+        s[1] ^= s[2];
+        s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = rotl(s[3], 45);
+        return result;
+    }
+    double uniform() { return static_cast<double>(static_cast<int64_t>(next() >> 11)) * 0x1.0p-53; }
+};
+
+// Ziggurat tables of 256 equal-area regions under exp(-x²/2), 2⁵² fixed point
+// (Marsaglia & Tsang 2000; region/sign/position split after Doornik 2005):
+// the tail start r solves "the top layer closes at f = 1" by bisection.
+struct Ziggurat {
+    uint64_t k[256];
+    double w[256], f[256], r;
+};
+Ziggurat make_ziggurat() {
+    auto f = [](double x) { return std::exp(-0.5 * x * x); };
+    auto v_of = [&](double r) {
+        return r * f(r) + std::sqrt(0.5 * 3.14159265358979323846) * std::erfc(r / 1.41421356237309504880);
+    };
+    double x[256] = {};
+    auto mismatch = [&](double r) {
+        const double v = v_of(r);
+        x[255] = r;
+        for (int i = 255; i >= 2; --i) {
+            const double y = f(x[i]) + v / x[i];
+            if (y >= 1.0) return 1.0;
+            x[i - 1] = std::sqrt(-2.0 * std::log(y));
+        }
+        return f(x[1]) + v / x[1] - 1.0;
+    };
+    double lo = 3.0, hi = 4.5;
+    for (;;) {
+        const double mid = 0.5 * (lo + hi);
+        if (mid == lo || mid == hi) break;
+        (mismatch(mid) > 0.0 ? lo : hi) = mid;
+    }
+    Ziggurat z{};
+    z.r = hi;
+    (void)mismatch(z.r);
+    const double two52 = 0x1.0p52;
+    const double base = v_of(z.r) / f(z.r);
+    z.k[0] = static_cast<uint64_t>(two52 * (z.r / base));
+    z.w[0] = base / two52;
+    z.f[0] = 1.0;
+    for (int i = 1; i < 256; ++i) {
+        z.k[i] = i == 1 ? 0 : static_cast<uint64_t>(two52 * (x[i - 1] / x[i]));
+        z.w[i] = x[i] / two52;
+        z.f[i] = f(x[i]);
+    }
+    return z;
+}
+
+double median_in_place(std::vector<double>& v) {
+    const std::size_t n = v.size(), mid = n / 2;
+    std::nth_element(v.begin(), v.begin() + static_cast<std::ptrdiff_t>(mid), v.end());
+    const double upper = v[mid];
+    if (n % 2 == 1) return upper;
+    const double lower = *std::max_element(v.begin(), v.begin() + static_cast<std::ptrdiff_t>(mid));
+    return 0.5 * (lower + upper);
+}
+double robust_spread(const double* x, std::size_t n) {
+    if (n == 0) return 0.0;
+    std::vector<double> s(x, x + n);
+    const double centre = median_in_place(s);
+    for (std::size_t i = 0; i < n; ++i) s[i] = std::abs(x[i] - centre);
+    return 1.4826 * median_in_place(s);
+}
+
+// Flyvbjerg-Petersen blocking: standard error at each pairwise level; the
+// estimate is the largest one among levels that keep at least 8 blocks.
+void reblock(const std::vector<double>& series, double& mean, double& err) {
+    mean = 0.0;
+    err = 0.0;
+    if (series.empty()) return;
+    for (double x : series) mean += x;
+    mean /= static_cast<double>(series.size());
+    std::vector<double> cur = series;
+    while (cur.size() >= 8) {
+        const double n = static_cast<double>(cur.size());
+        double m = 0.0, v = 0.0;
+        for (double x : cur) m += x;
+        m /= n;
+        for (double x : cur) v += (x - m) * (x - m);
+        v /= (n - 1.0);
+        err = std::max(err, std::sqrt(v / n));
+        std::vector<double> next(cur.size() / 2);
+        for (std::size_t i = 0; i < next.size(); ++i) next[i] = 0.5 * (cur[2 * i] + cur[2 * i + 1]);
+        cur.swap(next);
+    }
+}
+
+}  // namespace
+
+// ───────────────────────── context ──────────────────────────────────────
+
+struct alea_gpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DevSys sys{};
+    void* arena = nullptr;
+    int capacity = 0, nw = 0;
+    double* rec[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* randoms = nullptr;
+    int rnd_sweeps = 0;
+    uint64_t* streams = nullptr;
+    int n_streams = 0, streams_cap = 0;
+    int2* pairs = nullptr;
+    int npair = 0;
+    double* d_buf = nullptr;       // staging [max(np*dim, 8) * capacity]
+    double* d_sigma = nullptr;     // [np*dim]
+    double sigma_tau = -1.0;
+    int* d_src = nullptr;
+    uint8_t* d_mask = nullptr;
+    size_t smem = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    std::vector<double> h_inv_mass;
+    std::vector<double> h_w, h_el, h_ids, h_par, h_nacc, h_ncut;
+    double next_id = 1.0;
+};
+
+namespace {
+
+int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                               \
+    do {                                                                                  \
+        cudaError_t e_ = (expr);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail((ctx), ALEA_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+long round4(long x) { return (x + 3) & ~3L; }
+
+// Cell from the lattice rows: axis alignment, 2-D Gauss reduction, (Aᵀ)⁻¹,
+// the orthorhombic fold, the 3×3 candidate shell, reciprocal vectors.
+int setup_cell(alea_gpu_ctx* c, const alea_gpu_system* in, DevSys& s) {
+    s.periodic = in->periodic;
+    s.ortho = 0;
+    if (!s.periodic) return ALEA_OK;
+    double a[4] = {in->lattice[0], in->lattice[1], in->lattice[2], in->lattice[3]};
+    // axis_align
+    int axis[2], used[2] = {0, 0};
+    bool aligned = true;
+    for (int i = 0; i < 2 && aligned; ++i) {
+        int nz = 0, which = 0;
+        for (int d = 0; d < 2; ++d)
+            if (a[i * 2 + d] != 0.0) {
+                ++nz;
+                which = d;
+            }
+        if (nz != 1 || used[which]) aligned = false;
+        else {
+            axis[i] = which;
+            used[which] = 1;
+        }
+    }
+    if (aligned) {
+        double r[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 2; ++i)
+            for (int d = 0; d < 2; ++d) r[axis[i] * 2 + d] = a[i * 2 + d];
+        std::memcpy(a, r, sizeof a);
+        s.ortho = 1;
+    } else {
+        for (int guard = 0; guard < 64; ++guard) {
+            const double n0 = a[0] * a[0] + a[1] * a[1], n1 = a[2] * a[2] + a[3] * a[3];
+            if (n1 < n0) {
+                std::swap(a[0], a[2]);
+                std::swap(a[1], a[3]);
+                continue;
+            }
+            if (n0 == 0.0) break;
+            const double mu = std::nearbyint((a[0] * a[2] + a[1] * a[3]) / n0);
+            if (mu == 0.0) break;
+            a[2] -= mu * a[0];
+            a[3] -= mu * a[1];
+        }
+    }
+    const double det = a[0] * a[3] - a[1] * a[2];
+    if (det == 0.0) return fail(c, ALEA_ERR_INVALID, "lattice vectors are singular");
+    const double inv_det = 1.0 / det;
+    std::memcpy(s.a, a, sizeof a);
+    s.ainv[0] = a[3] * inv_det;
+    s.ainv[1] = -a[2] * inv_det;
+    s.ainv[2] = -a[1] * inv_det;
+    s.ainv[3] = a[0] * inv_det;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int k = 0; k < 4; ++k) s.recip[k] = two_pi * s.ainv[k];
+    if (s.ortho)
+        for (int d = 0; d < 2; ++d) {
+            s.box[d] = std::abs(a[d * 2 + d]);
+            s.inv_box[d] = 1.0 / s.box[d];
+        }
+    int nc = 1;
+    s.cand[0] = s.cand[1] = 0.0;
+    if (!s.ortho)
+        for (int n0 = -1; n0 <= 1; ++n0)
+            for (int n1 = -1; n1 <= 1; ++n1) {
+                if (n0 == 0 && n1 == 0) continue;
+                for (int d = 0; d < 2; ++d) {
+                    double acc = 0.0;
+                    acc += n0 * a[0 * 2 + d];
+                    acc += n1 * a[1 * 2 + d];
+                    s.cand[nc * 2 + d] = acc;
+                }
+                ++nc;
+            }
+    return ALEA_OK;
+}
+
+// Host arena of tables, uploaded once; pointers are patched after cudaMalloc.
+struct Arena {
+    std::vector<char> bytes;
+    size_t add(const void* p, size_t n) {
+        const size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + n);
+        if (n) std::memcpy(bytes.data() + off, p, n);
+        return off;
+    }
+};
+
+int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
+    DevSys& s = c->sys;
+    s = DevSys{};
+    if (!in) return fail(c, ALEA_ERR_INVALID, "null system");
+    if (in->dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "the walker kernels implement dim = 2");
+    const int np = in->n_particles;
+    if (np < 1 || np > 1024) return fail(c, ALEA_ERR_INVALID, "n_particles must be in [1, 1024]");
+    s.dim = 2;
+    s.np = np;
+    if (int rc = setup_cell(c, in, s)) return rc;
+    Arena ar;
+    struct Patch { size_t off; const void** slot; };
+    std::vector<Patch> patches;
+    auto put = [&](const void* p, size_t n, const void** slot) {
+        patches.push_back({ar.add(p, n), slot});
+    };
+    // groups
+    if (in->n_groups < 1 || in->n_groups > kMaxGroups) return fail(c, ALEA_ERR_INVALID, "bad n_groups");
+    s.ngroups = in->n_groups;
+    std::vector<double> inv_mass(np * 2, 0.0), charge(np, 0.0);
+    std::vector<int> group_of(np, -1);
+    for (int g = 0; g < in->n_groups; ++g) {
+        const alea_gpu_group& G = in->groups[g];
+        if (G.first < 0 || G.last > np || G.first >= G.last)
+            return fail(c, ALEA_ERR_INVALID, "group range out of bounds");
+        s.gfirst[g] = G.first;
+        s.glast[g] = G.last;
+        s.gcharge[g] = G.charge;
+        for (int i = G.first; i < G.last; ++i) {
+            if (group_of[i] >= 0) return fail(c, ALEA_ERR_INVALID, "groups overlap");
+            group_of[i] = g;
+            charge[i] = G.charge;
+            inv_mass[i * 2] = G.inv_mass[0];
+            inv_mass[i * 2 + 1] = G.inv_mass[1];
+        }
+    }
+    for (int i = 0; i < np; ++i)
+        if (group_of[i] < 0) return fail(c, ALEA_ERR_INVALID, "a particle belongs to no group");
+    c->h_inv_mass = inv_mass;
+    put(inv_mass.data(), inv_mass.size() * 8, reinterpret_cast<const void**>(&s.inv_mass));
+    put(charge.data(), charge.size() * 8, reinterpret_cast<const void**>(&s.charge));
+    put(group_of.data(), group_of.size() * 4, reinterpret_cast<const void**>(&s.group_of));
+
+    // record layout, hot part
+    long o = 0;
+    s.o_pos = o; o += np * 2;
+    s.o_jg = o; o += np * 2;
+    s.o_jl = o; o += np * 2;
+    s.o_sg = o; o += np * 2;
+    s.o_sl = o; o += np * 2;
+    s.o_scal = o; o += S_NSCAL;
+    // determinant blocks
+    if (in->n_blocks < 0 || in->n_blocks > kMaxBlocks) return fail(c, ALEA_ERR_INVALID, "bad n_blocks");
+    s.nblocks = in->n_blocks;
+    s.maxN = 1;
+    std::vector<std::vector<double>> sin_flags(in->n_blocks);
+    for (int b = 0; b < in->n_blocks; ++b) {
+        const alea_gpu_orbitals& B = in->blocks[b];
+        DevBlock& D = s.blocks[b];
+        D.first = B.first;
+        D.last = B.last;
+        D.n = B.last - B.first;
+        D.type = B.type;
+        if (D.n < 1 || D.n > kMaxN || B.first < 0 || B.last > np)
+            return fail(c, ALEA_ERR_UNSUPPORTED, "determinant blocks must have 1..64 particles");
+        s.maxN = std::max(s.maxN, D.n);
+        if (B.type == ALEA_ORB_PLANE_WAVE) {
+            if (!B.k || !B.is_sin) return fail(c, ALEA_ERR_INVALID, "plane-wave block without tables");
+            put(B.k, D.n * 2 * 8, reinterpret_cast<const void**>(&D.k));
+            sin_flags[b].resize(D.n);
+            for (int i = 0; i < D.n; ++i) sin_flags[b][i] = B.is_sin[i] ? 1.0 : 0.0;
+            put(sin_flags[b].data(), D.n * 8, reinterpret_cast<const void**>(&D.is_sin));
+        } else if (B.type == ALEA_ORB_GAUSSIAN) {
+            if (!B.centers || !B.alphas) return fail(c, ALEA_ERR_INVALID, "Gaussian block without tables");
+            put(B.centers, D.n * 2 * 8, reinterpret_cast<const void**>(&D.centers));
+            put(B.alphas, D.n * 8, reinterpret_cast<const void**>(&D.alphas));
+        } else {
+            return fail(c, ALEA_ERR_INVALID, "unknown orbital type");
+        }
+        D.oA = static_cast<int>(o);
+        o += D.n * D.n;
+    }
+    for (int b = 0; b < s.nblocks; ++b) {
+        s.blocks[b].orabs = static_cast<int>(o);
+        o += s.blocks[b].n;
+    }
+    // pair terms and the shared Jastrow k set
+    if (in->n_terms < 0 || in->n_terms > kMaxTerms) return fail(c, ALEA_ERR_INVALID, "bad n_terms");
+    s.nterms = in->n_terms;
+    const alea_gpu_kset* kref = nullptr;
+    std::vector<double> kx2, ky2;
+    for (int t = 0; t < in->n_terms; ++t) {
+        const alea_gpu_pair_term& T = in->terms[t];
+        DevTerm& D = s.terms[t];
+        D.kind = T.kind;
+        D.npairs = T.n_pairs;
+        if (T.n_pairs < 1 || T.n_pairs > ALEA_GPU_MAX_PAIRS) return fail(c, ALEA_ERR_INVALID, "bad n_pairs");
+        for (int q = 0; q < T.n_pairs; ++q)
+            for (int k = 0; k < 4; ++k) {
+                D.pairs[q][k] = T.pairs[q][k];
+                if (T.pairs[q][k] < 0 || T.pairs[q][k] > np)
+                    return fail(c, ALEA_ERR_INVALID, "pair range out of bounds");
+            }
+        D.same0 = T.pairs[0][0] == T.pairs[0][2] && T.pairs[0][1] == T.pairs[0][3];
+        if (T.kind == ALEA_PAIR_PADE) {
+            if (T.n_pairs != 1) return fail(c, ALEA_ERR_INVALID, "a Padé term has one group pair");
+            if (T.num_order + T.den_order > 16 || T.num_order < 0 || T.den_order < 0)
+                return fail(c, ALEA_ERR_INVALID, "Padé order too large");
+            D.nnum = T.num_order;
+            D.nden = T.den_order;
+            for (int k = 0; k < D.nnum + D.nden; ++k) D.coef[k] = T.coeffs[k];
+            D.image = T.image_sum;
+            if (T.image_sum) {
+                if (!s.periodic) return fail(c, ALEA_ERR_INVALID, "image sum in an open cell");
+                const alea_gpu_spline& sp = T.short_range;
+                if (!sp.scaled || sp.n_knots < 2) return fail(c, ALEA_ERR_INVALID, "bad image-sum spline");
+                D.sp.r_cut = sp.r_cut;
+                D.sp.inv_delta = sp.inv_delta;
+                D.sp.n_knots = sp.n_knots;
+                put(sp.scaled, 3 * sp.n_knots * 8, reinterpret_cast<const void**>(&D.sp.scaled));
+                D.u_inf = T.u_inf;
+                const alea_gpu_kset& ks = T.kset;
+                if (ks.n_k < 1 || !ks.n1 || !ks.n2 || !ks.kx || !ks.ky || !ks.weight)
+                    return fail(c, ALEA_ERR_INVALID, "bad image-sum k set");
+                if (!kref) {
+                    kref = &ks;
+                } else if (ks.n_k != kref->n_k || std::memcmp(ks.n1, kref->n1, 4 * ks.n_k) ||
+                           std::memcmp(ks.n2, kref->n2, 4 * ks.n_k)) {
+                    return fail(c, ALEA_ERR_UNSUPPORTED, "image-summed terms must share one k set");
+                }
+                put(ks.weight, ks.n_k * 8, reinterpret_cast<const void**>(&D.kw));
+                // the structure factor is kept per particle group
+                for (int side = 0; side < 2; ++side) {
+                    const int f0 = T.pairs[0][side * 2], f1 = T.pairs[0][side * 2 + 1];
+                    bool ok = false;
+                    for (int g = 0; g < s.ngroups; ++g) ok |= s.gfirst[g] == f0 && s.glast[g] == f1;
+                    if (!ok) return fail(c, ALEA_ERR_UNSUPPORTED, "image-summed term on a partial group");
+                }
+            }
+        } else if (T.kind == ALEA_PAIR_DRUMMOND) {
+            if (T.C < 2 || T.n_coeffs < 1 || T.n_coeffs > 16) return fail(c, ALEA_ERR_INVALID, "bad Drummond term");
+            D.C = T.C;
+            D.gamma = T.gamma;
+            D.L = T.L;
+            D.ncoef = T.n_coeffs;
+            for (int k = 0; k < T.n_coeffs; ++k) D.dc[k] = T.dcoeffs[k];
+            double ipw = 1.0;
+            for (int i = 0; i < T.C; ++i) ipw *= -T.L;
+            D.alpha1 = T.gamma / ipw + D.dc[0] * static_cast<double>(T.C) / T.L;
+        } else {
+            return fail(c, ALEA_ERR_INVALID, "unknown pair term");
+        }
+    }
+    if (kref) {
+        s.nkJ = kref->n_k;
+        int m1 = 0, m2 = 0;
+        for (int k = 0; k < kref->n_k; ++k) {
+            m1 = std::max(m1, std::abs(kref->n1[k]));
+            m2 = std::max(m2, std::abs(kref->n2[k]));
+            kx2.push_back(kref->kx[k] * kref->kx[k]);
+            ky2.push_back(kref->ky[k] * kref->ky[k]);
+        }
+        if (m1 > kMaxLadder || m2 > kMaxLadder) return fail(c, ALEA_ERR_UNSUPPORTED, "k index too large");
+        s.m1J = m1;
+        s.m2J = m2;
+        put(kref->n1, 4 * s.nkJ, reinterpret_cast<const void**>(&s.n1J));
+        put(kref->n2, 4 * s.nkJ, reinterpret_cast<const void**>(&s.n2J));
+        put(kref->kx, 8 * s.nkJ, reinterpret_cast<const void**>(&s.kxJ));
+        put(kref->ky, 8 * s.nkJ, reinterpret_cast<const void**>(&s.kyJ));
+        put(kx2.data(), 8 * s.nkJ, reinterpret_cast<const void**>(&s.kx2J));
+        put(ky2.data(), 8 * s.nkJ, reinterpret_cast<const void**>(&s.ky2J));
+    }
+    s.o_rho = static_cast<int>(o);
+    o += static_cast<long>(s.ngroups) * 2 * s.nkJ;
+    s.o_pc = static_cast<int>(o);
+    o += static_cast<long>(np) * 2 * s.nkJ;
+    s.hot = static_cast<int>(round4(o));
+    o = s.hot;
+    for (int b = 0; b < s.nblocks; ++b) {
+        DevBlock& D = s.blocks[b];
+        D.oD = o; o += D.n * D.n;
+        D.oDg = o; o += D.n * D.n * 2;
+        D.oDl = o; o += D.n * D.n * 2;
+    }
+    s.rec = round4(o);
+    // Ewald
+    s.ewald = in->ewald.enabled;
+    if (s.ewald) {
+        const alea_gpu_ewald& E = in->ewald;
+        if (!s.periodic) return fail(c, ALEA_ERR_INVALID, "Ewald in an open cell");
+        if (!E.long_range.scaled || E.kset.n_k < 0 || (E.kset.n_k > 0 && (!E.kset.n1 || !E.kset.n2 || !E.kset.weight)))
+            return fail(c, ALEA_ERR_INVALID, "bad Ewald tables");
+        s.esp.r_cut = E.long_range.r_cut;
+        s.esp.inv_delta = E.long_range.inv_delta;
+        s.esp.n_knots = E.long_range.n_knots;
+        put(E.long_range.scaled, 3 * E.long_range.n_knots * 8, reinterpret_cast<const void**>(&s.esp.scaled));
+        s.e_rcut = E.r_cut;
+        s.e_inv_eps = E.inv_eps;
+        s.e_const = E.constant;
+        s.enk = E.kset.n_k;
+        int m1 = 0, m2 = 0;
+        for (int k = 0; k < s.enk; ++k) {
+            m1 = std::max(m1, std::abs(E.kset.n1[k]));
+            m2 = std::max(m2, std::abs(E.kset.n2[k]));
+        }
+        if (m1 > kMaxLadder || m2 > kMaxLadder) return fail(c, ALEA_ERR_UNSUPPORTED, "Ewald k index too large");
+        s.e_m1 = m1;
+        s.e_m2 = m2;
+        if (s.enk > 0) {
+            put(E.kset.n1, 4 * s.enk, reinterpret_cast<const void**>(&s.en1));
+            put(E.kset.n2, 4 * s.enk, reinterpret_cast<const void**>(&s.en2));
+            put(E.kset.weight, 8 * s.enk, reinterpret_cast<const void**>(&s.ew));
+        }
+    }
+    if (in->n_coulomb < 0 || in->n_coulomb > kMaxCoulomb) return fail(c, ALEA_ERR_INVALID, "bad n_coulomb");
+    s.ncoul = in->n_coulomb;
+    for (int k = 0; k < s.ncoul; ++k) {
+        const alea_gpu_coulomb& C = in->coulomb[k];
+        s.coul[k][0] = C.a_first;
+        s.coul[k][1] = C.a_last;
+        s.coul[k][2] = C.b_first;
+        s.coul[k][3] = C.b_last;
+        s.coul_coef[k] = C.coef;
+    }
+    // ziggurat tables
+    const Ziggurat z = make_ziggurat();
+    put(z.k, sizeof z.k, reinterpret_cast<const void**>(&s.zk));
+    put(z.w, sizeof z.w, reinterpret_cast<const void**>(&s.zw));
+    put(z.f, sizeof z.f, reinterpret_cast<const void**>(&s.zf));
+    s.zr = z.r;
+    // shared-memory layout after the hot part
+    long m = s.hot;
+    auto take = [&](long n) {
+        const long at = m;
+        m += round4(std::max(n, 1L));
+        return static_cast<int>(at);
+    };
+    s.s_newpos = take(4);
+    s.s_nval = take(s.maxN);
+    s.s_ngrad = take(2 * s.maxN);
+    s.s_nlap = take(2 * s.maxN);
+    s.s_rad = take(static_cast<long>(s.nterms) * np * 6 + np * 6);
+    s.s_cn = take(s.nkJ);
+    s.s_sn = take(s.nkJ);
+    s.s_dr = take(s.nkJ);
+    s.s_di = take(s.nkJ);
+    s.s_col = take(s.maxN);
+    s.s_rowp = take(s.maxN);
+    s.s_red = take(kWarps * 16 + 16);
+    s.s_misc = take(32 + 4 * (kMaxLadder + 1));
+    long work = static_cast<long>(s.maxN) * s.maxN;
+    work = std::max(work, static_cast<long>(np) * 2 * (s.e_m1 + s.e_m2 + 2));
+    work = std::max(work, static_cast<long>(np) * 2 * (s.m1J + s.m2J + 2));
+    s.s_work = take(work);
+    s.s_total = static_cast<int>(m);
+    c->smem = static_cast<size_t>(s.s_total) * 8;
+    if (c->smem > 227 * 1024)
+        return fail(c, ALEA_ERR_UNSUPPORTED,
+                    "walker state needs " + std::to_string(c->smem) + " bytes of shared memory (> 227 KB)");
+    // upload the arena and patch pointers
+    CUDA_TRY(c, cudaMalloc(&c->arena, std::max<size_t>(ar.bytes.size(), 256)));
+    CUDA_TRY(c, cudaMemcpy(c->arena, ar.bytes.data(), ar.bytes.size(), cudaMemcpyHostToDevice));
+    for (const Patch& p : patches) *p.slot = static_cast<char*>(c->arena) + p.off;
+    // the DevSys copy keeps const double* etc.; nothing else to patch
+    return ALEA_OK;
+}
+
+int ensure_streams(alea_gpu_ctx* c, int n) {
+    if (n > c->streams_cap) {
+        if (c->streams) cudaFree(c->streams);
+        c->streams = nullptr;
+        CUDA_TRY(c, cudaMalloc(&c->streams, sizeof(uint64_t) * 4 * static_cast<size_t>(n)));
+        c->streams_cap = n;
+    }
+    return ALEA_OK;
+}
+
+int ensure_randoms(alea_gpu_ctx* c, int sweeps) {
+    if (sweeps > c->rnd_sweeps) {
+        if (c->randoms) cudaFree(c->randoms);
+        c->randoms = nullptr;
+        const size_t n = static_cast<size_t>(sweeps) * c->sys.np * 3 * c->capacity;
+        CUDA_TRY(c, cudaMalloc(&c->randoms, n * 8));
+        c->rnd_sweeps = sweeps;
+    }
+    return ALEA_OK;
+}
+
+int set_sigma(alea_gpu_ctx* c, double tau) {
+    if (tau == c->sigma_tau) return ALEA_OK;
+    std::vector<double> sg(c->h_inv_mass.size());
+    for (size_t i = 0; i < sg.size(); ++i) sg[i] = std::sqrt(tau * c->h_inv_mass[i]);
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_sigma, sg.data(), sg.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->sigma_tau = tau;
+    return ALEA_OK;
+}
+
+double* records(alea_gpu_ctx* c) { return c->rec[c->cur]; }
+
+int read_scalars(alea_gpu_ctx* c, int slot, std::vector<double>& out) {
+    out.resize(c->nw);
+    if (c->nw == 0) return ALEA_OK;
+    scalar_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
+                                                              c->sys.o_scal + slot, c->d_buf);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(out.data(), c->d_buf, 8 * c->nw, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
+}
+
+int write_scalars(alea_gpu_ctx* c, int slot, const std::vector<double>& in) {
+    if (c->nw == 0) return ALEA_OK;
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_buf, in.data(), 8 * c->nw, cudaMemcpyHostToDevice, c->stream));
+    from_soa_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
+                                                                c->sys.o_scal + slot, 1, c->d_buf);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
+}
+
+int check_errors(alea_gpu_ctx* c) {
+    std::vector<double> e;
+    if (int rc = read_scalars(c, S_ERR, e)) return rc;
+    for (int w = 0; w < c->nw; ++w)
+        if (e[w] != 0.0)
+            return fail(c, ALEA_ERR_SINGULAR,
+                        "walker " + std::to_string(w) + ": accepted determinant is singular or nonfinite");
+    return ALEA_OK;
+}
+
+int launch_evaluate(alea_gpu_ctx* c) {
+    if (c->nw == 0) return ALEA_OK;
+    evaluate_kernel<<<c->nw, kThreads, c->smem, c->stream>>>(c->sys, records(c), c->nw, c->pairs, c->npair);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_errors(c);
+}
+
+// One sweep-kernel launch (VMC step or DMC advance) with its randoms.
+int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, double etrial, double eref,
+              double e_cut, double e_max) {
+    if (c->nw == 0) return ALEA_OK;
+    if (c->n_streams < 1) return fail(c, ALEA_ERR_INVALID, "no random streams (alea_gpu_set_streams)");
+    if (n_sub < 1) return fail(c, ALEA_ERR_INVALID, "n_substeps must be >= 1");
+    if (int rc = ensure_randoms(c, n_sub)) return rc;
+    if (int rc = set_sigma(c, tau)) return rc;
+    const long stride = c->nw;
+    const int nt = std::min(c->n_streams, c->nw);
+    draw_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, stride,
+                                                         n_sub, c->sys.zk, c->sys.zw, c->sys.zf, c->sys.zr,
+                                                         c->randoms, 0);
+    CUDA_TRY(c, cudaGetLastError());
+    SweepParams prm{};
+    prm.mode = mode;
+    prm.n_sub = n_sub;
+    prm.drift = drift;
+    prm.tau = tau;
+    prm.sigma = c->d_sigma;
+    prm.etrial = etrial;
+    prm.eref = eref;
+    prm.e_cut = e_cut;
+    prm.e_max = e_max;
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    sweep_kernel<<<c->nw, kThreads, c->smem, c->stream>>>(c->sys, records(c), c->nw, c->randoms, stride, prm,
+                                                          c->pairs, c->npair);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+    return check_errors(c);
+}
+
+}  // namespace
+
+// ───────────────────────── C ABI ────────────────────────────────────────
+
+extern "C" {
+
+int alea_gpu_abi_version(void) { return ALEA_GPU_ABI_VERSION; }
+
+const char* alea_gpu_last_error(const alea_gpu_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_gpu_ctx** out) {
+    if (!out) return fail(nullptr, ALEA_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    if (capacity < 1) return fail(nullptr, ALEA_ERR_INVALID, "capacity must be >= 1");
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
+        return fail(nullptr, ALEA_ERR_CUDA, "no CUDA device");
+    if (device < 0 || device >= n_dev) return fail(nullptr, ALEA_ERR_INVALID, "bad device index");
+    auto* c = new alea_gpu_ctx();
+    c->device = device;
+    c->capacity = capacity;
+    auto bail = [&](int rc) {
+        g_create_error = c->err;
+        alea_gpu_destroy(c);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) {
+        c->err = "cudaSetDevice failed";
+        return bail(ALEA_ERR_CUDA);
+    }
+    if (int rc = build_system(c, sys)) return bail(rc);
+    const DevSys& s = c->sys;
+    const size_t recb = static_cast<size_t>(s.rec) * 8 * capacity;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->rec[0], recb) != cudaSuccess || cudaMalloc(&c->rec[1], recb) != cudaSuccess ||
+        cudaMalloc(&c->d_buf, static_cast<size_t>(std::max(s.np * 2, 8)) * 8 * capacity) != cudaSuccess ||
+        cudaMalloc(&c->d_sigma, static_cast<size_t>(s.np) * 2 * 8) != cudaSuccess ||
+        cudaMalloc(&c->d_src, sizeof(int) * static_cast<size_t>(capacity)) != cudaSuccess ||
+        cudaMalloc(&c->d_mask, static_cast<size_t>(capacity)) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        c->err = "device allocation failed";
+        return bail(ALEA_ERR_NOMEM);
+    }
+    cudaMemset(c->rec[0], 0, recb);
+    cudaMemset(c->rec[1], 0, recb);
+    // pair list i < j for the Ewald real-space sum
+    std::vector<int2> pl;
+    for (int i = 0; i < s.np; ++i)
+        for (int j = i + 1; j < s.np; ++j) pl.push_back(make_int2(i, j));
+    c->npair = static_cast<int>(pl.size());
+    if (c->npair > 0) {
+        if (cudaMalloc(&c->pairs, pl.size() * sizeof(int2)) != cudaSuccess ||
+            cudaMemcpy(c->pairs, pl.data(), pl.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+            c->err = "device allocation failed";
+            return bail(ALEA_ERR_NOMEM);
+        }
+    }
+    for (const void* k : {reinterpret_cast<const void*>(evaluate_kernel), reinterpret_cast<const void*>(measure_kernel),
+                          reinterpret_cast<const void*>(move_kernel), reinterpret_cast<const void*>(sweep_kernel)}) {
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(c->smem)) !=
+            cudaSuccess) {
+            c->err = "cannot reserve " + std::to_string(c->smem) + " bytes of shared memory";
+            return bail(ALEA_ERR_UNSUPPORTED);
+        }
+    }
+    *out = c;
+    return ALEA_OK;
+}
+
+int alea_gpu_destroy(alea_gpu_ctx* c) {
+    if (!c) return ALEA_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : {static_cast<void*>(c->arena), static_cast<void*>(c->rec[0]), static_cast<void*>(c->rec[1]),
+                    static_cast<void*>(c->randoms), static_cast<void*>(c->streams), static_cast<void*>(c->pairs),
+                    static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
+                    static_cast<void*>(c->d_mask)})
+        if (p) cudaFree(p);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ALEA_OK;
+}
+
+int alea_gpu_num_walkers(const alea_gpu_ctx* c, int* nw) {
+    if (!c || !nw) return ALEA_ERR_INVALID;
+    *nw = c->nw;
+    return ALEA_OK;
+}
+
+int alea_gpu_upload_walkers(alea_gpu_ctx* c, const double* positions, int nw) {
+    if (!c) return ALEA_ERR_INVALID;
+    if (nw < 1 || nw > c->capacity) return fail(c, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
+    if (!positions) return fail(c, ALEA_ERR_INVALID, "null positions");
+    cudaSetDevice(c->device);
+    c->cur = 0;
+    c->nw = nw;
+    const DevSys& s = c->sys;
+    CUDA_TRY(c, cudaMemsetAsync(records(c), 0, static_cast<size_t>(s.rec) * 8 * nw, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_buf, positions, static_cast<size_t>(s.np) * 2 * nw * 8,
+                                cudaMemcpyHostToDevice, c->stream));
+    const long n = static_cast<long>(s.np) * 2 * nw;
+    from_soa_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_pos,
+                                                                             s.np * 2, c->d_buf);
+    set_scalar_kernel<<<(nw + 255) / 256, 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_scal + S_WEIGHT, 1.0);
+    CUDA_TRY(c, cudaGetLastError());
+    c->next_id = 1.0;
+    return launch_evaluate(c);
+}
+
+int alea_gpu_evaluate(alea_gpu_ctx* c) {
+    if (!c) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    return launch_evaluate(c);
+}
+
+int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_psi, double* gradients,
+                              double* laplacians, double* local_energy, double* weights) {
+    if (!c) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    const DevSys& s = c->sys;
+    const int nw = c->nw;
+    if (nw == 0) return ALEA_OK;
+    const long n = static_cast<long>(s.np) * 2 * nw;
+    const int grid = static_cast<int>((n + 255) / 256);
+    auto plane = [&](int off, double* dst) -> int {
+        to_soa_kernel<<<grid, 256, 0, c->stream>>>(records(c), nw, s.rec, off, s.np * 2, c->d_buf);
+        CUDA_TRY(c, cudaGetLastError());
+        CUDA_TRY(c, cudaMemcpyAsync(dst, c->d_buf, n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        return ALEA_OK;
+    };
+    if (positions)
+        if (int rc = plane(s.o_pos, positions)) return rc;
+    if (gradients || laplacians) {
+        std::vector<double> a(n), b(n);
+        for (int which = 0; which < 2; ++which) {
+            double* dst = which == 0 ? gradients : laplacians;
+            if (!dst) continue;
+            if (int rc = plane(which == 0 ? s.o_sg : s.o_sl, a.data())) return rc;
+            if (int rc = plane(which == 0 ? s.o_jg : s.o_jl, b.data())) return rc;
+            for (long i = 0; i < n; ++i) dst[i] = a[i] + b[i];
+        }
+    }
+    std::vector<double> tmp;
+    if (log_psi) {
+        if (int rc = read_scalars(c, S_LOGPSI, tmp)) return rc;
+        std::copy(tmp.begin(), tmp.end(), log_psi);
+    }
+    if (local_energy) {
+        if (int rc = read_scalars(c, S_EL, tmp)) return rc;
+        std::copy(tmp.begin(), tmp.end(), local_energy);
+    }
+    if (weights) {
+        if (int rc = read_scalars(c, S_WEIGHT, tmp)) return rc;
+        std::copy(tmp.begin(), tmp.end(), weights);
+    }
+    return ALEA_OK;
+}
+
+int alea_gpu_move(alea_gpu_ctx* c, int p, const double* new_pos, const uint8_t* accept, double* log_ratio,
+                  double* phase, double* new_grad, double* new_lap) {
+    if (!c || !new_pos) return ALEA_ERR_INVALID;
+    const DevSys& s = c->sys;
+    if (p < 0 || p >= s.np) return fail(c, ALEA_ERR_INVALID, "particle index out of range");
+    cudaSetDevice(c->device);
+    const int nw = c->nw;
+    if (nw == 0) return ALEA_OK;
+    double* d_np = c->d_buf;
+    double* d_out = c->d_buf + 2 * nw;
+    if (static_cast<long>(8) * nw > static_cast<long>(std::max(s.np * 2, 8)) * c->capacity)
+        return fail(c, ALEA_ERR_NOMEM, "staging buffer too small");
+    CUDA_TRY(c, cudaMemcpyAsync(d_np, new_pos, 16L * nw, cudaMemcpyHostToDevice, c->stream));
+    if (accept) CUDA_TRY(c, cudaMemcpyAsync(c->d_mask, accept, nw, cudaMemcpyHostToDevice, c->stream));
+    move_kernel<<<nw, kThreads, c->smem, c->stream>>>(s, records(c), nw, p, d_np, accept ? c->d_mask : nullptr,
+                                                      d_out);
+    CUDA_TRY(c, cudaGetLastError());
+    std::vector<double> out(6L * nw);
+    CUDA_TRY(c, cudaMemcpyAsync(out.data(), d_out, 48L * nw, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (int w = 0; w < nw; ++w) {
+        if (log_ratio) log_ratio[w] = out[w];
+        if (phase) phase[w] = out[nw + w];
+        if (new_grad) {
+            new_grad[w] = out[2 * nw + w];
+            new_grad[nw + w] = out[3 * nw + w];
+        }
+        if (new_lap) {
+            new_lap[w] = out[4 * nw + w];
+            new_lap[nw + w] = out[5 * nw + w];
+        }
+    }
+    return accept ? check_errors(c) : ALEA_OK;
+}
+
+int alea_gpu_measure(alea_gpu_ctx* c) {
+    if (!c) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (c->nw == 0) return ALEA_OK;
+    measure_kernel<<<c->nw, kThreads, c->smem, c->stream>>>(c->sys, records(c), c->nw, c->pairs, c->npair);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
+}
+
+int alea_gpu_set_streams(alea_gpu_ctx* c, uint64_t seed, uint64_t kind, int n) {
+    if (!c || n < 1) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (int rc = ensure_streams(c, n)) return rc;
+    std::vector<uint64_t> st(4L * n);
+    for (int t = 0; t < n; ++t) {
+        HostXo x(stream_seed(seed, kind, static_cast<uint64_t>(t)));
+        for (int k = 0; k < 4; ++k) st[4L * t + k] = x.s[k];
+    }
+    CUDA_TRY(c, cudaMemcpy(c->streams, st.data(), st.size() * 8, cudaMemcpyHostToDevice));
+    c->n_streams = n;
+    return ALEA_OK;
+}
+
+int alea_gpu_vmc_step(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out) {
+    if (!c || !prm) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (int rc = run_sweep(c, 0, prm->n_substeps, prm->tau, prm->use_drift, 0, 0, 0, 0)) return rc;
+    if (out) {
+        std::vector<double> el, na;
+        if (int rc = read_scalars(c, S_EL, el)) return rc;
+        if (int rc = read_scalars(c, S_NACC, na)) return rc;
+        *out = alea_gpu_step_stats{};
+        for (int w = 0; w < c->nw; ++w) {
+            out->energy_sum += el[w];
+            out->energy_sq_sum += el[w] * el[w];
+            out->n_accepted += static_cast<int64_t>(na[w]);
+        }
+        out->weight_sum = c->nw;
+        out->n_proposed = static_cast<int64_t>(prm->n_substeps) * c->sys.np * c->nw;
+        out->n_walkers = c->nw;
+    }
+    return ALEA_OK;
+}
+
+int alea_gpu_dmc_advance(alea_gpu_ctx* c, const alea_gpu_dmc_params* prm, alea_gpu_step_stats* out) {
+    if (!c || !prm) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (int rc = run_sweep(c, 1, prm->n_substeps, prm->tau, 1, prm->e_trial, prm->e_ref, prm->e_cut, prm->e_max))
+        return rc;
+    if (int rc = read_scalars(c, S_WEIGHT, c->h_w)) return rc;
+    if (int rc = read_scalars(c, S_EL, c->h_el)) return rc;
+    if (out) {
+        if (int rc = read_scalars(c, S_NACC, c->h_nacc)) return rc;
+        if (int rc = read_scalars(c, S_NCUT, c->h_ncut)) return rc;
+        *out = alea_gpu_step_stats{};
+        // Σ w E and Σ w per crowd, then over crowds (dmc.cpp:713-724)
+        const int nw = c->nw;
+        const int nact = std::min(c->n_streams, nw);
+        const int base = nw / nact, rem = nw % nact;
+        for (int t = 0; t < nact; ++t) {
+            const int w0 = t * base + std::min(t, rem), cnt = base + (t < rem ? 1 : 0);
+            double e = 0.0, ws = 0.0;
+            for (int w = w0; w < w0 + cnt; ++w) {
+                e += c->h_w[w] * c->h_el[w];
+                ws += c->h_w[w];
+            }
+            out->energy_sum += e;
+            out->weight_sum += ws;
+        }
+        for (int w = 0; w < nw; ++w) {
+            out->n_accepted += static_cast<int64_t>(c->h_nacc[w]);
+            out->n_cut += static_cast<int64_t>(c->h_ncut[w]);
+            out->energy_sq_sum += c->h_w[w] * c->h_el[w] * c->h_el[w];
+        }
+        out->n_proposed = static_cast<int64_t>(prm->n_substeps) * c->sys.np * nw;
+        out->n_walkers = nw;
+    }
+    return ALEA_OK;
+}
+
+int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
+    if (!c || !state || target < 1) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    const int n = c->nw;
+    if (n == 0) return ALEA_OK;
+    std::vector<double> w;
+    if (int rc = read_scalars(c, S_WEIGHT, w)) return rc;
+    HostXo rng;
+    std::memcpy(rng.s, state, 32);
+    std::vector<int> src;
+    src.reserve(2 * target + 2);
+    for (int i = 0; i < n; ++i) {
+        const int m = static_cast<int>(w[i] + rng.uniform());
+        for (int k = 0; k < m; ++k) src.push_back(i);
+    }
+    const size_t n_max = 2 * static_cast<size_t>(target) + 1, n_min = static_cast<size_t>(target) / 5 + 1;
+    if (src.empty()) {
+        int best = 0;
+        for (int i = 1; i < n; ++i)
+            if (w[i] > w[best]) best = i;
+        src.push_back(best);
+    }
+    while (src.size() > n_max) {
+        const size_t i = static_cast<size_t>(rng.uniform() * static_cast<double>(src.size()));
+        src[i] = src.back();
+        src.pop_back();
+    }
+    while (src.size() < n_min) {
+        const size_t i = static_cast<size_t>(rng.uniform() * static_cast<double>(src.size()));
+        src.push_back(src[i]);
+    }
+    std::memcpy(state, rng.s, 32);
+    if (static_cast<int>(src.size()) > c->capacity)
+        return fail(c, ALEA_ERR_NOMEM, "branching exceeded the walker capacity");
+    // genealogy (walker_set.cpp:221-238)
+    std::vector<double> ids, par;
+    if (int rc = read_scalars(c, S_ID, ids)) return rc;
+    if (int rc = read_scalars(c, S_PARENT, par)) return rc;
+    std::vector<char> seen(n, 0);
+    std::vector<double> nid(src.size()), npar(src.size());
+    for (size_t j = 0; j < src.size(); ++j) {
+        nid[j] = ids[src[j]];
+        npar[j] = par[src[j]];
+        if (seen[src[j]]) {
+            npar[j] = nid[j];
+            nid[j] = c->next_id;
+            c->next_id += 1.0;
+        } else {
+            seen[src[j]] = 1;
+        }
+    }
+    const int nn = static_cast<int>(src.size());
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_src, src.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, c->stream));
+    gather_kernel<<<nn, 256, 0, c->stream>>>(c->rec[1 - c->cur], c->rec[c->cur], c->d_src, nn, c->sys.rec);
+    CUDA_TRY(c, cudaGetLastError());
+    c->cur = 1 - c->cur;
+    c->nw = nn;
+    set_scalar_kernel<<<(nn + 255) / 256, 256, 0, c->stream>>>(records(c), nn, c->sys.rec,
+                                                                c->sys.o_scal + S_WEIGHT, 1.0);
+    CUDA_TRY(c, cudaGetLastError());
+    if (int rc = write_scalars(c, S_ID, nid)) return rc;
+    if (int rc = write_scalars(c, S_PARENT, npar)) return rc;
+    return ALEA_OK;
+}
+
+int alea_gpu_last_kernel_ms(const alea_gpu_ctx* c, double* ms) {
+    if (!c || !ms) return ALEA_ERR_INVALID;
+    *ms = c->last_ms;
+    return ALEA_OK;
+}
+
+int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
+                     double* block_energies) {
+    if (!c || !cfg || !res) return ALEA_ERR_INVALID;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int nw = c->nw;
+    const int T = std::min(std::max(cfg->n_streams, 1), nw);
+    if (int rc = alea_gpu_set_streams(c, cfg->seed, ALEA_STREAM_VMC, T)) return rc;
+    alea_gpu_vmc_params prm{cfg->tau, cfg->n_substeps, cfg->use_drift};
+    std::vector<double> blocks;   // [T][n_acc], chain-major
+    std::vector<std::vector<double>> chain(T);
+    double e_sum = 0, e2_sum = 0;
+    int64_t n_tot = 0, acc = 0, prop = 0;
+    const int base = nw / T, rem = nw % T;
+    for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
+        const bool measure = b >= cfg->n_equilibration_blocks;
+        std::vector<double> blk(T, 0.0);
+        std::vector<int64_t> blk_n(T, 0);
+        for (int st = 0; st < cfg->n_steps; ++st) {
+            alea_gpu_step_stats s{};
+            if (int rc = alea_gpu_vmc_step(c, &prm, &s)) return rc;
+            if (!measure) continue;
+            std::vector<double> el;
+            if (int rc = read_scalars(c, S_EL, el)) return rc;
+            for (int t = 0; t < T; ++t) {
+                const int w0 = t * base + std::min(t, rem), cnt = base + (t < rem ? 1 : 0);
+                for (int w = w0; w < w0 + cnt; ++w) {
+                    blk[t] += el[w];
+                    e_sum += el[w];
+                    e2_sum += el[w] * el[w];
+                }
+                blk_n[t] += cnt;
+                n_tot += cnt;
+            }
+            acc += s.n_accepted;
+            prop += s.n_proposed;
+        }
+        if (measure)
+            for (int t = 0; t < T; ++t) chain[t].push_back(blk[t] / static_cast<double>(blk_n[t]));
+    }
+    for (int t = 0; t < T; ++t) blocks.insert(blocks.end(), chain[t].begin(), chain[t].end());
+    double mean = 0.0, err = 0.0;
+    reblock(blocks, mean, err);
+    res->energy = mean;
+    res->energy_error = err;
+    const double m = n_tot ? e_sum / static_cast<double>(n_tot) : 0.0;
+    res->variance = n_tot ? e2_sum / static_cast<double>(n_tot) - m * m : 0.0;
+    res->acceptance = prop ? static_cast<double>(acc) / static_cast<double>(prop) : 0.0;
+    res->walltime_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    res->n_walkers = c->nw;
+    res->e_trial = 0.0;
+    if (block_energies) std::copy(blocks.begin(), blocks.end(), block_energies);
+    return ALEA_OK;
+}
+
+int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
+                     double* block_energies) {
+    if (!c || !cfg || !res) return ALEA_ERR_INVALID;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int target = cfg->target_walkers > 0 ? cfg->target_walkers : c->nw;
+    const int n_threads = std::max(1, std::min(cfg->n_streams > 0 ? cfg->n_streams : c->nw, c->nw));
+    if (int rc = alea_gpu_set_streams(c, cfg->seed, ALEA_STREAM_DMC, n_threads)) return rc;
+    HostXo brng(stream_seed(cfg->seed, ALEA_STREAM_BRANCH, 0));
+    uint64_t bstate[4];
+    std::memcpy(bstate, brng.s, 32);
+    // diffusing particles (dmc.cpp:50-66)
+    double max_inv = 0.0;
+    for (double x : c->h_inv_mass) max_inv = std::max(max_inv, x);
+    int n_diff = 0;
+    for (int g = 0; g < c->sys.ngroups; ++g) {
+        const int i = c->sys.gfirst[g];
+        const double gi = std::max(c->h_inv_mass[i * 2], c->h_inv_mass[i * 2 + 1]);
+        if (gi >= 1e-3 * max_inv) n_diff += c->sys.glast[g] - c->sys.gfirst[g];
+    }
+    n_diff = std::max(n_diff, 1);
+    const double tau = cfg->tau;
+    const double t_step = tau * std::max(1, cfg->n_substeps);
+    const double feedback = (t_step > 0.0 && cfg->population_generations > 0.0)
+                                ? 1.0 / (cfg->population_generations * t_step) : 0.0;
+    const double alpha = cfg->branch_cutoff_alpha > 0.0 ? cfg->branch_cutoff_alpha : 2.0;
+    std::vector<double> el;
+    if (int rc = read_scalars(c, S_EL, el)) return rc;
+    double e0 = 0.0;
+    for (double x : el) e0 += x;
+    double etrial = e0 / static_cast<double>(c->nw), eref = etrial, eref_sum = 0.0, eref_wsum = 0.0;
+    double e_cut = INFINITY, e_max = INFINITY;
+    auto refresh_spread = [&](const std::vector<double>& e) {
+        const double sigma = robust_spread(e.data(), e.size());
+        if (!(std::isfinite(sigma) && sigma > 0.0 && tau > 0.0)) {
+            e_cut = e_max = INFINITY;
+        } else {
+            e_cut = alpha * std::sqrt(sigma * std::sqrt(static_cast<double>(n_diff)) / tau);
+            e_max = 1.5 * e_cut;
+        }
+    };
+    refresh_spread(el);
+    std::vector<double> blocks;
+    int64_t acc = 0, prop = 0;
+    for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
+        const bool measure = b >= cfg->n_equilibration_blocks;
+        if (b == cfg->n_equilibration_blocks) eref_sum = eref_wsum = 0.0;
+        double blk_e = 0.0, blk_w = 0.0;
+        for (int st = 0; st < cfg->n_steps; ++st) {
+            alea_gpu_dmc_params prm{tau, cfg->n_substeps, etrial, eref, e_cut, e_max};
+            alea_gpu_step_stats s{};
+            if (int rc = alea_gpu_dmc_advance(c, &prm, &s)) return rc;
+            acc += s.n_accepted;
+            prop += s.n_proposed;
+            blk_e += s.energy_sum;
+            blk_w += s.weight_sum;
+            const double ens_e = s.weight_sum > 0.0 ? s.energy_sum / s.weight_sum : etrial;
+            if (int rc = alea_gpu_dmc_branch(c, bstate, target)) return rc;
+            if (measure) {
+                eref_sum += ens_e * s.weight_sum;
+                eref_wsum += s.weight_sum;
+                if (eref_wsum > 0.0) eref = eref_sum / eref_wsum;
+            } else {
+                eref = ens_e;
+            }
+            if (s.weight_sum > 0.0)
+                etrial = eref - feedback * std::log(s.weight_sum / static_cast<double>(target));
+        }
+        if (measure) blocks.push_back(blk_w > 0.0 ? blk_e / blk_w : 0.0);
+        else {
+            if (int rc = read_scalars(c, S_EL, el)) return rc;
+            refresh_spread(el);
+        }
+    }
+    double mean = 0.0, err = 0.0;
+    reblock(blocks, mean, err);
+    res->energy = mean;
+    res->energy_error = err;
+    double var = 0.0;
+    for (double x : blocks) var += (x - mean) * (x - mean);
+    res->variance = blocks.size() >= 2 ? var / static_cast<double>(blocks.size() - 1) : 0.0;
+    res->acceptance = prop ? static_cast<double>(acc) / static_cast<double>(prop) : 0.0;
+    res->walltime_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    res->n_walkers = c->nw;
+    res->e_trial = etrial;
+    if (block_energies) std::copy(blocks.begin(), blocks.end(), block_energies);
+    return ALEA_OK;
+}
+
+}  // extern "C"

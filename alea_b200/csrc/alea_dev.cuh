@@ -1,0 +1,433 @@
+// Device-side system description, walker record layout and the per-walker
+// math shared by the walker kernels (sm_100a).
+//
+// One CTA owns one walker for a whole sweep.  The walker's hot state (position,
+// Jastrow and Slater gradient/Laplacian planes, inverse matrices, k-space
+// structure factors and phase cache) is staged from its HBM record into shared
+// memory at kernel start and written back at the end; the orbital rows D, ∇D,
+// ∇²D stay in HBM and are touched one row per accepted move.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace alea_gpu {
+
+constexpr int kThreads = 128;          // threads per walker CTA
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxBlocks = 4;
+constexpr int kMaxTerms = 8;
+constexpr int kMaxGroups = 8;
+constexpr int kMaxCoulomb = 8;
+constexpr int kMaxN = 64;              // largest determinant block
+constexpr int kMaxLadder = 64;         // largest |n| of a reciprocal index
+
+// Scalar slots of a walker record.
+enum : int {
+    S_LOGPSI = 0, S_EL, S_WEIGHT, S_EPREV, S_RRP, S_RRA, S_AGE, S_ID, S_PARENT, S_ERR,
+    S_NACC, S_NCUT, S_BLOCK0 /* 3 per block: log|det|, updates, condition */,
+    S_NSCAL = S_BLOCK0 + 3 * kMaxBlocks
+};
+
+struct DevSpline {
+    double r_cut, inv_delta;
+    int n_knots;
+    const double* scaled;
+};
+
+struct DevTerm {
+    int kind;                 // 0 Padé, 1 Drummond
+    int npairs;
+    int pairs[4][4];
+    int nnum, nden;
+    double coef[16];
+    int image;
+    DevSpline sp;
+    double u_inf;
+    const double* kw;         // weights on the shared Jastrow k set
+    int same0;                // pairs[0] is a same-group pair
+    int C;
+    double gamma, L, alpha1;
+    int ncoef;
+    double dc[16];
+};
+
+struct DevBlock {
+    int first, last, n, type;
+    const double* k;          // plane waves [n*dim]
+    const double* is_sin;     // [n] (0/1)
+    const double* centers;    // Gaussians [n*dim]
+    const double* alphas;     // [n]
+    int oA;                   // record offset of A (hot)
+    int orabs;                // record offset of the row |D| sums (hot)
+    long oD, oDg, oDl;        // record offsets of D, ∇D, ∇²D (cold)
+};
+
+struct DevSys {
+    int dim, np, periodic, ortho;
+    double a[4], ainv[4], box[3], inv_box[3], cand[18], recip[4];
+    int ngroups;
+    int gfirst[kMaxGroups], glast[kMaxGroups];
+    double gcharge[kMaxGroups];
+    const double* inv_mass;   // [np*dim]
+    const double* charge;     // [np]
+    const int* group_of;      // [np]
+    int nblocks, maxN;
+    DevBlock blocks[kMaxBlocks];
+    int nterms;
+    DevTerm terms[kMaxTerms];
+    // reciprocal vectors shared by every image-summed Jastrow term
+    int nkJ, m1J, m2J;
+    const int *n1J, *n2J;
+    const double *kxJ, *kyJ, *kx2J, *ky2J;
+    // Ewald
+    int ewald;
+    DevSpline esp;
+    double e_rcut, e_inv_eps, e_const;
+    int enk, e_m1, e_m2;
+    const int *en1, *en2;
+    const double* ew;
+    int ncoul;
+    int coul[kMaxCoulomb][4];
+    double coul_coef[kMaxCoulomb];
+    // record layout (doubles): hot part [0, hot) is staged in shared memory
+    long rec;                 // record stride
+    int hot;
+    int o_pos, o_jg, o_jl, o_sg, o_sl, o_scal, o_rho, o_pc;
+    // shared-memory scratch layout (doubles, after the hot part)
+    int s_newpos, s_nval, s_ngrad, s_nlap, s_rad, s_cn, s_sn, s_dr, s_di, s_col, s_rowp,
+        s_red, s_misc, s_work, s_total;
+    // ziggurat tables
+    const uint64_t* zk;
+    const double *zw, *zf;
+    double zr;
+};
+
+// ───────────────────────── cell ─────────────────────────────────────────
+
+__device__ __forceinline__ void min_image(const DevSys& s, double* del) {
+    if (!s.periodic) return;
+    if (s.ortho) {
+        for (int d = 0; d < s.dim; ++d) del[d] = fma(-s.box[d], rint(del[d] * s.inv_box[d]), del[d]);
+        return;
+    }
+    // General 2-D Bravais fold, in the operation order (and with the FMA
+    // contraction) of the reference's fold_bravais_2d, branch-free select.
+    double x0 = del[0], x1 = del[1];
+    const double f0 = rint(fma(s.ainv[1], x1, s.ainv[0] * x0));
+    const double f1 = rint(fma(s.ainv[3], x1, s.ainv[2] * x0));
+    x0 -= fma(f1, s.a[2], f0 * s.a[0]);
+    x1 -= fma(f1, s.a[3], f0 * s.a[1]);
+    double b0 = x0, b1 = x1, best2 = fma(x1, x1, x0 * x0);
+    for (int c = 1; c < 9; ++c) {
+        const double y0 = x0 + s.cand[c * 2 + 0];
+        const double y1 = x1 + s.cand[c * 2 + 1];
+        const double r2 = fma(y1, y1, y0 * y0);
+        const double take = (r2 < best2) ? 1.0 : 0.0;
+        best2 = fma(take, r2 - best2, best2);
+        b0 = fma(take, y0 - b0, b0);
+        b1 = fma(take, y1 - b1, b1);
+    }
+    del[0] = b0;
+    del[1] = b1;
+}
+
+__device__ __forceinline__ void wrap_pos(const DevSys& s, double* r) {
+    if (!s.periodic) return;
+    if (s.ortho) {
+        for (int d = 0; d < s.dim; ++d) r[d] = fma(-s.box[d], rint(r[d] * s.inv_box[d]), r[d]);
+        return;
+    }
+    const double f0 = rint(fma(s.ainv[1], r[1], s.ainv[0] * r[0]));
+    const double f1 = rint(fma(s.ainv[3], r[1], s.ainv[2] * r[0]));
+    r[0] -= fma(f1, s.a[2], f0 * s.a[0]);
+    r[1] -= fma(f1, s.a[3], f0 * s.a[1]);
+}
+
+// Folded displacement xi - xj and its length.
+__device__ __forceinline__ double fold_dist(const DevSys& s, const double* xi, const double* xj,
+                                            double* del) {
+    for (int d = 0; d < s.dim; ++d) del[d] = xi[d] - xj[d];
+    min_image(s, del);
+    double r2 = del[0] * del[0];
+    for (int d = 1; d < s.dim; ++d) r2 = fma(del[d], del[d], r2);
+    return sqrt(r2);
+}
+
+// ───────────────────────── radial functions ─────────────────────────────
+
+__device__ __forceinline__ void spline3(const DevSpline& sp, double r, double& f, double& df,
+                                        double& d2f) {
+    if (r >= sp.r_cut) {
+        f = df = d2f = 0.0;
+        return;
+    }
+    const double t = r * sp.inv_delta;
+    int i = static_cast<int>(t);
+    if (i > sp.n_knots - 2) i = sp.n_knots - 2;
+    const double x = t - i, y = 1.0 - x;
+    const double* a = sp.scaled + 3 * i;
+    const double* b = a + 3;
+    const double x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x;
+    const double y2 = y * y, y3 = y2 * y, y4 = y3 * y, y5 = y4 * y;
+    const double p0 = 1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5;
+    const double p1 = x - 6.0 * x3 + 8.0 * x4 - 3.0 * x5;
+    const double p2 = 0.5 * x2 - 1.5 * x3 + 1.5 * x4 - 0.5 * x5;
+    const double q0 = 1.0 - 10.0 * y3 + 15.0 * y4 - 6.0 * y5;
+    const double q1 = y - 6.0 * y3 + 8.0 * y4 - 3.0 * y5;
+    const double q2 = 0.5 * y2 - 1.5 * y3 + 1.5 * y4 - 0.5 * y5;
+    const double dp0 = -30.0 * x2 + 60.0 * x3 - 30.0 * x4;
+    const double dp1 = 1.0 - 18.0 * x2 + 32.0 * x3 - 15.0 * x4;
+    const double dp2 = x - 4.5 * x2 + 6.0 * x3 - 2.5 * x4;
+    const double dq0 = -30.0 * y2 + 60.0 * y3 - 30.0 * y4;
+    const double dq1 = 1.0 - 18.0 * y2 + 32.0 * y3 - 15.0 * y4;
+    const double dq2 = y - 4.5 * y2 + 6.0 * y3 - 2.5 * y4;
+    const double ddp0 = -60.0 * x + 180.0 * x2 - 120.0 * x3;
+    const double ddp1 = -36.0 * x + 96.0 * x2 - 60.0 * x3;
+    const double ddp2 = 1.0 - 9.0 * x + 18.0 * x2 - 10.0 * x3;
+    const double ddq0 = -60.0 * y + 180.0 * y2 - 120.0 * y3;
+    const double ddq1 = -36.0 * y + 96.0 * y2 - 60.0 * y3;
+    const double ddq2 = 1.0 - 9.0 * y + 18.0 * y2 - 10.0 * y3;
+    f = a[0] * p0 + a[1] * p1 + a[2] * p2 + b[0] * q0 - b[1] * q1 + b[2] * q2;
+    df = sp.inv_delta * (a[0] * dp0 + a[1] * dp1 + a[2] * dp2 - (b[0] * dq0 - b[1] * dq1 + b[2] * dq2));
+    d2f = sp.inv_delta * sp.inv_delta *
+          (a[0] * ddp0 + a[1] * ddp1 + a[2] * ddp2 + b[0] * ddq0 - b[1] * ddq1 + b[2] * ddq2);
+}
+
+__device__ __forceinline__ double spline1(const DevSpline& sp, double r) {
+    if (r >= sp.r_cut) return 0.0;
+    const double t = r * sp.inv_delta;
+    int i = static_cast<int>(t);
+    if (i > sp.n_knots - 2) i = sp.n_knots - 2;
+    const double x = t - i, y = 1.0 - x;
+    const double* a = sp.scaled + 3 * i;
+    const double* b = a + 3;
+    const double x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x;
+    const double y2 = y * y, y3 = y2 * y, y4 = y3 * y, y5 = y4 * y;
+    const double p0 = 1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5;
+    const double p1 = x - 6.0 * x3 + 8.0 * x4 - 3.0 * x5;
+    const double p2 = 0.5 * x2 - 1.5 * x3 + 1.5 * x4 - 0.5 * x5;
+    const double q0 = 1.0 - 10.0 * y3 + 15.0 * y4 - 6.0 * y5;
+    const double q1 = y - 6.0 * y3 + 8.0 * y4 - 3.0 * y5;
+    const double q2 = 0.5 * y2 - 1.5 * y3 + 1.5 * y4 - 0.5 * y5;
+    return a[0] * p0 + a[1] * p1 + a[2] * p2 + b[0] * q0 - b[1] * q1 + b[2] * q2;
+}
+
+__device__ __forceinline__ void poly_acc(const double* c, int n, double r, double& v, double& dv,
+                                         double& d2v) {
+    double r_km1 = 1.0, r_km2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const int k = i + 1;
+        v += c[i] * r_km1 * r;
+        dv += c[i] * k * r_km1;
+        d2v += c[i] * k * (k - 1) * r_km2;
+        r_km2 = r_km1;
+        r_km1 *= r;
+    }
+}
+
+// u, u', u'' of a pair term at r (the short-range half for an image sum).
+__device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, double& du,
+                                       double& d2u) {
+    if (T.kind == 0) {
+        double p = 0.0, dp = 0.0, d2p = 0.0;
+        poly_acc(T.coef, T.nnum, r, p, dp, d2p);
+        double q = 1.0, dq = 0.0, d2q = 0.0;
+        poly_acc(T.coef + T.nnum, T.nden, r, q, dq, d2q);
+        const double inv_q = 1.0 / q;
+        u = p * inv_q;
+        du = (dp * q - p * dq) * inv_q * inv_q;
+        d2u = (d2p - (2.0 * dp * dq - 2.0 * p * dq * dq * inv_q + p * d2q) * inv_q) * inv_q;
+        if (T.image) {
+            if (r >= T.sp.r_cut) {
+                u = du = d2u = 0.0;
+                return;
+            }
+            double f, df, d2f;
+            spline3(T.sp, r, f, df, d2f);
+            u -= T.u_inf + f;
+            du -= df;
+            d2u -= d2f;
+        }
+        return;
+    }
+    const double t = r - T.L;
+    double tCm2 = 1.0;
+    for (int i = 0; i < T.C - 2; ++i) tCm2 *= t;
+    const double tCm1 = tCm2 * t, tC = tCm1 * t;
+    const double g = tC, dg = static_cast<double>(T.C) * tCm1,
+                 d2g = static_cast<double>(T.C) * (T.C - 1) * tCm2;
+    double P = T.dc[0] + T.alpha1 * r, dP = T.alpha1, d2P = 0.0;
+    double r_lm2 = 1.0, r_lm1 = r, r_l = r * r;
+    for (int k = 1; k < T.ncoef; ++k) {
+        const int l = k + 1;
+        const double c = T.dc[k];
+        P += c * r_l;
+        dP += c * l * r_lm1;
+        d2P += c * l * (l - 1) * r_lm2;
+        r_lm2 = r_lm1;
+        r_lm1 = r_l;
+        r_l *= r;
+    }
+    const double m = (r < T.L) ? 1.0 : 0.0;
+    u = m * (g * P);
+    du = m * (dg * P + g * dP);
+    d2u = m * (d2g * P + 2.0 * dg * dP + g * d2P);
+}
+
+// Does term T couple particles p and k (any of its group pairs)?
+__device__ __forceinline__ bool couples(const DevTerm& T, int p, int k) {
+    for (int q = 0; q < T.npairs; ++q) {
+        const int af = T.pairs[q][0], al = T.pairs[q][1], bf = T.pairs[q][2], bl = T.pairs[q][3];
+        const bool pa = p >= af && p < al, pb = p >= bf && p < bl;
+        const bool ka = k >= af && k < al, kb = k >= bf && k < bl;
+        if (af == bf && al == bl) {
+            if (pa && ka && p != k) return true;
+        } else if ((pa && kb) || (pb && ka)) {
+            return true;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool in_term(const DevTerm& T, int p) {
+    for (int q = 0; q < T.npairs; ++q)
+        if ((p >= T.pairs[q][0] && p < T.pairs[q][1]) || (p >= T.pairs[q][2] && p < T.pairs[q][3]))
+            return true;
+    return false;
+}
+
+// ───────────────────────── orbitals ─────────────────────────────────────
+
+// Orbital i of block B at position r: value, gradient[dim], Laplacian[dim].
+__device__ __forceinline__ void orbital(const DevSys& s, const DevBlock& B, int i, const double* r,
+                                        double& val, double* grad, double* lap) {
+    const int dim = s.dim;
+    if (B.type == 0) {
+        const double* ki = B.k + i * dim;
+        double phase = 0.0;
+        for (int d = 0; d < dim; ++d) phase += ki[d] * r[d];
+        double sn, c;
+        sincos(phase, &sn, &c);
+        if (B.is_sin[i] != 0.0) {
+            val = sn;
+            for (int d = 0; d < dim; ++d) {
+                grad[d] = ki[d] * c;
+                lap[d] = -ki[d] * ki[d] * sn;
+            }
+        } else {
+            val = c;
+            for (int d = 0; d < dim; ++d) {
+                grad[d] = -ki[d] * sn;
+                lap[d] = -ki[d] * ki[d] * c;
+            }
+        }
+    } else {
+        const double alpha = B.alphas[i];
+        double del[3];
+        for (int d = 0; d < dim; ++d) del[d] = r[d] - B.centers[i * dim + d];
+        min_image(s, del);
+        double r2 = 0.0;
+        for (int d = 0; d < dim; ++d) r2 += del[d] * del[d];
+        const double phi = exp(-alpha * r2);
+        val = phi;
+        for (int d = 0; d < dim; ++d) {
+            grad[d] = phi * (-2.0 * alpha * del[d]);
+            lap[d] = phi * (4.0 * alpha * alpha * del[d] * del[d] - 2.0 * alpha);
+        }
+    }
+}
+
+// ───────────────────────── reductions ───────────────────────────────────
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum K values over the CTA; every thread gets the totals.  `red` holds
+// kWarps*K + K doubles.  Contains two barriers.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[warp * K + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double t = 0.0;
+        for (int w = 0; w < kWarps; ++w) t += red[w * K + threadIdx.x];
+        red[kWarps * K + threadIdx.x] = t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = red[kWarps * K + k];
+    __syncthreads();
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double m = red[0];
+    for (int w = 1; w < kWarps; ++w) m = fmax(m, red[w]);
+    __syncthreads();
+    return m;
+}
+
+// ───────────────────────── random numbers ───────────────────────────────
+
+struct Xo {
+    uint64_t s0, s1, s2, s3;
+};
+
+__device__ __forceinline__ uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+__device__ __forceinline__ uint64_t xo_next(Xo& r) {
+    const uint64_t result = rotl64(r.s0 + r.s3, 23) + r.s0;
+    const uint64_t t = r.s1 << 17;
+    r.s2 ^= r.s0;
+    r.s3 ^= r.s1;
+    r.s1 ^= r.s2;
+    r.s0 ^= r.s3;
+    r.s2 ^= t;
+    r.s3 = rotl64(r.s3, 45);
+    return result;
+}
+
+__device__ __forceinline__ double xo_uniform(Xo& r) {
+    return static_cast<double>(static_cast<int64_t>(xo_next(r) >> 11)) * 0x1.0p-53;
+}
+
+// Ziggurat normal deviate with the region/sign/position split of the
+// reference's XoshiroRandom::gaussian.
+__device__ __forceinline__ double xo_gaussian(Xo& r, const uint64_t* zk, const double* zw,
+                                              const double* zf, double zr) {
+    for (int guard = 0; guard < 1 << 20; ++guard) {
+        const uint64_t bits = xo_next(r);
+        const unsigned i = static_cast<unsigned>(bits & 0xff);
+        const uint64_t sign = (bits & 0x100) << 55;
+        const uint64_t position = (bits >> 9) & ((uint64_t{1} << 52) - 1);
+        const double x = static_cast<double>(static_cast<int64_t>(position)) * zw[i];
+        if (position < zk[i]) return __longlong_as_double(__double_as_longlong(x) ^ sign);
+        if (i == 0) {
+            for (int g2 = 0; g2 < 1 << 20; ++g2) {
+                const double xi = -log1p(-xo_uniform(r)) / zr;
+                const double y = -log1p(-xo_uniform(r));
+                if (y + y > xi * xi)
+                    return __longlong_as_double(__double_as_longlong(zr + xi) ^ sign);
+            }
+            return 0.0;
+        }
+        if (zf[i] + xo_uniform(r) * (zf[i - 1] - zf[i]) < exp(-0.5 * x * x))
+            return __longlong_as_double(__double_as_longlong(x) ^ sign);
+    }
+    return 0.0;
+}
+
+}  // namespace alea_gpu

@@ -1,0 +1,1073 @@
+// Walker kernels for sm_100a: full evaluation, the fused VMC/DMC sweep
+// (propose → ratio → accept → commit for every particle, then the derivative
+// refresh, E_L and the DMC branch factor), single moves for the component-level
+// ABI, the per-stream random-number draw and the branching gather.
+//
+// Algorithms restated from the reference (ItaloAlb/alea):
+//   sweep          src/qmc/vmc.cpp:82-155 (Metropolis / Langevin),
+//                  src/qmc/dmc.cpp:203-337 (Umrigar drift, node gate, drift
+//                  Green's function), src/numerics/green_function.h:20-58
+//   Slater         src/wavefunction/slater_determinant.cpp:395-437 (ratio),
+//                  :515-726 (Sherman-Morrison commit and rebuild triggers),
+//                  :862-903 (derivative refresh), :905-993 (Gauss-Jordan)
+//   pair Jastrows  src/wavefunction/pade_jastrow.cpp:347-634,
+//                  src/wavefunction/radial_pair_jastrow_impl.h
+//   image sums     src/wavefunction/kspace_pair_sum.cpp:139-301
+//   E_L            src/hamiltonian/kinetic.cpp:45-72, ewald_term.cpp:368-612,
+//                  coulomb.cpp:31-61
+//   branch weight  src/qmc/population_control.cpp:56-77
+//   randoms        src/qmc/sweep_blocking.h:39-48
+//
+// Parallel layout: one CTA of kThreads threads per walker.  Work inside a
+// move is spread over orbitals (Slater), partners (pair terms), k-vectors
+// (image sums), matrix elements (rank-one update) and seers (k-space partner
+// gradients); partial sums meet in block reductions.
+#include <cstdio>
+
+#include "alea_dev.cuh"
+#include "alea_kernels.h"
+
+namespace alea_gpu {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kEps = 2.220446049250313e-16;
+
+struct Smem {
+    double *pos, *jg, *jl, *sg, *sl, *scal, *rho, *pc;
+    double *newpos, *nval, *ngrad, *nlap, *rad, *geo, *cn, *sn, *dr, *di, *col, *rowp, *red,
+        *misc, *work;
+};
+
+__device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
+    Smem v;
+    v.pos = sm + s.o_pos;
+    v.jg = sm + s.o_jg;
+    v.jl = sm + s.o_jl;
+    v.sg = sm + s.o_sg;
+    v.sl = sm + s.o_sl;
+    v.scal = sm + s.o_scal;
+    v.rho = sm + s.o_rho;
+    v.pc = sm + s.o_pc;
+    v.newpos = sm + s.s_newpos;
+    v.nval = sm + s.s_nval;
+    v.ngrad = sm + s.s_ngrad;
+    v.nlap = sm + s.s_nlap;
+    v.rad = sm + s.s_rad;
+    v.geo = v.rad + static_cast<long>(s.nterms) * s.np * 6;
+    v.cn = sm + s.s_cn;
+    v.sn = sm + s.s_sn;
+    v.dr = sm + s.s_dr;
+    v.di = sm + s.s_di;
+    v.col = sm + s.s_col;
+    v.rowp = sm + s.s_rowp;
+    v.red = sm + s.s_red;
+    v.misc = sm + s.s_misc;
+    v.work = sm + s.s_work;
+    return v;
+}
+
+// misc slots
+enum : int {
+    M_R = 0, M_SCALE, M_LOGR, M_PHASE, M_ACCEPT, M_REBUILD, M_LOGDET, M_ERR, M_NORMD,
+    M_SGX, M_SGY, M_SLX, M_SLY, M_JGX, M_JGY, M_JLX, M_JLY, M_U, M_SCFWD, M_GOX, M_GOY,
+    M_LAD /* two ladders of kMaxLadder + 1 complex values follow */
+};
+
+__device__ __forceinline__ void load_hot(const DevSys& s, const double* rec, double* sm) {
+    const double2* src = reinterpret_cast<const double2*>(rec);
+    double2* dst = reinterpret_cast<double2*>(sm);
+    for (int i = threadIdx.x; i < s.hot / 2; i += kThreads) dst[i] = src[i];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void store_hot(const DevSys& s, double* rec, const double* sm) {
+    __syncthreads();
+    const double2* src = reinterpret_cast<const double2*>(sm);
+    double2* dst = reinterpret_cast<double2*>(rec);
+    for (int i = threadIdx.x; i < s.hot / 2; i += kThreads) dst[i] = src[i];
+}
+
+__device__ __forceinline__ int block_of(const DevSys& s, int p) {
+    for (int b = 0; b < s.nblocks; ++b)
+        if (p >= s.blocks[b].first && p < s.blocks[b].last) return b;
+    return -1;
+}
+
+// e^{i n θ} for n = 0..m into (re, im) pairs at out[2n], out[2n+1].
+__device__ __forceinline__ void ladder(double theta, int m, double* out) {
+    double c, sn;
+    sincos(theta, &sn, &c);
+    double r = 1.0, i = 0.0;
+    out[0] = 1.0;
+    out[1] = 0.0;
+    for (int n = 1; n <= m; ++n) {
+        const double nr = r * c - i * sn;
+        const double ni = r * sn + i * c;
+        r = nr;
+        i = ni;
+        out[2 * n] = r;
+        out[2 * n + 1] = i;
+    }
+}
+
+__device__ __forceinline__ void ladder_pick(const double* lad, int n, double& re, double& im) {
+    const int a = n < 0 ? -n : n;
+    re = lad[2 * a];
+    im = n < 0 ? -lad[2 * a + 1] : lad[2 * a + 1];
+}
+
+// ───────────────────────── Gauss-Jordan rebuild ─────────────────────────
+
+// A = D⁻¹ of block b from its committed rows in HBM, by pivoted Gauss-Jordan
+// (first maximum |pivot| in each column, as the reference's rebuild_inverse).
+// Returns log|det D| in misc[M_LOGDET]; flags a singular matrix in misc[M_ERR].
+__device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, int b) {
+    const DevBlock& B = s.blocks[b];
+    const int N = B.n;
+    double* A = v.scal - s.o_scal + B.oA;   // hot-part base + offset
+    double* m = v.work;
+    const double* D = grec + B.oD;
+    for (int e = threadIdx.x; e < N * N; e += kThreads) {
+        m[e] = D[e];
+        A[e] = (e / N == e % N) ? 1.0 : 0.0;
+    }
+    if (threadIdx.x == 0) v.misc[M_LOGDET] = 0.0;
+    __syncthreads();
+    __shared__ int s_piv;
+    for (int k = 0; k < N; ++k) {
+        if (threadIdx.x < 32) {
+            // warp argmax over rows r >= k of |m[r][k]|, ties to the lowest row
+            double best = -1.0;
+            int bi = N;
+            for (int r = k + static_cast<int>(threadIdx.x); r < N; r += 32) {
+                const double a = fabs(m[r * N + k]);
+                if (a > best) {
+                    best = a;
+                    bi = r;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                s_piv = bi;
+                const double diag = m[bi * N + k];
+                if (diag == 0.0 || !isfinite(diag)) v.misc[M_ERR] = 1.0;
+                v.misc[M_LOGDET] += log(fabs(diag));
+            }
+        }
+        __syncthreads();
+        const int piv = s_piv;
+        if (piv != k)
+            for (int c = threadIdx.x; c < N; c += kThreads) {
+                double t = m[k * N + c];
+                m[k * N + c] = m[piv * N + c];
+                m[piv * N + c] = t;
+                t = A[k * N + c];
+                A[k * N + c] = A[piv * N + c];
+                A[piv * N + c] = t;
+            }
+        __syncthreads();
+        const double diag = m[k * N + k];
+        __syncthreads();
+        for (int c = threadIdx.x; c < N; c += kThreads) {
+            m[k * N + c] /= diag;
+            A[k * N + c] /= diag;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < N; r += kThreads) v.col[r] = m[r * N + k];
+        __syncthreads();
+        for (int e = threadIdx.x; e < N * N; e += kThreads) {
+            const int r = e / N, c = e % N;
+            if (r == k) continue;
+            const double f = v.col[r];
+            m[e] -= f * m[k * N + c];
+            A[e] -= f * A[k * N + c];
+        }
+        __syncthreads();
+    }
+}
+
+// ───────────────────────── Slater ───────────────────────────────────────
+
+// Slater derivatives of particle p from A and the committed rows.
+__device__ void slater_refresh_particle(const DevSys& s, const Smem& v, const double* grec, int p) {
+    const int b = block_of(s, p);
+    if (b < 0) return;   // block-uniform
+    const DevBlock& B = s.blocks[b];
+    const int N = B.n, kr = p - B.first;
+    const double* A = v.scal - s.o_scal + B.oA;
+    const double* Dg = grec + B.oDg;
+    const double* Dl = grec + B.oDl;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int m = threadIdx.x; m < N; m += kThreads) {
+        const double a = A[m * N + kr];
+        acc[0] += a * Dg[(kr * N + m) * 2 + 0];
+        acc[1] += a * Dg[(kr * N + m) * 2 + 1];
+        acc[2] += a * Dl[(kr * N + m) * 2 + 0];
+        acc[3] += a * Dl[(kr * N + m) * 2 + 1];
+    }
+    block_sum<4>(acc, v.red);
+    if (threadIdx.x == 0) {
+        v.sg[p * 2 + 0] = acc[0];
+        v.sg[p * 2 + 1] = acc[1];
+        v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
+        v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
+    }
+    __syncthreads();
+}
+
+// Every particle's Slater derivatives (refresh_derivatives).
+__device__ void slater_refresh_all(const DevSys& s, const Smem& v, const double* grec) {
+    for (int b = 0; b < s.nblocks; ++b) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n;
+        const double* A = v.scal - s.o_scal + B.oA;
+        const double* Dg = grec + B.oDg;
+        const double* Dl = grec + B.oDl;
+        for (int t = threadIdx.x; t < N * 2; t += kThreads) {
+            const int kr = t >> 1, d = t & 1;
+            double g = 0.0, l = 0.0;
+            for (int m = 0; m < N; ++m) {
+                const double a = A[m * N + kr];
+                g += a * Dg[(kr * N + m) * 2 + d];
+                l += a * Dl[(kr * N + m) * 2 + d];
+            }
+            const int part = B.first + kr;
+            v.sg[part * 2 + d] = g;
+            v.sl[part * 2 + d] = l - g * g;
+        }
+    }
+    __syncthreads();
+}
+
+// ───────────────────────── ratio ────────────────────────────────────────
+
+// ln|ψ'/ψ| of moving p to v.newpos; leaves in misc: R, scale, the log ratio,
+// phase, the Slater and Jastrow parts of ∇ ln ψ and ∂² ln ψ at the proposal;
+// in smem: new orbital row (nval/ngrad/nlap), per (term, partner) radial
+// values (rad), partner geometry (geo) and p's new phases (cn/sn).
+__device__ void ratio_step(const DevSys& s, const Smem& v, int p) {
+    const int np = s.np;
+    const int b = block_of(s, p);
+    bool kspace = false;
+    for (int t = 0; t < s.nterms; ++t)
+        if (s.terms[t].image && in_term(s.terms[t], p)) kspace = true;
+    // phase 1: ladders of p's new position, orbitals, partners
+    double acc[11];
+#pragma unroll
+    for (int i = 0; i < 11; ++i) acc[i] = 0.0;
+    if (kspace && threadIdx.x < 2) {
+        const int q = threadIdx.x;
+        const double th = s.recip[q * 2] * v.newpos[0] + s.recip[q * 2 + 1] * v.newpos[1];
+        ladder(th, q == 0 ? s.m1J : s.m2J, v.misc + M_LAD + q * 2 * (kMaxLadder + 1));
+    }
+    if (b >= 0) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, jrow = p - B.first;
+        const double* A = v.scal - s.o_scal + B.oA;
+        for (int m = threadIdx.x; m < N; m += kThreads) {
+            double val, g[3], l[3];
+            orbital(s, B, m, v.newpos, val, g, l);
+            v.nval[m] = val;
+            v.ngrad[m * 2 + 0] = g[0];
+            v.ngrad[m * 2 + 1] = g[1];
+            v.nlap[m * 2 + 0] = l[0];
+            v.nlap[m * 2 + 1] = l[1];
+            const double a = A[m * N + jrow];
+            const double term = a * val;
+            acc[0] += term;
+            acc[1] += fabs(term);
+            acc[2] += a * g[0];
+            acc[3] += a * g[1];
+            acc[4] += a * l[0];
+            acc[5] += a * l[1];
+        }
+    }
+    for (int k = threadIdx.x; k < np; k += kThreads) {
+        if (k == p) continue;
+        double dn[3], dold[3];
+        const double rn = fold_dist(s, v.newpos, v.pos + k * 2, dn);
+        const double ro = fold_dist(s, v.pos + p * 2, v.pos + k * 2, dold);
+        double* geo = v.geo + k * 6;
+        geo[0] = dn[0];
+        geo[1] = dn[1];
+        geo[2] = rn;
+        geo[3] = dold[0];
+        geo[4] = dold[1];
+        geo[5] = ro;
+        const double invr = 1.0 / rn;
+        for (int t = 0; t < s.nterms; ++t) {
+            const DevTerm& T = s.terms[t];
+            if (!couples(T, p, k)) continue;
+            double* rad = v.rad + (static_cast<long>(t) * np + k) * 6;
+            radial(T, ro, rad[0], rad[1], rad[2]);
+            radial(T, rn, rad[3], rad[4], rad[5]);
+            acc[6] += rad[3] - rad[0];
+            for (int d = 0; d < 2; ++d) {
+                const double dor = dn[d] * invr;
+                acc[7 + d] += rad[4] * dor;
+                acc[9 + d] += rad[5] * dor * dor + rad[4] * invr * (1.0 - dor * dor);
+            }
+        }
+    }
+    __syncthreads();
+    // phase 2: p's new phases and the reciprocal half of every image sum
+    if (kspace) {
+        const double* l1 = v.misc + M_LAD;
+        const double* l2 = v.misc + M_LAD + 2 * (kMaxLadder + 1);
+        const int nk = s.nkJ;
+        const double* co = v.pc + p * 2 * nk;
+        const double* so = co + nk;
+        const int gp = s.group_of[p];
+        for (int k = threadIdx.x; k < nk; k += kThreads) {
+            double ar, ai, br, bi;
+            ladder_pick(l1, s.n1J[k], ar, ai);
+            ladder_pick(l2, s.n2J[k], br, bi);
+            const double c = ar * br - ai * bi;
+            const double sn = ar * bi + ai * br;
+            v.cn[k] = c;
+            v.sn[k] = sn;
+            for (int t = 0; t < s.nterms; ++t) {
+                const DevTerm& T = s.terms[t];
+                if (!T.image || !in_term(T, p)) continue;
+                const double w = T.kw[k];
+                const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+                const double* mr = v.rho + gp * 2 * nk;
+                double pr, pi, self, dlog;
+                if (T.same0) {
+                    const double qr = mr[k] + c - co[k];
+                    const double qi = mr[nk + k] + sn - so[k];
+                    dlog = w * (qr * qr + qi * qi - mr[k] * mr[k] - mr[nk + k] * mr[nk + k]);
+                    pr = qr;
+                    pi = qi;
+                    self = 1.0;
+                } else {
+                    const int go = gp == ga ? gb : ga;
+                    const double* orr = v.rho + go * 2 * nk;
+                    dlog = 2.0 * w * ((c - co[k]) * orr[k] + (sn - so[k]) * orr[nk + k]);
+                    pr = orr[k];
+                    pi = orr[nk + k];
+                    self = 0.0;
+                }
+                const double g = 2.0 * w * (c * pi - sn * pr);
+                const double l = 2.0 * w * (self - (c * pr + sn * pi));
+                acc[6] += dlog;
+                acc[7] += s.kxJ[k] * g;
+                acc[8] += s.kyJ[k] * g;
+                acc[9] += s.kx2J[k] * l;
+                acc[10] += s.ky2J[k] * l;
+            }
+        }
+    }
+    block_sum<11>(acc, v.red);
+    if (threadIdx.x == 0) {
+        double logr = acc[6], phase = 0.0, sgx = 0.0, sgy = 0.0, slx = 0.0, sly = 0.0;
+        if (b >= 0) {
+            const double R = acc[0];
+            logr += log(fmax(fabs(R), 1e-300));
+            if (R < 0.0) phase = kPi;
+            const double invR = (R != 0.0) ? 1.0 / R : 0.0;
+            sgx = invR * acc[2];
+            sgy = invR * acc[3];
+            slx = invR * acc[4] - sgx * sgx;
+            sly = invR * acc[5] - sgy * sgy;
+        }
+        v.misc[M_R] = acc[0];
+        v.misc[M_SCALE] = acc[1];
+        v.misc[M_LOGR] = logr;
+        v.misc[M_PHASE] = phase;
+        v.misc[M_SGX] = sgx;
+        v.misc[M_SGY] = sgy;
+        v.misc[M_SLX] = slx;
+        v.misc[M_SLY] = sly;
+        v.misc[M_JGX] = acc[7];
+        v.misc[M_JGY] = acc[8];
+        v.misc[M_JLX] = acc[9];
+        v.misc[M_JLY] = acc[10];
+    }
+    __syncthreads();
+}
+
+// ───────────────────────── commit ───────────────────────────────────────
+
+__device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p) {
+    const int np = s.np;
+    const int b = block_of(s, p);
+    // Slater: Sherman-Morrison with the reference's rebuild triggers
+    if (b >= 0) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, jrow = p - B.first;
+        double* A = v.scal - s.o_scal + B.oA;
+        double* bs = v.scal + S_BLOCK0 + 3 * b;
+        double* D = grec + B.oD;
+        double* Dg = grec + B.oDg;
+        double* Dl = grec + B.oDl;
+        double* rabs = v.scal - s.o_scal + B.orabs;
+        for (int c = threadIdx.x; c < N; c += kThreads) {
+            double prod = 0.0;
+            for (int m = 0; m < N; ++m) prod += v.nval[m] * A[m * N + c];
+            v.rowp[c] = prod - (c == jrow ? 1.0 : 0.0);
+            v.col[c] = A[c * N + jrow];
+            D[jrow * N + c] = v.nval[c];
+            Dg[(jrow * N + c) * 2 + 0] = v.ngrad[c * 2 + 0];
+            Dg[(jrow * N + c) * 2 + 1] = v.ngrad[c * 2 + 1];
+            Dl[(jrow * N + c) * 2 + 0] = v.nlap[c * 2 + 0];
+            Dl[(jrow * N + c) * 2 + 1] = v.nlap[c * 2 + 1];
+        }
+        if (threadIdx.x == 0) {
+            const double R = v.misc[M_R];
+            bs[1] += 1.0;
+            const bool rebuild = bs[1] >= 64.0 || !isfinite(R) || fabs(R) < 1e-5 || bs[2] > 1e8 ||
+                                 fabs(R) <= 1e4 * kEps * v.misc[M_SCALE];
+            v.misc[M_REBUILD] = rebuild ? 1.0 : 0.0;
+            double rd = 0.0;
+            for (int m = 0; m < N; ++m) rd += fabs(v.nval[m]);
+            rabs[jrow] = rd;
+        }
+        __syncthreads();
+        const double old_log = bs[0];
+        bool rebuild = v.misc[M_REBUILD] != 0.0;
+        if (rebuild) {
+            __threadfence_block();
+            gj_rebuild(s, v, grec, b);
+        } else {
+            const double R = v.misc[M_R];
+            for (int e = threadIdx.x; e < N * N; e += kThreads) {
+                const int a = e / N, c = e % N;
+                const double factor = v.col[a] / R;
+                A[e] = A[e] - factor * v.rowp[c];
+            }
+            __syncthreads();
+        }
+        double ra = 0.0, rdm = 0.0;
+        for (int a = threadIdx.x; a < N; a += kThreads) {
+            double t = 0.0;
+            for (int c = 0; c < N; ++c) t += fabs(A[a * N + c]);
+            ra = fmax(ra, t);
+            rdm = fmax(rdm, rabs[a]);
+        }
+        const double norm_a = block_max(ra, v.red);
+        const double norm_d = block_max(rdm, v.red);
+        const double cond = norm_d * norm_a;
+        if (!rebuild && (!isfinite(cond) || cond > 1e8)) {
+            gj_rebuild(s, v, grec, b);
+            rebuild = true;
+        }
+        if (threadIdx.x == 0) {
+            bs[2] = cond;
+            if (rebuild) {
+                bs[0] = v.misc[M_LOGDET];
+                bs[1] = 0.0;
+                if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+            } else {
+                bs[0] = old_log + log(fabs(v.misc[M_R]));
+            }
+            v.scal[S_LOGPSI] += bs[0] - old_log;
+        }
+        // the moved particle's Slater derivatives at the committed inverse
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int m = threadIdx.x; m < N; m += kThreads) {
+            const double a = A[m * N + jrow];
+            acc[0] += a * v.ngrad[m * 2 + 0];
+            acc[1] += a * v.ngrad[m * 2 + 1];
+            acc[2] += a * v.nlap[m * 2 + 0];
+            acc[3] += a * v.nlap[m * 2 + 1];
+        }
+        block_sum<4>(acc, v.red);
+        if (threadIdx.x == 0) {
+            v.sg[p * 2 + 0] = acc[0];
+            v.sg[p * 2 + 1] = acc[1];
+            v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
+            v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
+        }
+    }
+    // pair terms: partner gradients and Laplacians
+    for (int k = threadIdx.x; k < np; k += kThreads) {
+        if (k == p) continue;
+        const double* geo = v.geo + k * 6;
+        const double irn = 1.0 / geo[2], iro = 1.0 / geo[5];
+        for (int t = 0; t < s.nterms; ++t) {
+            const DevTerm& T = s.terms[t];
+            if (!couples(T, p, k)) continue;
+            const double* rad = v.rad + (static_cast<long>(t) * np + k) * 6;
+            for (int d = 0; d < 2; ++d) {
+                const double dor_old = -geo[3 + d] * iro, dor_new = -geo[d] * irn;
+                const double g_old = rad[1] * dor_old, g_new = rad[4] * dor_new;
+                v.jg[k * 2 + d] += g_new - g_old;
+                const double lap_old = rad[2] * dor_old * dor_old + rad[1] * iro * (1.0 - dor_old * dor_old);
+                const double lap_new = rad[5] * dor_new * dor_new + rad[4] * irn * (1.0 - dor_new * dor_new);
+                v.jl[k * 2 + d] += lap_new - lap_old;
+            }
+        }
+    }
+    // k-space: every particle that sees p's group density shifts by the δρ form
+    bool kspace = false;
+    for (int t = 0; t < s.nterms; ++t)
+        if (s.terms[t].image && in_term(s.terms[t], p)) kspace = true;
+    if (kspace) {
+        const int nk = s.nkJ;
+        const int gp = s.group_of[p];
+        const double* co = v.pc + p * 2 * nk;
+        for (int k = threadIdx.x; k < nk; k += kThreads) {
+            v.dr[k] = v.cn[k] - co[k];
+            v.di[k] = v.sn[k] - co[nk + k];
+        }
+        __syncthreads();
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int t = 0; t < s.nterms; ++t) {
+            const DevTerm& T = s.terms[t];
+            if (!T.image || !in_term(T, p)) continue;
+            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+            const int gs = T.same0 ? gp : (gp == ga ? gb : ga);
+            const int f0 = s.gfirst[gs], f1 = s.glast[gs];
+            for (int i = f0 + warp; i < f1; i += kWarps) {
+                if (i == p) continue;
+                const double* ci = v.pc + i * 2 * nk;
+                double gx = 0.0, gy = 0.0, lx = 0.0, ly = 0.0;
+                for (int k = lane; k < nk; k += 32) {
+                    const double w = T.kw[k];
+                    const double g = 2.0 * w * (ci[k] * v.di[k] - ci[nk + k] * v.dr[k]);
+                    const double l = 2.0 * w * (0.0 - (ci[k] * v.dr[k] + ci[nk + k] * v.di[k]));
+                    gx += s.kxJ[k] * g;
+                    gy += s.kyJ[k] * g;
+                    lx += s.kx2J[k] * l;
+                    ly += s.ky2J[k] * l;
+                }
+                gx = warp_sum(gx);
+                gy = warp_sum(gy);
+                lx = warp_sum(lx);
+                ly = warp_sum(ly);
+                if (lane == 0) {
+                    v.jg[i * 2 + 0] += gx;
+                    v.jg[i * 2 + 1] += gy;
+                    v.jl[i * 2 + 0] += lx;
+                    v.jl[i * 2 + 1] += ly;
+                }
+            }
+            __syncthreads();
+        }
+        double* mr = v.rho + gp * 2 * nk;
+        double* pcp = v.pc + p * 2 * nk;
+        for (int k = threadIdx.x; k < nk; k += kThreads) {
+            mr[k] += v.dr[k];
+            mr[nk + k] += v.di[k];
+            pcp[k] = v.cn[k];
+            pcp[nk + k] = v.sn[k];
+        }
+    }
+    if (threadIdx.x == 0) {
+        // p: new Jastrow derivatives, position (wrapped) and ln ψ of the Jastrow part
+        v.jg[p * 2 + 0] = v.misc[M_JGX];
+        v.jg[p * 2 + 1] = v.misc[M_JGY];
+        v.jl[p * 2 + 0] = v.misc[M_JLX];
+        v.jl[p * 2 + 1] = v.misc[M_JLY];
+        double r[3] = {v.newpos[0], v.newpos[1], 0.0};
+        wrap_pos(s, r);
+        v.pos[p * 2 + 0] = r[0];
+        v.pos[p * 2 + 1] = r[1];
+        double jlog = v.misc[M_LOGR];
+        if (b >= 0) jlog -= log(fmax(fabs(v.misc[M_R]), 1e-300));
+        v.scal[S_LOGPSI] += jlog;
+    }
+    __syncthreads();
+}
+
+// ───────────────────────── local energy ─────────────────────────────────
+
+__device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs, int npair) {
+    const int np = s.np;
+    double acc[1] = {0.0};
+    for (int t = threadIdx.x; t < np * 2; t += kThreads) {
+        const double g = v.sg[t] + v.jg[t], l = v.sl[t] + v.jl[t];
+        acc[0] += -0.5 * s.inv_mass[t] * (l + g * g);
+    }
+    if (s.ewald) {
+        for (int q = threadIdx.x; q < npair; q += kThreads) {
+            const int i = pairs[q].x, j = pairs[q].y;
+            const double coeff = s.charge[i] * s.charge[j];
+            if (coeff == 0.0) continue;
+            double del[3];
+            const double r = fold_dist(s, v.pos + i * 2, v.pos + j * 2, del);
+            if (r < s.e_rcut) acc[0] += coeff * (s.e_inv_eps / r - spline1(s.esp, r));
+        }
+        // ladders e^{i n b_q·r_i}, n = 0..m_q, per particle
+        double* lad = v.work;
+        const int L1 = s.e_m1 + 1, L2 = s.e_m2 + 1;
+        for (int i = threadIdx.x; i < np; i += kThreads) {
+            const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
+            ladder(s.recip[0] * x + s.recip[1] * y, s.e_m1, lad + i * 2 * (L1 + L2));
+            ladder(s.recip[2] * x + s.recip[3] * y, s.e_m2, lad + i * 2 * (L1 + L2) + 2 * L1);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < s.enk; k += kThreads) {
+            const int n1 = s.en1[k], n2 = s.en2[k];
+            double rr = 0.0, ri = 0.0;
+            for (int i = 0; i < np; ++i) {
+                const double q = s.charge[i];
+                if (q == 0.0) continue;
+                double ar, ai, br, bi;
+                ladder_pick(lad + i * 2 * (L1 + L2), n1, ar, ai);
+                ladder_pick(lad + i * 2 * (L1 + L2) + 2 * L1, n2, br, bi);
+                rr += q * (ar * br - ai * bi);
+                ri += q * (ar * bi + ai * br);
+            }
+            acc[0] += s.ew[k] * (rr * rr + ri * ri);
+        }
+    }
+    for (int c = 0; c < s.ncoul; ++c) {
+        const int af = s.coul[c][0], al = s.coul[c][1], bf = s.coul[c][2], bl = s.coul[c][3];
+        const bool same = af == bf && al == bl;
+        const int na = al - af, nb = bl - bf;
+        const int tot = same ? na * na : na * nb;
+        for (int q = threadIdx.x; q < tot; q += kThreads) {
+            const int i = af + q / (same ? na : nb), j = (same ? af : bf) + q % (same ? na : nb);
+            if (same && j <= i) continue;
+            double del[3];
+            const double r = fold_dist(s, v.pos + i * 2, v.pos + j * 2, del);
+            acc[0] += s.coul_coef[c] / r;
+        }
+    }
+    block_sum<1>(acc, v.red);
+    return acc[0] + (s.ewald ? s.e_const : 0.0);
+}
+
+// ───────────────────────── full evaluation ──────────────────────────────
+
+__device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, const int2* pairs,
+                                int npair) {
+    const int np = s.np;
+    // wrap every position into the cell (WalkerSet::load_all)
+    for (int i = threadIdx.x; i < np; i += kThreads) {
+        double r[3] = {v.pos[i * 2], v.pos[i * 2 + 1], 0.0};
+        wrap_pos(s, r);
+        v.pos[i * 2] = r[0];
+        v.pos[i * 2 + 1] = r[1];
+    }
+    for (int i = threadIdx.x; i < np * 2; i += kThreads) v.jg[i] = v.jl[i] = v.sg[i] = v.sl[i] = 0.0;
+    if (threadIdx.x == 0) {
+        v.scal[S_LOGPSI] = 0.0;
+        v.scal[S_ERR] = 0.0;
+        v.misc[M_ERR] = 0.0;
+    }
+    __syncthreads();
+    double lp[1] = {0.0};
+    // Slater: rows, A = D⁻¹ by Gauss-Jordan, log|det|, condition, derivatives
+    for (int b = 0; b < s.nblocks; ++b) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n;
+        double* D = grec + B.oD;
+        double* Dg = grec + B.oDg;
+        double* Dl = grec + B.oDl;
+        double* rabs = v.scal - s.o_scal + B.orabs;
+        for (int e = threadIdx.x; e < N * N; e += kThreads) {
+            const int kr = e / N, m = e % N;
+            double val, g[3], l[3];
+            orbital(s, B, m, v.pos + (B.first + kr) * 2, val, g, l);
+            D[e] = val;
+            Dg[e * 2 + 0] = g[0];
+            Dg[e * 2 + 1] = g[1];
+            Dl[e * 2 + 0] = l[0];
+            Dl[e * 2 + 1] = l[1];
+        }
+        __syncthreads();
+        for (int kr = threadIdx.x; kr < N; kr += kThreads) {
+            double sum = 0.0;
+            for (int i = 0; i < N; ++i) sum += fabs(D[kr * N + i]);
+            rabs[kr] = sum;
+        }
+        __syncthreads();
+        gj_rebuild(s, v, grec, b);
+        double* A = v.scal - s.o_scal + B.oA;
+        double ra = 0.0, rdm = 0.0;
+        for (int a = threadIdx.x; a < N; a += kThreads) {
+            double t = 0.0;
+            for (int c = 0; c < N; ++c) t += fabs(A[a * N + c]);
+            ra = fmax(ra, t);
+            rdm = fmax(rdm, rabs[a]);
+        }
+        const double na = block_max(ra, v.red);
+        const double nd = block_max(rdm, v.red);
+        if (threadIdx.x == 0) {
+            double* bs = v.scal + S_BLOCK0 + 3 * b;
+            bs[0] = v.misc[M_LOGDET];
+            bs[1] = 0.0;
+            bs[2] = nd * na;
+            if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+        }
+        lp[0] += threadIdx.x == 0 ? v.misc[M_LOGDET] : 0.0;
+        __syncthreads();
+    }
+    slater_refresh_all(s, v, grec);
+    // pair terms: each thread owns particle i and sums over its partners
+    for (int i = threadIdx.x; i < np; i += kThreads) {
+        double g[2] = {0.0, 0.0}, l[2] = {0.0, 0.0}, u_half = 0.0;
+        for (int j = 0; j < np; ++j) {
+            if (j == i) continue;
+            double del[3];
+            bool any = false;
+            double r = 0.0;
+            for (int t = 0; t < s.nterms; ++t) {
+                const DevTerm& T = s.terms[t];
+                if (!couples(T, i, j)) continue;
+                if (!any) {
+                    r = fold_dist(s, v.pos + i * 2, v.pos + j * 2, del);
+                    any = true;
+                }
+                double u, du, d2u;
+                radial(T, r, u, du, d2u);
+                const double invr = 1.0 / r;
+                u_half += 0.5 * u;
+                for (int d = 0; d < 2; ++d) {
+                    const double dor = del[d] * invr;
+                    g[d] += du * dor;
+                    l[d] += d2u * dor * dor + du * invr * (1.0 - dor * dor);
+                }
+            }
+        }
+        v.jg[i * 2] += g[0];
+        v.jg[i * 2 + 1] += g[1];
+        v.jl[i * 2] += l[0];
+        v.jl[i * 2 + 1] += l[1];
+        lp[0] += u_half;
+    }
+    __syncthreads();
+    // image sums: phase cache, ρ per group, then Σ w T and every particle's k terms
+    if (s.nkJ > 0) {
+        const int nk = s.nkJ;
+        double* lad = v.work;
+        const int L1 = s.m1J + 1, L2 = s.m2J + 1;
+        for (int i = threadIdx.x; i < np; i += kThreads) {
+            const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
+            ladder(s.recip[0] * x + s.recip[1] * y, s.m1J, lad + i * 2 * (L1 + L2));
+            ladder(s.recip[2] * x + s.recip[3] * y, s.m2J, lad + i * 2 * (L1 + L2) + 2 * L1);
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < np * nk; e += kThreads) {
+            const int i = e / nk, k = e % nk;
+            double ar, ai, br, bi;
+            ladder_pick(lad + i * 2 * (L1 + L2), s.n1J[k], ar, ai);
+            ladder_pick(lad + i * 2 * (L1 + L2) + 2 * L1, s.n2J[k], br, bi);
+            v.pc[i * 2 * nk + k] = ar * br - ai * bi;
+            v.pc[i * 2 * nk + nk + k] = ar * bi + ai * br;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < s.ngroups * nk; e += kThreads) {
+            const int g = e / nk, k = e % nk;
+            double re = 0.0, im = 0.0;
+            for (int i = s.gfirst[g]; i < s.glast[g]; ++i) {
+                re += v.pc[i * 2 * nk + k];
+                im += v.pc[i * 2 * nk + nk + k];
+            }
+            v.rho[g * 2 * nk + k] = re;
+            v.rho[g * 2 * nk + nk + k] = im;
+        }
+        __syncthreads();
+        for (int t = 0; t < s.nterms; ++t) {
+            const DevTerm& T = s.terms[t];
+            if (!T.image) continue;
+            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+            const double* ar = v.rho + ga * 2 * nk;
+            const double* br = v.rho + gb * 2 * nk;
+            for (int k = threadIdx.x; k < nk; k += kThreads) {
+                const double w = T.kw[k];
+                lp[0] += T.same0 ? w * (ar[k] * ar[k] + ar[nk + k] * ar[nk + k])
+                                 : 2.0 * w * (ar[k] * br[k] + ar[nk + k] * br[nk + k]);
+            }
+            for (int i = threadIdx.x; i < np; i += kThreads) {
+                const int gi = s.group_of[i];
+                if (gi != ga && gi != gb) continue;
+                const double* pr = v.rho + (T.same0 ? ga : (gi == ga ? gb : ga)) * 2 * nk;
+                const double self = T.same0 ? 1.0 : 0.0;
+                const double* ci = v.pc + i * 2 * nk;
+                double gx = 0.0, gy = 0.0, lx = 0.0, ly = 0.0;
+                for (int k = 0; k < nk; ++k) {
+                    const double w = T.kw[k];
+                    const double g = 2.0 * w * (ci[k] * pr[nk + k] - ci[nk + k] * pr[k]);
+                    const double l = 2.0 * w * (self - (ci[k] * pr[k] + ci[nk + k] * pr[nk + k]));
+                    gx += s.kxJ[k] * g;
+                    gy += s.kyJ[k] * g;
+                    lx += s.kx2J[k] * l;
+                    ly += s.ky2J[k] * l;
+                }
+                v.jg[i * 2] += gx;
+                v.jg[i * 2 + 1] += gy;
+                v.jl[i * 2] += lx;
+                v.jl[i * 2 + 1] += ly;
+            }
+            __syncthreads();
+        }
+    }
+    block_sum<1>(lp, v.red);
+    const double el = local_energy(s, v, pairs, npair);
+    if (threadIdx.x == 0) {
+        v.scal[S_LOGPSI] = lp[0];
+        v.scal[S_EL] = el;
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+// ───────────────────────── kernels ──────────────────────────────────────
+
+__global__ void __launch_bounds__(kThreads) evaluate_kernel(DevSys s, double* records, int nw,
+                                                            const int2* pairs, int npair) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    double* rec = records + static_cast<long>(w) * s.rec;
+    load_hot(s, rec, sm);
+    const Smem v = view(s, sm);
+    evaluate_walker(s, v, rec, pairs, npair);
+    store_hot(s, rec, sm);
+}
+
+__global__ void __launch_bounds__(kThreads) measure_kernel(DevSys s, double* records, int nw,
+                                                           const int2* pairs, int npair) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    double* rec = records + static_cast<long>(w) * s.rec;
+    load_hot(s, rec, sm);
+    const Smem v = view(s, sm);
+    slater_refresh_all(s, v, rec);
+    const double el = local_energy(s, v, pairs, npair);
+    if (threadIdx.x == 0) v.scal[S_EL] = el;
+    store_hot(s, rec, sm);
+}
+
+__global__ void __launch_bounds__(kThreads) move_kernel(DevSys s, double* records, int nw, int p,
+                                                        const double* new_pos,
+                                                        const uint8_t* accept, double* out) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    double* rec = records + static_cast<long>(w) * s.rec;
+    load_hot(s, rec, sm);
+    const Smem v = view(s, sm);
+    if (threadIdx.x == 0) {
+        v.newpos[0] = new_pos[w];
+        v.newpos[1] = new_pos[nw + w];
+        v.misc[M_ERR] = 0.0;
+    }
+    __syncthreads();
+    ratio_step(s, v, p);
+    if (threadIdx.x == 0) {
+        // log ratio, phase, new ∇ln ψ (dim), new ∂² ln ψ (dim), per walker
+        out[0 * nw + w] = v.misc[M_LOGR];
+        out[1 * nw + w] = v.misc[M_PHASE];
+        out[2 * nw + w] = v.misc[M_SGX] + v.misc[M_JGX];
+        out[3 * nw + w] = v.misc[M_SGY] + v.misc[M_JGY];
+        out[4 * nw + w] = v.misc[M_SLX] + v.misc[M_JLX];
+        out[5 * nw + w] = v.misc[M_SLY] + v.misc[M_JLY];
+    }
+    if (accept != nullptr && accept[w] != 0) commit_step(s, v, rec, p);
+    store_hot(s, rec, sm);
+}
+
+// Fused sweep kernel.  mode 0: VMC step (n_sub sweeps, then refresh + E_L);
+// mode 1: DMC advance (per sweep: refresh + E_L + branch factor).
+__global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* records, int nw,
+                                                         const double* randoms, long stride,
+                                                         SweepParams prm, const int2* pairs,
+                                                         int npair) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    double* rec = records + static_cast<long>(w) * s.rec;
+    load_hot(s, rec, sm);
+    const Smem v = view(s, sm);
+    const int np = s.np;
+    const bool dmc = prm.mode == 1;
+    const bool drift = dmc || prm.drift != 0;
+    if (threadIdx.x == 0) {
+        v.scal[S_NACC] = 0.0;
+        v.scal[S_NCUT] = 0.0;
+        if (dmc) {
+            v.scal[S_RRP] = 0.0;
+            v.scal[S_RRA] = 0.0;
+            v.scal[S_WEIGHT] = 1.0;
+            v.scal[S_EPREV] = v.scal[S_EL];
+        }
+        v.misc[M_ERR] = 0.0;
+    }
+    __syncthreads();
+    for (int sub = 0; sub < prm.n_sub; ++sub) {
+        const double* rnd = randoms + static_cast<long>(sub) * np * 3 * stride;
+        for (int p = 0; p < np; ++p) {
+            if (drift) slater_refresh_particle(s, v, rec, p);
+            if (threadIdx.x == 0) {
+                const double* g = rnd + static_cast<long>(p) * 3 * stride;
+                const double tm = prm.tau * s.inv_mass[p * 2];
+                double sc = tm;
+                const double gx = v.sg[p * 2] + v.jg[p * 2], gy = v.sg[p * 2 + 1] + v.jg[p * 2 + 1];
+                if (dmc) {
+                    const double vsq = gx * gx + gy * gy;
+                    sc = vsq < 1e-10 ? tm : (-1.0 + sqrt(1.0 + 2.0 * tm * vsq)) / vsq;
+                }
+                v.misc[M_SCFWD] = sc;   // forward drift scale
+                const double sig0 = prm.sigma[p * 2], sig1 = prm.sigma[p * 2 + 1];
+                if (drift) {
+                    const double tm0 = dmc ? sc : prm.tau * s.inv_mass[p * 2];
+                    const double tm1 = dmc ? sc : prm.tau * s.inv_mass[p * 2 + 1];
+                    v.newpos[0] = fma(sig0, g[0 * stride + w], fma(tm0, gx, v.pos[p * 2]));
+                    v.newpos[1] = fma(sig1, g[1 * stride + w], fma(tm1, gy, v.pos[p * 2 + 1]));
+                } else {
+                    v.newpos[0] = fma(sig0, g[0 * stride + w], v.pos[p * 2]);
+                    v.newpos[1] = fma(sig1, g[1 * stride + w], v.pos[p * 2 + 1]);
+                }
+                v.misc[M_U] = g[2 * stride + w];
+                v.misc[M_GOX] = gx;   // old total gradient, kept for the Green's function
+                v.misc[M_GOY] = gy;
+            }
+            __syncthreads();
+            ratio_step(s, v, p);
+            if (threadIdx.x == 0) {
+                const double logr = v.misc[M_LOGR];
+                const double u = v.misc[M_U];
+                const double gx = v.misc[M_GOX], gy = v.misc[M_GOY];
+                const double ngx = v.misc[M_SGX] + v.misc[M_JGX];
+                const double ngy = v.misc[M_SGY] + v.misc[M_JGY];
+                const double dx = v.newpos[0] - v.pos[p * 2], dy = v.newpos[1] - v.pos[p * 2 + 1];
+                bool acc;
+                if (dmc) {
+                    acc = false;
+                    if (!(cos(v.misc[M_PHASE]) < kEps)) {
+                        const double tm = prm.tau * s.inv_mass[p * 2];
+                        const double vsq = ngx * ngx + ngy * ngy;
+                        const double sb = vsq < 1e-10 ? tm : (-1.0 + sqrt(1.0 + 2.0 * tm * vsq)) / vsq;
+                        const double sf = v.misc[M_SCFWD];
+                        double lc = 0.0;
+                        const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
+                        if (tm0 > 0.0) {
+                            const double df = sf * gx, db = sb * ngx;
+                            lc += (-dx * (df + db) + 0.5 * (df * df - db * db)) / tm0;
+                        }
+                        if (tm1 > 0.0) {
+                            const double df = sf * gy, db = sb * ngy;
+                            lc += (-dy * (df + db) + 0.5 * (df * df - db * db)) / tm1;
+                        }
+                        const double la = 2.0 * logr + lc;
+                        const double pacc = la >= 0.0 ? 1.0 : exp(la);
+                        acc = la >= 0.0 || u < pacc;
+                    }
+                    const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
+                    const double rr = tm0 * dx * dx + tm1 * dy * dy;
+                    v.scal[S_RRP] += rr;
+                    if (acc) v.scal[S_RRA] += rr;
+                } else if (prm.drift) {
+                    const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
+                    double lc = -dx * (gx + ngx) + 0.5 * tm0 * (gx * gx - ngx * ngx);
+                    lc += -dy * (gy + ngy) + 0.5 * tm1 * (gy * gy - ngy * ngy);
+                    const double la = 2.0 * logr + lc;
+                    acc = la >= 0.0 || u < exp(la);
+                } else {
+                    acc = u < exp(2.0 * logr);
+                }
+                v.misc[M_ACCEPT] = acc ? 1.0 : 0.0;
+                if (acc) v.scal[S_NACC] += 1.0;
+            }
+            __syncthreads();
+            if (v.misc[M_ACCEPT] != 0.0) commit_step(s, v, rec, p);
+        }
+        if (dmc || sub == prm.n_sub - 1) {
+            slater_refresh_all(s, v, rec);
+            const double el = local_energy(s, v, pairs, npair);
+            if (threadIdx.x == 0) {
+                v.scal[S_EL] = el;
+                if (dmc) {
+                    const double enew = el, eold = v.scal[S_EPREV];
+                    double half_tau = 0.5 * prm.tau;
+                    const double x = fmax(prm.eref - enew, prm.eref - eold);
+                    if (x > prm.e_max)
+                        half_tau = 0.0;
+                    else if (x > prm.e_cut)
+                        half_tau *= 1.0 - (x - prm.e_cut) / (prm.e_max - prm.e_cut);
+                    v.scal[S_WEIGHT] *= exp(half_tau * (2.0 * prm.etrial - enew - eold));
+                    if (x > prm.e_cut) v.scal[S_NCUT] += 1.0;
+                    v.scal[S_EPREV] = enew;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (dmc && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
+        if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+    }
+    store_hot(s, rec, sm);
+}
+
+// One sweep's (or several sweeps') random numbers per stream: stream t fills
+// its crowd [w0, w1) in the reference's order (per particle: dim·n Gaussians
+// dimension-major, then n uniforms).  out[(sweep*np + p)*(dim+1)*stride + d*stride + w].
+__global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
+                            int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
+                            double zr, double* out, int crowd_mode) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_streams) return;
+    const int n_active = n_streams < nw ? n_streams : nw;
+    if (t >= n_active) return;
+    const long base = nw / n_active, rem = nw % n_active;
+    const long w0 = t * base + (t < rem ? t : rem);
+    const long cnt = base + (t < rem ? 1 : 0);
+    (void)crowd_mode;
+    Xo r{states[t * 4 + 0], states[t * 4 + 1], states[t * 4 + 2], states[t * 4 + 3]};
+    for (int sw = 0; sw < n_sweeps; ++sw)
+        for (int p = 0; p < np; ++p) {
+            double* row = out + (static_cast<long>(sw) * np + p) * 3 * stride;
+            for (int d = 0; d < 2; ++d)
+                for (long w = w0; w < w0 + cnt; ++w) row[d * stride + w] = xo_gaussian(r, zk, zw, zf, zr);
+            for (long w = w0; w < w0 + cnt; ++w) row[2 * stride + w] = xo_uniform(r);
+        }
+    states[t * 4 + 0] = r.s0;
+    states[t * 4 + 1] = r.s1;
+    states[t * 4 + 2] = r.s2;
+    states[t * 4 + 3] = r.s3;
+}
+
+// dst record j ← src record src_idx[j] (branching), 16-byte vector copies.
+__global__ void gather_kernel(double* dst, const double* src, const int* src_idx, int n, long rec) {
+    const int j = blockIdx.x;
+    if (j >= n) return;
+    const double2* a = reinterpret_cast<const double2*>(src + static_cast<long>(src_idx[j]) * rec);
+    double2* b = reinterpret_cast<double2*>(dst + static_cast<long>(j) * rec);
+    for (long i = threadIdx.x; i < rec / 2; i += blockDim.x) b[i] = a[i];
+}
+
+// Scalars of every walker into a packed [nw] array (slot k of the record).
+__global__ void scalar_kernel(const double* records, int nw, long rec, int offset, double* out) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < nw) out[w] = records[static_cast<long>(w) * rec + offset];
+}
+
+// Walker-major record planes [w][i] ↔ SoA [i*nw + w] (positions, gradients).
+__global__ void to_soa_kernel(const double* records, int nw, long rec, int offset, int n,
+                              double* out) {
+    const long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<long>(n) * nw) return;
+    const int i = static_cast<int>(e / nw), w = static_cast<int>(e % nw);
+    out[e] = records[static_cast<long>(w) * rec + offset + i];
+}
+__global__ void from_soa_kernel(double* records, int nw, long rec, int offset, int n,
+                                const double* in) {
+    const long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<long>(n) * nw) return;
+    const int i = static_cast<int>(e / nw), w = static_cast<int>(e % nw);
+    records[static_cast<long>(w) * rec + offset + i] = in[e];
+}
+
+__global__ void set_scalar_kernel(double* records, int nw, long rec, int offset, double value) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < nw) records[static_cast<long>(w) * rec + offset] = value;
+}
+
+}  // namespace alea_gpu

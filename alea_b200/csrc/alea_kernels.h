@@ -1,0 +1,35 @@
+// Kernel entry points shared by alea_kernels.cu and the host code.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "alea_dev.cuh"
+
+namespace alea_gpu {
+
+struct SweepParams {
+    int mode;                 // 0 VMC step, 1 DMC advance
+    int n_sub;                // sweeps per call
+    int drift;                // VMC: Langevin proposals
+    double tau;
+    const double* sigma;      // [np*dim] sqrt(tau / m)
+    double etrial, eref, e_cut, e_max;
+};
+
+__global__ void evaluate_kernel(DevSys s, double* records, int nw, const int2* pairs, int npair);
+__global__ void measure_kernel(DevSys s, double* records, int nw, const int2* pairs, int npair);
+__global__ void move_kernel(DevSys s, double* records, int nw, int p, const double* new_pos,
+                            const uint8_t* accept, double* out);
+__global__ void sweep_kernel(DevSys s, double* records, int nw, const double* randoms, long stride,
+                             SweepParams prm, const int2* pairs, int npair);
+__global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
+                            int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
+                            double zr, double* out, int crowd_mode);
+__global__ void gather_kernel(double* dst, const double* src, const int* src_idx, int n, long rec);
+__global__ void scalar_kernel(const double* records, int nw, long rec, int offset, double* out);
+__global__ void to_soa_kernel(const double* records, int nw, long rec, int offset, int n, double* out);
+__global__ void from_soa_kernel(double* records, int nw, long rec, int offset, int n, const double* in);
+__global__ void set_scalar_kernel(double* records, int nw, long rec, int offset, double value);
+
+}  // namespace alea_gpu

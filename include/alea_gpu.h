@@ -1,0 +1,267 @@
+/*
+ * alea_gpu.h — C ABI of the B200 walker hot path (VMC/DMC) for Alea.
+ *
+ * A host that already builds Alea's trial wavefunction and Hamiltonian (the
+ * reference's builders, or this library's own host setup) describes the
+ * system once with a flat alea_gpu_system, creates a context on a device, and
+ * then drives walkers that stay resident in HBM.  Plain C types only; every
+ * function returns ALEA_OK (0) or an ALEA_ERR_* code, and
+ * alea_gpu_last_error() returns the context's last message.
+ *
+ * Reference interfaces these entry points replace (paths in ItaloAlb/alea):
+ *   alea_gpu_create / destroy      the per-thread ψ/H clones and WalkerSet of
+ *                                  src/qmc/vmc.cpp:23-62, src/qmc/dmc.cpp:69-163
+ *   alea_gpu_upload_walkers        WalkerSet::load_all (src/population/walker_set.cpp:54-70)
+ *   alea_gpu_evaluate              TrialWavefunction::evaluate_batch
+ *                                  (src/wavefunction/trial_wavefunction.cpp:19-35) +
+ *                                  Hamiltonian::evaluate_batch (src/hamiltonian/hamiltonian.cpp:18-29)
+ *   alea_gpu_download_walkers      WalkerSet positions/log_psi/gradients/laplacians/
+ *                                  local_energies/weights (src/population/walker_set.h:86-152)
+ *   alea_gpu_move                  ParticleBatch::propose_move_batch + TrialWavefunction::
+ *                                  ratio_batch + apply_move_batch_deferred + WalkerSet::apply_move
+ *                                  (src/population/particle_batch.cpp:43-57,
+ *                                  src/wavefunction/trial_wavefunction.cpp:46-91,
+ *                                  src/population/walker_set.cpp:72-107)
+ *   alea_gpu_vmc_step              VMC::run_step (src/qmc/vmc.cpp:157-187), per-thread streams
+ *                                  of VMC::VMC (src/qmc/vmc.cpp:45-61)
+ *   alea_gpu_dmc_advance           DMC::advance_measure over the crowds of DMC::run_one_step
+ *                                  (src/qmc/dmc.cpp:339-419, :693-702)
+ *   alea_gpu_dmc_branch            WalkerSet::branch + TrialWavefunction::permute_caches
+ *                                  (src/population/walker_set.cpp:187-239, src/qmc/dmc.cpp:733-734)
+ *   alea_gpu_vmc_run / dmc_run     VMC::run / DMC::run (src/qmc/vmc.cpp:189-431,
+ *                                  src/qmc/dmc.cpp:525-884)
+ *
+ * Layouts follow the reference's WalkerSet: positions, gradients and
+ * Laplacians are SoA with the walker index fastest, [p*dim*nw + d*nw + w].
+ */
+#ifndef ALEA_GPU_H
+#define ALEA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALEA_GPU_ABI_VERSION 1
+
+enum {
+    ALEA_OK = 0,
+    ALEA_ERR_INVALID = 1,      /* bad argument or system description */
+    ALEA_ERR_CUDA = 2,         /* a CUDA call failed */
+    ALEA_ERR_UNSUPPORTED = 3,  /* valid, but outside what the kernels implement */
+    ALEA_ERR_SINGULAR = 4,     /* a determinant became singular or nonfinite */
+    ALEA_ERR_TIMEOUT = 5,      /* a bounded device wait ran out */
+    ALEA_ERR_NOMEM = 6         /* device allocation failed / capacity exceeded */
+};
+
+enum { ALEA_ORB_PLANE_WAVE = 0, ALEA_ORB_GAUSSIAN = 1 };
+enum { ALEA_PAIR_PADE = 0, ALEA_PAIR_DRUMMOND = 1 };
+
+#define ALEA_GPU_MAX_GROUPS 8
+#define ALEA_GPU_MAX_BLOCKS 4
+#define ALEA_GPU_MAX_TERMS 8
+#define ALEA_GPU_MAX_PAIRS 4
+#define ALEA_GPU_MAX_COULOMB 8
+
+/* Quintic-Hermite long-range spline of the optimized breakup
+ * (src/numerics/long_range_spline.h:41-48): 3 coefficients per knot, scaled
+ * by delta^alpha. */
+typedef struct {
+    double r_cut;
+    double inv_delta;
+    int n_knots;
+    const double* scaled; /* [3 * n_knots] */
+} alea_gpu_spline;
+
+/* Half-space reciprocal vectors k = n1 b1 + n2 b2 with their weights
+ * (src/numerics/ewald_breakup.h:73-77). */
+typedef struct {
+    int n_k;
+    const int* n1;
+    const int* n2;
+    const double* kx;
+    const double* ky;
+    const double* weight;
+} alea_gpu_kset;
+
+typedef struct {
+    int first, last;      /* particle index range [first, last) */
+    double charge;
+    double inv_mass[3];   /* per dimension */
+} alea_gpu_group;
+
+/* One determinant block (src/wavefunction/slater_determinant.h:60-64). */
+typedef struct {
+    int first, last;
+    int type;                 /* ALEA_ORB_* */
+    const double* k;          /* plane waves: [n * dim] */
+    const int* is_sin;        /* plane waves: [n], nonzero = sine */
+    const double* centers;    /* Gaussians: [n * dim] */
+    const double* alphas;     /* Gaussians: [n] */
+} alea_gpu_orbitals;
+
+/* A pair Jastrow: Padé u = Σ a_k r^k / (1 + Σ b_k r^k) on one group pair,
+ * optionally summed over periodic images (short-range spline + k-space
+ * weights), or Drummond-Towler-Needs on one or more group pairs. */
+typedef struct {
+    int kind;                               /* ALEA_PAIR_* */
+    int n_pairs;
+    int pairs[ALEA_GPU_MAX_PAIRS][4];       /* a_first, a_last, b_first, b_last */
+    int num_order, den_order;               /* Padé */
+    double coeffs[16];                      /* Padé [a_1..a_N, b_1..b_M] */
+    int image_sum;                          /* Padé in a periodic cell with Ewald */
+    alea_gpu_spline short_range;            /* f_long of u - u_inf, subtracted inside r_cut */
+    double u_inf;
+    alea_gpu_kset kset;                     /* reciprocal half of the image sum */
+    int C;                                  /* Drummond truncation order */
+    double gamma, L;                        /* Drummond cusp and cutoff */
+    int n_coeffs;
+    double dcoeffs[16];                     /* Drummond [alpha_0, alpha_2..alpha_N] */
+} alea_gpu_pair_term;
+
+/* 2-D Ewald sum of the Coulomb interaction (src/hamiltonian/ewald_term.h). */
+typedef struct {
+    int enabled;
+    double r_cut;
+    double inv_eps;
+    double constant;              /* self + background energy */
+    alea_gpu_spline long_range;
+    alea_gpu_kset kset;
+} alea_gpu_ewald;
+
+/* Open-boundary Coulomb between two groups (src/hamiltonian/coulomb.h). */
+typedef struct {
+    int a_first, a_last, b_first, b_last;
+    double coef;                  /* q_a q_b / epsilon */
+} alea_gpu_coulomb;
+
+typedef struct {
+    int dim;                      /* 2 (3 for open cells) */
+    int n_particles;
+    int periodic;
+    double lattice[9];            /* reduced lattice vectors, row-major [i*dim + d]
+                                     (SimulationCell::vectors()) */
+    int n_groups;
+    alea_gpu_group groups[ALEA_GPU_MAX_GROUPS];
+    int n_blocks;
+    alea_gpu_orbitals blocks[ALEA_GPU_MAX_BLOCKS];
+    int n_terms;
+    alea_gpu_pair_term terms[ALEA_GPU_MAX_TERMS];
+    alea_gpu_ewald ewald;
+    int n_coulomb;
+    alea_gpu_coulomb coulomb[ALEA_GPU_MAX_COULOMB];
+} alea_gpu_system;
+
+typedef struct alea_gpu_ctx alea_gpu_ctx;
+
+/* Create a context for `sys` on CUDA device `device` with room for
+ * `capacity` walkers.  Copies every table; `sys` may be freed afterwards. */
+int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_gpu_ctx** out);
+int alea_gpu_destroy(alea_gpu_ctx* ctx);
+/* Last error message of the context (or of the last failed create when ctx
+ * is NULL).  Valid until the next call on the context. */
+const char* alea_gpu_last_error(const alea_gpu_ctx* ctx);
+int alea_gpu_abi_version(void);
+
+/* Positions of nw walkers, SoA [p*dim*nw + d*nw + w]; they are wrapped into
+ * the cell and fully evaluated (ψ, derivatives, E_L).  Weights reset to 1. */
+int alea_gpu_upload_walkers(alea_gpu_ctx* ctx, const double* positions, int nw);
+int alea_gpu_evaluate(alea_gpu_ctx* ctx);
+int alea_gpu_num_walkers(const alea_gpu_ctx* ctx, int* nw);
+/* Copies of the committed walker state; any pointer may be NULL.
+ * gradients/laplacians are the totals ∇ln ψ and ∂²_d ln ψ, SoA like positions. */
+int alea_gpu_download_walkers(alea_gpu_ctx* ctx, double* positions, double* log_psi,
+                              double* gradients, double* laplacians, double* local_energy,
+                              double* weights);
+
+/* One single-particle move of particle p for every walker: propose
+ * new_pos [d*nw + w], compute log|ψ'/ψ|, its phase (π on a node crossing),
+ * ∇ln ψ and ∂²_d ln ψ of p at the proposed position, then commit the walkers
+ * with accept[w] != 0 (accept may be NULL: ratio only).  Outputs may be NULL. */
+int alea_gpu_move(alea_gpu_ctx* ctx, int p, const double* new_pos, const uint8_t* accept,
+                  double* log_ratio, double* phase, double* new_grad, double* new_lap);
+/* Refresh every derivative and recompute E_L (before reading them after moves). */
+int alea_gpu_measure(alea_gpu_ctx* ctx);
+
+/* Random streams: stream t starts from xoshiro256++ seeded with
+ * stream_seed(seed, kind, t) (src/numerics/random.h:52-56). */
+#define ALEA_STREAM_VMC 0x766d632d74687264ULL   /* "vmc-thrd" */
+#define ALEA_STREAM_DMC 0x646d632d74687264ULL   /* "dmc-thrd" */
+#define ALEA_STREAM_BRANCH 0x646d632d62726368ULL /* "dmc-brch" */
+int alea_gpu_set_streams(alea_gpu_ctx* ctx, uint64_t seed, uint64_t kind, int n_streams);
+
+typedef struct {
+    double tau;
+    int n_substeps;
+    int use_drift;       /* Langevin (1) or symmetric Metropolis (0) */
+} alea_gpu_vmc_params;
+
+typedef struct {
+    double energy_sum;       /* Σ_w E_L (VMC) or Σ_w weight·E_L (DMC) */
+    double energy_sq_sum;
+    double weight_sum;       /* DMC: Σ_w weight */
+    int64_t n_accepted;
+    int64_t n_proposed;
+    int64_t n_cut;           /* DMC: walker sweeps tapered by the branch cutoff */
+    int n_walkers;           /* walkers at the end of the step */
+} alea_gpu_step_stats;
+
+/* One VMC step: n_substeps sweeps, then the derivative refresh and E_L.  The
+ * walkers are split over the streams in contiguous even ranges, as VMC's
+ * threads are (src/qmc/vmc.cpp:45-61). */
+int alea_gpu_vmc_step(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out);
+
+typedef struct {
+    double tau;
+    int n_substeps;
+    double e_trial, e_ref;          /* PopulationControl state before the step */
+    double e_cut, e_max;            /* branch-weight cutoff window */
+} alea_gpu_dmc_params;
+
+/* One DMC advance (no branching): every crowd sweeps its walkers n_substeps
+ * times with drift-diffusion moves, refreshes, evaluates E_L and multiplies
+ * the weights by each sweep's branch factor.  Crowds are the contiguous
+ * ranges of min(n_streams, nw) even splits of the current population. */
+int alea_gpu_dmc_advance(alea_gpu_ctx* ctx, const alea_gpu_dmc_params* prm, alea_gpu_step_stats* out);
+/* Branch on the serial stream state[4] (xoshiro256++, advanced in place):
+ * multiplicities floor(w + U), clipping to [target/5 + 1, 2 target + 1],
+ * walker state gathered, weights reset to 1. */
+int alea_gpu_dmc_branch(alea_gpu_ctx* ctx, uint64_t* state, int target);
+
+typedef struct {
+    int n_equilibration_blocks, n_accumulation_blocks, n_steps, n_substeps;
+    double tau;
+    int use_drift;
+    int n_streams;
+    uint64_t seed;
+    /* DMC only */
+    int target_walkers;
+    double population_generations;
+    double branch_cutoff_alpha;
+} alea_gpu_run_config;
+
+typedef struct {
+    double energy, energy_error, variance, acceptance;
+    double walltime_s;
+    int n_walkers;
+    double e_trial;
+} alea_gpu_run_result;
+
+/* Whole VMC / DMC runs, the reference drivers' loops with device sweeps.
+ * block_energies (nullable) receives one mean per accumulation block (VMC:
+ * one per block and stream chain, stream-major). */
+int alea_gpu_vmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
+                     double* block_energies);
+int alea_gpu_dmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
+                     double* block_energies);
+
+/* Device time of the last alea_gpu_*_step / advance call's sweep kernel, in
+ * milliseconds (CUDA events on the context's stream). */
+int alea_gpu_last_kernel_ms(const alea_gpu_ctx* ctx, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALEA_GPU_H */

@@ -1,0 +1,74 @@
+"""Regenerate the golden fixtures in this directory from the compiled reference.
+
+    make -C oracle ref            # builds oracle/_ref/ref_harness from the reference tree
+    python tests/golden/make_fixtures.py
+
+Every fixture is the output of the reference's own code (its VMC/DMC drivers,
+components and setup-time breakups) run through oracle/_ref/ref_harness:
+
+* ``setup_<name>.json``  system description: cell, groups, orbitals, Padé /
+  Drummond parameters, image-sum and Ewald tables (the reference's breakups);
+* ``eval_<name>.json``   4 walkers from the reference App's initialisation
+  (mt19937_64, seed 12345): ln|psi|, E_L, gradients, Laplacians;
+* ``vmc_<name>.json``    VMC::run with one stream per walker (threads = nw):
+  initial positions, per-walker E_L of every accumulation step, final
+  positions, acceptance;
+* ``dmc_<name>.json``    DMC::run with one crowd per walker: per-step
+  populations, weights, energies, ids, final positions.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import run_ref_harness  # noqa: E402
+
+SYSTEMS = {
+    "exciton": dict(system="exciton"),
+    "heg10": dict(system="heg", nu=5, nd=5, rs=30),
+    "crystal16": dict(system="crystal", nx=4, ny=4, rs=40),
+    "heg42": dict(system="heg", nu=21, nd=21, rs=30),
+}
+VMC = {
+    "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
+    "heg10": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=225.0),
+    "heg10_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
+    "crystal16": dict(nw=4, seed=17, eq=0, acc=2, steps=2, substeps=1, tau=400.0),
+}
+DMC = {
+    "exciton": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.05),
+    "heg10": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
+}
+
+
+def dump(name, obj):
+    with open(os.path.join(HERE, name), "w") as f:
+        json.dump(obj, f, separators=(",", ":"))
+    print("wrote", name)
+
+
+def main():
+    for name, args in SYSTEMS.items():
+        dump(f"setup_{name}.json", run_ref_harness("setup", **args))
+        ev = run_ref_harness("eval", nw=4, seed=12345, **args)
+        ev.pop("mode", None)
+        dump(f"eval_{name}.json", ev)
+    for name, run in VMC.items():
+        sysname = name.split("_")[0]
+        r = run_ref_harness("vmc", **run, **SYSTEMS[sysname])
+        r["params"] = run
+        r["system"] = sysname
+        dump(f"vmc_{name}.json", r)
+    for name, run in DMC.items():
+        r = run_ref_harness("dmc", **run, **SYSTEMS[name])
+        r["params"] = run
+        r["system"] = name
+        dump(f"dmc_{name}.json", r)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,139 @@
+"""GPU path vs the oracle, through the C ABI (libalea_b200.so).
+
+Same system tables and inputs on both sides.  Tolerances: local energies and
+log ratios 1e-10 relative; symmetric-Metropolis VMC positions bit for bit
+(every accept decision identical); DMC populations and branching identical.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import Oracle
+from oracle.oracle import S_EL, S_LOGPSI
+
+pytestmark = pytest.mark.gpu
+
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42"]
+
+
+def walkers(setup, capacity):
+    import alea_b200
+    return alea_b200.Walkers(setup, capacity=capacity)
+
+
+def rel(a, b, floor=1e-12):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_evaluate_matches_oracle(name):
+    setup = golden(f"setup_{name}.json")
+    pos = np.array(golden(f"eval_{name}.json")["positions"])
+    o = Oracle(setup)
+    o.init(pos)
+    g = walkers(setup, 8)
+    g.upload(pos)
+    d = g.download()
+    assert rel(d["local_energy"], o.scalar(S_EL)[:4]) < 1e-10
+    assert rel(d["log_psi"], o.scalar(S_LOGPSI)[:4], floor=1.0) < 1e-10
+    scale = max(1.0, np.abs(o.grad()[:4]).max())
+    assert np.max(np.abs(d["grad"] - o.grad()[:4])) < 1e-10 * scale
+    lscale = max(1.0, np.abs(o.lap()[:4]).max())
+    assert np.max(np.abs(d["lap"] - o.lap()[:4])) < 1e-9 * lscale
+    assert np.array_equal(d["positions"], o.pos()[:4])
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_single_moves_match_oracle(name):
+    setup = golden(f"setup_{name}.json")
+    pos = np.array(golden(f"eval_{name}.json")["positions"])
+    nw = pos.shape[0]
+    o = Oracle(setup)
+    o.init(pos)
+    g = walkers(setup, 8)
+    g.upload(pos)
+    rng = np.random.default_rng(3)
+    npart, dim = o.np, o.dim
+    step = 0.3 if name == "exciton" else 8.0
+    for it, p in enumerate([0, npart - 1, npart // 2, 1 % npart]):
+        cur = g.download()["positions"].reshape(nw, npart, dim)[:, p, :]
+        new = cur + step * rng.standard_normal(cur.shape)
+        acc = np.array([(w + it) % 2 == 0 for w in range(nw)])
+        lr, ph, ng, nl = g.move(p, new, acc)
+        for w in range(nw):
+            out = o.move(w, p, new[w], bool(acc[w]))
+            assert abs(lr[w] - out[0]) < 1e-10 * max(1.0, abs(out[0]))
+            assert ph[w] == out[1]
+            assert np.max(np.abs(ng[w] - out[2:4])) < 1e-9 * max(1.0, np.abs(out[2:4]).max())
+            assert np.max(np.abs(nl[w] - out[4:6])) < 1e-9 * max(1.0, np.abs(out[4:6]).max())
+    g.measure()
+    d = g.download()
+    for w in range(nw):
+        o.measure(w)
+    assert np.array_equal(d["positions"], o.pos()[:nw])
+    assert rel(d["local_energy"], o.scalar(S_EL)[:nw]) < 1e-10
+
+
+@pytest.mark.parametrize("name,drift", [("exciton", False), ("heg10", False), ("heg10", True),
+                                        ("crystal16", False), ("heg42", False)])
+def test_vmc_steps_match_oracle(name, drift):
+    import alea_b200
+    setup = golden(f"setup_{name}.json")
+    pos = np.array(golden(f"eval_{name}.json")["positions"])
+    nw = pos.shape[0]
+    tau = {"exciton": 0.05, "heg10": 225.0, "crystal16": 400.0, "heg42": 225.0}[name]
+    n_steps, n_sub, seed = 4, 2, 21
+    o = Oracle(setup)
+    o.init(pos)
+    el_o, st_o = o.vmc(nw, seed, 0, 1, n_steps, n_sub, tau, drift=drift)
+    g = walkers(setup, nw)
+    g.upload(pos)
+    g.set_streams(seed, alea_b200.STREAM_VMC, nw)
+    acc = 0
+    for s in range(n_steps):
+        st = g.vmc_step(tau, n_sub, drift)
+        acc += st.n_accepted
+        assert rel(g.download()["local_energy"], el_o[s]) < 1e-10
+    assert acc == int(st_o[0])
+    fin = g.download()["positions"]
+    if drift:
+        assert np.max(np.abs(fin - o.pos()[:nw])) < 1e-9 * np.abs(fin).max()
+    else:
+        assert np.array_equal(fin, o.pos()[:nw])
+
+
+@pytest.mark.parametrize("name", ["exciton", "heg10"])
+def test_dmc_run_matches_oracle(name):
+    setup = golden(f"setup_{name}.json")
+    r = golden(f"dmc_{name}.json")
+    p = r["params"]
+    nw = p["nw"]
+    pos = np.array(r["initial_positions"])
+    o = Oracle(setup)
+    o.init(pos, capacity=4 * nw + 4)
+    tr = o.dmc(nw, p["seed"], p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], target=nw)
+    g = walkers(setup, 4 * nw + 4)
+    g.upload(pos)
+    res, blocks = g.dmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], nw,
+                            p["seed"], target=nw)
+    n_eq = p["eq"] * p["steps"]
+    ref_blocks = [tr[n_eq + b * p["steps"]: n_eq + (b + 1) * p["steps"], 1].sum() /
+                  tr[n_eq + b * p["steps"]: n_eq + (b + 1) * p["steps"], 2].sum()
+                  for b in range(p["acc"])]
+    assert rel(blocks, ref_blocks) < 1e-10
+    assert g.nw == o.nw                       # identical branching history
+    assert rel(g.download()["local_energy"], o.scalar(S_EL)[: o.nw]) < 1e-9
+
+
+def test_exciton_exact_energy_zero_variance():
+    import alea_b200
+    setup = golden("setup_exciton.json")
+    pos = np.array(golden("eval_exciton.json")["positions"])
+    pos = np.concatenate([pos] * 8)
+    g = walkers(setup, len(pos))
+    g.upload(pos)
+    res, blocks = g.vmc_run(1, 4, 5, 2, 0.05, len(pos), 42)
+    assert abs(res.energy + 1.0) < 1e-12
+    assert res.variance < 1e-20
+    assert 0.5 < res.acceptance < 1.0
