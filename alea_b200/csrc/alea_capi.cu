@@ -328,6 +328,8 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     s.o_pos = o; o += np * 2;
     s.o_jg = o; o += np * 2;
     s.o_jl = o; o += np * 2;
+    s.o_kg = o; o += np * 2;
+    s.o_kl = o; o += np * 2;
     s.o_sg = o; o += np * 2;
     s.o_sl = o; o += np * 2;
     s.o_scal = o; o += S_NSCAL;
@@ -360,11 +362,11 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
             return fail(c, ALEA_ERR_INVALID, "unknown orbital type");
         }
         D.oA = static_cast<int>(o);
-        o += D.n * D.n;
+        o += round4(D.n * D.n);
     }
     for (int b = 0; b < s.nblocks; ++b) {
         s.blocks[b].orabs = static_cast<int>(o);
-        o += s.blocks[b].n;
+        o += round4(s.blocks[b].n);
     }
     // pair terms and the shared Jastrow k set
     if (in->n_terms < 0 || in->n_terms > kMaxTerms) return fail(c, ALEA_ERR_INVALID, "bad n_terms");
@@ -454,15 +456,13 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     }
     s.o_rho = static_cast<int>(o);
     o += static_cast<long>(s.ngroups) * 2 * s.nkJ;
-    s.o_pc = static_cast<int>(o);
-    o += static_cast<long>(np) * 2 * s.nkJ;
     s.hot = static_cast<int>(round4(o));
     o = s.hot;
     for (int b = 0; b < s.nblocks; ++b) {
         DevBlock& D = s.blocks[b];
-        D.oD = o; o += D.n * D.n;
-        D.oDg = o; o += D.n * D.n * 2;
-        D.oDl = o; o += D.n * D.n * 2;
+        D.oD = o; o += round4(D.n * D.n);
+        D.oDg = o; o += round4(D.n * D.n * 2);
+        D.oDl = o; o += round4(D.n * D.n * 2);
     }
     s.rec = round4(o);
     // Ewald
@@ -521,15 +521,15 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     s.s_nval = take(s.maxN);
     s.s_ngrad = take(2 * s.maxN);
     s.s_nlap = take(2 * s.maxN);
-    s.s_rad = take(static_cast<long>(s.nterms) * np * 6 + np * 6);
+    s.s_rad = take(static_cast<long>(np) * 4 + np * 6);
     s.s_cn = take(s.nkJ);
     s.s_sn = take(s.nkJ);
-    s.s_dr = take(s.nkJ);
-    s.s_di = take(s.nkJ);
+    s.s_co = take(s.nkJ);
+    s.s_so = take(s.nkJ);
     s.s_col = take(s.maxN);
     s.s_rowp = take(s.maxN);
     s.s_red = take(kWarps * 16 + 16);
-    s.s_misc = take(32 + 4 * (kMaxLadder + 1));
+    s.s_misc = take(64 + 4 * 2 * (kMaxLadder + 1));
     long work = static_cast<long>(s.maxN) * s.maxN;
     work = std::max(work, static_cast<long>(np) * 2 * (s.e_m1 + s.e_m2 + 2));
     work = std::max(work, static_cast<long>(np) * 2 * (s.m1J + s.m2J + 2));
@@ -799,6 +799,8 @@ int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_ps
             if (int rc = plane(which == 0 ? s.o_sg : s.o_sl, a.data())) return rc;
             if (int rc = plane(which == 0 ? s.o_jg : s.o_jl, b.data())) return rc;
             for (long i = 0; i < n; ++i) dst[i] = a[i] + b[i];
+            if (int rc = plane(which == 0 ? s.o_kg : s.o_kl, b.data())) return rc;
+            for (long i = 0; i < n; ++i) dst[i] += b[i];
         }
     }
     std::vector<double> tmp;

@@ -2,10 +2,11 @@
 // math shared by the walker kernels (sm_100a).
 //
 // One CTA owns one walker for a whole sweep.  The walker's hot state (position,
-// Jastrow and Slater gradient/Laplacian planes, inverse matrices, k-space
-// structure factors and phase cache) is staged from its HBM record into shared
-// memory at kernel start and written back at the end; the orbital rows D, ∇D,
-// ∇²D stay in HBM and are touched one row per accepted move.
+// the gradient/Laplacian planes of the pair Jastrows, the k-space image sums
+// and the determinants, the inverse matrices and the per-group structure
+// factors ρ(k)) is staged from its HBM record into shared memory at kernel
+// start and written back at the end; the orbital rows D, ∇D, ∇²D stay in HBM
+// and are touched one row per move.
 #pragma once
 
 #include <cstdint>
@@ -20,7 +21,7 @@ constexpr int kMaxTerms = 8;
 constexpr int kMaxGroups = 8;
 constexpr int kMaxCoulomb = 8;
 constexpr int kMaxN = 64;              // largest determinant block
-constexpr int kMaxLadder = 64;         // largest |n| of a reciprocal index
+constexpr int kMaxLadder = 32;         // largest |n| of a reciprocal index
 
 // Scalar slots of a walker record.
 enum : int {
@@ -93,9 +94,9 @@ struct DevSys {
     // record layout (doubles): hot part [0, hot) is staged in shared memory
     long rec;                 // record stride
     int hot;
-    int o_pos, o_jg, o_jl, o_sg, o_sl, o_scal, o_rho, o_pc;
+    int o_pos, o_jg, o_jl, o_kg, o_kl, o_sg, o_sl, o_scal, o_rho;
     // shared-memory scratch layout (doubles, after the hot part)
-    int s_newpos, s_nval, s_ngrad, s_nlap, s_rad, s_cn, s_sn, s_dr, s_di, s_col, s_rowp,
+    int s_newpos, s_nval, s_ngrad, s_nlap, s_rad, s_cn, s_sn, s_co, s_so, s_col, s_rowp,
         s_red, s_misc, s_work, s_total;
     // ziggurat tables
     const uint64_t* zk;

@@ -12,7 +12,7 @@
 //                  :862-903 (derivative refresh), :905-993 (Gauss-Jordan)
 //   pair Jastrows  src/wavefunction/pade_jastrow.cpp:347-634,
 //                  src/wavefunction/radial_pair_jastrow_impl.h
-//   image sums     src/wavefunction/kspace_pair_sum.cpp:139-301
+//   image sums     src/wavefunction/kspace_pair_sum.cpp:105-301
 //   E_L            src/hamiltonian/kinetic.cpp:45-72, ewald_term.cpp:368-612,
 //                  coulomb.cpp:31-61
 //   branch weight  src/qmc/population_control.cpp:56-77
@@ -20,8 +20,16 @@
 //
 // Parallel layout: one CTA of kThreads threads per walker.  Work inside a
 // move is spread over orbitals (Slater), partners (pair terms), k-vectors
-// (image sums), matrix elements (rank-one update) and seers (k-space partner
-// gradients); partial sums meet in block reductions.
+// (image sums) and matrix elements (rank-one update); partial sums meet in
+// block reductions.
+//
+// Deferred derivatives.  Like the reference's determinant (deferred partner
+// refresh, slater_determinant.cpp:862-903), the k-space half of an image-summed
+// Jastrow commits only ρ(k) and the moved particle's own derivatives; every
+// other particle's k-space gradient and Laplacian is recomputed from ρ(k) and
+// its phases when it is next read (its own move's drift, or the local energy).
+// That turns the O(N·n_k) partner update of every accepted move into O(n_k)
+// per read, and no per-particle phase cache is kept.
 #include <cstdio>
 
 #include "alea_dev.cuh"
@@ -33,10 +41,11 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kEps = 2.220446049250313e-16;
+constexpr int kLad = 2 * (kMaxLadder + 1);   // doubles per ladder
 
 struct Smem {
-    double *pos, *jg, *jl, *sg, *sl, *scal, *rho, *pc;
-    double *newpos, *nval, *ngrad, *nlap, *rad, *geo, *cn, *sn, *dr, *di, *col, *rowp, *red,
+    double *pos, *jg, *jl, *kg, *kl, *sg, *sl, *scal, *rho;
+    double *newpos, *nval, *ngrad, *nlap, *rad, *geo, *cn, *sn, *co, *so, *col, *rowp, *red,
         *misc, *work;
 };
 
@@ -45,21 +54,22 @@ __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
     v.pos = sm + s.o_pos;
     v.jg = sm + s.o_jg;
     v.jl = sm + s.o_jl;
+    v.kg = sm + s.o_kg;
+    v.kl = sm + s.o_kl;
     v.sg = sm + s.o_sg;
     v.sl = sm + s.o_sl;
     v.scal = sm + s.o_scal;
     v.rho = sm + s.o_rho;
-    v.pc = sm + s.o_pc;
     v.newpos = sm + s.s_newpos;
     v.nval = sm + s.s_nval;
     v.ngrad = sm + s.s_ngrad;
     v.nlap = sm + s.s_nlap;
     v.rad = sm + s.s_rad;
-    v.geo = v.rad + static_cast<long>(s.nterms) * s.np * 6;
+    v.geo = v.rad + static_cast<long>(s.np) * 4;
     v.cn = sm + s.s_cn;
     v.sn = sm + s.s_sn;
-    v.dr = sm + s.s_dr;
-    v.di = sm + s.s_di;
+    v.co = sm + s.s_co;
+    v.so = sm + s.s_so;
     v.col = sm + s.s_col;
     v.rowp = sm + s.s_rowp;
     v.red = sm + s.s_red;
@@ -70,9 +80,9 @@ __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
 
 // misc slots
 enum : int {
-    M_R = 0, M_SCALE, M_LOGR, M_PHASE, M_ACCEPT, M_REBUILD, M_LOGDET, M_ERR, M_NORMD,
-    M_SGX, M_SGY, M_SLX, M_SLY, M_JGX, M_JGY, M_JLX, M_JLY, M_U, M_SCFWD, M_GOX, M_GOY,
-    M_LAD /* two ladders of kMaxLadder + 1 complex values follow */
+    M_R = 0, M_SCALE, M_LOGR, M_PHASE, M_ACCEPT, M_REBUILD, M_LOGDET, M_ERR, M_U, M_SCFWD,
+    M_GOX, M_GOY, M_SGX, M_SGY, M_SLX, M_SLY, M_JGX, M_JGY, M_JLX, M_JLY, M_KGX, M_KGY,
+    M_KLX, M_KLY, M_LAD /* four ladders of kMaxLadder + 1 complex values follow */
 };
 
 __device__ __forceinline__ void load_hot(const DevSys& s, const double* rec, double* sm) {
@@ -95,7 +105,14 @@ __device__ __forceinline__ int block_of(const DevSys& s, int p) {
     return -1;
 }
 
-// e^{i n θ} for n = 0..m into (re, im) pairs at out[2n], out[2n+1].
+__device__ __forceinline__ bool kspace_of(const DevSys& s, int p) {
+    for (int t = 0; t < s.nterms; ++t)
+        if (s.terms[t].image && in_term(s.terms[t], p)) return true;
+    return false;
+}
+
+// e^{i n θ} for n = 0..m into (re, im) pairs at out[2n], out[2n+1]
+// (the integer ladders of reciprocal_phases.h).
 __device__ __forceinline__ void ladder(double theta, int m, double* out) {
     double c, sn;
     sincos(theta, &sn, &c);
@@ -118,15 +135,52 @@ __device__ __forceinline__ void ladder_pick(const double* lad, int n, double& re
     im = n < 0 ? -lad[2 * a + 1] : lad[2 * a + 1];
 }
 
+// e^{ik·r} for the Jastrow k set from the two ladders of r.
+__device__ __forceinline__ void phase_k(const DevSys& s, const double* l1, const double* l2, int k,
+                                        double& c, double& sn) {
+    double ar, ai, br, bi;
+    ladder_pick(l1, s.n1J[k], ar, ai);
+    ladder_pick(l2, s.n2J[k], br, bi);
+    c = ar * br - ai * bi;
+    sn = ar * bi + ai * br;
+}
+
+// Gradient/Laplacian terms of one k for a particle with phases (c, sn) that
+// sees the density (pr, pi) (kspace_pair_sum.cpp:76-97).
+__device__ __forceinline__ void kterm(const DevSys& s, double w, int k, double c, double sn,
+                                      double pr, double pi, double self, double* acc) {
+    const double g = 2.0 * w * (c * pi - sn * pr);
+    const double l = 2.0 * w * (self - (c * pr + sn * pi));
+    acc[0] += s.kxJ[k] * g;
+    acc[1] += s.kyJ[k] * g;
+    acc[2] += s.kx2J[k] * l;
+    acc[3] += s.ky2J[k] * l;
+}
+
+// Every image-summed term's k-space gradient/Laplacian of particle i (group
+// gi) from its phases, added to acc[4].
+__device__ __forceinline__ void kspace_particle_k(const DevSys& s, const Smem& v, int i, int gi, int k,
+                                                  double c, double sn, double* acc) {
+    const int nk = s.nkJ;
+    for (int t = 0; t < s.nterms; ++t) {
+        const DevTerm& T = s.terms[t];
+        if (!T.image || !in_term(T, i)) continue;
+        const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+        const int go = T.same0 ? gi : (gi == ga ? gb : ga);
+        const double* pr = v.rho + go * 2 * nk;
+        kterm(s, T.kw[k], k, c, sn, pr[k], pr[nk + k], T.same0 ? 1.0 : 0.0, acc);
+    }
+}
+
 // ───────────────────────── Gauss-Jordan rebuild ─────────────────────────
 
 // A = D⁻¹ of block b from its committed rows in HBM, by pivoted Gauss-Jordan
 // (first maximum |pivot| in each column, as the reference's rebuild_inverse).
-// Returns log|det D| in misc[M_LOGDET]; flags a singular matrix in misc[M_ERR].
+// Leaves log|det D| in misc[M_LOGDET]; flags a singular matrix in misc[M_ERR].
 __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, int b) {
     const DevBlock& B = s.blocks[b];
     const int N = B.n;
-    double* A = v.scal - s.o_scal + B.oA;   // hot-part base + offset
+    double* A = v.scal - s.o_scal + B.oA;
     double* m = v.work;
     const double* D = grec + B.oD;
     for (int e = threadIdx.x; e < N * N; e += kThreads) {
@@ -138,7 +192,6 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
     __shared__ int s_piv;
     for (int k = 0; k < N; ++k) {
         if (threadIdx.x < 32) {
-            // warp argmax over rows r >= k of |m[r][k]|, ties to the lowest row
             double best = -1.0;
             int bi = N;
             for (int r = k + static_cast<int>(threadIdx.x); r < N; r += 32) {
@@ -195,37 +248,68 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
     }
 }
 
-// ───────────────────────── Slater ───────────────────────────────────────
+// ───────────────────────── refresh ──────────────────────────────────────
 
-// Slater derivatives of particle p from A and the committed rows.
-__device__ void slater_refresh_particle(const DevSys& s, const Smem& v, const double* grec, int p) {
+// Drift refresh of particle p: its determinant derivatives from A and the
+// committed rows, and its k-space derivatives from ρ(k) and its phases (left
+// in co/so for the ratio).  Ends with the block reduction's barriers.
+__device__ void refresh_particle(const DevSys& s, const Smem& v, const double* grec, int p) {
     const int b = block_of(s, p);
-    if (b < 0) return;   // block-uniform
-    const DevBlock& B = s.blocks[b];
-    const int N = B.n, kr = p - B.first;
-    const double* A = v.scal - s.o_scal + B.oA;
-    const double* Dg = grec + B.oDg;
-    const double* Dl = grec + B.oDl;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int m = threadIdx.x; m < N; m += kThreads) {
-        const double a = A[m * N + kr];
-        acc[0] += a * Dg[(kr * N + m) * 2 + 0];
-        acc[1] += a * Dg[(kr * N + m) * 2 + 1];
-        acc[2] += a * Dl[(kr * N + m) * 2 + 0];
-        acc[3] += a * Dl[(kr * N + m) * 2 + 1];
+    const bool ks = kspace_of(s, p);
+    if (ks && threadIdx.x < 2) {
+        const int q = threadIdx.x;
+        const double th = s.recip[q * 2] * v.pos[p * 2] + s.recip[q * 2 + 1] * v.pos[p * 2 + 1];
+        ladder(th, q == 0 ? s.m1J : s.m2J, v.misc + M_LAD + q * kLad);
     }
-    block_sum<4>(acc, v.red);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (b >= 0) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, kr = p - B.first;
+        const double* A = v.scal - s.o_scal + B.oA;
+        const double* Dg = grec + B.oDg + kr * N * 2;
+        const double* Dl = grec + B.oDl + kr * N * 2;
+        for (int m = threadIdx.x; m < N; m += kThreads) {
+            const double a = A[m * N + kr];
+            const double2 g = reinterpret_cast<const double2*>(Dg)[m];
+            const double2 l = reinterpret_cast<const double2*>(Dl)[m];
+            acc[0] += a * g.x;
+            acc[1] += a * g.y;
+            acc[2] += a * l.x;
+            acc[3] += a * l.y;
+        }
+    }
+    if (ks) {
+        __syncthreads();
+        const int gp = s.group_of[p];
+        for (int k = threadIdx.x; k < s.nkJ; k += kThreads) {
+            double c, sn;
+            phase_k(s, v.misc + M_LAD, v.misc + M_LAD + kLad, k, c, sn);
+            v.co[k] = c;
+            v.so[k] = sn;
+            kspace_particle_k(s, v, p, gp, k, c, sn, acc + 4);
+        }
+    }
+    block_sum<8>(acc, v.red);
     if (threadIdx.x == 0) {
-        v.sg[p * 2 + 0] = acc[0];
-        v.sg[p * 2 + 1] = acc[1];
-        v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
-        v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
+        if (b >= 0) {
+            v.sg[p * 2 + 0] = acc[0];
+            v.sg[p * 2 + 1] = acc[1];
+            v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
+            v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
+        }
+        if (ks) {
+            v.kg[p * 2 + 0] = acc[4];
+            v.kg[p * 2 + 1] = acc[5];
+            v.kl[p * 2 + 0] = acc[6];
+            v.kl[p * 2 + 1] = acc[7];
+        }
     }
     __syncthreads();
 }
 
-// Every particle's Slater derivatives (refresh_derivatives).
-__device__ void slater_refresh_all(const DevSys& s, const Smem& v, const double* grec) {
+// Every particle's determinant and k-space derivatives (refresh_derivatives).
+__device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) {
+    const int np = s.np;
     for (int b = 0; b < s.nblocks; ++b) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n;
@@ -245,29 +329,59 @@ __device__ void slater_refresh_all(const DevSys& s, const Smem& v, const double*
             v.sl[part * 2 + d] = l - g * g;
         }
     }
+    if (s.nkJ > 0) {
+        double* lad = v.work;
+        const int LS = 2 * (s.m1J + 1 + s.m2J + 1), L2 = 2 * (s.m1J + 1);
+        __syncthreads();
+        for (int i = threadIdx.x; i < np; i += kThreads) {
+            const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
+            ladder(s.recip[0] * x + s.recip[1] * y, s.m1J, lad + i * LS);
+            ladder(s.recip[2] * x + s.recip[3] * y, s.m2J, lad + i * LS + L2);
+        }
+        __syncthreads();
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int i = warp; i < np; i += kWarps) {
+            const int gi = s.group_of[i];
+            double acc[4] = {0, 0, 0, 0};
+            const double* l1 = lad + i * LS;
+            for (int k = lane; k < s.nkJ; k += 32) {
+                double c, sn;
+                phase_k(s, l1, l1 + L2, k, c, sn);
+                kspace_particle_k(s, v, i, gi, k, c, sn, acc);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = warp_sum(acc[q]);
+            if (lane == 0) {
+                v.kg[i * 2] = acc[0];
+                v.kg[i * 2 + 1] = acc[1];
+                v.kl[i * 2] = acc[2];
+                v.kl[i * 2 + 1] = acc[3];
+            }
+        }
+    }
     __syncthreads();
 }
 
 // ───────────────────────── ratio ────────────────────────────────────────
 
-// ln|ψ'/ψ| of moving p to v.newpos; leaves in misc: R, scale, the log ratio,
-// phase, the Slater and Jastrow parts of ∇ ln ψ and ∂² ln ψ at the proposal;
-// in smem: new orbital row (nval/ngrad/nlap), per (term, partner) radial
-// values (rad), partner geometry (geo) and p's new phases (cn/sn).
-__device__ void ratio_step(const DevSys& s, const Smem& v, int p) {
+// ln|ψ'/ψ| of moving p to v.newpos.  `have_old` says whether co/so already
+// hold p's current phases (a drift refresh computed them).  Leaves in misc:
+// R, scale, the log ratio, the phase and the determinant, pair and k-space
+// parts of ∇ln ψ and ∂² ln ψ of p at the proposal; in shared memory: the new
+// orbital row, the per-partner radial derivatives (rad) and geometry (geo),
+// and p's new phases (cn/sn).
+__device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old) {
     const int np = s.np;
     const int b = block_of(s, p);
-    bool kspace = false;
-    for (int t = 0; t < s.nterms; ++t)
-        if (s.terms[t].image && in_term(s.terms[t], p)) kspace = true;
-    // phase 1: ladders of p's new position, orbitals, partners
-    double acc[11];
+    const bool ks = kspace_of(s, p);
+    double acc[15];
 #pragma unroll
-    for (int i = 0; i < 11; ++i) acc[i] = 0.0;
-    if (kspace && threadIdx.x < 2) {
-        const int q = threadIdx.x;
-        const double th = s.recip[q * 2] * v.newpos[0] + s.recip[q * 2 + 1] * v.newpos[1];
-        ladder(th, q == 0 ? s.m1J : s.m2J, v.misc + M_LAD + q * 2 * (kMaxLadder + 1));
+    for (int i = 0; i < 15; ++i) acc[i] = 0.0;
+    if (ks && threadIdx.x < (have_old ? 2 : 4)) {
+        const int q = threadIdx.x & 1;
+        const double* r = threadIdx.x < 2 ? v.newpos : v.pos + p * 2;
+        const double th = s.recip[q * 2] * r[0] + s.recip[q * 2 + 1] * r[1];
+        ladder(th, q == 0 ? s.m1J : s.m2J, v.misc + M_LAD + threadIdx.x * kLad);
     }
     if (b >= 0) {
         const DevBlock& B = s.blocks[b];
@@ -293,6 +407,9 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p) {
     }
     for (int k = threadIdx.x; k < np; k += kThreads) {
         if (k == p) continue;
+        bool any = false;
+        for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
+        if (!any) continue;
         double dn[3], dold[3];
         const double rn = fold_dist(s, v.newpos, v.pos + k * 2, dn);
         const double ro = fold_dist(s, v.pos + p * 2, v.pos + k * 2, dold);
@@ -303,36 +420,46 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p) {
         geo[3] = dold[0];
         geo[4] = dold[1];
         geo[5] = ro;
-        const double invr = 1.0 / rn;
+        double du_o = 0.0, d2u_o = 0.0, du_n = 0.0, d2u_n = 0.0;
         for (int t = 0; t < s.nterms; ++t) {
             const DevTerm& T = s.terms[t];
             if (!couples(T, p, k)) continue;
-            double* rad = v.rad + (static_cast<long>(t) * np + k) * 6;
-            radial(T, ro, rad[0], rad[1], rad[2]);
-            radial(T, rn, rad[3], rad[4], rad[5]);
-            acc[6] += rad[3] - rad[0];
-            for (int d = 0; d < 2; ++d) {
-                const double dor = dn[d] * invr;
-                acc[7 + d] += rad[4] * dor;
-                acc[9 + d] += rad[5] * dor * dor + rad[4] * invr * (1.0 - dor * dor);
-            }
+            double uo, duo, d2uo, un, dun, d2un;
+            radial(T, ro, uo, duo, d2uo);
+            radial(T, rn, un, dun, d2un);
+            acc[6] += un - uo;
+            du_o += duo;
+            d2u_o += d2uo;
+            du_n += dun;
+            d2u_n += d2un;
+        }
+        double* rad = v.rad + k * 4;
+        rad[0] = du_o;
+        rad[1] = d2u_o;
+        rad[2] = du_n;
+        rad[3] = d2u_n;
+        const double invr = 1.0 / rn;
+        for (int d = 0; d < 2; ++d) {
+            const double dor = dn[d] * invr;
+            acc[7 + d] += du_n * dor;
+            acc[9 + d] += d2u_n * dor * dor + du_n * invr * (1.0 - dor * dor);
         }
     }
-    __syncthreads();
-    // phase 2: p's new phases and the reciprocal half of every image sum
-    if (kspace) {
-        const double* l1 = v.misc + M_LAD;
-        const double* l2 = v.misc + M_LAD + 2 * (kMaxLadder + 1);
+    if (ks) {
+        __syncthreads();
         const int nk = s.nkJ;
-        const double* co = v.pc + p * 2 * nk;
-        const double* so = co + nk;
         const int gp = s.group_of[p];
         for (int k = threadIdx.x; k < nk; k += kThreads) {
-            double ar, ai, br, bi;
-            ladder_pick(l1, s.n1J[k], ar, ai);
-            ladder_pick(l2, s.n2J[k], br, bi);
-            const double c = ar * br - ai * bi;
-            const double sn = ar * bi + ai * br;
+            double c, sn, co, so;
+            phase_k(s, v.misc + M_LAD, v.misc + M_LAD + kLad, k, c, sn);
+            if (have_old) {
+                co = v.co[k];
+                so = v.so[k];
+            } else {
+                phase_k(s, v.misc + M_LAD + 2 * kLad, v.misc + M_LAD + 3 * kLad, k, co, so);
+                v.co[k] = co;
+                v.so[k] = so;
+            }
             v.cn[k] = c;
             v.sn[k] = sn;
             for (int t = 0; t < s.nterms; ++t) {
@@ -341,33 +468,21 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p) {
                 const double w = T.kw[k];
                 const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
                 const double* mr = v.rho + gp * 2 * nk;
-                double pr, pi, self, dlog;
                 if (T.same0) {
-                    const double qr = mr[k] + c - co[k];
-                    const double qi = mr[nk + k] + sn - so[k];
-                    dlog = w * (qr * qr + qi * qi - mr[k] * mr[k] - mr[nk + k] * mr[nk + k]);
-                    pr = qr;
-                    pi = qi;
-                    self = 1.0;
+                    const double qr = mr[k] + c - co;
+                    const double qi = mr[nk + k] + sn - so;
+                    acc[6] += w * (qr * qr + qi * qi - mr[k] * mr[k] - mr[nk + k] * mr[nk + k]);
+                    kterm(s, w, k, c, sn, qr, qi, 1.0, acc + 11);
                 } else {
                     const int go = gp == ga ? gb : ga;
                     const double* orr = v.rho + go * 2 * nk;
-                    dlog = 2.0 * w * ((c - co[k]) * orr[k] + (sn - so[k]) * orr[nk + k]);
-                    pr = orr[k];
-                    pi = orr[nk + k];
-                    self = 0.0;
+                    acc[6] += 2.0 * w * ((c - co) * orr[k] + (sn - so) * orr[nk + k]);
+                    kterm(s, w, k, c, sn, orr[k], orr[nk + k], 0.0, acc + 11);
                 }
-                const double g = 2.0 * w * (c * pi - sn * pr);
-                const double l = 2.0 * w * (self - (c * pr + sn * pi));
-                acc[6] += dlog;
-                acc[7] += s.kxJ[k] * g;
-                acc[8] += s.kyJ[k] * g;
-                acc[9] += s.kx2J[k] * l;
-                acc[10] += s.ky2J[k] * l;
             }
         }
     }
-    block_sum<11>(acc, v.red);
+    block_sum<15>(acc, v.red);
     if (threadIdx.x == 0) {
         double logr = acc[6], phase = 0.0, sgx = 0.0, sgy = 0.0, slx = 0.0, sly = 0.0;
         if (b >= 0) {
@@ -392,6 +507,10 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p) {
         v.misc[M_JGY] = acc[8];
         v.misc[M_JLX] = acc[9];
         v.misc[M_JLY] = acc[10];
+        v.misc[M_KGX] = acc[11];
+        v.misc[M_KGY] = acc[12];
+        v.misc[M_KLX] = acc[13];
+        v.misc[M_KLY] = acc[14];
     }
     __syncthreads();
 }
@@ -411,19 +530,19 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         double* Dg = grec + B.oDg;
         double* Dl = grec + B.oDl;
         double* rabs = v.scal - s.o_scal + B.orabs;
+        const double R = v.misc[M_R];
         for (int c = threadIdx.x; c < N; c += kThreads) {
             double prod = 0.0;
             for (int m = 0; m < N; ++m) prod += v.nval[m] * A[m * N + c];
             v.rowp[c] = prod - (c == jrow ? 1.0 : 0.0);
-            v.col[c] = A[c * N + jrow];
+            v.col[c] = A[c * N + jrow] / R;   // factor of row c of the update
             D[jrow * N + c] = v.nval[c];
-            Dg[(jrow * N + c) * 2 + 0] = v.ngrad[c * 2 + 0];
-            Dg[(jrow * N + c) * 2 + 1] = v.ngrad[c * 2 + 1];
-            Dl[(jrow * N + c) * 2 + 0] = v.nlap[c * 2 + 0];
-            Dl[(jrow * N + c) * 2 + 1] = v.nlap[c * 2 + 1];
+            reinterpret_cast<double2*>(Dg + jrow * N * 2)[c] =
+                make_double2(v.ngrad[c * 2 + 0], v.ngrad[c * 2 + 1]);
+            reinterpret_cast<double2*>(Dl + jrow * N * 2)[c] =
+                make_double2(v.nlap[c * 2 + 0], v.nlap[c * 2 + 1]);
         }
         if (threadIdx.x == 0) {
-            const double R = v.misc[M_R];
             bs[1] += 1.0;
             const bool rebuild = bs[1] >= 64.0 || !isfinite(R) || fabs(R) < 1e-5 || bs[2] > 1e8 ||
                                  fabs(R) <= 1e4 * kEps * v.misc[M_SCALE];
@@ -436,14 +555,11 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         const double old_log = bs[0];
         bool rebuild = v.misc[M_REBUILD] != 0.0;
         if (rebuild) {
-            __threadfence_block();
             gj_rebuild(s, v, grec, b);
         } else {
-            const double R = v.misc[M_R];
             for (int e = threadIdx.x; e < N * N; e += kThreads) {
-                const int a = e / N, c = e % N;
-                const double factor = v.col[a] / R;
-                A[e] = A[e] - factor * v.rowp[c];
+                const int a = e / N, c = e - a * N;
+                A[e] = A[e] - v.col[a] * v.rowp[c];
             }
             __syncthreads();
         }
@@ -461,18 +577,7 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
             gj_rebuild(s, v, grec, b);
             rebuild = true;
         }
-        if (threadIdx.x == 0) {
-            bs[2] = cond;
-            if (rebuild) {
-                bs[0] = v.misc[M_LOGDET];
-                bs[1] = 0.0;
-                if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
-            } else {
-                bs[0] = old_log + log(fabs(v.misc[M_R]));
-            }
-            v.scal[S_LOGPSI] += bs[0] - old_log;
-        }
-        // the moved particle's Slater derivatives at the committed inverse
+        // the moved particle's determinant derivatives at the committed inverse
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int m = threadIdx.x; m < N; m += kThreads) {
             const double a = A[m * N + jrow];
@@ -483,92 +588,57 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         }
         block_sum<4>(acc, v.red);
         if (threadIdx.x == 0) {
+            bs[2] = cond;
+            if (rebuild) {
+                bs[0] = v.misc[M_LOGDET];
+                bs[1] = 0.0;
+                if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+            } else {
+                bs[0] = old_log + log(fabs(R));
+            }
+            v.scal[S_LOGPSI] += bs[0] - old_log;
             v.sg[p * 2 + 0] = acc[0];
             v.sg[p * 2 + 1] = acc[1];
             v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
             v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
         }
     }
-    // pair terms: partner gradients and Laplacians
+    // pair terms: partner gradients and Laplacians (eager, as the reference)
     for (int k = threadIdx.x; k < np; k += kThreads) {
         if (k == p) continue;
+        bool any = false;
+        for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
+        if (!any) continue;
         const double* geo = v.geo + k * 6;
+        const double* rad = v.rad + k * 4;
         const double irn = 1.0 / geo[2], iro = 1.0 / geo[5];
-        for (int t = 0; t < s.nterms; ++t) {
-            const DevTerm& T = s.terms[t];
-            if (!couples(T, p, k)) continue;
-            const double* rad = v.rad + (static_cast<long>(t) * np + k) * 6;
-            for (int d = 0; d < 2; ++d) {
-                const double dor_old = -geo[3 + d] * iro, dor_new = -geo[d] * irn;
-                const double g_old = rad[1] * dor_old, g_new = rad[4] * dor_new;
-                v.jg[k * 2 + d] += g_new - g_old;
-                const double lap_old = rad[2] * dor_old * dor_old + rad[1] * iro * (1.0 - dor_old * dor_old);
-                const double lap_new = rad[5] * dor_new * dor_new + rad[4] * irn * (1.0 - dor_new * dor_new);
-                v.jl[k * 2 + d] += lap_new - lap_old;
-            }
+        for (int d = 0; d < 2; ++d) {
+            const double dor_old = -geo[3 + d] * iro, dor_new = -geo[d] * irn;
+            const double g_old = rad[0] * dor_old, g_new = rad[2] * dor_new;
+            v.jg[k * 2 + d] += g_new - g_old;
+            const double lap_old = rad[1] * dor_old * dor_old + rad[0] * iro * (1.0 - dor_old * dor_old);
+            const double lap_new = rad[3] * dor_new * dor_new + rad[2] * irn * (1.0 - dor_new * dor_new);
+            v.jl[k * 2 + d] += lap_new - lap_old;
         }
     }
-    // k-space: every particle that sees p's group density shifts by the δρ form
-    bool kspace = false;
-    for (int t = 0; t < s.nterms; ++t)
-        if (s.terms[t].image && in_term(s.terms[t], p)) kspace = true;
-    if (kspace) {
+    // k-space: ρ of p's group follows the move; partners refresh on their next read
+    if (kspace_of(s, p)) {
         const int nk = s.nkJ;
-        const int gp = s.group_of[p];
-        const double* co = v.pc + p * 2 * nk;
+        double* mr = v.rho + s.group_of[p] * 2 * nk;
         for (int k = threadIdx.x; k < nk; k += kThreads) {
-            v.dr[k] = v.cn[k] - co[k];
-            v.di[k] = v.sn[k] - co[nk + k];
-        }
-        __syncthreads();
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int t = 0; t < s.nterms; ++t) {
-            const DevTerm& T = s.terms[t];
-            if (!T.image || !in_term(T, p)) continue;
-            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
-            const int gs = T.same0 ? gp : (gp == ga ? gb : ga);
-            const int f0 = s.gfirst[gs], f1 = s.glast[gs];
-            for (int i = f0 + warp; i < f1; i += kWarps) {
-                if (i == p) continue;
-                const double* ci = v.pc + i * 2 * nk;
-                double gx = 0.0, gy = 0.0, lx = 0.0, ly = 0.0;
-                for (int k = lane; k < nk; k += 32) {
-                    const double w = T.kw[k];
-                    const double g = 2.0 * w * (ci[k] * v.di[k] - ci[nk + k] * v.dr[k]);
-                    const double l = 2.0 * w * (0.0 - (ci[k] * v.dr[k] + ci[nk + k] * v.di[k]));
-                    gx += s.kxJ[k] * g;
-                    gy += s.kyJ[k] * g;
-                    lx += s.kx2J[k] * l;
-                    ly += s.ky2J[k] * l;
-                }
-                gx = warp_sum(gx);
-                gy = warp_sum(gy);
-                lx = warp_sum(lx);
-                ly = warp_sum(ly);
-                if (lane == 0) {
-                    v.jg[i * 2 + 0] += gx;
-                    v.jg[i * 2 + 1] += gy;
-                    v.jl[i * 2 + 0] += lx;
-                    v.jl[i * 2 + 1] += ly;
-                }
-            }
-            __syncthreads();
-        }
-        double* mr = v.rho + gp * 2 * nk;
-        double* pcp = v.pc + p * 2 * nk;
-        for (int k = threadIdx.x; k < nk; k += kThreads) {
-            mr[k] += v.dr[k];
-            mr[nk + k] += v.di[k];
-            pcp[k] = v.cn[k];
-            pcp[nk + k] = v.sn[k];
+            mr[k] += v.cn[k] - v.co[k];
+            mr[nk + k] += v.sn[k] - v.so[k];
         }
     }
     if (threadIdx.x == 0) {
-        // p: new Jastrow derivatives, position (wrapped) and ln ψ of the Jastrow part
         v.jg[p * 2 + 0] = v.misc[M_JGX];
         v.jg[p * 2 + 1] = v.misc[M_JGY];
         v.jl[p * 2 + 0] = v.misc[M_JLX];
         v.jl[p * 2 + 1] = v.misc[M_JLY];
+        v.kg[p * 2 + 0] = v.misc[M_KGX];
+        v.kg[p * 2 + 1] = v.misc[M_KGY];
+        v.kl[p * 2 + 0] = v.misc[M_KLX];
+        v.kl[p * 2 + 1] = v.misc[M_KLY];
         double r[3] = {v.newpos[0], v.newpos[1], 0.0};
         wrap_pos(s, r);
         v.pos[p * 2 + 0] = r[0];
@@ -582,25 +652,27 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
 
 // ───────────────────────── local energy ─────────────────────────────────
 
+// E_L from refreshed derivatives: kinetic + Ewald (real, reciprocal,
+// constants) + open Coulomb.
 __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs, int npair) {
     const int np = s.np;
     double acc[1] = {0.0};
     for (int t = threadIdx.x; t < np * 2; t += kThreads) {
-        const double g = v.sg[t] + v.jg[t], l = v.sl[t] + v.jl[t];
+        const double g = v.sg[t] + v.jg[t] + v.kg[t], l = v.sl[t] + v.jl[t] + v.kl[t];
         acc[0] += -0.5 * s.inv_mass[t] * (l + g * g);
     }
     if (s.ewald) {
         for (int q = threadIdx.x; q < npair; q += kThreads) {
-            const int i = pairs[q].x, j = pairs[q].y;
-            const double coeff = s.charge[i] * s.charge[j];
+            const int2 pq = pairs[q];
+            const double coeff = s.charge[pq.x] * s.charge[pq.y];
             if (coeff == 0.0) continue;
             double del[3];
-            const double r = fold_dist(s, v.pos + i * 2, v.pos + j * 2, del);
+            const double r = fold_dist(s, v.pos + pq.x * 2, v.pos + pq.y * 2, del);
             if (r < s.e_rcut) acc[0] += coeff * (s.e_inv_eps / r - spline1(s.esp, r));
         }
-        // ladders e^{i n b_q·r_i}, n = 0..m_q, per particle
         double* lad = v.work;
         const int L1 = s.e_m1 + 1, L2 = s.e_m2 + 1;
+        __syncthreads();
         for (int i = threadIdx.x; i < np; i += kThreads) {
             const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
             ladder(s.recip[0] * x + s.recip[1] * y, s.e_m1, lad + i * 2 * (L1 + L2));
@@ -651,7 +723,8 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
         v.pos[i * 2] = r[0];
         v.pos[i * 2 + 1] = r[1];
     }
-    for (int i = threadIdx.x; i < np * 2; i += kThreads) v.jg[i] = v.jl[i] = v.sg[i] = v.sl[i] = 0.0;
+    for (int i = threadIdx.x; i < np * 2; i += kThreads)
+        v.jg[i] = v.jl[i] = v.kg[i] = v.kl[i] = v.sg[i] = v.sl[i] = 0.0;
     if (threadIdx.x == 0) {
         v.scal[S_LOGPSI] = 0.0;
         v.scal[S_ERR] = 0.0;
@@ -659,7 +732,7 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
     }
     __syncthreads();
     double lp[1] = {0.0};
-    // Slater: rows, A = D⁻¹ by Gauss-Jordan, log|det|, condition, derivatives
+    // determinants: rows, A = D⁻¹ by Gauss-Jordan, log|det|, condition
     for (int b = 0; b < s.nblocks; ++b) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n;
@@ -701,11 +774,10 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
             bs[1] = 0.0;
             bs[2] = nd * na;
             if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+            lp[0] += v.misc[M_LOGDET];
         }
-        lp[0] += threadIdx.x == 0 ? v.misc[M_LOGDET] : 0.0;
         __syncthreads();
     }
-    slater_refresh_all(s, v, grec);
     // pair terms: each thread owns particle i and sums over its partners
     for (int i = threadIdx.x; i < np; i += kThreads) {
         double g[2] = {0.0, 0.0}, l[2] = {0.0, 0.0}, u_half = 0.0;
@@ -732,39 +804,32 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
                 }
             }
         }
-        v.jg[i * 2] += g[0];
-        v.jg[i * 2 + 1] += g[1];
-        v.jl[i * 2] += l[0];
-        v.jl[i * 2 + 1] += l[1];
+        v.jg[i * 2] = g[0];
+        v.jg[i * 2 + 1] = g[1];
+        v.jl[i * 2] = l[0];
+        v.jl[i * 2 + 1] = l[1];
         lp[0] += u_half;
     }
-    __syncthreads();
-    // image sums: phase cache, ρ per group, then Σ w T and every particle's k terms
+    // image sums: ρ per group from every particle's phases, then Σ w T
     if (s.nkJ > 0) {
         const int nk = s.nkJ;
         double* lad = v.work;
-        const int L1 = s.m1J + 1, L2 = s.m2J + 1;
+        const int LS = 2 * (s.m1J + 1 + s.m2J + 1), L2 = 2 * (s.m1J + 1);
+        __syncthreads();
         for (int i = threadIdx.x; i < np; i += kThreads) {
             const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
-            ladder(s.recip[0] * x + s.recip[1] * y, s.m1J, lad + i * 2 * (L1 + L2));
-            ladder(s.recip[2] * x + s.recip[3] * y, s.m2J, lad + i * 2 * (L1 + L2) + 2 * L1);
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < np * nk; e += kThreads) {
-            const int i = e / nk, k = e % nk;
-            double ar, ai, br, bi;
-            ladder_pick(lad + i * 2 * (L1 + L2), s.n1J[k], ar, ai);
-            ladder_pick(lad + i * 2 * (L1 + L2) + 2 * L1, s.n2J[k], br, bi);
-            v.pc[i * 2 * nk + k] = ar * br - ai * bi;
-            v.pc[i * 2 * nk + nk + k] = ar * bi + ai * br;
+            ladder(s.recip[0] * x + s.recip[1] * y, s.m1J, lad + i * LS);
+            ladder(s.recip[2] * x + s.recip[3] * y, s.m2J, lad + i * LS + L2);
         }
         __syncthreads();
         for (int e = threadIdx.x; e < s.ngroups * nk; e += kThreads) {
             const int g = e / nk, k = e % nk;
             double re = 0.0, im = 0.0;
             for (int i = s.gfirst[g]; i < s.glast[g]; ++i) {
-                re += v.pc[i * 2 * nk + k];
-                im += v.pc[i * 2 * nk + nk + k];
+                double c, sn;
+                phase_k(s, lad + i * LS, lad + i * LS + L2, k, c, sn);
+                re += c;
+                im += sn;
             }
             v.rho[g * 2 * nk + k] = re;
             v.rho[g * 2 * nk + nk + k] = im;
@@ -781,31 +846,10 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
                 lp[0] += T.same0 ? w * (ar[k] * ar[k] + ar[nk + k] * ar[nk + k])
                                  : 2.0 * w * (ar[k] * br[k] + ar[nk + k] * br[nk + k]);
             }
-            for (int i = threadIdx.x; i < np; i += kThreads) {
-                const int gi = s.group_of[i];
-                if (gi != ga && gi != gb) continue;
-                const double* pr = v.rho + (T.same0 ? ga : (gi == ga ? gb : ga)) * 2 * nk;
-                const double self = T.same0 ? 1.0 : 0.0;
-                const double* ci = v.pc + i * 2 * nk;
-                double gx = 0.0, gy = 0.0, lx = 0.0, ly = 0.0;
-                for (int k = 0; k < nk; ++k) {
-                    const double w = T.kw[k];
-                    const double g = 2.0 * w * (ci[k] * pr[nk + k] - ci[nk + k] * pr[k]);
-                    const double l = 2.0 * w * (self - (ci[k] * pr[k] + ci[nk + k] * pr[nk + k]));
-                    gx += s.kxJ[k] * g;
-                    gy += s.kyJ[k] * g;
-                    lx += s.kx2J[k] * l;
-                    ly += s.ky2J[k] * l;
-                }
-                v.jg[i * 2] += gx;
-                v.jg[i * 2 + 1] += gy;
-                v.jl[i * 2] += lx;
-                v.jl[i * 2 + 1] += ly;
-            }
-            __syncthreads();
         }
     }
     block_sum<1>(lp, v.red);
+    refresh_all(s, v, grec);
     const double el = local_energy(s, v, pairs, npair);
     if (threadIdx.x == 0) {
         v.scal[S_LOGPSI] = lp[0];
@@ -838,7 +882,7 @@ __global__ void __launch_bounds__(kThreads) measure_kernel(DevSys s, double* rec
     double* rec = records + static_cast<long>(w) * s.rec;
     load_hot(s, rec, sm);
     const Smem v = view(s, sm);
-    slater_refresh_all(s, v, rec);
+    refresh_all(s, v, rec);
     const double el = local_energy(s, v, pairs, npair);
     if (threadIdx.x == 0) v.scal[S_EL] = el;
     store_hot(s, rec, sm);
@@ -859,15 +903,15 @@ __global__ void __launch_bounds__(kThreads) move_kernel(DevSys s, double* record
         v.misc[M_ERR] = 0.0;
     }
     __syncthreads();
-    ratio_step(s, v, p);
+    ratio_step(s, v, p, false);
     if (threadIdx.x == 0) {
         // log ratio, phase, new ∇ln ψ (dim), new ∂² ln ψ (dim), per walker
         out[0 * nw + w] = v.misc[M_LOGR];
         out[1 * nw + w] = v.misc[M_PHASE];
-        out[2 * nw + w] = v.misc[M_SGX] + v.misc[M_JGX];
-        out[3 * nw + w] = v.misc[M_SGY] + v.misc[M_JGY];
-        out[4 * nw + w] = v.misc[M_SLX] + v.misc[M_JLX];
-        out[5 * nw + w] = v.misc[M_SLY] + v.misc[M_JLY];
+        out[2 * nw + w] = v.misc[M_SGX] + v.misc[M_JGX] + v.misc[M_KGX];
+        out[3 * nw + w] = v.misc[M_SGY] + v.misc[M_JGY] + v.misc[M_KGY];
+        out[4 * nw + w] = v.misc[M_SLX] + v.misc[M_JLX] + v.misc[M_KLX];
+        out[5 * nw + w] = v.misc[M_SLY] + v.misc[M_JLY] + v.misc[M_KLY];
     }
     if (accept != nullptr && accept[w] != 0) commit_step(s, v, rec, p);
     store_hot(s, rec, sm);
@@ -903,50 +947,51 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
     for (int sub = 0; sub < prm.n_sub; ++sub) {
         const double* rnd = randoms + static_cast<long>(sub) * np * 3 * stride;
         for (int p = 0; p < np; ++p) {
-            if (drift) slater_refresh_particle(s, v, rec, p);
+            if (drift) refresh_particle(s, v, rec, p);
             if (threadIdx.x == 0) {
                 const double* g = rnd + static_cast<long>(p) * 3 * stride;
                 const double tm = prm.tau * s.inv_mass[p * 2];
+                const double gx = v.sg[p * 2] + v.jg[p * 2] + v.kg[p * 2];
+                const double gy = v.sg[p * 2 + 1] + v.jg[p * 2 + 1] + v.kg[p * 2 + 1];
                 double sc = tm;
-                const double gx = v.sg[p * 2] + v.jg[p * 2], gy = v.sg[p * 2 + 1] + v.jg[p * 2 + 1];
                 if (dmc) {
                     const double vsq = gx * gx + gy * gy;
                     sc = vsq < 1e-10 ? tm : (-1.0 + sqrt(1.0 + 2.0 * tm * vsq)) / vsq;
                 }
-                v.misc[M_SCFWD] = sc;   // forward drift scale
+                v.misc[M_SCFWD] = sc;
                 const double sig0 = prm.sigma[p * 2], sig1 = prm.sigma[p * 2 + 1];
                 if (drift) {
-                    const double tm0 = dmc ? sc : prm.tau * s.inv_mass[p * 2];
-                    const double tm1 = dmc ? sc : prm.tau * s.inv_mass[p * 2 + 1];
-                    v.newpos[0] = fma(sig0, g[0 * stride + w], fma(tm0, gx, v.pos[p * 2]));
-                    v.newpos[1] = fma(sig1, g[1 * stride + w], fma(tm1, gy, v.pos[p * 2 + 1]));
+                    const double t0 = dmc ? sc : prm.tau * s.inv_mass[p * 2];
+                    const double t1 = dmc ? sc : prm.tau * s.inv_mass[p * 2 + 1];
+                    v.newpos[0] = fma(sig0, g[0 * stride + w], fma(t0, gx, v.pos[p * 2]));
+                    v.newpos[1] = fma(sig1, g[1 * stride + w], fma(t1, gy, v.pos[p * 2 + 1]));
                 } else {
                     v.newpos[0] = fma(sig0, g[0 * stride + w], v.pos[p * 2]);
                     v.newpos[1] = fma(sig1, g[1 * stride + w], v.pos[p * 2 + 1]);
                 }
                 v.misc[M_U] = g[2 * stride + w];
-                v.misc[M_GOX] = gx;   // old total gradient, kept for the Green's function
+                v.misc[M_GOX] = gx;   // current total gradient, for the Green's function
                 v.misc[M_GOY] = gy;
             }
             __syncthreads();
-            ratio_step(s, v, p);
+            ratio_step(s, v, p, drift);
             if (threadIdx.x == 0) {
                 const double logr = v.misc[M_LOGR];
                 const double u = v.misc[M_U];
                 const double gx = v.misc[M_GOX], gy = v.misc[M_GOY];
-                const double ngx = v.misc[M_SGX] + v.misc[M_JGX];
-                const double ngy = v.misc[M_SGY] + v.misc[M_JGY];
+                const double ngx = v.misc[M_SGX] + v.misc[M_JGX] + v.misc[M_KGX];
+                const double ngy = v.misc[M_SGY] + v.misc[M_JGY] + v.misc[M_KGY];
                 const double dx = v.newpos[0] - v.pos[p * 2], dy = v.newpos[1] - v.pos[p * 2 + 1];
+                const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
                 bool acc;
                 if (dmc) {
                     acc = false;
-                    if (!(cos(v.misc[M_PHASE]) < kEps)) {
-                        const double tm = prm.tau * s.inv_mass[p * 2];
+                    // a real ratio's phase is 0 or π: the fixed-node gate (cos φ < ε)
+                    if (v.misc[M_PHASE] == 0.0) {
                         const double vsq = ngx * ngx + ngy * ngy;
-                        const double sb = vsq < 1e-10 ? tm : (-1.0 + sqrt(1.0 + 2.0 * tm * vsq)) / vsq;
+                        const double sb = vsq < 1e-10 ? tm0 : (-1.0 + sqrt(1.0 + 2.0 * tm0 * vsq)) / vsq;
                         const double sf = v.misc[M_SCFWD];
                         double lc = 0.0;
-                        const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
                         if (tm0 > 0.0) {
                             const double df = sf * gx, db = sb * ngx;
                             lc += (-dx * (df + db) + 0.5 * (df * df - db * db)) / tm0;
@@ -956,15 +1001,12 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
                             lc += (-dy * (df + db) + 0.5 * (df * df - db * db)) / tm1;
                         }
                         const double la = 2.0 * logr + lc;
-                        const double pacc = la >= 0.0 ? 1.0 : exp(la);
-                        acc = la >= 0.0 || u < pacc;
+                        acc = la >= 0.0 || u < exp(la);
                     }
-                    const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
                     const double rr = tm0 * dx * dx + tm1 * dy * dy;
                     v.scal[S_RRP] += rr;
                     if (acc) v.scal[S_RRA] += rr;
                 } else if (prm.drift) {
-                    const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
                     double lc = -dx * (gx + ngx) + 0.5 * tm0 * (gx * gx - ngx * ngx);
                     lc += -dy * (gy + ngy) + 0.5 * tm1 * (gy * gy - ngy * ngy);
                     const double la = 2.0 * logr + lc;
@@ -979,7 +1021,7 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
             if (v.misc[M_ACCEPT] != 0.0) commit_step(s, v, rec, p);
         }
         if (dmc || sub == prm.n_sub - 1) {
-            slater_refresh_all(s, v, rec);
+            refresh_all(s, v, rec);
             const double el = local_energy(s, v, pairs, npair);
             if (threadIdx.x == 0) {
                 v.scal[S_EL] = el;
@@ -1007,13 +1049,13 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
 }
 
 // One sweep's (or several sweeps') random numbers per stream: stream t fills
-// its crowd [w0, w1) in the reference's order (per particle: dim·n Gaussians
-// dimension-major, then n uniforms).  out[(sweep*np + p)*(dim+1)*stride + d*stride + w].
+// its crowd [w0, w1) of min(n_streams, nw) even splits in the reference's
+// order (per particle: dim·n Gaussians dimension-major, then n uniforms).
+// out[(sweep*np + p)*(dim+1)*stride + d*stride + w].
 __global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
                             int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
                             double zr, double* out, int crowd_mode) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_streams) return;
     const int n_active = n_streams < nw ? n_streams : nw;
     if (t >= n_active) return;
     const long base = nw / n_active, rem = nw % n_active;
@@ -1043,7 +1085,7 @@ __global__ void gather_kernel(double* dst, const double* src, const int* src_idx
     for (long i = threadIdx.x; i < rec / 2; i += blockDim.x) b[i] = a[i];
 }
 
-// Scalars of every walker into a packed [nw] array (slot k of the record).
+// Scalar slot of every walker into a packed [nw] array.
 __global__ void scalar_kernel(const double* records, int nw, long rec, int offset, double* out) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w < nw) out[w] = records[static_cast<long>(w) * rec + offset];
