@@ -263,6 +263,24 @@ class Walkers:
             ctypes.POINTER(ctypes.c_uint64)), int(target)))
         state[:] = st
 
+    def stream_handle(self) -> int:
+        """The cudaStream_t (as an int) the context's work is ordered on."""
+        v = ctypes.c_void_p()
+        self._check(self.lib.alea_gpu_stream(self.ctx, ctypes.byref(v)))
+        return int(v.value or 0)
+
+    def transfer_bytes(self):
+        """(host->device, device->host) bytes copied by this context so far."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self.lib.alea_gpu_transfer_bytes(self.ctx, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def launch_count(self) -> int:
+        """Kernels launched by this context so far."""
+        v = ctypes.c_uint64()
+        self._check(self.lib.alea_gpu_launch_count(self.ctx, ctypes.byref(v)))
+        return v.value
+
     def last_kernel_ms(self) -> float:
         v = ctypes.c_double()
         self._check(self.lib.alea_gpu_last_kernel_ms(self.ctx, ctypes.byref(v)))

@@ -102,7 +102,8 @@ class RunResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("energy_error", ctypes.c_double),
                 ("variance", ctypes.c_double), ("acceptance", ctypes.c_double),
                 ("walltime_s", ctypes.c_double), ("n_walkers", ctypes.c_int),
-                ("e_trial", ctypes.c_double)]
+                ("e_trial", ctypes.c_double), ("n_moves", ctypes.c_int64),
+                ("n_evaluations", ctypes.c_int64)]
 
 
 EXPORTS = [
@@ -110,7 +111,11 @@ EXPORTS = [
     "alea_gpu_upload_walkers", "alea_gpu_evaluate", "alea_gpu_num_walkers",
     "alea_gpu_download_walkers", "alea_gpu_move", "alea_gpu_measure", "alea_gpu_set_streams",
     "alea_gpu_vmc_step", "alea_gpu_dmc_advance", "alea_gpu_dmc_branch", "alea_gpu_vmc_run",
-    "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms",
+    "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms", "alea_gpu_stream", "alea_gpu_transfer_bytes",
+    "alea_gpu_launch_count",
+    "alea_gpu_setup_heg2d", "alea_gpu_setup_crystal2d", "alea_gpu_setup_exciton2d",
+    "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
+    "alea_gpu_setup_free",
 ]
 
 _LIB = None
@@ -144,6 +149,18 @@ def load() -> ctypes.CDLL:
         "alea_gpu_vmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),
         "alea_gpu_dmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),
         "alea_gpu_last_kernel_ms": ([P, c_dp], I),
+        "alea_gpu_stream": ([P, ctypes.POINTER(P)], I),
+        "alea_gpu_launch_count": ([P, ctypes.POINTER(ctypes.c_uint64)], I),
+        "alea_gpu_transfer_bytes": ([P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)], I),
+        "alea_gpu_setup_heg2d": ([I, I, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
+                                  ctypes.c_size_t], I),
+        "alea_gpu_setup_crystal2d": ([I, I, D, D, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
+                                      ctypes.c_size_t], I),
+        "alea_gpu_setup_exciton2d": ([D, ctypes.POINTER(P)], I),
+        "alea_gpu_setup_system": ([P], ctypes.POINTER(System)),
+        "alea_gpu_setup_json": ([P], ctypes.c_char_p),
+        "alea_gpu_setup_positions": ([P, ctypes.c_uint64, I, c_dp], I),
+        "alea_gpu_setup_free": ([P], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

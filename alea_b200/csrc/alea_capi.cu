@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -169,11 +170,14 @@ struct alea_gpu_ctx {
     int* d_src = nullptr;
     uint8_t* d_mask = nullptr;
     size_t smem = 0;
+    int nt = 128;                  // threads per walker CTA
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     std::vector<double> h_inv_mass;
     std::vector<double> h_w, h_el, h_ids, h_par, h_nacc, h_ncut;
     double next_id = 1.0;
+    uint64_t h2d = 0, d2h = 0;     // bytes copied host->device / device->host
+    uint64_t launches = 0;         // kernels launched by this context
 };
 
 namespace {
@@ -192,6 +196,30 @@ int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
     } while (0)
 
 long round4(long x) { return (x + 3) & ~3L; }
+
+// Host<->device copies on the context's stream, counted.
+cudaError_t copy_in(alea_gpu_ctx* c, void* dst, const void* src, size_t n) {
+    c->h2d += n;
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, c->stream);
+}
+cudaError_t copy_out(alea_gpu_ctx* c, void* dst, const void* src, size_t n) {
+    c->d2h += n;
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, c->stream);
+}
+
+// Threads per walker CTA: one warp while a move has at most a few tens of
+// independent items (orbitals, partners, k vectors), wider for larger systems.
+// ALEA_GPU_THREADS overrides (32, 64 or 128).
+int pick_threads(const DevSys& s) {
+    if (const char* e = std::getenv("ALEA_GPU_THREADS")) {
+        const int v = std::atoi(e);
+        if (v == 32 || v == 64 || v == 128) return v;
+    }
+    if (s.maxN <= 32 && s.np <= 64) return 32;
+    if (s.maxN <= 48 && s.np <= 128) return 64;
+    return 128;
+}
+
 
 // Cell from the lattice rows: axis alignment, 2-D Gauss reduction, (Aᵀ)⁻¹,
 // the orthorhombic fold, the 3×3 candidate shell, reciprocal vectors.
@@ -521,19 +549,22 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     s.s_nval = take(s.maxN);
     s.s_ngrad = take(2 * s.maxN);
     s.s_nlap = take(2 * s.maxN);
-    s.s_rad = take(static_cast<long>(np) * 4 + np * 6);
     s.s_cn = take(s.nkJ);
     s.s_sn = take(s.nkJ);
     s.s_co = take(s.nkJ);
     s.s_so = take(s.nkJ);
     s.s_col = take(s.maxN);
     s.s_rowp = take(s.maxN);
-    s.s_red = take(kWarps * 16 + 16);
-    s.s_misc = take(64 + 4 * 2 * (kMaxLadder + 1));
+    s.s_red = take(4 * 16 + 16);
+    s.s_misc = take(32 + 4 * 2 * (kMaxLadder + 1));
+    // One union: the per-partner scratch of a move (read by the commit before
+    // any rebuild), the Gauss-Jordan work matrix, and the ρ(k) accumulators
+    // of the local energy.
     long work = static_cast<long>(s.maxN) * s.maxN;
-    work = std::max(work, static_cast<long>(np) * 2 * (s.e_m1 + s.e_m2 + 2));
-    work = std::max(work, static_cast<long>(np) * 2 * (s.m1J + s.m2J + 2));
+    work = std::max(work, 2L * s.enk);
+    work = std::max(work, static_cast<long>(np) * 10);
     s.s_work = take(work);
+    s.s_rad = s.s_work;
     s.s_total = static_cast<int>(m);
     c->smem = static_cast<size_t>(s.s_total) * 8;
     if (c->smem > 227 * 1024)
@@ -572,7 +603,7 @@ int set_sigma(alea_gpu_ctx* c, double tau) {
     if (tau == c->sigma_tau) return ALEA_OK;
     std::vector<double> sg(c->h_inv_mass.size());
     for (size_t i = 0; i < sg.size(); ++i) sg[i] = std::sqrt(tau * c->h_inv_mass[i]);
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_sigma, sg.data(), sg.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, copy_in(c, c->d_sigma, sg.data(), sg.size() * 8));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->sigma_tau = tau;
     return ALEA_OK;
@@ -583,17 +614,19 @@ double* records(alea_gpu_ctx* c) { return c->rec[c->cur]; }
 int read_scalars(alea_gpu_ctx* c, int slot, std::vector<double>& out) {
     out.resize(c->nw);
     if (c->nw == 0) return ALEA_OK;
+    ++c->launches;
     scalar_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
                                                               c->sys.o_scal + slot, c->d_buf);
     CUDA_TRY(c, cudaGetLastError());
-    CUDA_TRY(c, cudaMemcpyAsync(out.data(), c->d_buf, 8 * c->nw, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, copy_out(c, out.data(), c->d_buf, 8 * c->nw));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return ALEA_OK;
 }
 
 int write_scalars(alea_gpu_ctx* c, int slot, const std::vector<double>& in) {
     if (c->nw == 0) return ALEA_OK;
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_buf, in.data(), 8 * c->nw, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, copy_in(c, c->d_buf, in.data(), 8 * c->nw));
+    ++c->launches;
     from_soa_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
                                                                 c->sys.o_scal + slot, 1, c->d_buf);
     CUDA_TRY(c, cudaGetLastError());
@@ -613,8 +646,8 @@ int check_errors(alea_gpu_ctx* c) {
 
 int launch_evaluate(alea_gpu_ctx* c) {
     if (c->nw == 0) return ALEA_OK;
-    evaluate_kernel<<<c->nw, kThreads, c->smem, c->stream>>>(c->sys, records(c), c->nw, c->pairs, c->npair);
-    CUDA_TRY(c, cudaGetLastError());
+    ++c->launches;
+    CUDA_TRY(c, launch_evaluate(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_errors(c);
 }
@@ -629,6 +662,7 @@ int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, doubl
     if (int rc = set_sigma(c, tau)) return rc;
     const long stride = c->nw;
     const int nt = std::min(c->n_streams, c->nw);
+    ++c->launches;
     draw_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, stride,
                                                          n_sub, c->sys.zk, c->sys.zw, c->sys.zf, c->sys.zr,
                                                          c->randoms, 0);
@@ -644,9 +678,9 @@ int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, doubl
     prm.e_cut = e_cut;
     prm.e_max = e_max;
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-    sweep_kernel<<<c->nw, kThreads, c->smem, c->stream>>>(c->sys, records(c), c->nw, c->randoms, stride, prm,
-                                                          c->pairs, c->npair);
-    CUDA_TRY(c, cudaGetLastError());
+    ++c->launches;
+    CUDA_TRY(c, launch_sweep(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->randoms, stride, prm,
+                             c->pairs, c->npair));
     CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     float ms = 0.f;
@@ -714,13 +748,10 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
             return bail(ALEA_ERR_NOMEM);
         }
     }
-    for (const void* k : {reinterpret_cast<const void*>(evaluate_kernel), reinterpret_cast<const void*>(measure_kernel),
-                          reinterpret_cast<const void*>(move_kernel), reinterpret_cast<const void*>(sweep_kernel)}) {
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(c->smem)) !=
-            cudaSuccess) {
-            c->err = "cannot reserve " + std::to_string(c->smem) + " bytes of shared memory";
-            return bail(ALEA_ERR_UNSUPPORTED);
-        }
+    c->nt = pick_threads(s);
+    if (reserve_smem(c->smem) != cudaSuccess) {
+        c->err = "cannot reserve " + std::to_string(c->smem) + " bytes of shared memory";
+        return bail(ALEA_ERR_UNSUPPORTED);
     }
     *out = c;
     return ALEA_OK;
@@ -756,11 +787,12 @@ int alea_gpu_upload_walkers(alea_gpu_ctx* c, const double* positions, int nw) {
     c->nw = nw;
     const DevSys& s = c->sys;
     CUDA_TRY(c, cudaMemsetAsync(records(c), 0, static_cast<size_t>(s.rec) * 8 * nw, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_buf, positions, static_cast<size_t>(s.np) * 2 * nw * 8,
-                                cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, copy_in(c, c->d_buf, positions, static_cast<size_t>(s.np) * 2 * nw * 8));
     const long n = static_cast<long>(s.np) * 2 * nw;
+    ++c->launches;
     from_soa_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_pos,
                                                                              s.np * 2, c->d_buf);
+    ++c->launches;
     set_scalar_kernel<<<(nw + 255) / 256, 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_scal + S_WEIGHT, 1.0);
     CUDA_TRY(c, cudaGetLastError());
     c->next_id = 1.0;
@@ -783,9 +815,10 @@ int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_ps
     const long n = static_cast<long>(s.np) * 2 * nw;
     const int grid = static_cast<int>((n + 255) / 256);
     auto plane = [&](int off, double* dst) -> int {
+        ++c->launches;
         to_soa_kernel<<<grid, 256, 0, c->stream>>>(records(c), nw, s.rec, off, s.np * 2, c->d_buf);
         CUDA_TRY(c, cudaGetLastError());
-        CUDA_TRY(c, cudaMemcpyAsync(dst, c->d_buf, n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, copy_out(c, dst, c->d_buf, n * 8));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         return ALEA_OK;
     };
@@ -831,13 +864,13 @@ int alea_gpu_move(alea_gpu_ctx* c, int p, const double* new_pos, const uint8_t* 
     double* d_out = c->d_buf + 2 * nw;
     if (static_cast<long>(8) * nw > static_cast<long>(std::max(s.np * 2, 8)) * c->capacity)
         return fail(c, ALEA_ERR_NOMEM, "staging buffer too small");
-    CUDA_TRY(c, cudaMemcpyAsync(d_np, new_pos, 16L * nw, cudaMemcpyHostToDevice, c->stream));
-    if (accept) CUDA_TRY(c, cudaMemcpyAsync(c->d_mask, accept, nw, cudaMemcpyHostToDevice, c->stream));
-    move_kernel<<<nw, kThreads, c->smem, c->stream>>>(s, records(c), nw, p, d_np, accept ? c->d_mask : nullptr,
-                                                      d_out);
-    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, copy_in(c, d_np, new_pos, 16L * nw));
+    if (accept) CUDA_TRY(c, copy_in(c, c->d_mask, accept, nw));
+    ++c->launches;
+    CUDA_TRY(c, launch_move(c->nt, nw, c->smem, c->stream, s, records(c), p, d_np,
+                            accept ? c->d_mask : nullptr, d_out));
     std::vector<double> out(6L * nw);
-    CUDA_TRY(c, cudaMemcpyAsync(out.data(), d_out, 48L * nw, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, copy_out(c, out.data(), d_out, 48L * nw));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     for (int w = 0; w < nw; ++w) {
         if (log_ratio) log_ratio[w] = out[w];
@@ -858,8 +891,8 @@ int alea_gpu_measure(alea_gpu_ctx* c) {
     if (!c) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->nw == 0) return ALEA_OK;
-    measure_kernel<<<c->nw, kThreads, c->smem, c->stream>>>(c->sys, records(c), c->nw, c->pairs, c->npair);
-    CUDA_TRY(c, cudaGetLastError());
+    ++c->launches;
+    CUDA_TRY(c, launch_measure(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return ALEA_OK;
 }
@@ -873,7 +906,8 @@ int alea_gpu_set_streams(alea_gpu_ctx* c, uint64_t seed, uint64_t kind, int n) {
         HostXo x(stream_seed(seed, kind, static_cast<uint64_t>(t)));
         for (int k = 0; k < 4; ++k) st[4L * t + k] = x.s[k];
     }
-    CUDA_TRY(c, cudaMemcpy(c->streams, st.data(), st.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy_in(c, c->streams, st.data(), st.size() * 8));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->n_streams = n;
     return ALEA_OK;
 }
@@ -987,16 +1021,37 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
         }
     }
     const int nn = static_cast<int>(src.size());
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_src, src.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, copy_in(c, c->d_src, src.data(), sizeof(int) * nn));
+    ++c->launches;
     gather_kernel<<<nn, 256, 0, c->stream>>>(c->rec[1 - c->cur], c->rec[c->cur], c->d_src, nn, c->sys.rec);
     CUDA_TRY(c, cudaGetLastError());
     c->cur = 1 - c->cur;
     c->nw = nn;
+    ++c->launches;
     set_scalar_kernel<<<(nn + 255) / 256, 256, 0, c->stream>>>(records(c), nn, c->sys.rec,
                                                                 c->sys.o_scal + S_WEIGHT, 1.0);
     CUDA_TRY(c, cudaGetLastError());
     if (int rc = write_scalars(c, S_ID, nid)) return rc;
     if (int rc = write_scalars(c, S_PARENT, npar)) return rc;
+    return ALEA_OK;
+}
+
+int alea_gpu_stream(const alea_gpu_ctx* c, void** stream) {
+    if (!c || !stream) return ALEA_ERR_INVALID;
+    *stream = static_cast<void*>(c->stream);
+    return ALEA_OK;
+}
+
+int alea_gpu_transfer_bytes(const alea_gpu_ctx* c, uint64_t* h2d, uint64_t* d2h) {
+    if (!c) return ALEA_ERR_INVALID;
+    if (h2d) *h2d = c->h2d;
+    if (d2h) *d2h = c->d2h;
+    return ALEA_OK;
+}
+
+int alea_gpu_launch_count(const alea_gpu_ctx* c, uint64_t* launches) {
+    if (!c || !launches) return ALEA_ERR_INVALID;
+    *launches = c->launches;
     return ALEA_OK;
 }
 
@@ -1017,7 +1072,7 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     std::vector<double> blocks;   // [T][n_acc], chain-major
     std::vector<std::vector<double>> chain(T);
     double e_sum = 0, e2_sum = 0;
-    int64_t n_tot = 0, acc = 0, prop = 0;
+    int64_t n_tot = 0, acc = 0, prop = 0, all_moves = 0, all_evals = 0;
     const int base = nw / T, rem = nw % T;
     for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
         const bool measure = b >= cfg->n_equilibration_blocks;
@@ -1026,6 +1081,8 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
         for (int st = 0; st < cfg->n_steps; ++st) {
             alea_gpu_step_stats s{};
             if (int rc = alea_gpu_vmc_step(c, &prm, &s)) return rc;
+            all_moves += s.n_proposed;
+            all_evals += s.n_walkers;
             if (!measure) continue;
             std::vector<double> el;
             if (int rc = read_scalars(c, S_EL, el)) return rc;
@@ -1056,6 +1113,8 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     res->walltime_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     res->n_walkers = c->nw;
     res->e_trial = 0.0;
+    res->n_moves = all_moves;
+    res->n_evaluations = all_evals;
     if (block_energies) std::copy(blocks.begin(), blocks.end(), block_energies);
     return ALEA_OK;
 }
@@ -1102,7 +1161,7 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     };
     refresh_spread(el);
     std::vector<double> blocks;
-    int64_t acc = 0, prop = 0;
+    int64_t acc = 0, prop = 0, all_evals = 0;
     for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
         const bool measure = b >= cfg->n_equilibration_blocks;
         if (b == cfg->n_equilibration_blocks) eref_sum = eref_wsum = 0.0;
@@ -1113,6 +1172,7 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             if (int rc = alea_gpu_dmc_advance(c, &prm, &s)) return rc;
             acc += s.n_accepted;
             prop += s.n_proposed;
+            all_evals += static_cast<int64_t>(std::max(1, cfg->n_substeps)) * s.n_walkers;
             blk_e += s.energy_sum;
             blk_w += s.weight_sum;
             const double ens_e = s.weight_sum > 0.0 ? s.energy_sum / s.weight_sum : etrial;
@@ -1144,6 +1204,8 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     res->walltime_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     res->n_walkers = c->nw;
     res->e_trial = etrial;
+    res->n_moves = prop;
+    res->n_evaluations = all_evals;
     if (block_energies) std::copy(blocks.begin(), blocks.end(), block_energies);
     return ALEA_OK;
 }

@@ -14,14 +14,12 @@
 
 namespace alea_gpu {
 
-constexpr int kThreads = 128;          // threads per walker CTA
-constexpr int kWarps = kThreads / 32;
 constexpr int kMaxBlocks = 4;
 constexpr int kMaxTerms = 8;
 constexpr int kMaxGroups = 8;
 constexpr int kMaxCoulomb = 8;
 constexpr int kMaxN = 64;              // largest determinant block
-constexpr int kMaxLadder = 32;         // largest |n| of a reciprocal index
+constexpr int kMaxLadder = 16;         // largest |n| of a reciprocal index
 
 // Scalar slots of a walker record.
 enum : int {
@@ -347,38 +345,47 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Sum K values over the CTA; every thread gets the totals.  `red` holds
-// kWarps*K + K doubles.  Contains two barriers.
-template <int K>
+// Sum K values over the CTA of NT threads; every thread gets the totals.  A
+// one-warp CTA uses shuffles only; wider ones go through `red`
+// (NT/32*K + K doubles) with two barriers.
+template <int NT, int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
-    if (lane == 0)
+    if constexpr (NT > 32) {
+        constexpr int W = NT / 32;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0)
 #pragma unroll
-        for (int k = 0; k < K; ++k) red[warp * K + k] = v[k];
-    __syncthreads();
-    if (threadIdx.x < K) {
-        double t = 0.0;
-        for (int w = 0; w < kWarps; ++w) t += red[w * K + threadIdx.x];
-        red[kWarps * K + threadIdx.x] = t;
+            for (int k = 0; k < K; ++k) red[warp * K + k] = v[k];
+        __syncthreads();
+        if (threadIdx.x < K) {
+            double t = 0.0;
+            for (int w = 0; w < W; ++w) t += red[w * K + threadIdx.x];
+            red[W * K + threadIdx.x] = t;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = red[W * K + k];
+        __syncthreads();
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = red[kWarps * K + k];
-    __syncthreads();
 }
 
+template <int NT>
 __device__ __forceinline__ double block_max(double v, double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    double m = red[0];
-    for (int w = 1; w < kWarps; ++w) m = fmax(m, red[w]);
-    __syncthreads();
-    return m;
+    if constexpr (NT > 32) {
+        constexpr int W = NT / 32;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        double m = red[0];
+        for (int w = 1; w < W; ++w) m = fmax(m, red[w]);
+        __syncthreads();
+        return m;
+    }
+    return v;
 }
 
 // ───────────────────────── random numbers ───────────────────────────────

@@ -18,10 +18,13 @@
 //   branch weight  src/qmc/population_control.cpp:56-77
 //   randoms        src/qmc/sweep_blocking.h:39-48
 //
-// Parallel layout: one CTA of kThreads threads per walker.  Work inside a
-// move is spread over orbitals (Slater), partners (pair terms), k-vectors
-// (image sums) and matrix elements (rank-one update); partial sums meet in
-// block reductions.
+// Parallel layout: one CTA of NT threads per walker (NT = 32, 64 or 128,
+// chosen per system: a move of a small system has only tens of independent
+// items, and a one-warp CTA needs no cross-warp barrier).  Work inside a move
+// is spread over orbitals (Slater), partners (pair terms), k-vectors (image
+// sums) and matrix elements (rank-one update); partial sums meet in
+// reductions.  Reciprocal phase ladders e^{inθ} are computed one entry per
+// thread (sincos(nθ)) instead of by the serial recurrence.
 //
 // Deferred derivatives.  Like the reference's determinant (deferred partner
 // refresh, slater_determinant.cpp:862-903), the k-space half of an image-summed
@@ -46,7 +49,7 @@ constexpr int kLad = 2 * (kMaxLadder + 1);   // doubles per ladder
 struct Smem {
     double *pos, *jg, *jl, *kg, *kl, *sg, *sl, *scal, *rho;
     double *newpos, *nval, *ngrad, *nlap, *rad, *geo, *cn, *sn, *co, *so, *col, *rowp, *red,
-        *misc, *work;
+        *misc, *lad, *work;
 };
 
 __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
@@ -74,6 +77,7 @@ __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
     v.rowp = sm + s.s_rowp;
     v.red = sm + s.s_red;
     v.misc = sm + s.s_misc;
+    v.lad = v.misc + 32;          // four ladders of kLad doubles
     v.work = sm + s.s_work;
     return v;
 }
@@ -82,21 +86,23 @@ __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
 enum : int {
     M_R = 0, M_SCALE, M_LOGR, M_PHASE, M_ACCEPT, M_REBUILD, M_LOGDET, M_ERR, M_U, M_SCFWD,
     M_GOX, M_GOY, M_SGX, M_SGY, M_SLX, M_SLY, M_JGX, M_JGY, M_JLX, M_JLY, M_KGX, M_KGY,
-    M_KLX, M_KLY, M_LAD /* four ladders of kMaxLadder + 1 complex values follow */
+    M_KLX, M_KLY
 };
 
+template <int NT>
 __device__ __forceinline__ void load_hot(const DevSys& s, const double* rec, double* sm) {
     const double2* src = reinterpret_cast<const double2*>(rec);
     double2* dst = reinterpret_cast<double2*>(sm);
-    for (int i = threadIdx.x; i < s.hot / 2; i += kThreads) dst[i] = src[i];
+    for (int i = threadIdx.x; i < s.hot / 2; i += NT) dst[i] = src[i];
     __syncthreads();
 }
 
+template <int NT>
 __device__ __forceinline__ void store_hot(const DevSys& s, double* rec, const double* sm) {
     __syncthreads();
     const double2* src = reinterpret_cast<const double2*>(sm);
     double2* dst = reinterpret_cast<double2*>(rec);
-    for (int i = threadIdx.x; i < s.hot / 2; i += kThreads) dst[i] = src[i];
+    for (int i = threadIdx.x; i < s.hot / 2; i += NT) dst[i] = src[i];
 }
 
 __device__ __forceinline__ int block_of(const DevSys& s, int p) {
@@ -111,21 +117,27 @@ __device__ __forceinline__ bool kspace_of(const DevSys& s, int p) {
     return false;
 }
 
-// e^{i n θ} for n = 0..m into (re, im) pairs at out[2n], out[2n+1]
-// (the integer ladders of reciprocal_phases.h).
-__device__ __forceinline__ void ladder(double theta, int m, double* out) {
-    double c, sn;
-    sincos(theta, &sn, &c);
-    double r = 1.0, i = 0.0;
-    out[0] = 1.0;
-    out[1] = 0.0;
-    for (int n = 1; n <= m; ++n) {
-        const double nr = r * c - i * sn;
-        const double ni = r * sn + i * c;
-        r = nr;
-        i = ni;
-        out[2 * n] = r;
-        out[2 * n + 1] = i;
+// Ladders e^{inθ_q}, n = 0..m_q, of up to four angles, one entry per thread,
+// into out[q*kLad + 2n], out[q*kLad + 2n + 1].  No barrier.
+template <int NT>
+__device__ __forceinline__ void ladders(const double* theta, const int* m, int nq, double* out) {
+    int total = 0;
+    for (int q = 0; q < nq; ++q) total += m[q] + 1;
+    for (int e = threadIdx.x; e < total; e += NT) {
+        int q = 0, n = e;
+        while (n > m[q]) {
+            n -= m[q] + 1;
+            ++q;
+        }
+        double c, sn;
+        if (n == 0) {
+            c = 1.0;
+            sn = 0.0;
+        } else {
+            sincos(static_cast<double>(n) * theta[q], &sn, &c);
+        }
+        out[q * kLad + 2 * n] = c;
+        out[q * kLad + 2 * n + 1] = sn;
     }
 }
 
@@ -177,13 +189,15 @@ __device__ __forceinline__ void kspace_particle_k(const DevSys& s, const Smem& v
 // A = D⁻¹ of block b from its committed rows in HBM, by pivoted Gauss-Jordan
 // (first maximum |pivot| in each column, as the reference's rebuild_inverse).
 // Leaves log|det D| in misc[M_LOGDET]; flags a singular matrix in misc[M_ERR].
+template <int NT>
 __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, int b) {
     const DevBlock& B = s.blocks[b];
     const int N = B.n;
     double* A = v.scal - s.o_scal + B.oA;
     double* m = v.work;
     const double* D = grec + B.oD;
-    for (int e = threadIdx.x; e < N * N; e += kThreads) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < N * N; e += NT) {
         m[e] = D[e];
         A[e] = (e / N == e % N) ? 1.0 : 0.0;
     }
@@ -219,7 +233,7 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
         __syncthreads();
         const int piv = s_piv;
         if (piv != k)
-            for (int c = threadIdx.x; c < N; c += kThreads) {
+            for (int c = threadIdx.x; c < N; c += NT) {
                 double t = m[k * N + c];
                 m[k * N + c] = m[piv * N + c];
                 m[piv * N + c] = t;
@@ -230,14 +244,14 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
         __syncthreads();
         const double diag = m[k * N + k];
         __syncthreads();
-        for (int c = threadIdx.x; c < N; c += kThreads) {
+        for (int c = threadIdx.x; c < N; c += NT) {
             m[k * N + c] /= diag;
             A[k * N + c] /= diag;
         }
         __syncthreads();
-        for (int r = threadIdx.x; r < N; r += kThreads) v.col[r] = m[r * N + k];
+        for (int r = threadIdx.x; r < N; r += NT) v.col[r] = m[r * N + k];
         __syncthreads();
-        for (int e = threadIdx.x; e < N * N; e += kThreads) {
+        for (int e = threadIdx.x; e < N * N; e += NT) {
             const int r = e / N, c = e % N;
             if (r == k) continue;
             const double f = v.col[r];
@@ -252,26 +266,28 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
 
 // Drift refresh of particle p: its determinant derivatives from A and the
 // committed rows, and its k-space derivatives from ρ(k) and its phases (left
-// in co/so for the ratio).  Ends with the block reduction's barriers.
+// in co/so for the ratio).
+template <int NT>
 __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* grec, int p) {
     const int b = block_of(s, p);
     const bool ks = kspace_of(s, p);
-    if (ks && threadIdx.x < 2) {
-        const int q = threadIdx.x;
-        const double th = s.recip[q * 2] * v.pos[p * 2] + s.recip[q * 2 + 1] * v.pos[p * 2 + 1];
-        ladder(th, q == 0 ? s.m1J : s.m2J, v.misc + M_LAD + q * kLad);
+    if (ks) {
+        const double th[2] = {s.recip[0] * v.pos[p * 2] + s.recip[1] * v.pos[p * 2 + 1],
+                              s.recip[2] * v.pos[p * 2] + s.recip[3] * v.pos[p * 2 + 1]};
+        const int m[2] = {s.m1J, s.m2J};
+        ladders<NT>(th, m, 2, v.lad);
     }
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (b >= 0) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n, kr = p - B.first;
         const double* A = v.scal - s.o_scal + B.oA;
-        const double* Dg = grec + B.oDg + kr * N * 2;
-        const double* Dl = grec + B.oDl + kr * N * 2;
-        for (int m = threadIdx.x; m < N; m += kThreads) {
+        const double2* Dg = reinterpret_cast<const double2*>(grec + B.oDg + kr * N * 2);
+        const double2* Dl = reinterpret_cast<const double2*>(grec + B.oDl + kr * N * 2);
+        for (int m = threadIdx.x; m < N; m += NT) {
             const double a = A[m * N + kr];
-            const double2 g = reinterpret_cast<const double2*>(Dg)[m];
-            const double2 l = reinterpret_cast<const double2*>(Dl)[m];
+            const double2 g = Dg[m];
+            const double2 l = Dl[m];
             acc[0] += a * g.x;
             acc[1] += a * g.y;
             acc[2] += a * l.x;
@@ -281,15 +297,15 @@ __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* g
     if (ks) {
         __syncthreads();
         const int gp = s.group_of[p];
-        for (int k = threadIdx.x; k < s.nkJ; k += kThreads) {
+        for (int k = threadIdx.x; k < s.nkJ; k += NT) {
             double c, sn;
-            phase_k(s, v.misc + M_LAD, v.misc + M_LAD + kLad, k, c, sn);
+            phase_k(s, v.lad, v.lad + kLad, k, c, sn);
             v.co[k] = c;
             v.so[k] = sn;
             kspace_particle_k(s, v, p, gp, k, c, sn, acc + 4);
         }
     }
-    block_sum<8>(acc, v.red);
+    block_sum<NT>(acc, v.red);
     if (threadIdx.x == 0) {
         if (b >= 0) {
             v.sg[p * 2 + 0] = acc[0];
@@ -308,6 +324,7 @@ __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* g
 }
 
 // Every particle's determinant and k-space derivatives (refresh_derivatives).
+template <int NT>
 __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) {
     const int np = s.np;
     for (int b = 0; b < s.nblocks; ++b) {
@@ -316,7 +333,7 @@ __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) 
         const double* A = v.scal - s.o_scal + B.oA;
         const double* Dg = grec + B.oDg;
         const double* Dl = grec + B.oDl;
-        for (int t = threadIdx.x; t < N * 2; t += kThreads) {
+        for (int t = threadIdx.x; t < N * 2; t += NT) {
             const int kr = t >> 1, d = t & 1;
             double g = 0.0, l = 0.0;
             for (int m = 0; m < N; ++m) {
@@ -330,28 +347,23 @@ __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) 
         }
     }
     if (s.nkJ > 0) {
-        double* lad = v.work;
-        const int LS = 2 * (s.m1J + 1 + s.m2J + 1), L2 = 2 * (s.m1J + 1);
-        __syncthreads();
-        for (int i = threadIdx.x; i < np; i += kThreads) {
-            const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
-            ladder(s.recip[0] * x + s.recip[1] * y, s.m1J, lad + i * LS);
-            ladder(s.recip[2] * x + s.recip[3] * y, s.m2J, lad + i * LS + L2);
-        }
-        __syncthreads();
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int i = warp; i < np; i += kWarps) {
+        const int m[2] = {s.m1J, s.m2J};
+        for (int i = 0; i < np; ++i) {
+            if (!kspace_of(s, i)) continue;
+            __syncthreads();
+            const double th[2] = {s.recip[0] * v.pos[i * 2] + s.recip[1] * v.pos[i * 2 + 1],
+                                  s.recip[2] * v.pos[i * 2] + s.recip[3] * v.pos[i * 2 + 1]};
+            ladders<NT>(th, m, 2, v.lad);
+            __syncthreads();
             const int gi = s.group_of[i];
             double acc[4] = {0, 0, 0, 0};
-            const double* l1 = lad + i * LS;
-            for (int k = lane; k < s.nkJ; k += 32) {
+            for (int k = threadIdx.x; k < s.nkJ; k += NT) {
                 double c, sn;
-                phase_k(s, l1, l1 + L2, k, c, sn);
+                phase_k(s, v.lad, v.lad + kLad, k, c, sn);
                 kspace_particle_k(s, v, i, gi, k, c, sn, acc);
             }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = warp_sum(acc[q]);
-            if (lane == 0) {
+            block_sum<NT>(acc, v.red);
+            if (threadIdx.x == 0) {
                 v.kg[i * 2] = acc[0];
                 v.kg[i * 2 + 1] = acc[1];
                 v.kl[i * 2] = acc[2];
@@ -370,6 +382,7 @@ __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) 
 // parts of ∇ln ψ and ∂² ln ψ of p at the proposal; in shared memory: the new
 // orbital row, the per-partner radial derivatives (rad) and geometry (geo),
 // and p's new phases (cn/sn).
+template <int NT>
 __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old) {
     const int np = s.np;
     const int b = block_of(s, p);
@@ -377,17 +390,20 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
     double acc[15];
 #pragma unroll
     for (int i = 0; i < 15; ++i) acc[i] = 0.0;
-    if (ks && threadIdx.x < (have_old ? 2 : 4)) {
-        const int q = threadIdx.x & 1;
-        const double* r = threadIdx.x < 2 ? v.newpos : v.pos + p * 2;
-        const double th = s.recip[q * 2] * r[0] + s.recip[q * 2 + 1] * r[1];
-        ladder(th, q == 0 ? s.m1J : s.m2J, v.misc + M_LAD + threadIdx.x * kLad);
+    if (ks) {
+        const double* r = v.pos + p * 2;
+        const double th[4] = {s.recip[0] * v.newpos[0] + s.recip[1] * v.newpos[1],
+                              s.recip[2] * v.newpos[0] + s.recip[3] * v.newpos[1],
+                              s.recip[0] * r[0] + s.recip[1] * r[1],
+                              s.recip[2] * r[0] + s.recip[3] * r[1]};
+        const int m[4] = {s.m1J, s.m2J, s.m1J, s.m2J};
+        ladders<NT>(th, m, have_old ? 2 : 4, v.lad);
     }
     if (b >= 0) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n, jrow = p - B.first;
         const double* A = v.scal - s.o_scal + B.oA;
-        for (int m = threadIdx.x; m < N; m += kThreads) {
+        for (int m = threadIdx.x; m < N; m += NT) {
             double val, g[3], l[3];
             orbital(s, B, m, v.newpos, val, g, l);
             v.nval[m] = val;
@@ -405,7 +421,7 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
             acc[5] += a * l[1];
         }
     }
-    for (int k = threadIdx.x; k < np; k += kThreads) {
+    for (int k = threadIdx.x; k < np; k += NT) {
         if (k == p) continue;
         bool any = false;
         for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
@@ -449,14 +465,14 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
         __syncthreads();
         const int nk = s.nkJ;
         const int gp = s.group_of[p];
-        for (int k = threadIdx.x; k < nk; k += kThreads) {
+        for (int k = threadIdx.x; k < nk; k += NT) {
             double c, sn, co, so;
-            phase_k(s, v.misc + M_LAD, v.misc + M_LAD + kLad, k, c, sn);
+            phase_k(s, v.lad, v.lad + kLad, k, c, sn);
             if (have_old) {
                 co = v.co[k];
                 so = v.so[k];
             } else {
-                phase_k(s, v.misc + M_LAD + 2 * kLad, v.misc + M_LAD + 3 * kLad, k, co, so);
+                phase_k(s, v.lad + 2 * kLad, v.lad + 3 * kLad, k, co, so);
                 v.co[k] = co;
                 v.so[k] = so;
             }
@@ -482,7 +498,7 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
             }
         }
     }
-    block_sum<15>(acc, v.red);
+    block_sum<NT>(acc, v.red);
     if (threadIdx.x == 0) {
         double logr = acc[6], phase = 0.0, sgx = 0.0, sgy = 0.0, slx = 0.0, sly = 0.0;
         if (b >= 0) {
@@ -517,9 +533,38 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
 
 // ───────────────────────── commit ───────────────────────────────────────
 
+template <int NT>
 __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p) {
     const int np = s.np;
     const int b = block_of(s, p);
+    // pair terms first (their scratch shares space with the rebuild's work
+    // matrix): partner gradients and Laplacians, eager as in the reference
+    for (int k = threadIdx.x; k < np; k += NT) {
+        if (k == p) continue;
+        bool any = false;
+        for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
+        if (!any) continue;
+        const double* geo = v.geo + k * 6;
+        const double* rad = v.rad + k * 4;
+        const double irn = 1.0 / geo[2], iro = 1.0 / geo[5];
+        for (int d = 0; d < 2; ++d) {
+            const double dor_old = -geo[3 + d] * iro, dor_new = -geo[d] * irn;
+            const double g_old = rad[0] * dor_old, g_new = rad[2] * dor_new;
+            v.jg[k * 2 + d] += g_new - g_old;
+            const double lap_old = rad[1] * dor_old * dor_old + rad[0] * iro * (1.0 - dor_old * dor_old);
+            const double lap_new = rad[3] * dor_new * dor_new + rad[2] * irn * (1.0 - dor_new * dor_new);
+            v.jl[k * 2 + d] += lap_new - lap_old;
+        }
+    }
+    // k-space: ρ of p's group follows the move; partners refresh on their next read
+    if (kspace_of(s, p)) {
+        const int nk = s.nkJ;
+        double* mr = v.rho + s.group_of[p] * 2 * nk;
+        for (int k = threadIdx.x; k < nk; k += NT) {
+            mr[k] += v.cn[k] - v.co[k];
+            mr[nk + k] += v.sn[k] - v.so[k];
+        }
+    }
     // Slater: Sherman-Morrison with the reference's rebuild triggers
     if (b >= 0) {
         const DevBlock& B = s.blocks[b];
@@ -531,7 +576,7 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         double* Dl = grec + B.oDl;
         double* rabs = v.scal - s.o_scal + B.orabs;
         const double R = v.misc[M_R];
-        for (int c = threadIdx.x; c < N; c += kThreads) {
+        for (int c = threadIdx.x; c < N; c += NT) {
             double prod = 0.0;
             for (int m = 0; m < N; ++m) prod += v.nval[m] * A[m * N + c];
             v.rowp[c] = prod - (c == jrow ? 1.0 : 0.0);
@@ -555,38 +600,38 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         const double old_log = bs[0];
         bool rebuild = v.misc[M_REBUILD] != 0.0;
         if (rebuild) {
-            gj_rebuild(s, v, grec, b);
+            gj_rebuild<NT>(s, v, grec, b);
         } else {
-            for (int e = threadIdx.x; e < N * N; e += kThreads) {
+            for (int e = threadIdx.x; e < N * N; e += NT) {
                 const int a = e / N, c = e - a * N;
                 A[e] = A[e] - v.col[a] * v.rowp[c];
             }
             __syncthreads();
         }
         double ra = 0.0, rdm = 0.0;
-        for (int a = threadIdx.x; a < N; a += kThreads) {
+        for (int a = threadIdx.x; a < N; a += NT) {
             double t = 0.0;
             for (int c = 0; c < N; ++c) t += fabs(A[a * N + c]);
             ra = fmax(ra, t);
             rdm = fmax(rdm, rabs[a]);
         }
-        const double norm_a = block_max(ra, v.red);
-        const double norm_d = block_max(rdm, v.red);
+        const double norm_a = block_max<NT>(ra, v.red);
+        const double norm_d = block_max<NT>(rdm, v.red);
         const double cond = norm_d * norm_a;
         if (!rebuild && (!isfinite(cond) || cond > 1e8)) {
-            gj_rebuild(s, v, grec, b);
+            gj_rebuild<NT>(s, v, grec, b);
             rebuild = true;
         }
         // the moved particle's determinant derivatives at the committed inverse
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int m = threadIdx.x; m < N; m += kThreads) {
+        for (int m = threadIdx.x; m < N; m += NT) {
             const double a = A[m * N + jrow];
             acc[0] += a * v.ngrad[m * 2 + 0];
             acc[1] += a * v.ngrad[m * 2 + 1];
             acc[2] += a * v.nlap[m * 2 + 0];
             acc[3] += a * v.nlap[m * 2 + 1];
         }
-        block_sum<4>(acc, v.red);
+        block_sum<NT>(acc, v.red);
         if (threadIdx.x == 0) {
             bs[2] = cond;
             if (rebuild) {
@@ -601,33 +646,6 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
             v.sg[p * 2 + 1] = acc[1];
             v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
             v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
-        }
-    }
-    // pair terms: partner gradients and Laplacians (eager, as the reference)
-    for (int k = threadIdx.x; k < np; k += kThreads) {
-        if (k == p) continue;
-        bool any = false;
-        for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
-        if (!any) continue;
-        const double* geo = v.geo + k * 6;
-        const double* rad = v.rad + k * 4;
-        const double irn = 1.0 / geo[2], iro = 1.0 / geo[5];
-        for (int d = 0; d < 2; ++d) {
-            const double dor_old = -geo[3 + d] * iro, dor_new = -geo[d] * irn;
-            const double g_old = rad[0] * dor_old, g_new = rad[2] * dor_new;
-            v.jg[k * 2 + d] += g_new - g_old;
-            const double lap_old = rad[1] * dor_old * dor_old + rad[0] * iro * (1.0 - dor_old * dor_old);
-            const double lap_new = rad[3] * dor_new * dor_new + rad[2] * irn * (1.0 - dor_new * dor_new);
-            v.jl[k * 2 + d] += lap_new - lap_old;
-        }
-    }
-    // k-space: ρ of p's group follows the move; partners refresh on their next read
-    if (kspace_of(s, p)) {
-        const int nk = s.nkJ;
-        double* mr = v.rho + s.group_of[p] * 2 * nk;
-        for (int k = threadIdx.x; k < nk; k += kThreads) {
-            mr[k] += v.cn[k] - v.co[k];
-            mr[nk + k] += v.sn[k] - v.so[k];
         }
     }
     if (threadIdx.x == 0) {
@@ -653,16 +671,18 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
 // ───────────────────────── local energy ─────────────────────────────────
 
 // E_L from refreshed derivatives: kinetic + Ewald (real, reciprocal,
-// constants) + open Coulomb.
+// constants) + open Coulomb.  Reciprocal ρ(k) accumulates particle by
+// particle in `work` (one slot per k, owned by one thread).
+template <int NT>
 __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs, int npair) {
     const int np = s.np;
     double acc[1] = {0.0};
-    for (int t = threadIdx.x; t < np * 2; t += kThreads) {
+    for (int t = threadIdx.x; t < np * 2; t += NT) {
         const double g = v.sg[t] + v.jg[t] + v.kg[t], l = v.sl[t] + v.jl[t] + v.kl[t];
         acc[0] += -0.5 * s.inv_mass[t] * (l + g * g);
     }
     if (s.ewald) {
-        for (int q = threadIdx.x; q < npair; q += kThreads) {
+        for (int q = threadIdx.x; q < npair; q += NT) {
             const int2 pq = pairs[q];
             const double coeff = s.charge[pq.x] * s.charge[pq.y];
             if (coeff == 0.0) continue;
@@ -670,36 +690,34 @@ __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs
             const double r = fold_dist(s, v.pos + pq.x * 2, v.pos + pq.y * 2, del);
             if (r < s.e_rcut) acc[0] += coeff * (s.e_inv_eps / r - spline1(s.esp, r));
         }
-        double* lad = v.work;
-        const int L1 = s.e_m1 + 1, L2 = s.e_m2 + 1;
-        __syncthreads();
-        for (int i = threadIdx.x; i < np; i += kThreads) {
-            const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
-            ladder(s.recip[0] * x + s.recip[1] * y, s.e_m1, lad + i * 2 * (L1 + L2));
-            ladder(s.recip[2] * x + s.recip[3] * y, s.e_m2, lad + i * 2 * (L1 + L2) + 2 * L1);
-        }
-        __syncthreads();
-        for (int k = threadIdx.x; k < s.enk; k += kThreads) {
-            const int n1 = s.en1[k], n2 = s.en2[k];
-            double rr = 0.0, ri = 0.0;
-            for (int i = 0; i < np; ++i) {
-                const double q = s.charge[i];
-                if (q == 0.0) continue;
+        double* rr = v.work;
+        double* ri = v.work + s.enk;
+        for (int k = threadIdx.x; k < s.enk; k += NT) rr[k] = ri[k] = 0.0;
+        const int m[2] = {s.e_m1, s.e_m2};
+        for (int i = 0; i < np; ++i) {
+            const double q = s.charge[i];
+            if (q == 0.0) continue;
+            __syncthreads();
+            const double th[2] = {s.recip[0] * v.pos[i * 2] + s.recip[1] * v.pos[i * 2 + 1],
+                                  s.recip[2] * v.pos[i * 2] + s.recip[3] * v.pos[i * 2 + 1]};
+            ladders<NT>(th, m, 2, v.lad);
+            __syncthreads();
+            for (int k = threadIdx.x; k < s.enk; k += NT) {
                 double ar, ai, br, bi;
-                ladder_pick(lad + i * 2 * (L1 + L2), n1, ar, ai);
-                ladder_pick(lad + i * 2 * (L1 + L2) + 2 * L1, n2, br, bi);
-                rr += q * (ar * br - ai * bi);
-                ri += q * (ar * bi + ai * br);
+                ladder_pick(v.lad, s.en1[k], ar, ai);
+                ladder_pick(v.lad + kLad, s.en2[k], br, bi);
+                rr[k] += q * (ar * br - ai * bi);
+                ri[k] += q * (ar * bi + ai * br);
             }
-            acc[0] += s.ew[k] * (rr * rr + ri * ri);
         }
+        for (int k = threadIdx.x; k < s.enk; k += NT) acc[0] += s.ew[k] * (rr[k] * rr[k] + ri[k] * ri[k]);
     }
     for (int c = 0; c < s.ncoul; ++c) {
         const int af = s.coul[c][0], al = s.coul[c][1], bf = s.coul[c][2], bl = s.coul[c][3];
         const bool same = af == bf && al == bl;
         const int na = al - af, nb = bl - bf;
         const int tot = same ? na * na : na * nb;
-        for (int q = threadIdx.x; q < tot; q += kThreads) {
+        for (int q = threadIdx.x; q < tot; q += NT) {
             const int i = af + q / (same ? na : nb), j = (same ? af : bf) + q % (same ? na : nb);
             if (same && j <= i) continue;
             double del[3];
@@ -707,23 +725,24 @@ __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs
             acc[0] += s.coul_coef[c] / r;
         }
     }
-    block_sum<1>(acc, v.red);
+    block_sum<NT>(acc, v.red);
     return acc[0] + (s.ewald ? s.e_const : 0.0);
 }
 
 // ───────────────────────── full evaluation ──────────────────────────────
 
+template <int NT>
 __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, const int2* pairs,
                                 int npair) {
     const int np = s.np;
     // wrap every position into the cell (WalkerSet::load_all)
-    for (int i = threadIdx.x; i < np; i += kThreads) {
+    for (int i = threadIdx.x; i < np; i += NT) {
         double r[3] = {v.pos[i * 2], v.pos[i * 2 + 1], 0.0};
         wrap_pos(s, r);
         v.pos[i * 2] = r[0];
         v.pos[i * 2 + 1] = r[1];
     }
-    for (int i = threadIdx.x; i < np * 2; i += kThreads)
+    for (int i = threadIdx.x; i < np * 2; i += NT)
         v.jg[i] = v.jl[i] = v.kg[i] = v.kl[i] = v.sg[i] = v.sl[i] = 0.0;
     if (threadIdx.x == 0) {
         v.scal[S_LOGPSI] = 0.0;
@@ -740,7 +759,7 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
         double* Dg = grec + B.oDg;
         double* Dl = grec + B.oDl;
         double* rabs = v.scal - s.o_scal + B.orabs;
-        for (int e = threadIdx.x; e < N * N; e += kThreads) {
+        for (int e = threadIdx.x; e < N * N; e += NT) {
             const int kr = e / N, m = e % N;
             double val, g[3], l[3];
             orbital(s, B, m, v.pos + (B.first + kr) * 2, val, g, l);
@@ -751,23 +770,22 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
             Dl[e * 2 + 1] = l[1];
         }
         __syncthreads();
-        for (int kr = threadIdx.x; kr < N; kr += kThreads) {
+        for (int kr = threadIdx.x; kr < N; kr += NT) {
             double sum = 0.0;
             for (int i = 0; i < N; ++i) sum += fabs(D[kr * N + i]);
             rabs[kr] = sum;
         }
-        __syncthreads();
-        gj_rebuild(s, v, grec, b);
+        gj_rebuild<NT>(s, v, grec, b);
         double* A = v.scal - s.o_scal + B.oA;
         double ra = 0.0, rdm = 0.0;
-        for (int a = threadIdx.x; a < N; a += kThreads) {
+        for (int a = threadIdx.x; a < N; a += NT) {
             double t = 0.0;
             for (int c = 0; c < N; ++c) t += fabs(A[a * N + c]);
             ra = fmax(ra, t);
             rdm = fmax(rdm, rabs[a]);
         }
-        const double na = block_max(ra, v.red);
-        const double nd = block_max(rdm, v.red);
+        const double na = block_max<NT>(ra, v.red);
+        const double nd = block_max<NT>(rdm, v.red);
         if (threadIdx.x == 0) {
             double* bs = v.scal + S_BLOCK0 + 3 * b;
             bs[0] = v.misc[M_LOGDET];
@@ -779,7 +797,7 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
         __syncthreads();
     }
     // pair terms: each thread owns particle i and sums over its partners
-    for (int i = threadIdx.x; i < np; i += kThreads) {
+    for (int i = threadIdx.x; i < np; i += NT) {
         double g[2] = {0.0, 0.0}, l[2] = {0.0, 0.0}, u_half = 0.0;
         for (int j = 0; j < np; ++j) {
             if (j == i) continue;
@@ -813,26 +831,21 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
     // image sums: ρ per group from every particle's phases, then Σ w T
     if (s.nkJ > 0) {
         const int nk = s.nkJ;
-        double* lad = v.work;
-        const int LS = 2 * (s.m1J + 1 + s.m2J + 1), L2 = 2 * (s.m1J + 1);
-        __syncthreads();
-        for (int i = threadIdx.x; i < np; i += kThreads) {
-            const double x = v.pos[i * 2], y = v.pos[i * 2 + 1];
-            ladder(s.recip[0] * x + s.recip[1] * y, s.m1J, lad + i * LS);
-            ladder(s.recip[2] * x + s.recip[3] * y, s.m2J, lad + i * LS + L2);
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < s.ngroups * nk; e += kThreads) {
-            const int g = e / nk, k = e % nk;
-            double re = 0.0, im = 0.0;
-            for (int i = s.gfirst[g]; i < s.glast[g]; ++i) {
+        for (int e = threadIdx.x; e < s.ngroups * 2 * nk; e += NT) v.rho[e] = 0.0;
+        const int m[2] = {s.m1J, s.m2J};
+        for (int i = 0; i < np; ++i) {
+            __syncthreads();
+            const double th[2] = {s.recip[0] * v.pos[i * 2] + s.recip[1] * v.pos[i * 2 + 1],
+                                  s.recip[2] * v.pos[i * 2] + s.recip[3] * v.pos[i * 2 + 1]};
+            ladders<NT>(th, m, 2, v.lad);
+            __syncthreads();
+            double* rg = v.rho + s.group_of[i] * 2 * nk;
+            for (int k = threadIdx.x; k < nk; k += NT) {
                 double c, sn;
-                phase_k(s, lad + i * LS, lad + i * LS + L2, k, c, sn);
-                re += c;
-                im += sn;
+                phase_k(s, v.lad, v.lad + kLad, k, c, sn);
+                rg[k] += c;
+                rg[nk + k] += sn;
             }
-            v.rho[g * 2 * nk + k] = re;
-            v.rho[g * 2 * nk + nk + k] = im;
         }
         __syncthreads();
         for (int t = 0; t < s.nterms; ++t) {
@@ -841,16 +854,17 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
             const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
             const double* ar = v.rho + ga * 2 * nk;
             const double* br = v.rho + gb * 2 * nk;
-            for (int k = threadIdx.x; k < nk; k += kThreads) {
+            for (int k = threadIdx.x; k < nk; k += NT) {
                 const double w = T.kw[k];
                 lp[0] += T.same0 ? w * (ar[k] * ar[k] + ar[nk + k] * ar[nk + k])
                                  : 2.0 * w * (ar[k] * br[k] + ar[nk + k] * br[nk + k]);
             }
         }
     }
-    block_sum<1>(lp, v.red);
-    refresh_all(s, v, grec);
-    const double el = local_energy(s, v, pairs, npair);
+    block_sum<NT>(lp, v.red);
+    __syncthreads();
+    refresh_all<NT>(s, v, grec);
+    const double el = local_energy<NT>(s, v, pairs, npair);
     if (threadIdx.x == 0) {
         v.scal[S_LOGPSI] = lp[0];
         v.scal[S_EL] = el;
@@ -862,40 +876,43 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
 
 // ───────────────────────── kernels ──────────────────────────────────────
 
-__global__ void __launch_bounds__(kThreads) evaluate_kernel(DevSys s, double* records, int nw,
-                                                            const int2* pairs, int npair) {
+template <int NT>
+__global__ void __launch_bounds__(NT) evaluate_kernel(DevSys s, double* records, int nw,
+                                                      const int2* pairs, int npair) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
     if (w >= nw) return;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot(s, rec, sm);
+    load_hot<NT>(s, rec, sm);
     const Smem v = view(s, sm);
-    evaluate_walker(s, v, rec, pairs, npair);
-    store_hot(s, rec, sm);
+    evaluate_walker<NT>(s, v, rec, pairs, npair);
+    store_hot<NT>(s, rec, sm);
 }
 
-__global__ void __launch_bounds__(kThreads) measure_kernel(DevSys s, double* records, int nw,
-                                                           const int2* pairs, int npair) {
+template <int NT>
+__global__ void __launch_bounds__(NT) measure_kernel(DevSys s, double* records, int nw,
+                                                     const int2* pairs, int npair) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
     if (w >= nw) return;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot(s, rec, sm);
+    load_hot<NT>(s, rec, sm);
     const Smem v = view(s, sm);
-    refresh_all(s, v, rec);
-    const double el = local_energy(s, v, pairs, npair);
+    refresh_all<NT>(s, v, rec);
+    const double el = local_energy<NT>(s, v, pairs, npair);
     if (threadIdx.x == 0) v.scal[S_EL] = el;
-    store_hot(s, rec, sm);
+    store_hot<NT>(s, rec, sm);
 }
 
-__global__ void __launch_bounds__(kThreads) move_kernel(DevSys s, double* records, int nw, int p,
-                                                        const double* new_pos,
-                                                        const uint8_t* accept, double* out) {
+template <int NT>
+__global__ void __launch_bounds__(NT) move_kernel(DevSys s, double* records, int nw, int p,
+                                                  const double* new_pos, const uint8_t* accept,
+                                                  double* out) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
     if (w >= nw) return;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot(s, rec, sm);
+    load_hot<NT>(s, rec, sm);
     const Smem v = view(s, sm);
     if (threadIdx.x == 0) {
         v.newpos[0] = new_pos[w];
@@ -903,7 +920,7 @@ __global__ void __launch_bounds__(kThreads) move_kernel(DevSys s, double* record
         v.misc[M_ERR] = 0.0;
     }
     __syncthreads();
-    ratio_step(s, v, p, false);
+    ratio_step<NT>(s, v, p, false);
     if (threadIdx.x == 0) {
         // log ratio, phase, new ∇ln ψ (dim), new ∂² ln ψ (dim), per walker
         out[0 * nw + w] = v.misc[M_LOGR];
@@ -913,21 +930,21 @@ __global__ void __launch_bounds__(kThreads) move_kernel(DevSys s, double* record
         out[4 * nw + w] = v.misc[M_SLX] + v.misc[M_JLX] + v.misc[M_KLX];
         out[5 * nw + w] = v.misc[M_SLY] + v.misc[M_JLY] + v.misc[M_KLY];
     }
-    if (accept != nullptr && accept[w] != 0) commit_step(s, v, rec, p);
-    store_hot(s, rec, sm);
+    if (accept != nullptr && accept[w] != 0) commit_step<NT>(s, v, rec, p);
+    store_hot<NT>(s, rec, sm);
 }
 
 // Fused sweep kernel.  mode 0: VMC step (n_sub sweeps, then refresh + E_L);
 // mode 1: DMC advance (per sweep: refresh + E_L + branch factor).
-__global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* records, int nw,
-                                                         const double* randoms, long stride,
-                                                         SweepParams prm, const int2* pairs,
-                                                         int npair) {
+template <int NT>
+__global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, int nw,
+                                                   const double* randoms, long stride,
+                                                   SweepParams prm, const int2* pairs, int npair) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
     if (w >= nw) return;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot(s, rec, sm);
+    load_hot<NT>(s, rec, sm);
     const Smem v = view(s, sm);
     const int np = s.np;
     const bool dmc = prm.mode == 1;
@@ -947,7 +964,7 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
     for (int sub = 0; sub < prm.n_sub; ++sub) {
         const double* rnd = randoms + static_cast<long>(sub) * np * 3 * stride;
         for (int p = 0; p < np; ++p) {
-            if (drift) refresh_particle(s, v, rec, p);
+            if (drift) refresh_particle<NT>(s, v, rec, p);
             if (threadIdx.x == 0) {
                 const double* g = rnd + static_cast<long>(p) * 3 * stride;
                 const double tm = prm.tau * s.inv_mass[p * 2];
@@ -974,7 +991,7 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
                 v.misc[M_GOY] = gy;
             }
             __syncthreads();
-            ratio_step(s, v, p, drift);
+            ratio_step<NT>(s, v, p, drift);
             if (threadIdx.x == 0) {
                 const double logr = v.misc[M_LOGR];
                 const double u = v.misc[M_U];
@@ -1018,11 +1035,11 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
                 if (acc) v.scal[S_NACC] += 1.0;
             }
             __syncthreads();
-            if (v.misc[M_ACCEPT] != 0.0) commit_step(s, v, rec, p);
+            if (v.misc[M_ACCEPT] != 0.0) commit_step<NT>(s, v, rec, p);
         }
         if (dmc || sub == prm.n_sub - 1) {
-            refresh_all(s, v, rec);
-            const double el = local_energy(s, v, pairs, npair);
+            refresh_all<NT>(s, v, rec);
+            const double el = local_energy<NT>(s, v, pairs, npair);
             if (threadIdx.x == 0) {
                 v.scal[S_EL] = el;
                 if (dmc) {
@@ -1045,8 +1062,60 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(DevSys s, double* recor
         if (dmc && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
         if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
     }
-    store_hot(s, rec, sm);
+    store_hot<NT>(s, rec, sm);
 }
+
+// ───────────────────────── launchers ────────────────────────────────────
+
+#define ALEA_LAUNCH(nt, KERNEL, grid, smem, st, ...)                                     \
+    do {                                                                                 \
+        if ((nt) == 32) KERNEL<32><<<(grid), 32, (smem), (st)>>>(__VA_ARGS__);           \
+        else if ((nt) == 64) KERNEL<64><<<(grid), 64, (smem), (st)>>>(__VA_ARGS__);      \
+        else KERNEL<128><<<(grid), 128, (smem), (st)>>>(__VA_ARGS__);                    \
+    } while (0)
+
+cudaError_t reserve_smem(size_t smem) {
+    const int b = static_cast<int>(smem);
+    const void* kernels[] = {
+        reinterpret_cast<const void*>(evaluate_kernel<32>), reinterpret_cast<const void*>(measure_kernel<32>),
+        reinterpret_cast<const void*>(move_kernel<32>), reinterpret_cast<const void*>(sweep_kernel<32>),
+        reinterpret_cast<const void*>(evaluate_kernel<64>), reinterpret_cast<const void*>(measure_kernel<64>),
+        reinterpret_cast<const void*>(move_kernel<64>), reinterpret_cast<const void*>(sweep_kernel<64>),
+        reinterpret_cast<const void*>(evaluate_kernel<128>), reinterpret_cast<const void*>(measure_kernel<128>),
+        reinterpret_cast<const void*>(move_kernel<128>), reinterpret_cast<const void*>(sweep_kernel<128>)};
+    for (const void* k : kernels) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                            double* records, const int2* pairs, int npair) {
+    ALEA_LAUNCH(nt, evaluate_kernel, nw, smem, st, s, records, nw, pairs, npair);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_measure(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                           double* records, const int2* pairs, int npair) {
+    ALEA_LAUNCH(nt, measure_kernel, nw, smem, st, s, records, nw, pairs, npair);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_move(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                        double* records, int p, const double* new_pos, const uint8_t* accept,
+                        double* out) {
+    ALEA_LAUNCH(nt, move_kernel, nw, smem, st, s, records, nw, p, new_pos, accept, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                         double* records, const double* randoms, long stride,
+                         const SweepParams& prm, const int2* pairs, int npair) {
+    ALEA_LAUNCH(nt, sweep_kernel, nw, smem, st, s, records, nw, randoms, stride, prm, pairs, npair);
+    return cudaGetLastError();
+}
+#undef ALEA_LAUNCH
 
 // One sweep's (or several sweeps') random numbers per stream: stream t fills
 // its crowd [w0, w1) of min(n_streams, nw) even splits in the reference's

@@ -17,12 +17,19 @@ struct SweepParams {
     double etrial, eref, e_cut, e_max;
 };
 
-__global__ void evaluate_kernel(DevSys s, double* records, int nw, const int2* pairs, int npair);
-__global__ void measure_kernel(DevSys s, double* records, int nw, const int2* pairs, int npair);
-__global__ void move_kernel(DevSys s, double* records, int nw, int p, const double* new_pos,
-                            const uint8_t* accept, double* out);
-__global__ void sweep_kernel(DevSys s, double* records, int nw, const double* randoms, long stride,
-                             SweepParams prm, const int2* pairs, int npair);
+// Walker kernels, one CTA of nt threads (32, 64 or 128) per walker and nw
+// CTAs; host-side launchers that dispatch on nt.
+cudaError_t reserve_smem(size_t smem);
+cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                            double* records, const int2* pairs, int npair);
+cudaError_t launch_measure(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                           double* records, const int2* pairs, int npair);
+cudaError_t launch_move(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                        double* records, int p, const double* new_pos, const uint8_t* accept,
+                        double* out);
+cudaError_t launch_sweep(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
+                         double* records, const double* randoms, long stride,
+                         const SweepParams& prm, const int2* pairs, int npair);
 __global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
                             int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
                             double zr, double* out, int crowd_mode);

@@ -1,0 +1,1056 @@
+// Host-side system setup: the tables the walker kernels read, computed once
+// before a run (the device never fits anything).  The equivalent of the
+// reference's builders for the systems this library runs:
+//
+//   cell             lattice from r_s and N (src/qmc/app.cpp:288-336)
+//   plane waves      closed reciprocal shells (src/wavefunction/orbital_set.h:575-665)
+//   cusps            Kato Γ = 2 μ R / (2ℓ + d − 1) (src/builders/jastrow.cpp:48-98)
+//   Ewald            optimized breakup of 1/r (src/numerics/ewald_breakup.cpp:205-276)
+//   Padé image sum   u − u∞ split by the same breakup with the Jastrow options
+//                    (src/wavefunction/periodic_pair_sum.cpp:21-60) and the tail
+//                    transform of the Padé (src/numerics/pair_radial.cpp)
+//   initial walkers  App::initialize_positions (src/qmc/app.cpp:56-112)
+//
+// The breakup is Natoli & Ceperley, J. Comput. Phys. 117, 171 (1995): a
+// locally piecewise quintic Hermite basis on [0, r_c] whose coefficients are
+// fitted, by Householder QR on the weighted rectangular system, so that the
+// long-range part's transform vanishes above k_cut (lattice shells up to
+// k_continuum, the 2-D density of states (A/2π) k dk beyond).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <functional>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/alea_gpu.h"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 2.0 * kPi;
+
+// ───────────────────────── special functions, quadrature ────────────────
+
+// J0: the standard library below x = 40, Hankel's asymptotic expansion
+// (Abramowitz & Stegun 9.2.5, four terms of P and Q) above.
+double bessel_j0(double x) {
+    if (x < 40.0) return std::cyl_bessel_j(0.0, x);
+    const double z = 1.0 / x, z2 = z * z;
+    // a_k from a_k = a_{k-1} (μ − (2k−1)²)/(8k) at μ = 0
+    double a[9];
+    a[0] = 1.0;
+    for (int k = 1; k < 9; ++k) a[k] = a[k - 1] * (0.0 - (2.0 * k - 1) * (2.0 * k - 1)) / (8.0 * k);
+    const double p = a[0] - a[2] * z2 + a[4] * z2 * z2 - a[6] * z2 * z2 * z2 + a[8] * z2 * z2 * z2 * z2;
+    const double q = z * (a[1] - a[3] * z2 + a[5] * z2 * z2 - a[7] * z2 * z2 * z2);
+    const double w = x - 0.25 * kPi;
+    return std::sqrt(2.0 / (kPi * x)) * (p * std::cos(w) - q * std::sin(w));
+}
+
+// 20-point Gauss-Legendre nodes and weights (the positive half).
+const double kGx[10] = {0.0765265211334973, 0.2277858511416451, 0.3737060887154195,
+                        0.5108670019508271, 0.6360536807265150, 0.7463319064601508,
+                        0.8391169718222188, 0.9122344282513259, 0.9639719272779138,
+                        0.9931285991850949};
+const double kGw[10] = {0.1527533871307258, 0.1491729864726037, 0.1420961093183820,
+                        0.1316886384491766, 0.1181945319615184, 0.1019301198172404,
+                        0.0832767415767048, 0.0626720483341091, 0.0406014298003869,
+                        0.0176140071391521};
+
+template <class F>
+double gauss20(F&& f, double a, double b) {
+    const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+    double s = 0.0;
+    for (int i = 0; i < 10; ++i) s += kGw[i] * (f(c + h * kGx[i]) + f(c - h * kGx[i]));
+    return s * h;
+}
+template <class F>
+double gauss20_panels(F&& f, double a, double b, int np) {
+    np = std::max(np, 1);
+    const double h = (b - a) / np;
+    double s = 0.0;
+    for (int i = 0; i < np; ++i) s += gauss20(f, a + i * h, a + (i + 1) * h);
+    return s;
+}
+// panels of about one radian of J0(kr)'s phase
+template <class F>
+double panel_integral(F&& f, double a, double b, double k) {
+    return gauss20_panels(f, a, b, std::clamp(1 + static_cast<int>(k * (b - a)), 1, 4000));
+}
+
+// ───────────────────────── LPQHI basis ──────────────────────────────────
+
+struct Lpqhi {
+    int n_knots = 0;
+    double rc = 0.0, delta = 0.0;
+    static constexpr double S[3][6] = {{1, 0, 0, -10, 15, -6}, {0, 1, 0, -6, 8, -3}, {0, 0, 0.5, -1.5, 1.5, -0.5}};
+    static constexpr double mirror[3] = {1, -1, 1};
+    Lpqhi() = default;
+    Lpqhi(int n, double r) : n_knots(n), rc(r), delta(r / (n - 1)) {}
+    int size() const { return 3 * n_knots; }
+    double lo(int n) const { return std::max(0.0, delta * (n / 3 - 1)); }
+    double hi(int n) const { return std::min(rc, delta * (n / 3 + 1)); }
+    double knot(int i) const { return delta * i; }
+    double h(int n, double r) const {
+        const int i = n / 3, a = n - 3 * i;
+        const double rb = delta * i;
+        if (r < delta * (i - 1) || r > hi(n)) return 0.0;
+        const bool left = r <= rb;
+        const double x = left ? (rb - r) / delta : (r - rb) / delta;
+        double p = 0.0;
+        for (int m = 5; m >= 0; --m) p = p * x + S[a][m];
+        const double s = std::pow(delta, a) * p;
+        return left ? mirror[a] * s : s;
+    }
+};
+
+// body(i) for i in [0, n) on the host's hardware threads (rows of the fit
+// are independent; each writes only its own outputs).
+template <class F>
+void parallel_for(size_t n, F&& body) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(hw, std::max<size_t>(1, n / 4));
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) body(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (size_t i; (i = next.fetch_add(1)) < n;) body(i);
+        });
+    for (auto& th : pool) th.join();
+}
+
+struct Radial {
+    std::function<double(double)> value, d1, d2, fourier, tail;
+};
+
+struct BreakupOptions {
+    int n_knots = 20;
+    double k_cut = 0.0, k_continuum = 0.0, k_max = 0.0;
+    int n_continuum = 400;
+};
+
+struct Breakup {
+    Lpqhi basis;
+    std::vector<double> coefs, kx, ky, weight, scaled;
+    std::vector<int> n1, n2;
+    double k_cut = 0.0, residual = 0.0, condition = 0.0, long_range_zero = 0.0, sr_k0 = 0.0;
+};
+
+double basis_transform(const Lpqhi& b, int n, double k) {
+    const int i = n / 3;
+    const double lo = b.lo(n), mid = b.knot(i), hi = b.hi(n);
+    auto f = [&](double r) { return r * bessel_j0(k * r) * b.h(n, r); };
+    double s = 0.0;
+    if (mid > lo) s += panel_integral(f, lo, mid, k);
+    if (hi > mid) s += panel_integral(f, mid, hi, k);
+    return kTwoPi * s;
+}
+
+// Σ over halving panels [b/2, b] from r_c down to 1e-14 r_c of ∫ g.
+template <class G>
+double halving(G&& g, double rc, double k) {
+    double s = 0.0, b = rc;
+    for (int j = 0; j < 60 && b > 1e-14 * rc; ++j) {
+        const double a = 0.5 * b;
+        s += panel_integral(g, a, b, k);
+        b = a;
+    }
+    return s;
+}
+
+// X(k) = −∫_{r > r_c} f e^{−ik·r} d²r
+double fit_target(const Radial& f, double rc, double k) {
+    if (f.tail) return -f.tail(k);
+    const double inner = halving([&](double r) { return r * bessel_j0(k * r) * f.value(r); }, rc, k);
+    return -f.fourier(k) + kTwoPi * inner;
+}
+
+Breakup build_breakup(const double* b, double area, double rc, const Radial& f, const BreakupOptions& opt) {
+    Breakup out;
+    out.basis = Lpqhi(opt.n_knots, rc);
+    const double b1x = b[0], b1y = b[1], b2x = b[2], b2y = b[3];
+    const double b_min = std::min(std::hypot(b1x, b1y), std::hypot(b2x, b2y));
+    const double k_cut = opt.k_cut > 0.0 ? opt.k_cut : 8.0 * b_min;
+    const double k_cont = opt.k_continuum > 0.0 ? opt.k_continuum : 60.0 * kPi / rc;
+    const double k_max = opt.k_max > 0.0 ? opt.k_max : 6000.0 / rc;
+    if (!(k_cut < k_cont && k_cont < k_max)) throw std::invalid_argument("breakup: need k_cut < k_continuum < k_max");
+    out.k_cut = k_cut;
+    // fit rows: exact shells up to k_continuum, then the continuum tail
+    std::vector<double> kf, kw;
+    {
+        const int nmax = static_cast<int>(std::ceil(k_cont / b_min)) + 1;
+        std::vector<double> raw;
+        for (int i = -nmax; i <= nmax; ++i)
+            for (int j = -nmax; j <= nmax; ++j) {
+                if (i == 0 && j == 0) continue;
+                const double k = std::hypot(i * b1x + j * b2x, i * b1y + j * b2y);
+                if (k > k_cut && k <= k_cont) raw.push_back(k);
+            }
+        std::sort(raw.begin(), raw.end());
+        for (size_t a = 0; a < raw.size();) {
+            size_t z = a;
+            while (z < raw.size() && raw[z] - raw[a] < 1e-9 * b_min) ++z;
+            kf.push_back(raw[a]);
+            kw.push_back(static_cast<double>(z - a));
+            a = z;
+        }
+        const double lo = std::log(k_cont), hi = std::log(k_max), dl = (hi - lo) / opt.n_continuum;
+        for (int i = 0; i < opt.n_continuum; ++i) {
+            const double k = std::exp(lo + (i + 0.5) * dl);
+            kf.push_back(k);
+            kw.push_back(area * k * (k * dl) / kTwoPi);
+        }
+    }
+    const int nb = out.basis.size(), nfree = nb - 3;
+    out.coefs.assign(nb, 0.0);
+    out.coefs[nb - 3] = f.value(rc);
+    out.coefs[nb - 2] = f.d1(rc);
+    out.coefs[nb - 1] = f.d2(rc);
+    const size_t nr = kf.size();
+    std::vector<double> cnk(nr * nb), target(nr);
+    parallel_for(nr, [&](size_t r) {
+        for (int n = 0; n < nb; ++n) cnk[r * nb + n] = basis_transform(out.basis, n, kf[r]);
+        double x = fit_target(f, rc, kf[r]);
+        for (int n = nfree; n < nb; ++n) x -= out.coefs[n] * cnk[r * nb + n];
+        target[r] = x;
+    });
+    // weighted least squares by Householder QR
+    std::vector<double> d(nr * nfree), y(nr), diag(nfree, 0.0);
+    for (size_t r = 0; r < nr; ++r) {
+        const double sw = std::sqrt(kw[r]);
+        for (int n = 0; n < nfree; ++n) d[r * nfree + n] = sw * cnk[r * nb + n];
+        y[r] = sw * target[r];
+    }
+    for (int j = 0; j < nfree; ++j) {
+        double norm2 = 0.0;
+        for (size_t r = j; r < nr; ++r) norm2 += d[r * nfree + j] * d[r * nfree + j];
+        const double norm = std::sqrt(norm2);
+        if (norm < 1e-300) continue;
+        const double head = d[static_cast<size_t>(j) * nfree + j];
+        const double alpha = head > 0.0 ? -norm : norm;
+        const double v0 = head - alpha;
+        const double vn2 = norm2 - head * head + v0 * v0;
+        if (vn2 < 1e-300) {
+            diag[j] = alpha;
+            continue;
+        }
+        d[static_cast<size_t>(j) * nfree + j] = v0;
+        for (int c = j + 1; c < nfree; ++c) {
+            double dot = 0.0;
+            for (size_t r = j; r < nr; ++r) dot += d[r * nfree + j] * d[r * nfree + c];
+            const double s = 2.0 * dot / vn2;
+            for (size_t r = j; r < nr; ++r) d[r * nfree + c] -= s * d[r * nfree + j];
+        }
+        double dot = 0.0;
+        for (size_t r = j; r < nr; ++r) dot += d[r * nfree + j] * y[r];
+        const double s = 2.0 * dot / vn2;
+        for (size_t r = j; r < nr; ++r) y[r] -= s * d[r * nfree + j];
+        diag[j] = alpha;
+    }
+    for (int i = nfree - 1; i >= 0; --i) {
+        double s = y[i];
+        for (int j = i + 1; j < nfree; ++j) s -= d[static_cast<size_t>(i) * nfree + j] * out.coefs[j];
+        out.coefs[i] = std::abs(diag[i]) > 1e-300 ? s / diag[i] : 0.0;
+    }
+    {
+        double hi = 0.0, lo = 1e300;
+        for (int i = 0; i < nfree; ++i) {
+            const double a = std::abs(diag[i]);
+            hi = std::max(hi, a);
+            if (a > 1e-300) lo = std::min(lo, a);
+        }
+        out.condition = lo < 1e299 ? hi / lo : 0.0;
+    }
+    out.scaled.resize(nb);
+    for (int n = 0; n < nb; ++n) out.scaled[n] = out.coefs[n] * std::pow(out.basis.delta, n % 3);
+    out.long_range_zero = out.coefs[0];
+    {
+        double integral = kTwoPi * halving([&](double r) { return r * f.value(r); }, rc, 0.0);
+        for (int n = 0; n < nb; ++n) integral -= out.coefs[n] * basis_transform(out.basis, n, 0.0);
+        out.sr_k0 = integral / area;
+    }
+    for (size_t r = 0; r < nr; ++r) {
+        if (kf[r] > k_cont) continue;
+        double resid = target[r];
+        for (int n = 0; n < nfree; ++n) resid -= out.coefs[n] * cnk[r * nb + n];
+        out.residual = std::max(out.residual, std::abs(resid));
+    }
+    // retained half-space vectors and weights f̃_long(k)/A
+    const int nmax = static_cast<int>(std::ceil(k_cut / b_min)) + 1;
+    for (int i = -nmax; i <= nmax; ++i)
+        for (int j = -nmax; j <= nmax; ++j) {
+            if (i < 0 || (i == 0 && j <= 0)) continue;
+            const double kx = i * b1x + j * b2x, ky = i * b1y + j * b2y;
+            const double k = std::hypot(kx, ky);
+            if (k > k_cut || k == 0.0) continue;
+            double fs = 0.0;
+            for (int n = 0; n < nb; ++n) fs += out.coefs[n] * basis_transform(out.basis, n, k);
+            out.kx.push_back(kx);
+            out.ky.push_back(ky);
+            out.weight.push_back((-fit_target(f, rc, k) + fs) / area);
+            out.n1.push_back(i);
+            out.n2.push_back(j);
+        }
+    return out;
+}
+
+// ───────────────────────── Padé radial function ─────────────────────────
+
+// u = P/Q, P = Σ a_k r^k, Q = 1 + Σ b_k r^k, with u' and u''.
+struct Rational {
+    std::vector<double> a, b;
+    void eval(double r, double& u, double& du, double& d2u) const {
+        double p = 0, dp = 0, d2p = 0, q = 1, dq = 0, d2q = 0;
+        for (size_t i = 0; i < a.size(); ++i) {
+            const double k = static_cast<double>(i + 1);
+            p += a[i] * std::pow(r, k);
+            dp += k * a[i] * std::pow(r, k - 1);
+            if (i >= 1) d2p += k * (k - 1) * a[i] * std::pow(r, k - 2);
+        }
+        for (size_t i = 0; i < b.size(); ++i) {
+            const double k = static_cast<double>(i + 1);
+            q += b[i] * std::pow(r, k);
+            dq += k * b[i] * std::pow(r, k - 1);
+            if (i >= 1) d2q += k * (k - 1) * b[i] * std::pow(r, k - 2);
+        }
+        u = p / q;
+        du = (dp - u * dq) / q;
+        d2u = (d2p - 2.0 * du * dq - u * d2q) / q;
+    }
+};
+
+// u(1/x) = A(x)/B(x) as the power series Σ e_j x^j (N ≤ M).
+std::vector<double> large_r_series(const Rational& f, int n) {
+    const size_t M = f.b.size();
+    std::vector<double> A(M + 1, 0.0), B(M + 1, 0.0), e(n, 0.0);
+    for (size_t k = 1; k <= f.a.size(); ++k) A[M - k] += f.a[k - 1];
+    B[M] = 1.0;
+    for (size_t k = 1; k <= M; ++k) B[M - k] += f.b[k - 1];
+    for (int j = 0; j < n; ++j) {
+        double s = j <= static_cast<int>(M) ? A[j] : 0.0;
+        for (int i = 1; i <= j && i <= static_cast<int>(M); ++i) s -= B[i] * e[j - i];
+        e[j] = s / B[0];
+    }
+    return e;
+}
+
+// Largest |root| of 1 + Σ b_k r^k (Durand-Kerner on the monic form).
+double pole_radius(const std::vector<double>& b) {
+    const size_t M = b.size();
+    if (M == 0) return 0.0;
+    std::vector<double> c(M);
+    c[0] = 1.0 / b.back();
+    for (size_t j = 1; j < M; ++j) c[j] = b[j - 1] / b.back();
+    std::vector<std::complex<double>> z(M);
+    for (size_t i = 0; i < M; ++i) z[i] = std::pow(std::complex<double>(0.4, 0.9), static_cast<double>(i));
+    for (int it = 0; it < 500; ++it) {
+        double change = 0.0;
+        for (size_t i = 0; i < M; ++i) {
+            std::complex<double> p = 1.0;
+            for (size_t j = M; j-- > 0;) p = p * z[i] + c[j];
+            std::complex<double> den = 1.0;
+            for (size_t l = 0; l < M; ++l)
+                if (l != i) den *= z[i] - z[l];
+            const std::complex<double> dz = p / den;
+            z[i] -= dz;
+            change = std::max(change, std::abs(dz));
+        }
+        if (change < 1e-14) break;
+    }
+    double r = 0.0;
+    for (const auto& zi : z) r = std::max(r, std::abs(zi));
+    return r;
+}
+
+double smooth_window(double r, double lo, double hi) {
+    if (r <= lo) return 1.0;
+    if (r >= hi) return 0.0;
+    const double t = (r - lo) / (hi - lo);
+    const double p = std::exp(-1.0 / (1.0 - t)), q = std::exp(-1.0 / t);
+    return p / (p + q);
+}
+
+// f = u − u∞ for the breakup, with tail(k) = 2π ∫_{r_c}^∞ r J0(kr) f dr from
+// an analytic large-r model (Σ_n d_n (r² + s²)^{−n/2}, whose 2-D Hankel
+// transforms are Bessel K functions, Gradshteyn & Ryzhik 6.565.4) plus the
+// numerically integrated remainder.
+Radial pade_radial(std::vector<double> a, std::vector<double> b, double rc, double& u_inf) {
+    while (!a.empty() && a.back() == 0.0) a.pop_back();
+    while (!b.empty() && b.back() == 0.0) b.pop_back();
+    if (a.size() > b.size())
+        throw std::invalid_argument("padé: numerator of higher order than the denominator has no image sum");
+    for (int i = 0; i <= 4000; ++i) {
+        const double r = 1e-6 * std::pow(1e14, i / 4000.0);
+        double q = 1.0;
+        for (size_t k = 0; k < b.size(); ++k) q += b[k] * std::pow(r, static_cast<double>(k + 1));
+        if (q <= 0.0) throw std::invalid_argument("padé: the denominator vanishes at some r > 0");
+    }
+    auto f = std::make_shared<const Rational>(Rational{a, b});
+    constexpr int kTerms = 16;
+    const std::vector<double> e = large_r_series(*f, kTerms + 1);
+    u_inf = e[0];
+    const double uinf = u_inf;
+    Radial out;
+    out.value = [f, uinf](double r) { double u, d1, d2; f->eval(r, u, d1, d2); return u - uinf; };
+    out.d1 = [f](double r) { double u, d1, d2; f->eval(r, u, d1, d2); return d1; };
+    out.d2 = [f](double r) { double u, d1, d2; f->eval(r, u, d1, d2); return d2; };
+    const double s = std::max(0.5 * rc, 2.0 * pole_radius(b));
+    std::vector<double> d(kTerms + 1, 0.0);
+    for (int m = 1; m <= kTerms; ++m) {
+        double v = e[m];
+        for (int n = m - 2; n >= 1; n -= 2) {
+            const int i = (m - n) / 2;
+            double c = 1.0;   // binomial C(−n/2, i)
+            for (int t = 0; t < i; ++t) c *= (-0.5 * n - t) / (t + 1);
+            v -= d[n] * c * std::pow(s, m - n);
+        }
+        d[m] = v;
+    }
+    auto model = [d, s](double r) {
+        const double w = 1.0 / std::sqrt(r * r + s * s);
+        double acc = 0.0;
+        for (int n = kTerms; n >= 1; --n) acc = w * (d[n] + acc);
+        return acc;
+    };
+    auto remainder = [f, uinf, model](double r) {
+        double u, d1, d2;
+        f->eval(r, u, d1, d2);
+        return u - uinf - model(r);
+    };
+    const double scale = std::max(std::abs(out.value(rc)) * rc * rc, 1e-300);
+    const double far = 64.0 * std::max(rc, s);
+    double R = 2.0 * rc;
+    while (R < far && std::abs(remainder(R)) * R * R > 1e-12 * scale) R *= 1.2;
+    out.tail = [d, s, model, remainder, rc, R](double k) {
+        const double ks = k * s;
+        double total = 0.0;
+        for (int n = 1; n <= kTerms; ++n) {
+            if (d[n] == 0.0) continue;
+            const double mu = 0.5 * n - 1.0;
+            total += d[n] * std::pow(k / s, mu) * std::cyl_bessel_k(std::abs(mu), ks) /
+                     (std::pow(2.0, mu) * std::tgamma(mu + 1.0));
+        }
+        const int n_in = 1 + static_cast<int>(k * rc + 4.0 * rc / s);
+        total -= gauss20_panels([&](double r) { return r * bessel_j0(k * r) * model(r); }, 0.0, rc, n_in);
+        total += gauss20_panels(
+            [&](double r) { return r * bessel_j0(k * r) * remainder(r) * smooth_window(r, rc, 2.0 * rc); },
+            rc, 2.0 * rc, 40 + static_cast<int>(k * rc));
+        if (k * rc < 100.0)
+            total += gauss20_panels(
+                [&](double r) {
+                    return r * bessel_j0(k * r) * remainder(r) * (1.0 - smooth_window(r, rc, 2.0 * rc));
+                },
+                rc, R, 40 + static_cast<int>(k * (R - rc) + 8.0 * (R - rc) / rc));
+        return kTwoPi * total;
+    };
+    return out;
+}
+
+// ───────────────────────── cell, shells ─────────────────────────────────
+
+struct Cell {
+    double a[4] = {0, 0, 0, 0};   // reduced rows
+    double b[4] = {0, 0, 0, 0};   // reciprocal, b_i · a_j = 2π δ_ij
+    double area = 0.0, ws = 0.0;
+};
+
+Cell make_cell(double lx, double ly) {
+    Cell c;
+    c.a[0] = lx;
+    c.a[3] = ly;
+    const double det = lx * ly;
+    c.area = std::abs(det);
+    const double inv = 1.0 / det;
+    const double ainv[4] = {c.a[3] * inv, -c.a[2] * inv, -c.a[1] * inv, c.a[0] * inv};
+    for (int k = 0; k < 4; ++k) c.b[k] = kTwoPi * ainv[k];
+    double shortest2 = 0.0;
+    for (int n0 = -2; n0 <= 2; ++n0)
+        for (int n1 = -2; n1 <= 2; ++n1) {
+            if (n0 == 0 && n1 == 0) continue;
+            const double x = n0 * c.a[0] + n1 * c.a[2], y = n0 * c.a[1] + n1 * c.a[3];
+            const double r2 = x * x + y * y;
+            if (shortest2 == 0.0 || r2 < shortest2) shortest2 = r2;
+        }
+    c.ws = 0.5 * std::sqrt(shortest2);
+    return c;
+}
+
+// The first `want` real plane waves of closed reciprocal shells (k = 0 gives
+// one cosine, every ±k pair a cosine and a sine).
+void plane_wave_shells(const Cell& c, int want, std::vector<double>& k, std::vector<int>& is_sin) {
+    const double* b = c.b;
+    const double area = std::abs(b[0] * b[3] - b[1] * b[2]);
+    const double h_min = area / std::max(std::hypot(b[0], b[1]), std::hypot(b[2], b[3]));
+    struct Kv { double k2, x, y; };
+    std::vector<int> closed;
+    for (int M = 4; M <= 4096; M *= 2) {
+        const double r2 = (M * h_min) * (M * h_min) * (1.0 + 1e-12);
+        std::vector<Kv> kv;
+        for (int i = -M; i <= M; ++i)
+            for (int j = -M; j <= M; ++j) {
+                Kv e{0, i * b[0] + j * b[2], i * b[1] + j * b[3]};
+                e.k2 = e.x * e.x + e.y * e.y;
+                if (e.k2 <= r2) kv.push_back(e);
+            }
+        std::sort(kv.begin(), kv.end(), [](const Kv& p, const Kv& q) {
+            if (p.k2 != q.k2) return p.k2 < q.k2;
+            if (p.x != q.x) return p.x < q.x;
+            return p.y < q.y;
+        });
+        k.clear();
+        is_sin.clear();
+        closed.clear();
+        size_t s = 0;
+        while (s < kv.size()) {
+            size_t e = s + 1;
+            while (e < kv.size() && std::abs(kv[e].k2 - kv[s].k2) <= 1e-9 * (1.0 + kv[s].k2)) ++e;
+            if (kv[s].k2 <= 1e-12 * (1.0 + kv[s].k2)) {
+                k.push_back(0.0);
+                k.push_back(0.0);
+                is_sin.push_back(0);
+            } else {
+                for (size_t q = s; q < e; ++q) {
+                    const bool positive = kv[q].x > 1e-12 || (!(kv[q].x < -1e-12) && kv[q].y > 1e-12);
+                    if (!positive) continue;
+                    for (int which = 0; which < 2; ++which) {
+                        k.push_back(kv[q].x);
+                        k.push_back(kv[q].y);
+                        is_sin.push_back(which);
+                    }
+                }
+            }
+            closed.push_back(static_cast<int>(is_sin.size()));
+            s = e;
+        }
+        if (static_cast<int>(is_sin.size()) >= want) break;
+    }
+    if (std::find(closed.begin(), closed.end(), want) == closed.end())
+        throw std::invalid_argument("plane waves: " + std::to_string(want) +
+                                    " orbitals leave a reciprocal shell partly filled");
+    k.resize(2 * static_cast<size_t>(want));
+    is_sin.resize(want);
+}
+
+// ───────────────────────── JSON ─────────────────────────────────────────
+
+struct Json {
+    std::string s;
+    bool first = true;
+    void sep() {
+        if (!first) s += ",";
+        first = false;
+    }
+    void key(const std::string& k) {
+        sep();
+        s += "\"" + k + "\":";
+        first = true;
+    }
+    void num(double x) {
+        sep();
+        char b[40];
+        std::snprintf(b, sizeof b, "%.17g", x);
+        s += b;
+    }
+    void open(char c) {
+        sep();
+        s += c;
+        first = true;
+    }
+    void close(char c) {
+        s += c;
+        first = false;
+    }
+    template <class V>
+    void arr(const std::string& k, const V& v) {
+        if (!k.empty()) key(k);
+        open('[');
+        for (auto x : v) num(static_cast<double>(x));
+        close(']');
+    }
+    void kv(const std::string& k, double x) {
+        key(k);
+        num(x);
+    }
+    void ks(const std::string& k, const std::string& x) {
+        key(k);
+        sep();
+        s += "\"" + x + "\"";
+    }
+};
+
+}  // namespace
+
+// ───────────────────────── setup object ─────────────────────────────────
+
+struct alea_gpu_setup {
+    alea_gpu_system sys{};
+    std::string json;
+    std::string err;
+    // owned tables
+    std::vector<std::vector<double>> dv;
+    std::vector<std::vector<int>> iv;
+    std::vector<double> anchors;   // [np*2] crystal sites (empty: uniform)
+    double jitter = 0.0;
+    double open_L = 1.0;
+    const double* keep(std::vector<double> v) {
+        dv.push_back(std::move(v));
+        return dv.back().data();
+    }
+    const int* keepi(std::vector<int> v) {
+        iv.push_back(std::move(v));
+        return iv.back().data();
+    }
+};
+
+namespace {
+
+void set_spline(alea_gpu_setup* S, alea_gpu_spline& sp, const Breakup& br) {
+    sp.r_cut = br.basis.rc;
+    sp.inv_delta = 1.0 / br.basis.delta;
+    sp.n_knots = br.basis.n_knots;
+    sp.scaled = S->keep(br.scaled);
+}
+void set_kset(alea_gpu_setup* S, alea_gpu_kset& ks, const Breakup& br) {
+    ks.n_k = static_cast<int>(br.weight.size());
+    ks.n1 = S->keepi(br.n1);
+    ks.n2 = S->keepi(br.n2);
+    ks.kx = S->keep(br.kx);
+    ks.ky = S->keep(br.ky);
+    ks.weight = S->keep(br.weight);
+}
+
+// Coulomb 1/(ε r) Ewald tables (n_knots auto-tuned, default k set).
+Breakup ewald_breakup(const Cell& c, double tol) {
+    Radial f;
+    f.value = [](double r) { return 1.0 / r; };
+    f.fourier = [](double k) { return kTwoPi / k; };
+    f.d1 = [](double r) { return -1.0 / (r * r); };
+    f.d2 = [](double r) { return 2.0 / (r * r * r); };
+    Breakup br;
+    for (int nk : {12, 16, 20, 24}) {
+        BreakupOptions opt;
+        opt.n_knots = nk;
+        br = build_breakup(c.b, c.area, c.ws, f, opt);
+        if (br.residual < tol) return br;
+    }
+    throw std::runtime_error("ewald: the breakup did not reach the requested tolerance");
+}
+
+// Image-summed Padé tables (the Jastrow breakup options).
+Breakup pade_breakup(const Cell& c, const std::vector<double>& a, const std::vector<double>& b,
+                     double& u_inf) {
+    const Radial f = pade_radial(a, b, c.ws, u_inf);
+    BreakupOptions opt;
+    opt.k_continuum = 20.0 * kPi / c.ws;
+    opt.k_max = 300.0 / c.ws;
+    opt.n_continuum = 150;
+    opt.k_cut = 5.0 * std::min(std::hypot(c.b[0], c.b[1]), std::hypot(c.b[2], c.b[3]));
+    return build_breakup(c.b, c.area, c.ws, f, opt);
+}
+
+void json_spline(Json& j, const std::string& k, const alea_gpu_spline& sp) {
+    j.key(k);
+    j.open('{');
+    j.kv("r_cut", sp.r_cut);
+    j.kv("inv_delta", sp.inv_delta);
+    j.kv("n_knots", sp.n_knots);
+    j.arr("scaled", std::vector<double>(sp.scaled, sp.scaled + 3 * sp.n_knots));
+    j.close('}');
+}
+void json_kset(Json& j, const alea_gpu_kset& ks) {
+    j.arr("n1", std::vector<int>(ks.n1, ks.n1 + ks.n_k));
+    j.arr("n2", std::vector<int>(ks.n2, ks.n2 + ks.n_k));
+    j.arr("kx", std::vector<double>(ks.kx, ks.kx + ks.n_k));
+    j.arr("ky", std::vector<double>(ks.ky, ks.ky + ks.n_k));
+    j.arr("weight", std::vector<double>(ks.weight, ks.weight + ks.n_k));
+}
+
+// The system description as JSON (the schema alea_b200.pack_system reads).
+void write_json(alea_gpu_setup* S, const std::string& kind, double ewald_self, double ewald_bg) {
+    const alea_gpu_system& y = S->sys;
+    Json j;
+    j.open('{');
+    j.ks("kind", kind);
+    j.kv("dim", y.dim);
+    j.kv("np", y.n_particles);
+    j.key("cell");
+    j.open('{');
+    j.kv("periodic", y.periodic);
+    j.kv("dim", y.dim);
+    if (y.periodic) j.arr("vectors", std::vector<double>(y.lattice, y.lattice + 4));
+    j.close('}');
+    j.key("groups");
+    j.open('[');
+    for (int g = 0; g < y.n_groups; ++g) {
+        j.open('{');
+        j.kv("first", y.groups[g].first);
+        j.kv("last", y.groups[g].last);
+        j.kv("charge", y.groups[g].charge);
+        j.arr("inv_mass", std::vector<double>(y.groups[g].inv_mass, y.groups[g].inv_mass + 2));
+        j.close('}');
+    }
+    j.close(']');
+    j.key("slater");
+    j.open('[');
+    for (int b = 0; b < y.n_blocks; ++b) {
+        const alea_gpu_orbitals& B = y.blocks[b];
+        const int n = B.last - B.first;
+        j.open('{');
+        j.kv("first", B.first);
+        j.kv("last", B.last);
+        if (B.type == ALEA_ORB_PLANE_WAVE) {
+            j.ks("type", "plane_wave");
+            j.arr("k", std::vector<double>(B.k, B.k + 2 * n));
+            j.arr("is_sin", std::vector<int>(B.is_sin, B.is_sin + n));
+        } else {
+            j.ks("type", "gaussian");
+            j.arr("centers", std::vector<double>(B.centers, B.centers + 2 * n));
+            j.arr("alphas", std::vector<double>(B.alphas, B.alphas + n));
+        }
+        j.close('}');
+    }
+    j.close(']');
+    j.key("pade");
+    j.open('[');
+    for (int t = 0; t < y.n_terms; ++t) {
+        const alea_gpu_pair_term& T = y.terms[t];
+        if (T.kind != ALEA_PAIR_PADE) continue;
+        j.open('{');
+        j.arr("ga", std::vector<int>{T.pairs[0][0], T.pairs[0][1]});
+        j.arr("gb", std::vector<int>{T.pairs[0][2], T.pairs[0][3]});
+        j.arr("a", std::vector<double>(T.coeffs, T.coeffs + T.num_order));
+        j.arr("b", std::vector<double>(T.coeffs + T.num_order, T.coeffs + T.num_order + T.den_order));
+        if (T.image_sum) {
+            j.key("image_sum");
+            j.open('{');
+            json_spline(j, "spline", T.short_range);
+            j.kv("u_inf", T.u_inf);
+            json_kset(j, T.kset);
+            j.close('}');
+        }
+        j.close('}');
+    }
+    j.close(']');
+    j.key("drummond");
+    j.open('[');
+    for (int t = 0; t < y.n_terms; ++t) {
+        const alea_gpu_pair_term& T = y.terms[t];
+        if (T.kind != ALEA_PAIR_DRUMMOND) continue;
+        j.open('{');
+        j.kv("C", T.C);
+        j.kv("gamma", T.gamma);
+        j.kv("L", T.L);
+        j.arr("coeffs", std::vector<double>(T.dcoeffs, T.dcoeffs + T.n_coeffs));
+        j.key("pairs");
+        j.open('[');
+        for (int q = 0; q < T.n_pairs; ++q)
+            j.arr("", std::vector<int>{T.pairs[q][0], T.pairs[q][1], T.pairs[q][2], T.pairs[q][3]});
+        j.close(']');
+        j.close('}');
+    }
+    j.close(']');
+    if (y.ewald.enabled) {
+        j.key("ewald");
+        j.open('{');
+        j.kv("r_cut", y.ewald.r_cut);
+        json_spline(j, "spline", y.ewald.long_range);
+        json_kset(j, y.ewald.kset);
+        j.kv("inv_eps", y.ewald.inv_eps);
+        j.kv("self_energy", ewald_self);
+        j.kv("background_energy", ewald_bg);
+        j.close('}');
+    }
+    j.key("coulomb");
+    j.open('[');
+    for (int cidx = 0; cidx < y.n_coulomb; ++cidx) {
+        const alea_gpu_coulomb& C = y.coulomb[cidx];
+        j.open('{');
+        j.arr("ga", std::vector<int>{C.a_first, C.a_last});
+        j.arr("gb", std::vector<int>{C.b_first, C.b_last});
+        j.kv("coef", C.coef);
+        j.close('}');
+    }
+    j.close(']');
+    if (!S->anchors.empty()) {
+        j.arr("anchors", S->anchors);
+        j.kv("jitter", S->jitter);
+    }
+    j.close('}');
+    S->json = j.s;
+}
+
+void add_group(alea_gpu_system& y, int first, int n, double charge) {
+    alea_gpu_group& g = y.groups[y.n_groups++];
+    g.first = first;
+    g.last = first + n;
+    g.charge = charge;
+    g.inv_mass[0] = g.inv_mass[1] = 1.0;
+    g.inv_mass[2] = 0.0;
+}
+
+// Ewald tables into the system; returns (self, background) energies.
+void add_ewald(alea_gpu_setup* S, const Cell& c, double tol, double& self, double& bg) {
+    alea_gpu_system& y = S->sys;
+    const Breakup br = ewald_breakup(c, tol);
+    y.ewald.enabled = 1;
+    y.ewald.r_cut = c.ws;
+    y.ewald.inv_eps = 1.0;
+    set_spline(S, y.ewald.long_range, br);
+    set_kset(S, y.ewald.kset, br);
+    double q2 = 0.0, Q = 0.0;
+    for (int g = 0; g < y.n_groups; ++g) {
+        const int n = y.groups[g].last - y.groups[g].first;
+        q2 += y.groups[g].charge * y.groups[g].charge * n;
+        Q += y.groups[g].charge * n;
+    }
+    self = -0.5 * br.long_range_zero * q2;
+    bg = -0.5 * Q * Q * br.sr_k0;
+    y.ewald.constant = self + bg;
+}
+
+}  // namespace
+
+extern "C" {
+
+const alea_gpu_system* alea_gpu_setup_system(const alea_gpu_setup* s) { return s ? &s->sys : nullptr; }
+const char* alea_gpu_setup_json(const alea_gpu_setup* s) { return s ? s->json.c_str() : ""; }
+void alea_gpu_setup_free(alea_gpu_setup* s) { delete s; }
+
+// 2-D homogeneous electron gas in a square cell of area N π r_s², plane-wave
+// determinants per spin, image-summed Padé u = a₁ r/(1 + b r) on every spin
+// pair (a₁ from the Kato cusp, or `pade_a` when positive for the opposite
+// spins and half of it for equal spins), Ewald Coulomb.
+int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pade_a,
+                         double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len) {
+    if (!out) return ALEA_ERR_INVALID;
+    *out = nullptr;
+    auto* S = new alea_gpu_setup();
+    try {
+        if (n_up < 1 || n_down < 0 || !(rs > 0.0)) throw std::invalid_argument("heg2d: bad sizes");
+        alea_gpu_system& y = S->sys;
+        const int np = n_up + n_down;
+        y.dim = 2;
+        y.n_particles = np;
+        y.periodic = 1;
+        const double L = std::sqrt(np * kPi * rs * rs);
+        const Cell c = make_cell(L, L);
+        std::copy(c.a, c.a + 4, y.lattice);
+        add_group(y, 0, n_up, -1.0);
+        if (n_down > 0) add_group(y, n_up, n_down, -1.0);
+        for (int g = 0; g < y.n_groups; ++g) {
+            std::vector<double> k;
+            std::vector<int> is_sin;
+            plane_wave_shells(c, y.groups[g].last - y.groups[g].first, k, is_sin);
+            alea_gpu_orbitals& B = y.blocks[y.n_blocks++];
+            B.first = y.groups[g].first;
+            B.last = y.groups[g].last;
+            B.type = ALEA_ORB_PLANE_WAVE;
+            B.k = S->keep(k);
+            B.is_sin = S->keepi(is_sin);
+        }
+        double self = 0.0, bg = 0.0;
+        add_ewald(S, c, ewald_tol > 0.0 ? ewald_tol : 1e-6, self, bg);
+        for (int ga = 0; ga < y.n_groups; ++ga)
+            for (int gb = ga; gb < y.n_groups; ++gb) {
+                const alea_gpu_group& A = y.groups[ga];
+                const alea_gpu_group& B = y.groups[gb];
+                if (ga == gb && A.last - A.first < 2) continue;
+                const int ell = ga == gb ? 1 : 0;
+                const double R = A.charge * B.charge;   // q_a q_b / ε
+                double a1 = 2.0 * 0.5 * R / (2 * ell + 2 - 1);
+                if (pade_a > 0.0) a1 = ga == gb ? 0.5 * pade_a : pade_a;
+                alea_gpu_pair_term& T = y.terms[y.n_terms++];
+                T.kind = ALEA_PAIR_PADE;
+                T.n_pairs = 1;
+                T.pairs[0][0] = A.first;
+                T.pairs[0][1] = A.last;
+                T.pairs[0][2] = B.first;
+                T.pairs[0][3] = B.last;
+                T.num_order = 1;
+                T.den_order = 1;
+                T.coeffs[0] = a1;
+                T.coeffs[1] = pade_b;
+                T.image_sum = 1;
+                // equal-spin pairs share one table
+                int same = -1;
+                for (int q = 0; q + 1 < y.n_terms; ++q)
+                    if (y.terms[q].coeffs[0] == a1) same = q;
+                if (same >= 0) {
+                    T.short_range = y.terms[same].short_range;
+                    T.u_inf = y.terms[same].u_inf;
+                    T.kset = y.terms[same].kset;
+                    continue;
+                }
+                double u_inf = 0.0;
+                const Breakup br = pade_breakup(c, {a1}, {pade_b}, u_inf);
+                set_spline(S, T.short_range, br);
+                T.u_inf = u_inf;
+                set_kset(S, T.kset, br);
+            }
+        write_json(S, "heg", self, bg);
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        delete S;
+        return ALEA_ERR_INVALID;
+    }
+    *out = S;
+    return ALEA_OK;
+}
+
+// 2-D Wigner crystal: a triangular lattice of nx × ny sites (ny even) in the
+// rectangular cell nx a × ny a √3/2 at density r_s, spin up on even rows and
+// down on odd rows, Gaussian orbitals exp(−c |r − R|²) with c = gauss_c / r_s²,
+// Drummond-Towler-Needs Jastrows (C = 3) with cutoff `cutoff_frac` × the
+// Wigner-Seitz inradius and cusp-derived α₁ (same spins, opposite spins),
+// Ewald Coulomb.  Initial walkers: sites + N(0, jitter).
+int alea_gpu_setup_crystal2d(int nx, int ny, double rs, double gauss_c, double alpha0,
+                             double cutoff_frac, double jitter, double ewald_tol,
+                             alea_gpu_setup** out, char* err, size_t err_len) {
+    if (!out) return ALEA_ERR_INVALID;
+    *out = nullptr;
+    auto* S = new alea_gpu_setup();
+    try {
+        if (nx < 1 || ny < 2 || ny % 2 || !(rs > 0.0)) throw std::invalid_argument("crystal2d: bad sizes");
+        alea_gpu_system& y = S->sys;
+        const int N = nx * ny, nu = N / 2, nd = N - nu;
+        y.dim = 2;
+        y.n_particles = N;
+        y.periodic = 1;
+        const double alat = rs * std::sqrt(2.0 * kPi / std::sqrt(3.0));
+        const double Lx = nx * alat, Ly = ny * alat * std::sqrt(3.0) / 2.0;
+        const Cell c = make_cell(Lx, Ly);
+        std::copy(c.a, c.a + 4, y.lattice);
+        add_group(y, 0, nu, -1.0);
+        add_group(y, nu, nd, -1.0);
+        std::vector<double> up, dn;
+        for (int r = 0; r < ny; ++r)
+            for (int col = 0; col < nx; ++col) {
+                auto& dst = (r % 2 == 0) ? up : dn;
+                dst.push_back((col + 0.5 * (r % 2)) * alat - 0.5 * Lx);
+                dst.push_back(r * alat * std::sqrt(3.0) / 2.0 - 0.5 * Ly);
+            }
+        const double alpha = gauss_c / (rs * rs);
+        for (int g = 0; g < 2; ++g) {
+            alea_gpu_orbitals& B = y.blocks[y.n_blocks++];
+            B.first = y.groups[g].first;
+            B.last = y.groups[g].last;
+            B.type = ALEA_ORB_GAUSSIAN;
+            B.centers = S->keep(g == 0 ? up : dn);
+            B.alphas = S->keep(std::vector<double>(B.last - B.first, alpha));
+        }
+        S->anchors = up;
+        S->anchors.insert(S->anchors.end(), dn.begin(), dn.end());
+        S->jitter = jitter > 0.0 ? jitter : 1.0 / std::sqrt(4.0 * alpha);
+        double self = 0.0, bg = 0.0;
+        add_ewald(S, c, ewald_tol > 0.0 ? ewald_tol : 1e-6, self, bg);
+        const double Lcut = (cutoff_frac > 0.0 ? cutoff_frac : 0.999) * c.ws;
+        for (int item = 0; item < 2; ++item) {
+            alea_gpu_pair_term& T = y.terms[y.n_terms++];
+            T.kind = ALEA_PAIR_DRUMMOND;
+            if (item == 0) {
+                T.n_pairs = 2;
+                for (int g = 0; g < 2; ++g) {
+                    T.pairs[g][0] = T.pairs[g][2] = y.groups[g].first;
+                    T.pairs[g][1] = T.pairs[g][3] = y.groups[g].last;
+                }
+            } else {
+                T.n_pairs = 1;
+                T.pairs[0][0] = y.groups[0].first;
+                T.pairs[0][1] = y.groups[0].last;
+                T.pairs[0][2] = y.groups[1].first;
+                T.pairs[0][3] = y.groups[1].last;
+            }
+            T.C = 3;
+            T.gamma = 2.0 * 0.5 * 1.0 / (2 * (item == 0 ? 1 : 0) + 1);
+            T.L = Lcut;
+            T.n_coeffs = 1;
+            T.dcoeffs[0] = alpha0;
+        }
+        write_json(S, "crystal", self, bg);
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        delete S;
+        return ALEA_ERR_INVALID;
+    }
+    *out = S;
+    return ALEA_OK;
+}
+
+// Open 2-D exciton: electron and hole, exact trial u = −r (Padé with the
+// Kato cusp a₁ = −1), open Coulomb −1/r.  E = −1 with zero variance.
+int alea_gpu_setup_exciton2d(double L_init, alea_gpu_setup** out) {
+    if (!out) return ALEA_ERR_INVALID;
+    auto* S = new alea_gpu_setup();
+    alea_gpu_system& y = S->sys;
+    y.dim = 2;
+    y.n_particles = 2;
+    y.periodic = 0;
+    add_group(y, 0, 1, -1.0);
+    add_group(y, 1, 1, 1.0);
+    alea_gpu_pair_term& T = y.terms[y.n_terms++];
+    T.kind = ALEA_PAIR_PADE;
+    T.n_pairs = 1;
+    T.pairs[0][0] = 0;
+    T.pairs[0][1] = 1;
+    T.pairs[0][2] = 1;
+    T.pairs[0][3] = 2;
+    T.num_order = 1;
+    T.den_order = 0;
+    T.coeffs[0] = 2.0 * 0.5 * (-1.0) / 1.0;
+    alea_gpu_coulomb& C = y.coulomb[y.n_coulomb++];
+    C.a_first = 0;
+    C.a_last = 1;
+    C.b_first = 1;
+    C.b_last = 2;
+    C.coef = -1.0;
+    S->open_L = L_init > 0.0 ? L_init : 1.0;
+    write_json(S, "exciton", 0.0, 0.0);
+    *out = S;
+    return ALEA_OK;
+}
+
+// Initial positions with the reference App's semantics (app.cpp:56-112):
+// one mt19937_64 seeded with `seed`, walkers in order, particles in order;
+// uniform fractional coordinates in [−½, ½) through the cell vectors, uniform
+// in [−L/2, L/2) for an open cell, or site + jitter × N(0, 1) for a crystal.
+// lo + (hi − lo) u and the lattice sums are fused multiply-adds, the rounding
+// of the reference built with FMA contraction.  positions: AoS [w][p][d].
+int alea_gpu_setup_positions(const alea_gpu_setup* S, uint64_t seed, int nw, double* positions) {
+    if (!S || !positions || nw < 0) return ALEA_ERR_INVALID;
+    const alea_gpu_system& y = S->sys;
+    std::mt19937_64 eng(seed);
+    std::uniform_real_distribution<double> uni(0.0, 1.0);
+    std::normal_distribution<double> gau(0.0, 1.0);
+    const int np = y.n_particles;
+    for (int w = 0; w < nw; ++w)
+        for (int p = 0; p < np; ++p) {
+            double* r = positions + (static_cast<size_t>(w) * np + p) * 2;
+            if (!S->anchors.empty()) {
+                for (int d = 0; d < 2; ++d) r[d] = std::fma(S->jitter, gau(eng), S->anchors[p * 2 + d]);
+            } else if (y.periodic) {
+                double f[2];
+                for (int i = 0; i < 2; ++i) f[i] = std::fma(1.0, uni(eng), -0.5);
+                for (int d = 0; d < 2; ++d) {
+                    double acc = 0.0;
+                    for (int i = 0; i < 2; ++i) acc = std::fma(f[i], y.lattice[i * 2 + d], acc);
+                    r[d] = acc;
+                }
+            } else {
+                for (int d = 0; d < 2; ++d) r[d] = std::fma(S->open_L, uni(eng), -0.5 * S->open_L);
+            }
+        }
+    return ALEA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,78 @@
+"""Host setup of the systems the walker kernels run, through the C ABI.
+
+Each builder returns a :class:`Setup`: ``desc`` is the system description dict
+that :func:`alea_b200.pack_system` and :class:`alea_b200.Walkers` take, and
+``positions(seed, nw)`` draws initial walkers as the reference App does
+(src/qmc/app.cpp:56-112).  The tables (plane-wave shells, Ewald and
+image-summed Padé breakups, cusps) are computed by ``alea_setup.cpp`` inside
+``libalea_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+
+import numpy as np
+
+from . import _capi
+
+
+class Setup:
+    def __init__(self, handle: ctypes.c_void_p):
+        self._lib = _capi.load()
+        self._h = handle
+        self.desc = json.loads(self._lib.alea_gpu_setup_json(handle).decode())
+
+    def positions(self, seed: int, nw: int) -> np.ndarray:
+        """Initial walkers, AoS [nw, np, dim]."""
+        np_, dim = int(self.desc["np"]), int(self.desc["dim"])
+        out = np.zeros((nw, np_, dim), dtype=np.float64)
+        rc = self._lib.alea_gpu_setup_positions(self._h, ctypes.c_uint64(seed), nw,
+                                                out.ctypes.data_as(_capi.c_dp))
+        if rc != 0:
+            raise ValueError(f"alea_gpu_setup_positions failed ({rc})")
+        return out
+
+    def close(self):
+        if self._h:
+            self._lib.alea_gpu_setup_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _make(fn, *args) -> Setup:
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    err = ctypes.create_string_buffer(512)
+    rc = getattr(lib, fn)(*args, ctypes.byref(h), err, len(err))
+    if rc != 0:
+        raise ValueError(f"{fn}: {err.value.decode()}")
+    return Setup(h)
+
+
+def heg2d(n_up: int, n_down: int, rs: float, pade_b: float = 0.3, pade_a: float = 0.0,
+          ewald_tol: float = 1e-6) -> Setup:
+    """2-D electron gas (square cell, plane waves, image-summed Padé, Ewald)."""
+    return _make("alea_gpu_setup_heg2d", n_up, n_down, rs, pade_b, pade_a, ewald_tol)
+
+
+def crystal2d(nx: int, ny: int, rs: float, gauss_c: float = 0.1, alpha0: float = 0.0,
+              cutoff_frac: float = 0.999, jitter: float = 0.0, ewald_tol: float = 1e-6) -> Setup:
+    """2-D Wigner crystal (triangular sites, Gaussians, Drummond, Ewald)."""
+    return _make("alea_gpu_setup_crystal2d", nx, ny, rs, gauss_c, alpha0, cutoff_frac, jitter,
+                 ewald_tol)
+
+
+def exciton2d(L_init: float = 1.0) -> Setup:
+    """Open 2-D exciton with the exact trial function (E = -1)."""
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    rc = lib.alea_gpu_setup_exciton2d(L_init, ctypes.byref(h))
+    if rc != 0:
+        raise ValueError(f"alea_gpu_setup_exciton2d failed ({rc})")
+    return Setup(h)

@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Benchmark: fixed-node DMC of the 2-D electron gas on the B200 walker path.
+
+Workload: N = 42 electrons (21 up / 21 down) at r_s = 30 in a square periodic
+cell, plane-wave Slater determinants times an image-summed Padé Jastrow
+(a from the Kato cusp, b = 0.3), 2-D Ewald Coulomb; 16384 walkers, τ = 0.5,
+one sweep per step, population control toward 16384.  All arithmetic FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one DMC generation: every walker sweeps its 42 electrons with
+drift-diffusion moves, refreshes its derivatives, evaluates E_L and its branch
+weight (one sweep kernel), then the population branches (host serial stream,
+device gather).  `value` is electron-moves/s of K such steps with the walkers
+resident in HBM, CUDA events on the context's stream; `e2e` is the same
+metric through the C ABI's run call from pinned host positions, with the
+upload, the run's per-step weight reads and branch maps, and the download of
+positions and local energies inside the timed region.
+
+Under torchrun each rank runs an independent replica (its own seed) on its
+GPU; value = moves of all ranks / the slowest rank's time.
+
+--impl reference times the reference's own OpenMP DMC (oracle/_ref, compiled
+from the reference sources) on the host cores on a bounded walker sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_UP, N_DOWN, RS, PADE_B = 21, 21, 30.0, 0.3
+NP = N_UP + N_DOWN
+DIM = 2
+TAU = 0.5
+VMC_TAU = (0.5 * RS) ** 2          # Metropolis step 0.5 r_s for the pre-equilibration
+GENERATIONS = 10.0
+CUTOFF_ALPHA = 2.0
+WORKLOAD = (f"DMC 2-D electron gas N={NP} ({N_UP} up/{N_DOWN} down) rs={RS:g}, "
+            f"tau={TAU}, 1 sweep per step, FP64")
+METRIC = "electron-moves/s"
+UNIT = "moves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--walkers", type=int, default=16384)
+    ap.add_argument("--pre", type=int, default=20, help="untimed VMC pre-equilibration steps")
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--cpu-walkers", type=int, default=1024,
+                    help="walker sample of the host-CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ───────────────────────── algorithmic work per unit ─────────────────────
+
+def work_per_unit(desc):
+    """Bytes per electron-move (state streamed once per sweep, per move) and
+    per local-energy evaluation, from the system's sizes."""
+    blocks = [b["last"] - b["first"] for b in desc["slater"]]
+    n_g = len(desc["groups"])
+    n_kj = max((len(p["image_sum"]["weight"]) for p in desc.get("pade", []) if "image_sum" in p),
+               default=0)
+    s_w = (sum(n * n for n in blocks) + NP * DIM + NP * (NP - 1) // 2 + 2 * NP * DIM
+           + 2 * n_g * n_kj + 4)
+    b_move = 2.0 * 8.0 * s_w / NP
+    b_eval = 8.0 * (NP * (NP - 1) / 2 + 3 * NP * DIM + 2)
+    return b_move, b_eval, n_kj, len(desc["ewald"]["weight"])
+
+
+# ───────────────────────── measured peaks, clocks ───────────────────────
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of one GPU's clocks during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str | None):
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if device_id:
+            cmd += ["-i", device_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 8:
+                continue
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profiled_traffic_per_walker():
+    """DRAM bytes per walker per sweep-kernel launch from the committed ncu
+    summary of that kernel (a `dram_bytes_per_walker:` line), or None."""
+    path = os.path.join(ROOT, "profiles", "sweep_dmc_heg42.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("dram_bytes_per_walker:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ───────────────────────── reference (host CPU) arm ─────────────────────
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_cpu(nw: int, steps: int, warmup: int, seed: int):
+    """Reference OpenMP DMC on the host cores: returns (moves/s, info)."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    threads = host_threads()
+    if os.path.exists(harness):
+        args = [harness, "bench", "system=heg", f"nu={N_UP}", f"nd={N_DOWN}", f"rs={RS:g}",
+                f"b={PADE_B:g}", f"nw={nw}", f"steps={warmup + steps + 1}", f"tau={TAU}",
+                f"seed={seed}", f"threads={threads}"]
+        out = subprocess.run(args, capture_output=True, text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        d = json.loads(out.stdout)
+        stamps = np.array(d["stamps"])
+        walkers = np.array(d["walkers"])
+        dt = np.diff(stamps)[warmup:warmup + steps]
+        moves = float(np.sum(walkers[warmup + 1:warmup + 1 + steps])) * NP
+        return moves / float(np.sum(dt)), {"kind": "reference", "cores": int(d["threads"]),
+                                           "sample": f"{nw} walkers x {steps} DMC steps "
+                                                     f"(after {warmup} untimed), same system"}
+    # the compiled reference is absent: the oracle restatement (one thread)
+    from oracle import Oracle
+    from alea_b200 import setup as S
+    st = S.heg2d(N_UP, N_DOWN, RS, PADE_B)
+    o = Oracle(st.desc)
+    o.init(st.positions(seed, nw), capacity=2 * nw + 2)
+    t0 = time.perf_counter()
+    o.dmc(1, seed, 0, 1, steps, 1, TAU, nw)
+    dt = time.perf_counter() - t0
+    return nw * NP * steps / dt, {"kind": "port", "cores": 1,
+                                  "sample": f"{nw} walkers x {steps} DMC steps, oracle restatement"}
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nw = min(a.walkers, a.cpu_walkers)
+    v, info = run_reference_cpu(nw, a.steps, a.warmup, a.seed)
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: seeded uniform initial walkers (mt19937_64)",
+        "config": {"workload": WORKLOAD, "walkers": nw, "n_particles": NP, "rs": RS, "tau": TAU},
+        "cpu_baseline": dict(value=v, unit=UNIT, **info),
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ───────────────────────── GPU arm ──────────────────────────────────────
+
+class DmcLoop:
+    """Population control around dmc_advance/dmc_branch, the loop of
+    DMC::run_one_step (src/qmc/dmc.cpp:693-739) with PopulationControl's
+    trial-energy feedback (src/qmc/population_control.cpp:37-103)."""
+
+    def __init__(self, walkers, target, seed):
+        import alea_b200
+        self.g = walkers
+        self.target = target
+        walkers.set_streams(seed, alea_b200.STREAM_DMC, target)
+        self.state = branch_stream_state(seed)
+        el = walkers.download()["local_energy"]
+        self.etrial = self.eref = float(np.mean(el))
+        med = np.median(el)
+        sigma = 1.4826 * np.median(np.abs(el - med))
+        self.e_cut = CUTOFF_ALPHA * np.sqrt(sigma * np.sqrt(NP) / TAU) if sigma > 0 else np.inf
+        self.e_max = 1.5 * self.e_cut
+        self.feedback = 1.0 / (GENERATIONS * TAU)
+
+    def step(self):
+        g = self.g
+        st = g.dmc_advance(TAU, 1, self.etrial, self.eref, self.e_cut, self.e_max)
+        ms = g.last_kernel_ms()
+        g.dmc_branch(self.state, self.target)
+        if st.weight_sum > 0:
+            self.eref = st.energy_sum / st.weight_sum
+            self.etrial = self.eref - self.feedback * np.log(st.weight_sum / self.target)
+        return st, ms
+
+
+def _splitmix64(x):
+    m = (1 << 64) - 1
+    x = (x + 0x9E3779B97F4A7C15) & m
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & m
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & m
+    return x ^ (x >> 31)
+
+
+def branch_stream_state(seed):
+    """xoshiro256++ state of the serial branch stream, as alea_gpu_dmc_run
+    seeds it: stream_seed(seed, "dmc-brch", 0) expanded by splitmix64."""
+    import alea_b200
+    base = _splitmix64(_splitmix64(_splitmix64(seed) ^ alea_b200.STREAM_BRANCH) ^ 0)
+    m = (1 << 64) - 1
+    return np.array([_splitmix64((base + i * 0x9E3779B97F4A7C15) & m) for i in range(4)],
+                    dtype=np.uint64)
+
+
+def gpu_arm(a):
+    import torch
+    import torch.distributed as dist
+
+    import alea_b200
+    from alea_b200 import _capi
+    from alea_b200 import setup as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the walker path has no CPU fallback")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allreduce(x, op):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    nw = a.walkers
+    setup = S.heg2d(N_UP, N_DOWN, RS, PADE_B)
+    desc = setup.desc
+    b_move, b_eval, n_kj, n_ke = work_per_unit(desc)
+    seed = a.seed + 7919 * rank
+    g = alea_b200.Walkers(desc, capacity=2 * nw + 2, device=local)
+    g.upload(setup.positions(seed, nw))
+    # untimed VMC pre-equilibration from the uniform start
+    if a.pre > 0:
+        g.vmc_run(0, 1, a.pre, 1, VMC_TAU, nw, seed)
+    loop = DmcLoop(g, nw, seed)
+    for _ in range(a.warmup):
+        loop.step()
+    stream = torch.cuda.ExternalStream(g.stream_handle(), device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # ── device-resident timed region ──
+    dev_uuid = None
+    try:
+        dev_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(dev_uuid)
+    l0 = g.launch_count()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    moves = evals = 0
+    sweep_ms = []
+    sweep_walkers = []
+    for _ in range(a.steps):
+        st, ms = loop.step()
+        moves += st.n_proposed
+        evals += st.n_walkers
+        sweep_ms.append(ms)
+        sweep_walkers.append(st.n_walkers)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = g.launch_count() - l0
+    clk = clocks.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = allreduce(ms, dist.ReduceOp.MAX if world > 1 else None)
+    moves_all = allreduce(float(moves), dist.ReduceOp.SUM if world > 1 else None)
+    evals_all = allreduce(float(evals), dist.ReduceOp.SUM if world > 1 else None)
+    launches_all = allreduce(float(launches), dist.ReduceOp.SUM if world > 1 else None)
+    value = moves_all / (ms_max * 1e-3)
+
+    # roofline of the sweep kernel (the dominant launch)
+    hbm_peak, peak_kind = measured_peaks()
+    t_sweep = float(np.sum(sweep_ms)) * 1e-3
+    bytes_alg = moves * b_move + evals * b_eval
+    achieved = bytes_alg / t_sweep / 1e9
+    per_walker = profiled_traffic_per_walker()
+    traffic = per_walker * float(np.mean(sweep_walkers)) if per_walker else None
+
+    # ── end to end through the C ABI from pinned host buffers ──
+    lib = _capi.load()
+    final = g.download()
+    n_w = final["positions"].shape[0]
+    pin_pos = torch.empty(NP * DIM * n_w, dtype=torch.float64, pin_memory=True)
+    pin_pos.numpy()[:] = np.ascontiguousarray(final["positions"].T).ravel()
+    pin_out = torch.empty(NP * DIM * (2 * nw + 2), dtype=torch.float64, pin_memory=True)
+    pin_el = torch.empty(2 * nw + 2, dtype=torch.float64, pin_memory=True)
+    cfg = _capi.RunConfig(0, 1, a.steps, 1, TAU, 1, nw, np.uint64(seed + 1).item(), nw,
+                          GENERATIONS, CUTOFF_ALPHA)
+    res = _capi.RunResult()
+    dp = lambda t: ctypes_ptr(t, _capi)
+    h0, d0 = g.transfer_bytes()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g._check(lib.alea_gpu_upload_walkers(g.ctx, dp(pin_pos), n_w))
+    g._check(lib.alea_gpu_dmc_run(g.ctx, cfg, res, None))
+    g._check(lib.alea_gpu_download_walkers(g.ctx, dp(pin_out), None, None, None, dp(pin_el), None))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    h1, d1 = g.transfer_bytes()
+    e_ms = allreduce(e0.elapsed_time(e1), dist.ReduceOp.MAX if world > 1 else None)
+    e_moves = allreduce(float(res.n_moves), dist.ReduceOp.SUM if world > 1 else None)
+    e2e = {"value": e_moves / (e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int((h1 - h0) / a.steps), "d2h_bytes_per_step": int((d1 - d0) / a.steps),
+           "path": "alea_gpu_upload_walkers + alea_gpu_dmc_run + alea_gpu_download_walkers, pinned host buffers"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            v, info = run_reference_cpu(min(nw, a.cpu_walkers), 3, 1, a.seed)
+            cpu = dict(value=v, unit=UNIT, **info)
+        except Exception as exc:   # reported, never substituted for the GPU number
+            cpu = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded uniform initial walkers (mt19937_64), VMC-equilibrated "
+                    f"for {a.pre} steps; trial function and tables built on the host",
+            "config": {"workload": WORKLOAD, "walkers": nw, "n_particles": NP, "rs": RS, "tau": TAU,
+                       "pade": "u = a r/(1 + 0.3 r), a from the cusp: 1 (up-down), 1/3 (same spin)",
+                       "ewald_k_vectors": n_ke, "jastrow_k_vectors": n_kj,
+                       "l2": "no flush: walker records (~50 KB x walkers) exceed the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "el_evals_per_s": evals_all / (ms_max * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": traffic,
+                         "kernel": "sweep_kernel (DMC mode)", "peak_kind": peak_kind,
+                         "bytes_per_move": b_move, "bytes_per_eval": b_eval,
+                         "sweep_ms_per_launch": float(np.mean(sweep_ms)),
+                         "sweep_share_of_step": t_sweep / (ms * 1e-3)},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches_all),
+            "clocks": clk,
+            "population": int(g.nw),
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_ptr(t, _capi):
+    import ctypes
+    return ctypes.cast(ctypes.c_void_p(t.data_ptr()), _capi.c_dp)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return reference_arm(a)
+    return gpu_arm(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

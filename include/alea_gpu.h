@@ -247,6 +247,8 @@ typedef struct {
     double walltime_s;
     int n_walkers;
     double e_trial;
+    int64_t n_moves;         /* single-particle moves proposed, all blocks */
+    int64_t n_evaluations;   /* local energies evaluated, all blocks */
 } alea_gpu_run_result;
 
 /* Whole VMC / DMC runs, the reference drivers' loops with device sweeps.
@@ -260,6 +262,50 @@ int alea_gpu_dmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu
 /* Device time of the last alea_gpu_*_step / advance call's sweep kernel, in
  * milliseconds (CUDA events on the context's stream). */
 int alea_gpu_last_kernel_ms(const alea_gpu_ctx* ctx, double* ms);
+
+/* The cudaStream_t every call of this context is ordered on (no counterpart
+ * in the reference: a host that times or overlaps work records its events
+ * on this stream). */
+int alea_gpu_stream(const alea_gpu_ctx* ctx, void** stream);
+/* Bytes this context has copied host->device and device->host so far
+ * (instrumentation; no counterpart in the reference). */
+int alea_gpu_transfer_bytes(const alea_gpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
+/* Kernels this context has launched so far (instrumentation; no counterpart
+ * in the reference). */
+int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
+
+/* ── Host setup ─────────────────────────────────────────────────────────
+ * Builds an alea_gpu_system (and its JSON description) for the systems the
+ * reference's App assembles from a config, computing the same tables on the
+ * host: cell from r_s (src/qmc/app.cpp:288-336), plane-wave shells
+ * (src/wavefunction/orbital_set.h:575-665), Kato cusps
+ * (src/builders/jastrow.cpp:48-98), the optimized Ewald breakup
+ * (src/numerics/ewald_breakup.cpp:205-276, n_knots ladder of
+ * src/hamiltonian/ewald_term.cpp) and the image-summed Padé
+ * (src/wavefunction/periodic_pair_sum.cpp:21-60).  The setup owns every
+ * table the system points to; free it after alea_gpu_create. */
+typedef struct alea_gpu_setup alea_gpu_setup;
+
+/* 2-D electron gas: n_up + n_down electrons at density rs in a square cell,
+ * Padé u = a r/(1 + pade_b r) per spin pair (a from the cusp when pade_a <= 0),
+ * Ewald tolerance ewald_tol (<= 0: 1e-6).  err receives a message on failure. */
+int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pade_a,
+                         double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len);
+/* 2-D Wigner crystal of nx × ny triangular sites (ny even), Gaussian
+ * orbitals exp(-(gauss_c / rs²) |r - R|²), Drummond Jastrows with alpha0 and
+ * cutoff cutoff_frac × the Wigner-Seitz radius (<= 0: 0.999), initial
+ * jitter (<= 0: 1/sqrt(4 gauss_c / rs²)). */
+int alea_gpu_setup_crystal2d(int nx, int ny, double rs, double gauss_c, double alpha0,
+                             double cutoff_frac, double jitter, double ewald_tol,
+                             alea_gpu_setup** out, char* err, size_t err_len);
+/* Open 2-D exciton with the exact trial function (E = -1). */
+int alea_gpu_setup_exciton2d(double L_init, alea_gpu_setup** out);
+const alea_gpu_system* alea_gpu_setup_system(const alea_gpu_setup* s);
+const char* alea_gpu_setup_json(const alea_gpu_setup* s);
+/* Initial walkers, AoS [w][p][d], with App::initialize_positions' draws
+ * (src/qmc/app.cpp:56-112): one mt19937_64 seeded with `seed`. */
+int alea_gpu_setup_positions(const alea_gpu_setup* s, uint64_t seed, int nw, double* positions);
+void alea_gpu_setup_free(alea_gpu_setup* s);
 
 #ifdef __cplusplus
 }

@@ -667,11 +667,12 @@ int run(const std::string& mode, const Args& a) {
             c.population_generations = getd(a, "generations", 10.0);
             if (!bench) put_positions(out, "initial_positions", ens);
             DMC dmc(c, ens, sys->psi, sys->ham);
-            std::vector<double> stamps, wsum, ewsum;
+            std::vector<double> stamps, wsum, ewsum, nws;
             std::vector<std::vector<double>> el, wt, ids;
             dmc.set_measure_hook([&](const WalkerSet& ws, const TrialWavefunction&) {
                 stamps.push_back(std::chrono::duration<double>(
                     std::chrono::steady_clock::now().time_since_epoch()).count());
+                nws.push_back(static_cast<double>(ws.num_walkers()));
                 double sw = 0.0, se = 0.0;
                 for (std::size_t w = 0; w < ws.num_walkers(); ++w) {
                     sw += ws.weights()[w];
@@ -692,6 +693,7 @@ int run(const std::string& mode, const Args& a) {
             out.ki("threads", c.n_threads);
             out.kv("wall", wall);
             out.arr("stamps", stamps);
+            out.arr("walkers", nws);
             out.arr("weight_sum", wsum);
             out.arr("weighted_energy_sum", ewsum);
             out.ks("summary_first_line", "");

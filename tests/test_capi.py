@@ -41,10 +41,12 @@ def test_struct_layout_matches_header():
 #include <stdio.h>
 #include "alea_gpu.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(alea_gpu_system), sizeof(alea_gpu_pair_term),
-         sizeof(alea_gpu_orbitals), sizeof(alea_gpu_ewald), offsetof(alea_gpu_system, terms),
-         offsetof(alea_gpu_system, ewald), offsetof(alea_gpu_system, coulomb),
-         sizeof(alea_gpu_run_config), sizeof(alea_gpu_step_stats));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(alea_gpu_system),
+         sizeof(alea_gpu_pair_term), sizeof(alea_gpu_orbitals), sizeof(alea_gpu_ewald),
+         offsetof(alea_gpu_system, terms), offsetof(alea_gpu_system, ewald),
+         offsetof(alea_gpu_system, coulomb), sizeof(alea_gpu_run_config),
+         sizeof(alea_gpu_step_stats), sizeof(alea_gpu_run_result),
+         offsetof(alea_gpu_run_result, n_moves));
   return 0;
 }
 """
@@ -57,7 +59,8 @@ int main(void) {
     want = [ctypes.sizeof(_capi.System), ctypes.sizeof(_capi.PairTerm), ctypes.sizeof(_capi.Orbitals),
             ctypes.sizeof(_capi.Ewald), _capi.System.terms.offset, _capi.System.ewald.offset,
             _capi.System.coulomb.offset, ctypes.sizeof(_capi.RunConfig),
-            ctypes.sizeof(_capi.StepStats)]
+            ctypes.sizeof(_capi.StepStats), ctypes.sizeof(_capi.RunResult),
+            _capi.RunResult.n_moves.offset]
     assert got == want
 
 

@@ -1,0 +1,125 @@
+"""Host setup (alea_setup.cpp through the C ABI) against the tables and local
+energies of the compiled reference's builders.
+
+The breakup coefficients need not agree bit for bit (the optimized fit
+amplifies rounding differences of the quadrature to ~1e-8 relative, the
+reference's own breakup tolerance), but the physics they encode must: the
+local energy of every fixture walker agrees with the reference-built system
+to 1e-10 relative, through the oracle, on the CPU.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+alea_setup = pytest.importorskip("alea_b200.setup")
+
+CASES = {
+    "heg42": ("heg2d", dict(n_up=21, n_down=21, rs=30.0, pade_b=0.3)),
+    "heg10": ("heg2d", dict(n_up=5, n_down=5, rs=30.0, pade_b=0.3)),
+    "crystal16": ("crystal2d", dict(nx=4, ny=4, rs=40.0, gauss_c=0.1)),
+}
+
+E_L_RTOL = 1e-10        # local energy, reference-built vs this setup
+TABLE_RTOL = 1e-7       # breakup tables (fit conditioning), relative to max|.|
+INIT_SEED = 12345       # the seed the eval fixtures' walkers were drawn with
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request):
+    fn, kw = CASES[request.param]
+    s = getattr(alea_setup, fn)(**kw)
+    return request.param, s, golden(f"setup_{request.param}.json")
+
+
+def _close(a, b, rtol):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    assert a.shape == b.shape
+    scale = max(np.max(np.abs(b)) if b.size else 0.0, 1e-300)
+    assert np.max(np.abs(a - b)) <= rtol * scale if a.size else True
+
+
+def test_cell_orbitals_cusps(case):
+    name, s, g = case
+    d = s.desc
+    _close(d["cell"]["vectors"], g["cell"]["vectors"], 1e-15)
+    assert [(x["first"], x["last"], x["charge"]) for x in d["groups"]] == \
+        [(x["first"], x["last"], x["charge"]) for x in g["groups"]]
+    for mb, gb in zip(d["slater"], g["slater"]):
+        assert mb["type"] == gb["type"]
+        if gb["type"] == "plane_wave":
+            _close(mb["k"], gb["k"], 1e-15)
+            assert mb["is_sin"] == gb["is_sin"]
+        else:
+            _close(mb["centers"], gb["centers"], 1e-15)
+            _close(mb["alphas"], gb["alphas"], 1e-15)
+    for mp, gp in zip(d.get("pade", []), g.get("pade", [])):
+        assert (mp["ga"], mp["gb"]) == (gp["ga"], gp["gb"])
+        _close(mp["a"], gp["a"], 1e-15)
+        _close(mp["b"], gp["b"], 1e-15)
+    for md, gd in zip(d.get("drummond", []), g.get("drummond", [])):
+        assert md["pairs"] == gd["pairs"] and md["C"] == gd["C"]
+        assert md["gamma"] == pytest.approx(gd["gamma"], rel=1e-15)
+        assert md["L"] == pytest.approx(gd["L"], rel=1e-15)
+
+
+def test_breakup_tables(case):
+    name, s, g = case
+    d = s.desc
+    pairs = [(d["ewald"], g["ewald"])]
+    pairs += [(a["image_sum"], b["image_sum"]) for a, b in zip(d.get("pade", []), g.get("pade", []))
+              if "image_sum" in b]
+    for mine, ref in pairs:
+        assert mine["n1"] == ref["n1"] and mine["n2"] == ref["n2"]
+        _close(mine["kx"], ref["kx"], 1e-15)
+        _close(mine["weight"], ref["weight"], TABLE_RTOL)
+        sp, rp = mine["spline"], ref["spline"]
+        assert sp["n_knots"] == rp["n_knots"]
+        _close(sp["scaled"], rp["scaled"], TABLE_RTOL)
+    if "self_energy" in g["ewald"]:
+        assert d["ewald"]["self_energy"] == pytest.approx(g["ewald"]["self_energy"], rel=TABLE_RTOL)
+
+
+def test_local_energy_matches_reference_tables(case):
+    from oracle import Oracle
+    name, s, g = case
+    ev = golden(f"eval_{name}.json")
+    pos = np.array(ev["positions"])
+    el = []
+    for desc in (s.desc, g):
+        o = Oracle(desc)
+        o.init(pos, capacity=len(pos))
+        el.append(np.array([o.measure(i) for i in range(len(pos))]))
+    np.testing.assert_allclose(el[0], el[1], rtol=E_L_RTOL)
+    np.testing.assert_allclose(el[1], ev["local_energy"], rtol=E_L_RTOL)
+
+
+def test_initial_positions(case):
+    name, s, g = case
+    ev = golden(f"eval_{name}.json")
+    pos = np.array(ev["positions"])
+    mine = s.positions(INIT_SEED, len(pos)).reshape(pos.shape)
+    np.testing.assert_allclose(mine, pos, rtol=0, atol=1e-12 * np.max(np.abs(pos)))
+
+
+def test_exciton_setup():
+    s = alea_setup.exciton2d()
+    g = golden("setup_exciton.json")
+    assert s.desc["pade"][0]["a"] == g["pade"][0]["a"]
+    assert s.desc["coulomb"][0]["coef"] == g["coulomb"][0]["coef"]
+    ev = golden("eval_exciton.json")
+    ref = np.array(ev["positions"])
+    pos = s.positions(INIT_SEED, len(ref)).reshape(ref.shape)
+    np.testing.assert_array_equal(pos, ref)
+
+
+def test_setup_rejects_bad_input():
+    with pytest.raises(ValueError):
+        alea_setup.heg2d(0, 0, 30.0)
+    with pytest.raises(ValueError, match="shell"):
+        alea_setup.heg2d(4, 4, 30.0)        # 4 plane waves leave a shell open
+    with pytest.raises(ValueError):
+        alea_setup.crystal2d(4, 3, 30.0)    # odd row count
