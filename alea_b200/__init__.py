@@ -251,6 +251,13 @@ class Walkers:
         self._check(self.lib.alea_gpu_vmc_step(self.ctx, ctypes.byref(prm), ctypes.byref(st)))
         return st
 
+    def vmc_step_noalloc(self, tau: float, n_substeps: int = 1, drift: bool = False) -> _capi.StepStats:
+        """alea_gpu_vmc_step_noalloc: the VMC step with its scratch in a static device array."""
+        prm = _capi.VmcParams(tau, n_substeps, 1 if drift else 0)
+        st = _capi.StepStats()
+        self._check(self.lib.alea_gpu_vmc_step_noalloc(self.ctx, ctypes.byref(prm), ctypes.byref(st)))
+        return st
+
     def dmc_advance(self, tau, n_substeps, e_trial, e_ref, e_cut, e_max) -> _capi.StepStats:
         prm = _capi.DmcParams(tau, n_substeps, e_trial, e_ref, e_cut, e_max)
         st = _capi.StepStats()

@@ -112,7 +112,7 @@ EXPORTS = [
     "alea_gpu_download_walkers", "alea_gpu_move", "alea_gpu_measure", "alea_gpu_set_streams",
     "alea_gpu_vmc_step", "alea_gpu_dmc_advance", "alea_gpu_dmc_branch", "alea_gpu_vmc_run",
     "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms", "alea_gpu_stream", "alea_gpu_transfer_bytes",
-    "alea_gpu_launch_count",
+    "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc",
     "alea_gpu_setup_heg2d", "alea_gpu_setup_crystal2d", "alea_gpu_setup_exciton2d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
     "alea_gpu_setup_free",
@@ -144,6 +144,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_measure": ([P], I),
         "alea_gpu_set_streams": ([P, ctypes.c_uint64, ctypes.c_uint64, I], I),
         "alea_gpu_vmc_step": ([P, ctypes.POINTER(VmcParams), ctypes.POINTER(StepStats)], I),
+        "alea_gpu_vmc_step_noalloc": ([P, ctypes.POINTER(VmcParams), ctypes.POINTER(StepStats)], I),
         "alea_gpu_dmc_advance": ([P, ctypes.POINTER(DmcParams), ctypes.POINTER(StepStats)], I),
         "alea_gpu_dmc_branch": ([P, ctypes.POINTER(ctypes.c_uint64), I], I),
         "alea_gpu_vmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),

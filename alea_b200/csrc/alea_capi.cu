@@ -178,6 +178,7 @@ struct alea_gpu_ctx {
     double next_id = 1.0;
     uint64_t h2d = 0, d2h = 0;     // bytes copied host->device / device->host
     uint64_t launches = 0;         // kernels launched by this context
+    double* noalloc_scratch = nullptr;   // device address of g_noalloc_scratch on `device`
 };
 
 namespace {
@@ -689,6 +690,50 @@ int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, doubl
     return check_errors(c);
 }
 
+// ───────────────────────── allocation-free VMC step ─────────────────────
+//
+// Scratch of alea_gpu_vmc_step_noalloc: the sweep's random numbers
+// [(sweep·np + p)·3·nw + d·nw + w], then the step's reduced statistics.  A
+// file-scope device array exists once per device, so every context on a
+// device shares it; each call writes all of the scratch it reads (randoms by
+// draw_kernel, statistics by noalloc_stats_kernel) before reading it, so
+// nothing in it needs to start at zero.
+constexpr size_t kNoAllocRandoms = size_t(1) << 20;   // doubles (8 MiB)
+constexpr size_t kNoAllocStats = 32;                  // doubles, 4 used
+static_assert(kNoAllocRandoms == ALEA_GPU_NOALLOC_RANDOMS, "header and scratch size disagree");
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocRandoms + kNoAllocStats];
+
+// One block of 256 threads: Σ E_L, Σ E_L², Σ accepted moves and max |error
+// flag| over the walkers, written (not accumulated) to out[0..3].
+__global__ void __launch_bounds__(256) noalloc_stats_kernel(const double* records, int nw, long rec,
+                                                             int o_scal, double* out) {
+    __shared__ double red[4][256];
+    double e = 0.0, e2 = 0.0, na = 0.0, er = 0.0;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+        const double* r = records + static_cast<size_t>(w) * rec + o_scal;
+        const double el = r[S_EL];
+        e += el;
+        e2 += el * el;
+        na += r[S_NACC];
+        er = fmax(er, fabs(r[S_ERR]));
+    }
+    red[0][threadIdx.x] = e;
+    red[1][threadIdx.x] = e2;
+    red[2][threadIdx.x] = na;
+    red[3][threadIdx.x] = er;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + h];
+            red[1][threadIdx.x] += red[1][threadIdx.x + h];
+            red[2][threadIdx.x] += red[2][threadIdx.x + h];
+            red[3][threadIdx.x] = fmax(red[3][threadIdx.x], red[3][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
 }  // namespace
 
 // ───────────────────────── C ABI ────────────────────────────────────────
@@ -926,6 +971,71 @@ int alea_gpu_vmc_step(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, alea_gpu_
             out->energy_sq_sum += el[w] * el[w];
             out->n_accepted += static_cast<int64_t>(na[w]);
         }
+        out->weight_sum = c->nw;
+        out->n_proposed = static_cast<int64_t>(prm->n_substeps) * c->sys.np * c->nw;
+        out->n_walkers = c->nw;
+    }
+    return ALEA_OK;
+}
+
+int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out) {
+    if (!c || !prm) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    if (c->nw == 0) {
+        if (out) *out = alea_gpu_step_stats{};
+        return ALEA_OK;
+    }
+    if (c->n_streams < 1) return fail(c, ALEA_ERR_INVALID, "no random streams (alea_gpu_set_streams)");
+    if (prm->n_substeps < 1) return fail(c, ALEA_ERR_INVALID, "n_substeps must be >= 1");
+    const size_t need = static_cast<size_t>(prm->n_substeps) * c->sys.np * 3 * c->nw;
+    if (need > kNoAllocRandoms)
+        return fail(c, ALEA_ERR_INVALID,
+                    "alea_gpu_vmc_step_noalloc: n_substeps x particles x 3 x walkers = " + std::to_string(need) +
+                        " random numbers exceed the static scratch of " + std::to_string(kNoAllocRandoms));
+    if (!c->noalloc_scratch) {   // set-up, once per context (and so per device)
+        void* p = nullptr;
+        CUDA_TRY(c, cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        c->noalloc_scratch = static_cast<double*>(p);
+    }
+    if (prm->tau != c->sigma_tau) {   // sqrt(τ/m) per coordinate, staged from the stack
+        double sg[2 * 1024];
+        const size_t n = c->h_inv_mass.size();
+        if (n > sizeof sg / sizeof sg[0]) return fail(c, ALEA_ERR_UNSUPPORTED, "too many particles");
+        for (size_t i = 0; i < n; ++i) sg[i] = std::sqrt(prm->tau * c->h_inv_mass[i]);
+        CUDA_TRY(c, copy_in(c, c->d_sigma, sg, n * 8));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        c->sigma_tau = prm->tau;
+    }
+    double* rnd = c->noalloc_scratch;
+    double* stats = c->noalloc_scratch + kNoAllocRandoms;
+    const long stride = c->nw;
+    const int nt = std::min(c->n_streams, c->nw);
+    ++c->launches;
+    draw_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, stride,
+                                                         prm->n_substeps, c->sys.zk, c->sys.zw, c->sys.zf,
+                                                         c->sys.zr, rnd, 0);
+    CUDA_TRY(c, cudaGetLastError());
+    SweepParams sp{};
+    sp.mode = 0;
+    sp.n_sub = prm->n_substeps;
+    sp.drift = prm->use_drift;
+    sp.tau = prm->tau;
+    sp.sigma = c->d_sigma;
+    ++c->launches;
+    CUDA_TRY(c, launch_sweep(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), rnd, stride, sp, c->pairs,
+                             c->npair));
+    ++c->launches;
+    noalloc_stats_kernel<<<1, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec, c->sys.o_scal, stats);
+    CUDA_TRY(c, cudaGetLastError());
+    double h[4];
+    CUDA_TRY(c, copy_out(c, h, stats, sizeof h));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (h[3] != 0.0) return fail(c, ALEA_ERR_SINGULAR, "a walker's accepted determinant is singular or nonfinite");
+    if (out) {
+        *out = alea_gpu_step_stats{};
+        out->energy_sum = h[0];
+        out->energy_sq_sum = h[1];
+        out->n_accepted = static_cast<int64_t>(h[2]);
         out->weight_sum = c->nw;
         out->n_proposed = static_cast<int64_t>(prm->n_substeps) * c->sys.np * c->nw;
         out->n_walkers = c->nw;

@@ -213,6 +213,30 @@ typedef struct {
  * threads are (src/qmc/vmc.cpp:45-61). */
 int alea_gpu_vmc_step(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out);
 
+/* The same VMC step as alea_gpu_vmc_step, allocating nothing (no counterpart
+ * in the reference).  For callers that must not allocate device memory once
+ * a run is set up: a serving loop that admits jobs by their HBM footprint
+ * has reserved that memory at admission, and alea_gpu_vmc_step's scratch
+ * grows with cudaFree + cudaMalloc (a cudaMalloc that can then fail mid-run,
+ * a cudaFree that synchronizes the whole device under the other jobs).
+ *   - Scratch: the sweep's random numbers and the step's reduced statistics
+ *     live in one file-scope static device array of ALEA_GPU_NOALLOC_RANDOMS
+ *     + 32 doubles (8 MiB + 256 B).  A step needs n_substeps × n_particles ×
+ *     3 × walkers doubles of it; a larger step returns ALEA_ERR_INVALID with a
+ *     message and launches nothing.
+ *   - Set-up: the first call on a context looks up the array's device
+ *     address (cudaGetSymbolAddress, with the context's device current);
+ *     make that first call before any stream capture.
+ *   - Sharing: the array exists once per device and every context on that
+ *     device uses it, so calls that overlap on the GPU race.  It keeps the
+ *     last call's contents; each call writes all the scratch it reads before
+ *     reading it, so nothing in it needs to start at zero.
+ *   - alea_gpu_set_streams must have been called (that call may allocate).
+ * Results equal alea_gpu_vmc_step's: same kernels, same random numbers;
+ * the energy sums are reduced on the device (rounding order differs). */
+#define ALEA_GPU_NOALLOC_RANDOMS 1048576
+int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out);
+
 typedef struct {
     double tau;
     int n_substeps;
