@@ -114,6 +114,7 @@ EXPORTS = [
     "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms", "alea_gpu_stream", "alea_gpu_transfer_bytes",
     "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc",
     "alea_gpu_setup_heg2d", "alea_gpu_setup_crystal2d", "alea_gpu_setup_exciton2d",
+    "alea_gpu_setup_charges2d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
     "alea_gpu_setup_free",
 ]
@@ -158,6 +159,8 @@ def load() -> ctypes.CDLL:
         "alea_gpu_setup_crystal2d": ([I, I, D, D, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
                                       ctypes.c_size_t], I),
         "alea_gpu_setup_exciton2d": ([D, ctypes.POINTER(P)], I),
+        "alea_gpu_setup_charges2d": ([c_dp, I, c_ip, c_dp, D, ctypes.POINTER(P), ctypes.c_char_p,
+                                      ctypes.c_size_t], I),
         "alea_gpu_setup_system": ([P], ctypes.POINTER(System)),
         "alea_gpu_setup_json": ([P], ctypes.c_char_p),
         "alea_gpu_setup_positions": ([P, ctypes.c_uint64, I, c_dp], I),

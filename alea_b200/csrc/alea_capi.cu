@@ -198,6 +198,35 @@ int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
 
 long round4(long x) { return (x + 3) & ~3L; }
 
+// Per-interval monomial coefficients of a quintic Hermite spline: on interval
+// i, with y = 1 − x,
+//   f = a0 h0(x) + a1 h1(x) + a2 h2(x) + b0 h0(y) − b1 h1(y) + b2 h2(y),
+//   h0 = 1 − 10x³ + 15x⁴ − 6x⁵, h1 = x − 6x³ + 8x⁴ − 3x⁵,
+//   h2 = x²/2 − 3x³/2 + 3x⁴/2 − x⁵/2,
+// (a, b the scaled data of knots i, i+1) expanded into c_0 + ... + c_5 x^5.
+std::vector<double> hermite_to_monomial(const double* scaled, int n_knots) {
+    static const double H[3][6] = {{1, 0, 0, -10, 15, -6}, {0, 1, 0, -6, 8, -3}, {0, 0, 0.5, -1.5, 1.5, -0.5}};
+    // h_j(1 − x) in monomials of x
+    double G[3][6] = {};
+    for (int j = 0; j < 3; ++j)
+        for (int m = 0; m < 6; ++m) {
+            double binom = 1.0;   // C(m, q) (−1)^q
+            for (int q = 0; q <= m; ++q) {
+                G[j][q] += H[j][m] * binom;
+                binom = -binom * (m - q) / (q + 1);
+            }
+        }
+    std::vector<double> out(6 * static_cast<size_t>(std::max(n_knots - 1, 1)), 0.0);
+    for (int i = 0; i + 1 < n_knots; ++i) {
+        const double* a = scaled + 3 * i;
+        const double* b = a + 3;
+        for (int q = 0; q < 6; ++q)
+            out[6 * i + q] = a[0] * H[0][q] + a[1] * H[1][q] + a[2] * H[2][q] + b[0] * G[0][q] -
+                             b[1] * G[1][q] + b[2] * G[2][q];
+    }
+    return out;
+}
+
 // Host<->device copies on the context's stream, counted.
 cudaError_t copy_in(alea_gpu_ctx* c, void* dst, const void* src, size_t n) {
     c->h2d += n;
@@ -325,6 +354,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     auto put = [&](const void* p, size_t n, const void** slot) {
         patches.push_back({ar.add(p, n), slot});
     };
+    std::vector<std::vector<double>> poly_tables;
     // groups
     if (in->n_groups < 1 || in->n_groups > kMaxGroups) return fail(c, ALEA_ERR_INVALID, "bad n_groups");
     s.ngroups = in->n_groups;
@@ -431,6 +461,9 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
                 D.sp.inv_delta = sp.inv_delta;
                 D.sp.n_knots = sp.n_knots;
                 put(sp.scaled, 3 * sp.n_knots * 8, reinterpret_cast<const void**>(&D.sp.scaled));
+                poly_tables.push_back(hermite_to_monomial(sp.scaled, sp.n_knots));
+                put(poly_tables.back().data(), poly_tables.back().size() * 8,
+                    reinterpret_cast<const void**>(&D.sp.poly));
                 D.u_inf = T.u_inf;
                 const alea_gpu_kset& ks = T.kset;
                 if (ks.n_k < 1 || !ks.n1 || !ks.n2 || !ks.kx || !ks.ky || !ks.weight)
@@ -463,6 +496,27 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         } else {
             return fail(c, ALEA_ERR_INVALID, "unknown pair term");
         }
+    }
+    // group-pair coupling masks, when every term's ranges are whole groups
+    {
+        auto group_at = [&](int f, int l) {
+            for (int g = 0; g < s.ngroups; ++g)
+                if (s.gfirst[g] == f && s.glast[g] == l) return g;
+            return -1;
+        };
+        s.pair_by_group = 1;
+        std::memset(s.gterms, 0, sizeof s.gterms);
+        for (int t = 0; t < s.nterms; ++t)
+            for (int q = 0; q < s.terms[t].npairs; ++q) {
+                const int ga = group_at(s.terms[t].pairs[q][0], s.terms[t].pairs[q][1]);
+                const int gb = group_at(s.terms[t].pairs[q][2], s.terms[t].pairs[q][3]);
+                if (ga < 0 || gb < 0) {
+                    s.pair_by_group = 0;
+                    continue;
+                }
+                s.gterms[ga][gb] |= static_cast<uint8_t>(1u << t);
+                s.gterms[gb][ga] |= static_cast<uint8_t>(1u << t);
+            }
     }
     if (kref) {
         s.nkJ = kref->n_k;
@@ -505,6 +559,8 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         s.esp.inv_delta = E.long_range.inv_delta;
         s.esp.n_knots = E.long_range.n_knots;
         put(E.long_range.scaled, 3 * E.long_range.n_knots * 8, reinterpret_cast<const void**>(&s.esp.scaled));
+        poly_tables.push_back(hermite_to_monomial(E.long_range.scaled, E.long_range.n_knots));
+        put(poly_tables.back().data(), poly_tables.back().size() * 8, reinterpret_cast<const void**>(&s.esp.poly));
         s.e_rcut = E.r_cut;
         s.e_inv_eps = E.inv_eps;
         s.e_const = E.constant;
@@ -1090,11 +1146,23 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
     std::memcpy(rng.s, state, 32);
     std::vector<int> src;
     src.reserve(2 * target + 2);
+    const size_t n_max = 2 * static_cast<size_t>(target) + 1, n_min = static_cast<size_t>(target) / 5 + 1;
+    // Multiplicities far beyond the population bound come only from weights
+    // that escaped the branch cutoff (an unequilibrated start); the copy-then-
+    // remove loop below would spend ~m steps on them (the reference converts
+    // such m to int).  Refuse them instead of running away.
+    const double m_limit = 64.0 * static_cast<double>(n_max);
+    double m_total = 0.0;
     for (int i = 0; i < n; ++i) {
-        const int m = static_cast<int>(w[i] + rng.uniform());
+        const double mw = std::floor(w[i] + rng.uniform());
+        m_total += mw > 0.0 ? mw : 0.0;
+        if (!(m_total <= m_limit))
+            return fail(c, ALEA_ERR_INVALID,
+                        "branch multiplicities exceed 64 x (2 target + 1) (walker " + std::to_string(i) +
+                            ", weight " + std::to_string(w[i]) + "): equilibrate before branching");
+        const int m = static_cast<int>(mw);
         for (int k = 0; k < m; ++k) src.push_back(i);
     }
-    const size_t n_max = 2 * static_cast<size_t>(target) + 1, n_min = static_cast<size_t>(target) / 5 + 1;
     if (src.empty()) {
         int best = 0;
         for (int i = 1; i < n; ++i)

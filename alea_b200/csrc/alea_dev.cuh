@@ -31,7 +31,8 @@ enum : int {
 struct DevSpline {
     double r_cut, inv_delta;
     int n_knots;
-    const double* scaled;
+    const double* scaled;     // quintic Hermite data, 3 per knot (value, δ·f', δ²·f'')
+    const double* poly;       // the same pieces as monomials in the local x: 6 per interval
 };
 
 struct DevTerm {
@@ -75,6 +76,10 @@ struct DevSys {
     DevBlock blocks[kMaxBlocks];
     int nterms;
     DevTerm terms[kMaxTerms];
+    // bit t of gterms[ga][gb]: term t couples groups ga and gb (valid when
+    // every term's pair ranges are whole groups, pair_by_group != 0)
+    int pair_by_group;
+    uint8_t gterms[kMaxGroups][kMaxGroups];
     // reciprocal vectors shared by every image-summed Jastrow term
     int nkJ, m1J, m2J;
     const int *n1J, *n2J;
@@ -155,6 +160,9 @@ __device__ __forceinline__ double fold_dist(const DevSys& s, const double* xi, c
 
 // ───────────────────────── radial functions ─────────────────────────────
 
+// The breakup's quintic Hermite spline, evaluated from its per-interval
+// monomial form c_0 + c_1 x + ... + c_5 x^5 in the local coordinate
+// x = r/δ - i (the host expands each interval's Hermite data once).
 __device__ __forceinline__ void spline3(const DevSpline& sp, double r, double& f, double& df,
                                         double& d2f) {
     if (r >= sp.r_cut) {
@@ -164,33 +172,14 @@ __device__ __forceinline__ void spline3(const DevSpline& sp, double r, double& f
     const double t = r * sp.inv_delta;
     int i = static_cast<int>(t);
     if (i > sp.n_knots - 2) i = sp.n_knots - 2;
-    const double x = t - i, y = 1.0 - x;
-    const double* a = sp.scaled + 3 * i;
-    const double* b = a + 3;
-    const double x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x;
-    const double y2 = y * y, y3 = y2 * y, y4 = y3 * y, y5 = y4 * y;
-    const double p0 = 1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5;
-    const double p1 = x - 6.0 * x3 + 8.0 * x4 - 3.0 * x5;
-    const double p2 = 0.5 * x2 - 1.5 * x3 + 1.5 * x4 - 0.5 * x5;
-    const double q0 = 1.0 - 10.0 * y3 + 15.0 * y4 - 6.0 * y5;
-    const double q1 = y - 6.0 * y3 + 8.0 * y4 - 3.0 * y5;
-    const double q2 = 0.5 * y2 - 1.5 * y3 + 1.5 * y4 - 0.5 * y5;
-    const double dp0 = -30.0 * x2 + 60.0 * x3 - 30.0 * x4;
-    const double dp1 = 1.0 - 18.0 * x2 + 32.0 * x3 - 15.0 * x4;
-    const double dp2 = x - 4.5 * x2 + 6.0 * x3 - 2.5 * x4;
-    const double dq0 = -30.0 * y2 + 60.0 * y3 - 30.0 * y4;
-    const double dq1 = 1.0 - 18.0 * y2 + 32.0 * y3 - 15.0 * y4;
-    const double dq2 = y - 4.5 * y2 + 6.0 * y3 - 2.5 * y4;
-    const double ddp0 = -60.0 * x + 180.0 * x2 - 120.0 * x3;
-    const double ddp1 = -36.0 * x + 96.0 * x2 - 60.0 * x3;
-    const double ddp2 = 1.0 - 9.0 * x + 18.0 * x2 - 10.0 * x3;
-    const double ddq0 = -60.0 * y + 180.0 * y2 - 120.0 * y3;
-    const double ddq1 = -36.0 * y + 96.0 * y2 - 60.0 * y3;
-    const double ddq2 = 1.0 - 9.0 * y + 18.0 * y2 - 10.0 * y3;
-    f = a[0] * p0 + a[1] * p1 + a[2] * p2 + b[0] * q0 - b[1] * q1 + b[2] * q2;
-    df = sp.inv_delta * (a[0] * dp0 + a[1] * dp1 + a[2] * dp2 - (b[0] * dq0 - b[1] * dq1 + b[2] * dq2));
-    d2f = sp.inv_delta * sp.inv_delta *
-          (a[0] * ddp0 + a[1] * ddp1 + a[2] * ddp2 + b[0] * ddq0 - b[1] * ddq1 + b[2] * ddq2);
+    const double x = t - i;
+    const double2* c2 = reinterpret_cast<const double2*>(sp.poly + 6 * i);
+    const double2 c01 = __ldg(c2), c23 = __ldg(c2 + 1), c45 = __ldg(c2 + 2);
+    f = fma(fma(fma(fma(fma(c45.y, x, c45.x), x, c23.y), x, c23.x), x, c01.y), x, c01.x);
+    const double g = fma(fma(fma(fma(5.0 * c45.y, x, 4.0 * c45.x), x, 3.0 * c23.y), x, 2.0 * c23.x), x, c01.y);
+    const double h = fma(fma(fma(20.0 * c45.y, x, 12.0 * c45.x), x, 6.0 * c23.y), x, 2.0 * c23.x);
+    df = sp.inv_delta * g;
+    d2f = sp.inv_delta * sp.inv_delta * h;
 }
 
 __device__ __forceinline__ double spline1(const DevSpline& sp, double r) {
@@ -198,18 +187,10 @@ __device__ __forceinline__ double spline1(const DevSpline& sp, double r) {
     const double t = r * sp.inv_delta;
     int i = static_cast<int>(t);
     if (i > sp.n_knots - 2) i = sp.n_knots - 2;
-    const double x = t - i, y = 1.0 - x;
-    const double* a = sp.scaled + 3 * i;
-    const double* b = a + 3;
-    const double x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x;
-    const double y2 = y * y, y3 = y2 * y, y4 = y3 * y, y5 = y4 * y;
-    const double p0 = 1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5;
-    const double p1 = x - 6.0 * x3 + 8.0 * x4 - 3.0 * x5;
-    const double p2 = 0.5 * x2 - 1.5 * x3 + 1.5 * x4 - 0.5 * x5;
-    const double q0 = 1.0 - 10.0 * y3 + 15.0 * y4 - 6.0 * y5;
-    const double q1 = y - 6.0 * y3 + 8.0 * y4 - 3.0 * y5;
-    const double q2 = 0.5 * y2 - 1.5 * y3 + 1.5 * y4 - 0.5 * y5;
-    return a[0] * p0 + a[1] * p1 + a[2] * p2 + b[0] * q0 - b[1] * q1 + b[2] * q2;
+    const double x = t - i;
+    const double2* c2 = reinterpret_cast<const double2*>(sp.poly + 6 * i);
+    const double2 c01 = __ldg(c2), c23 = __ldg(c2 + 1), c45 = __ldg(c2 + 2);
+    return fma(fma(fma(fma(fma(c45.y, x, c45.x), x, c23.y), x, c23.x), x, c01.y), x, c01.x);
 }
 
 __device__ __forceinline__ void poly_acc(const double* c, int n, double r, double& v, double& dv,
@@ -287,6 +268,15 @@ __device__ __forceinline__ bool couples(const DevTerm& T, int p, int k) {
         }
     }
     return false;
+}
+
+// Bit mask of the terms coupling particles p and k.
+__device__ __forceinline__ unsigned coupling(const DevSys& s, int p, int k) {
+    if (s.pair_by_group) return s.gterms[s.group_of[p]][s.group_of[k]];
+    unsigned m = 0;
+    for (int t = 0; t < s.nterms; ++t)
+        if (couples(s.terms[t], p, k)) m |= 1u << t;
+    return m;
 }
 
 __device__ __forceinline__ bool in_term(const DevTerm& T, int p) {

@@ -184,6 +184,25 @@ __device__ __forceinline__ void kspace_particle_k(const DevSys& s, const Smem& v
     }
 }
 
+// Visit the elements (r, c) of an N×N matrix with the CTA's NT threads, no
+// integer division inside the loop: when N ≤ NT each thread owns column c and
+// rows r0, r0 + NT/N, ... (⌊NT/N⌋ rows in flight); otherwise each thread owns
+// columns c, c + NT, ... and walks all rows.
+template <int NT, class F>
+__device__ __forceinline__ void for_each_elem(int N, F&& f) {
+    if (N <= NT) {
+        const int per = NT / N;
+        if (static_cast<int>(threadIdx.x) < per * N) {
+            const int r0 = static_cast<int>(threadIdx.x) / N;
+            const int c = static_cast<int>(threadIdx.x) - r0 * N;
+            for (int r = r0; r < N; r += per) f(r, c);
+        }
+    } else {
+        for (int c = threadIdx.x; c < N; c += NT)
+            for (int r = 0; r < N; ++r) f(r, c);
+    }
+}
+
 // ───────────────────────── Gauss-Jordan rebuild ─────────────────────────
 
 // A = D⁻¹ of block b from its committed rows in HBM, by pivoted Gauss-Jordan
@@ -197,10 +216,10 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
     double* m = v.work;
     const double* D = grec + B.oD;
     __syncthreads();
-    for (int e = threadIdx.x; e < N * N; e += NT) {
-        m[e] = D[e];
-        A[e] = (e / N == e % N) ? 1.0 : 0.0;
-    }
+    for_each_elem<NT>(N, [&](int r, int c) {
+        m[r * N + c] = D[r * N + c];
+        A[r * N + c] = (r == c) ? 1.0 : 0.0;
+    });
     if (threadIdx.x == 0) v.misc[M_LOGDET] = 0.0;
     __syncthreads();
     __shared__ int s_piv;
@@ -251,13 +270,12 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
         __syncthreads();
         for (int r = threadIdx.x; r < N; r += NT) v.col[r] = m[r * N + k];
         __syncthreads();
-        for (int e = threadIdx.x; e < N * N; e += NT) {
-            const int r = e / N, c = e % N;
-            if (r == k) continue;
+        for_each_elem<NT>(N, [&](int r, int c) {
+            if (r == k) return;
             const double f = v.col[r];
-            m[e] -= f * m[k * N + c];
-            A[e] -= f * A[k * N + c];
-        }
+            m[r * N + c] -= f * m[k * N + c];
+            A[r * N + c] -= f * A[k * N + c];
+        });
         __syncthreads();
     }
 }
@@ -423,9 +441,8 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
     }
     for (int k = threadIdx.x; k < np; k += NT) {
         if (k == p) continue;
-        bool any = false;
-        for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
-        if (!any) continue;
+        const unsigned cm = coupling(s, p, k);
+        if (!cm) continue;
         double dn[3], dold[3];
         const double rn = fold_dist(s, v.newpos, v.pos + k * 2, dn);
         const double ro = fold_dist(s, v.pos + p * 2, v.pos + k * 2, dold);
@@ -437,9 +454,8 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
         geo[4] = dold[1];
         geo[5] = ro;
         double du_o = 0.0, d2u_o = 0.0, du_n = 0.0, d2u_n = 0.0;
-        for (int t = 0; t < s.nterms; ++t) {
-            const DevTerm& T = s.terms[t];
-            if (!couples(T, p, k)) continue;
+        for (unsigned bits = cm; bits; bits &= bits - 1) {
+            const DevTerm& T = s.terms[__ffs(bits) - 1];
             double uo, duo, d2uo, un, dun, d2un;
             radial(T, ro, uo, duo, d2uo);
             radial(T, rn, un, dun, d2un);
@@ -540,10 +556,7 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
     // pair terms first (their scratch shares space with the rebuild's work
     // matrix): partner gradients and Laplacians, eager as in the reference
     for (int k = threadIdx.x; k < np; k += NT) {
-        if (k == p) continue;
-        bool any = false;
-        for (int t = 0; t < s.nterms && !any; ++t) any = couples(s.terms[t], p, k);
-        if (!any) continue;
+        if (k == p || !coupling(s, p, k)) continue;
         const double* geo = v.geo + k * 6;
         const double* rad = v.rad + k * 4;
         const double irn = 1.0 / geo[2], iro = 1.0 / geo[5];
@@ -602,10 +615,7 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         if (rebuild) {
             gj_rebuild<NT>(s, v, grec, b);
         } else {
-            for (int e = threadIdx.x; e < N * N; e += NT) {
-                const int a = e / N, c = e - a * N;
-                A[e] = A[e] - v.col[a] * v.rowp[c];
-            }
+            for_each_elem<NT>(N, [&](int a, int c) { A[a * N + c] = A[a * N + c] - v.col[a] * v.rowp[c]; });
             __syncthreads();
         }
         double ra = 0.0, rdm = 0.0;

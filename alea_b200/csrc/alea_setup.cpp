@@ -465,11 +465,54 @@ struct Cell {
     double area = 0.0, ws = 0.0;
 };
 
-Cell make_cell(double lx, double ly) {
+// Lattice rows a = (a1, a2) as the device context reduces them: rows along
+// the axes are permuted onto x, y; any other pair is Lagrange-Gauss reduced.
+// Reciprocal vectors and k indices then refer to the same basis as the
+// device's ladders.
+void reduce_lattice(double a[4]) {
+    int axis[2], used[2] = {0, 0};
+    bool aligned = true;
+    for (int i = 0; i < 2 && aligned; ++i) {
+        int nz = 0, which = 0;
+        for (int d = 0; d < 2; ++d)
+            if (a[i * 2 + d] != 0.0) {
+                ++nz;
+                which = d;
+            }
+        if (nz != 1 || used[which]) aligned = false;
+        else {
+            axis[i] = which;
+            used[which] = 1;
+        }
+    }
+    if (aligned) {
+        double r[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 2; ++i)
+            for (int d = 0; d < 2; ++d) r[axis[i] * 2 + d] = a[i * 2 + d];
+        std::copy(r, r + 4, a);
+        return;
+    }
+    for (int guard = 0; guard < 64; ++guard) {
+        const double n0 = a[0] * a[0] + a[1] * a[1], n1 = a[2] * a[2] + a[3] * a[3];
+        if (n1 < n0) {
+            std::swap(a[0], a[2]);
+            std::swap(a[1], a[3]);
+            continue;
+        }
+        if (n0 == 0.0) break;
+        const double mu = std::nearbyint((a[0] * a[2] + a[1] * a[3]) / n0);
+        if (mu == 0.0) break;
+        a[2] -= mu * a[0];
+        a[3] -= mu * a[1];
+    }
+}
+
+Cell make_cell(const double a_in[4]) {
     Cell c;
-    c.a[0] = lx;
-    c.a[3] = ly;
-    const double det = lx * ly;
+    std::copy(a_in, a_in + 4, c.a);
+    reduce_lattice(c.a);
+    const double det = c.a[0] * c.a[3] - c.a[1] * c.a[2];
+    if (det == 0.0) throw std::invalid_argument("cell: singular lattice vectors");
     c.area = std::abs(det);
     const double inv = 1.0 / det;
     const double ainv[4] = {c.a[3] * inv, -c.a[2] * inv, -c.a[1] * inv, c.a[0] * inv};
@@ -484,6 +527,11 @@ Cell make_cell(double lx, double ly) {
         }
     c.ws = 0.5 * std::sqrt(shortest2);
     return c;
+}
+
+Cell make_cell(double lx, double ly) {
+    const double a[4] = {lx, 0.0, 0.0, ly};
+    return make_cell(a);
 }
 
 // The first `want` real plane waves of closed reciprocal shells (k = 0 gives
@@ -978,6 +1026,42 @@ int alea_gpu_setup_crystal2d(int nx, int ny, double rs, double gauss_c, double a
             T.dcoeffs[0] = alpha0;
         }
         write_json(S, "crystal", self, bg);
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        delete S;
+        return ALEA_ERR_INVALID;
+    }
+    *out = S;
+    return ALEA_OK;
+}
+
+// Point charges in a periodic 2-D cell with Ewald Coulomb only (no
+// wavefunction factors, so E_L is the electrostatic energy): n_groups
+// consecutive groups of counts[g] particles of charge charges[g].  The cell's
+// rows are reduced as the device reduces them.  Initial walkers: uniform.
+int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* counts, const double* charges,
+                             double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len) {
+    if (!out) return ALEA_ERR_INVALID;
+    *out = nullptr;
+    auto* S = new alea_gpu_setup();
+    try {
+        if (!lattice || !counts || !charges || n_groups < 1 || n_groups > ALEA_GPU_MAX_GROUPS)
+            throw std::invalid_argument("charges2d: bad groups");
+        alea_gpu_system& y = S->sys;
+        y.dim = 2;
+        y.periodic = 1;
+        const Cell c = make_cell(lattice);
+        std::copy(c.a, c.a + 4, y.lattice);
+        int first = 0;
+        for (int g = 0; g < n_groups; ++g) {
+            if (counts[g] < 1) throw std::invalid_argument("charges2d: empty group");
+            add_group(y, first, counts[g], charges[g]);
+            first += counts[g];
+        }
+        y.n_particles = first;
+        double self = 0.0, bg = 0.0;
+        add_ewald(S, c, ewald_tol > 0.0 ? ewald_tol : 1e-6, self, bg);
+        write_json(S, "charges", self, bg);
     } catch (const std::exception& e) {
         if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
         delete S;

@@ -68,6 +68,17 @@ def crystal2d(nx: int, ny: int, rs: float, gauss_c: float = 0.1, alpha0: float =
                  ewald_tol)
 
 
+def charges2d(lattice, counts, charges, ewald_tol: float = 1e-6) -> Setup:
+    """Point charges in a periodic 2-D cell, Ewald Coulomb only."""
+    lat = np.ascontiguousarray(np.asarray(lattice, dtype=np.float64).ravel())
+    cnt = np.ascontiguousarray(np.asarray(counts, dtype=np.int32))
+    q = np.ascontiguousarray(np.asarray(charges, dtype=np.float64))
+    if lat.size != 4 or cnt.size != q.size:
+        raise ValueError("charges2d: lattice needs 4 numbers, one charge per group")
+    return _make("alea_gpu_setup_charges2d", lat.ctypes.data_as(_capi.c_dp), int(cnt.size),
+                 cnt.ctypes.data_as(_capi.c_ip), q.ctypes.data_as(_capi.c_dp), ewald_tol)
+
+
 def exciton2d(L_init: float = 1.0) -> Setup:
     """Open 2-D exciton with the exact trial function (E = -1)."""
     lib = _capi.load()

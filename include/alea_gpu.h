@@ -322,6 +322,12 @@ int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double 
 int alea_gpu_setup_crystal2d(int nx, int ny, double rs, double gauss_c, double alpha0,
                              double cutoff_frac, double jitter, double ewald_tol,
                              alea_gpu_setup** out, char* err, size_t err_len);
+/* Point charges in a periodic 2-D cell (rows of `lattice`, reduced as the
+ * device reduces them) with Ewald Coulomb only: n_groups consecutive groups
+ * of counts[g] particles of charge charges[g].  E_L is the electrostatic
+ * energy (src/hamiltonian/ewald_term.cpp:368-612). */
+int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* counts, const double* charges,
+                             double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len);
 /* Open 2-D exciton with the exact trial function (E = -1). */
 int alea_gpu_setup_exciton2d(double L_init, alea_gpu_setup** out);
 const alea_gpu_system* alea_gpu_setup_system(const alea_gpu_setup* s);

@@ -14,7 +14,10 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
   initial positions, per-walker E_L of every accumulation step, final
   positions, acceptance;
 * ``dmc_<name>.json``    DMC::run with one crowd per walker: per-step
-  populations, weights, energies, ids, final positions.
+  populations, weights, energies, ids, final positions;
+* ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
+  reduced here to accumulation-block energies, their mean and its reblocked
+  standard error (the statistical reference for the device's DMC).
 """
 from __future__ import annotations
 
@@ -45,6 +48,24 @@ DMC = {
 }
 
 
+DMC_STAT = {
+    "heg10": dict(nw=1024, seed=424242, eq=10, acc=50, steps=10, substeps=1, tau=0.5, threads=8),
+}
+
+
+def reblock(x):
+    """Mean and the largest standard error over pairwise blocking levels with
+    at least 8 blocks."""
+    import numpy as np
+    x = np.asarray(x, dtype=float)
+    mean = float(x.mean())
+    err = 0.0
+    while len(x) >= 8:
+        err = max(err, float(x.std(ddof=1) / np.sqrt(len(x))))
+        x = 0.5 * (x[0:len(x) // 2 * 2:2] + x[1:len(x) // 2 * 2:2])
+    return mean, err
+
+
 def dump(name, obj):
     with open(os.path.join(HERE, name), "w") as f:
         json.dump(obj, f, separators=(",", ":"))
@@ -68,6 +89,16 @@ def main():
         r["params"] = run
         r["system"] = name
         dump(f"dmc_{name}.json", r)
+    for name, run in DMC_STAT.items():
+        r = run_ref_harness("bench", method="dmc", **run, **SYSTEMS[name])
+        n_acc_steps = run["acc"] * run["steps"]
+        w = r["weight_sum"][-n_acc_steps:]
+        we = r["weighted_energy_sum"][-n_acc_steps:]
+        blocks = [sum(we[b * run["steps"]:(b + 1) * run["steps"]]) /
+                  sum(w[b * run["steps"]:(b + 1) * run["steps"]]) for b in range(run["acc"])]
+        mean, err = reblock(blocks)
+        dump(f"dmcstat_{name}.json", {"params": run, "system": name, "block_energies": blocks,
+                                      "energy": mean, "energy_error": err})
 
 
 if __name__ == "__main__":

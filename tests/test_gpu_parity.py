@@ -137,3 +137,43 @@ def test_exciton_exact_energy_zero_variance():
     assert abs(res.energy + 1.0) < 1e-12
     assert res.variance < 1e-20
     assert 0.5 < res.acceptance < 1.0
+
+
+@pytest.mark.gpu
+def test_ewald_madelung_on_device():
+    """Square-lattice Madelung constant from the device Ewald sum (reference
+    known answer 1.6155426267, tests/test_ewald.cpp:212-225), equal to the
+    oracle's to 1e-10."""
+    import alea_b200
+    from alea_b200 import setup as S
+    from oracle import Oracle
+    s = S.charges2d([2.0, 0.0, 0.0, 2.0], [2, 2], [1.0, -1.0], ewald_tol=1e-8)
+    pos = np.array([[0.0, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0, 1.0]])
+    g = alea_b200.Walkers(s.desc, capacity=1)
+    g.upload(pos)
+    e_dev = g.download()["local_energy"][0]
+    o = Oracle(s.desc)
+    o.init(pos)
+    assert abs(e_dev - o.measure(0)) < 1e-10 * abs(e_dev)
+    assert -2.0 * e_dev / 4.0 == pytest.approx(1.6155426267, abs=1e-6)
+
+
+@pytest.mark.gpu
+def test_dmc_energy_agrees_with_reference_statistically():
+    """A long device DMC run (independent seed and start) against the compiled
+    reference's DMC on the same system and parameters: the block-averaged
+    energies agree within 2 combined standard errors."""
+    import alea_b200
+    from alea_b200 import setup as S
+    ref = golden("dmcstat_heg10.json")
+    p = ref["params"]
+    desc = golden("setup_heg10.json")
+    start = S.heg2d(5, 5, 30.0).positions(777, p["nw"])
+    g = alea_b200.Walkers(desc, capacity=2 * p["nw"] + 2)
+    g.upload(start)
+    res, blocks = g.dmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], p["threads"],
+                            seed=778, target=p["nw"], generations=10.0)
+    assert len(blocks) == p["acc"] and np.all(np.isfinite(blocks))
+    sigma = float(np.hypot(res.energy_error, ref["energy_error"]))
+    assert res.energy_error > 0 and abs(res.energy - ref["energy"]) < 2.0 * sigma, \
+        (res.energy, res.energy_error, ref["energy"], ref["energy_error"])

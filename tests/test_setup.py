@@ -123,3 +123,30 @@ def test_setup_rejects_bad_input():
         alea_setup.heg2d(4, 4, 30.0)        # 4 plane waves leave a shell open
     with pytest.raises(ValueError):
         alea_setup.crystal2d(4, 3, 30.0)    # odd row count
+
+
+MADELUNG_2D_SQUARE = 1.6155426267   # tests/test_ewald.cpp:212-225 of the reference
+
+
+def _madelung_system(tol=1e-8):
+    # ±1 charges on a square lattice of spacing 1: (0,0)+ (1,1)+ | (1,0)- (0,1)- in a 2x2 cell
+    s = alea_setup.charges2d([2.0, 0.0, 0.0, 2.0], [2, 2], [1.0, -1.0], ewald_tol=tol)
+    pos = np.array([[0.0, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0, 1.0]])
+    return s, pos
+
+
+def test_ewald_reproduces_square_madelung_constant():
+    """E = -(N/2) M q²/a for N = 4 ions: the reference's Madelung known answer,
+    through this library's breakup tables and the oracle's Ewald sum."""
+    from oracle import Oracle
+    s, pos = _madelung_system()
+    o = Oracle(s.desc)
+    o.init(pos)
+    M = -2.0 * o.measure(0) / 4.0
+    assert M == pytest.approx(MADELUNG_2D_SQUARE, abs=1e-6)
+    # periodic translation of one ion by a lattice vector leaves E unchanged
+    moved = pos.copy()
+    moved[0, 2] += 3 * 2.0
+    moved[0, 3] -= 2 * 2.0
+    o.init(moved)
+    assert -2.0 * o.measure(0) / 4.0 == pytest.approx(M, abs=1e-12)
