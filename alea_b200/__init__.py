@@ -88,6 +88,8 @@ def pack_system(desc: Dict[str, Any]):
         terms.append(("pade", p))
     for d in desc.get("drummond", []):
         terms.append(("drummond", d))
+    for z in desc.get("zero_energy", []):
+        terms.append(("zero_energy", z))
     s.n_terms = len(terms)
     for i, (kind, t) in enumerate(terms):
         T = s.terms[i]
@@ -116,6 +118,16 @@ def pack_system(desc: Dict[str, Any]):
                 T.kset.kx = _dp(f64(im["kx"]))
                 T.kset.ky = _dp(f64(im["ky"]))
                 T.kset.weight = _dp(f64(im["weight"]))
+        elif kind == "zero_energy":
+            T.kind = _capi.PAIR_ZERO_ENERGY
+            T.n_pairs = 1
+            pr = [int(t["ga"][0]), int(t["ga"][1]), int(t["gb"][0]), int(t["gb"][1])]
+            for k in range(4):
+                T.pairs[0][k] = pr[k]
+            T.ze_b = float(t["b"])
+            T.ze_exponent = float(t["exponent"])
+            T.ze_matching_radius = float(t["matching_radius"])
+            T.ze_cutoff = float(t["cutoff"])
         else:
             T.kind = _capi.PAIR_DRUMMOND
             T.n_pairs = len(t["pairs"])
@@ -153,6 +165,13 @@ def pack_system(desc: Dict[str, Any]):
         C.a_first, C.a_last = int(c["ga"][0]), int(c["ga"][1])
         C.b_first, C.b_last = int(c["gb"][0]), int(c["gb"][1])
         C.coef = float(c["coef"])
+    ip = desc.get("inverse_power", [])
+    s.n_inverse_power = len(ip)
+    for i, c in enumerate(ip):
+        V = s.inverse_power[i]
+        V.a_first, V.a_last = int(c["ga"][0]), int(c["ga"][1])
+        V.b_first, V.b_last = int(c["gb"][0]), int(c["gb"][1])
+        V.strength, V.exponent, V.tail = float(c["strength"]), float(c["exponent"]), float(c["tail"])
     return s, keep
 
 

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libalea_b200.so")
 ALEA_OK = 0
 ERRORS = {1: "invalid", 2: "cuda", 3: "unsupported", 4: "singular", 5: "timeout", 6: "nomem"}
 ORB_PLANE_WAVE, ORB_GAUSSIAN = 0, 1
-PAIR_PADE, PAIR_DRUMMOND = 0, 1
+PAIR_PADE, PAIR_DRUMMOND, PAIR_ZERO_ENERGY = 0, 1, 2
 STREAM_VMC = 0x766D632D74687264
 STREAM_DMC = 0x646D632D74687264
 STREAM_BRANCH = 0x646D632D62726368
@@ -51,7 +51,9 @@ class PairTerm(ctypes.Structure):
                 ("image_sum", ctypes.c_int), ("short_range", Spline), ("u_inf", ctypes.c_double),
                 ("kset", KSet), ("C", ctypes.c_int), ("gamma", ctypes.c_double),
                 ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int),
-                ("dcoeffs", ctypes.c_double * 16)]
+                ("dcoeffs", ctypes.c_double * 16), ("ze_b", ctypes.c_double),
+                ("ze_exponent", ctypes.c_double), ("ze_matching_radius", ctypes.c_double),
+                ("ze_cutoff", ctypes.c_double)]
 
 
 class Ewald(ctypes.Structure):
@@ -65,12 +67,19 @@ class Coulomb(ctypes.Structure):
                 ("b_last", ctypes.c_int), ("coef", ctypes.c_double)]
 
 
+class InversePower(ctypes.Structure):
+    _fields_ = [("a_first", ctypes.c_int), ("a_last", ctypes.c_int), ("b_first", ctypes.c_int),
+                ("b_last", ctypes.c_int), ("strength", ctypes.c_double),
+                ("exponent", ctypes.c_double), ("tail", ctypes.c_double)]
+
+
 class System(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("n_particles", ctypes.c_int), ("periodic", ctypes.c_int),
                 ("lattice", ctypes.c_double * 9), ("n_groups", ctypes.c_int),
                 ("groups", Group * 8), ("n_blocks", ctypes.c_int), ("blocks", Orbitals * 4),
                 ("n_terms", ctypes.c_int), ("terms", PairTerm * 8), ("ewald", Ewald),
-                ("n_coulomb", ctypes.c_int), ("coulomb", Coulomb * 8)]
+                ("n_coulomb", ctypes.c_int), ("coulomb", Coulomb * 8), ("n_inverse_power", ctypes.c_int),
+                ("inverse_power", InversePower * 8)]
 
 
 class VmcParams(ctypes.Structure):
@@ -114,7 +123,7 @@ EXPORTS = [
     "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms", "alea_gpu_stream", "alea_gpu_transfer_bytes",
     "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc",
     "alea_gpu_setup_heg2d", "alea_gpu_setup_crystal2d", "alea_gpu_setup_exciton2d",
-    "alea_gpu_setup_charges2d",
+    "alea_gpu_setup_charges2d", "alea_gpu_setup_dipoles2d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
     "alea_gpu_setup_free",
 ]
@@ -159,6 +168,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_setup_crystal2d": ([I, I, D, D, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
                                       ctypes.c_size_t], I),
         "alea_gpu_setup_exciton2d": ([D, ctypes.POINTER(P)], I),
+        "alea_gpu_setup_dipoles2d": ([I, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p, ctypes.c_size_t], I),
         "alea_gpu_setup_charges2d": ([c_dp, I, c_ip, c_dp, D, ctypes.POINTER(P), ctypes.c_char_p,
                                       ctypes.c_size_t], I),
         "alea_gpu_setup_system": ([P], ctypes.POINTER(System)),

@@ -198,6 +198,79 @@ int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
 
 long round4(long x) { return (x + 3) & ~3L; }
 
+// e^x K0(x), e^x K1(x) on the host: the ascending series for x <= 2 (DLMF
+// 10.31.1-2), the standard library's K_nu times e^x up to x = 30, and the
+// Hankel asymptotic series e^x K_nu(x) = sqrt(π/2x) Σ a_k(ν)/x^k beyond
+// (a_k = a_{k-1} (4ν² - (2k-1)²)/(8k); DLMF 10.40.2), summed to 1e-17.
+void host_k01e(double x, double& k0e, double& k1e) {
+    if (x <= 2.0) {
+        const double euler_gamma = 0.57721566490153286060651209008240243;
+        const double y = 0.25 * x * x;
+        double term0 = 1.0, term1 = 1.0, harmonic = 0.0, i0 = 0.0, s0 = 0.0, i1 = 0.0, s1 = 0.0;
+        for (int k = 0; k < 15; ++k) {
+            if (k > 0) {
+                term0 *= y / (static_cast<double>(k) * k);
+                term1 *= y / (static_cast<double>(k) * (k + 1));
+                harmonic += 1.0 / k;
+            }
+            const double harmonic_next = harmonic + 1.0 / (k + 1);
+            i0 += term0;
+            s0 += harmonic * term0;
+            i1 += term1;
+            s1 += (harmonic + harmonic_next - 2.0 * euler_gamma) * term1;
+        }
+        const double lh = std::log(0.5 * x);
+        const double ex = std::exp(x);
+        k0e = ex * (-(lh + euler_gamma) * i0 + s0);
+        k1e = ex * (1.0 / x + lh * (0.5 * x * i1) - 0.25 * x * s1);
+        return;
+    }
+    if (x <= 30.0) {
+        const double ex = std::exp(x);
+        k0e = ex * std::cyl_bessel_k(0.0, x);
+        k1e = ex * std::cyl_bessel_k(1.0, x);
+        return;
+    }
+    const double pre = std::sqrt(3.14159265358979323846 / (2.0 * x));
+    for (int nu = 0; nu < 2; ++nu) {
+        const double mu = 4.0 * nu * nu;
+        double a = 1.0, sum = 1.0;
+        for (int k = 1; k < 60; ++k) {
+            a *= (mu - (2.0 * k - 1) * (2.0 * k - 1)) / (8.0 * k * x);
+            sum += a;
+            if (std::abs(a) < 1e-17 * std::abs(sum)) break;
+        }
+        (nu == 0 ? k0e : k1e) = pre * sum;
+    }
+}
+
+// Chebyshev coefficients of sqrt(x) e^x K_nu(x) in ξ = 4/x - 1 for ν = 0, 1
+// (24 each), projected on 192 first-kind nodes ξ_j = cos θ_j.
+std::vector<double> bessel_k01_chebyshev() {
+    constexpr int kTerms = 24, M = 8 * kTerms;
+    std::vector<double> f0(M), f1(M), theta(M), c(2 * kTerms, 0.0);
+    for (int j = 0; j < M; ++j) {
+        theta[j] = 3.14159265358979323846 * (j + 0.5) / M;
+        const double x = 4.0 / (std::cos(theta[j]) + 1.0);
+        double k0e, k1e;
+        host_k01e(x, k0e, k1e);
+        f0[j] = std::sqrt(x) * k0e;
+        f1[j] = std::sqrt(x) * k1e;
+    }
+    for (int k = 0; k < kTerms; ++k) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int j = 0; j < M; ++j) {
+            const double ck = std::cos(k * theta[j]);
+            s0 += f0[j] * ck;
+            s1 += f1[j] * ck;
+        }
+        const double norm = (k == 0 ? 1.0 : 2.0) / M;
+        c[k] = norm * s0;
+        c[kTerms + k] = norm * s1;
+    }
+    return c;
+}
+
 // Per-interval monomial coefficients of a quintic Hermite spline: on interval
 // i, with y = 1 − x,
 //   f = a0 h0(x) + a1 h1(x) + a2 h2(x) + b0 h0(y) − b1 h1(y) + b2 h2(y),
@@ -355,6 +428,9 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         patches.push_back({ar.add(p, n), slot});
     };
     std::vector<std::vector<double>> poly_tables;
+    std::vector<double> bessel_table;     // zero-energy terms' Chebyshev table (one per system)
+    const double* bessel_dev = nullptr;   // patched to its device address
+    std::vector<int> ze_terms;
     // groups
     if (in->n_groups < 1 || in->n_groups > kMaxGroups) return fail(c, ALEA_ERR_INVALID, "bad n_groups");
     s.ngroups = in->n_groups;
@@ -493,6 +569,33 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
             double ipw = 1.0;
             for (int i = 0; i < T.C; ++i) ipw *= -T.L;
             D.alpha1 = T.gamma / ipw + D.dc[0] * static_cast<double>(T.C) / T.L;
+        } else if (T.kind == ALEA_PAIR_ZERO_ENERGY) {
+            // ZeroEnergyFunction (src/wavefunction/zero_energy_jastrow.cpp:16-60)
+            if (T.n_pairs != 1) return fail(c, ALEA_ERR_INVALID, "a zero-energy term has one group pair");
+            const double b = T.ze_b, p = T.ze_exponent, rm = T.ze_matching_radius, rc = T.ze_cutoff;
+            if (!(std::isfinite(b) && b > 0.0) || !(std::isfinite(p) && p > 2.0) ||
+                !(std::isfinite(rc) && rc > 0.0) || !(rm > 0.0 && rm < rc))
+                return fail(c, ALEA_ERR_INVALID,
+                            "zero-energy term needs b > 0, exponent > 2 and 0 < matching radius < cutoff");
+            if (bessel_table.empty()) {
+                bessel_table = bessel_k01_chebyshev();
+                put(bessel_table.data(), bessel_table.size() * 8, reinterpret_cast<const void**>(&bessel_dev));
+            }
+            D.ze_s = 0.5 * (p - 2.0);
+            D.ze_kappa = std::sqrt(b) / D.ze_s;
+            D.ze_rm = rm;
+            D.ze_rc = rc;
+            const double x = D.ze_kappa * std::pow(rm, -D.ze_s);
+            double k0e, k1e;
+            host_k01e(x, k0e, k1e);
+            const double q = k1e / k0e, sx = D.ze_s * x;
+            const double u0 = std::log(k0e) - x, du0 = sx * q / rm;
+            const double cc = 2.0 * rc - rm;
+            const double h = 1.0 / (rm * rm) - 1.0 / (cc * cc);
+            D.ze_c3 = du0 / h;
+            D.ze_logc2 = 2.0 * D.ze_c3 / rc;
+            D.ze_logc1 = D.ze_logc2 - D.ze_c3 / rm - D.ze_c3 / cc - u0;
+            ze_terms.push_back(t);
         } else {
             return fail(c, ALEA_ERR_INVALID, "unknown pair term");
         }
@@ -589,6 +692,26 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         s.coul[k][3] = C.b_last;
         s.coul_coef[k] = C.coef;
     }
+    if (in->n_inverse_power < 0 || in->n_inverse_power > kMaxCoulomb)
+        return fail(c, ALEA_ERR_INVALID, "bad n_inverse_power");
+    s.nip = in->n_inverse_power;
+    s.ip_tail = 0.0;
+    for (int k = 0; k < s.nip; ++k) {
+        const alea_gpu_inverse_power& V = in->inverse_power[k];
+        if (V.a_first < 0 || V.a_last > np || V.b_first < 0 || V.b_last > np || V.a_first >= V.a_last ||
+            V.b_first >= V.b_last || !(std::isfinite(V.exponent) && V.exponent > 0.0) ||
+            !std::isfinite(V.strength))
+            return fail(c, ALEA_ERR_INVALID, "bad inverse-power term");
+        s.ip[k][0] = V.a_first;
+        s.ip[k][1] = V.a_last;
+        s.ip[k][2] = V.b_first;
+        s.ip[k][3] = V.b_last;
+        s.ip_c[k] = V.strength;
+        s.ip_p[k] = V.exponent;
+        const double rp = std::nearbyint(V.exponent);
+        s.ip_pint[k] = (rp == V.exponent && rp <= 16.0) ? static_cast<int>(rp) : 0;
+        s.ip_tail += V.tail;
+    }
     // ziggurat tables
     const Ziggurat z = make_ziggurat();
     put(z.k, sizeof z.k, reinterpret_cast<const void**>(&s.zk));
@@ -631,7 +754,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     CUDA_TRY(c, cudaMalloc(&c->arena, std::max<size_t>(ar.bytes.size(), 256)));
     CUDA_TRY(c, cudaMemcpy(c->arena, ar.bytes.data(), ar.bytes.size(), cudaMemcpyHostToDevice));
     for (const Patch& p : patches) *p.slot = static_cast<char*>(c->arena) + p.off;
-    // the DevSys copy keeps const double* etc.; nothing else to patch
+    for (int t : ze_terms) s.terms[t].ze_cheb = bessel_dev;
     return ALEA_OK;
 }
 

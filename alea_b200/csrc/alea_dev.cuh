@@ -50,6 +50,10 @@ struct DevTerm {
     double gamma, L, alpha1;
     int ncoef;
     double dc[16];
+    // kind 2, zero-energy: s = (p-2)/2, kappa, R_m, r_c, matching constants,
+    // Chebyshev coefficients of sqrt(x) e^x K_{0,1}(x) in 4/x - 1 (2 x 24)
+    double ze_s, ze_kappa, ze_rm, ze_rc, ze_c3, ze_logc1, ze_logc2;
+    const double* ze_cheb;
 };
 
 struct DevBlock {
@@ -94,6 +98,12 @@ struct DevSys {
     int ncoul;
     int coul[kMaxCoulomb][4];
     double coul_coef[kMaxCoulomb];
+    // inverse-power pair potentials C r^-p (integer p <= 16 by products, else pow)
+    int nip;
+    int ip[kMaxCoulomb][4];
+    double ip_c[kMaxCoulomb], ip_p[kMaxCoulomb];
+    int ip_pint[kMaxCoulomb];
+    double ip_tail;
     // record layout (doubles): hot part [0, hot) is staged in shared memory
     long rec;                 // record stride
     int hot;
@@ -206,9 +216,75 @@ __device__ __forceinline__ void poly_acc(const double* c, int n, double r, doubl
     }
 }
 
+// e^x K0(x) and e^x K1(x), x > 0: the ascending series for x <= 2 (DLMF
+// 10.31.1-2, 15 terms), else the Chebyshev series of sqrt(x) e^x K_nu(x) in
+// ξ = 4/x - 1 summed by Clenshaw's recurrence (24 terms per order).
+__device__ __forceinline__ void bessel_k01e(const double* cheb, double x, double& k0e, double& k1e) {
+    if (x <= 2.0) {
+        const double euler_gamma = 0.57721566490153286060651209008240243;
+        const double y = 0.25 * x * x;
+        double term0 = 1.0, term1 = 1.0, harmonic = 0.0;
+        double i0 = 0.0, s0 = 0.0, i1 = 0.0, s1 = 0.0;
+        for (int k = 0; k < 15; ++k) {
+            if (k > 0) {
+                term0 *= y / (static_cast<double>(k) * k);
+                term1 *= y / (static_cast<double>(k) * (k + 1));
+                harmonic += 1.0 / k;
+            }
+            const double harmonic_next = harmonic + 1.0 / (k + 1);
+            i0 += term0;
+            s0 += harmonic * term0;
+            i1 += term1;
+            s1 += (harmonic + harmonic_next - 2.0 * euler_gamma) * term1;
+        }
+        const double lh = log(0.5 * x);
+        const double k0 = -(lh + euler_gamma) * i0 + s0;
+        const double k1 = 1.0 / x + lh * (0.5 * x * i1) - 0.25 * x * s1;
+        const double ex = exp(x);
+        k0e = ex * k0;
+        k1e = ex * k1;
+        return;
+    }
+    const double xi = 4.0 / x - 1.0, two_xi = 2.0 * xi;
+    double b0 = 0.0, b0p = 0.0, b1 = 0.0, b1p = 0.0;
+    for (int k = 23; k >= 1; --k) {
+        const double t0 = two_xi * b0 - b0p + __ldg(cheb + k);
+        const double t1 = two_xi * b1 - b1p + __ldg(cheb + 24 + k);
+        b0p = b0;
+        b0 = t0;
+        b1p = b1;
+        b1 = t1;
+    }
+    const double isx = 1.0 / sqrt(x);
+    k0e = (xi * b0 - b0p + __ldg(cheb)) * isx;
+    k1e = (xi * b1 - b1p + __ldg(cheb + 24)) * isx;
+}
+
 // u, u', u'' of a pair term at r (the short-range half for an image sum).
 __device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, double& du,
                                        double& d2u) {
+    if (T.kind == 2) {
+        if (r < T.ze_rm) {   // ln[C1 K0(κ r^-s)]
+            const double x = T.ze_kappa * pow(r, -T.ze_s);
+            double k0e, k1e;
+            bessel_k01e(T.ze_cheb, x, k0e, k1e);
+            const double q = k1e / k0e;
+            const double sx = T.ze_s * x;
+            u = log(k0e) - x + T.ze_logc1;
+            du = sx * q / r;
+            d2u = sx / (r * r) * (sx * (1.0 - q) * (1.0 + q) - q);
+            return;
+        }
+        const double rr = fmin(r, T.ze_rc);
+        const double inv_r = 1.0 / rr;
+        const double inv_c = 1.0 / (2.0 * T.ze_rc - rr);
+        const double m = (r < T.ze_rc) ? 1.0 : 0.0;
+        const double a = T.ze_c3;
+        u = m * (T.ze_logc2 - a * inv_r - a * inv_c);
+        du = m * (a * inv_r * inv_r - a * inv_c * inv_c);
+        d2u = m * (-2.0 * a * inv_r * inv_r * inv_r - 2.0 * a * inv_c * inv_c * inv_c);
+        return;
+    }
     if (T.kind == 0) {
         double p = 0.0, dp = 0.0, d2p = 0.0;
         poly_acc(T.coef, T.nnum, r, p, dp, d2p);

@@ -735,8 +735,29 @@ __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs
             acc[0] += s.coul_coef[c] / r;
         }
     }
+    // C r^-p at the minimum image (the continuum tail is a constant below)
+    for (int c = 0; c < s.nip; ++c) {
+        const int af = s.ip[c][0], al = s.ip[c][1], bf = s.ip[c][2], bl = s.ip[c][3];
+        const bool same = af == bf && al == bl;
+        const int na = al - af, nb = bl - bf;
+        const int tot = same ? na * na : na * nb;
+        for (int q = threadIdx.x; q < tot; q += NT) {
+            const int i = af + q / (same ? na : nb), j = (same ? af : bf) + q % (same ? na : nb);
+            if (same && j <= i) continue;
+            double del[3];
+            const double r = fold_dist(s, v.pos + i * 2, v.pos + j * 2, del);
+            if (s.ip_pint[c] > 0) {
+                const double inv_r = 1.0 / r;
+                double inv_rp = inv_r;
+                for (int k = 1; k < s.ip_pint[c]; ++k) inv_rp *= inv_r;
+                acc[0] += s.ip_c[c] * inv_rp;
+            } else {
+                acc[0] += s.ip_c[c] * pow(r, -s.ip_p[c]);
+            }
+        }
+    }
     block_sum<NT>(acc, v.red);
-    return acc[0] + (s.ewald ? s.e_const : 0.0);
+    return acc[0] + (s.ewald ? s.e_const : 0.0) + s.ip_tail;
 }
 
 // ───────────────────────── full evaluation ──────────────────────────────

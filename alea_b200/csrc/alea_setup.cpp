@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <functional>
+#include <limits>
 #include <memory>
 #include <random>
 #include <stdexcept>
@@ -534,6 +535,35 @@ Cell make_cell(double lx, double ly) {
     return make_cell(a);
 }
 
+// ∫ outside the Wigner-Seitz cell of a radial function, as ∮ dθ f(ρ(θ)) with
+// ρ(θ) = min over lattice translations L (u·L > 0) of |L|²/(2 u·L), by a
+// 2^18-point midpoint rule in θ (its error comes only from the cell's
+// corners, ~1e-10 relative).  f(ρ) = ∫_ρ^∞ v(r) r dr is the caller's tail.
+template <class F>
+double ws_exterior_integral(const Cell& c, F&& f) {
+    std::vector<double> lx, ly;
+    for (int s = -2; s <= 2; ++s)
+        for (int t = -2; t <= 2; ++t) {
+            if (s == 0 && t == 0) continue;
+            lx.push_back(s * c.a[0] + t * c.a[2]);
+            ly.push_back(s * c.a[1] + t * c.a[3]);
+        }
+    constexpr size_t n_theta = size_t{1} << 18;
+    const double dtheta = kTwoPi / static_cast<double>(n_theta);
+    double sum = 0.0;
+    for (size_t k = 0; k < n_theta; ++k) {
+        const double theta = (static_cast<double>(k) + 0.5) * dtheta;
+        const double ux = std::cos(theta), uy = std::sin(theta);
+        double rho = std::numeric_limits<double>::infinity();
+        for (size_t q = 0; q < lx.size(); ++q) {
+            const double proj = ux * lx[q] + uy * ly[q];
+            if (proj > 0.0) rho = std::min(rho, 0.5 * (lx[q] * lx[q] + ly[q] * ly[q]) / proj);
+        }
+        sum += f(rho);
+    }
+    return sum * dtheta;
+}
+
 // The first `want` real plane waves of closed reciprocal shells (k = 0 gives
 // one cosine, every ±k pair a cosine and a sine).
 void plane_wave_shells(const Cell& c, int want, std::vector<double>& k, std::vector<int>& is_sin) {
@@ -830,6 +860,34 @@ void write_json(alea_gpu_setup* S, const std::string& kind, double ewald_self, d
         j.close('}');
     }
     j.close(']');
+    j.key("zero_energy");
+    j.open('[');
+    for (int t = 0; t < y.n_terms; ++t) {
+        const alea_gpu_pair_term& T = y.terms[t];
+        if (T.kind != ALEA_PAIR_ZERO_ENERGY) continue;
+        j.open('{');
+        j.arr("ga", std::vector<int>{T.pairs[0][0], T.pairs[0][1]});
+        j.arr("gb", std::vector<int>{T.pairs[0][2], T.pairs[0][3]});
+        j.kv("b", T.ze_b);
+        j.kv("exponent", T.ze_exponent);
+        j.kv("matching_radius", T.ze_matching_radius);
+        j.kv("cutoff", T.ze_cutoff);
+        j.close('}');
+    }
+    j.close(']');
+    j.key("inverse_power");
+    j.open('[');
+    for (int k = 0; k < y.n_inverse_power; ++k) {
+        const alea_gpu_inverse_power& V = y.inverse_power[k];
+        j.open('{');
+        j.arr("ga", std::vector<int>{V.a_first, V.a_last});
+        j.arr("gb", std::vector<int>{V.b_first, V.b_last});
+        j.kv("strength", V.strength);
+        j.kv("exponent", V.exponent);
+        j.kv("tail", V.tail);
+        j.close('}');
+    }
+    j.close(']');
     if (!S->anchors.empty()) {
         j.arr("anchors", S->anchors);
         j.kv("jitter", S->jitter);
@@ -1062,6 +1120,62 @@ int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* cou
         double self = 0.0, bg = 0.0;
         add_ewald(S, c, ewald_tol > 0.0 ? ewald_tol : 1e-6, self, bg);
         write_json(S, "charges", self, bg);
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        delete S;
+        return ALEA_ERR_INVALID;
+    }
+    *out = S;
+    return ALEA_OK;
+}
+
+// 2-D dipolar bosons (the reference's configs/dipoles_2d_gas_n256.yaml
+// shape): n bosons of mass 1 in a hexagonal cell of area n π rs²
+// (app.cpp:314-330), C r^-p at the minimum image plus the continuum tail
+// outside the Wigner-Seitz cell (inverse_power.cpp:28-80), and the
+// zero-energy Jastrow with b = 2 μ C, μ = 1/2, cut off at the Wigner-Seitz
+// inradius (builders/jastrow.cpp:202-260).  Initial walkers: uniform.
+int alea_gpu_setup_dipoles2d(int n, double rs, double strength, double exponent, double matching_radius,
+                             alea_gpu_setup** out, char* err, size_t err_len) {
+    if (!out) return ALEA_ERR_INVALID;
+    *out = nullptr;
+    auto* S = new alea_gpu_setup();
+    try {
+        if (n < 2 || !(rs > 0.0) || !(exponent > 2.0) || !(strength > 0.0))
+            throw std::invalid_argument("dipoles2d: needs n >= 2, rs > 0, strength > 0, exponent > 2");
+        alea_gpu_system& y = S->sys;
+        y.dim = 2;
+        y.n_particles = n;
+        y.periodic = 1;
+        const double area = n * kPi * rs * rs;
+        const double L = std::sqrt(2.0 * area / std::sqrt(3.0));
+        const double lat[4] = {L, 0.0, 0.5 * L, L * std::sqrt(3.0) / 2.0};
+        const Cell c = make_cell(lat);
+        std::copy(c.a, c.a + 4, y.lattice);
+        add_group(y, 0, n, 0.0);
+        if (!(matching_radius > 0.0 && matching_radius < c.ws))
+            throw std::invalid_argument("dipoles2d: the matching radius must lie inside (0, r_WS = " +
+                                        std::to_string(c.ws) + ")");
+        alea_gpu_pair_term& T = y.terms[y.n_terms++];
+        T.kind = ALEA_PAIR_ZERO_ENERGY;
+        T.n_pairs = 1;
+        T.pairs[0][0] = T.pairs[0][2] = 0;
+        T.pairs[0][1] = T.pairs[0][3] = n;
+        T.ze_b = 2.0 * 0.5 * strength;
+        T.ze_exponent = exponent;
+        T.ze_matching_radius = matching_radius;
+        T.ze_cutoff = c.ws;
+        alea_gpu_inverse_power& V = y.inverse_power[y.n_inverse_power++];
+        V.a_first = V.b_first = 0;
+        V.a_last = V.b_last = n;
+        V.strength = strength;
+        V.exponent = exponent;
+        const double outside =
+            ws_exterior_integral(c, [&](double rho) { return std::pow(rho, 2.0 - exponent); }) /
+            (exponent - 2.0);
+        const double pairs = 0.5 * static_cast<double>(n) * static_cast<double>(n);
+        V.tail = pairs / c.area * strength * outside;
+        write_json(S, "dipoles", 0.0, 0.0);
     } catch (const std::exception& e) {
         if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
         delete S;

@@ -79,6 +79,12 @@ def charges2d(lattice, counts, charges, ewald_tol: float = 1e-6) -> Setup:
                  cnt.ctypes.data_as(_capi.c_ip), q.ctypes.data_as(_capi.c_dp), ewald_tol)
 
 
+def dipoles2d(n: int, rs: float, strength: float = 1.0, exponent: float = 3.0,
+              matching_radius: float = 0.0459) -> Setup:
+    """2-D dipolar bosons: zero-energy Jastrow, C/r^p with its continuum tail."""
+    return _make("alea_gpu_setup_dipoles2d", n, rs, strength, exponent, matching_radius)
+
+
 def exciton2d(L_init: float = 1.0) -> Setup:
     """Open 2-D exciton with the exact trial function (E = -1)."""
     lib = _capi.load()

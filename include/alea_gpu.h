@@ -57,7 +57,7 @@ enum {
 };
 
 enum { ALEA_ORB_PLANE_WAVE = 0, ALEA_ORB_GAUSSIAN = 1 };
-enum { ALEA_PAIR_PADE = 0, ALEA_PAIR_DRUMMOND = 1 };
+enum { ALEA_PAIR_PADE = 0, ALEA_PAIR_DRUMMOND = 1, ALEA_PAIR_ZERO_ENERGY = 2 };
 
 #define ALEA_GPU_MAX_GROUPS 8
 #define ALEA_GPU_MAX_BLOCKS 4
@@ -119,6 +119,12 @@ typedef struct {
     double gamma, L;                        /* Drummond cusp and cutoff */
     int n_coeffs;
     double dcoeffs[16];                     /* Drummond [alpha_0, alpha_2..alpha_N] */
+    /* zero-energy pair function on one group pair
+       (src/wavefunction/zero_energy_jastrow.h:16-55): C1 K0(kappa r^-s) inside
+       the matching radius, C2 exp(-C3/r - C3/(2 r_c - r)) up to the cutoff */
+    double ze_b;                            /* 2 mu C of the pair's C/r^p core */
+    double ze_exponent;                     /* p > 2 */
+    double ze_matching_radius, ze_cutoff;
 } alea_gpu_pair_term;
 
 /* 2-D Ewald sum of the Coulomb interaction (src/hamiltonian/ewald_term.h). */
@@ -137,6 +143,14 @@ typedef struct {
     double coef;                  /* q_a q_b / epsilon */
 } alea_gpu_coulomb;
 
+/* C / r^p between two groups at the minimum image, plus the continuum tail
+ * of the images outside the Wigner-Seitz cell (src/hamiltonian/inverse_power.h). */
+typedef struct {
+    int a_first, a_last, b_first, b_last;
+    double strength, exponent;
+    double tail;                  /* constant added to every configuration */
+} alea_gpu_inverse_power;
+
 typedef struct {
     int dim;                      /* 2 (3 for open cells) */
     int n_particles;
@@ -152,6 +166,8 @@ typedef struct {
     alea_gpu_ewald ewald;
     int n_coulomb;
     alea_gpu_coulomb coulomb[ALEA_GPU_MAX_COULOMB];
+    int n_inverse_power;
+    alea_gpu_inverse_power inverse_power[ALEA_GPU_MAX_COULOMB];
 } alea_gpu_system;
 
 typedef struct alea_gpu_ctx alea_gpu_ctx;
@@ -328,6 +344,11 @@ int alea_gpu_setup_crystal2d(int nx, int ny, double rs, double gauss_c, double a
  * energy (src/hamiltonian/ewald_term.cpp:368-612). */
 int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* counts, const double* charges,
                              double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len);
+/* 2-D dipolar bosons: n of mass 1 in a hexagonal cell at density rs, C/r^p
+ * (strength, exponent) with its continuum tail, and the zero-energy Jastrow
+ * with the given matching radius, cut off at the Wigner-Seitz inradius. */
+int alea_gpu_setup_dipoles2d(int n, double rs, double strength, double exponent, double matching_radius,
+                             alea_gpu_setup** out, char* err, size_t err_len);
 /* Open 2-D exciton with the exact trial function (E = -1). */
 int alea_gpu_setup_exciton2d(double L_init, alea_gpu_setup** out);
 const alea_gpu_system* alea_gpu_setup_system(const alea_gpu_setup* s);

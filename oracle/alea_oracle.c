@@ -197,6 +197,10 @@ typedef struct {
     int nk, m1, m2; const double *n1, *n2, *kx, *ky, *w; double *kx2, *ky2;
     int C; double gamma, L, alpha1; int ncoef; double dc[16];
     int n_cached;                  /* k-space phase-cache rows */
+    /* kind 2, zero-energy (zero_energy_jastrow.cpp): s, kappa, R_m, r_c and the
+       matching constants; Chebyshev coefficients of sqrt(x) e^x K_{0,1}(x) */
+    double ze_s, ze_kappa, ze_rm, ze_rc, ze_c3, ze_logc1, ze_logc2;
+    const double* ze_cheb;         /* [2 * 24]: order 0, then order 1 */
 } term_t;
 
 typedef struct {
@@ -218,6 +222,10 @@ typedef struct {
     int ewald; spline_t esp; double e_rcut, e_inv_eps, e_const; int enk, en1max, en2max;
     const double *en1, *en2, *ew;
     int ncoul; int coul[MAXC][4]; double coul_coef[MAXC];
+    /* inverse-power pair terms (inverse_power.cpp): pair ranges, C, p, integer p
+       (0 when not a small integer), and the sum of their continuum tails */
+    int nip; int ip[MAXC][4]; double ip_c[MAXC], ip_p[MAXC]; int ip_pint[MAXC];
+    double ip_tail;
     /* walker layout (offsets into one walker's double record) */
     long W, o_pos, o_dist, o_grad, o_lap, o_scal, o_lpc, o_gc, o_lc;
     long o_A[MAXB], o_D[MAXB], o_Dg[MAXB], o_Dl[MAXB], o_rabs[MAXB], o_bs[MAXB];
@@ -379,6 +387,61 @@ static double fold_dist(const sys_t* s, const double* xi, const double* xj, doub
     return sqrt(r2);
 }
 
+/* e^x K0(x), e^x K1(x) for x > 0 (numerics/scaled_bessel_k01.h): the ascending
+ * series (DLMF 10.31.1-2) for x <= 2, else the Chebyshev series in 4/x - 1 of
+ * sqrt(x) e^x K_nu(x), summed by Clenshaw's recurrence. */
+static void k01e(const double* cheb, double x, double* k0e, double* k1e) {
+    if (x <= 2.0) {
+        const double euler_gamma = 0.57721566490153286060651209008240243;
+        const double y = 0.25 * x * x;
+        double term0 = 1.0, term1 = 1.0, harmonic = 0.0;
+        double i0 = 0.0, s0 = 0.0, i1 = 0.0, s1 = 0.0;
+        for (int k = 0; k < 15; ++k) {
+            if (k > 0) {
+                term0 *= y / ((double)k * k);
+                term1 *= y / ((double)k * (k + 1));
+                harmonic += 1.0 / k;
+            }
+            const double harmonic_next = harmonic + 1.0 / (k + 1);
+            i0 += term0;
+            s0 += harmonic * term0;
+            i1 += term1;
+            s1 += (harmonic + harmonic_next - 2.0 * euler_gamma) * term1;
+        }
+        const double lh = log(0.5 * x);
+        const double k0 = -(lh + euler_gamma) * i0 + s0;
+        const double k1 = 1.0 / x + lh * (0.5 * x * i1) - 0.25 * x * s1;
+        const double ex = exp(x);
+        *k0e = ex * k0;
+        *k1e = ex * k1;
+        return;
+    }
+    const double xi = 4.0 / x - 1.0, two_xi = 2.0 * xi;
+    double b0 = 0.0, b0p = 0.0, b1 = 0.0, b1p = 0.0;
+    for (int k = 23; k >= 1; --k) {
+        const double t0 = two_xi * b0 - b0p + cheb[k];
+        const double t1 = two_xi * b1 - b1p + cheb[24 + k];
+        b0p = b0; b0 = t0;
+        b1p = b1; b1 = t1;
+    }
+    const double isx = 1.0 / sqrt(x);
+    *k0e = (xi * b0 - b0p + cheb[0]) * isx;
+    *k1e = (xi * b1 - b1p + cheb[24]) * isx;
+}
+
+/* u0 = ln K0(kappa r^-s) and its r-derivatives (ZeroEnergyFunction::
+ * zero_energy_solution). */
+static void ze_solution(const term_t* T, double r, double* u0, double* du0, double* d2u0) {
+    const double x = T->ze_kappa * pow(r, -T->ze_s);
+    double k0e, k1e;
+    k01e(T->ze_cheb, x, &k0e, &k1e);
+    const double q = k1e / k0e;
+    const double sx = T->ze_s * x;
+    *u0 = log(k0e) - x;
+    *du0 = sx * q / r;
+    *d2u0 = sx / (r * r) * (sx * (1.0 - q) * (1.0 + q) - q);
+}
+
 /*
  * Blob layout (all float64; integers stored exactly):
  *   dim, np, periodic, vectors[dim*dim]
@@ -390,8 +453,10 @@ static double fold_dist(const sys_t* s, const double* xi, const double* xj, doub
  *                    image != 0: spline(r_cut, inv_delta, n_knots, scaled[3 n]),
  *                                u_inf, nk, n1[nk], n2[nk], kx[nk], ky[nk], w[nk]
  *     kind 1 (Drummond): npairs, pairs[4*npairs], C, gamma, L, ncoef, coef[ncoef]
+ *     kind 2 (zero-energy): npairs(=1), pair[4], b, exponent, R_m, r_c, cheb[48]
  *   ewald; if ewald: spline, r_cut, inv_eps, constant, nk, n1, n2, w
  *   ncoul; per term: pair[4], coef (q_a q_b / eps)
+ *   nip; per term: pair[4], strength, exponent, tail   (optional: absent = 0)
  */
 static int blob_read(sys_t* s, const double* blob, long n) {
     rd_t r = {blob, n, 0, 0};
@@ -470,6 +535,21 @@ static int blob_read(sys_t* s, const double* blob, long n) {
                 T->n_cached = (T->pairs[0][1] - T->pairs[0][0]) +
                               (same ? 0 : T->pairs[0][3] - T->pairs[0][2]);
             }
+        } else if (T->kind == 2) {
+            const double b = rd(&r), p = rd(&r);
+            T->ze_rm = rd(&r);
+            T->ze_rc = rd(&r);
+            T->ze_cheb = rdv(&r, 48);
+            T->ze_s = 0.5 * (p - 2.0);
+            T->ze_kappa = sqrt(b) / T->ze_s;
+            /* matching at R_m: u, u' continuous, u(r_c) = 0 */
+            double u0, du0, d2u0;
+            ze_solution(T, T->ze_rm, &u0, &du0, &d2u0);
+            const double c = 2.0 * T->ze_rc - T->ze_rm;
+            const double h = 1.0 / (T->ze_rm * T->ze_rm) - 1.0 / (c * c);
+            T->ze_c3 = du0 / h;
+            T->ze_logc2 = 2.0 * T->ze_c3 / T->ze_rc;
+            T->ze_logc1 = T->ze_logc2 - T->ze_c3 / T->ze_rm - T->ze_c3 / c - u0;
         } else {
             T->C = (int)rd(&r);
             T->gamma = rd(&r);
@@ -502,6 +582,20 @@ static int blob_read(sys_t* s, const double* blob, long n) {
     for (int c = 0; c < s->ncoul; ++c) {
         for (int k = 0; k < 4; ++k) s->coul[c][k] = (int)rd(&r);
         s->coul_coef[c] = rd(&r);
+    }
+    s->nip = 0;
+    s->ip_tail = 0.0;
+    if (r.i < r.n) {
+        s->nip = (int)rd(&r);
+        if (s->nip > MAXC) return -8;
+        for (int c = 0; c < s->nip; ++c) {
+            for (int k = 0; k < 4; ++k) s->ip[c][k] = (int)rd(&r);
+            s->ip_c[c] = rd(&r);
+            s->ip_p[c] = rd(&r);
+            s->ip_tail += rd(&r);
+            const double rp = nearbyint(s->ip_p[c]);
+            s->ip_pint[c] = (rp == s->ip_p[c] && rp <= 16.0) ? (int)rp : 0;
+        }
     }
     return r.bad ? -7 : 0;
 }
@@ -656,6 +750,22 @@ static void radial(const term_t* T, double r, double* u, double* du, double* d2u
             *du -= df;
             *d2u -= d2f;
         }
+        return;
+    }
+    if (T->kind == 2) {   /* ZeroEnergyFunction::evaluate */
+        if (r < T->ze_rm) {
+            ze_solution(T, r, u, du, d2u);
+            *u += T->ze_logc1;
+            return;
+        }
+        const double rr = r < T->ze_rc ? r : T->ze_rc;
+        const double inv_r = 1.0 / rr;
+        const double inv_c = 1.0 / (2.0 * T->ze_rc - rr);
+        const double m = (r < T->ze_rc) ? 1.0 : 0.0;
+        const double a = T->ze_c3;
+        *u = m * (T->ze_logc2 - a * inv_r - a * inv_c);
+        *du = m * (a * inv_r * inv_r - a * inv_c * inv_c);
+        *d2u = m * (-2.0 * a * inv_r * inv_r * inv_r - 2.0 * a * inv_c * inv_c * inv_c);
         return;
     }
     /* Drummond–Towler–Needs, drummond_jastrow.cpp eval_one */
@@ -1142,6 +1252,24 @@ static double local_energy(const sys_t* s, const double* w) {
                 le += s->coul_coef[c] / sqrt(r * r + 0.0);
             }
     }
+    /* InversePowerTerm::evaluate_potential: C r^-p at the minimum image, plus tail */
+    for (int c = 0; c < s->nip; ++c) {
+        const int af = s->ip[c][0], al = s->ip[c][1], bf = s->ip[c][2], bl = s->ip[c][3];
+        const int same = af == bf && al == bl;
+        for (int i = af; i < al; ++i)
+            for (int j = same ? i + 1 : bf; j < (same ? al : bl); ++j) {
+                const double r = dist[i * np + j];
+                if (s->ip_pint[c] > 0) {
+                    const double inv_r = 1.0 / r;
+                    double inv_rp = inv_r;
+                    for (int k = 1; k < s->ip_pint[c]; ++k) inv_rp *= inv_r;
+                    le += s->ip_c[c] * inv_rp;
+                } else {
+                    le += s->ip_c[c] * pow(r, -s->ip_p[c]);
+                }
+            }
+    }
+    le += s->ip_tail;
     return le;
 }
 

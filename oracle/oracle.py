@@ -99,6 +99,11 @@ def blob_from_setup(sd: Dict[str, Any]) -> np.ndarray:
             t += list(pr)
         t += [d["C"], d["gamma"], d["L"], len(d["coeffs"])] + list(d["coeffs"])
         terms.append(t)
+    for z in sd.get("zero_energy", []):
+        t = [2, 1, z["ga"][0], z["ga"][1], z["gb"][0], z["gb"][1], z["b"], z["exponent"],
+             z["matching_radius"], z["cutoff"]]
+        t += list(bessel_k01_chebyshev())
+        terms.append(t)
     out.append(len(terms))
     for t in terms:
         out += t
@@ -115,7 +120,30 @@ def blob_from_setup(sd: Dict[str, Any]) -> np.ndarray:
     out.append(len(cl))
     for c in cl:
         out += [c["ga"][0], c["ga"][1], c["gb"][0], c["gb"][1], c["coef"]]
+    ip = sd.get("inverse_power", [])
+    out.append(len(ip))
+    for c in ip:
+        out += [c["ga"][0], c["ga"][1], c["gb"][0], c["gb"][1], c["strength"], c["exponent"], c["tail"]]
     return np.asarray(out, dtype=np.float64)
+
+
+def bessel_k01_chebyshev(terms: int = 24) -> np.ndarray:
+    """Chebyshev coefficients of sqrt(x) e^x K_nu(x), nu = 0, 1, in xi = 4/x - 1
+    (numerics/scaled_bessel_k01.h: projection on 8 x terms first-kind nodes),
+    from scipy's k0e/k1e.  Order 0 in [0, terms), order 1 in [terms, 2 terms)."""
+    from scipy.special import k0e, k1e
+    m = 8 * terms
+    theta = np.pi * (np.arange(m) + 0.5) / m
+    x = 4.0 / (np.cos(theta) + 1.0)
+    f0 = np.sqrt(x) * k0e(x)
+    f1 = np.sqrt(x) * k1e(x)
+    c = np.zeros(2 * terms)
+    for k in range(terms):
+        ck = np.cos(k * theta)
+        norm = (1.0 if k == 0 else 2.0) / m
+        c[k] = norm * np.sum(f0 * ck)
+        c[terms + k] = norm * np.sum(f1 * ck)
+    return c
 
 
 class Oracle:

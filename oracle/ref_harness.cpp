@@ -31,6 +31,7 @@
 
 #include "hamiltonian/coulomb.h"
 #include "hamiltonian/ewald_term.h"
+#include "hamiltonian/inverse_power.h"
 #include "hamiltonian/hamiltonian.h"
 #include "hamiltonian/kinetic.h"
 #include "numerics/long_range_breakup.h"
@@ -47,6 +48,7 @@
 #include "wavefunction/pade_jastrow.h"
 #include "wavefunction/slater_determinant.h"
 #include "wavefunction/trial_wavefunction.h"
+#include "wavefunction/zero_energy_jastrow.h"
 
 using namespace alea;
 
@@ -499,11 +501,74 @@ std::unique_ptr<System> build_exciton(const Args& a) {
     return s;
 }
 
+// 2D dipolar bosons (configs/dipoles_2d_gas_n256.yaml shape): n bosons of
+// mass 1 in a hexagonal cell of area n π rs² (app.cpp:314-330), C/r^p at the
+// minimum image plus the continuum tail (InversePowerTerm), and the
+// zero-energy Jastrow with b = 2 μ C (μ = 1/2) and r_c = the Wigner-Seitz
+// inradius (builders/jastrow.cpp:202-260).  Initial positions: uniform.
+std::unique_ptr<System> build_dipoles(const Args& a) {
+    auto s = std::make_unique<System>();
+    s->kind = "dipoles";
+    const std::size_t n = static_cast<std::size_t>(geti(a, "n", 64));
+    const double rs = getd(a, "rs", 0.03526184897173477);
+    const double C = getd(a, "strength", 1.0);
+    const double p = getd(a, "exponent", 3.0);
+    const double rm = getd(a, "rm", 0.0459);
+    const double pi = 3.14159265358979323846;
+    s->dim = 2;
+    s->np = n;
+    const double area = static_cast<double>(n) * pi * rs * rs;
+    const double L = std::sqrt(2.0 * area / std::sqrt(3.0));
+    const std::vector<double> vec{L, 0.0, 0.5 * L, L * std::sqrt(3.0) / 2.0};
+    s->cell = SimulationCell(2, vec);
+    s->groups.push_back(make_group("dipoles", 0, n, 0.0, 2));
+    s->ham.add_component(std::make_unique<Kinetic>(s->groups));
+    auto ip = std::make_unique<InversePowerTerm>(s->groups[0], s->groups[0], C, p, s->cell);
+    const double tail = ip->tail_energy();
+    s->ham.add_component(std::move(ip));
+    const double b = 2.0 * 0.5 * C;
+    const double rc = s->cell.ws_radius();
+    std::vector<Parameter> params{Parameter{"matching_radius", rm, true}};
+    s->psi.add_component(
+        std::make_unique<ZeroEnergyJastrow>(b, p, rc, s->groups[0], s->groups[0], params));
+    Json& j = s->setup;
+    j.open('{');
+    j.ks("kind", "dipoles");
+    j.ki("dim", 2);
+    j.ki("np", static_cast<long long>(n));
+    dump_cell(j, s->cell);
+    dump_groups(j, s->groups);
+    j.key("zero_energy");
+    j.open('[');
+    j.open('{');
+    j.arr("ga", std::vector<double>{0, double(n)});
+    j.arr("gb", std::vector<double>{0, double(n)});
+    j.kv("b", b);
+    j.kv("exponent", p);
+    j.kv("matching_radius", rm);
+    j.kv("cutoff", rc);
+    j.close('}');
+    j.close(']');
+    j.key("inverse_power");
+    j.open('[');
+    j.open('{');
+    j.arr("ga", std::vector<double>{0, double(n)});
+    j.arr("gb", std::vector<double>{0, double(n)});
+    j.kv("strength", C);
+    j.kv("exponent", p);
+    j.kv("tail", tail);
+    j.close('}');
+    j.close(']');
+    j.close('}');
+    return s;
+}
+
 std::unique_ptr<System> build_system(const Args& a) {
     const std::string k = gets(a, "system", "heg");
     if (k == "heg") return build_heg(a);
     if (k == "crystal") return build_crystal(a);
     if (k == "exciton") return build_exciton(a);
+    if (k == "dipoles") return build_dipoles(a);
     throw std::runtime_error("unknown system " + k);
 }
 

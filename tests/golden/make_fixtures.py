@@ -35,16 +35,19 @@ SYSTEMS = {
     "heg10": dict(system="heg", nu=5, nd=5, rs=30),
     "crystal16": dict(system="crystal", nx=4, ny=4, rs=40),
     "heg42": dict(system="heg", nu=21, nd=21, rs=30),
+    "dipoles16": dict(system="dipoles", n=16),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
     "heg10": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=225.0),
     "heg10_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
     "crystal16": dict(nw=4, seed=17, eq=0, acc=2, steps=2, substeps=1, tau=400.0),
+    "dipoles16": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.0003),
 }
 DMC = {
     "exciton": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.05),
     "heg10": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
+    "dipoles16": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=1e-5),
 }
 
 
@@ -72,24 +75,32 @@ def dump(name, obj):
     print("wrote", name)
 
 
-def main():
+def main(only=None):
     for name, args in SYSTEMS.items():
+        if only and name not in only:
+            continue
         dump(f"setup_{name}.json", run_ref_harness("setup", **args))
         ev = run_ref_harness("eval", nw=4, seed=12345, **args)
         ev.pop("mode", None)
         dump(f"eval_{name}.json", ev)
     for name, run in VMC.items():
         sysname = name.split("_")[0]
+        if only and sysname not in only:
+            continue
         r = run_ref_harness("vmc", **run, **SYSTEMS[sysname])
         r["params"] = run
         r["system"] = sysname
         dump(f"vmc_{name}.json", r)
     for name, run in DMC.items():
+        if only and name not in only:
+            continue
         r = run_ref_harness("dmc", **run, **SYSTEMS[name])
         r["params"] = run
         r["system"] = name
         dump(f"dmc_{name}.json", r)
     for name, run in DMC_STAT.items():
+        if only and name not in only:
+            continue
         r = run_ref_harness("bench", method="dmc", **run, **SYSTEMS[name])
         n_acc_steps = run["acc"] * run["steps"]
         w = r["weight_sum"][-n_acc_steps:]
@@ -102,4 +113,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or None)   # optional system names: regenerate only those

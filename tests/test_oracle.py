@@ -12,7 +12,7 @@ from conftest import golden
 from oracle import Oracle
 from oracle.oracle import S_EL, S_LOGPSI, load_oracle_lib
 
-SYSTEMS = ["exciton", "heg10", "crystal16", "heg42"]
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16"]
 
 
 def rel(a, b):
@@ -69,7 +69,7 @@ def test_oracle_evaluate_matches_reference(name):
     assert np.max(np.abs(o.grad()[:4] - g_ref)) < 1e-9 * max(1.0, np.abs(g_ref).max())
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "heg10_drift", "crystal16"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "heg10_drift", "crystal16", "dipoles16"])
 def test_oracle_vmc_matches_reference(name):
     r = golden(f"vmc_{name}.json")
     p = r["params"]
@@ -89,7 +89,7 @@ def test_oracle_vmc_matches_reference(name):
         assert np.array_equal(o.pos()[: p["nw"]], fp)
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16"])
 def test_oracle_dmc_matches_reference(name):
     r = golden(f"dmc_{name}.json")
     p = r["params"]
