@@ -43,6 +43,7 @@
  * (oracle/_ref) by the tests.
  */
 #define _GNU_SOURCE
+#include <complex.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -204,8 +205,8 @@ typedef struct {
 } term_t;
 
 typedef struct {
-    int first, last, type;         /* type 0 plane waves, 1 Gaussians */
-    const double *k, *is_sin, *centers, *alphas;
+    int first, last, type;         /* type 0 plane waves, 1 Gaussians, 2 twisted plane waves */
+    const double *k, *is_sin, *centers, *alphas;   /* type 2: k holds q = k + θ */
 } block_t;
 
 typedef struct {
@@ -218,6 +219,7 @@ typedef struct {
     double* inv_mass;              /* [np*dim] */
     double* charge;                /* [np] */
     int nblocks; block_t blocks[MAXB];
+    int cplx;                      /* the determinant is complex (twisted plane waves) */
     int nterms; term_t terms[MAXT];
     int ewald; spline_t esp; double e_rcut, e_inv_eps, e_const; int enk, en1max, en2max;
     const double *en1, *en2, *ew;
@@ -228,6 +230,7 @@ typedef struct {
     double ip_tail;
     /* walker layout (offsets into one walker's double record) */
     long W, o_pos, o_dist, o_grad, o_lap, o_scal, o_lpc, o_gc, o_lc;
+    long o_pgrad, o_plap, o_pgc, o_plc;   /* phase planes (complex determinant) */
     long o_A[MAXB], o_D[MAXB], o_Dg[MAXB], o_Dl[MAXB], o_rabs[MAXB], o_bs[MAXB];
     long o_rho[MAXT], o_pc[MAXT];
     int ncomp;
@@ -235,7 +238,8 @@ typedef struct {
 } sys_t;
 
 /* scalars of a walker record, at o_scal */
-enum { S_LOGPSI, S_EL, S_WEIGHT, S_EPREV, S_RRP, S_RRA, S_AGE, S_ID, S_PARENT, S_ERR, S_NSCAL };
+enum { S_LOGPSI, S_EL, S_WEIGHT, S_EPREV, S_RRP, S_RRA, S_AGE, S_ID, S_PARENT, S_ERR, S_ELI,
+       S_NSCAL };
 
 /* blob reader */
 typedef struct { const double* p; long n, i; int bad; } rd_t;
@@ -447,7 +451,8 @@ static void ze_solution(const term_t* T, double r, double* u0, double* du0, doub
  *   dim, np, periodic, vectors[dim*dim]
  *   ngroups; per group: first, last, charge, inv_mass[dim]
  *   nblocks; per block: first, last, type,
- *            type 0: k[n*dim], is_sin[n];  type 1: centers[n*dim], alphas[n]
+ *            type 0: k[n*dim], is_sin[n];  type 1: centers[n*dim], alphas[n];
+ *            type 2: q[n*dim] (twisted plane waves; every block then type 2)
  *   nterms; per term: kind,
  *     kind 0 (Padé): npairs(=1), pair[4], nnum, nden, coef[nnum+nden], image,
  *                    image != 0: spline(r_cut, inv_delta, n_knots, scaled[3 n]),
@@ -494,6 +499,9 @@ static int blob_read(sys_t* s, const double* blob, long n) {
         if (B->type == 0) {
             B->k = rdv(&r, (long)nb * s->dim);
             B->is_sin = rdv(&r, nb);
+        } else if (B->type == 2) {
+            B->k = rdv(&r, (long)nb * s->dim);
+            s->cplx = 1;
         } else {
             B->centers = rdv(&r, (long)nb * s->dim);
             B->alphas = rdv(&r, nb);
@@ -612,9 +620,13 @@ static void layout(sys_t* s) {
     s->o_lpc = o; o += s->ncomp;
     s->o_gc = o; o += s->ncomp * np * dim;
     s->o_lc = o; o += s->ncomp * np * dim;
+    s->o_pgrad = o; o += s->cplx ? np * dim : 0;
+    s->o_plap = o; o += s->cplx ? np * dim : 0;
+    s->o_pgc = o; o += s->cplx ? np * dim : 0;
+    s->o_plc = o; o += s->cplx ? np * dim : 0;
     for (int b = 0; b < s->nblocks; ++b) {
         const long N = s->blocks[b].last - s->blocks[b].first;
-        s->o_A[b] = o; o += N * N;
+        s->o_A[b] = o; o += (s->cplx ? 2 : 1) * N * N;
         s->o_D[b] = o; o += N * N;
         s->o_Dg[b] = o; o += N * N * dim;
         s->o_Dl[b] = o; o += N * N * dim;
@@ -661,7 +673,8 @@ void o_layout(void* p, long* out) {
     const sys_t* s = p;
     out[0] = s->W; out[1] = s->o_pos; out[2] = s->o_dist; out[3] = s->o_grad;
     out[4] = s->o_lap; out[5] = s->o_scal; out[6] = s->o_lpc; out[7] = s->o_gc;
-    out[8] = s->o_lc; out[9] = s->ncomp;
+    out[8] = s->o_lc; out[9] = s->ncomp; out[10] = s->cplx ? s->o_pgrad : -1;
+    out[11] = s->cplx ? s->o_plap : -1;
 }
 
 /* ───────────────────────── radial functions ─────────────────────────── */
@@ -813,11 +826,11 @@ static void phases(const sys_t* s, const term_t* T, double x, double y, double* 
     const int M[2] = {T->m1, T->m2};
     const double th[2] = {th1, th2};
     double* R[2] = {e1r, e2r};
-    double* I[2] = {e1i, e2i};
+    double* Im[2] = {e1i, e2i};
     for (int q = 0; q < 2; ++q) {
         const int m = M[q];
         double* rr = R[q] + m;
-        double* ii = I[q] + m;
+        double* ii = Im[q] + m;
         const double cc = cos(th[q]), ss = sin(th[q]);
         rr[0] = 1.0;
         ii[0] = 0.0;
@@ -1008,7 +1021,7 @@ static void slater_evaluate(const sys_t* s, double* w) {
  * (slater_determinant.cpp:862-893). */
 static void slater_refresh(const sys_t* s, double* w, int p) {
     const int b = block_of(s, p);
-    if (b < 0) return;
+    if (b < 0 || s->cplx) return;   /* the complex determinant is eager */
     const block_t* B = &s->blocks[b];
     const int N = B->last - B->first, kr = p - B->first, dim = s->dim;
     const double* A = w + s->o_A[b];
@@ -1032,11 +1045,143 @@ static void slater_refresh(const sys_t* s, double* w, int p) {
     }
 }
 
+/* ───────────────────────── complex Slater determinant ─────────────────
+ * complex_slater_determinant.cpp: twisted plane waves φ_i = e^{i q_i·r}
+ * (complex_orbital_set.h TwistedPlaneWaveOrbitalSet), complex inverse per
+ * block stored as re[N²] then im[N²], A[m][c] = (D⁻¹)_{m,c}; ln|det| per
+ * block; the modulus part of ∇ln ψ, ∂²ln ψ in the component planes and the
+ * phase part in the phase planes.  Eager: every accepted move re-inverts the
+ * block and recomputes all its particles' derivatives (as the reference). */
+
+typedef double complex zc;
+
+static zc corb(const block_t* B, int i, int dim, const double* r) {
+    const double* q = B->k + i * dim;
+    double arg = 0.0;
+    for (int d = 0; d < dim; ++d) arg += q[d] * r[d];
+    return CMPLX(cos(arg), sin(arg));
+}
+
+/* Complex Gauss-Jordan inverse of M (rows kr) into Ar/Ai; ln|det|. */
+static double cgj(int N, const zc* M0, double* Ar, double* Ai, int* err) {
+    zc m[64 * 64], a[64 * 64];
+    for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) {
+            m[r * N + c] = M0[r * N + c];
+            a[r * N + c] = r == c ? 1.0 : 0.0;
+        }
+    double log_det = 0.0;
+    for (int k = 0; k < N; ++k) {
+        int piv = k;
+        for (int r = k + 1; r < N; ++r)
+            if (cabs(m[r * N + k]) > cabs(m[piv * N + k])) piv = r;
+        const zc diag = m[piv * N + k];
+        if (cabs(diag) == 0.0 || !isfinite(creal(diag)) || !isfinite(cimag(diag))) { *err = 1; return 0.0; }
+        log_det += log(cabs(diag));
+        if (piv != k)
+            for (int c = 0; c < N; ++c) {
+                zc t = m[k * N + c]; m[k * N + c] = m[piv * N + c]; m[piv * N + c] = t;
+                t = a[k * N + c]; a[k * N + c] = a[piv * N + c]; a[piv * N + c] = t;
+            }
+        const zc inv = 1.0 / diag;
+        for (int c = 0; c < N; ++c) {
+            m[k * N + c] *= inv;
+            a[k * N + c] *= inv;
+        }
+        for (int r = 0; r < N; ++r) {
+            if (r == k) continue;
+            const zc f = m[r * N + k];
+            for (int c = 0; c < N; ++c) {
+                m[r * N + c] -= f * m[k * N + c];
+                a[r * N + c] -= f * a[k * N + c];
+            }
+        }
+    }
+    for (int e = 0; e < N * N; ++e) {
+        Ar[e] = creal(a[e]);
+        Ai[e] = cimag(a[e]);
+    }
+    return log_det;
+}
+
+/* Rows of block b at the walker's positions (particle `moved` at `np_`). */
+static void crows(const sys_t* s, const double* w, int b, int moved, const double* np_, zc* D) {
+    const block_t* B = &s->blocks[b];
+    const int N = B->last - B->first, dim = s->dim;
+    for (int kr = 0; kr < N; ++kr) {
+        const int part = B->first + kr;
+        const double* r = part == moved ? np_ : POS(s, w) + part * dim;
+        for (int i = 0; i < N; ++i) D[kr * N + i] = corb(B, i, dim, r);
+    }
+}
+
+/* G_d = Σ_m A[m][kr] ∂_d φ_m(r), L_d = Σ_m A[m][kr] ∂²_d φ_m(r) - G_d² at r. */
+static void cderivs(const sys_t* s, const double* w, int b, int kr, const double* r, zc* G, zc* L) {
+    const block_t* B = &s->blocks[b];
+    const int N = B->last - B->first, dim = s->dim;
+    const double* Ar = w + s->o_A[b];
+    const double* Ai = Ar + N * N;
+    for (int d = 0; d < dim; ++d) {
+        zc g = 0.0, l = 0.0;
+        for (int m = 0; m < N; ++m) {
+            const zc a = CMPLX(Ar[m * N + kr], Ai[m * N + kr]);
+            const zc phi = corb(B, m, dim, r);
+            const double qd = B->k[m * dim + d];
+            g += a * (I * qd * phi);
+            l += a * (-qd * qd * phi);
+        }
+        G[d] = g;
+        L[d] = l - g * g;
+    }
+}
+
+static void cslater_evaluate(const sys_t* s, double* w) {
+    const int dim = s->dim, np = s->np;
+    double* gc = GC(s, w, 0);
+    double* lc = LC(s, w, 0);
+    double* pgc = w + s->o_pgc;
+    double* plc = w + s->o_plc;
+    LPC(s, w)[0] = 0.0;
+    memset(gc, 0, sizeof(double) * np * dim);
+    memset(lc, 0, sizeof(double) * np * dim);
+    memset(pgc, 0, sizeof(double) * np * dim);
+    memset(plc, 0, sizeof(double) * np * dim);
+    for (int b = 0; b < s->nblocks; ++b) {
+        const block_t* B = &s->blocks[b];
+        const int N = B->last - B->first;
+        zc D[64 * 64];
+        crows(s, w, b, -1, NULL, D);
+        double* Ar = w + s->o_A[b];
+        int err = 0;
+        const double ld = cgj(N, D, Ar, Ar + N * N, &err);
+        if (err) SC(s, w)[S_ERR] = 1.0;
+        double* bs = w + s->o_bs[b];
+        bs[0] = ld;
+        bs[1] = 0.0;
+        bs[2] = 0.0;
+        LPC(s, w)[0] += ld;
+        for (int kr = 0; kr < N; ++kr) {
+            const int part = B->first + kr;
+            zc G[3], L[3];
+            cderivs(s, w, b, kr, POS(s, w) + part * dim, G, L);
+            for (int d = 0; d < dim; ++d) {
+                gc[part * dim + d] += creal(G[d]);
+                lc[part * dim + d] += creal(L[d]);
+                pgc[part * dim + d] += cimag(G[d]);
+                plc[part * dim + d] += cimag(L[d]);
+            }
+        }
+    }
+    memcpy(w + s->o_pgrad, pgc, sizeof(double) * np * dim);
+    memcpy(w + s->o_plap, plc, sizeof(double) * np * dim);
+}
+
 /* ───────────────────────── move scratch ─────────────────────────────── */
 
 typedef struct {
     double new_pos[3], pend[1024];      /* pending distances [np] */
     double new_grad[3], new_lap[3], log_ratio, phase;
+    double new_pgrad[3], new_plap[3];   /* phase part (complex determinant) */
     double nval[64], ngrad[64 * 3], nlap[64 * 3];
     double pg[MAXT][3], pl[MAXT][3];    /* per-term pending grad/lap */
     double rad[MAXT][1024][6];          /* u_old, du_old, d2u_old, u_new, du_new, d2u_new */
@@ -1160,7 +1305,10 @@ static void build_tables(const sys_t* s, double* w) {
 /* TrialWavefunction::evaluate_batch: totals = Σ components. */
 static void psi_evaluate(const sys_t* s, double* w) {
     const int n = s->np * s->dim;
-    if (s->nblocks) slater_evaluate(s, w);
+    if (s->nblocks) {
+        if (s->cplx) cslater_evaluate(s, w);
+        else slater_evaluate(s, w);
+    }
     for (int t = 0; t < s->nterms; ++t) term_evaluate(s, w, t);
     double lp = 0.0;
     memset(GRAD(s, w), 0, sizeof(double) * n);
@@ -1180,12 +1328,18 @@ static void psi_evaluate(const sys_t* s, double* w) {
 static double local_energy(const sys_t* s, const double* w) {
     const int np = s->np, dim = s->dim;
     double le = 0.0;
-    /* kinetic */
+    /* kinetic (Kinetic::evaluate_batch; add_phase_terms for a complex ψ) */
     for (int i = 0; i < np; ++i)
         for (int d = 0; d < dim; ++d) {
             const double g = GRAD(s, w)[i * dim + d], l = LAP(s, w)[i * dim + d];
             le += -0.5 * s->inv_mass[i * dim + d] * (l + g * g);
         }
+    if (s->cplx)
+        for (int i = 0; i < np; ++i)
+            for (int d = 0; d < dim; ++d) {
+                const double pg = w[s->o_pgrad + i * dim + d];
+                le += 0.5 * s->inv_mass[i * dim + d] * pg * pg;
+            }
     const double* dist = DIST(s, w);
     if (s->ewald) {
         /* real space, group pairs g <= h */
@@ -1273,6 +1427,19 @@ static double local_energy(const sys_t* s, const double* w) {
     return le;
 }
 
+/* Imaginary part of E_L of a complex ψ: -½ Σ (1/m)(∂²φ + 2 ∂ln|ψ|·∂φ)
+ * (Kinetic::add_phase_terms). */
+static double local_energy_imag(const sys_t* s, const double* w) {
+    if (!s->cplx) return 0.0;
+    double im = 0.0;
+    for (int i = 0; i < s->np; ++i)
+        for (int d = 0; d < s->dim; ++d) {
+            const int k = i * s->dim + d;
+            im += -0.5 * s->inv_mass[k] * (w[s->o_plap + k] + 2.0 * GRAD(s, w)[k] * w[s->o_pgrad + k]);
+        }
+    return im;
+}
+
 /* Initialise walkers from AoS positions [w][p][d] and evaluate psi and H. */
 int o_init(void* p, double* walkers, long nw, const double* pos_aos) {
     const sys_t* s = p;
@@ -1284,6 +1451,8 @@ int o_init(void* p, double* walkers, long nw, const double* pos_aos) {
         build_tables(s, w);
         psi_evaluate(s, w);
         SC(s, w)[S_EL] = local_energy(s, w);
+    SC(s, w)[S_ELI] = local_energy_imag(s, w);
+        SC(s, w)[S_ELI] = local_energy_imag(s, w);
         SC(s, w)[S_WEIGHT] = 1.0;
         SC(s, w)[S_ID] = 0.0;   /* Walker ids start at 0 (walker.h) */
     }
@@ -1291,6 +1460,7 @@ int o_init(void* p, double* walkers, long nw, const double* pos_aos) {
 }
 
 void o_refresh_all(const sys_t* s, double* w) {
+    if (s->cplx) return;   /* the complex determinant keeps its derivatives current */
     for (int b = 0; b < s->nblocks; ++b)
         for (int q = s->blocks[b].first; q < s->blocks[b].last; ++q) slater_refresh(s, w, q);
 }
@@ -1324,11 +1494,36 @@ static void ratio(const sys_t* s, const double* w, int p, move_t* mv) {
         }
     }
     for (int d = 0; d < dim; ++d) mv->new_grad[d] = mv->new_lap[d] = 0.0;
+    for (int d = 0; d < dim; ++d) mv->new_pgrad[d] = mv->new_plap[d] = 0.0;
     mv->log_ratio = 0.0;
     mv->phase = 0.0;
     /* Slater */
     const int b = block_of(s, p);
-    if (b >= 0) {
+    if (b >= 0 && s->cplx) {   /* ComplexSlaterDeterminant::ratio_batch */
+        const block_t* B = &s->blocks[b];
+        const int N = B->last - B->first, jrow = p - B->first;
+        const double* Ar = w + s->o_A[b];
+        const double* Ai = Ar + N * N;
+        zc R = 0.0;
+        for (int m = 0; m < N; ++m)
+            R += CMPLX(Ar[m * N + jrow], Ai[m * N + jrow]) * corb(B, m, dim, mv->new_pos);
+        const double absR = cabs(R);
+        mv->log_ratio += log(fmax(absR, 1e-300));
+        mv->phase += carg(R);
+        const zc invR = absR > 0.0 ? 1.0 / R : 0.0;
+        zc G[3], L[3];
+        cderivs(s, w, b, jrow, mv->new_pos, G, L);
+        for (int d = 0; d < dim; ++d) {
+            /* cderivs gave L = Lraw - G²; the ratio wants Lraw/R - (G/R)² */
+            const zc Lraw = L[d] + G[d] * G[d];
+            const zc Gp = invR * G[d];
+            const zc Lp = invR * Lraw - Gp * Gp;
+            mv->new_grad[d] += creal(Gp);
+            mv->new_lap[d] += creal(Lp);
+            mv->new_pgrad[d] += cimag(Gp);
+            mv->new_plap[d] += cimag(Lp);
+        }
+    } else if (b >= 0) {
         const block_t* B = &s->blocks[b];
         const int N = B->last - B->first, jrow = p - B->first;
         const double* A = w + s->o_A[b];
@@ -1425,7 +1620,49 @@ static void commit(const sys_t* s, double* w, int p, move_t* mv) {
     double* bl = LAP(s, w);
     /* Slater, walker-tile path of apply_move_impl (deferred) */
     const int b = block_of(s, p);
-    if (b >= 0) {
+    if (b >= 0 && s->cplx) {   /* ComplexSlaterDeterminant::apply_move_batch (eager) */
+        const block_t* B = &s->blocks[b];
+        const int N = B->last - B->first, jrow = p - B->first;
+        double* Ar = w + s->o_A[b];
+        double* Ai = Ar + N * N;
+        double* bs = w + s->o_bs[b];
+        zc D[64 * 64];
+        crows(s, w, b, p, mv->new_pos, D);
+        zc R = 0.0;
+        for (int m = 0; m < N; ++m) R += CMPLX(Ar[m * N + jrow], Ai[m * N + jrow]) * D[jrow * N + m];
+        const double dlog = log(fmax(cabs(R), 1e-300));
+        bs[0] += dlog;
+        LPC(s, w)[0] += dlog;
+        SC(s, w)[S_LOGPSI] += dlog;
+        int err = 0;
+        cgj(N, D, Ar, Ai, &err);
+        if (err) SC(s, w)[S_ERR] = 1.0;
+        double* gc = GC(s, w, 0);
+        double* lc = LC(s, w, 0);
+        double* pgc = w + s->o_pgc;
+        double* plc = w + s->o_plc;
+        double* pgt = w + s->o_pgrad;
+        double* plt = w + s->o_plap;
+        for (int kr = 0; kr < N; ++kr) {
+            const int part = B->first + kr;
+            const double* r = part == p ? mv->new_pos : pos + part * dim;
+            zc G[3], L[3];
+            cderivs(s, w, b, kr, r, G, L);
+            for (int d = 0; d < dim; ++d) {
+                const int idx = part * dim + d;
+                if (kr != jrow) {
+                    bg[idx] += creal(G[d]) - gc[idx];
+                    bl[idx] += creal(L[d]) - lc[idx];
+                    pgt[idx] += cimag(G[d]) - pgc[idx];
+                    plt[idx] += cimag(L[d]) - plc[idx];
+                }
+                gc[idx] = creal(G[d]);
+                lc[idx] = creal(L[d]);
+                pgc[idx] = cimag(G[d]);
+                plc[idx] = cimag(L[d]);
+            }
+        }
+    } else if (b >= 0) {
         const block_t* B = &s->blocks[b];
         const int N = B->last - B->first, jrow = p - B->first;
         double* A = w + s->o_A[b];
@@ -1618,6 +1855,11 @@ static void commit(const sys_t* s, double* w, int p, move_t* mv) {
         bg[p * dim + d] = mv->new_grad[d];
         bl[p * dim + d] = mv->new_lap[d];
     }
+    if (s->cplx)
+        for (int d = 0; d < dim; ++d) {
+            w[s->o_pgrad + p * dim + d] = mv->new_pgrad[d];
+            w[s->o_plap + p * dim + d] = mv->new_plap[d];
+        }
 }
 
 /*
@@ -1766,7 +2008,8 @@ static long dmc_sweep_walker(const sys_t* s, double* w, const double* rnd, long 
         }
         ratio(s, w, p, mv);
         int accept = 0;
-        if (!(cos(mv->phase) < 2.220446049250313e-16)) {
+        /* fixed node: a sign change rejects; fixed phase (complex ψ): no gate */
+        if (s->cplx || !(cos(mv->phase) < 2.220446049250313e-16)) {
             double vn = 0.0;
             for (int d = 0; d < dim; ++d) vn += mv->new_grad[d] * mv->new_grad[d];
             const double sc_bwd = umrigar(tm_p, vn);

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB: Optional[ctypes.CDLL] = None
 
 # scalar slots of an oracle walker record (alea_oracle.c, enum S_*)
-S_LOGPSI, S_EL, S_WEIGHT, S_EPREV, S_RRP, S_RRA, S_AGE, S_ID, S_PARENT, S_ERR = range(10)
+S_LOGPSI, S_EL, S_WEIGHT, S_EPREV, S_RRP, S_RRA, S_AGE, S_ID, S_PARENT, S_ERR, S_ELI = range(11)
 
 
 def load_oracle_lib() -> ctypes.CDLL:
@@ -75,9 +75,12 @@ def blob_from_setup(sd: Dict[str, Any]) -> np.ndarray:
     blocks = sd.get("slater", [])
     out.append(len(blocks))
     for b in blocks:
-        out += [b["first"], b["last"], 0 if b["type"] == "plane_wave" else 1]
+        btype = {"plane_wave": 0, "gaussian": 1, "twisted_plane_wave": 2}[b["type"]]
+        out += [b["first"], b["last"], btype]
         if b["type"] == "plane_wave":
             out += list(b["k"]) + list(b["is_sin"])
+        elif b["type"] == "twisted_plane_wave":
+            out += list(b["q"])
         else:
             out += list(b["centers"]) + list(b["alphas"])
     terms = []
@@ -156,10 +159,10 @@ class Oracle:
         self.sys = self.lib.o_sys_new(_dp(self._blob), len(self._blob))
         if not self.sys:
             raise ValueError("oracle: malformed system description")
-        lay = (ctypes.c_long * 10)()
+        lay = (ctypes.c_long * 12)()
         self.lib.o_layout(self.sys, lay)
         (self.W, self.o_pos, self.o_dist, self.o_grad, self.o_lap, self.o_scal,
-         self.o_lpc, self.o_gc, self.o_lc, self.ncomp) = list(lay)
+         self.o_lpc, self.o_gc, self.o_lc, self.ncomp, self.o_pgrad, self.o_plap) = list(lay)
         self.np = int(setup["np"])
         self.dim = int(setup["dim"])
         self.walkers = np.zeros((0, self.W))
@@ -179,6 +182,14 @@ class Oracle:
     def grad(self):
         n = self.np * self.dim
         return self.walkers[:, self.o_grad:self.o_grad + n]
+
+    def phase_grad(self):
+        n = self.np * self.dim
+        return self.walkers[:, self.o_pgrad:self.o_pgrad + n] if self.o_pgrad >= 0 else None
+
+    def phase_lap(self):
+        n = self.np * self.dim
+        return self.walkers[:, self.o_plap:self.o_plap + n] if self.o_plap >= 0 else None
 
     def lap(self):
         n = self.np * self.dim

@@ -43,6 +43,8 @@
 #include "population/walker_set.h"
 #include "qmc/dmc.h"
 #include "qmc/vmc.h"
+#include "wavefunction/complex_orbital_set.h"
+#include "wavefunction/complex_slater_determinant.h"
 #include "wavefunction/drummond_jastrow.h"
 #include "wavefunction/orbital_set.h"
 #include "wavefunction/pade_jastrow.h"
@@ -257,11 +259,36 @@ std::unique_ptr<System> build_heg(const Args& a) {
     dump_cell(j, s->cell);
     dump_groups(j, s->groups);
 
+    // Twisted boundary conditions (builders/slater.cpp:244-262): twisted plane
+    // waves e^{i(k+θ)·r}, θ = t1 b1 + t2 b2, in a complex determinant.
+    const std::vector<double> twist{getd(a, "tx", 0.0), getd(a, "ty", 0.0)};
+    const bool twisted = std::abs(twist[0] - std::nearbyint(twist[0])) >= 1e-12 ||
+                         std::abs(twist[1] - std::nearbyint(twist[1])) >= 1e-12;
+    if (twisted) {
+        std::vector<ComplexSlaterDeterminant::Block> cblocks;
+        j.key("slater");
+        j.open('[');
+        for (const ParticleGroup& g : s->groups) {
+            auto orb = make_twisted_plane_wave_orbitals(s->cell, g.size(), twist);
+            j.open('{');
+            j.ki("first", static_cast<long long>(g.first));
+            j.ki("last", static_cast<long long>(g.last));
+            j.ks("type", "twisted_plane_wave");
+            const auto q = orb->wavevectors();
+            j.arr("q", std::vector<double>(q.begin(), q.end()));
+            j.arr("twist", twist);
+            j.close('}');
+            cblocks.push_back({g.first, g.last, std::move(orb)});
+        }
+        j.close(']');
+        s->psi.add_component(std::make_unique<ComplexSlaterDeterminant>(std::move(cblocks)));
+    }
     // Slater: one plane-wave block per spin group (builders/slater.cpp:267).
     std::vector<SlaterDeterminant::Block> blocks;
-    j.key("slater");
-    j.open('[');
+    if (!twisted) j.key("slater");
+    if (!twisted) j.open('[');
     for (const ParticleGroup& g : s->groups) {
+        if (twisted) break;
         auto orb = make_plane_wave_orbitals(s->cell, g.size());
         j.open('{');
         j.ki("first", static_cast<long long>(g.first));
@@ -275,8 +302,10 @@ std::unique_ptr<System> build_heg(const Args& a) {
         j.close('}');
         blocks.push_back({g.first, g.last, std::move(orb)});
     }
-    j.close(']');
-    s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
+    if (!twisted) {
+        j.close(']');
+        s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
+    }
 
     // Padé on every group pair, a1 = 2 mu R/(2 l + d - 1) (builders/jastrow.cpp:48-63):
     // same-spin pairs of a determinant group are P-wave (l = 1), opposite spins S-wave.
@@ -656,6 +685,11 @@ int run(const std::string& mode, const Args& a) {
         out.arr("local_energy", ws.local_energies());
         out.arr("grad", ws.gradients());
         out.arr("lap", ws.laplacians());
+        if (ws.has_phase()) {
+            out.arr("phase_grad", ws.phase_gradients());
+            out.arr("phase_lap", ws.phase_laplacians());
+            out.arr("local_energy_imag", ws.local_energies_imag());
+        }
         out.key("component_log_psi");
         out.open('[');
         for (const auto& c : psi.components()) out.arr("", c->log_psi_c());

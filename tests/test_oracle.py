@@ -12,7 +12,7 @@ from conftest import golden
 from oracle import Oracle
 from oracle.oracle import S_EL, S_LOGPSI, load_oracle_lib
 
-SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16"]
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t"]
 
 
 def rel(a, b):
@@ -69,7 +69,8 @@ def test_oracle_evaluate_matches_reference(name):
     assert np.max(np.abs(o.grad()[:4] - g_ref)) < 1e-9 * max(1.0, np.abs(g_ref).max())
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "heg10_drift", "crystal16", "dipoles16"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "heg10_drift", "crystal16", "dipoles16",
+                                  "heg10t", "heg10t_drift"])
 def test_oracle_vmc_matches_reference(name):
     r = golden(f"vmc_{name}.json")
     p = r["params"]
@@ -89,7 +90,7 @@ def test_oracle_vmc_matches_reference(name):
         assert np.array_equal(o.pos()[: p["nw"]], fp)
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t"])
 def test_oracle_dmc_matches_reference(name):
     r = golden(f"dmc_{name}.json")
     p = r["params"]
@@ -111,3 +112,30 @@ def test_exciton_exact_zero_variance():
     o.init(np.array(ev["positions"]))
     el, _ = o.vmc(4, 1, 0, 3, 5, 2, 0.05)
     assert np.max(np.abs(el + 1.0)) < 1e-12
+
+
+def test_oracle_twisted_phase_planes_match_reference():
+    """Complex determinant: the phase part of ∇ln ψ and ∂²ln ψ and Im E_L."""
+    from oracle.oracle import S_ELI
+    ev = golden("eval_heg10t.json")
+    o = Oracle(golden("setup_heg10t.json"))
+    o.init(np.array(ev["positions"]))
+    n = o.np * o.dim
+    for mine, key in ((o.phase_grad(), "phase_grad"), (o.phase_lap(), "phase_lap")):
+        ref = np.array(ev[key]).reshape(n, -1).T
+        assert np.max(np.abs(mine[:4] - ref)) < 1e-10 * max(1.0, np.abs(ref).max())
+    assert np.max(np.abs(o.scalar(S_ELI)[:4] - np.array(ev["local_energy_imag"]))) < 1e-12
+
+
+def test_oracle_free_twisted_determinant_kinetic_energy():
+    """A determinant of twisted plane waves alone is an eigenstate of the
+    kinetic energy: E_L = Σ |k + θ|²/2 for every configuration
+    (complex_orbital_set.h kinetic_energy_sum)."""
+    s = golden("setup_heg10t.json")
+    free = {k: v for k, v in s.items() if k not in ("pade", "ewald")}
+    ev = golden("eval_heg10t.json")
+    o = Oracle(free)
+    o.init(np.array(ev["positions"]))
+    q = np.concatenate([np.array(b["q"]) for b in s["slater"]])
+    exact = 0.5 * np.sum(q * q)
+    assert np.max(np.abs(o.scalar(S_EL)[:4] - exact)) < 1e-12 * abs(exact) + 1e-15
