@@ -75,7 +75,10 @@ def pack_system(desc: Dict[str, Any]):
     for i, b in enumerate(blocks):
         B = s.blocks[i]
         B.first, B.last = int(b["first"]), int(b["last"])
-        if b["type"] == "plane_wave":
+        if b["type"] == "twisted_plane_wave":
+            B.type = _capi.ORB_TWISTED_PLANE_WAVE
+            B.k = _dp(f64(b["q"]))
+        elif b["type"] == "plane_wave":
             B.type = _capi.ORB_PLANE_WAVE
             B.k = _dp(f64(b["k"]))
             B.is_sin = _ip(i32(b["is_sin"]))
@@ -242,6 +245,17 @@ class Walkers:
             "lap": lap.reshape(n, nw).T.copy(),
             "log_psi": lp, "local_energy": el, "weights": w,
         }
+
+    def download_phase(self) -> Dict[str, np.ndarray]:
+        """Phase planes and Im E_L of a complex (twisted) trial function."""
+        nw = self.nw
+        n = self.np * self.dim
+        pg = np.zeros(n * nw)
+        pl = np.zeros(n * nw)
+        eli = np.zeros(nw)
+        self._check(self.lib.alea_gpu_download_phase(self.ctx, _dp(pg), _dp(pl), _dp(eli)))
+        return {"phase_grad": pg.reshape(n, nw).T.copy(), "phase_lap": pl.reshape(n, nw).T.copy(),
+                "local_energy_imag": eli}
 
     def move(self, p: int, new_pos_aos: np.ndarray, accept: Optional[Sequence[bool]] = None):
         """Single-particle move of p for every walker; new_pos_aos [w][d]."""

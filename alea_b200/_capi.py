@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libalea_b200.so")
 
 ALEA_OK = 0
 ERRORS = {1: "invalid", 2: "cuda", 3: "unsupported", 4: "singular", 5: "timeout", 6: "nomem"}
-ORB_PLANE_WAVE, ORB_GAUSSIAN = 0, 1
+ORB_PLANE_WAVE, ORB_GAUSSIAN, ORB_TWISTED_PLANE_WAVE = 0, 1, 2
 PAIR_PADE, PAIR_DRUMMOND, PAIR_ZERO_ENERGY = 0, 1, 2
 STREAM_VMC = 0x766D632D74687264
 STREAM_DMC = 0x646D632D74687264
@@ -121,7 +121,7 @@ EXPORTS = [
     "alea_gpu_download_walkers", "alea_gpu_move", "alea_gpu_measure", "alea_gpu_set_streams",
     "alea_gpu_vmc_step", "alea_gpu_dmc_advance", "alea_gpu_dmc_branch", "alea_gpu_vmc_run",
     "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms", "alea_gpu_stream", "alea_gpu_transfer_bytes",
-    "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc",
+    "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc", "alea_gpu_download_phase",
     "alea_gpu_setup_heg2d", "alea_gpu_setup_crystal2d", "alea_gpu_setup_exciton2d",
     "alea_gpu_setup_charges2d", "alea_gpu_setup_dipoles2d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
@@ -150,6 +150,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_evaluate": ([P], I),
         "alea_gpu_num_walkers": ([P, c_ip], I),
         "alea_gpu_download_walkers": ([P, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp], I),
+        "alea_gpu_download_phase": ([P, c_dp, c_dp, c_dp], I),
         "alea_gpu_move": ([P, I, c_dp, ctypes.POINTER(ctypes.c_uint8), c_dp, c_dp, c_dp, c_dp], I),
         "alea_gpu_measure": ([P], I),
         "alea_gpu_set_streams": ([P, ctypes.c_uint64, ctypes.c_uint64, I], I),

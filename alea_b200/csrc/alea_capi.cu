@@ -468,6 +468,15 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     s.o_sg = o; o += np * 2;
     s.o_sl = o; o += np * 2;
     s.o_scal = o; o += S_NSCAL;
+    // a complex determinant is all twisted plane-wave blocks
+    s.cplx = 0;
+    for (int b = 0; b < in->n_blocks; ++b) s.cplx |= in->blocks[b].type == ALEA_ORB_TWISTED_PLANE_WAVE;
+    if (s.cplx)
+        for (int b = 0; b < in->n_blocks; ++b)
+            if (in->blocks[b].type != ALEA_ORB_TWISTED_PLANE_WAVE)
+                return fail(c, ALEA_ERR_UNSUPPORTED, "twisted plane-wave blocks cannot be mixed with real ones");
+    s.o_pg = static_cast<int>(o); o += s.cplx ? np * 2 : 0;
+    s.o_pl = static_cast<int>(o); o += s.cplx ? np * 2 : 0;
     // determinant blocks
     if (in->n_blocks < 0 || in->n_blocks > kMaxBlocks) return fail(c, ALEA_ERR_INVALID, "bad n_blocks");
     s.nblocks = in->n_blocks;
@@ -489,6 +498,9 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
             sin_flags[b].resize(D.n);
             for (int i = 0; i < D.n; ++i) sin_flags[b][i] = B.is_sin[i] ? 1.0 : 0.0;
             put(sin_flags[b].data(), D.n * 8, reinterpret_cast<const void**>(&D.is_sin));
+        } else if (B.type == ALEA_ORB_TWISTED_PLANE_WAVE) {
+            if (!B.k) return fail(c, ALEA_ERR_INVALID, "twisted plane-wave block without wavevectors");
+            put(B.k, D.n * 2 * 8, reinterpret_cast<const void**>(&D.k));
         } else if (B.type == ALEA_ORB_GAUSSIAN) {
             if (!B.centers || !B.alphas) return fail(c, ALEA_ERR_INVALID, "Gaussian block without tables");
             put(B.centers, D.n * 2 * 8, reinterpret_cast<const void**>(&D.centers));
@@ -497,7 +509,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
             return fail(c, ALEA_ERR_INVALID, "unknown orbital type");
         }
         D.oA = static_cast<int>(o);
-        o += round4(D.n * D.n);
+        o += (s.cplx ? 2 : 1) * round4(D.n * D.n);
     }
     for (int b = 0; b < s.nblocks; ++b) {
         s.blocks[b].orabs = static_cast<int>(o);
@@ -644,11 +656,12 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     o += static_cast<long>(s.ngroups) * 2 * s.nkJ;
     s.hot = static_cast<int>(round4(o));
     o = s.hot;
-    for (int b = 0; b < s.nblocks; ++b) {
+    for (int b = 0; b < s.nblocks; ++b) {   // twisted plane waves recompute their rows
         DevBlock& D = s.blocks[b];
-        D.oD = o; o += round4(D.n * D.n);
-        D.oDg = o; o += round4(D.n * D.n * 2);
-        D.oDl = o; o += round4(D.n * D.n * 2);
+        const long f = s.cplx ? 0 : 1;
+        D.oD = o; o += f * round4(D.n * D.n);
+        D.oDg = o; o += f * round4(D.n * D.n * 2);
+        D.oDl = o; o += f * round4(D.n * D.n * 2);
     }
     s.rec = round4(o);
     // Ewald
@@ -725,22 +738,23 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         m += round4(std::max(n, 1L));
         return static_cast<int>(at);
     };
+    const long cf = s.cplx ? 2 : 1;   // complex rows and factors: re | im
     s.s_newpos = take(4);
-    s.s_nval = take(s.maxN);
+    s.s_nval = take(cf * s.maxN);
     s.s_ngrad = take(2 * s.maxN);
     s.s_nlap = take(2 * s.maxN);
     s.s_cn = take(s.nkJ);
     s.s_sn = take(s.nkJ);
     s.s_co = take(s.nkJ);
     s.s_so = take(s.nkJ);
-    s.s_col = take(s.maxN);
-    s.s_rowp = take(s.maxN);
+    s.s_col = take(cf * s.maxN);
+    s.s_rowp = take(cf * s.maxN);
     s.s_red = take(4 * 16 + 16);
     s.s_misc = take(32 + 4 * 2 * (kMaxLadder + 1));
     // One union: the per-partner scratch of a move (read by the commit before
     // any rebuild), the Gauss-Jordan work matrix, and the ρ(k) accumulators
     // of the local energy.
-    long work = static_cast<long>(s.maxN) * s.maxN;
+    long work = cf * s.maxN * s.maxN;
     work = std::max(work, 2L * s.enk);
     work = std::max(work, static_cast<long>(np) * 10);
     s.s_work = take(work);
@@ -1027,6 +1041,34 @@ int alea_gpu_evaluate(alea_gpu_ctx* c) {
     if (!c) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     return launch_evaluate(c);
+}
+
+int alea_gpu_download_phase(alea_gpu_ctx* c, double* phase_gradients, double* phase_laplacians,
+                            double* local_energy_imag) {
+    if (!c) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    const DevSys& s = c->sys;
+    if (!s.cplx) return fail(c, ALEA_ERR_INVALID, "the trial function is real: it has no phase planes");
+    const int nw = c->nw;
+    if (nw == 0) return ALEA_OK;
+    const long n = static_cast<long>(s.np) * 2 * nw;
+    const int grid = static_cast<int>((n + 255) / 256);
+    for (int which = 0; which < 2; ++which) {
+        double* dst = which == 0 ? phase_gradients : phase_laplacians;
+        if (!dst) continue;
+        ++c->launches;
+        to_soa_kernel<<<grid, 256, 0, c->stream>>>(records(c), nw, s.rec, which == 0 ? s.o_pg : s.o_pl,
+                                                   s.np * 2, c->d_buf);
+        CUDA_TRY(c, cudaGetLastError());
+        CUDA_TRY(c, copy_out(c, dst, c->d_buf, n * 8));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+    if (local_energy_imag) {
+        std::vector<double> tmp;
+        if (int rc = read_scalars(c, S_ELI, tmp)) return rc;
+        std::copy(tmp.begin(), tmp.end(), local_energy_imag);
+    }
+    return ALEA_OK;
 }
 
 int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_psi, double* gradients,

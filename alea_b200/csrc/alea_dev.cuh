@@ -24,7 +24,8 @@ constexpr int kMaxLadder = 16;         // largest |n| of a reciprocal index
 // Scalar slots of a walker record.
 enum : int {
     S_LOGPSI = 0, S_EL, S_WEIGHT, S_EPREV, S_RRP, S_RRA, S_AGE, S_ID, S_PARENT, S_ERR,
-    S_NACC, S_NCUT, S_BLOCK0 /* 3 per block: log|det|, updates, condition */,
+    S_NACC, S_NCUT, S_ELI /* Im E_L of a complex ψ */,
+    S_BLOCK0 /* 3 per block: log|det|, updates, condition */,
     S_NSCAL = S_BLOCK0 + 3 * kMaxBlocks
 };
 
@@ -57,8 +58,8 @@ struct DevTerm {
 };
 
 struct DevBlock {
-    int first, last, n, type;
-    const double* k;          // plane waves [n*dim]
+    int first, last, n, type;  // type 0 plane waves, 1 Gaussians, 2 twisted plane waves
+    const double* k;          // plane waves [n*dim]; twisted: q = k + θ
     const double* is_sin;     // [n] (0/1)
     const double* centers;    // Gaussians [n*dim]
     const double* alphas;     // [n]
@@ -77,6 +78,7 @@ struct DevSys {
     const double* charge;     // [np]
     const int* group_of;      // [np]
     int nblocks, maxN;
+    int cplx;                 // complex determinant (twisted plane waves): A = re | im
     DevBlock blocks[kMaxBlocks];
     int nterms;
     DevTerm terms[kMaxTerms];
@@ -108,6 +110,7 @@ struct DevSys {
     long rec;                 // record stride
     int hot;
     int o_pos, o_jg, o_jl, o_kg, o_kl, o_sg, o_sl, o_scal, o_rho;
+    int o_pg, o_pl;           // phase part of ∇ln ψ, ∂²ln ψ (complex determinant)
     // shared-memory scratch layout (doubles, after the hot part)
     int s_newpos, s_nval, s_ngrad, s_nlap, s_rad, s_cn, s_sn, s_co, s_so, s_col, s_rowp,
         s_red, s_misc, s_work, s_total;

@@ -47,7 +47,7 @@ constexpr double kEps = 2.220446049250313e-16;
 constexpr int kLad = 2 * (kMaxLadder + 1);   // doubles per ladder
 
 struct Smem {
-    double *pos, *jg, *jl, *kg, *kl, *sg, *sl, *scal, *rho;
+    double *pos, *jg, *jl, *kg, *kl, *sg, *sl, *scal, *rho, *pg, *pl;
     double *newpos, *nval, *ngrad, *nlap, *rad, *geo, *cn, *sn, *co, *so, *col, *rowp, *red,
         *misc, *lad, *work;
 };
@@ -63,6 +63,8 @@ __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
     v.sl = sm + s.o_sl;
     v.scal = sm + s.o_scal;
     v.rho = sm + s.o_rho;
+    v.pg = sm + s.o_pg;
+    v.pl = sm + s.o_pl;
     v.newpos = sm + s.s_newpos;
     v.nval = sm + s.s_nval;
     v.ngrad = sm + s.s_ngrad;
@@ -86,7 +88,8 @@ __device__ __forceinline__ Smem view(const DevSys& s, double* sm) {
 enum : int {
     M_R = 0, M_SCALE, M_LOGR, M_PHASE, M_ACCEPT, M_REBUILD, M_LOGDET, M_ERR, M_U, M_SCFWD,
     M_GOX, M_GOY, M_SGX, M_SGY, M_SLX, M_SLY, M_JGX, M_JGY, M_JLX, M_JLY, M_KGX, M_KGY,
-    M_KLX, M_KLY
+    M_KLX, M_KLY, M_RI /* Im R */, M_PGX, M_PGY, M_PLX, M_PLY /* phase part at the proposal */,
+    M_LOGDR /* determinant part of the log ratio */
 };
 
 template <int NT>
@@ -280,6 +283,157 @@ __device__ void gj_rebuild(const DevSys& s, const Smem& v, const double* grec, i
     }
 }
 
+// ───────────────────────── complex determinant ─────────────────────────
+//
+// Twisted plane waves φ_m = e^{i q_m·r} (complex_orbital_set.h:78-182) in a
+// complex determinant (complex_slater_determinant.cpp).  The inverse lives in
+// shared memory as re[N²] then im[N²]; the orbital rows are recomputed from
+// the positions when needed (one sincos each), so nothing is kept in HBM.
+// With t = A[m][kr] φ_m(r): ∂_d φ = i q_d φ and ∂²_d φ = -q_d² φ give
+// G_d = Σ_m i q_d t and Lraw_d = Σ_m -q_d² t.
+
+__device__ __forceinline__ void c_orb(const DevBlock& B, int m, const double* r, double& c, double& sn) {
+    const double arg = fma(B.k[m * 2 + 1], r[1], B.k[m * 2] * r[0]);
+    sincos(arg, &sn, &c);
+}
+
+// One orbital's contributions at r to R = Σ t, G and Lraw (re and im).
+__device__ __forceinline__ void c_accumulate(const DevBlock& B, int m, double ar, double ai, double c,
+                                             double sn, double* R, double* Gr, double* Gi,
+                                             double* Lr, double* Li) {
+    const double tr = ar * c - ai * sn, ti = ar * sn + ai * c;
+    R[0] += tr;
+    R[1] += ti;
+    for (int d = 0; d < 2; ++d) {
+        const double q = B.k[m * 2 + d];
+        Gr[d] += -q * ti;
+        Gi[d] += q * tr;
+        Lr[d] += -q * q * tr;
+        Li[d] += -q * q * ti;
+    }
+}
+
+// A = D⁻¹ of block b, D[kr][m] = φ_m(r_kr) (particle `moved` at `npos`), by
+// Gauss-Jordan with the pivot of largest modulus.  log|det D| to
+// misc[M_LOGDET], a singular matrix flagged in misc[M_ERR].
+template <int NT>
+__device__ void c_gj_rebuild(const DevSys& s, const Smem& v, int b, int moved, const double* npos) {
+    const DevBlock& B = s.blocks[b];
+    const int N = B.n, NN = N * N;
+    double* Ar = v.scal - s.o_scal + B.oA;
+    double* Ai = Ar + ((NN + 3) & ~3);
+    double* mr = v.work;
+    double* mi = v.work + NN;
+    __syncthreads();
+    for_each_elem<NT>(N, [&](int r, int c) {
+        const int part = B.first + r;
+        const double* pr = part == moved ? npos : v.pos + part * 2;
+        double cs, sn;
+        c_orb(B, c, pr, cs, sn);
+        mr[r * N + c] = cs;
+        mi[r * N + c] = sn;
+        Ar[r * N + c] = (r == c) ? 1.0 : 0.0;
+        Ai[r * N + c] = 0.0;
+    });
+    if (threadIdx.x == 0) v.misc[M_LOGDET] = 0.0;
+    __syncthreads();
+    __shared__ int s_piv;
+    for (int k = 0; k < N; ++k) {
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = N;
+            for (int r = k + static_cast<int>(threadIdx.x); r < N; r += 32) {
+                const double a = mr[r * N + k] * mr[r * N + k] + mi[r * N + k] * mi[r * N + k];
+                if (a > best) {
+                    best = a;
+                    bi = r;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                s_piv = bi;
+                if (!(best > 0.0) || !isfinite(best)) v.misc[M_ERR] = 1.0;
+                v.misc[M_LOGDET] += 0.5 * log(best);
+            }
+        }
+        __syncthreads();
+        const int piv = s_piv;
+        if (piv != k)
+            for (int c = threadIdx.x; c < N; c += NT) {
+                double t = mr[k * N + c]; mr[k * N + c] = mr[piv * N + c]; mr[piv * N + c] = t;
+                t = mi[k * N + c]; mi[k * N + c] = mi[piv * N + c]; mi[piv * N + c] = t;
+                t = Ar[k * N + c]; Ar[k * N + c] = Ar[piv * N + c]; Ar[piv * N + c] = t;
+                t = Ai[k * N + c]; Ai[k * N + c] = Ai[piv * N + c]; Ai[piv * N + c] = t;
+            }
+        __syncthreads();
+        const double dr = mr[k * N + k], di = mi[k * N + k];
+        const double dd = dr * dr + di * di;
+        const double ir = dr / dd, ii = -di / dd;   // 1 / diag
+        __syncthreads();
+        for (int c = threadIdx.x; c < N; c += NT) {
+            double xr = mr[k * N + c], xi = mi[k * N + c];
+            mr[k * N + c] = xr * ir - xi * ii;
+            mi[k * N + c] = xr * ii + xi * ir;
+            xr = Ar[k * N + c];
+            xi = Ai[k * N + c];
+            Ar[k * N + c] = xr * ir - xi * ii;
+            Ai[k * N + c] = xr * ii + xi * ir;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < N; r += NT) {
+            v.col[r] = mr[r * N + k];
+            v.col[N + r] = mi[r * N + k];
+        }
+        __syncthreads();
+        for_each_elem<NT>(N, [&](int r, int c) {
+            if (r == k) return;
+            const double fr = v.col[r], fi = v.col[N + r];
+            const double pr_ = mr[k * N + c], pi_ = mi[k * N + c];
+            mr[r * N + c] -= fr * pr_ - fi * pi_;
+            mi[r * N + c] -= fr * pi_ + fi * pr_;
+            const double qr = Ar[k * N + c], qi = Ai[k * N + c];
+            Ar[r * N + c] -= fr * qr - fi * qi;
+            Ai[r * N + c] -= fr * qi + fi * qr;
+        });
+        __syncthreads();
+    }
+}
+
+// Modulus and phase parts of ∇ln ψ and ∂²ln ψ of the complex determinant for
+// every particle of every block, one particle per thread.
+template <int NT>
+__device__ void c_refresh_all(const DevSys& s, const Smem& v) {
+    for (int b = 0; b < s.nblocks; ++b) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n;
+        const double* Ar = v.scal - s.o_scal + B.oA;
+        const double* Ai = Ar + ((N * N + 3) & ~3);
+        for (int kr = threadIdx.x; kr < N; kr += NT) {
+            const int part = B.first + kr;
+            double R[2] = {0, 0}, Gr[2] = {0, 0}, Gi[2] = {0, 0}, Lr[2] = {0, 0}, Li[2] = {0, 0};
+            for (int m = 0; m < N; ++m) {
+                double cs, sn;
+                c_orb(B, m, v.pos + part * 2, cs, sn);
+                c_accumulate(B, m, Ar[m * N + kr], Ai[m * N + kr], cs, sn, R, Gr, Gi, Lr, Li);
+            }
+            for (int d = 0; d < 2; ++d) {
+                v.sg[part * 2 + d] = Gr[d];
+                v.pg[part * 2 + d] = Gi[d];
+                v.sl[part * 2 + d] = Lr[d] - (Gr[d] * Gr[d] - Gi[d] * Gi[d]);
+                v.pl[part * 2 + d] = Li[d] - 2.0 * Gr[d] * Gi[d];
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // ───────────────────────── refresh ──────────────────────────────────────
 
 // Drift refresh of particle p: its determinant derivatives from A and the
@@ -295,8 +449,20 @@ __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* g
         const int m[2] = {s.m1J, s.m2J};
         ladders<NT>(th, m, 2, v.lad);
     }
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (b >= 0) {
+    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (b >= 0 && s.cplx) {
+        // acc[0..1] Re G, [2..3] Re Lraw, [8..9] Im G, [10..11] Im Lraw
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, kr = p - B.first;
+        const double* Ar = v.scal - s.o_scal + B.oA;
+        const double* Ai = Ar + ((N * N + 3) & ~3);
+        for (int m = threadIdx.x; m < N; m += NT) {
+            double cs, sn, R[2] = {0, 0};
+            c_orb(B, m, v.pos + p * 2, cs, sn);
+            c_accumulate(B, m, Ar[m * N + kr], Ai[m * N + kr], cs, sn, R, acc + 0, acc + 8, acc + 2,
+                         acc + 10);
+        }
+    } else if (b >= 0) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n, kr = p - B.first;
         const double* A = v.scal - s.o_scal + B.oA;
@@ -323,9 +489,18 @@ __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* g
             kspace_particle_k(s, v, p, gp, k, c, sn, acc + 4);
         }
     }
-    block_sum<NT>(acc, v.red);
+    if (s.cplx) block_sum<NT>(acc, v.red);
+    else block_sum<NT>(reinterpret_cast<double(&)[8]>(acc), v.red);
     if (threadIdx.x == 0) {
-        if (b >= 0) {
+        if (b >= 0 && s.cplx) {
+            for (int d = 0; d < 2; ++d) {
+                const double gr = acc[d], gi = acc[8 + d];
+                v.sg[p * 2 + d] = gr;
+                v.pg[p * 2 + d] = gi;
+                v.sl[p * 2 + d] = acc[2 + d] - (gr * gr - gi * gi);
+                v.pl[p * 2 + d] = acc[10 + d] - 2.0 * gr * gi;
+            }
+        } else if (b >= 0) {
             v.sg[p * 2 + 0] = acc[0];
             v.sg[p * 2 + 1] = acc[1];
             v.sl[p * 2 + 0] = acc[2] - acc[0] * acc[0];
@@ -345,7 +520,8 @@ __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* g
 template <int NT>
 __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) {
     const int np = s.np;
-    for (int b = 0; b < s.nblocks; ++b) {
+    if (s.cplx) c_refresh_all<NT>(s, v);
+    for (int b = 0; b < (s.cplx ? 0 : s.nblocks); ++b) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n;
         const double* A = v.scal - s.o_scal + B.oA;
@@ -405,9 +581,12 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
     const int np = s.np;
     const int b = block_of(s, p);
     const bool ks = kspace_of(s, p);
-    double acc[15];
+    // acc: 0 R (Re R), 1 Σ|terms| (Im R when complex), 2-5 determinant ∇, ∂² of p
+    // (Re parts), 6 Jastrow log ratio, 7-10 pair ∇, ∂², 11-14 k-space ∇, ∂²,
+    // 15-18 determinant Im ∇, Im ∂² (complex)
+    double acc[19];
 #pragma unroll
-    for (int i = 0; i < 15; ++i) acc[i] = 0.0;
+    for (int i = 0; i < 19; ++i) acc[i] = 0.0;
     if (ks) {
         const double* r = v.pos + p * 2;
         const double th[4] = {s.recip[0] * v.newpos[0] + s.recip[1] * v.newpos[1],
@@ -417,7 +596,20 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
         const int m[4] = {s.m1J, s.m2J, s.m1J, s.m2J};
         ladders<NT>(th, m, have_old ? 2 : 4, v.lad);
     }
-    if (b >= 0) {
+    if (b >= 0 && s.cplx) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, jrow = p - B.first;
+        const double* Ar = v.scal - s.o_scal + B.oA;
+        const double* Ai = Ar + ((N * N + 3) & ~3);
+        for (int m = threadIdx.x; m < N; m += NT) {
+            double cs, sn;
+            c_orb(B, m, v.newpos, cs, sn);
+            v.nval[m] = cs;
+            v.nval[N + m] = sn;
+            c_accumulate(B, m, Ar[m * N + jrow], Ai[m * N + jrow], cs, sn, acc, acc + 2, acc + 15,
+                         acc + 4, acc + 17);
+        }
+    } else if (b >= 0) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n, jrow = p - B.first;
         const double* A = v.scal - s.o_scal + B.oA;
@@ -514,12 +706,30 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
             }
         }
     }
-    block_sum<NT>(acc, v.red);
+    if (s.cplx) block_sum<NT>(acc, v.red);
+    else block_sum<NT>(reinterpret_cast<double(&)[15]>(acc), v.red);
     if (threadIdx.x == 0) {
         double logr = acc[6], phase = 0.0, sgx = 0.0, sgy = 0.0, slx = 0.0, sly = 0.0;
-        if (b >= 0) {
+        double pgx = 0.0, pgy = 0.0, plx = 0.0, ply = 0.0, logdr = 0.0;
+        if (b >= 0 && s.cplx) {
+            // R = Σ A[m][j] φ_m(r'); ∇ln ψ' = G/R, ∂²ln ψ' = Lraw/R - (G/R)²
+            const double rr = acc[0], ri = acc[1];
+            const double a2 = rr * rr + ri * ri;
+            logdr = log(fmax(sqrt(a2), 1e-300));
+            phase = atan2(ri, rr);
+            const double ir = a2 > 0.0 ? rr / a2 : 0.0, ii = a2 > 0.0 ? -ri / a2 : 0.0;
+            double gr[2], gi[2], lr[2], li[2];
+            for (int d = 0; d < 2; ++d) {
+                gr[d] = acc[2 + d] * ir - acc[15 + d] * ii;
+                gi[d] = acc[2 + d] * ii + acc[15 + d] * ir;
+                lr[d] = acc[4 + d] * ir - acc[17 + d] * ii - (gr[d] * gr[d] - gi[d] * gi[d]);
+                li[d] = acc[4 + d] * ii + acc[17 + d] * ir - 2.0 * gr[d] * gi[d];
+            }
+            sgx = gr[0]; sgy = gr[1]; slx = lr[0]; sly = lr[1];
+            pgx = gi[0]; pgy = gi[1]; plx = li[0]; ply = li[1];
+        } else if (b >= 0) {
             const double R = acc[0];
-            logr += log(fmax(fabs(R), 1e-300));
+            logdr = log(fmax(fabs(R), 1e-300));
             if (R < 0.0) phase = kPi;
             const double invR = (R != 0.0) ? 1.0 / R : 0.0;
             sgx = invR * acc[2];
@@ -527,6 +737,13 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
             slx = invR * acc[4] - sgx * sgx;
             sly = invR * acc[5] - sgy * sgy;
         }
+        logr += logdr;
+        v.misc[M_LOGDR] = logdr;
+        v.misc[M_RI] = s.cplx ? acc[1] : 0.0;
+        v.misc[M_PGX] = pgx;
+        v.misc[M_PGY] = pgy;
+        v.misc[M_PLX] = plx;
+        v.misc[M_PLY] = ply;
         v.misc[M_R] = acc[0];
         v.misc[M_SCALE] = acc[1];
         v.misc[M_LOGR] = logr;
@@ -578,8 +795,77 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
             mr[nk + k] += v.sn[k] - v.so[k];
         }
     }
-    // Slater: Sherman-Morrison with the reference's rebuild triggers
-    if (b >= 0) {
+    // complex determinant: complex Sherman-Morrison, rebuilt by Gauss-Jordan
+    // from recomputed rows every 64 updates or at a small or nonfinite ratio
+    if (b >= 0 && s.cplx) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, jrow = p - B.first;
+        double* Ar = v.scal - s.o_scal + B.oA;
+        double* Ai = Ar + ((N * N + 3) & ~3);
+        double* bs = v.scal + S_BLOCK0 + 3 * b;
+        const double rr = v.misc[M_R], ri = v.misc[M_RI];
+        const double a2 = rr * rr + ri * ri;
+        const double ir = rr / a2, ii = -ri / a2;
+        const double* nr = v.nval;
+        const double* ni = v.nval + N;
+        for (int c = threadIdx.x; c < N; c += NT) {
+            double pr = 0.0, pi = 0.0;
+            for (int m = 0; m < N; ++m) {
+                const double xr = nr[m], xi = ni[m], ar = Ar[m * N + c], ai = Ai[m * N + c];
+                pr += xr * ar - xi * ai;
+                pi += xr * ai + xi * ar;
+            }
+            v.rowp[c] = pr - (c == jrow ? 1.0 : 0.0);
+            v.rowp[N + c] = pi;
+            const double cr = Ar[c * N + jrow], ci = Ai[c * N + jrow];
+            v.col[c] = cr * ir - ci * ii;   // A[c][j] / R
+            v.col[N + c] = cr * ii + ci * ir;
+        }
+        if (threadIdx.x == 0) {
+            bs[1] += 1.0;
+            const bool rebuild = bs[1] >= 64.0 || !isfinite(a2) || sqrt(a2) < 1e-5;
+            v.misc[M_REBUILD] = rebuild ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        const double old_log = bs[0];
+        const bool rebuild = v.misc[M_REBUILD] != 0.0;
+        if (rebuild) {
+            c_gj_rebuild<NT>(s, v, b, p, v.newpos);
+        } else {
+            for_each_elem<NT>(N, [&](int a, int c) {
+                const double fr = v.col[a], fi = v.col[N + a];
+                const double qr = v.rowp[c], qi = v.rowp[N + c];
+                Ar[a * N + c] -= fr * qr - fi * qi;
+                Ai[a * N + c] -= fr * qi + fi * qr;
+            });
+            __syncthreads();
+        }
+        // the moved particle's derivatives at the committed inverse
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int m = threadIdx.x; m < N; m += NT) {
+            double R[2] = {0, 0};
+            c_accumulate(B, m, Ar[m * N + jrow], Ai[m * N + jrow], nr[m], ni[m], R, acc + 0, acc + 4,
+                         acc + 2, acc + 6);
+        }
+        block_sum<NT>(acc, v.red);
+        if (threadIdx.x == 0) {
+            if (rebuild) {
+                bs[0] = v.misc[M_LOGDET];
+                bs[1] = 0.0;
+                if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+            } else {
+                bs[0] = old_log + v.misc[M_LOGDR];
+            }
+            v.scal[S_LOGPSI] += bs[0] - old_log;
+            for (int d = 0; d < 2; ++d) {
+                const double gr = acc[d], gi = acc[4 + d];
+                v.sg[p * 2 + d] = gr;
+                v.pg[p * 2 + d] = gi;
+                v.sl[p * 2 + d] = acc[2 + d] - (gr * gr - gi * gi);
+                v.pl[p * 2 + d] = acc[6 + d] - 2.0 * gr * gi;
+            }
+        }
+    } else if (b >= 0) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n, jrow = p - B.first;
         double* A = v.scal - s.o_scal + B.oA;
@@ -671,11 +957,30 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
         wrap_pos(s, r);
         v.pos[p * 2 + 0] = r[0];
         v.pos[p * 2 + 1] = r[1];
-        double jlog = v.misc[M_LOGR];
-        if (b >= 0) jlog -= log(fmax(fabs(v.misc[M_R]), 1e-300));
-        v.scal[S_LOGPSI] += jlog;
+        v.scal[S_LOGPSI] += v.misc[M_LOGR] - v.misc[M_LOGDR];
     }
     __syncthreads();
+    // Wrapping p into the cell moved it by a lattice vector Δ; a twisted
+    // plane wave picks up the same phase e^{iθ·Δ} = e^{iq·Δ} for every
+    // orbital, so the inverse's column of p is re-gauged by e^{-iq·Δ} to stay
+    // the inverse of the rows at the stored positions.
+    if (s.cplx && b >= 0) {
+        const DevBlock& B = s.blocks[b];
+        const int N = B.n, jrow = p - B.first;
+        const double dx = v.pos[p * 2] - v.newpos[0], dy = v.pos[p * 2 + 1] - v.newpos[1];
+        if (dx != 0.0 || dy != 0.0) {
+            double* Ar = v.scal - s.o_scal + B.oA;
+            double* Ai = Ar + ((N * N + 3) & ~3);
+            double sa, ca;
+            sincos(fma(B.k[1], dy, B.k[0] * dx), &sa, &ca);
+            for (int m = threadIdx.x; m < N; m += NT) {
+                const double ar = Ar[m * N + jrow], ai = Ai[m * N + jrow];
+                Ar[m * N + jrow] = ar * ca + ai * sa;
+                Ai[m * N + jrow] = ai * ca - ar * sa;
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // ───────────────────────── local energy ─────────────────────────────────
@@ -686,10 +991,14 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
 template <int NT>
 __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs, int npair) {
     const int np = s.np;
-    double acc[1] = {0.0};
+    double acc[2] = {0.0, 0.0};   // Re, Im E_L
     for (int t = threadIdx.x; t < np * 2; t += NT) {
         const double g = v.sg[t] + v.jg[t] + v.kg[t], l = v.sl[t] + v.jl[t] + v.kl[t];
         acc[0] += -0.5 * s.inv_mass[t] * (l + g * g);
+        if (s.cplx) {   // Kinetic::add_phase_terms
+            acc[0] += 0.5 * s.inv_mass[t] * v.pg[t] * v.pg[t];
+            acc[1] += -0.5 * s.inv_mass[t] * (v.pl[t] + 2.0 * g * v.pg[t]);
+        }
     }
     if (s.ewald) {
         for (int q = threadIdx.x; q < npair; q += NT) {
@@ -757,6 +1066,7 @@ __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs
         }
     }
     block_sum<NT>(acc, v.red);
+    if (threadIdx.x == 0) v.scal[S_ELI] = acc[1];
     return acc[0] + (s.ewald ? s.e_const : 0.0) + s.ip_tail;
 }
 
@@ -773,8 +1083,10 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
         v.pos[i * 2] = r[0];
         v.pos[i * 2 + 1] = r[1];
     }
-    for (int i = threadIdx.x; i < np * 2; i += NT)
+    for (int i = threadIdx.x; i < np * 2; i += NT) {
         v.jg[i] = v.jl[i] = v.kg[i] = v.kl[i] = v.sg[i] = v.sl[i] = 0.0;
+        if (s.cplx) v.pg[i] = v.pl[i] = 0.0;
+    }
     if (threadIdx.x == 0) {
         v.scal[S_LOGPSI] = 0.0;
         v.scal[S_ERR] = 0.0;
@@ -782,8 +1094,21 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
     }
     __syncthreads();
     double lp[1] = {0.0};
+    // complex determinant: A = D⁻¹ from recomputed rows
+    for (int b = 0; b < (s.cplx ? s.nblocks : 0); ++b) {
+        c_gj_rebuild<NT>(s, v, b, -1, nullptr);
+        if (threadIdx.x == 0) {
+            double* bs = v.scal + S_BLOCK0 + 3 * b;
+            bs[0] = v.misc[M_LOGDET];
+            bs[1] = 0.0;
+            bs[2] = 0.0;
+            if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+            lp[0] += v.misc[M_LOGDET];
+        }
+        __syncthreads();
+    }
     // determinants: rows, A = D⁻¹ by Gauss-Jordan, log|det|, condition
-    for (int b = 0; b < s.nblocks; ++b) {
+    for (int b = 0; b < (s.cplx ? 0 : s.nblocks); ++b) {
         const DevBlock& B = s.blocks[b];
         const int N = B.n;
         double* D = grec + B.oD;
@@ -1035,7 +1360,8 @@ __global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, in
                 if (dmc) {
                     acc = false;
                     // a real ratio's phase is 0 or π: the fixed-node gate (cos φ < ε)
-                    if (v.misc[M_PHASE] == 0.0) {
+                    // fixed phase (complex ψ) has no gate
+                    if (s.cplx || v.misc[M_PHASE] == 0.0) {
                         const double vsq = ngx * ngx + ngy * ngy;
                         const double sb = vsq < 1e-10 ? tm0 : (-1.0 + sqrt(1.0 + 2.0 * tm0 * vsq)) / vsq;
                         const double sf = v.misc[M_SCFWD];

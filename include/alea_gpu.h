@@ -56,7 +56,7 @@ enum {
     ALEA_ERR_NOMEM = 6         /* device allocation failed / capacity exceeded */
 };
 
-enum { ALEA_ORB_PLANE_WAVE = 0, ALEA_ORB_GAUSSIAN = 1 };
+enum { ALEA_ORB_PLANE_WAVE = 0, ALEA_ORB_GAUSSIAN = 1, ALEA_ORB_TWISTED_PLANE_WAVE = 2 };
 enum { ALEA_PAIR_PADE = 0, ALEA_PAIR_DRUMMOND = 1, ALEA_PAIR_ZERO_ENERGY = 2 };
 
 #define ALEA_GPU_MAX_GROUPS 8
@@ -92,11 +92,15 @@ typedef struct {
     double inv_mass[3];   /* per dimension */
 } alea_gpu_group;
 
-/* One determinant block (src/wavefunction/slater_determinant.h:60-64). */
+/* One determinant block (src/wavefunction/slater_determinant.h:60-64).
+ * Twisted plane waves e^{i(k+θ)·r} (src/wavefunction/complex_orbital_set.h:78-182)
+ * make the determinant complex (ComplexSlaterDeterminant,
+ * src/wavefunction/complex_slater_determinant.h:20-104); then every block is
+ * twisted and DMC runs fixed phase. */
 typedef struct {
     int first, last;
     int type;                 /* ALEA_ORB_* */
-    const double* k;          /* plane waves: [n * dim] */
+    const double* k;          /* plane waves: [n * dim]; twisted: q = k + θ [n * dim] */
     const int* is_sin;        /* plane waves: [n], nonzero = sine */
     const double* centers;    /* Gaussians: [n * dim] */
     const double* alphas;     /* Gaussians: [n] */
@@ -191,6 +195,13 @@ int alea_gpu_num_walkers(const alea_gpu_ctx* ctx, int* nw);
 int alea_gpu_download_walkers(alea_gpu_ctx* ctx, double* positions, double* log_psi,
                               double* gradients, double* laplacians, double* local_energy,
                               double* weights);
+/* Phase part of ∇ln ψ and ∂²_d ln ψ (SoA like positions) and Im E_L per
+ * walker, for a complex (twisted) determinant: the phase planes of WalkerSet
+ * (src/population/walker_set.h:104-131) and the imaginary local energy of
+ * Kinetic::add_phase_terms (src/hamiltonian/kinetic.cpp:75-99).  Any pointer
+ * may be NULL; ALEA_ERR_INVALID for a real trial function. */
+int alea_gpu_download_phase(alea_gpu_ctx* ctx, double* phase_gradients, double* phase_laplacians,
+                            double* local_energy_imag);
 
 /* One single-particle move of particle p for every walker: propose
  * new_pos [d*nw + w], compute log|ψ'/ψ|, its phase (π on a node crossing),

@@ -1451,7 +1451,6 @@ int o_init(void* p, double* walkers, long nw, const double* pos_aos) {
         build_tables(s, w);
         psi_evaluate(s, w);
         SC(s, w)[S_EL] = local_energy(s, w);
-    SC(s, w)[S_ELI] = local_energy_imag(s, w);
         SC(s, w)[S_ELI] = local_energy_imag(s, w);
         SC(s, w)[S_WEIGHT] = 1.0;
         SC(s, w)[S_ID] = 0.0;   /* Walker ids start at 0 (walker.h) */
@@ -1470,6 +1469,7 @@ void o_measure(void* p, double* w) {
     const sys_t* s = p;
     o_refresh_all(s, w);
     SC(s, w)[S_EL] = local_energy(s, w);
+    SC(s, w)[S_ELI] = local_energy_imag(s, w);
 }
 
 /* ───────────────────────── one move ─────────────────────────────────── */

@@ -13,7 +13,7 @@ from oracle.oracle import S_EL, S_LOGPSI
 
 pytestmark = pytest.mark.gpu
 
-SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16"]
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t"]
 
 
 def walkers(setup, capacity):
@@ -64,7 +64,10 @@ def test_single_moves_match_oracle(name):
         for w in range(nw):
             out = o.move(w, p, new[w], bool(acc[w]))
             assert abs(lr[w] - out[0]) < 1e-10 * max(1.0, abs(out[0]))
-            assert ph[w] == out[1]
+            if "twisted" in str(setup.get("slater", [{}])[0].get("type", "")):
+                assert abs(np.angle(np.exp(1j * (ph[w] - out[1])))) < 1e-10   # continuous phase
+            else:
+                assert ph[w] == out[1]                                        # 0 or π
             assert np.max(np.abs(ng[w] - out[2:4])) < 1e-9 * max(1.0, np.abs(out[2:4]).max())
             assert np.max(np.abs(nl[w] - out[4:6])) < 1e-9 * max(1.0, np.abs(out[4:6]).max())
     g.measure()
@@ -77,14 +80,14 @@ def test_single_moves_match_oracle(name):
 
 @pytest.mark.parametrize("name,drift", [("exciton", False), ("heg10", False), ("heg10", True),
                                         ("crystal16", False), ("heg42", False), ("dipoles16", False),
-                                        ("dipoles16", True)])
+                                        ("dipoles16", True), ("heg10t", False), ("heg10t", True)])
 def test_vmc_steps_match_oracle(name, drift):
     import alea_b200
     setup = golden(f"setup_{name}.json")
     pos = np.array(golden(f"eval_{name}.json")["positions"])
     nw = pos.shape[0]
     tau = {"exciton": 0.05, "heg10": 225.0, "crystal16": 400.0, "heg42": 225.0,
-           "dipoles16": 0.0003}[name]
+           "dipoles16": 0.0003, "heg10t": 225.0}[name]
     n_steps, n_sub, seed = 4, 2, 21
     o = Oracle(setup)
     o.init(pos)
@@ -105,7 +108,7 @@ def test_vmc_steps_match_oracle(name, drift):
         assert np.array_equal(fin, o.pos()[:nw])
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t"])
 def test_dmc_run_matches_oracle(name):
     setup = golden(f"setup_{name}.json")
     r = golden(f"dmc_{name}.json")
@@ -179,3 +182,44 @@ def test_dmc_energy_agrees_with_reference_statistically():
     sigma = float(np.hypot(res.energy_error, ref["energy_error"]))
     assert res.energy_error > 0 and abs(res.energy - ref["energy"]) < 2.0 * sigma, \
         (res.energy, res.energy_error, ref["energy"], ref["energy_error"])
+
+
+@pytest.mark.gpu
+def test_twisted_phase_planes_match_oracle():
+    """Complex determinant: phase part of ∇ln ψ, ∂²ln ψ and Im E_L after a
+    full evaluation and after VMC steps (Sherman-Morrison updates)."""
+    import alea_b200
+    from oracle.oracle import S_ELI
+    setup = golden("setup_heg10t.json")
+    pos = np.array(golden("eval_heg10t.json")["positions"])
+    nw = pos.shape[0]
+    o = Oracle(setup)
+    o.init(pos)
+    g = walkers(setup, nw)
+    g.upload(pos)
+    ph = g.download_phase()
+    scale = np.abs(o.phase_lap()[:nw]).max()
+    assert np.max(np.abs(ph["phase_grad"] - o.phase_grad()[:nw])) < 1e-10 * scale
+    assert np.max(np.abs(ph["phase_lap"] - o.phase_lap()[:nw])) < 1e-10 * scale
+    assert np.max(np.abs(ph["local_energy_imag"] - o.scalar(S_ELI)[:nw])) < 1e-12
+    el_o, _ = o.vmc(nw, 7, 0, 1, 3, 2, 225.0)
+    g.set_streams(7, alea_b200.STREAM_VMC, nw)
+    for _ in range(3):
+        g.vmc_step(225.0, 2, False)
+    ph = g.download_phase()
+    assert np.max(np.abs(ph["phase_grad"] - o.phase_grad()[:nw])) < 1e-9 * scale
+    assert np.max(np.abs(ph["local_energy_imag"] - o.scalar(S_ELI)[:nw])) < 1e-10
+    assert rel(g.download()["local_energy"], el_o[-1]) < 1e-10
+
+
+@pytest.mark.gpu
+def test_free_twisted_determinant_kinetic_energy_on_device():
+    """Twisted plane waves alone: E_L = Σ |k + θ|²/2 for every walker."""
+    s = golden("setup_heg10t.json")
+    free = {k: v for k, v in s.items() if k not in ("pade", "ewald")}
+    pos = np.array(golden("eval_heg10t.json")["positions"])
+    g = walkers(free, len(pos))
+    g.upload(pos)
+    q = np.concatenate([np.array(b["q"]) for b in s["slater"]])
+    exact = 0.5 * np.sum(q * q)
+    assert np.max(np.abs(g.download()["local_energy"] - exact)) < 1e-12 * abs(exact) + 1e-15
