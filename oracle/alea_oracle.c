@@ -54,6 +54,7 @@
 #define MAXT 8   /* pair terms (Padé / Drummond) */
 #define MAXC 8   /* open Coulomb terms */
 #define MAXPAIR 4
+#define BF_MAXE (64 * 256)   /* rows x particles of one backflow determinant's pair tables */
 
 /* ───────────────────────── random numbers ───────────────────────────── */
 
@@ -204,6 +205,22 @@ typedef struct {
     const double* ze_cheb;         /* [2 * 24]: order 0, then order 1 */
 } term_t;
 
+/* One backflow channel: sources [sf, sl) displace every row by η(r) r,
+ * η = (1 - r/L)^C Σ_k c_k r^k (backflow_function.h; c_1 already derived for
+ * a like-spin channel). */
+typedef struct { int sf, sl, C; double L; int nc; double c[16]; } bfch_t;
+
+/* A backflow determinant over the rows [first, last) of one group
+ * (backflow_slater_determinant.h): one orbital block, its channels, and the
+ * walker-record offsets of x (quasi-coordinates), A = M⁻¹, F = A^T ∇φ(x)
+ * and (log|det|, sign). */
+typedef struct {
+    int first, last, type;
+    const double *k, *is_sin, *centers, *alphas;
+    int nch; bfch_t ch[4];
+    long o_x, o_A, o_F, o_ls;
+} bfdet_t;
+
 typedef struct {
     int first, last, type;         /* type 0 plane waves, 1 Gaussians, 2 twisted plane waves */
     const double *k, *is_sin, *centers, *alphas;   /* type 2: k holds q = k + θ */
@@ -228,6 +245,7 @@ typedef struct {
        (0 when not a small integer), and the sum of their continuum tails */
     int nip; int ip[MAXC][4]; double ip_c[MAXC], ip_p[MAXC]; int ip_pint[MAXC];
     double ip_tail;
+    int nbf; bfdet_t bf[2];        /* backflow determinants (after the pair terms) */
     /* walker layout (offsets into one walker's double record) */
     long W, o_pos, o_dist, o_grad, o_lap, o_scal, o_lpc, o_gc, o_lc;
     long o_pgrad, o_plap, o_pgc, o_plc;   /* phase planes (complex determinant) */
@@ -462,6 +480,9 @@ static void ze_solution(const term_t* T, double r, double* u0, double* du0, doub
  *   ewald; if ewald: spline, r_cut, inv_eps, constant, nk, n1, n2, w
  *   ncoul; per term: pair[4], coef (q_a q_b / eps)
  *   nip; per term: pair[4], strength, exponent, tail   (optional: absent = 0)
+ *   nbf; per backflow determinant: first, last, type, type 0: k, is_sin;
+ *        type 1: centers, alphas; nch; per channel: source_first, source_last,
+ *        C, L, ncoef, coeffs[ncoef]   (optional)
  */
 static int blob_read(sys_t* s, const double* blob, long n) {
     rd_t r = {blob, n, 0, 0};
@@ -605,6 +626,38 @@ static int blob_read(sys_t* s, const double* blob, long n) {
             s->ip_pint[c] = (rp == s->ip_p[c] && rp <= 16.0) ? (int)rp : 0;
         }
     }
+    s->nbf = 0;
+    if (r.i < r.n) {
+        s->nbf = (int)rd(&r);
+        if (s->nbf > 2) return -9;
+        for (int d = 0; d < s->nbf; ++d) {
+            bfdet_t* D = &s->bf[d];
+            D->first = (int)rd(&r);
+            D->last = (int)rd(&r);
+            D->type = (int)rd(&r);
+            const int n = D->last - D->first;
+            if (n < 1 || n > 64) return -10;
+            if (D->type == 0) {
+                D->k = rdv(&r, (long)n * s->dim);
+                D->is_sin = rdv(&r, n);
+            } else {
+                D->centers = rdv(&r, (long)n * s->dim);
+                D->alphas = rdv(&r, n);
+            }
+            D->nch = (int)rd(&r);
+            if (D->nch > 4 || (long)n * s->np > BF_MAXE || s->dim != 2) return -11;
+            for (int c = 0; c < D->nch; ++c) {
+                bfch_t* C = &D->ch[c];
+                C->sf = (int)rd(&r);
+                C->sl = (int)rd(&r);
+                C->C = (int)rd(&r);
+                C->L = rd(&r);
+                C->nc = (int)rd(&r);
+                if (C->nc > 16 || C->nc < 1) return -12;
+                for (int q = 0; q < C->nc; ++q) C->c[q] = rd(&r);
+            }
+        }
+    }
     return r.bad ? -7 : 0;
 }
 
@@ -616,7 +669,7 @@ static void layout(sys_t* s) {
     s->o_grad = o; o += np * dim;
     s->o_lap = o; o += np * dim;
     s->o_scal = o; o += S_NSCAL;
-    s->ncomp = (s->nblocks ? 1 : 0) + s->nterms;
+    s->ncomp = (s->nblocks ? 1 : 0) + s->nterms + s->nbf;
     s->o_lpc = o; o += s->ncomp;
     s->o_gc = o; o += s->ncomp * np * dim;
     s->o_lc = o; o += s->ncomp * np * dim;
@@ -637,6 +690,14 @@ static void layout(sys_t* s) {
         const term_t* T = &s->terms[t];
         s->o_rho[t] = o; o += T->image ? 4L * T->nk : 0;
         s->o_pc[t] = o; o += T->image ? 2L * T->nk * T->n_cached : 0;
+    }
+    for (int d = 0; d < s->nbf; ++d) {
+        bfdet_t* D = &s->bf[d];
+        const long N = D->last - D->first;
+        D->o_x = o; o += N * dim;
+        D->o_A = o; o += N * N;
+        D->o_F = o; o += N * dim;
+        D->o_ls = o; o += 2;
     }
     s->W = o;
 }
@@ -1176,6 +1237,364 @@ static void cslater_evaluate(const sys_t* s, double* w) {
     memcpy(w + s->o_plap, plc, sizeof(double) * np * dim);
 }
 
+/* ───────────────────────── backflow determinant ──────────────────────
+ * backflow_slater_determinant.cpp / backflow_transformation.cpp: rows
+ * M[i][m] = φ_m(x_i), x_i = r_i + Σ_c Σ_j η_c(r_ij) r_ij (minimum image),
+ * inverted per move by pivoted Gauss-Jordan; ∂_kβ ln|D| = Σ F·J and
+ * ∂²_kβ ln|D| = Σ F·S + Σ_i vᵀT_i v - Σ_{ij} U_ji U_ij with the pair tables
+ * B(r) = η δ + η' r̂ r̂ᵀ r and s(r) = ∂²_β[η r_α]. */
+
+static int bf_comp(const sys_t* s, int d) { return (s->nblocks ? 1 : 0) + s->nterms + d; }
+
+static int bf_affects(const bfdet_t* D, int k) {
+    if (k >= D->first && k < D->last) return 1;
+    for (int c = 0; c < D->nch; ++c)
+        if (k >= D->ch[c].sf && k < D->ch[c].sl) return 1;
+    return 0;
+}
+
+/* η, η', η'' of a channel at r (backflow_function.h evaluate). */
+static void bf_eta(const bfch_t* C, double r, double* eta, double* e1, double* e2) {
+    if (r >= C->L) { *eta = *e1 = *e2 = 0.0; return; }
+    const double t = 1.0 - r / C->L;
+    double tc2 = 1.0;
+    for (int i = 0; i < C->C - 2; ++i) tc2 *= t;
+    const double f = tc2 * t * t;
+    const double fp = -(double)C->C / C->L * tc2 * t;
+    const double fpp = (double)C->C * (double)(C->C - 1) / (C->L * C->L) * tc2;
+    double P = 0.0, Pp = 0.0, Ppp = 0.0;
+    for (int k = C->nc - 1; k >= 0; --k) {
+        Ppp = Ppp * r + 2.0 * Pp;
+        Pp = Pp * r + P;
+        P = P * r + C->c[k];
+    }
+    *eta = f * P;
+    *e1 = fp * P + f * Pp;
+    *e2 = fpp * P + 2.0 * fp * Pp + f * Ppp;
+}
+
+/* One pair: sign η r_ij added to x; B and S (2x2) when B is given. */
+static int bf_pair(const sys_t* s, const bfch_t* C, const double* ri, const double* rj, double sign,
+                   double* x, double* B, double* S) {
+    double del[3] = {ri[0] - rj[0], ri[1] - rj[1], 0.0};
+    min_image(s, del);
+    const double r = sqrt(del[0] * del[0] + del[1] * del[1]);
+    if (r >= C->L) return 0;
+    double eta, e1, e2;
+    bf_eta(C, r, &eta, &e1, &e2);
+    for (int d = 0; d < 2; ++d) x[d] += sign * eta * del[d];
+    if (!B) return 1;
+    const double inv_r = r > 0.0 ? 1.0 / r : 0.0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            B[a * 2 + b] = (a == b ? eta : 0.0) + e1 * del[a] * del[b] * inv_r;
+            const double rb2 = del[b] * del[b] * inv_r * inv_r;
+            S[a * 2 + b] = (a == b ? 2.0 * e1 * del[b] * inv_r : 0.0) +
+                           del[a] * (e2 * rb2 + e1 * inv_r * (1.0 - rb2));
+        }
+    return 1;
+}
+
+/* pair tables of one configuration: [row * np + j] */
+typedef struct { double b[BF_MAXE * 4], sx[BF_MAXE * 4]; char lk[BF_MAXE]; } bftab_t;
+static bftab_t g_tab;
+
+static void bf_clear(int np, int e) {
+    g_tab.lk[e] = 0;
+    (void)np;
+    for (int q = 0; q < 4; ++q) g_tab.b[e * 4 + q] = g_tab.sx[e * 4 + q] = 0.0;
+}
+
+static void bf_full(const sys_t* s, const bfdet_t* D, const double* pos, double* x) {
+    const int np = s->np, N = D->last - D->first;
+    for (int t = 0; t < N; ++t) {
+        const int P = D->first + t;
+        double* xt = x + t * 2;
+        xt[0] = pos[P * 2];
+        xt[1] = pos[P * 2 + 1];
+        for (int j = 0; j < np; ++j) bf_clear(np, t * np + j);
+        for (int c = 0; c < D->nch; ++c)
+            for (int j = D->ch[c].sf; j < D->ch[c].sl; ++j) {
+                if (j == P) continue;
+                const int e = t * np + j;
+                g_tab.lk[e] = (char)bf_pair(s, &D->ch[c], pos + P * 2, pos + j * 2, 1.0, xt, g_tab.b + e * 4,
+                                            g_tab.sx + e * 4);
+            }
+    }
+}
+
+static void bf_particle_tables(const sys_t* s, const bfdet_t* D, const double* pos, int k, double* x) {
+    const int np = s->np, N = D->last - D->first;
+    const int tk = (k >= D->first && k < D->last) ? k - D->first : -1;
+    if (tk >= 0) {
+        double* xt = x + tk * 2;
+        xt[0] = pos[k * 2];
+        xt[1] = pos[k * 2 + 1];
+        for (int j = 0; j < np; ++j) bf_clear(np, tk * np + j);
+        for (int c = 0; c < D->nch; ++c)
+            for (int j = D->ch[c].sf; j < D->ch[c].sl; ++j) {
+                if (j == k) continue;
+                const int e = tk * np + j;
+                g_tab.lk[e] = (char)bf_pair(s, &D->ch[c], pos + k * 2, pos + j * 2, 1.0, xt, g_tab.b + e * 4,
+                                            g_tab.sx + e * 4);
+            }
+    }
+    for (int t = 0; t < N; ++t) {
+        const int P = D->first + t;
+        if (P == k) continue;
+        const int e = t * np + k;
+        bf_clear(np, e);
+        for (int c = 0; c < D->nch; ++c) {
+            if (k < D->ch[c].sf || k >= D->ch[c].sl) continue;
+            double unused[2] = {0, 0};
+            g_tab.lk[e] = (char)bf_pair(s, &D->ch[c], pos + P * 2, pos + k * 2, 1.0, unused, g_tab.b + e * 4,
+                                        g_tab.sx + e * 4);
+        }
+    }
+}
+
+static void bf_shift(const sys_t* s, const bfdet_t* D, const double* pos, int k, const double* old_r,
+                     double* x) {
+    for (int c = 0; c < D->nch; ++c) {
+        if (k < D->ch[c].sf || k >= D->ch[c].sl) continue;
+        for (int P = D->first; P < D->last; ++P) {
+            if (P == k) continue;
+            double* xt = x + (P - D->first) * 2;
+            bf_pair(s, &D->ch[c], pos + P * 2, pos + k * 2, 1.0, xt, NULL, NULL);
+            bf_pair(s, &D->ch[c], pos + P * 2, old_r, -1.0, xt, NULL, NULL);
+        }
+    }
+}
+
+/* orbitals with Hessians at x_i for every row: val[i*N+m], grad[(i*N+m)*2+a],
+ * hess[((i*N+m)*2+a)*2+b] */
+static void bf_rows(const sys_t* s, const bfdet_t* D, const double* x, double* val, double* grad,
+                    double* hess) {
+    const int N = D->last - D->first;
+    for (int i = 0; i < N; ++i)
+        for (int m = 0; m < N; ++m) {
+            const double* r = x + i * 2;
+            const int o = i * N + m;
+            if (D->type == 0) {
+                const double* km = D->k + m * 2;
+                const double ph = km[0] * r[0] + km[1] * r[1];
+                const double sn = sin(ph), c = cos(ph);
+                const double v = D->is_sin[m] != 0.0 ? sn : c;
+                const double dv = D->is_sin[m] != 0.0 ? c : -sn;
+                val[o] = v;
+                for (int a = 0; a < 2; ++a) {
+                    grad[o * 2 + a] = km[a] * dv;
+                    for (int b = 0; b < 2; ++b) hess[(o * 2 + a) * 2 + b] = -km[a] * km[b] * v;
+                }
+            } else {
+                const double al = D->alphas[m];
+                double del[3] = {r[0] - D->centers[m * 2], r[1] - D->centers[m * 2 + 1], 0.0};
+                min_image(s, del);
+                const double phi = exp(-al * (del[0] * del[0] + del[1] * del[1]));
+                val[o] = phi;
+                for (int a = 0; a < 2; ++a) {
+                    grad[o * 2 + a] = -2.0 * al * del[a] * phi;
+                    for (int b = 0; b < 2; ++b)
+                        hess[(o * 2 + a) * 2 + b] = (4.0 * al * al * del[a] * del[b] - (a == b ? 2.0 * al : 0.0)) * phi;
+                }
+            }
+        }
+}
+
+/* Pivoted Gauss-Jordan with log|det| and sign (m destroyed); 0 if singular. */
+static int bf_invert(int n, double* m, double* a, double* log_det, double* sign) {
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) a[r * n + c] = r == c ? 1.0 : 0.0;
+    *log_det = 0.0;
+    *sign = 1.0;
+    for (int k = 0; k < n; ++k) {
+        int piv = k;
+        for (int r = k + 1; r < n; ++r)
+            if (fabs(m[r * n + k]) > fabs(m[piv * n + k])) piv = r;
+        const double diag = m[piv * n + k];
+        if (diag == 0.0 || !isfinite(diag)) return 0;
+        *log_det += log(fabs(diag));
+        if (diag < 0.0) *sign = -*sign;
+        if (piv != k) {
+            for (int c = 0; c < n; ++c) {
+                double t = m[k * n + c]; m[k * n + c] = m[piv * n + c]; m[piv * n + c] = t;
+                t = a[k * n + c]; a[k * n + c] = a[piv * n + c]; a[piv * n + c] = t;
+            }
+            *sign = -*sign;
+        }
+        const double inv = 1.0 / diag;
+        for (int c = k + 1; c < n; ++c) m[k * n + c] *= inv;
+        for (int c = 0; c < n; ++c) a[k * n + c] *= inv;
+        for (int r = 0; r < n; ++r) {
+            if (r == k) continue;
+            const double f = m[r * n + k];
+            if (f == 0.0) continue;
+            for (int c = k + 1; c < n; ++c) m[r * n + c] -= f * m[k * n + c];
+            for (int c = 0; c < n; ++c) a[r * n + c] -= f * a[k * n + c];
+        }
+    }
+    return 1;
+}
+
+/* F_iα = Σ_m A[m][i] ∂_α φ_m(x_i) */
+static void bf_f(int N, const double* A, const double* grad, double* F) {
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < 2; ++a) {
+            double acc = 0.0;
+            for (int m = 0; m < N; ++m) acc += A[m * N + i] * grad[(i * N + m) * 2 + a];
+            F[i * 2 + a] = acc;
+        }
+}
+
+/* v = Jacobian column (k, β) over the rows; returns Σ F·S. */
+static double bf_jcol(const sys_t* s, const bfdet_t* D, const double* F, int k, int beta, double* v) {
+    const int np = s->np, N = D->last - D->first;
+    for (int q = 0; q < N * 2; ++q) v[q] = 0.0;
+    double fs = 0.0;
+    const int tk = (k >= D->first && k < D->last) ? k - D->first : -1;
+    if (tk >= 0) {
+        double* vk = v + tk * 2;
+        vk[beta] = 1.0;
+        for (int j = 0; j < np; ++j) {
+            const int e = tk * np + j;
+            if (!g_tab.lk[e]) continue;
+            for (int a = 0; a < 2; ++a) {
+                vk[a] += g_tab.b[e * 4 + a * 2 + beta];
+                fs += F[tk * 2 + a] * g_tab.sx[e * 4 + a * 2 + beta];
+            }
+        }
+    }
+    for (int t = 0; t < N; ++t) {
+        const int e = t * np + k;
+        if (t == tk || !g_tab.lk[e]) continue;
+        for (int a = 0; a < 2; ++a) {
+            v[t * 2 + a] = -g_tab.b[e * 4 + a * 2 + beta];
+            fs += F[t * 2 + a] * g_tab.sx[e * 4 + a * 2 + beta];
+        }
+    }
+    return fs;
+}
+
+/* ∂_k ln|D| = Σ_t F_t · ∂x_t/∂r_k */
+static void bf_gradient(const sys_t* s, const bfdet_t* D, const double* F, int k, double* out) {
+    const int np = s->np, N = D->last - D->first;
+    out[0] = out[1] = 0.0;
+    const int tk = (k >= D->first && k < D->last) ? k - D->first : -1;
+    if (tk >= 0) {
+        const double* Fk = F + tk * 2;
+        out[0] += Fk[0];
+        out[1] += Fk[1];
+        for (int j = 0; j < np; ++j) {
+            const int e = tk * np + j;
+            if (!g_tab.lk[e]) continue;
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) out[b] += Fk[a] * g_tab.b[e * 4 + a * 2 + b];
+        }
+    }
+    for (int t = 0; t < N; ++t) {
+        const int e = t * np + k;
+        if (t == tk || !g_tab.lk[e]) continue;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) out[b] -= F[t * 2 + a] * g_tab.b[e * 4 + a * 2 + b];
+    }
+}
+
+/* Every particle's gradient and Laplacian from committed A, F and rows
+ * (BackflowSlaterDeterminant::all_derivatives). */
+static void bf_all(const sys_t* s, const bfdet_t* D, const double* A, const double* F, const double* grad,
+                   const double* hess, double* g_out, double* l_out) {
+    const int np = s->np, N = D->last - D->first;
+    static double T[64 * 4], G[2][64 * 64], v[128], U[64 * 64];
+    for (int i = 0; i < N; ++i)
+        for (int ag = 0; ag < 4; ++ag) {
+            double acc = 0.0;
+            for (int m = 0; m < N; ++m) acc += A[m * N + i] * hess[(i * N + m) * 4 + ag];
+            T[i * 4 + ag] = acc;
+        }
+    for (int a = 0; a < 2; ++a)
+        for (int j = 0; j < N; ++j)
+            for (int r = 0; r < N; ++r) {
+                double acc = 0.0;
+                for (int m = 0; m < N; ++m) acc += A[m * N + j] * grad[(r * N + m) * 2 + a];
+                G[a][j * N + r] = acc;
+            }
+    for (int k = 0; k < np; ++k) {
+        g_out[k * 2] = g_out[k * 2 + 1] = l_out[k * 2] = l_out[k * 2 + 1] = 0.0;
+        if (!bf_affects(D, k)) continue;
+        bf_gradient(s, D, F, k, g_out + k * 2);
+        for (int beta = 0; beta < 2; ++beta) {
+            double l = bf_jcol(s, D, F, k, beta, v);
+            for (int i = 0; i < N; ++i)
+                for (int a = 0; a < 2; ++a)
+                    for (int g = 0; g < 2; ++g) l += v[i * 2 + a] * v[i * 2 + g] * T[i * 4 + a * 2 + g];
+            for (int j = 0; j < N; ++j)
+                for (int r = 0; r < N; ++r)
+                    U[j * N + r] = v[r * 2] * G[0][j * N + r] + v[r * 2 + 1] * G[1][j * N + r];
+            double uu = 0.0;
+            for (int j = 0; j < N; ++j)
+                for (int r = 0; r < N; ++r) uu += U[j * N + r] * U[r * N + j];
+            l_out[k * 2 + beta] = l - uu;
+        }
+    }
+}
+
+static double g_bval[64 * 64], g_bgrad[64 * 64 * 2], g_bhess[64 * 64 * 4], g_bwork[64 * 64];
+
+static void bf_evaluate(const sys_t* s, double* w, int d) {
+    const bfdet_t* D = &s->bf[d];
+    const int N = D->last - D->first, np = s->np, c = bf_comp(s, d);
+    double* x = w + D->o_x;
+    double* A = w + D->o_A;
+    double* F = w + D->o_F;
+    double* ls = w + D->o_ls;
+    bf_full(s, D, POS(s, w), x);
+    bf_rows(s, D, x, g_bval, g_bgrad, g_bhess);
+    memcpy(g_bwork, g_bval, sizeof(double) * N * N);
+    if (!bf_invert(N, g_bwork, A, &ls[0], &ls[1])) SC(s, w)[S_ERR] = 1.0;
+    bf_f(N, A, g_bgrad, F);
+    bf_all(s, D, A, F, g_bgrad, g_bhess, GC(s, w, c), LC(s, w, c));
+    LPC(s, w)[c] = ls[0];
+    (void)np;
+}
+
+/* refresh_walker: x rebuilt from the positions, every particle's derivatives
+ * from the committed A and F, into the component and (by difference) the
+ * totals. */
+static void bf_refresh_all(const sys_t* s, double* w, int d) {
+    const bfdet_t* D = &s->bf[d];
+    const int np = s->np, c = bf_comp(s, d);
+    double* x = w + D->o_x;
+    bf_full(s, D, POS(s, w), x);
+    bf_rows(s, D, x, g_bval, g_bgrad, g_bhess);
+    static double go[2048], lo[2048];
+    bf_all(s, D, w + D->o_A, w + D->o_F, g_bgrad, g_bhess, go, lo);
+    double* gc = GC(s, w, c);
+    double* lc = LC(s, w, c);
+    for (int j = 0; j < np * 2; ++j) {
+        if (go[j] != gc[j]) GRAD(s, w)[j] = (GRAD(s, w)[j] - gc[j]) + go[j];
+        if (lo[j] != lc[j]) LAP(s, w)[j] = (LAP(s, w)[j] - lc[j]) + lo[j];
+        gc[j] = go[j];
+        lc[j] = lo[j];
+    }
+}
+
+/* refresh_particle_derivatives: the gradient of p only (what a drift reads). */
+static void bf_refresh_particle(const sys_t* s, double* w, int d, int p) {
+    const bfdet_t* D = &s->bf[d];
+    if (!bf_affects(D, p)) return;
+    const int c = bf_comp(s, d);
+    static double xs[128];
+    bf_particle_tables(s, D, POS(s, w), p, xs);
+    double g[2];
+    bf_gradient(s, D, w + D->o_F, p, g);
+    double* gc = GC(s, w, c);
+    for (int k = 0; k < 2; ++k) {
+        const int j = p * 2 + k;
+        if (g[k] != gc[j]) GRAD(s, w)[j] = (GRAD(s, w)[j] - gc[j]) + g[k];
+        gc[j] = g[k];
+    }
+}
+
 /* ───────────────────────── move scratch ─────────────────────────────── */
 
 typedef struct {
@@ -1186,6 +1605,9 @@ typedef struct {
     double pg[MAXT][3], pl[MAXT][3];    /* per-term pending grad/lap */
     double rad[MAXT][1024][6];          /* u_old, du_old, d2u_old, u_new, du_new, d2u_new */
     double pc[MAXT][512], ps[MAXT][512];/* pending phases */
+    /* backflow: pending x, A, F, (log|det|, sign), p's gradient, validity */
+    double bx[2][128], bA[2][64 * 64], bF[2][128], bls[2][2], bg[2][2];
+    int bvalid[2], bused[2];
 } move_t;
 
 /* Does term T couple particles p and k?  Calls f for every partner of p. */
@@ -1310,6 +1732,7 @@ static void psi_evaluate(const sys_t* s, double* w) {
         else slater_evaluate(s, w);
     }
     for (int t = 0; t < s->nterms; ++t) term_evaluate(s, w, t);
+    for (int d = 0; d < s->nbf; ++d) bf_evaluate(s, w, d);
     double lp = 0.0;
     memset(GRAD(s, w), 0, sizeof(double) * n);
     memset(LAP(s, w), 0, sizeof(double) * n);
@@ -1459,6 +1882,7 @@ int o_init(void* p, double* walkers, long nw, const double* pos_aos) {
 }
 
 void o_refresh_all(const sys_t* s, double* w) {
+    for (int d = 0; d < s->nbf; ++d) bf_refresh_all(s, w, d);
     if (s->cplx) return;   /* the complex determinant keeps its derivatives current */
     for (int b = 0; b < s->nblocks; ++b)
         for (int q = s->blocks[b].first; q < s->blocks[b].last; ++q) slater_refresh(s, w, q);
@@ -1608,6 +2032,39 @@ static void ratio(const sys_t* s, const double* w, int p, move_t* mv) {
             mv->new_grad[d] += mv->pg[t][d];
             mv->new_lap[d] += mv->pl[t][d];
         }
+    }
+    /* backflow determinants: BackflowSlaterDeterminant::ratio_batch, without the
+       proposal Laplacian (the VMC/DMC drivers switch it off) */
+    for (int d = 0; d < s->nbf; ++d) {
+        const bfdet_t* D = &s->bf[d];
+        mv->bused[d] = bf_affects(D, p);
+        mv->bvalid[d] = 0;
+        if (!mv->bused[d]) continue;
+        const int N = D->last - D->first;
+        static double pos2[2048];
+        memcpy(pos2, pos, sizeof(double) * np * dim);
+        const double old_r[2] = {pos[p * 2], pos[p * 2 + 1]};
+        pos2[p * 2] = mv->new_pos[0];
+        pos2[p * 2 + 1] = mv->new_pos[1];
+        double* x = mv->bx[d];
+        memcpy(x, w + D->o_x, sizeof(double) * N * 2);
+        bf_shift(s, D, pos2, p, old_r, x);
+        bf_particle_tables(s, D, pos2, p, x);
+        bf_rows(s, D, x, g_bval, g_bgrad, g_bhess);
+        memcpy(g_bwork, g_bval, sizeof(double) * N * N);
+        const double* ls = w + D->o_ls;
+        if (!bf_invert(N, g_bwork, mv->bA[d], &mv->bls[d][0], &mv->bls[d][1])) {
+            mv->log_ratio += -700.0;
+            mv->bg[d][0] = mv->bg[d][1] = 0.0;
+            continue;
+        }
+        mv->bvalid[d] = 1;
+        mv->log_ratio += mv->bls[d][0] - ls[0];
+        if (mv->bls[d][1] * ls[1] < 0.0) mv->phase += 3.14159265358979323846;
+        bf_f(N, mv->bA[d], g_bgrad, mv->bF[d]);
+        bf_gradient(s, D, mv->bF[d], p, mv->bg[d]);
+        mv->new_grad[0] += mv->bg[d][0];
+        mv->new_grad[1] += mv->bg[d][1];
     }
 }
 
@@ -1842,6 +2299,25 @@ static void commit(const sys_t* s, double* w, int p, move_t* mv) {
             bl[p * dim + d] += dlp;
         }
     }
+    /* backflow determinants: the pending state becomes committed */
+    for (int d = 0; d < s->nbf; ++d) {
+        if (!mv->bused[d]) continue;
+        const bfdet_t* D = &s->bf[d];
+        const int N = D->last - D->first, c = bf_comp(s, d);
+        if (!mv->bvalid[d]) SC(s, w)[S_ERR] = 1.0;
+        memcpy(w + D->o_x, mv->bx[d], sizeof(double) * N * 2);
+        memcpy(w + D->o_A, mv->bA[d], sizeof(double) * N * N);
+        memcpy(w + D->o_F, mv->bF[d], sizeof(double) * N * 2);
+        const double old = w[D->o_ls];
+        w[D->o_ls] = mv->bls[d][0];
+        w[D->o_ls + 1] = mv->bls[d][1];
+        LPC(s, w)[c] = mv->bls[d][0];
+        SC(s, w)[S_LOGPSI] += mv->bls[d][0] - old;
+        for (int k = 0; k < 2; ++k) {
+            GC(s, w, c)[p * 2 + k] = mv->bg[d][k];
+            LC(s, w, c)[p * 2 + k] = 0.0;
+        }
+    }
     /* WalkerSet::apply_move: distance rows (masked commit form), position, wrap, grad/lap of p */
     double* dist = DIST(s, w);
     for (int k = 0; k < np; ++k) {
@@ -1908,7 +2384,10 @@ static long vmc_sweep_walker(const sys_t* s, double* w, const double* rnd, long 
     long acc = 0;
     move_t* mv = &g_mv;
     for (int p = 0; p < np; ++p) {
-        if (drift) slater_refresh(s, w, p);
+        if (drift) {
+            slater_refresh(s, w, p);
+            for (int d = 0; d < s->nbf; ++d) bf_refresh_particle(s, w, d, p);
+        }
         const double* gauss = rnd + (long)p * (dim + 1) * n;
         const double u = gauss[dim * n + iw];
         for (int d = 0; d < dim; ++d) {
@@ -1996,6 +2475,7 @@ static long dmc_sweep_walker(const sys_t* s, double* w, const double* rnd, long 
     double* sc = SC(s, w);
     for (int p = 0; p < np; ++p) {
         slater_refresh(s, w, p);
+        for (int d = 0; d < s->nbf; ++d) bf_refresh_particle(s, w, d, p);
         const double tm_p = tau * s->inv_mass[p * dim];
         const double* gauss = rnd + (long)p * (dim + 1) * stride;
         const double u = gauss[dim * stride + iw];

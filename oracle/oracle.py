@@ -127,6 +127,17 @@ def blob_from_setup(sd: Dict[str, Any]) -> np.ndarray:
     out.append(len(ip))
     for c in ip:
         out += [c["ga"][0], c["ga"][1], c["gb"][0], c["gb"][1], c["strength"], c["exponent"], c["tail"]]
+    bf = sd.get("backflow", [])
+    out.append(len(bf))
+    for b in bf:
+        out += [b["first"], b["last"], 0 if b["type"] == "plane_wave" else 1]
+        if b["type"] == "plane_wave":
+            out += list(b["k"]) + list(b["is_sin"])
+        else:
+            out += list(b["centers"]) + list(b["alphas"])
+        out.append(len(b["channels"]))
+        for c in b["channels"]:
+            out += [c["source_first"], c["source_last"], c["C"], c["L"], len(c["coeffs"])] + list(c["coeffs"])
     return np.asarray(out, dtype=np.float64)
 
 

@@ -43,6 +43,7 @@
 #include "population/walker_set.h"
 #include "qmc/dmc.h"
 #include "qmc/vmc.h"
+#include "wavefunction/backflow_slater_determinant.h"
 #include "wavefunction/complex_orbital_set.h"
 #include "wavefunction/complex_slater_determinant.h"
 #include "wavefunction/drummond_jastrow.h"
@@ -283,12 +284,71 @@ std::unique_ptr<System> build_heg(const Args& a) {
         j.close(']');
         s->psi.add_component(std::make_unique<ComplexSlaterDeterminant>(std::move(cblocks)));
     }
+    // Backflow (builders/slater.cpp:117-167): one backflow determinant per
+    // spin group (one plane-wave block), channels from the own group (like
+    // spin, c_1 derived) and from the other group, C = 3, L = the Wigner-Seitz
+    // inradius.
+    const bool backflow = geti(a, "bf", 0) != 0;
+    if (backflow && !twisted) {
+        const double c_like = getd(a, "bf_like", 0.3);
+        const double c_un0 = getd(a, "bf_un0", 0.2), c_un1 = getd(a, "bf_un1", 0.002);
+        const double L = s->cell.ws_radius();
+        j.key("backflow");
+        j.open('[');
+        for (std::size_t gi = 0; gi < s->groups.size(); ++gi) {
+            const ParticleGroup& g = s->groups[gi];
+            auto orb = make_plane_wave_orbitals(s->cell, g.size());
+            j.open('{');
+            j.ki("first", static_cast<long long>(g.first));
+            j.ki("last", static_cast<long long>(g.last));
+            j.ks("type", "plane_wave");
+            j.arr("k", orb->kvectors());
+            const ReciprocalShellTable t = reciprocal_shell_table(s->cell, g.size());
+            std::vector<double> is_sin(t.is_sin.begin(), t.is_sin.begin() + g.size());
+            j.arr("is_sin", is_sin);
+            std::vector<BackflowSlaterDeterminant::Channel> chans;
+            j.key("channels");
+            j.open('[');
+            for (std::size_t hi = 0; hi < s->groups.size(); ++hi) {
+                const ParticleGroup& h = s->groups[hi];
+                BackflowSlaterDeterminant::Channel ch;
+                ch.source_first = h.first;
+                ch.source_last = h.last;
+                ch.truncation = 3;
+                std::vector<double> full;   // c_0 .. c_N as BackflowFunction holds them
+                if (hi == gi) {
+                    ch.params = {Parameter{"", c_like, false}, Parameter{"", L, true}};
+                    full = {c_like, 3.0 * c_like / L};
+                } else {
+                    ch.params = {Parameter{"", c_un0, false}, Parameter{"", c_un1, false},
+                                 Parameter{"", L, true}};
+                    full = {c_un0, c_un1};
+                }
+                j.open('{');
+                j.ki("source_first", static_cast<long long>(h.first));
+                j.ki("source_last", static_cast<long long>(h.last));
+                j.ki("C", 3);
+                j.arr("coeffs", full);
+                j.kv("L", L);
+                j.close('}');
+                chans.push_back(std::move(ch));
+            }
+            j.close(']');
+            j.close('}');
+            std::vector<BackflowSlaterDeterminant::Block> bb;
+            bb.push_back({g.first, g.last, std::move(orb)});
+            s->psi.add_component(std::make_unique<BackflowSlaterDeterminant>(
+                std::move(bb), std::move(chans), s->cell));
+        }
+        j.close(']');
+    }
     // Slater: one plane-wave block per spin group (builders/slater.cpp:267).
     std::vector<SlaterDeterminant::Block> blocks;
-    if (!twisted) j.key("slater");
-    if (!twisted) j.open('[');
+    const bool plain = !twisted && !backflow;
+    if (plain) j.key("slater");
+    if (plain) j.open('[');
     for (const ParticleGroup& g : s->groups) {
-        if (twisted) break;
+        if (!plain) break;
         auto orb = make_plane_wave_orbitals(s->cell, g.size());
         j.open('{');
         j.ki("first", static_cast<long long>(g.first));
@@ -302,7 +362,7 @@ std::unique_ptr<System> build_heg(const Args& a) {
         j.close('}');
         blocks.push_back({g.first, g.last, std::move(orb)});
     }
-    if (!twisted) {
+    if (plain) {
         j.close(']');
         s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
     }

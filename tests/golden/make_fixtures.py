@@ -37,6 +37,7 @@ SYSTEMS = {
     "heg42": dict(system="heg", nu=21, nd=21, rs=30),
     "dipoles16": dict(system="dipoles", n=16),
     "heg10t": dict(system="heg", nu=5, nd=5, rs=30, tx=0.25, ty=0.125),
+    "heg10bf": dict(system="heg", nu=5, nd=5, rs=30, bf=1),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
@@ -46,12 +47,15 @@ VMC = {
     "dipoles16": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.0003),
     "heg10t": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=225.0),
     "heg10t_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
+    "heg10bf": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=225.0),
+    "heg10bf_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
 }
 DMC = {
     "exciton": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.05),
     "heg10": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
     "dipoles16": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=1e-5),
     "heg10t": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
+    "heg10bf": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
 }
 
 

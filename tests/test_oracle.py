@@ -12,7 +12,7 @@ from conftest import golden
 from oracle import Oracle
 from oracle.oracle import S_EL, S_LOGPSI, load_oracle_lib
 
-SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t"]
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t", "heg10bf"]
 
 
 def rel(a, b):
@@ -70,7 +70,7 @@ def test_oracle_evaluate_matches_reference(name):
 
 
 @pytest.mark.parametrize("name", ["exciton", "heg10", "heg10_drift", "crystal16", "dipoles16",
-                                  "heg10t", "heg10t_drift"])
+                                  "heg10t", "heg10t_drift", "heg10bf", "heg10bf_drift"])
 def test_oracle_vmc_matches_reference(name):
     r = golden(f"vmc_{name}.json")
     p = r["params"]
@@ -90,7 +90,7 @@ def test_oracle_vmc_matches_reference(name):
         assert np.array_equal(o.pos()[: p["nw"]], fp)
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t", "heg10bf"])
 def test_oracle_dmc_matches_reference(name):
     r = golden(f"dmc_{name}.json")
     p = r["params"]
