@@ -175,6 +175,27 @@ def pack_system(desc: Dict[str, Any]):
         V.a_first, V.a_last = int(c["ga"][0]), int(c["ga"][1])
         V.b_first, V.b_last = int(c["gb"][0]), int(c["gb"][1])
         V.strength, V.exponent, V.tail = float(c["strength"]), float(c["exponent"]), float(c["tail"])
+    bf = desc.get("backflow", [])
+    s.n_backflow = len(bf)
+    for i, b in enumerate(bf):
+        F = s.backflow[i]
+        F.first, F.last = int(b["first"]), int(b["last"])
+        if b["type"] == "plane_wave":
+            F.type = _capi.ORB_PLANE_WAVE
+            F.k = _dp(f64(b["k"]))
+            F.is_sin = _ip(i32(b["is_sin"]))
+        else:
+            F.type = _capi.ORB_GAUSSIAN
+            F.centers = _dp(f64(b["centers"]))
+            F.alphas = _dp(f64(b["alphas"]))
+        F.n_channels = len(b["channels"])
+        for q, ch in enumerate(b["channels"]):
+            C = F.channels[q]
+            C.source_first, C.source_last = int(ch["source_first"]), int(ch["source_last"])
+            C.C, C.L = int(ch["C"]), float(ch["L"])
+            C.n_coeffs = len(ch["coeffs"])
+            for k, v in enumerate(ch["coeffs"]):
+                C.coeffs[k] = float(v)
     return s, keep
 
 

@@ -73,13 +73,25 @@ class InversePower(ctypes.Structure):
                 ("exponent", ctypes.c_double), ("tail", ctypes.c_double)]
 
 
+class BackflowChannel(ctypes.Structure):
+    _fields_ = [("source_first", ctypes.c_int), ("source_last", ctypes.c_int), ("C", ctypes.c_int),
+                ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int), ("coeffs", ctypes.c_double * 16)]
+
+
+class Backflow(ctypes.Structure):
+    _fields_ = [("first", ctypes.c_int), ("last", ctypes.c_int), ("type", ctypes.c_int),
+                ("k", c_dp), ("is_sin", c_ip), ("centers", c_dp), ("alphas", c_dp),
+                ("n_channels", ctypes.c_int), ("channels", BackflowChannel * 4)]
+
+
 class System(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("n_particles", ctypes.c_int), ("periodic", ctypes.c_int),
                 ("lattice", ctypes.c_double * 9), ("n_groups", ctypes.c_int),
                 ("groups", Group * 8), ("n_blocks", ctypes.c_int), ("blocks", Orbitals * 4),
                 ("n_terms", ctypes.c_int), ("terms", PairTerm * 8), ("ewald", Ewald),
                 ("n_coulomb", ctypes.c_int), ("coulomb", Coulomb * 8), ("n_inverse_power", ctypes.c_int),
-                ("inverse_power", InversePower * 8)]
+                ("inverse_power", InversePower * 8), ("n_backflow", ctypes.c_int),
+                ("backflow", Backflow * 2)]
 
 
 class VmcParams(ctypes.Structure):

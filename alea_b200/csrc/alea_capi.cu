@@ -431,6 +431,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     std::vector<double> bessel_table;     // zero-energy terms' Chebyshev table (one per system)
     const double* bessel_dev = nullptr;   // patched to its device address
     std::vector<int> ze_terms;
+    std::vector<double> bf_sin[2];
     // groups
     if (in->n_groups < 1 || in->n_groups > kMaxGroups) return fail(c, ALEA_ERR_INVALID, "bad n_groups");
     s.ngroups = in->n_groups;
@@ -514,6 +515,55 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     for (int b = 0; b < s.nblocks; ++b) {
         s.blocks[b].orabs = static_cast<int>(o);
         o += round4(s.blocks[b].n);
+    }
+    // backflow determinants (BackflowSlaterDeterminant): x, A = M⁻¹, F, (log|det|, sign)
+    if (in->n_backflow < 0 || in->n_backflow > 2) return fail(c, ALEA_ERR_INVALID, "bad n_backflow");
+    s.nbf = in->n_backflow;
+    if (s.nbf > 0 && s.nblocks > 0)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "backflow determinants cannot be mixed with plain blocks");
+    if (s.nbf > 0 && np > 256) return fail(c, ALEA_ERR_UNSUPPORTED, "backflow needs at most 256 particles");
+    for (int d = 0; d < s.nbf; ++d) {
+        const alea_gpu_backflow& F = in->backflow[d];
+        DevBF& D = s.bf[d];
+        D.first = F.first;
+        D.last = F.last;
+        D.n = F.last - F.first;
+        D.type = F.type;
+        if (D.n < 1 || D.n > kMaxN || F.first < 0 || F.last > np)
+            return fail(c, ALEA_ERR_UNSUPPORTED, "backflow determinants must have 1..64 rows");
+        s.maxN = std::max(s.maxN, D.n);
+        if (F.type == ALEA_ORB_PLANE_WAVE) {
+            if (!F.k || !F.is_sin) return fail(c, ALEA_ERR_INVALID, "backflow plane waves without tables");
+            put(F.k, D.n * 2 * 8, reinterpret_cast<const void**>(&D.k));
+            bf_sin[d].resize(D.n);
+            for (int i = 0; i < D.n; ++i) bf_sin[d][i] = F.is_sin[i] ? 1.0 : 0.0;
+            put(bf_sin[d].data(), D.n * 8, reinterpret_cast<const void**>(&D.is_sin));
+        } else if (F.type == ALEA_ORB_GAUSSIAN) {
+            if (!F.centers || !F.alphas) return fail(c, ALEA_ERR_INVALID, "backflow Gaussians without tables");
+            put(F.centers, D.n * 2 * 8, reinterpret_cast<const void**>(&D.centers));
+            put(F.alphas, D.n * 8, reinterpret_cast<const void**>(&D.alphas));
+        } else {
+            return fail(c, ALEA_ERR_UNSUPPORTED, "backflow orbitals must be plane waves or Gaussians");
+        }
+        if (F.n_channels < 1 || F.n_channels > 4) return fail(c, ALEA_ERR_INVALID, "bad backflow channels");
+        D.nch = F.n_channels;
+        for (int q = 0; q < D.nch; ++q) {
+            const alea_gpu_backflow_channel& C = F.channels[q];
+            DevBFCh& E = D.ch[q];
+            if (C.source_first < 0 || C.source_last > np || C.source_first >= C.source_last || C.C < 2 ||
+                !(C.L > 0.0) || C.n_coeffs < 1 || C.n_coeffs > 16)
+                return fail(c, ALEA_ERR_INVALID, "bad backflow channel");
+            E.sf = C.source_first;
+            E.sl = C.source_last;
+            E.C = C.C;
+            E.L = C.L;
+            E.nc = C.n_coeffs;
+            for (int k = 0; k < E.nc; ++k) E.c[k] = C.coeffs[k];
+        }
+        D.oX = static_cast<int>(o); o += round4(2 * D.n);
+        D.oA = static_cast<int>(o); o += round4(D.n * D.n);
+        D.oF = static_cast<int>(o); o += round4(2 * D.n);
+        D.oLS = static_cast<int>(o); o += 4;
     }
     // pair terms and the shared Jastrow k set
     if (in->n_terms < 0 || in->n_terms > kMaxTerms) return fail(c, ALEA_ERR_INVALID, "bad n_terms");
@@ -754,7 +804,16 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     // One union: the per-partner scratch of a move (read by the commit before
     // any rebuild), the Gauss-Jordan work matrix, and the ρ(k) accumulators
     // of the local energy.
+    for (int d = 0; d < s.nbf; ++d) {   // a proposal's pending backflow state
+        DevBF& D = s.bf[d];
+        D.pX = take(2 * D.n);
+        D.pA = take(D.n * D.n);
+        D.pF = take(2 * D.n);
+        D.pM = take(8);
+    }
     long work = cf * s.maxN * s.maxN;
+    // backflow: rows ∇φ (2N²) and G^α (2N²), T (4N), Jacobian columns (4N)
+    for (int d = 0; d < s.nbf; ++d) work = std::max(work, 4L * s.bf[d].n * s.bf[d].n + 8L * s.bf[d].n);
     work = std::max(work, 2L * s.enk);
     work = std::max(work, static_cast<long>(np) * 10);
     s.s_work = take(work);

@@ -68,6 +68,27 @@ struct DevBlock {
     long oD, oDg, oDl;        // record offsets of D, ∇D, ∇²D (cold)
 };
 
+struct DevBFCh {
+    int sf, sl, C, nc;
+    double L;
+    double c[16];
+};
+
+// A backflow determinant: rows [first, last), orbitals, channels; offsets of
+// its committed x, A, F, (log|det|, sign) in the hot record and of its
+// pending copies (a proposal's) in the shared-memory scratch.
+struct DevBF {
+    int first, last, n, type;
+    const double* k;
+    const double* is_sin;
+    const double* centers;
+    const double* alphas;
+    int nch;
+    DevBFCh ch[4];
+    int oX, oA, oF, oLS;
+    int pX, pA, pF, pM;   // pM: log|det|', sign', g_x, g_y, valid
+};
+
 struct DevSys {
     int dim, np, periodic, ortho;
     double a[4], ainv[4], box[3], inv_box[3], cand[18], recip[4];
@@ -101,6 +122,8 @@ struct DevSys {
     int coul[kMaxCoulomb][4];
     double coul_coef[kMaxCoulomb];
     // inverse-power pair potentials C r^-p (integer p <= 16 by products, else pow)
+    int nbf;
+    DevBF bf[2];
     int nip;
     int ip[kMaxCoulomb][4];
     double ip_c[kMaxCoulomb], ip_p[kMaxCoulomb];

@@ -434,6 +434,468 @@ __device__ void c_refresh_all(const DevSys& s, const Smem& v) {
     __syncthreads();
 }
 
+// ───────────────────────── backflow determinant ───────────────────────
+//
+// BackflowSlaterDeterminant (backflow_slater_determinant.cpp,
+// backflow_transformation.cpp): M[i][m] = φ_m(x_i) with quasi-coordinates
+// x_i = r_i + Σ_c Σ_j η_c(r_ij) r_ij, η = (1 - r/L)^C Σ_k c_k r^k.  A move of
+// p shifts every row it displaces and rebuilds p's own row; the new matrix
+// is inverted by pivoted Gauss-Jordan (no rank-one update applies), which
+// gives the ratio of determinants and, with F = Aᵀ∇φ(x) and the pair
+// tensors B(r) = η δ + η' r̂ r̂ᵀ r, the moved particle's gradient.  The
+// determinant part of every particle's ∇ and ∂² ln ψ lives in sg/sl (a
+// backflow system has no plain blocks), refreshed before it is read.
+
+__device__ __forceinline__ void bf_eta(const DevBFCh& C, double r, double& eta, double& e1, double& e2) {
+    if (r >= C.L) {
+        eta = e1 = e2 = 0.0;
+        return;
+    }
+    const double t = 1.0 - r / C.L;
+    double tc2 = 1.0;
+    for (int i = 0; i < C.C - 2; ++i) tc2 *= t;
+    const double f = tc2 * t * t;
+    const double fp = -static_cast<double>(C.C) / C.L * tc2 * t;
+    const double fpp = static_cast<double>(C.C) * static_cast<double>(C.C - 1) / (C.L * C.L) * tc2;
+    double P = 0.0, Pp = 0.0, Ppp = 0.0;
+    for (int k = C.nc - 1; k >= 0; --k) {
+        Ppp = Ppp * r + 2.0 * Pp;
+        Pp = Pp * r + P;
+        P = P * r + C.c[k];
+    }
+    eta = f * P;
+    e1 = fp * P + f * Pp;
+    e2 = fpp * P + 2.0 * fp * Pp + f * Ppp;
+}
+
+// One pair r_ij = ri - rj (minimum image): adds sign·η r_ij to x; fills the
+// tensors B and S (2x2, row α, column β) when B is given.  False beyond L.
+__device__ __forceinline__ bool bf_pair(const DevSys& s, const DevBFCh& C, const double* ri, const double* rj,
+                                        double sign, double* x, double* B, double* S) {
+    double del[3] = {ri[0] - rj[0], ri[1] - rj[1], 0.0};
+    min_image(s, del);
+    const double r = sqrt(del[0] * del[0] + del[1] * del[1]);
+    if (r >= C.L) return false;
+    double eta, e1, e2;
+    bf_eta(C, r, eta, e1, e2);
+    x[0] += sign * eta * del[0];
+    x[1] += sign * eta * del[1];
+    if (B) {
+        const double inv_r = r > 0.0 ? 1.0 / r : 0.0;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                B[a * 2 + b] = (a == b ? eta : 0.0) + e1 * del[a] * del[b] * inv_r;
+                const double rb2 = del[b] * del[b] * inv_r * inv_r;
+                S[a * 2 + b] = (a == b ? 2.0 * e1 * del[b] * inv_r : 0.0) +
+                               del[a] * (e2 * rb2 + e1 * inv_r * (1.0 - rb2));
+            }
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool bf_affects(const DevBF& D, int k) {
+    if (k >= D.first && k < D.last) return true;
+    for (int c = 0; c < D.nch; ++c)
+        if (k >= D.ch[c].sf && k < D.ch[c].sl) return true;
+    return false;
+}
+
+// Orbital m at x: value, gradient, Hessian [a*2+b].
+__device__ __forceinline__ void bf_orbital(const DevSys& s, const DevBF& D, int m, const double* x, double& val,
+                                           double* g, double* h) {
+    if (D.type == 0) {
+        const double kx = D.k[m * 2], ky = D.k[m * 2 + 1];
+        double sn, c;
+        sincos(kx * x[0] + ky * x[1], &sn, &c);
+        const bool is_s = D.is_sin[m] != 0.0;
+        const double v = is_s ? sn : c, dv = is_s ? c : -sn;
+        val = v;
+        g[0] = kx * dv;
+        g[1] = ky * dv;
+        if (h) {
+            h[0] = -kx * kx * v;
+            h[1] = h[2] = -kx * ky * v;
+            h[3] = -ky * ky * v;
+        }
+    } else {
+        const double al = D.alphas[m];
+        double del[3] = {x[0] - D.centers[m * 2], x[1] - D.centers[m * 2 + 1], 0.0};
+        min_image(s, del);
+        const double phi = exp(-al * (del[0] * del[0] + del[1] * del[1]));
+        val = phi;
+        g[0] = -2.0 * al * del[0] * phi;
+        g[1] = -2.0 * al * del[1] * phi;
+        if (h) {
+            h[0] = (4.0 * al * al * del[0] * del[0] - 2.0 * al) * phi;
+            h[1] = h[2] = 4.0 * al * al * del[0] * del[1] * phi;
+            h[3] = (4.0 * al * al * del[1] * del[1] - 2.0 * al) * phi;
+        }
+    }
+}
+
+// Pivoted Gauss-Jordan of m (N×N, destroyed) into a, with log|det| and sign
+// to out[0], out[1] and out[2] = 1 when regular (pivot of largest modulus,
+// ties to the lowest row).
+template <int NT>
+__device__ void bf_invert(int N, double* m, double* a, double* col, double* out) {
+    __syncthreads();
+    for_each_elem<NT>(N, [&](int r, int c) { a[r * N + c] = (r == c) ? 1.0 : 0.0; });
+    if (threadIdx.x == 0) {
+        out[0] = 0.0;
+        out[1] = 1.0;
+        out[2] = 1.0;
+    }
+    __syncthreads();
+    __shared__ int s_piv;
+    for (int k = 0; k < N; ++k) {
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = N;
+            for (int r = k + static_cast<int>(threadIdx.x); r < N; r += 32) {
+                const double v = fabs(m[r * N + k]);
+                if (v > best) {
+                    best = v;
+                    bi = r;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                s_piv = bi;
+                const double diag = m[bi * N + k];
+                if (diag == 0.0 || !isfinite(diag)) {
+                    out[2] = 0.0;
+                } else {
+                    out[0] += log(fabs(diag));
+                    if (diag < 0.0) out[1] = -out[1];
+                    if (bi != k) out[1] = -out[1];
+                }
+            }
+        }
+        __syncthreads();
+        if (out[2] == 0.0) return;
+        const int piv = s_piv;
+        if (piv != k)
+            for (int c = threadIdx.x; c < N; c += NT) {
+                double t = m[k * N + c]; m[k * N + c] = m[piv * N + c]; m[piv * N + c] = t;
+                t = a[k * N + c]; a[k * N + c] = a[piv * N + c]; a[piv * N + c] = t;
+            }
+        __syncthreads();
+        const double inv = 1.0 / m[k * N + k];
+        __syncthreads();
+        for (int c = threadIdx.x; c < N; c += NT) {
+            m[k * N + c] *= inv;
+            a[k * N + c] *= inv;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < N; r += NT) col[r] = m[r * N + k];
+        __syncthreads();
+        for_each_elem<NT>(N, [&](int r, int c) {
+            if (r == k) return;
+            const double f = col[r];
+            m[r * N + c] -= f * m[k * N + c];
+            a[r * N + c] -= f * a[k * N + c];
+        });
+        __syncthreads();
+    }
+}
+
+// x_t from scratch: r_t + Σ_c Σ_j η(r_tj) r_tj, with particle `moved` at npos.
+__device__ __forceinline__ void bf_row_x(const DevSys& s, const DevBF& D, const double* pos, int moved,
+                                         const double* npos, int P, double* xt) {
+    const double* rp = P == moved ? npos : pos + P * 2;
+    xt[0] = rp[0];
+    xt[1] = rp[1];
+    for (int c = 0; c < D.nch; ++c)
+        for (int j = D.ch[c].sf; j < D.ch[c].sl; ++j) {
+            if (j == P) continue;
+            const double* rj = j == moved ? npos : pos + j * 2;
+            bf_pair(s, D.ch[c], rp, rj, 1.0, xt, nullptr, nullptr);
+        }
+}
+
+// ∂_k ln|D| = F_k (1 + Σ_j B(r_kj)) - Σ_t F_t B(r_tk) at the given positions,
+// summed over the CTA (all threads return it).
+template <int NT>
+__device__ void bf_grad_of(const DevSys& s, const Smem& v, const DevBF& D, const double* F, int k, int moved,
+                           const double* npos, double* g) {
+    const int N = D.n, np = s.np;
+    const double* rk = k == moved ? npos : v.pos + k * 2;
+    const int tk = (k >= D.first && k < D.last) ? k - D.first : -1;
+    double acc[2] = {0.0, 0.0};
+    // own row: F_k e_β and F_k·B(r_kj) over the sources
+    if (tk >= 0) {
+        const double* Fk = F + tk * 2;
+        if (threadIdx.x == 0) {
+            acc[0] += Fk[0];
+            acc[1] += Fk[1];
+        }
+        for (int j = threadIdx.x; j < np; j += NT) {
+            if (j == k) continue;
+            const double* rj = j == moved ? npos : v.pos + j * 2;
+            for (int c = 0; c < D.nch; ++c) {
+                if (j < D.ch[c].sf || j >= D.ch[c].sl) continue;
+                double unused[2] = {0, 0}, B[4], S[4];
+                if (!bf_pair(s, D.ch[c], rk, rj, 1.0, unused, B, S)) continue;
+                for (int a = 0; a < 2; ++a)
+                    for (int b = 0; b < 2; ++b) acc[b] += Fk[a] * B[a * 2 + b];
+            }
+        }
+    }
+    // the rows that k displaces: - F_t·B(r_tk)
+    for (int t = threadIdx.x; t < N; t += NT) {
+        const int P = D.first + t;
+        if (P == k) continue;
+        const double* rt = P == moved ? npos : v.pos + P * 2;
+        for (int c = 0; c < D.nch; ++c) {
+            if (k < D.ch[c].sf || k >= D.ch[c].sl) continue;
+            double unused[2] = {0, 0}, B[4], S[4];
+            if (!bf_pair(s, D.ch[c], rt, rk, 1.0, unused, B, S)) continue;
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) acc[b] -= F[t * 2 + a] * B[a * 2 + b];
+        }
+    }
+    block_sum<NT>(acc, v.red);
+    g[0] = acc[0];
+    g[1] = acc[1];
+}
+
+// The proposal of p for determinant d: pending x', A', F', (log|det|', sign'),
+// p's gradient and validity in the pending area.
+template <int NT>
+__device__ void bf_propose(const DevSys& s, const Smem& v, int d, int p) {
+    const DevBF& D = s.bf[d];
+    const int N = D.n;
+    double* sm = v.scal - s.o_scal;   // shared-memory base
+    const double* x = sm + D.oX;
+    double* px = sm + D.pX;
+    double* pa = sm + D.pA;
+    double* pf = sm + D.pF;
+    double* pm = sm + D.pM;
+    // x': shift the rows p displaces, rebuild p's own row
+    for (int t = threadIdx.x; t < N; t += NT) {
+        const int P = D.first + t;
+        if (P == p) {
+            bf_row_x(s, D, v.pos, p, v.newpos, P, px + t * 2);
+            continue;
+        }
+        double xt[2] = {x[t * 2], x[t * 2 + 1]};
+        for (int c = 0; c < D.nch; ++c) {
+            if (p < D.ch[c].sf || p >= D.ch[c].sl) continue;
+            bf_pair(s, D.ch[c], v.pos + P * 2, v.newpos, 1.0, xt, nullptr, nullptr);
+            bf_pair(s, D.ch[c], v.pos + P * 2, v.pos + p * 2, -1.0, xt, nullptr, nullptr);
+        }
+        px[t * 2] = xt[0];
+        px[t * 2 + 1] = xt[1];
+    }
+    __syncthreads();
+    double* mrows = v.work;
+    for_each_elem<NT>(N, [&](int i, int m) {
+        double val, g[2];
+        bf_orbital(s, D, m, px + i * 2, val, g, nullptr);
+        mrows[i * N + m] = val;
+    });
+    bf_invert<NT>(N, mrows, pa, v.col, pm);
+    if (pm[2] == 0.0) {
+        __syncthreads();
+        return;
+    }
+    // F'_i = Σ_m A'[m][i] ∇φ_m(x'_i)
+    for (int i = threadIdx.x; i < N; i += NT) {
+        double f0 = 0.0, f1 = 0.0;
+        for (int m = 0; m < N; ++m) {
+            double val, g[2];
+            bf_orbital(s, D, m, px + i * 2, val, g, nullptr);
+            const double a = pa[m * N + i];
+            f0 += a * g[0];
+            f1 += a * g[1];
+        }
+        pf[i * 2] = f0;
+        pf[i * 2 + 1] = f1;
+    }
+    __syncthreads();
+    double g[2];
+    bf_grad_of<NT>(s, v, D, pf, p, p, v.newpos, g);
+    if (threadIdx.x == 0) {
+        pm[3] = g[0];
+        pm[4] = g[1];
+    }
+    __syncthreads();
+}
+
+// Every particle's determinant gradient and Laplacian of backflow
+// determinant d from the committed A and F, with x rebuilt from the
+// positions (BackflowSlaterDeterminant::refresh_walker); added into
+// sg/sl (zeroed by the caller).  evaluate != 0: the matrix is inverted and F
+// formed first (a full evaluation).
+template <int NT>
+__device__ void bf_derivatives(const DevSys& s, const Smem& v, int d, bool evaluate) {
+    const DevBF& D = s.bf[d];
+    const int N = D.n, np = s.np;
+    double* sm = v.scal - s.o_scal;
+    double* x = sm + D.oX;
+    double* A = sm + D.oA;
+    double* F = sm + D.oF;
+    double* ls = sm + D.oLS;
+    for (int t = threadIdx.x; t < N; t += NT) bf_row_x(s, D, v.pos, -1, nullptr, D.first + t, x + t * 2);
+    __syncthreads();
+    double* grow = v.work;                 // ∇φ_m(x_r) [(r*N + m)*2 + α]
+    double* G = v.work + 2 * N * N;        // G^α[j][r] at [α*N*N + j*N + r]
+    double* T = G + 2 * N * N;             // T_i [i*4 + αγ]
+    double* V = T + 4 * N;                 // Jacobian columns [β][t*2 + α]
+    if (evaluate) {
+        for_each_elem<NT>(N, [&](int i, int m) {
+            double val, g[2];
+            bf_orbital(s, D, m, x + i * 2, val, g, nullptr);
+            grow[i * N + m] = val;
+        });
+        bf_invert<NT>(N, grow, A, v.col, v.misc + M_U);   // misc[M_U..M_U+2] scratch
+        if (threadIdx.x == 0) {
+            ls[0] = v.misc[M_U];
+            ls[1] = v.misc[M_U + 1];
+            if (v.misc[M_U + 2] == 0.0) v.scal[S_ERR] = 1.0;
+        }
+        __syncthreads();
+    }
+    for_each_elem<NT>(N, [&](int r, int m) {
+        double val, g[2];
+        bf_orbital(s, D, m, x + r * 2, val, g, nullptr);
+        grow[(r * N + m) * 2] = g[0];
+        grow[(r * N + m) * 2 + 1] = g[1];
+    });
+    __syncthreads();
+    if (evaluate) {
+        for (int i = threadIdx.x; i < N; i += NT) {
+            double f0 = 0.0, f1 = 0.0;
+            for (int m = 0; m < N; ++m) {
+                f0 += A[m * N + i] * grow[(i * N + m) * 2];
+                f1 += A[m * N + i] * grow[(i * N + m) * 2 + 1];
+            }
+            F[i * 2] = f0;
+            F[i * 2 + 1] = f1;
+        }
+    }
+    for (int i = threadIdx.x; i < N; i += NT) {
+        double t4[4] = {0, 0, 0, 0};
+        for (int m = 0; m < N; ++m) {
+            double val, g[2], h[4];
+            bf_orbital(s, D, m, x + i * 2, val, g, h);
+            for (int q = 0; q < 4; ++q) t4[q] += A[m * N + i] * h[q];
+        }
+        for (int q = 0; q < 4; ++q) T[i * 4 + q] = t4[q];
+    }
+    for_each_elem<NT>(N, [&](int j, int r) {
+        double g0 = 0.0, g1 = 0.0;
+        for (int m = 0; m < N; ++m) {
+            g0 += A[m * N + j] * grow[(r * N + m) * 2];
+            g1 += A[m * N + j] * grow[(r * N + m) * 2 + 1];
+        }
+        G[j * N + r] = g0;
+        G[N * N + j * N + r] = g1;
+    });
+    __syncthreads();
+    for (int k = 0; k < np; ++k) {
+        if (!bf_affects(D, k)) continue;
+        const int tk = (k >= D.first && k < D.last) ? k - D.first : -1;
+        // Jacobian columns v_β (β = 0, 1) over the rows, and Σ F·S
+        double fs[2] = {0.0, 0.0};
+        for (int t = threadIdx.x; t < N; t += NT) {
+            double vt[2][2] = {{0, 0}, {0, 0}};
+            const int P = D.first + t;
+            if (t == tk) {
+                vt[0][0] = 1.0;
+                vt[1][1] = 1.0;
+                for (int c = 0; c < D.nch; ++c)
+                    for (int j = D.ch[c].sf; j < D.ch[c].sl; ++j) {
+                        if (j == k) continue;
+                        double unused[2] = {0, 0}, B[4], S[4];
+                        if (!bf_pair(s, D.ch[c], v.pos + k * 2, v.pos + j * 2, 1.0, unused, B, S)) continue;
+                        for (int be = 0; be < 2; ++be)
+                            for (int a = 0; a < 2; ++a) {
+                                vt[be][a] += B[a * 2 + be];
+                                fs[be] += F[t * 2 + a] * S[a * 2 + be];
+                            }
+                    }
+            } else {
+                for (int c = 0; c < D.nch; ++c) {
+                    if (k < D.ch[c].sf || k >= D.ch[c].sl) continue;
+                    double unused[2] = {0, 0}, B[4], S[4];
+                    if (!bf_pair(s, D.ch[c], v.pos + P * 2, v.pos + k * 2, 1.0, unused, B, S)) continue;
+                    for (int be = 0; be < 2; ++be)
+                        for (int a = 0; a < 2; ++a) {
+                            vt[be][a] = -B[a * 2 + be];
+                            fs[be] += F[t * 2 + a] * S[a * 2 + be];
+                        }
+                }
+            }
+            for (int be = 0; be < 2; ++be) {
+                V[be * 2 * N + t * 2] = vt[be][0];
+                V[be * 2 * N + t * 2 + 1] = vt[be][1];
+            }
+        }
+        __syncthreads();
+        // Σ_t vᵀ T_t v and - Σ_{j,r} U_jr U_rj, U_jr = Σ_α v_rα G^α[j][r]
+        double acc[4] = {fs[0], fs[1], 0.0, 0.0};
+        for (int t = threadIdx.x; t < N; t += NT)
+            for (int be = 0; be < 2; ++be) {
+                const double* vt = V + be * 2 * N + t * 2;
+                const double* Tt = T + t * 4;
+                acc[be] += vt[0] * vt[0] * Tt[0] + vt[0] * vt[1] * (Tt[1] + Tt[2]) + vt[1] * vt[1] * Tt[3];
+            }
+        for_each_elem<NT>(N, [&](int j, int r) {
+            for (int be = 0; be < 2; ++be) {
+                const double* Vb = V + be * 2 * N;
+                const double ujr = Vb[r * 2] * G[j * N + r] + Vb[r * 2 + 1] * G[N * N + j * N + r];
+                const double urj = Vb[j * 2] * G[r * N + j] + Vb[j * 2 + 1] * G[N * N + r * N + j];
+                acc[be] -= ujr * urj;
+            }
+        });
+        block_sum<NT>(acc, v.red);
+        double g[2];
+        bf_grad_of<NT>(s, v, D, F, k, -1, nullptr, g);
+        if (threadIdx.x == 0) {
+            v.sg[k * 2] += g[0];
+            v.sg[k * 2 + 1] += g[1];
+            v.sl[k * 2] += acc[0];
+            v.sl[k * 2 + 1] += acc[1];
+        }
+        __syncthreads();
+    }
+}
+
+// Every backflow determinant's contribution to every particle (sg, sl).
+template <int NT>
+__device__ void bf_refresh_all(const DevSys& s, const Smem& v, bool evaluate) {
+    for (int i = threadIdx.x; i < s.np * 2; i += NT) v.sg[i] = v.sl[i] = 0.0;
+    __syncthreads();
+    for (int d = 0; d < s.nbf; ++d) bf_derivatives<NT>(s, v, d, evaluate);
+}
+
+// The drift's refresh of p: its determinant gradient from the committed F.
+template <int NT>
+__device__ void bf_refresh_particle(const DevSys& s, const Smem& v, int p) {
+    double tot[2] = {0.0, 0.0};
+    for (int d = 0; d < s.nbf; ++d) {
+        const DevBF& D = s.bf[d];
+        if (!bf_affects(D, p)) continue;
+        double g[2];
+        bf_grad_of<NT>(s, v, D, v.scal - s.o_scal + D.oF, p, -1, nullptr, g);
+        tot[0] += g[0];
+        tot[1] += g[1];
+    }
+    if (threadIdx.x == 0) {
+        v.sg[p * 2] = tot[0];
+        v.sg[p * 2 + 1] = tot[1];
+    }
+    __syncthreads();
+}
+
 // ───────────────────────── refresh ──────────────────────────────────────
 
 // Drift refresh of particle p: its determinant derivatives from A and the
@@ -514,12 +976,14 @@ __device__ void refresh_particle(const DevSys& s, const Smem& v, const double* g
         }
     }
     __syncthreads();
+    if (s.nbf > 0) bf_refresh_particle<NT>(s, v, p);
 }
 
 // Every particle's determinant and k-space derivatives (refresh_derivatives).
 template <int NT>
 __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) {
     const int np = s.np;
+    if (s.nbf > 0) bf_refresh_all<NT>(s, v, false);
     if (s.cplx) c_refresh_all<NT>(s, v);
     for (int b = 0; b < (s.cplx ? 0 : s.nblocks); ++b) {
         const DevBlock& B = s.blocks[b];
@@ -587,6 +1051,10 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
     double acc[19];
 #pragma unroll
     for (int i = 0; i < 19; ++i) acc[i] = 0.0;
+    // backflow determinants first: their proposal uses the work area that the
+    // pair loop below fills with partner scratch
+    for (int d = 0; d < s.nbf; ++d)
+        if (bf_affects(s.bf[d], p)) bf_propose<NT>(s, v, d, p);
     if (ks) {
         const double* r = v.pos + p * 2;
         const double th[4] = {s.recip[0] * v.newpos[0] + s.recip[1] * v.newpos[1],
@@ -736,6 +1204,20 @@ __device__ void ratio_step(const DevSys& s, const Smem& v, int p, bool have_old)
             sgy = invR * acc[3];
             slx = invR * acc[4] - sgx * sgx;
             sly = invR * acc[5] - sgy * sgy;
+        }
+        for (int d = 0; d < s.nbf; ++d) {   // BackflowSlaterDeterminant::ratio_batch
+            const DevBF& D = s.bf[d];
+            if (!bf_affects(D, p)) continue;
+            const double* pm = v.scal - s.o_scal + D.pM;
+            const double* ls = v.scal - s.o_scal + D.oLS;
+            if (pm[2] == 0.0) {
+                logdr += -700.0;   // a singular proposal is never accepted
+                continue;
+            }
+            logdr += pm[0] - ls[0];
+            if (pm[1] * ls[1] < 0.0) phase += kPi;
+            sgx += pm[3];
+            sgy += pm[4];
         }
         logr += logdr;
         v.misc[M_LOGDR] = logdr;
@@ -944,6 +1426,41 @@ __device__ void commit_step(const DevSys& s, const Smem& v, double* grec, int p)
             v.sl[p * 2 + 1] = acc[3] - acc[1] * acc[1];
         }
     }
+    // backflow determinants: the pending proposal becomes committed
+    if (s.nbf > 0) {
+        double* sm = v.scal - s.o_scal;
+        for (int d = 0; d < s.nbf; ++d) {
+            const DevBF& D = s.bf[d];
+            if (!bf_affects(D, p)) continue;
+            const int N = D.n;
+            for (int i = threadIdx.x; i < 2 * N; i += NT) {
+                sm[D.oX + i] = sm[D.pX + i];
+                sm[D.oF + i] = sm[D.pF + i];
+            }
+            for (int i = threadIdx.x; i < N * N; i += NT) sm[D.oA + i] = sm[D.pA + i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double g0 = 0.0, g1 = 0.0;
+            for (int d = 0; d < s.nbf; ++d) {
+                const DevBF& D = s.bf[d];
+                if (!bf_affects(D, p)) continue;
+                const double* pm = sm + D.pM;
+                double* ls = sm + D.oLS;
+                if (pm[2] == 0.0) v.scal[S_ERR] = 1.0;
+                v.scal[S_LOGPSI] += pm[0] - ls[0];
+                ls[0] = pm[0];
+                ls[1] = pm[1];
+                g0 += pm[3];
+                g1 += pm[4];
+            }
+            v.sg[p * 2] = g0;          // exact at the committed state
+            v.sg[p * 2 + 1] = g1;
+            v.sl[p * 2] = 0.0;         // proposal Laplacian skipped (refreshed before E_L)
+            v.sl[p * 2 + 1] = 0.0;
+        }
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
         v.jg[p * 2 + 0] = v.misc[M_JGX];
         v.jg[p * 2 + 1] = v.misc[M_JGY];
@@ -1105,6 +1622,13 @@ __device__ void evaluate_walker(const DevSys& s, const Smem& v, double* grec, co
             if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
             lp[0] += v.misc[M_LOGDET];
         }
+        __syncthreads();
+    }
+    // backflow determinants: x, M, A = M⁻¹, F and every derivative
+    if (s.nbf > 0) {
+        bf_refresh_all<NT>(s, v, true);
+        if (threadIdx.x == 0)
+            for (int d = 0; d < s.nbf; ++d) lp[0] += v.scal[s.bf[d].oLS - s.o_scal];
         __syncthreads();
     }
     // determinants: rows, A = D⁻¹ by Gauss-Jordan, log|det|, condition

@@ -155,6 +155,34 @@ typedef struct {
     double tail;                  /* constant added to every configuration */
 } alea_gpu_inverse_power;
 
+/* One backflow channel: the particles [source_first, source_last) displace
+ * every row of the determinant by η(r) r, η = (1 - r/L)^C Σ_k c_k r^k for
+ * r < L (src/wavefunction/backflow_function.h:11-37; coeffs are c_0..c_N with
+ * a like-spin channel's c_1 = C c_0 / L already filled in). */
+typedef struct {
+    int source_first, source_last;
+    int C;
+    double L;
+    int n_coeffs;
+    double coeffs[16];
+} alea_gpu_backflow_channel;
+
+/* A backflow Slater determinant over the rows [first, last) of one spin group
+ * (src/wavefunction/backflow_slater_determinant.h:15-80): orbitals (plane
+ * waves or Gaussians, as alea_gpu_orbitals) at the quasi-coordinates
+ * x_i = r_i + Σ_c Σ_j η_c(r_ij) r_ij.  A system with backflow determinants
+ * has no plain determinant blocks. */
+typedef struct {
+    int first, last;
+    int type;                 /* ALEA_ORB_PLANE_WAVE or ALEA_ORB_GAUSSIAN */
+    const double* k;
+    const int* is_sin;
+    const double* centers;
+    const double* alphas;
+    int n_channels;
+    alea_gpu_backflow_channel channels[4];
+} alea_gpu_backflow;
+
 typedef struct {
     int dim;                      /* 2 (3 for open cells) */
     int n_particles;
@@ -172,6 +200,8 @@ typedef struct {
     alea_gpu_coulomb coulomb[ALEA_GPU_MAX_COULOMB];
     int n_inverse_power;
     alea_gpu_inverse_power inverse_power[ALEA_GPU_MAX_COULOMB];
+    int n_backflow;
+    alea_gpu_backflow backflow[2];
 } alea_gpu_system;
 
 typedef struct alea_gpu_ctx alea_gpu_ctx;

@@ -13,7 +13,7 @@ from oracle.oracle import S_EL, S_LOGPSI
 
 pytestmark = pytest.mark.gpu
 
-SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t"]
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t", "heg10bf"]
 
 
 def walkers(setup, capacity):
@@ -80,14 +80,15 @@ def test_single_moves_match_oracle(name):
 
 @pytest.mark.parametrize("name,drift", [("exciton", False), ("heg10", False), ("heg10", True),
                                         ("crystal16", False), ("heg42", False), ("dipoles16", False),
-                                        ("dipoles16", True), ("heg10t", False), ("heg10t", True)])
+                                        ("dipoles16", True), ("heg10t", False), ("heg10t", True),
+                                        ("heg10bf", False), ("heg10bf", True)])
 def test_vmc_steps_match_oracle(name, drift):
     import alea_b200
     setup = golden(f"setup_{name}.json")
     pos = np.array(golden(f"eval_{name}.json")["positions"])
     nw = pos.shape[0]
     tau = {"exciton": 0.05, "heg10": 225.0, "crystal16": 400.0, "heg42": 225.0,
-           "dipoles16": 0.0003, "heg10t": 225.0}[name]
+           "dipoles16": 0.0003, "heg10t": 225.0, "heg10bf": 225.0}[name]
     n_steps, n_sub, seed = 4, 2, 21
     o = Oracle(setup)
     o.init(pos)
@@ -108,7 +109,7 @@ def test_vmc_steps_match_oracle(name, drift):
         assert np.array_equal(fin, o.pos()[:nw])
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t", "heg10bf"])
 def test_dmc_run_matches_oracle(name):
     setup = golden(f"setup_{name}.json")
     r = golden(f"dmc_{name}.json")
