@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import glob
 import os
+import re
 import subprocess
 import sys
 
@@ -38,11 +39,49 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in deps())
 
 
+def includes(path, seen=None):
+    """The file and every quoted #include it reaches, recursively."""
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    for line in open(path, encoding="utf-8"):
+        m = re.match(r'\s*#\s*include\s+"([^"]+)"', line)
+        if m:
+            includes(os.path.join(os.path.dirname(path), m.group(1)), seen)
+    return seen
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile the sources whose object is older than the source or any header
+    it includes, in parallel (the kernel files take minutes each), then link
+    the shared library."""
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB] + sources()
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    objs, jobs = [], []
+    for src in sources():
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        stale = force or not os.path.exists(obj) or any(
+            os.path.getmtime(d) > os.path.getmtime(obj) for d in includes(src))
+        if not stale:
+            continue
+        cmd = [nvcc] + compile_flags + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        jobs.append((obj, subprocess.Popen(cmd)))
+    failed = [obj for obj, proc in jobs if proc.wait() != 0]
+    if failed:
+        for obj in failed:
+            if os.path.exists(obj):
+                os.remove(obj)
+        raise subprocess.CalledProcessError(1, "nvcc -c " + " ".join(failed))
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -816,6 +816,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     for (int d = 0; d < s.nbf; ++d) work = std::max(work, 4L * s.bf[d].n * s.bf[d].n + 8L * s.bf[d].n);
     work = std::max(work, 2L * s.enk);
     work = std::max(work, static_cast<long>(np) * 10);
+    work = std::max(work, 3L * s.ngroups * s.nkJ);   // one-warp k-space refresh: E_g(k), S_g(k)
     s.s_work = take(work);
     s.s_rad = s.s_work;
     s.s_total = static_cast<int>(m);

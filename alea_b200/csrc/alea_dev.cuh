@@ -286,29 +286,39 @@ __device__ __forceinline__ void bessel_k01e(const double* cheb, double x, double
     k1e = (xi * b1 - b1p + __ldg(cheb + 24)) * isx;
 }
 
+// u, u', u'' of the zero-energy Jastrow at r (kind 2 below), out of line:
+// its Bessel series are long and rarely on the path of a move.
+static __device__ __noinline__ void radial_zero_energy(double r, double ze_s, double ze_kappa, double ze_rm,
+                                                double ze_rc, double ze_c3, double ze_logc1,
+                                                double ze_logc2, const double* ze_cheb, double& u,
+                                                double& du, double& d2u) {
+    if (r < ze_rm) {   // ln[C1 K0(κ r^-s)]
+        const double x = ze_kappa * pow(r, -ze_s);
+        double k0e, k1e;
+        bessel_k01e(ze_cheb, x, k0e, k1e);
+        const double q = k1e / k0e;
+        const double sx = ze_s * x;
+        u = log(k0e) - x + ze_logc1;
+        du = sx * q / r;
+        d2u = sx / (r * r) * (sx * (1.0 - q) * (1.0 + q) - q);
+        return;
+    }
+    const double rr = fmin(r, ze_rc);
+    const double inv_r = 1.0 / rr;
+    const double inv_c = 1.0 / (2.0 * ze_rc - rr);
+    const double m = (r < ze_rc) ? 1.0 : 0.0;
+    const double a = ze_c3;
+    u = m * (ze_logc2 - a * inv_r - a * inv_c);
+    du = m * (a * inv_r * inv_r - a * inv_c * inv_c);
+    d2u = m * (-2.0 * a * inv_r * inv_r * inv_r - 2.0 * a * inv_c * inv_c * inv_c);
+}
+
 // u, u', u'' of a pair term at r (the short-range half for an image sum).
 __device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, double& du,
                                        double& d2u) {
     if (T.kind == 2) {
-        if (r < T.ze_rm) {   // ln[C1 K0(κ r^-s)]
-            const double x = T.ze_kappa * pow(r, -T.ze_s);
-            double k0e, k1e;
-            bessel_k01e(T.ze_cheb, x, k0e, k1e);
-            const double q = k1e / k0e;
-            const double sx = T.ze_s * x;
-            u = log(k0e) - x + T.ze_logc1;
-            du = sx * q / r;
-            d2u = sx / (r * r) * (sx * (1.0 - q) * (1.0 + q) - q);
-            return;
-        }
-        const double rr = fmin(r, T.ze_rc);
-        const double inv_r = 1.0 / rr;
-        const double inv_c = 1.0 / (2.0 * T.ze_rc - rr);
-        const double m = (r < T.ze_rc) ? 1.0 : 0.0;
-        const double a = T.ze_c3;
-        u = m * (T.ze_logc2 - a * inv_r - a * inv_c);
-        du = m * (a * inv_r * inv_r - a * inv_c * inv_c);
-        d2u = m * (-2.0 * a * inv_r * inv_r * inv_r - 2.0 * a * inv_c * inv_c * inv_c);
+        radial_zero_energy(r, T.ze_s, T.ze_kappa, T.ze_rm, T.ze_rc, T.ze_c3, T.ze_logc1, T.ze_logc2,
+                           T.ze_cheb, u, du, d2u);
         return;
     }
     if (T.kind == 0) {

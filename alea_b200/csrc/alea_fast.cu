@@ -1,0 +1,748 @@
+// The one-warp VMC/DMC sweep (sm_100a) for systems of real determinants and
+// pair Jastrows of at most 64 particles: one CTA of 32 threads per walker,
+// the walker's hot state in shared memory as in the generic sweep, and every
+// per-item intermediate of a move in registers.
+//
+// Algorithms restated from the reference (ItaloAlb/alea), in the same steps
+// as the generic sweep of alea_kernels.cu:
+//   sweep          src/qmc/vmc.cpp:82-155, src/qmc/dmc.cpp:203-337,
+//                  src/numerics/green_function.h:20-58
+//   Slater         src/wavefunction/slater_determinant.cpp:395-437 (ratio),
+//                  :515-726 (Sherman-Morrison commit, rebuild triggers),
+//                  :862-903 (derivative refresh), :905-993 (Gauss-Jordan)
+//   pair Jastrows  src/wavefunction/pade_jastrow.cpp:347-634,
+//                  src/wavefunction/radial_pair_jastrow_impl.h
+//   image sums     src/wavefunction/kspace_pair_sum.cpp:157-301
+//   E_L, weights   src/hamiltonian/kinetic.cpp:45-72, ewald_term.cpp:368-612,
+//                  src/qmc/population_control.cpp:56-77
+//
+// Work split.  Lane l owns slot j = 0..S-1 of every list: partner l + 32j
+// (its displacement, radial terms and its own Jastrow-derivative change,
+// applied by the same lane if the move is accepted), orbital row l + 32j
+// (new orbital value and derivatives, its factor of the rank-one update, its
+// rows of D, ∇D, ∇²D written back), k-vector l + 32j (old and new phase, the
+// change of ρ(k)).  The per-move sums (ratio, ∇ and ∂² of the moved particle,
+// log J) meet in one 16-value warp reduce-scatter; every lane ends with the
+// same totals and takes the accept decision itself, so a move has no block
+// barrier.  The orbital rows of the next particle are fetched from HBM while
+// the current move runs, and a sweep's random numbers are read once per lane.
+#include "alea_walker.cuh"
+
+namespace alea_gpu {
+
+namespace {
+
+// k-space contribution of one k to the gradient/Laplacian of a particle with
+// phase (c, sn) that sees the density (pr, pi) (kspace_pair_sum.cpp:76-97).
+__device__ __forceinline__ void kterm_r(double kx, double ky, double w, double c, double sn, double pr,
+                                        double pi, double self, double* acc) {
+    const double g = 2.0 * w * (c * pi - sn * pr);
+    const double l = 2.0 * w * (self - (c * pr + sn * pi));
+    acc[0] += kx * g;
+    acc[1] += ky * g;
+    acc[2] += kx * kx * l;
+    acc[3] += ky * ky * l;
+}
+
+// Orbital rows ∇D, ∇²D of particle p (its block's row), lane slot j = column
+// l + 32j; nothing for a particle outside every determinant.
+template <int S>
+__device__ __forceinline__ void fetch_rows(const DevSys& s, const double* grec, int p, double2 (&dg)[S],
+                                           double2 (&dl)[S]) {
+    const int b = block_of(s, p);
+    if (b < 0) return;
+    const DevBlock& B = s.blocks[b];
+    const int N = B.n, kr = p - B.first;
+    const double2* rg = reinterpret_cast<const double2*>(grec + B.oDg) + kr * N;
+    const double2* rl = reinterpret_cast<const double2*>(grec + B.oDl) + kr * N;
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const int m = static_cast<int>(threadIdx.x) + 32 * j;
+        if (m < N) {
+            dg[j] = rg[m];
+            dl[j] = rl[m];
+        }
+    }
+}
+
+// ── 2-D geometry, in the operation order of min_image / wrap_pos ──
+
+__device__ __forceinline__ void min_image2(const DevSys& s, double& x0, double& x1) {
+    if (!s.periodic) return;
+    if (s.ortho) {
+        x0 = fma(-s.box[0], rint(x0 * s.inv_box[0]), x0);
+        x1 = fma(-s.box[1], rint(x1 * s.inv_box[1]), x1);
+        return;
+    }
+    const double f0 = rint(fma(s.ainv[1], x1, s.ainv[0] * x0));
+    const double f1 = rint(fma(s.ainv[3], x1, s.ainv[2] * x0));
+    x0 -= fma(f1, s.a[2], f0 * s.a[0]);
+    x1 -= fma(f1, s.a[3], f0 * s.a[1]);
+    double b0 = x0, b1 = x1, best2 = fma(x1, x1, x0 * x0);
+#pragma unroll
+    for (int c = 1; c < 9; ++c) {
+        const double y0 = x0 + s.cand[c * 2 + 0];
+        const double y1 = x1 + s.cand[c * 2 + 1];
+        const double r2 = fma(y1, y1, y0 * y0);
+        const double take = (r2 < best2) ? 1.0 : 0.0;
+        best2 = fma(take, r2 - best2, best2);
+        b0 = fma(take, y0 - b0, b0);
+        b1 = fma(take, y1 - b1, b1);
+    }
+    x0 = b0;
+    x1 = b1;
+}
+
+// Folded displacement a - b and its length.
+__device__ __forceinline__ double fold2(const DevSys& s, double ax, double ay, double bx, double by,
+                                        double& dx, double& dy) {
+    dx = ax - bx;
+    dy = ay - by;
+    min_image2(s, dx, dy);
+    return sqrt(fma(dy, dy, dx * dx));
+}
+
+__device__ __forceinline__ void wrap2(const DevSys& s, double& x, double& y) {
+    if (!s.periodic) return;
+    if (s.ortho) {
+        x = fma(-s.box[0], rint(x * s.inv_box[0]), x);
+        y = fma(-s.box[1], rint(y * s.inv_box[1]), y);
+        return;
+    }
+    const double f0 = rint(fma(s.ainv[1], y, s.ainv[0] * x));
+    const double f1 = rint(fma(s.ainv[3], y, s.ainv[2] * x));
+    x -= fma(f1, s.a[2], f0 * s.a[0]);
+    y -= fma(f1, s.a[3], f0 * s.a[1]);
+}
+
+// Orbital i of a real block at (x, y): value, gradient, diagonal second
+// derivatives (plane waves, orbital_set.h:436-474; Gaussians, :185-224).
+__device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int i, double x, double y,
+                                         double& val, double& gx, double& gy, double& lx, double& ly) {
+    if (B.type == 0) {
+        const double k0 = B.k[i * 2], k1 = B.k[i * 2 + 1];
+        double sn, c;
+        sincos(fma(k1, y, k0 * x), &sn, &c);
+        if (B.is_sin[i] != 0.0) {
+            val = sn;
+            gx = k0 * c;
+            gy = k1 * c;
+            lx = -k0 * k0 * sn;
+            ly = -k1 * k1 * sn;
+        } else {
+            val = c;
+            gx = -k0 * sn;
+            gy = -k1 * sn;
+            lx = -k0 * k0 * c;
+            ly = -k1 * k1 * c;
+        }
+    } else {
+        const double alpha = B.alphas[i];
+        double dx = x - B.centers[i * 2], dy = y - B.centers[i * 2 + 1];
+        min_image2(s, dx, dy);
+        const double phi = exp(-alpha * fma(dy, dy, dx * dx));
+        val = phi;
+        gx = phi * (-2.0 * alpha * dx);
+        gy = phi * (-2.0 * alpha * dy);
+        lx = phi * (4.0 * alpha * alpha * dx * dx - 2.0 * alpha);
+        ly = phi * (4.0 * alpha * alpha * dy * dy - 2.0 * alpha);
+    }
+}
+
+// A = D⁻¹ of an N x N block by pivoted Gauss-Jordan on one warp (first
+// maximum |pivot| of each column, as rebuild_inverse): lane l owns columns
+// l + 32j of the work copy m of D and of A.  Leaves log|det D| in
+// misc[M_LOGDET] and flags a zero or nonfinite pivot in misc[M_ERR].  Out of
+// line: it runs once per 64 accepted moves of a block.
+template <int S>
+__device__ __noinline__ void gj_rebuild_warp(double* A, double* m, double* col, const double* D, int N,
+                                             double* misc) {
+    const int lane = threadIdx.x;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const int c = lane + 32 * j;
+        if (c >= N) continue;
+        for (int r = 0; r < N; ++r) {
+            m[r * N + c] = D[r * N + c];
+            A[r * N + c] = (r == c) ? 1.0 : 0.0;
+        }
+    }
+    __syncwarp();
+    double logdet = 0.0;
+    bool bad = false;
+    for (int k = 0; k < N; ++k) {
+        // the pivot travels with its |value| and row through the butterfly,
+        // so no lane reads column k again after its owner starts the swap
+        double best = -1.0, bval = 0.0;
+        int bi = N;
+        for (int r = k + lane; r < N; r += 32) {
+            const double x = m[r * N + k];
+            if (fabs(x) > best) {
+                best = fabs(x);
+                bval = x;
+                bi = r;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(kAllLanes, best, o);
+            const double ov = __shfl_xor_sync(kAllLanes, bval, o);
+            const int oi = __shfl_xor_sync(kAllLanes, bi, o);
+            if (ob > best || (ob == best && oi < bi)) {
+                best = ob;
+                bval = ov;
+                bi = oi;
+            }
+        }
+        const int piv = bi < N ? bi : k;   // a column of NaNs has no pivot: flagged below
+        const double diag = bval;
+        if (lane == (k & 31)) {
+            logdet += log(fabs(diag));
+            bad |= diag == 0.0 || !isfinite(diag);
+        }
+        double pk[S], ak[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            const int c = lane + 32 * j;
+            pk[j] = ak[j] = 0.0;
+            if (c >= N) continue;
+            const double mk = m[k * N + c], mp = m[piv * N + c];
+            const double xk = A[k * N + c], xp = A[piv * N + c];
+            if (piv != k) {
+                m[piv * N + c] = mk;
+                A[piv * N + c] = xk;
+            }
+            pk[j] = (piv != k ? mp : mk) / diag;
+            ak[j] = (piv != k ? xp : xk) / diag;
+            m[k * N + c] = pk[j];
+            A[k * N + c] = ak[j];
+        }
+        __syncwarp();
+        for (int r = lane; r < N; r += 32) col[r] = m[r * N + k];
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            const int c = lane + 32 * j;
+            if (c >= N) continue;
+            for (int r0 = 0; r0 < N; r0 += 4) {
+                double f[4], x[4], y[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = r0 + u;
+                    const bool on = r < N && r != k;
+                    f[u] = on ? col[r] : 0.0;
+                    x[u] = on ? m[r * N + c] : 0.0;
+                    y[u] = on ? A[r * N + c] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = r0 + u;
+                    if (r < N && r != k) {
+                        m[r * N + c] = x[u] - f[u] * pk[j];
+                        A[r * N + c] = y[u] - f[u] * ak[j];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    logdet = warp_sum(logdet);
+    const bool any_bad = __any_sync(kAllLanes, bad);
+    if (lane == 0) {
+        misc[M_LOGDET] = logdet;
+        if (any_bad) misc[M_ERR] = 1.0;
+    }
+    __syncwarp();
+}
+
+// The local energy after a sweep: every particle's derivatives refreshed,
+// then kinetic + Ewald + open pair potentials.  Out of line: once per sweep.
+template <int S>
+__device__ __noinline__ double local_energy_warp(const DevSys& s, double* sm, const double* grec,
+                                                 const int2* pairs, int npair) {
+    const Smem v = view(s, sm);
+    refresh_all<32, S>(s, v, grec);
+    return local_energy<32, S>(s, v, pairs, npair);
+}
+
+// Select slot p >> 5 of a per-lane register array and read it from lane
+// p & 31 (warp-uniform result).
+template <int S, class T>
+__device__ __forceinline__ T from_owner(const T (&x)[S], int p) {
+    T mine = x[0];
+#pragma unroll
+    for (int j = 1; j < S; ++j)
+        if ((p >> 5) == j) mine = x[j];
+    return __shfl_sync(kAllLanes, mine, p & 31);
+}
+
+}  // namespace
+
+template <int S>
+__global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
+                                                        int nw, const double* randoms, long stride,
+                                                        SweepParams prm, const int2* pairs, int npair) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    const int lane = threadIdx.x;
+    double* rec = records + static_cast<long>(w) * s.rec;
+    load_hot<32>(s, rec, sm);
+    const Smem v = view(s, sm);
+    const int np = s.np, nk = s.nkJ;
+    const bool dmc = prm.mode == 1;
+    const bool drift = dmc || prm.drift != 0;
+    // partner slots: group, and the terms coupling the partner to each group
+    int kgrp[S];
+    unsigned long long cmask[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const int k = lane + 32 * j;
+        kgrp[j] = k < np ? s.group_of[k] : 0;
+        unsigned long long msk = 0;
+        if (k < np)
+            for (int g = 0; g < s.ngroups; ++g)
+                msk |= static_cast<unsigned long long>(s.gterms[g][kgrp[j]]) << (8 * g);
+        cmask[j] = msk;
+    }
+    // image-summed terms each group takes part in (bit t of byte g)
+    unsigned long long gimask = 0;
+    for (int g = 0; g < s.ngroups; ++g)
+        for (int t = 0; t < s.nterms; ++t)
+            if (s.terms[t].image && in_term(s.terms[t], s.gfirst[g]))
+                gimask |= 1ull << (8 * g + t);
+    if (lane == 0) {
+        v.scal[S_NACC] = 0.0;
+        v.scal[S_NCUT] = 0.0;
+        if (dmc) {
+            v.scal[S_RRP] = 0.0;
+            v.scal[S_RRA] = 0.0;
+            v.scal[S_WEIGHT] = 1.0;
+            v.scal[S_EPREV] = v.scal[S_EL];
+        }
+        v.misc[M_ERR] = 0.0;
+    }
+    __syncwarp();
+    for (int sub = 0; sub < prm.n_sub; ++sub) {
+        const double* rnd = randoms + static_cast<long>(sub) * np * 3 * stride;
+        double rz0[S], rz1[S], rzu[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            const int k = lane + 32 * j;
+            const double* g = rnd + static_cast<long>(k) * 3 * stride + w;
+            rz0[j] = k < np ? g[0] : 0.0;
+            rz1[j] = k < np ? g[stride] : 0.0;
+            rzu[j] = k < np ? g[2 * stride] : 0.0;
+        }
+        double2 dg[S], dl[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) dg[j] = dl[j] = make_double2(0.0, 0.0);
+        if (drift) fetch_rows<S>(s, rec, 0, dg, dl);
+        for (int p = 0; p < np; ++p) {
+            const int gp = from_owner<S>(kgrp, p);
+            const int b = block_of(s, p);
+            const unsigned imask = nk > 0 ? static_cast<unsigned>((gimask >> (8 * gp)) & 0xffu) : 0u;
+            const bool ks = imask != 0;
+            const double px = v.pos[p * 2], py = v.pos[p * 2 + 1];
+            // ── drift refresh of p: determinant and k-space derivatives ──
+            if (drift) {
+                double ra[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                if (b >= 0) {
+                    const DevBlock& B = s.blocks[b];
+                    const int N = B.n, kr = p - B.first;
+                    const double* A = v.scal - s.o_scal + B.oA;
+#pragma unroll
+                    for (int j = 0; j < S; ++j) {
+                        const int m = lane + 32 * j;
+                        if (m >= N) continue;
+                        const double a = A[m * N + kr];
+                        ra[0] += a * dg[j].x;
+                        ra[1] += a * dg[j].y;
+                        ra[2] += a * dl[j].x;
+                        ra[3] += a * dl[j].y;
+                    }
+                }
+                if (p + 1 < np) fetch_rows<S>(s, rec, p + 1, dg, dl);
+                if (ks) {
+#pragma unroll 1
+                    for (int q = lane; q < nk; q += 32) {
+                        const double kxq = s.kxJ[q], kyq = s.kyJ[q];
+                        double co, so;
+                        sincos(fma(kyq, py, kxq * px), &so, &co);
+                        v.co[q] = co;
+                        v.so[q] = so;
+                        for (unsigned bits = imask; bits; bits &= bits - 1) {
+                            const DevTerm& T = s.terms[__ffs(bits) - 1];
+                            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+                            const int go = T.same0 ? gp : (gp == ga ? gb : ga);
+                            const double* pr = v.rho + go * 2 * nk;
+                            kterm_r(kxq, kyq, T.kw[q], co, so, pr[q], pr[nk + q], T.same0 ? 1.0 : 0.0, ra + 4);
+                        }
+                    }
+                }
+                warp_allsum<8>(ra);
+                if (lane == 0) {
+                    if (b >= 0) {
+                        v.sg[p * 2 + 0] = ra[0];
+                        v.sg[p * 2 + 1] = ra[1];
+                        v.sl[p * 2 + 0] = ra[2] - ra[0] * ra[0];
+                        v.sl[p * 2 + 1] = ra[3] - ra[1] * ra[1];
+                    }
+                    if (ks) {
+                        v.kg[p * 2 + 0] = ra[4];
+                        v.kg[p * 2 + 1] = ra[5];
+                        v.kl[p * 2 + 0] = ra[6];
+                        v.kl[p * 2 + 1] = ra[7];
+                    }
+                }
+                __syncwarp();
+            }
+            // ── proposal (every lane, identical arithmetic) ──
+            const double r0 = from_owner<S>(rz0, p), r1 = from_owner<S>(rz1, p), u = from_owner<S>(rzu, p);
+            const double tm = prm.tau * s.inv_mass[p * 2];
+            const double gx = v.sg[p * 2] + v.jg[p * 2] + v.kg[p * 2];
+            const double gy = v.sg[p * 2 + 1] + v.jg[p * 2 + 1] + v.kg[p * 2 + 1];
+            double sc = tm;
+            if (dmc) {
+                const double vsq = gx * gx + gy * gy;
+                sc = vsq < 1e-10 ? tm : (-1.0 + sqrt(1.0 + 2.0 * tm * vsq)) / vsq;
+            }
+            const double sig0 = prm.sigma[p * 2], sig1 = prm.sigma[p * 2 + 1];
+            double nx, ny;
+            if (drift) {
+                const double t0 = dmc ? sc : prm.tau * s.inv_mass[p * 2];
+                const double t1 = dmc ? sc : prm.tau * s.inv_mass[p * 2 + 1];
+                nx = fma(sig0, r0, fma(t0, gx, px));
+                ny = fma(sig1, r1, fma(t1, gy, py));
+            } else {
+                nx = fma(sig0, r0, px);
+                ny = fma(sig1, r1, py);
+            }
+            // ── ratio ──
+            // acc: 0 R, 1 Σ|A φ|, 2-3 Σ A ∇φ, 4-5 Σ A ∂²φ, 6 log J, 7-8 pair ∇,
+            // 9-10 pair ∂², 11-12 k-space ∇, 13-14 k-space ∂², 15 Σ|φ(r')|
+            double acc[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+            if (b >= 0) {
+                const DevBlock& B = s.blocks[b];
+                const int N = B.n, jrow = p - B.first;
+                const double* A = v.scal - s.o_scal + B.oA;
+#pragma unroll 1
+                for (int m = lane; m < N; m += 32) {
+                    double val, ogx, ogy, olx, oly;
+                    orbital2(s, B, m, nx, ny, val, ogx, ogy, olx, oly);
+                    v.nval[m] = val;
+                    v.ngrad[m * 2 + 0] = ogx;
+                    v.ngrad[m * 2 + 1] = ogy;
+                    v.nlap[m * 2 + 0] = olx;
+                    v.nlap[m * 2 + 1] = oly;
+                    const double a = A[m * N + jrow];
+                    const double term = a * val;
+                    acc[0] += term;
+                    acc[1] += fabs(term);
+                    acc[2] += a * ogx;
+                    acc[3] += a * ogy;
+                    acc[4] += a * olx;
+                    acc[5] += a * oly;
+                    acc[15] += fabs(val);
+                }
+            }
+            // pair terms: p's new derivatives, the log ratio, and each
+            // partner's derivative change (kept in `work`, applied on accept)
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                const int k = lane + 32 * j;
+                const unsigned cm =
+                    (k < np && k != p) ? static_cast<unsigned>((cmask[j] >> (8 * gp)) & 0xffu) : 0u;
+                if (!cm) continue;
+                const double kx0 = v.pos[k * 2], ky0 = v.pos[k * 2 + 1];
+                double dnx, dny, dox, doy;
+                const double rn = fold2(s, nx, ny, kx0, ky0, dnx, dny);
+                const double ro = fold2(s, px, py, kx0, ky0, dox, doy);
+                double du_o = 0.0, d2u_o = 0.0, du_n = 0.0, d2u_n = 0.0;
+                for (unsigned bits = cm; bits; bits &= bits - 1) {
+                    const DevTerm& T = s.terms[__ffs(bits) - 1];
+                    double uo, duo, d2uo, un, dun, d2un;
+                    radial(T, ro, uo, duo, d2uo);
+                    radial(T, rn, un, dun, d2un);
+                    acc[6] += un - uo;
+                    du_o += duo;
+                    d2u_o += d2uo;
+                    du_n += dun;
+                    d2u_n += d2un;
+                }
+                const double irn = 1.0 / rn, iro = 1.0 / ro;
+                double* dj = v.work + k * 4;
+                {
+                    const double dor = dnx * irn;
+                    acc[7] += du_n * dor;
+                    acc[9] += d2u_n * dor * dor + du_n * irn * (1.0 - dor * dor);
+                    const double dor_old = -dox * iro, dor_new = -dnx * irn;
+                    dj[0] = du_n * dor_new - du_o * dor_old;
+                    dj[2] = (d2u_n * dor_new * dor_new + du_n * irn * (1.0 - dor_new * dor_new)) -
+                            (d2u_o * dor_old * dor_old + du_o * iro * (1.0 - dor_old * dor_old));
+                }
+                {
+                    const double dor = dny * irn;
+                    acc[8] += du_n * dor;
+                    acc[10] += d2u_n * dor * dor + du_n * irn * (1.0 - dor * dor);
+                    const double dor_old = -doy * iro, dor_new = -dny * irn;
+                    dj[1] = du_n * dor_new - du_o * dor_old;
+                    dj[3] = (d2u_n * dor_new * dor_new + du_n * irn * (1.0 - dor_new * dor_new)) -
+                            (d2u_o * dor_old * dor_old + du_o * iro * (1.0 - dor_old * dor_old));
+                }
+            }
+            // image sums: new phases of p, ratio and derivative terms; the
+            // change of p's phases is kept in cn/sn for the ρ(k) update
+            if (ks) {
+#pragma unroll 1
+                for (int q = lane; q < nk; q += 32) {
+                    const double kxq = s.kxJ[q], kyq = s.kyJ[q];
+                    double cn, sn, co, so;
+                    sincos(fma(kyq, ny, kxq * nx), &sn, &cn);
+                    if (drift) {
+                        co = v.co[q];
+                        so = v.so[q];
+                    } else {
+                        sincos(fma(kyq, py, kxq * px), &so, &co);
+                    }
+                    const double* mr = v.rho + gp * 2 * nk;
+                    for (unsigned bits = imask; bits; bits &= bits - 1) {
+                        const DevTerm& T = s.terms[__ffs(bits) - 1];
+                        const double wk = T.kw[q];
+                        if (T.same0) {
+                            const double qr = mr[q] + cn - co;
+                            const double qi = mr[nk + q] + sn - so;
+                            acc[6] += wk * (qr * qr + qi * qi - mr[q] * mr[q] - mr[nk + q] * mr[nk + q]);
+                            kterm_r(kxq, kyq, wk, cn, sn, qr, qi, 1.0, acc + 11);
+                        } else {
+                            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+                            const int go = gp == ga ? gb : ga;
+                            const double* orr = v.rho + go * 2 * nk;
+                            acc[6] += 2.0 * wk * ((cn - co) * orr[q] + (sn - so) * orr[nk + q]);
+                            kterm_r(kxq, kyq, wk, cn, sn, orr[q], orr[nk + q], 0.0, acc + 11);
+                        }
+                    }
+                    v.cn[q] = cn - co;
+                    v.sn[q] = sn - so;
+                }
+            }
+            warp_allsum<16>(acc);
+            double logr = acc[6], phase = 0.0, logdr = 0.0, sgx = 0.0, sgy = 0.0;
+            if (b >= 0) {
+                const double R = acc[0];
+                logdr = log(fmax(fabs(R), 1e-300));
+                if (R < 0.0) phase = kPi;
+                const double invR = (R != 0.0) ? 1.0 / R : 0.0;
+                sgx = invR * acc[2];
+                sgy = invR * acc[3];
+            }
+            logr += logdr;
+            // ── accept / reject (every lane, identical decision) ──
+            const double ngx_t = sgx + acc[7] + acc[11], ngy_t = sgy + acc[8] + acc[12];
+            const double dx = nx - px, dy = ny - py;
+            const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
+            bool accept;
+            if (dmc) {
+                accept = false;
+                if (phase == 0.0) {
+                    const double vsq = ngx_t * ngx_t + ngy_t * ngy_t;
+                    const double sb = vsq < 1e-10 ? tm0 : (-1.0 + sqrt(1.0 + 2.0 * tm0 * vsq)) / vsq;
+                    double lc = 0.0;
+                    if (tm0 > 0.0) {
+                        const double df = sc * gx, db = sb * ngx_t;
+                        lc += (-dx * (df + db) + 0.5 * (df * df - db * db)) / tm0;
+                    }
+                    if (tm1 > 0.0) {
+                        const double df = sc * gy, db = sb * ngy_t;
+                        lc += (-dy * (df + db) + 0.5 * (df * df - db * db)) / tm1;
+                    }
+                    const double la = 2.0 * logr + lc;
+                    accept = la >= 0.0 || u < exp(la);
+                }
+                if (lane == 0) {
+                    const double rr = tm0 * dx * dx + tm1 * dy * dy;
+                    v.scal[S_RRP] += rr;
+                    if (accept) v.scal[S_RRA] += rr;
+                }
+            } else if (prm.drift) {
+                double lc = -dx * (gx + ngx_t) + 0.5 * tm0 * (gx * gx - ngx_t * ngx_t);
+                lc += -dy * (gy + ngy_t) + 0.5 * tm1 * (gy * gy - ngy_t * ngy_t);
+                const double la = 2.0 * logr + lc;
+                accept = la >= 0.0 || u < exp(la);
+            } else {
+                accept = u < exp(2.0 * logr);
+            }
+            if (!accept) continue;
+            // ── commit ──
+            if (lane == 0) v.scal[S_NACC] += 1.0;
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                const int k = lane + 32 * j;
+                if (k >= np || k == p || ((cmask[j] >> (8 * gp)) & 0xffu) == 0) continue;
+                const double* dj = v.work + k * 4;
+                v.jg[k * 2 + 0] += dj[0];
+                v.jg[k * 2 + 1] += dj[1];
+                v.jl[k * 2 + 0] += dj[2];
+                v.jl[k * 2 + 1] += dj[3];
+            }
+            if (ks) {
+                double* mr = v.rho + gp * 2 * nk;
+                for (int q = lane; q < nk; q += 32) {
+                    mr[q] += v.cn[q];
+                    mr[nk + q] += v.sn[q];
+                }
+            }
+            if (b >= 0) {
+                const DevBlock& B = s.blocks[b];
+                const int N = B.n, jrow = p - B.first;
+                double* A = v.scal - s.o_scal + B.oA;
+                double* bs = v.scal + S_BLOCK0 + 3 * b;
+                double* D = rec + B.oD;
+                double2* Dg = reinterpret_cast<double2*>(rec + B.oDg) + jrow * N;
+                double2* Dl = reinterpret_cast<double2*>(rec + B.oDl) + jrow * N;
+                double* rabs = v.scal - s.o_scal + B.orabs;
+                const double R = acc[0];
+                __syncwarp();   // the new orbital row v.nval
+#pragma unroll 1
+                for (int c = lane; c < N; c += 32) {
+                    double prod = 0.0;
+                    for (int m = 0; m < N; ++m) prod += v.nval[m] * A[m * N + c];
+                    v.rowp[c] = prod - (c == jrow ? 1.0 : 0.0);
+                    v.col[c] = A[c * N + jrow] / R;   // factor of row c of the update
+                    D[jrow * N + c] = v.nval[c];
+                    Dg[c] = make_double2(v.ngrad[c * 2], v.ngrad[c * 2 + 1]);
+                    Dl[c] = make_double2(v.nlap[c * 2], v.nlap[c * 2 + 1]);
+                }
+                const double upd = bs[1] + 1.0;
+                const double old_log = bs[0];
+                bool rebuild = upd >= 64.0 || !isfinite(R) || fabs(R) < 1e-5 || bs[2] > 1e8 ||
+                               fabs(R) <= 1e4 * kEps * acc[1];
+                __syncwarp();
+                if (lane == 0) {
+                    bs[1] = upd;
+                    rabs[jrow] = acc[15];
+                }
+                double rs_max = 0.0;
+                if (rebuild) {
+                    gj_rebuild_warp<S>(A, v.work, v.col, D, N, v.misc);
+                } else {
+#pragma unroll 1
+                    for (int a = lane; a < N; a += 32) {
+                        const double ca = v.col[a];
+                        double rsum = 0.0;
+#pragma unroll 4
+                        for (int c = 0; c < N; ++c) {
+                            const double x = A[a * N + c] - ca * v.rowp[c];
+                            A[a * N + c] = x;
+                            rsum += fabs(x);
+                        }
+                        rs_max = fmax(rs_max, rsum);
+                    }
+                }
+                __syncwarp();
+                double rd_max = 0.0;
+                for (int a = lane; a < N; a += 32) {
+                    rd_max = fmax(rd_max, rabs[a]);
+                    if (rebuild) {
+                        double rsum = 0.0;
+                        for (int c = 0; c < N; ++c) rsum += fabs(A[a * N + c]);
+                        rs_max = fmax(rs_max, rsum);
+                    }
+                }
+                const double cond = warp_max(rd_max) * warp_max(rs_max);
+                if (!rebuild && (!isfinite(cond) || cond > 1e8)) {
+                    gj_rebuild_warp<S>(A, v.work, v.col, D, N, v.misc);
+                    rebuild = true;
+                }
+                // the moved particle's determinant derivatives at the committed inverse
+                double dv[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int m = lane; m < N; m += 32) {
+                    const double a = A[m * N + jrow];
+                    dv[0] += a * v.ngrad[m * 2 + 0];
+                    dv[1] += a * v.ngrad[m * 2 + 1];
+                    dv[2] += a * v.nlap[m * 2 + 0];
+                    dv[3] += a * v.nlap[m * 2 + 1];
+                }
+                warp_allsum<4>(dv);
+                if (lane == 0) {
+                    bs[2] = cond;
+                    if (rebuild) {
+                        bs[0] = v.misc[M_LOGDET];
+                        bs[1] = 0.0;
+                        if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+                    } else {
+                        bs[0] = old_log + log(fabs(R));
+                    }
+                    v.scal[S_LOGPSI] += bs[0] - old_log;
+                    v.sg[p * 2 + 0] = dv[0];
+                    v.sg[p * 2 + 1] = dv[1];
+                    v.sl[p * 2 + 0] = dv[2] - dv[0] * dv[0];
+                    v.sl[p * 2 + 1] = dv[3] - dv[1] * dv[1];
+                }
+            }
+            if (lane == 0) {
+                v.jg[p * 2 + 0] = acc[7];
+                v.jg[p * 2 + 1] = acc[8];
+                v.jl[p * 2 + 0] = acc[9];
+                v.jl[p * 2 + 1] = acc[10];
+                v.kg[p * 2 + 0] = acc[11];
+                v.kg[p * 2 + 1] = acc[12];
+                v.kl[p * 2 + 0] = acc[13];
+                v.kl[p * 2 + 1] = acc[14];
+                double wx = nx, wy = ny;
+                wrap2(s, wx, wy);
+                v.pos[p * 2 + 0] = wx;
+                v.pos[p * 2 + 1] = wy;
+                v.scal[S_LOGPSI] += logr - logdr;
+            }
+            __syncwarp();
+        }
+        if (dmc || sub == prm.n_sub - 1) {
+            __syncwarp();
+            const double el = local_energy_warp<S>(s, sm, rec, pairs, npair);
+            if (lane == 0) {
+                v.scal[S_EL] = el;
+                if (dmc) {
+                    const double enew = el, eold = v.scal[S_EPREV];
+                    double half_tau = 0.5 * prm.tau;
+                    const double x = fmax(prm.eref - enew, prm.eref - eold);
+                    if (x > prm.e_max)
+                        half_tau = 0.0;
+                    else if (x > prm.e_cut)
+                        half_tau *= 1.0 - (x - prm.e_cut) / (prm.e_max - prm.e_cut);
+                    v.scal[S_WEIGHT] *= exp(half_tau * (2.0 * prm.etrial - enew - eold));
+                    if (x > prm.e_cut) v.scal[S_NCUT] += 1.0;
+                    v.scal[S_EPREV] = enew;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        if (dmc && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
+        if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+    }
+    store_hot<32>(s, rec, sm);
+}
+
+bool fast_sweep_eligible(const DevSys& s) {
+    return s.dim == 2 && !s.cplx && s.nbf == 0 && s.pair_by_group && s.np <= 64 && s.maxN <= 64 &&
+           s.nkJ <= 64 && s.ngroups <= 8;
+}
+
+cudaError_t reserve_smem_fast(size_t smem) {
+    return cudaFuncSetAttribute(reinterpret_cast<const void*>(sweep_fast_kernel<2>),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+}
+
+cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
+                              const double* randoms, long stride, const SweepParams& prm, const int2* pairs,
+                              int npair) {
+    sweep_fast_kernel<2><<<nw, 32, smem, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
+    return cudaGetLastError();
+}
+
+}  // namespace alea_gpu

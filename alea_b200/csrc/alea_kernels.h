@@ -30,6 +30,15 @@ cudaError_t launch_move(int nt, int nw, size_t smem, cudaStream_t st, const DevS
 cudaError_t launch_sweep(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
                          double* records, const double* randoms, long stride,
                          const SweepParams& prm, const int2* pairs, int npair);
+// The one-warp sweep (alea_fast.cu): systems of real determinants and
+// group-wise pair terms with at most 64 particles, 64 orbitals per block and
+// 64 image-sum k-vectors.  launch_sweep takes it for 32-thread walkers unless
+// ALEA_GPU_SWEEP=generic is set in the environment.
+bool fast_sweep_eligible(const DevSys& s);
+cudaError_t reserve_smem_fast(size_t smem);
+cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
+                              const double* randoms, long stride, const SweepParams& prm, const int2* pairs,
+                              int npair);
 __global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
                             int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
                             double zr, double* out, int crowd_mode);

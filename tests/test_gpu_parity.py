@@ -224,3 +224,43 @@ def test_free_twisted_determinant_kinetic_energy_on_device():
     q = np.concatenate([np.array(b["q"]) for b in s["slater"]])
     exact = 0.5 * np.sum(q * q)
     assert np.max(np.abs(g.download()["local_energy"] - exact)) < 1e-12 * abs(exact) + 1e-15
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["heg42", "crystal16", "dipoles16"])
+def test_one_warp_sweep_matches_generic_sweep(name, monkeypatch):
+    """The one-warp sweep (taken by 32-thread walkers of real determinants)
+    and the generic CTA sweep (ALEA_GPU_SWEEP=generic) on the same walkers
+    and random streams: VMC positions bit for bit; after drift VMC and DMC
+    advances, positions to 1e-9 and E_L, weights, ln ψ to 1e-10."""
+    import alea_b200
+    setup = golden(f"setup_{name}.json")
+    pos = np.array(golden(f"eval_{name}.json")["positions"])
+    nw = pos.shape[0]
+    tau = {"heg42": 225.0, "crystal16": 400.0, "dipoles16": 0.0003}[name]
+    dtau = {"heg42": 0.5, "crystal16": 1.0, "dipoles16": 1e-5}[name]
+    out = []
+    for mode in ("generic", "fast"):
+        if mode == "generic":
+            monkeypatch.setenv("ALEA_GPU_SWEEP", "generic")
+        else:
+            monkeypatch.delenv("ALEA_GPU_SWEEP", raising=False)
+        g = walkers(setup, nw)
+        g.upload(pos)
+        g.set_streams(17, alea_b200.STREAM_VMC, nw)
+        g.vmc_step(tau, 2, False)
+        vmc_pos = g.download()["positions"]
+        g.vmc_step(dtau, 2, True)
+        g.set_streams(17, alea_b200.STREAM_DMC, nw)
+        el = g.download()["local_energy"]
+        e0 = float(np.mean(el))
+        g.dmc_advance(dtau, 1, e0, e0, 10.0, 15.0)
+        g.dmc_advance(dtau, 1, e0, e0, 10.0, 15.0)
+        out.append((vmc_pos, g.download()))
+        g.close()
+    (vp_g, d_g), (vp_f, d_f) = out
+    assert np.array_equal(vp_g, vp_f)
+    assert np.max(np.abs(d_f["positions"] - d_g["positions"])) < 1e-9 * np.abs(d_g["positions"]).max()
+    assert rel(d_f["local_energy"], d_g["local_energy"]) < 1e-10
+    assert rel(d_f["log_psi"], d_g["log_psi"], floor=1.0) < 1e-10
+    assert rel(d_f["weights"], d_g["weights"]) < 1e-10
