@@ -821,6 +821,44 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     s.s_rad = s.s_work;
     s.s_total = static_cast<int>(m);
     c->smem = static_cast<size_t>(s.s_total) * 8;
+    // the one-warp sweep's layout (see DevSys)
+    s.f_total = 0;
+    if (fast_sweep_eligible(s)) {
+        const long np2 = 2L * np;
+        long f = 0;
+        auto ftake = [&](long n) {
+            const long at = f;
+            f += round4(std::max(n, 1L));
+            return static_cast<int>(at);
+        };
+        s.f_pos = ftake(np2);
+        s.f_jg = ftake(np2);
+        s.f_jl = ftake(np2);
+        s.f_scal = ftake(s.hot - s.o_scal);
+        s.f_misc = ftake(8);   // the error flag lives through the whole sweep
+        const long scratch = f;
+        s.f_nval = ftake(s.maxN);
+        s.f_ngrad = ftake(2L * s.maxN);
+        s.f_nlap = ftake(2L * s.maxN);
+        s.f_col = ftake(s.maxN);
+        s.f_rowp = ftake(s.maxN);
+        s.f_work = static_cast<int>(f);
+        const long changes = round4(4L * np) + 4 * round4(std::max(s.nkJ, 1));
+        s.f_cn = s.f_work + static_cast<int>(round4(4L * np));
+        s.f_sn = s.f_cn + static_cast<int>(round4(std::max(s.nkJ, 1)));
+        s.f_co = s.f_sn + static_cast<int>(round4(std::max(s.nkJ, 1)));
+        s.f_so = s.f_co + static_cast<int>(round4(std::max(s.nkJ, 1)));
+        f += std::max(round4(static_cast<long>(s.maxN) * s.maxN), changes);
+        const long moves_end = f;
+        f = scratch;   // the local energy reuses the whole scratch area
+        s.f_sg = ftake(np2);
+        s.f_sl = ftake(np2);
+        s.f_kg = ftake(np2);
+        s.f_kl = ftake(np2);
+        s.f_elwork = static_cast<int>(f);
+        f += round4(std::max({3L * s.ngroups * s.nkJ, 2L * s.enk, 1L}));
+        s.f_total = static_cast<int>(std::max(f, moves_end));
+    }
     if (c->smem > 227 * 1024)
         return fail(c, ALEA_ERR_UNSUPPORTED,
                     "walker state needs " + std::to_string(c->smem) + " bytes of shared memory (> 227 KB)");

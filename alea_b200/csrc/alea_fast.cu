@@ -256,12 +256,78 @@ __device__ __noinline__ void gj_rebuild_warp(double* A, double* m, double* col, 
     __syncwarp();
 }
 
-// The local energy after a sweep: every particle's derivatives refreshed,
-// then kinetic + Ewald + open pair potentials.  Out of line: once per sweep.
+// Shared-memory view of the one-warp layout (DevSys f_*).  The sg, sl, kg,
+// kl planes exist only in the local-energy phase (el = true), on top of the
+// move scratch; `work` is the move union or the local energy's tables.
+__device__ __forceinline__ Smem view_fast(const DevSys& s, double* sm, bool el) {
+    Smem v{};
+    v.pos = sm + s.f_pos;
+    v.jg = sm + s.f_jg;
+    v.jl = sm + s.f_jl;
+    v.scal = sm + s.f_scal;
+    v.rho = v.scal - s.o_scal + s.o_rho;
+    v.nval = sm + s.f_nval;
+    v.ngrad = sm + s.f_ngrad;
+    v.nlap = sm + s.f_nlap;
+    v.col = sm + s.f_col;
+    v.rowp = sm + s.f_rowp;
+    v.misc = sm + s.f_misc;
+    v.cn = sm + s.f_cn;
+    v.sn = sm + s.f_sn;
+    v.co = sm + s.f_co;
+    v.so = sm + s.f_so;
+    v.work = sm + (el ? s.f_elwork : s.f_work);
+    if (el) {
+        v.sg = sm + s.f_sg;
+        v.sl = sm + s.f_sl;
+        v.kg = sm + s.f_kg;
+        v.kl = sm + s.f_kl;
+    }
+    return v;
+}
+
+// n doubles (n even, both ends 16-byte aligned) from src to dst by the warp.
+__device__ __forceinline__ void copy_warp(double* dst, const double* src, int n) {
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+    double2* d2 = reinterpret_cast<double2*>(dst);
+    for (int i = threadIdx.x; i < n / 2; i += 32) d2[i] = s2[i];
+}
+
+// The record's positions, pair-Jastrow planes and [scalars, end of the hot
+// part) into the one-warp layout, and back.
+__device__ __forceinline__ void load_fast(const DevSys& s, const double* rec, double* sm) {
+    const int n2 = 2 * s.np;
+    copy_warp(sm + s.f_pos, rec + s.o_pos, n2);
+    copy_warp(sm + s.f_jg, rec + s.o_jg, n2);
+    copy_warp(sm + s.f_jl, rec + s.o_jl, n2);
+    copy_warp(sm + s.f_scal, rec + s.o_scal, s.hot - s.o_scal);
+    __syncwarp();
+}
+
+__device__ __forceinline__ void store_fast(const DevSys& s, double* rec, const double* sm) {
+    __syncwarp();
+    const int n2 = 2 * s.np;
+    copy_warp(rec + s.o_pos, sm + s.f_pos, n2);
+    copy_warp(rec + s.o_jg, sm + s.f_jg, n2);
+    copy_warp(rec + s.o_jl, sm + s.f_jl, n2);
+    copy_warp(rec + s.o_scal, sm + s.f_scal, s.hot - s.o_scal);
+    copy_warp(rec + s.o_sg, sm + s.f_sg, n2);
+    copy_warp(rec + s.o_sl, sm + s.f_sl, n2);
+    copy_warp(rec + s.o_kg, sm + s.f_kg, n2);
+    copy_warp(rec + s.o_kl, sm + s.f_kl, n2);
+}
+
+// The local energy after a sweep: every particle's derivatives refreshed
+// into the local-energy planes (zero for particles outside every determinant
+// or image sum, as in the record), then kinetic + Ewald + open pair
+// potentials.  Out of line: once per sweep.
 template <int S>
 __device__ __noinline__ double local_energy_warp(const DevSys& s, double* sm, const double* grec,
                                                  const int2* pairs, int npair) {
-    const Smem v = view(s, sm);
+    const Smem v = view_fast(s, sm, true);
+    __syncwarp();
+    for (int i = threadIdx.x; i < 2 * s.np; i += 32) v.sg[i] = v.sl[i] = v.kg[i] = v.kl[i] = 0.0;
+    __syncwarp();
     refresh_all<32, S>(s, v, grec);
     return local_energy<32, S>(s, v, pairs, npair);
 }
@@ -288,8 +354,8 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
     if (w >= nw) return;
     const int lane = threadIdx.x;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot<32>(s, rec, sm);
-    const Smem v = view(s, sm);
+    load_fast(s, rec, sm);
+    const Smem v = view_fast(s, sm, false);
     const int np = s.np, nk = s.nkJ;
     const bool dmc = prm.mode == 1;
     const bool drift = dmc || prm.drift != 0;
@@ -346,6 +412,7 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
             const bool ks = imask != 0;
             const double px = v.pos[p * 2], py = v.pos[p * 2 + 1];
             // ── drift refresh of p: determinant and k-space derivatives ──
+            double sgp0 = 0.0, sgp1 = 0.0, kgp0 = 0.0, kgp1 = 0.0;
             if (drift) {
                 double ra[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 if (b >= 0) {
@@ -382,27 +449,17 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                     }
                 }
                 warp_allsum<8>(ra);
-                if (lane == 0) {
-                    if (b >= 0) {
-                        v.sg[p * 2 + 0] = ra[0];
-                        v.sg[p * 2 + 1] = ra[1];
-                        v.sl[p * 2 + 0] = ra[2] - ra[0] * ra[0];
-                        v.sl[p * 2 + 1] = ra[3] - ra[1] * ra[1];
-                    }
-                    if (ks) {
-                        v.kg[p * 2 + 0] = ra[4];
-                        v.kg[p * 2 + 1] = ra[5];
-                        v.kl[p * 2 + 0] = ra[6];
-                        v.kl[p * 2 + 1] = ra[7];
-                    }
-                }
+                sgp0 = ra[0];
+                sgp1 = ra[1];
+                kgp0 = ra[4];
+                kgp1 = ra[5];
                 __syncwarp();
             }
             // ── proposal (every lane, identical arithmetic) ──
             const double r0 = from_owner<S>(rz0, p), r1 = from_owner<S>(rz1, p), u = from_owner<S>(rzu, p);
             const double tm = prm.tau * s.inv_mass[p * 2];
-            const double gx = v.sg[p * 2] + v.jg[p * 2] + v.kg[p * 2];
-            const double gy = v.sg[p * 2 + 1] + v.jg[p * 2 + 1] + v.kg[p * 2 + 1];
+            const double gx = sgp0 + v.jg[p * 2] + kgp0;
+            const double gy = sgp1 + v.jg[p * 2 + 1] + kgp1;
             double sc = tm;
             if (dmc) {
                 const double vsq = gx * gx + gy * gy;
@@ -657,16 +714,8 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                     gj_rebuild_warp<S>(A, v.work, v.col, D, N, v.misc);
                     rebuild = true;
                 }
-                // the moved particle's determinant derivatives at the committed inverse
-                double dv[4] = {0.0, 0.0, 0.0, 0.0};
-                for (int m = lane; m < N; m += 32) {
-                    const double a = A[m * N + jrow];
-                    dv[0] += a * v.ngrad[m * 2 + 0];
-                    dv[1] += a * v.ngrad[m * 2 + 1];
-                    dv[2] += a * v.nlap[m * 2 + 0];
-                    dv[3] += a * v.nlap[m * 2 + 1];
-                }
-                warp_allsum<4>(dv);
+                // (the moved particle's determinant derivatives are not kept:
+                // a drift move refreshes them first, the local energy refreshes all)
                 if (lane == 0) {
                     bs[2] = cond;
                     if (rebuild) {
@@ -677,10 +726,6 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                         bs[0] = old_log + log(fabs(R));
                     }
                     v.scal[S_LOGPSI] += bs[0] - old_log;
-                    v.sg[p * 2 + 0] = dv[0];
-                    v.sg[p * 2 + 1] = dv[1];
-                    v.sl[p * 2 + 0] = dv[2] - dv[0] * dv[0];
-                    v.sl[p * 2 + 1] = dv[3] - dv[1] * dv[1];
                 }
             }
             if (lane == 0) {
@@ -688,10 +733,6 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                 v.jg[p * 2 + 1] = acc[8];
                 v.jl[p * 2 + 0] = acc[9];
                 v.jl[p * 2 + 1] = acc[10];
-                v.kg[p * 2 + 0] = acc[11];
-                v.kg[p * 2 + 1] = acc[12];
-                v.kl[p * 2 + 0] = acc[13];
-                v.kl[p * 2 + 1] = acc[14];
                 double wx = nx, wy = ny;
                 wrap2(s, wx, wy);
                 v.pos[p * 2 + 0] = wx;
@@ -725,7 +766,7 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
         if (dmc && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
         if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
     }
-    store_hot<32>(s, rec, sm);
+    store_fast(s, rec, sm);
 }
 
 bool fast_sweep_eligible(const DevSys& s) {
@@ -741,7 +782,9 @@ cudaError_t reserve_smem_fast(size_t smem) {
 cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
                               const double* randoms, long stride, const SweepParams& prm, const int2* pairs,
                               int npair) {
-    sweep_fast_kernel<2><<<nw, 32, smem, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
+    (void)smem;
+    sweep_fast_kernel<2><<<nw, 32, static_cast<size_t>(s.f_total) * 8, st>>>(s, records, nw, randoms, stride,
+                                                                             prm, pairs, npair);
     return cudaGetLastError();
 }
 
