@@ -33,10 +33,17 @@ def deps():
 
 
 def needs_build() -> bool:
+    """True when the library is missing or older than an object's sources."""
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(p) > t for p in deps())
+    for src in sources():
+        obj = os.path.join(HERE, "_build", os.path.basename(src) + ".o")
+        if not os.path.exists(obj) or os.path.getmtime(obj) > t:
+            return True
+        if any(os.path.getmtime(d) > os.path.getmtime(obj) for d in includes(src)):
+            return True
+    return False
 
 
 def includes(path, seen=None):
@@ -57,8 +64,6 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile the sources whose object is older than the source or any header
     it includes, in parallel (the kernel files take minutes each), then link
     the shared library."""
-    if not force and not needs_build():
-        return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     obj_dir = os.path.join(HERE, "_build")
     os.makedirs(obj_dir, exist_ok=True)
@@ -75,6 +80,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd))
         jobs.append((obj, subprocess.Popen(cmd)))
+    if not jobs and os.path.exists(LIB) and all(
+            os.path.exists(o) and os.path.getmtime(o) <= os.path.getmtime(LIB) for o in objs):
+        return LIB
     failed = [obj for obj, proc in jobs if proc.wait() != 0]
     if failed:
         for obj in failed:

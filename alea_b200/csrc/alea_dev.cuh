@@ -205,6 +205,21 @@ __device__ __forceinline__ double fold_dist(const DevSys& s, const double* xi, c
 
 // ───────────────────────── radial functions ─────────────────────────────
 
+// Read-only table loads that ask L1 to keep the line (evict_last): the
+// spline, k-vector and weight tables are shared by every walker on an SM,
+// while the walker records stream through.
+__device__ __forceinline__ double2 ldg_keep(const double2* p) {
+    double2 r;
+    asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
+    return r;
+}
+
+__device__ __forceinline__ double ldg_keep(const double* p) {
+    double r;
+    asm("ld.global.nc.L1::evict_last.f64 %0, [%1];" : "=d"(r) : "l"(p));
+    return r;
+}
+
 // The breakup's quintic Hermite spline, evaluated from its per-interval
 // monomial form c_0 + c_1 x + ... + c_5 x^5 in the local coordinate
 // x = r/δ - i (the host expands each interval's Hermite data once).
@@ -219,7 +234,7 @@ __device__ __forceinline__ void spline3(const DevSpline& sp, double r, double& f
     if (i > sp.n_knots - 2) i = sp.n_knots - 2;
     const double x = t - i;
     const double2* c2 = reinterpret_cast<const double2*>(sp.poly + 6 * i);
-    const double2 c01 = __ldg(c2), c23 = __ldg(c2 + 1), c45 = __ldg(c2 + 2);
+    const double2 c01 = ldg_keep(c2), c23 = ldg_keep(c2 + 1), c45 = ldg_keep(c2 + 2);
     f = fma(fma(fma(fma(fma(c45.y, x, c45.x), x, c23.y), x, c23.x), x, c01.y), x, c01.x);
     const double g = fma(fma(fma(fma(5.0 * c45.y, x, 4.0 * c45.x), x, 3.0 * c23.y), x, 2.0 * c23.x), x, c01.y);
     const double h = fma(fma(fma(20.0 * c45.y, x, 12.0 * c45.x), x, 6.0 * c23.y), x, 2.0 * c23.x);
@@ -234,7 +249,7 @@ __device__ __forceinline__ double spline1(const DevSpline& sp, double r) {
     if (i > sp.n_knots - 2) i = sp.n_knots - 2;
     const double x = t - i;
     const double2* c2 = reinterpret_cast<const double2*>(sp.poly + 6 * i);
-    const double2 c01 = __ldg(c2), c23 = __ldg(c2 + 1), c45 = __ldg(c2 + 2);
+    const double2 c01 = ldg_keep(c2), c23 = ldg_keep(c2 + 1), c45 = ldg_keep(c2 + 2);
     return fma(fma(fma(fma(fma(c45.y, x, c45.x), x, c23.y), x, c23.x), x, c01.y), x, c01.x);
 }
 
@@ -332,9 +347,17 @@ __device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, do
     }
     if (T.kind == 0) {
         double p = 0.0, dp = 0.0, d2p = 0.0;
-        poly_acc(T.coef, T.nnum, r, p, dp, d2p);
         double q = 1.0, dq = 0.0, d2q = 0.0;
-        poly_acc(T.coef + T.nnum, T.nden, r, q, dq, d2q);
+        if (T.nnum == 1 && T.nden == 1) {   // a r / (1 + b r): the sums below, unrolled
+            const double a = T.coef[0], b = T.coef[1];
+            p = a * r;
+            dp = a;
+            q = fma(b, r, 1.0);
+            dq = b;
+        } else {
+            poly_acc(T.coef, T.nnum, r, p, dp, d2p);
+            poly_acc(T.coef + T.nnum, T.nden, r, q, dq, d2q);
+        }
         const double inv_q = 1.0 / q;
         u = p * inv_q;
         du = (dp * q - p * dq) * inv_q * inv_q;

@@ -59,8 +59,8 @@ __device__ __forceinline__ void fetch_rows(const DevSys& s, const double* grec, 
     for (int j = 0; j < S; ++j) {
         const int m = static_cast<int>(threadIdx.x) + 32 * j;
         if (m < N) {
-            dg[j] = rg[m];
-            dl[j] = rl[m];
+            dg[j] = __ldcg(rg + m);
+            dl[j] = __ldcg(rl + m);
         }
     }
 }
@@ -164,7 +164,7 @@ __device__ __noinline__ void gj_rebuild_warp(double* A, double* m, double* col, 
         const int c = lane + 32 * j;
         if (c >= N) continue;
         for (int r = 0; r < N; ++r) {
-            m[r * N + c] = D[r * N + c];
+            m[r * N + c] = __ldcg(D + r * N + c);
             A[r * N + c] = (r == c) ? 1.0 : 0.0;
         }
     }
@@ -286,35 +286,42 @@ __device__ __forceinline__ Smem view_fast(const DevSys& s, double* sm, bool el) 
     return v;
 }
 
-// n doubles (n even, both ends 16-byte aligned) from src to dst by the warp.
-__device__ __forceinline__ void copy_warp(double* dst, const double* src, int n) {
+// n doubles (n even, both ends 16-byte aligned) between a record (global,
+// through L2 only: records stream through) and shared memory, by the warp.
+__device__ __forceinline__ void copy_in_warp(double* dst, const double* src, int n) {
     const double2* s2 = reinterpret_cast<const double2*>(src);
     double2* d2 = reinterpret_cast<double2*>(dst);
-    for (int i = threadIdx.x; i < n / 2; i += 32) d2[i] = s2[i];
+    for (int i = threadIdx.x; i < n / 2; i += 32) d2[i] = __ldcg(s2 + i);
+}
+
+__device__ __forceinline__ void copy_out_warp(double* dst, const double* src, int n) {
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+    double2* d2 = reinterpret_cast<double2*>(dst);
+    for (int i = threadIdx.x; i < n / 2; i += 32) __stcg(d2 + i, s2[i]);
 }
 
 // The record's positions, pair-Jastrow planes and [scalars, end of the hot
 // part) into the one-warp layout, and back.
 __device__ __forceinline__ void load_fast(const DevSys& s, const double* rec, double* sm) {
     const int n2 = 2 * s.np;
-    copy_warp(sm + s.f_pos, rec + s.o_pos, n2);
-    copy_warp(sm + s.f_jg, rec + s.o_jg, n2);
-    copy_warp(sm + s.f_jl, rec + s.o_jl, n2);
-    copy_warp(sm + s.f_scal, rec + s.o_scal, s.hot - s.o_scal);
+    copy_in_warp(sm + s.f_pos, rec + s.o_pos, n2);
+    copy_in_warp(sm + s.f_jg, rec + s.o_jg, n2);
+    copy_in_warp(sm + s.f_jl, rec + s.o_jl, n2);
+    copy_in_warp(sm + s.f_scal, rec + s.o_scal, s.hot - s.o_scal);
     __syncwarp();
 }
 
 __device__ __forceinline__ void store_fast(const DevSys& s, double* rec, const double* sm) {
     __syncwarp();
     const int n2 = 2 * s.np;
-    copy_warp(rec + s.o_pos, sm + s.f_pos, n2);
-    copy_warp(rec + s.o_jg, sm + s.f_jg, n2);
-    copy_warp(rec + s.o_jl, sm + s.f_jl, n2);
-    copy_warp(rec + s.o_scal, sm + s.f_scal, s.hot - s.o_scal);
-    copy_warp(rec + s.o_sg, sm + s.f_sg, n2);
-    copy_warp(rec + s.o_sl, sm + s.f_sl, n2);
-    copy_warp(rec + s.o_kg, sm + s.f_kg, n2);
-    copy_warp(rec + s.o_kl, sm + s.f_kl, n2);
+    copy_out_warp(rec + s.o_pos, sm + s.f_pos, n2);
+    copy_out_warp(rec + s.o_jg, sm + s.f_jg, n2);
+    copy_out_warp(rec + s.o_jl, sm + s.f_jl, n2);
+    copy_out_warp(rec + s.o_scal, sm + s.f_scal, s.hot - s.o_scal);
+    copy_out_warp(rec + s.o_sg, sm + s.f_sg, n2);
+    copy_out_warp(rec + s.o_sl, sm + s.f_sl, n2);
+    copy_out_warp(rec + s.o_kg, sm + s.f_kg, n2);
+    copy_out_warp(rec + s.o_kl, sm + s.f_kl, n2);
 }
 
 // The local energy after a sweep: every particle's derivatives refreshed
@@ -346,7 +353,7 @@ __device__ __forceinline__ T from_owner(const T (&x)[S], int p) {
 }  // namespace
 
 template <int S>
-__global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
+__global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
                                                         int nw, const double* randoms, long stride,
                                                         SweepParams prm, const int2* pairs, int npair) {
     extern __shared__ __align__(16) double sm[];
@@ -397,9 +404,9 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
         for (int j = 0; j < S; ++j) {
             const int k = lane + 32 * j;
             const double* g = rnd + static_cast<long>(k) * 3 * stride + w;
-            rz0[j] = k < np ? g[0] : 0.0;
-            rz1[j] = k < np ? g[stride] : 0.0;
-            rzu[j] = k < np ? g[2 * stride] : 0.0;
+            rz0[j] = k < np ? __ldcs(g) : 0.0;
+            rz1[j] = k < np ? __ldcs(g + stride) : 0.0;
+            rzu[j] = k < np ? __ldcs(g + 2 * stride) : 0.0;
         }
         double2 dg[S], dl[S];
 #pragma unroll
@@ -434,7 +441,7 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                 if (ks) {
 #pragma unroll 1
                     for (int q = lane; q < nk; q += 32) {
-                        const double kxq = s.kxJ[q], kyq = s.kyJ[q];
+                        const double kxq = ldg_keep(s.kxJ + q), kyq = ldg_keep(s.kyJ + q);
                         double co, so;
                         sincos(fma(kyq, py, kxq * px), &so, &co);
                         v.co[q] = co;
@@ -444,7 +451,8 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                             const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
                             const int go = T.same0 ? gp : (gp == ga ? gb : ga);
                             const double* pr = v.rho + go * 2 * nk;
-                            kterm_r(kxq, kyq, T.kw[q], co, so, pr[q], pr[nk + q], T.same0 ? 1.0 : 0.0, ra + 4);
+                            kterm_r(kxq, kyq, ldg_keep(T.kw + q), co, so, pr[q], pr[nk + q], T.same0 ? 1.0 : 0.0,
+                                    ra + 4);
                         }
                     }
                 }
@@ -507,48 +515,70 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                 }
             }
             // pair terms: p's new derivatives, the log ratio, and each
-            // partner's derivative change (kept in `work`, applied on accept)
+            // partner's derivative change (kept in `work`, applied on accept).
+            // Both partner slots go through each stage together so that their
+            // four radial evaluations overlap; an idle slot runs on a dummy
+            // partner at unit distance and contributes nothing.
+            {
+                unsigned cm[S];
+                double rn[S], ro[S], dnx[S], dny[S], dox[S], doy[S];
 #pragma unroll
-            for (int j = 0; j < S; ++j) {
-                const int k = lane + 32 * j;
-                const unsigned cm =
-                    (k < np && k != p) ? static_cast<unsigned>((cmask[j] >> (8 * gp)) & 0xffu) : 0u;
-                if (!cm) continue;
-                const double kx0 = v.pos[k * 2], ky0 = v.pos[k * 2 + 1];
-                double dnx, dny, dox, doy;
-                const double rn = fold2(s, nx, ny, kx0, ky0, dnx, dny);
-                const double ro = fold2(s, px, py, kx0, ky0, dox, doy);
-                double du_o = 0.0, d2u_o = 0.0, du_n = 0.0, d2u_n = 0.0;
-                for (unsigned bits = cm; bits; bits &= bits - 1) {
-                    const DevTerm& T = s.terms[__ffs(bits) - 1];
-                    double uo, duo, d2uo, un, dun, d2un;
-                    radial(T, ro, uo, duo, d2uo);
-                    radial(T, rn, un, dun, d2un);
-                    acc[6] += un - uo;
-                    du_o += duo;
-                    d2u_o += d2uo;
-                    du_n += dun;
-                    d2u_n += d2un;
+                for (int j = 0; j < S; ++j) {
+                    const int k = lane + 32 * j;
+                    cm[j] = (k < np && k != p) ? static_cast<unsigned>((cmask[j] >> (8 * gp)) & 0xffu) : 0u;
+                    const double kx0 = cm[j] ? v.pos[k * 2] : px + 1.0;
+                    const double ky0 = cm[j] ? v.pos[k * 2 + 1] : py;
+                    rn[j] = fold2(s, nx, ny, kx0, ky0, dnx[j], dny[j]);
+                    ro[j] = fold2(s, px, py, kx0, ky0, dox[j], doy[j]);
+                    if (!cm[j]) rn[j] = ro[j] = 1.0;
                 }
-                const double irn = 1.0 / rn, iro = 1.0 / ro;
-                double* dj = v.work + k * 4;
-                {
-                    const double dor = dnx * irn;
-                    acc[7] += du_n * dor;
-                    acc[9] += d2u_n * dor * dor + du_n * irn * (1.0 - dor * dor);
-                    const double dor_old = -dox * iro, dor_new = -dnx * irn;
-                    dj[0] = du_n * dor_new - du_o * dor_old;
-                    dj[2] = (d2u_n * dor_new * dor_new + du_n * irn * (1.0 - dor_new * dor_new)) -
-                            (d2u_o * dor_old * dor_old + du_o * iro * (1.0 - dor_old * dor_old));
+                double uo[S], duo[S], d2uo[S], un[S], dun[S], d2un[S];
+#pragma unroll
+                for (int j = 0; j < S; ++j) {
+                    const DevTerm& T = s.terms[cm[j] ? __ffs(cm[j]) - 1 : 0];
+                    radial(T, ro[j], uo[j], duo[j], d2uo[j]);
+                    radial(T, rn[j], un[j], dun[j], d2un[j]);
                 }
-                {
-                    const double dor = dny * irn;
-                    acc[8] += du_n * dor;
-                    acc[10] += d2u_n * dor * dor + du_n * irn * (1.0 - dor * dor);
-                    const double dor_old = -doy * iro, dor_new = -dny * irn;
-                    dj[1] = du_n * dor_new - du_o * dor_old;
-                    dj[3] = (d2u_n * dor_new * dor_new + du_n * irn * (1.0 - dor_new * dor_new)) -
-                            (d2u_o * dor_old * dor_old + du_o * iro * (1.0 - dor_old * dor_old));
+#pragma unroll
+                for (int j = 0; j < S; ++j) {
+                    // further terms on the same pair (rare)
+                    for (unsigned bits = cm[j] & (cm[j] - 1); bits; bits &= bits - 1) {
+                        const DevTerm& T = s.terms[__ffs(bits) - 1];
+                        double a0, a1, a2, b0, b1, b2;
+                        radial(T, ro[j], a0, a1, a2);
+                        radial(T, rn[j], b0, b1, b2);
+                        uo[j] += a0;
+                        duo[j] += a1;
+                        d2uo[j] += a2;
+                        un[j] += b0;
+                        dun[j] += b1;
+                        d2un[j] += b2;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < S; ++j) {
+                    if (!cm[j]) continue;
+                    const double irn = 1.0 / rn[j], iro = 1.0 / ro[j];
+                    acc[6] += un[j] - uo[j];
+                    double* dj = v.work + (lane + 32 * j) * 4;
+                    {
+                        const double dor = dnx[j] * irn;
+                        acc[7] += dun[j] * dor;
+                        acc[9] += d2un[j] * dor * dor + dun[j] * irn * (1.0 - dor * dor);
+                        const double dor_old = -dox[j] * iro, dor_new = -dnx[j] * irn;
+                        dj[0] = dun[j] * dor_new - duo[j] * dor_old;
+                        dj[2] = (d2un[j] * dor_new * dor_new + dun[j] * irn * (1.0 - dor_new * dor_new)) -
+                                (d2uo[j] * dor_old * dor_old + duo[j] * iro * (1.0 - dor_old * dor_old));
+                    }
+                    {
+                        const double dor = dny[j] * irn;
+                        acc[8] += dun[j] * dor;
+                        acc[10] += d2un[j] * dor * dor + dun[j] * irn * (1.0 - dor * dor);
+                        const double dor_old = -doy[j] * iro, dor_new = -dny[j] * irn;
+                        dj[1] = dun[j] * dor_new - duo[j] * dor_old;
+                        dj[3] = (d2un[j] * dor_new * dor_new + dun[j] * irn * (1.0 - dor_new * dor_new)) -
+                                (d2uo[j] * dor_old * dor_old + duo[j] * iro * (1.0 - dor_old * dor_old));
+                    }
                 }
             }
             // image sums: new phases of p, ratio and derivative terms; the
@@ -556,7 +586,7 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
             if (ks) {
 #pragma unroll 1
                 for (int q = lane; q < nk; q += 32) {
-                    const double kxq = s.kxJ[q], kyq = s.kyJ[q];
+                    const double kxq = ldg_keep(s.kxJ + q), kyq = ldg_keep(s.kyJ + q);
                     double cn, sn, co, so;
                     sincos(fma(kyq, ny, kxq * nx), &sn, &cn);
                     if (drift) {
@@ -568,7 +598,7 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                     const double* mr = v.rho + gp * 2 * nk;
                     for (unsigned bits = imask; bits; bits &= bits - 1) {
                         const DevTerm& T = s.terms[__ffs(bits) - 1];
-                        const double wk = T.kw[q];
+                        const double wk = ldg_keep(T.kw + q);
                         if (T.same0) {
                             const double qr = mr[q] + cn - co;
                             const double qi = mr[nk + q] + sn - so;
@@ -669,9 +699,9 @@ __global__ void __launch_bounds__(32) sweep_fast_kernel(const __grid_constant__ 
                     for (int m = 0; m < N; ++m) prod += v.nval[m] * A[m * N + c];
                     v.rowp[c] = prod - (c == jrow ? 1.0 : 0.0);
                     v.col[c] = A[c * N + jrow] / R;   // factor of row c of the update
-                    D[jrow * N + c] = v.nval[c];
-                    Dg[c] = make_double2(v.ngrad[c * 2], v.ngrad[c * 2 + 1]);
-                    Dl[c] = make_double2(v.nlap[c * 2], v.nlap[c * 2 + 1]);
+                    __stcg(D + jrow * N + c, v.nval[c]);
+                    __stcg(Dg + c, make_double2(v.ngrad[c * 2], v.ngrad[c * 2 + 1]));
+                    __stcg(Dl + c, make_double2(v.nlap[c * 2], v.nlap[c * 2 + 1]));
                 }
                 const double upd = bs[1] + 1.0;
                 const double old_log = bs[0];
