@@ -337,14 +337,10 @@ static __device__ __noinline__ void radial_zero_energy(double r, double ze_s, do
     d2u = m * (-2.0 * a * inv_r * inv_r * inv_r - 2.0 * a * inv_c * inv_c * inv_c);
 }
 
-// u, u', u'' of a pair term at r (the short-range half for an image sum).
-__device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, double& du,
-                                       double& d2u) {
-    if (T.kind == 2) {
-        radial_zero_energy(r, T.ze_s, T.ze_kappa, T.ze_rm, T.ze_rc, T.ze_c3, T.ze_logc1, T.ze_logc2,
-                           T.ze_cheb, u, du, d2u);
-        return;
-    }
+// u, u', u'' of a Padé (kind 0) or Drummond (kind 1) pair term at r (the
+// short-range half for an image sum).
+__device__ __forceinline__ void radial_pd(const DevTerm& T, double r, double& u, double& du,
+                                          double& d2u) {
     if (T.kind == 0) {
         double p = 0.0, dp = 0.0, d2p = 0.0;
         double q = 1.0, dq = 0.0, d2q = 0.0;
@@ -397,6 +393,17 @@ __device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, do
     u = m * (g * P);
     du = m * (dg * P + g * dP);
     d2u = m * (d2g * P + 2.0 * dg * dP + g * d2P);
+}
+
+// u, u', u'' of any pair term at r.
+__device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, double& du,
+                                       double& d2u) {
+    if (T.kind == 2) {
+        radial_zero_energy(r, T.ze_s, T.ze_kappa, T.ze_rm, T.ze_rc, T.ze_c3, T.ze_logc1, T.ze_logc2,
+                           T.ze_cheb, u, du, d2u);
+        return;
+    }
+    radial_pd(T, r, u, du, d2u);
 }
 
 // Does term T couple particles p and k (any of its group pairs)?

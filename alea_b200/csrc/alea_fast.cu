@@ -339,6 +339,17 @@ __device__ __noinline__ double local_energy_warp(const DevSys& s, double* sm, co
     return local_energy<32, S>(s, v, pairs, npair);
 }
 
+// A pair term's u, u', u'' for the one-warp sweep: without zero-energy terms
+// (ZE = false) only the inline Padé/Drummond forms are compiled, so the
+// move's pair stage makes no function call.
+template <bool ZE>
+__device__ __forceinline__ void radial_w(const DevTerm& T, double r, double& u, double& du, double& d2u) {
+    if constexpr (ZE)
+        radial(T, r, u, du, d2u);
+    else
+        radial_pd(T, r, u, du, d2u);
+}
+
 // Select slot p >> 5 of a per-lane register array and read it from lane
 // p & 31 (warp-uniform result).
 template <int S, class T>
@@ -352,7 +363,7 @@ __device__ __forceinline__ T from_owner(const T (&x)[S], int p) {
 
 }  // namespace
 
-template <int S>
+template <int S, bool ZE>
 __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
                                                         int nw, const double* randoms, long stride,
                                                         SweepParams prm, const int2* pairs, int npair) {
@@ -536,8 +547,8 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
                     const DevTerm& T = s.terms[cm[j] ? __ffs(cm[j]) - 1 : 0];
-                    radial(T, ro[j], uo[j], duo[j], d2uo[j]);
-                    radial(T, rn[j], un[j], dun[j], d2un[j]);
+                    radial_w<ZE>(T, ro[j], uo[j], duo[j], d2uo[j]);
+                    radial_w<ZE>(T, rn[j], un[j], dun[j], d2un[j]);
                 }
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
@@ -545,8 +556,8 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                     for (unsigned bits = cm[j] & (cm[j] - 1); bits; bits &= bits - 1) {
                         const DevTerm& T = s.terms[__ffs(bits) - 1];
                         double a0, a1, a2, b0, b1, b2;
-                        radial(T, ro[j], a0, a1, a2);
-                        radial(T, rn[j], b0, b1, b2);
+                        radial_w<ZE>(T, ro[j], a0, a1, a2);
+                        radial_w<ZE>(T, rn[j], b0, b1, b2);
                         uo[j] += a0;
                         duo[j] += a1;
                         d2uo[j] += a2;
@@ -712,10 +723,13 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                     bs[1] = upd;
                     rabs[jrow] = acc[15];
                 }
-                double rs_max = 0.0;
-                if (rebuild) {
-                    gj_rebuild_warp<S>(A, v.work, v.col, D, N, v.misc);
-                } else {
+                // rank-one update (or, on a trigger, the rebuild) and the
+                // condition estimate ||D||∞ ||A||∞ of the committed inverse;
+                // a rebuild taken for the estimate keeps the estimate from
+                // before it, as the reference does.  One call site of the
+                // out-of-line Gauss-Jordan.
+                double rs_max = 0.0, rd_max = 0.0;
+                if (!rebuild) {
 #pragma unroll 1
                     for (int a = lane; a < N; a += 32) {
                         const double ca = v.col[a];
@@ -730,18 +744,20 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                     }
                 }
                 __syncwarp();
-                double rd_max = 0.0;
-                for (int a = lane; a < N; a += 32) {
-                    rd_max = fmax(rd_max, rabs[a]);
-                    if (rebuild) {
-                        double rsum = 0.0;
-                        for (int c = 0; c < N; ++c) rsum += fabs(A[a * N + c]);
-                        rs_max = fmax(rs_max, rsum);
-                    }
-                }
-                const double cond = warp_max(rd_max) * warp_max(rs_max);
-                if (!rebuild && (!isfinite(cond) || cond > 1e8)) {
+                for (int a = lane; a < N; a += 32) rd_max = fmax(rd_max, rabs[a]);
+                rd_max = warp_max(rd_max);
+                double cond = rebuild ? 0.0 : rd_max * warp_max(rs_max);
+                const bool cond_rebuild = !rebuild && (!isfinite(cond) || cond > 1e8);
+                if (__builtin_expect(rebuild || cond_rebuild, 0)) {
                     gj_rebuild_warp<S>(A, v.work, v.col, D, N, v.misc);
+                    if (rebuild) {
+                        for (int a = lane; a < N; a += 32) {
+                            double rsum = 0.0;
+                            for (int c = 0; c < N; ++c) rsum += fabs(A[a * N + c]);
+                            rs_max = fmax(rs_max, rsum);
+                        }
+                        cond = rd_max * warp_max(rs_max);
+                    }
                     rebuild = true;
                 }
                 // (the moved particle's determinant derivatives are not kept:
@@ -804,17 +820,32 @@ bool fast_sweep_eligible(const DevSys& s) {
            s.nkJ <= 64 && s.ngroups <= 8;
 }
 
+// Does the system have a zero-energy pair term (the out-of-line radial form)?
+static bool has_zero_energy(const DevSys& s) {
+    for (int t = 0; t < s.nterms; ++t)
+        if (s.terms[t].kind == 2) return true;
+    return false;
+}
+
 cudaError_t reserve_smem_fast(size_t smem) {
-    return cudaFuncSetAttribute(reinterpret_cast<const void*>(sweep_fast_kernel<2>),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    for (const void* k : {reinterpret_cast<const void*>(sweep_fast_kernel<2, false>),
+                          reinterpret_cast<const void*>(sweep_fast_kernel<2, true>)}) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
                               const double* randoms, long stride, const SweepParams& prm, const int2* pairs,
                               int npair) {
     (void)smem;
-    sweep_fast_kernel<2><<<nw, 32, static_cast<size_t>(s.f_total) * 8, st>>>(s, records, nw, randoms, stride,
-                                                                             prm, pairs, npair);
+    const size_t bytes = static_cast<size_t>(s.f_total) * 8;
+    if (has_zero_energy(s))
+        sweep_fast_kernel<2, true><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
+    else
+        sweep_fast_kernel<2, false><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
     return cudaGetLastError();
 }
 
