@@ -203,6 +203,56 @@ __device__ __forceinline__ double fold_dist(const DevSys& s, const double* xi, c
     return sqrt(r2);
 }
 
+// 2-D forms of the above, same operation order, scalars instead of arrays.
+
+__device__ __forceinline__ void min_image2(const DevSys& s, double& x0, double& x1) {
+    if (!s.periodic) return;
+    if (s.ortho) {
+        x0 = fma(-s.box[0], rint(x0 * s.inv_box[0]), x0);
+        x1 = fma(-s.box[1], rint(x1 * s.inv_box[1]), x1);
+        return;
+    }
+    const double f0 = rint(fma(s.ainv[1], x1, s.ainv[0] * x0));
+    const double f1 = rint(fma(s.ainv[3], x1, s.ainv[2] * x0));
+    x0 -= fma(f1, s.a[2], f0 * s.a[0]);
+    x1 -= fma(f1, s.a[3], f0 * s.a[1]);
+    double b0 = x0, b1 = x1, best2 = fma(x1, x1, x0 * x0);
+#pragma unroll
+    for (int c = 1; c < 9; ++c) {
+        const double y0 = x0 + s.cand[c * 2 + 0];
+        const double y1 = x1 + s.cand[c * 2 + 1];
+        const double r2 = fma(y1, y1, y0 * y0);
+        const double take = (r2 < best2) ? 1.0 : 0.0;
+        best2 = fma(take, r2 - best2, best2);
+        b0 = fma(take, y0 - b0, b0);
+        b1 = fma(take, y1 - b1, b1);
+    }
+    x0 = b0;
+    x1 = b1;
+}
+
+// Folded displacement a - b and its length.
+__device__ __forceinline__ double fold2(const DevSys& s, double ax, double ay, double bx, double by,
+                                        double& dx, double& dy) {
+    dx = ax - bx;
+    dy = ay - by;
+    min_image2(s, dx, dy);
+    return sqrt(fma(dy, dy, dx * dx));
+}
+
+__device__ __forceinline__ void wrap2(const DevSys& s, double& x, double& y) {
+    if (!s.periodic) return;
+    if (s.ortho) {
+        x = fma(-s.box[0], rint(x * s.inv_box[0]), x);
+        y = fma(-s.box[1], rint(y * s.inv_box[1]), y);
+        return;
+    }
+    const double f0 = rint(fma(s.ainv[1], y, s.ainv[0] * x));
+    const double f1 = rint(fma(s.ainv[3], y, s.ainv[2] * x));
+    x -= fma(f1, s.a[2], f0 * s.a[0]);
+    y -= fma(f1, s.a[3], f0 * s.a[1]);
+}
+
 // ───────────────────────── radial functions ─────────────────────────────
 
 // Read-only table loads that ask L1 to keep the line (evict_last): the

@@ -65,56 +65,6 @@ __device__ __forceinline__ void fetch_rows(const DevSys& s, const double* grec, 
     }
 }
 
-// ── 2-D geometry, in the operation order of min_image / wrap_pos ──
-
-__device__ __forceinline__ void min_image2(const DevSys& s, double& x0, double& x1) {
-    if (!s.periodic) return;
-    if (s.ortho) {
-        x0 = fma(-s.box[0], rint(x0 * s.inv_box[0]), x0);
-        x1 = fma(-s.box[1], rint(x1 * s.inv_box[1]), x1);
-        return;
-    }
-    const double f0 = rint(fma(s.ainv[1], x1, s.ainv[0] * x0));
-    const double f1 = rint(fma(s.ainv[3], x1, s.ainv[2] * x0));
-    x0 -= fma(f1, s.a[2], f0 * s.a[0]);
-    x1 -= fma(f1, s.a[3], f0 * s.a[1]);
-    double b0 = x0, b1 = x1, best2 = fma(x1, x1, x0 * x0);
-#pragma unroll
-    for (int c = 1; c < 9; ++c) {
-        const double y0 = x0 + s.cand[c * 2 + 0];
-        const double y1 = x1 + s.cand[c * 2 + 1];
-        const double r2 = fma(y1, y1, y0 * y0);
-        const double take = (r2 < best2) ? 1.0 : 0.0;
-        best2 = fma(take, r2 - best2, best2);
-        b0 = fma(take, y0 - b0, b0);
-        b1 = fma(take, y1 - b1, b1);
-    }
-    x0 = b0;
-    x1 = b1;
-}
-
-// Folded displacement a - b and its length.
-__device__ __forceinline__ double fold2(const DevSys& s, double ax, double ay, double bx, double by,
-                                        double& dx, double& dy) {
-    dx = ax - bx;
-    dy = ay - by;
-    min_image2(s, dx, dy);
-    return sqrt(fma(dy, dy, dx * dx));
-}
-
-__device__ __forceinline__ void wrap2(const DevSys& s, double& x, double& y) {
-    if (!s.periodic) return;
-    if (s.ortho) {
-        x = fma(-s.box[0], rint(x * s.inv_box[0]), x);
-        y = fma(-s.box[1], rint(y * s.inv_box[1]), y);
-        return;
-    }
-    const double f0 = rint(fma(s.ainv[1], y, s.ainv[0] * x));
-    const double f1 = rint(fma(s.ainv[3], y, s.ainv[2] * x));
-    x -= fma(f1, s.a[2], f0 * s.a[0]);
-    y -= fma(f1, s.a[3], f0 * s.a[1]);
-}
-
 // Orbital i of a real block at (x, y): value, gradient, diagonal second
 // derivatives (plane waves, orbital_set.h:436-474; Gaussians, :185-224).
 __device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int i, double x, double y,
@@ -151,56 +101,68 @@ __device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int
 
 // A = D⁻¹ of an N x N block by pivoted Gauss-Jordan on one warp (first
 // maximum |pivot| of each column, as rebuild_inverse): lane l owns columns
-// l + 32j of the work copy m of D and of A.  Leaves log|det D| in
-// misc[M_LOGDET] and flags a zero or nonfinite pivot in misc[M_ERR].  Out of
-// line: it runs once per 64 accepted moves of a block.
+// l + 32j of the work copy m of D and of A.  The pivot is found with the
+// warp's integer max/min reductions on the bits of |x| (order-preserving for
+// non-negative doubles; NaNs never win, ties go to the lowest row) and its
+// value is broadcast from the lane that holds it, so no lane reads column k
+// while its owner swaps rows.  Leaves log|det D| in misc[M_LOGDET] and flags
+// a zero or nonfinite pivot in misc[M_ERR].
 template <int S>
-__device__ __noinline__ void gj_rebuild_warp(double* A, double* m, double* col, const double* D, int N,
-                                             double* misc) {
+__device__ __forceinline__ void gj_rebuild_warp(double* A, double* m, double* col, const double* D, int N,
+                                                double* misc) {
     const int lane = threadIdx.x;
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < S; ++j) {
         const int c = lane + 32 * j;
         if (c >= N) continue;
-        for (int r = 0; r < N; ++r) {
-            m[r * N + c] = __ldcg(D + r * N + c);
-            A[r * N + c] = (r == c) ? 1.0 : 0.0;
+        for (int r0 = 0; r0 < N; r0 += 8) {
+            double t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = (r0 + u < N) ? __ldcg(D + (r0 + u) * N + c) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = r0 + u;
+                if (r < N) {
+                    m[r * N + c] = t[u];
+                    A[r * N + c] = (r == c) ? 1.0 : 0.0;
+                }
+            }
         }
     }
     __syncwarp();
-    double logdet = 0.0;
+    double pivots[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) pivots[j] = 1.0;
     bool bad = false;
     for (int k = 0; k < N; ++k) {
-        // the pivot travels with its |value| and row through the butterfly,
-        // so no lane reads column k again after its owner starts the swap
-        double best = -1.0, bval = 0.0;
-        int bi = N;
+        unsigned long long key = 0ull;
+        int br = N;
+        double bv = 0.0;
         for (int r = k + lane; r < N; r += 32) {
             const double x = m[r * N + k];
-            if (fabs(x) > best) {
-                best = fabs(x);
-                bval = x;
-                bi = r;
+            const unsigned long long kx =
+                isnan(x) ? 0ull : static_cast<unsigned long long>(__double_as_longlong(fabs(x))) + 1ull;
+            if (kx > key) {
+                key = kx;
+                br = r;
+                bv = x;
             }
         }
+        const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+        const unsigned mhi = __reduce_max_sync(kAllLanes, hi);
+        const unsigned mlo = __reduce_max_sync(kAllLanes, hi == mhi ? lo : 0u);
+        const bool cand = hi == mhi && lo == mlo;
+        const unsigned prow = __reduce_min_sync(kAllLanes, cand ? static_cast<unsigned>(br) : 0xffffffffu);
+        const bool none = mhi == 0u && mlo == 0u;   // a column of NaNs has no pivot: flagged below
+        const int piv = none ? k : static_cast<int>(prow);
+        const unsigned owner = __ffs(__ballot_sync(kAllLanes, cand && br == piv && !none));
+        double diag = __shfl_sync(kAllLanes, bv, owner ? owner - 1 : 0);
+        if (none) diag = 0.0;
+        bad |= diag == 0.0 || !isfinite(diag);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(kAllLanes, best, o);
-            const double ov = __shfl_xor_sync(kAllLanes, bval, o);
-            const int oi = __shfl_xor_sync(kAllLanes, bi, o);
-            if (ob > best || (ob == best && oi < bi)) {
-                best = ob;
-                bval = ov;
-                bi = oi;
-            }
-        }
-        const int piv = bi < N ? bi : k;   // a column of NaNs has no pivot: flagged below
-        const double diag = bval;
-        if (lane == (k & 31)) {
-            logdet += log(fabs(diag));
-            bad |= diag == 0.0 || !isfinite(diag);
-        }
+        for (int j = 0; j < S; ++j)
+            if ((k >> 5) == j && lane == (k & 31)) pivots[j] = diag;
         double pk[S], ak[S];
 #pragma unroll
         for (int j = 0; j < S; ++j) {
@@ -247,11 +209,14 @@ __device__ __noinline__ void gj_rebuild_warp(double* A, double* m, double* col, 
         }
         __syncwarp();
     }
+    double logdet = 0.0;
+#pragma unroll
+    for (int j = 0; j < S; ++j)
+        if (lane + 32 * j < N) logdet += log(fabs(pivots[j]));
     logdet = warp_sum(logdet);
-    const bool any_bad = __any_sync(kAllLanes, bad);
     if (lane == 0) {
         misc[M_LOGDET] = logdet;
-        if (any_bad) misc[M_ERR] = 1.0;
+        if (bad) misc[M_ERR] = 1.0;
     }
     __syncwarp();
 }
@@ -390,6 +355,13 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                 msk |= static_cast<unsigned long long>(s.gterms[g][kgrp[j]]) << (8 * g);
         cmask[j] = msk;
     }
+    // groups of each term's first pair, 4 bits each: byte t = ga | gb << 4
+    unsigned long long tgrp = 0;
+    for (int t = 0; t < s.nterms; ++t) {
+        const unsigned ga = static_cast<unsigned>(s.group_of[s.terms[t].pairs[0][0]]);
+        const unsigned gb = static_cast<unsigned>(s.group_of[s.terms[t].pairs[0][2]]);
+        tgrp |= static_cast<unsigned long long>((ga & 15u) | ((gb & 15u) << 4)) << (8 * t);
+    }
     // image-summed terms each group takes part in (bit t of byte g)
     unsigned long long gimask = 0;
     for (int g = 0; g < s.ngroups; ++g)
@@ -458,8 +430,10 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                         v.co[q] = co;
                         v.so[q] = so;
                         for (unsigned bits = imask; bits; bits &= bits - 1) {
-                            const DevTerm& T = s.terms[__ffs(bits) - 1];
-                            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+                            const int t = __ffs(bits) - 1;
+                            const DevTerm& T = s.terms[t];
+                            const int ga = static_cast<int>((tgrp >> (8 * t)) & 15u);
+                            const int gb = static_cast<int>((tgrp >> (8 * t + 4)) & 15u);
                             const int go = T.same0 ? gp : (gp == ga ? gb : ga);
                             const double* pr = v.rho + go * 2 * nk;
                             kterm_r(kxq, kyq, ldg_keep(T.kw + q), co, so, pr[q], pr[nk + q], T.same0 ? 1.0 : 0.0,
@@ -476,7 +450,8 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
             }
             // ── proposal (every lane, identical arithmetic) ──
             const double r0 = from_owner<S>(rz0, p), r1 = from_owner<S>(rz1, p), u = from_owner<S>(rzu, p);
-            const double tm = prm.tau * s.inv_mass[p * 2];
+            const double im0 = ldg_keep(s.inv_mass + p * 2), im1 = ldg_keep(s.inv_mass + p * 2 + 1);
+            const double tm = prm.tau * im0;
             const double gx = sgp0 + v.jg[p * 2] + kgp0;
             const double gy = sgp1 + v.jg[p * 2 + 1] + kgp1;
             double sc = tm;
@@ -484,11 +459,11 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                 const double vsq = gx * gx + gy * gy;
                 sc = vsq < 1e-10 ? tm : (-1.0 + sqrt(1.0 + 2.0 * tm * vsq)) / vsq;
             }
-            const double sig0 = prm.sigma[p * 2], sig1 = prm.sigma[p * 2 + 1];
+            const double sig0 = ldg_keep(prm.sigma + p * 2), sig1 = ldg_keep(prm.sigma + p * 2 + 1);
             double nx, ny;
             if (drift) {
-                const double t0 = dmc ? sc : prm.tau * s.inv_mass[p * 2];
-                const double t1 = dmc ? sc : prm.tau * s.inv_mass[p * 2 + 1];
+                const double t0 = dmc ? sc : prm.tau * im0;
+                const double t1 = dmc ? sc : prm.tau * im1;
                 nx = fma(sig0, r0, fma(t0, gx, px));
                 ny = fma(sig1, r1, fma(t1, gy, py));
             } else {
@@ -608,7 +583,8 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                     }
                     const double* mr = v.rho + gp * 2 * nk;
                     for (unsigned bits = imask; bits; bits &= bits - 1) {
-                        const DevTerm& T = s.terms[__ffs(bits) - 1];
+                        const int t = __ffs(bits) - 1;
+                        const DevTerm& T = s.terms[t];
                         const double wk = ldg_keep(T.kw + q);
                         if (T.same0) {
                             const double qr = mr[q] + cn - co;
@@ -616,7 +592,8 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                             acc[6] += wk * (qr * qr + qi * qi - mr[q] * mr[q] - mr[nk + q] * mr[nk + q]);
                             kterm_r(kxq, kyq, wk, cn, sn, qr, qi, 1.0, acc + 11);
                         } else {
-                            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+                            const int ga = static_cast<int>((tgrp >> (8 * t)) & 15u);
+                            const int gb = static_cast<int>((tgrp >> (8 * t + 4)) & 15u);
                             const int go = gp == ga ? gb : ga;
                             const double* orr = v.rho + go * 2 * nk;
                             acc[6] += 2.0 * wk * ((cn - co) * orr[q] + (sn - so) * orr[nk + q]);
@@ -641,7 +618,7 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
             // ── accept / reject (every lane, identical decision) ──
             const double ngx_t = sgx + acc[7] + acc[11], ngy_t = sgy + acc[8] + acc[12];
             const double dx = nx - px, dy = ny - py;
-            const double tm0 = prm.tau * s.inv_mass[p * 2], tm1 = prm.tau * s.inv_mass[p * 2 + 1];
+            const double tm0 = prm.tau * im0, tm1 = prm.tau * im1;
             bool accept;
             if (dmc) {
                 accept = false;
@@ -706,9 +683,14 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                 __syncwarp();   // the new orbital row v.nval
 #pragma unroll 1
                 for (int c = lane; c < N; c += 32) {
-                    double prod = 0.0;
-                    for (int m = 0; m < N; ++m) prod += v.nval[m] * A[m * N + c];
-                    v.rowp[c] = prod - (c == jrow ? 1.0 : 0.0);
+                    double pa = 0.0, pb = 0.0;
+                    int m = 0;
+                    for (; m + 1 < N; m += 2) {
+                        pa += v.nval[m] * A[m * N + c];
+                        pb += v.nval[m + 1] * A[(m + 1) * N + c];
+                    }
+                    if (m < N) pa += v.nval[m] * A[m * N + c];
+                    v.rowp[c] = (pa + pb) - (c == jrow ? 1.0 : 0.0);
                     v.col[c] = A[c * N + jrow] / R;   // factor of row c of the update
                     __stcg(D + jrow * N + c, v.nval[c]);
                     __stcg(Dg + c, make_double2(v.ngrad[c * 2], v.ngrad[c * 2 + 1]));
@@ -733,14 +715,23 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
 #pragma unroll 1
                     for (int a = lane; a < N; a += 32) {
                         const double ca = v.col[a];
-                        double rsum = 0.0;
-#pragma unroll 4
-                        for (int c = 0; c < N; ++c) {
-                            const double x = A[a * N + c] - ca * v.rowp[c];
-                            A[a * N + c] = x;
-                            rsum += fabs(x);
+                        double ra = 0.0, rb = 0.0;
+                        int c = 0;
+#pragma unroll 2
+                        for (; c + 1 < N; c += 2) {
+                            const double x0 = A[a * N + c] - ca * v.rowp[c];
+                            const double x1 = A[a * N + c + 1] - ca * v.rowp[c + 1];
+                            A[a * N + c] = x0;
+                            A[a * N + c + 1] = x1;
+                            ra += fabs(x0);
+                            rb += fabs(x1);
                         }
-                        rs_max = fmax(rs_max, rsum);
+                        if (c < N) {
+                            const double x0 = A[a * N + c] - ca * v.rowp[c];
+                            A[a * N + c] = x0;
+                            ra += fabs(x0);
+                        }
+                        rs_max = fmax(rs_max, ra + rb);
                     }
                 }
                 __syncwarp();

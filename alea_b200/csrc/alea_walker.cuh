@@ -1175,6 +1175,34 @@ __device__ double ewald_recip_warp(const DevSys& s, const Smem& v) {
     return e;
 }
 
+// Ewald real-space sum Σ_{i<j} q_i q_j [1/(ε r) - V_long(r)] (r < r_cut) on
+// one warp: three pairs per lane in flight, no branch in the pair body.
+__device__ __forceinline__ double ewald_real_warp(const DevSys& s, const Smem& v, const int2* pairs,
+                                                  int npair) {
+    double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+    const int lane = threadIdx.x & 31;
+    for (int q0 = lane; q0 < npair; q0 += 96) {
+        double acc3[3];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const int q = q0 + 32 * u;
+            const bool on = q < npair;
+            const int2 pq = on ? pairs[q] : make_int2(0, 0);
+            const double coeff = on ? ldg_keep(s.charge + pq.x) * ldg_keep(s.charge + pq.y) : 0.0;
+            double dx, dy;
+            const double r = on ? fold2(s, v.pos[pq.x * 2], v.pos[pq.x * 2 + 1], v.pos[pq.y * 2],
+                                        v.pos[pq.y * 2 + 1], dx, dy)
+                                : 1.0;
+            const double t = coeff * (s.e_inv_eps / r - spline1(s.esp, r));
+            acc3[u] = (on && coeff != 0.0 && r < s.e_rcut) ? t : 0.0;
+        }
+        e0 += acc3[0];
+        e1 += acc3[1];
+        e2 += acc3[2];
+    }
+    return e0 + e1 + e2;
+}
+
 // Every particle's determinant and k-space derivatives (refresh_derivatives).
 // S > 0: the one-warp form (real determinants, lane-owned rows).
 template <int NT, int S = 0>
@@ -1748,7 +1776,8 @@ __device__ double local_energy(const DevSys& s, const Smem& v, const int2* pairs
         }
     }
     if (s.ewald) {
-        for (int q = threadIdx.x; q < npair; q += NT) {
+        if constexpr (S > 0) acc[0] += ewald_real_warp(s, v, pairs, npair);
+        for (int q = threadIdx.x; q < (S > 0 ? 0 : npair); q += NT) {
             const int2 pq = pairs[q];
             const double coeff = s.charge[pq.x] * s.charge[pq.y];
             if (coeff == 0.0) continue;
