@@ -406,7 +406,7 @@ def gpu_arm(a):
             "el_evals_per_s": evals_all / (ms_max * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic,
-                         "kernel": "sweep_kernel (DMC mode)", "peak_kind": peak_kind,
+                         "kernel": "sweep_fast_kernel (one-warp DMC sweep)", "peak_kind": peak_kind,
                          "bytes_per_move": b_move, "bytes_per_eval": b_eval,
                          "sweep_ms_per_launch": float(np.mean(sweep_ms)),
                          "sweep_share_of_step": t_sweep / (ms * 1e-3)},
