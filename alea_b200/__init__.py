@@ -20,7 +20,7 @@ import numpy as np
 from . import _capi
 from ._capi import load as _load
 
-__all__ = ["Walkers", "AleaGpuError", "pack_system", "STREAM_VMC", "STREAM_DMC", "STREAM_BRANCH"]
+__all__ = ["Walkers", "Server", "AleaGpuError", "pack_system", "STREAM_VMC", "STREAM_DMC", "STREAM_BRANCH"]
 
 STREAM_VMC = _capi.STREAM_VMC
 STREAM_DMC = _capi.STREAM_DMC
@@ -365,3 +365,72 @@ class Walkers:
                 generations=10.0):
         return self._run(self.lib.alea_gpu_dmc_run, n_eq, n_acc, n_steps, n_substeps, tau,
                          streams, seed, target=target, generations=generations, n_blocks_out=n_acc)
+
+
+class Server:
+    """Serving front end over alea_gpu_server (include/alea_gpu.h, serving):
+    jobs are queued, admitted by device-memory footprint and run
+    ``max_running`` at a time, each on its own context and stream.  The
+    packed system tables and positions of a job are kept alive here until
+    the job has finished."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_running: int = 8):
+        self.lib = _load()
+        h = ctypes.c_void_p()
+        rc = self.lib.alea_gpu_server_create(device, int(hbm_budget_bytes), int(max_running), ctypes.byref(h))
+        if rc != 0:
+            raise AleaGpuError(rc, "alea_gpu_server_create failed")
+        self.h = h
+        self._keep: Dict[int, Any] = {}
+
+    def submit(self, desc: Dict[str, Any], positions_aos: np.ndarray, mode: int, n_eq: int, n_acc: int,
+               n_steps: int, n_substeps: int, tau: float, seed: int, n_streams: int = 0,
+               use_drift: bool = False, target: int = 0, generations: float = 10.0,
+               cutoff_alpha: float = 2.0) -> int:
+        """Queue a VMC (mode 0) or DMC (mode 1) job; returns its id."""
+        sysc, keep = pack_system(desc)
+        np_ = int(desc["np"]) * int(desc["dim"])
+        pos = np.ascontiguousarray(np.asarray(positions_aos, dtype=np.float64).reshape(-1, np_))
+        nw = pos.shape[0]
+        job = _capi.Job()
+        job.system = ctypes.pointer(sysc)
+        job.positions = pos.ctypes.data_as(_capi.c_dp)
+        job.n_walkers = nw
+        job.mode = int(mode)
+        job.run = _capi.RunConfig(int(n_eq), int(n_acc), int(n_steps), int(n_substeps), float(tau),
+                                  int(bool(use_drift)), int(n_streams or nw), np.uint64(seed).item(),
+                                  int(target or nw), float(generations), float(cutoff_alpha))
+        jid = ctypes.c_uint64()
+        rc = self.lib.alea_gpu_submit_job(self.h, ctypes.byref(job), ctypes.byref(jid))
+        if rc != 0:
+            raise AleaGpuError(rc, self.lib.alea_gpu_server_last_error(self.h).decode())
+        self._keep[jid.value] = (sysc, keep, pos, job)
+        return jid.value
+
+    def poll(self, job_id: int, timeout_ms: int = 0) -> Optional[_capi.JobResult]:
+        """The job's result when it has finished, else None (after waiting
+        at most timeout_ms)."""
+        r = _capi.JobResult()
+        rc = self.lib.alea_gpu_poll(self.h, int(job_id), int(timeout_ms), ctypes.byref(r))
+        if rc == _capi.ERR_TIMEOUT:
+            return None
+        if rc != 0:
+            raise AleaGpuError(rc, "alea_gpu_poll: unknown job")
+        self._keep.pop(int(job_id), None)
+        return r
+
+    def cancel(self, job_id: int) -> bool:
+        """True if the job was queued or running and is now being cancelled."""
+        return self.lib.alea_gpu_cancel(self.h, int(job_id)) == 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.alea_gpu_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

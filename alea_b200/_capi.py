@@ -127,6 +127,21 @@ class RunResult(ctypes.Structure):
                 ("n_evaluations", ctypes.c_int64)]
 
 
+class Job(ctypes.Structure):
+    _fields_ = [("system", ctypes.POINTER(System)), ("positions", c_dp), ("n_walkers", ctypes.c_int),
+                ("mode", ctypes.c_int), ("run", RunConfig)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("result", RunResult), ("queue_ms", ctypes.c_double),
+                ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("footprint_bytes", ctypes.c_size_t)]
+
+
+JOB_VMC, JOB_DMC = 0, 1
+ERR_TIMEOUT, ERR_NOMEM, ERR_CANCELLED = 5, 6, 7
+
+
 EXPORTS = [
     "alea_gpu_abi_version", "alea_gpu_create", "alea_gpu_destroy", "alea_gpu_last_error",
     "alea_gpu_upload_walkers", "alea_gpu_evaluate", "alea_gpu_num_walkers",
@@ -134,10 +149,13 @@ EXPORTS = [
     "alea_gpu_vmc_step", "alea_gpu_dmc_advance", "alea_gpu_dmc_branch", "alea_gpu_vmc_run",
     "alea_gpu_dmc_run", "alea_gpu_last_kernel_ms", "alea_gpu_stream", "alea_gpu_transfer_bytes",
     "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc", "alea_gpu_download_phase",
-    "alea_gpu_setup_heg2d", "alea_gpu_setup_crystal2d", "alea_gpu_setup_exciton2d",
+    "alea_gpu_setup_heg2d", "alea_gpu_setup_heg2d_twisted", "alea_gpu_setup_crystal2d",
+    "alea_gpu_setup_exciton2d",
     "alea_gpu_setup_charges2d", "alea_gpu_setup_dipoles2d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
     "alea_gpu_setup_free",
+    "alea_gpu_server_create", "alea_gpu_submit_job", "alea_gpu_poll", "alea_gpu_cancel",
+    "alea_gpu_server_destroy", "alea_gpu_server_last_error",
 ]
 
 _LIB = None
@@ -178,6 +196,8 @@ def load() -> ctypes.CDLL:
         "alea_gpu_transfer_bytes": ([P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)], I),
         "alea_gpu_setup_heg2d": ([I, I, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
                                   ctypes.c_size_t], I),
+        "alea_gpu_setup_heg2d_twisted": ([I, I, D, D, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
+                                          ctypes.c_size_t], I),
         "alea_gpu_setup_crystal2d": ([I, I, D, D, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p,
                                       ctypes.c_size_t], I),
         "alea_gpu_setup_exciton2d": ([D, ctypes.POINTER(P)], I),
@@ -188,6 +208,12 @@ def load() -> ctypes.CDLL:
         "alea_gpu_setup_json": ([P], ctypes.c_char_p),
         "alea_gpu_setup_positions": ([P, ctypes.c_uint64, I, c_dp], I),
         "alea_gpu_setup_free": ([P], None),
+        "alea_gpu_server_create": ([I, ctypes.c_size_t, I, ctypes.POINTER(P)], I),
+        "alea_gpu_submit_job": ([P, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)], I),
+        "alea_gpu_poll": ([P, ctypes.c_uint64, I, ctypes.POINTER(JobResult)], I),
+        "alea_gpu_cancel": ([P, ctypes.c_uint64], I),
+        "alea_gpu_server_destroy": ([P], I),
+        "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -11,6 +11,7 @@
 //   branching      src/population/walker_set.cpp:187-239
 //   spread         src/numerics/statistics.cpp:297-315
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -20,6 +21,7 @@
 #include <vector>
 
 #include "../../include/alea_gpu.h"
+#include "alea_internal.h"
 #include "alea_dev.cuh"
 #include "alea_kernels.h"
 
@@ -27,7 +29,7 @@ using namespace alea_gpu;
 
 namespace {
 
-std::string g_create_error;
+thread_local std::string g_create_error;   // per host thread, as the ABI reads it
 
 // ───────────────────────── host random numbers ─────────────────────────
 
@@ -179,6 +181,7 @@ struct alea_gpu_ctx {
     uint64_t h2d = 0, d2h = 0;     // bytes copied host->device / device->host
     uint64_t launches = 0;         // kernels launched by this context
     double* noalloc_scratch = nullptr;   // device address of g_noalloc_scratch on `device`
+    const std::atomic<int>* cancel = nullptr;   // a server's cancel flag, read between steps
 };
 
 namespace {
@@ -1520,6 +1523,8 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
         std::vector<double> blk(T, 0.0);
         std::vector<int64_t> blk_n(T, 0);
         for (int st = 0; st < cfg->n_steps; ++st) {
+            if (c->cancel && c->cancel->load(std::memory_order_relaxed))
+                return fail(c, ALEA_ERR_CANCELLED, "cancelled");
             alea_gpu_step_stats s{};
             if (int rc = alea_gpu_vmc_step(c, &prm, &s)) return rc;
             all_moves += s.n_proposed;
@@ -1608,6 +1613,8 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
         if (b == cfg->n_equilibration_blocks) eref_sum = eref_wsum = 0.0;
         double blk_e = 0.0, blk_w = 0.0;
         for (int st = 0; st < cfg->n_steps; ++st) {
+            if (c->cancel && c->cancel->load(std::memory_order_relaxed))
+                return fail(c, ALEA_ERR_CANCELLED, "cancelled");
             alea_gpu_dmc_params prm{tau, cfg->n_substeps, etrial, eref, e_cut, e_max};
             alea_gpu_step_stats s{};
             if (int rc = alea_gpu_dmc_advance(c, &prm, &s)) return rc;
@@ -1652,3 +1659,43 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
 }
 
 }  // extern "C"
+
+// ───────────────────────── internal: serving support ───────────────────
+
+namespace alea_gpu {
+
+void set_cancel_flag(alea_gpu_ctx* c, const std::atomic<int>* flag) {
+    if (c) c->cancel = flag;
+}
+
+// Device bytes a context of `capacity` walkers of `sys` will hold, from the
+// record layout of build_system (hot part, orbital rows, image sums), both
+// record buffers, staging, one sweep's randoms per substep and the pair list.
+size_t footprint_bytes(const alea_gpu_system* sys, int capacity, int n_substeps) {
+    if (!sys || capacity < 1) return 0;
+    const long np = sys->n_particles;
+    bool cplx = false;
+    for (int b = 0; b < sys->n_blocks; ++b) cplx |= sys->blocks[b].type == ALEA_ORB_TWISTED_PLANE_WAVE;
+    long rec = 14 * np + S_NSCAL + (cplx ? 4 * np : 0);
+    for (int b = 0; b < sys->n_blocks; ++b) {
+        const long n = sys->blocks[b].last - sys->blocks[b].first;
+        rec += (cplx ? 2 : 1) * round4(n * n) + round4(n);
+        if (!cplx) rec += round4(n * n) + 2 * round4(2 * n * n);
+    }
+    for (int d = 0; d < sys->n_backflow; ++d) {
+        const long n = sys->backflow[d].last - sys->backflow[d].first;
+        rec += round4(2 * n) + round4(n * n) + round4(2 * n) + 4;
+    }
+    long nk = 0;
+    for (int t = 0; t < sys->n_terms; ++t) nk = std::max<long>(nk, sys->terms[t].kset.n_k);
+    rec += 2L * sys->n_groups * nk;
+    rec = round4(rec);
+    const size_t cap = static_cast<size_t>(capacity);
+    size_t bytes = 2 * cap * static_cast<size_t>(rec) * 8;
+    bytes += cap * static_cast<size_t>(std::max<long>(2 * np, 8)) * 8 + cap * 5;
+    bytes += static_cast<size_t>(std::max(n_substeps, 1)) * static_cast<size_t>(np) * 3 * cap * 8;
+    bytes += static_cast<size_t>(np) * static_cast<size_t>(np) * 4 + (1u << 20);
+    return bytes;
+}
+
+}  // namespace alea_gpu

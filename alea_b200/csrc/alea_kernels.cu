@@ -4,6 +4,7 @@
 // functions they call are in alea_walker.cuh.
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "alea_walker.cuh"
 
@@ -210,7 +211,17 @@ __global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, in
         else KERNEL<128><<<(grid), 128, (smem), (st)>>>(__VA_ARGS__);                    \
     } while (0)
 
+// The dynamic shared-memory cap is a property of each kernel function, shared
+// by every context on the device: it only ever grows, under a lock, so that
+// contexts of different systems created on different threads (a server's
+// workers) never lower it beneath a launch in flight.
 cudaError_t reserve_smem(size_t smem) {
+    static std::mutex mu;
+    static size_t reserved[64] = {};   // per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (smem <= reserved[dev]) return cudaSuccess;
     const int b = static_cast<int>(smem);
     const void* kernels[] = {
         reinterpret_cast<const void*>(evaluate_kernel<32>), reinterpret_cast<const void*>(measure_kernel<32>),
@@ -223,7 +234,9 @@ cudaError_t reserve_smem(size_t smem) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
         if (e != cudaSuccess) return e;
     }
-    return reserve_smem_fast(smem);
+    const cudaError_t e = reserve_smem_fast(smem);
+    if (e == cudaSuccess) reserved[dev] = smem;
+    return e;
 }
 
 cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,

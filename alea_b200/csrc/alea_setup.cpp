@@ -17,6 +17,8 @@
 // long-range part's transform vanishes above k_cut (lattice shells up to
 // k_continuum, the 2-D density of states (A/2π) k dk beyond).
 #include <algorithm>
+#include <mutex>
+#include <map>
 #include <atomic>
 #include <cmath>
 #include <complex>
@@ -620,6 +622,43 @@ void plane_wave_shells(const Cell& c, int want, std::vector<double>& k, std::vec
     is_sin.resize(want);
 }
 
+// The n lowest |k + θ| of the reciprocal lattice at twist θ = t_x b1 + t_y b2
+// (TwistedPlaneWaveOrbitalSet's occupation, complex_orbital_set.h:278-343):
+// enumerate the |i|, |j| <= M box, sort by |q|², grow M until every q with
+// |q| <= M h_min - |θ| is in the box, and refuse a twist at which the n-th
+// orbital splits a degenerate shell.  q holds (q_x, q_y) per orbital.
+void twisted_shells(const Cell& c, int n, double tx, double ty, std::vector<double>& q) {
+    const double* b = c.b;
+    const double th[2] = {tx * b[0] + ty * b[2], tx * b[1] + ty * b[3]};
+    const double th_norm = std::hypot(th[0], th[1]);
+    const double area = std::abs(b[0] * b[3] - b[1] * b[2]);
+    const double h_min = area / std::max(std::hypot(b[0], b[1]), std::hypot(b[2], b[3]));
+    struct Q { double q2, x, y; };
+    for (int M = 4; M <= 4096; M *= 2) {
+        std::vector<Q> qs;
+        for (int i = -M; i <= M; ++i)
+            for (int j = -M; j <= M; ++j) {
+                const double x = i * b[0] + j * b[2] + th[0];
+                const double y = i * b[1] + j * b[3] + th[1];
+                qs.push_back({x * x + y * y, x, y});
+            }
+        if (qs.size() <= static_cast<size_t>(n)) continue;
+        std::stable_sort(qs.begin(), qs.end(), [](const Q& a, const Q& z) { return a.q2 < z.q2; });
+        const double r_safe = M * h_min - th_norm;
+        if (r_safe <= 0.0 || qs[n].q2 > r_safe * r_safe) continue;
+        if (n > 0 && std::abs(qs[n].q2 - qs[n - 1].q2) <= 1e-9 * (1.0 + qs[n].q2))
+            throw std::invalid_argument("twisted plane waves: " + std::to_string(n) +
+                                        " orbitals split a degenerate |k+theta| shell at this twist");
+        q.clear();
+        for (int k = 0; k < n; ++k) {
+            q.push_back(qs[k].x);
+            q.push_back(qs[k].y);
+        }
+        return;
+    }
+    throw std::invalid_argument("twisted plane waves: enumeration did not converge");
+}
+
 // ───────────────────────── JSON ─────────────────────────────────────────
 
 struct Json {
@@ -709,7 +748,19 @@ void set_kset(alea_gpu_setup* S, alea_gpu_kset& ks, const Breakup& br) {
 }
 
 // Coulomb 1/(ε r) Ewald tables (n_knots auto-tuned, default k set).
-Breakup ewald_breakup(const Cell& c, double tol) {
+// Breakups depend only on the cell and the radial function's parameters;
+// builders of the same cell (twists of one electron gas, say) reuse them.
+std::mutex g_breakup_mu;
+std::map<std::vector<double>, Breakup> g_breakups;
+std::map<std::vector<double>, double> g_breakup_uinf;
+
+std::vector<double> breakup_key(const Cell& c, double kind, std::initializer_list<double> extra) {
+    std::vector<double> key{kind, c.a[0], c.a[1], c.a[2], c.a[3]};
+    key.insert(key.end(), extra.begin(), extra.end());
+    return key;
+}
+
+Breakup ewald_breakup_uncached(const Cell& c, double tol) {
     Radial f;
     f.value = [](double r) { return 1.0 / r; };
     f.fourier = [](double k) { return kTwoPi / k; };
@@ -725,16 +776,44 @@ Breakup ewald_breakup(const Cell& c, double tol) {
     throw std::runtime_error("ewald: the breakup did not reach the requested tolerance");
 }
 
+Breakup ewald_breakup(const Cell& c, double tol) {
+    const std::vector<double> key = breakup_key(c, 0.0, {tol});
+    {
+        std::lock_guard<std::mutex> lk(g_breakup_mu);
+        auto it = g_breakups.find(key);
+        if (it != g_breakups.end()) return it->second;
+    }
+    Breakup br = ewald_breakup_uncached(c, tol);
+    std::lock_guard<std::mutex> lk(g_breakup_mu);
+    g_breakups[key] = br;
+    return br;
+}
+
 // Image-summed Padé tables (the Jastrow breakup options).
 Breakup pade_breakup(const Cell& c, const std::vector<double>& a, const std::vector<double>& b,
                      double& u_inf) {
+    std::vector<double> key = breakup_key(c, 1.0, {static_cast<double>(a.size())});
+    key.insert(key.end(), a.begin(), a.end());
+    key.insert(key.end(), b.begin(), b.end());
+    {
+        std::lock_guard<std::mutex> lk(g_breakup_mu);
+        auto it = g_breakups.find(key);
+        if (it != g_breakups.end()) {
+            u_inf = g_breakup_uinf[key];
+            return it->second;
+        }
+    }
     const Radial f = pade_radial(a, b, c.ws, u_inf);
     BreakupOptions opt;
     opt.k_continuum = 20.0 * kPi / c.ws;
     opt.k_max = 300.0 / c.ws;
     opt.n_continuum = 150;
     opt.k_cut = 5.0 * std::min(std::hypot(c.b[0], c.b[1]), std::hypot(c.b[2], c.b[3]));
-    return build_breakup(c.b, c.area, c.ws, f, opt);
+    Breakup br = build_breakup(c.b, c.area, c.ws, f, opt);
+    std::lock_guard<std::mutex> lk(g_breakup_mu);
+    g_breakups[key] = br;
+    g_breakup_uinf[key] = u_inf;
+    return br;
 }
 
 void json_spline(Json& j, const std::string& k, const alea_gpu_spline& sp) {
@@ -791,6 +870,9 @@ void write_json(alea_gpu_setup* S, const std::string& kind, double ewald_self, d
             j.ks("type", "plane_wave");
             j.arr("k", std::vector<double>(B.k, B.k + 2 * n));
             j.arr("is_sin", std::vector<int>(B.is_sin, B.is_sin + n));
+        } else if (B.type == ALEA_ORB_TWISTED_PLANE_WAVE) {
+            j.ks("type", "twisted_plane_wave");
+            j.arr("q", std::vector<double>(B.k, B.k + 2 * n));
         } else {
             j.ks("type", "gaussian");
             j.arr("centers", std::vector<double>(B.centers, B.centers + 2 * n));
@@ -937,8 +1019,8 @@ void alea_gpu_setup_free(alea_gpu_setup* s) { delete s; }
 // determinants per spin, image-summed Padé u = a₁ r/(1 + b r) on every spin
 // pair (a₁ from the Kato cusp, or `pade_a` when positive for the opposite
 // spins and half of it for equal spins), Ewald Coulomb.
-int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pade_a,
-                         double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len) {
+static int setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pade_a, double tx, double ty,
+                       double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len) {
     if (!out) return ALEA_ERR_INVALID;
     *out = nullptr;
     auto* S = new alea_gpu_setup();
@@ -954,16 +1036,25 @@ int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double 
         std::copy(c.a, c.a + 4, y.lattice);
         add_group(y, 0, n_up, -1.0);
         if (n_down > 0) add_group(y, n_up, n_down, -1.0);
+        // an integer twist is Γ: the real closed-shell determinant
+        const bool twisted = std::abs(tx - std::nearbyint(tx)) >= 1e-12 || std::abs(ty - std::nearbyint(ty)) >= 1e-12;
         for (int g = 0; g < y.n_groups; ++g) {
             std::vector<double> k;
             std::vector<int> is_sin;
-            plane_wave_shells(c, y.groups[g].last - y.groups[g].first, k, is_sin);
+            const int n = y.groups[g].last - y.groups[g].first;
             alea_gpu_orbitals& B = y.blocks[y.n_blocks++];
             B.first = y.groups[g].first;
             B.last = y.groups[g].last;
-            B.type = ALEA_ORB_PLANE_WAVE;
-            B.k = S->keep(k);
-            B.is_sin = S->keepi(is_sin);
+            if (twisted) {
+                twisted_shells(c, n, tx, ty, k);
+                B.type = ALEA_ORB_TWISTED_PLANE_WAVE;
+                B.k = S->keep(k);
+            } else {
+                plane_wave_shells(c, n, k, is_sin);
+                B.type = ALEA_ORB_PLANE_WAVE;
+                B.k = S->keep(k);
+                B.is_sin = S->keepi(is_sin);
+            }
         }
         double self = 0.0, bg = 0.0;
         add_ewald(S, c, ewald_tol > 0.0 ? ewald_tol : 1e-6, self, bg);
@@ -1012,6 +1103,17 @@ int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double 
     }
     *out = S;
     return ALEA_OK;
+}
+
+int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pade_a,
+                         double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len) {
+    return setup_heg2d(n_up, n_down, rs, pade_b, pade_a, 0.0, 0.0, ewald_tol, out, err, err_len);
+}
+
+int alea_gpu_setup_heg2d_twisted(int n_up, int n_down, double rs, double pade_b, double pade_a,
+                                 double twist_x, double twist_y, double ewald_tol, alea_gpu_setup** out,
+                                 char* err, size_t err_len) {
+    return setup_heg2d(n_up, n_down, rs, pade_b, pade_a, twist_x, twist_y, ewald_tol, out, err, err_len);
 }
 
 // 2-D Wigner crystal: a triangular lattice of nx × ny sites (ny even) in the

@@ -61,6 +61,14 @@ def heg2d(n_up: int, n_down: int, rs: float, pade_b: float = 0.3, pade_a: float 
     return _make("alea_gpu_setup_heg2d", n_up, n_down, rs, pade_b, pade_a, ewald_tol)
 
 
+def heg2d_twisted(n_up: int, n_down: int, rs: float, twist, pade_b: float = 0.3, pade_a: float = 0.0,
+                  ewald_tol: float = 1e-6) -> Setup:
+    """2-D electron gas at a twist (t_x, t_y) in units of the reciprocal
+    vectors: twisted plane waves, complex determinant (real at an integer twist)."""
+    return _make("alea_gpu_setup_heg2d_twisted", n_up, n_down, rs, pade_b, pade_a, float(twist[0]),
+                 float(twist[1]), ewald_tol)
+
+
 def crystal2d(nx: int, ny: int, rs: float, gauss_c: float = 0.1, alpha0: float = 0.0,
               cutoff_frac: float = 0.999, jitter: float = 0.0, ewald_tol: float = 1e-6) -> Setup:
     """2-D Wigner crystal (triangular sites, Gaussians, Drummond, Ewald)."""

@@ -64,6 +64,11 @@ def parse():
     ap.add_argument("--cpu-walkers", type=int, default=1024,
                     help="walker sample of the host-CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving mix instead of the DMC step: Poisson VMC jobs through alea_gpu_server")
+    ap.add_argument("--serve-jobs", type=int, default=60)
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="arrivals per second")
+    ap.add_argument("--serve-slots", type=int, default=8, help="jobs running at once")
     return ap.parse_args()
 
 
@@ -423,6 +428,94 @@ def gpu_arm(a):
     return 0
 
 
+# ───────────────────────── serving mix ──────────────────────────────────
+
+SERVE_SAMPLES = 1 << 20          # electron moves per job
+SERVE_WALKERS = 256
+TWIST_GRID = [(i + 0.5) / 4.0 for i in range(4)]
+
+
+def serve_arm(a):
+    """The serving mix of the workload list: VMC jobs of 2^20 moves each,
+    arriving Poisson at --serve-rate, drawn uniformly from the 2-D electron gas
+    (N = 26, 42, 58, 90 at rs = 30, 40, 60, each at one of the 4x4 offset
+    twists that does not split a shell: complex determinants) and 2-D dipolar
+    bosons (N = 256, C/r^3, zero-energy Jastrow).  Every job runs through
+    alea_gpu_submit_job / alea_gpu_poll on one server; latency is submission
+    to completion.  One JSON line: aggregate moves/s, p50/p99 latency."""
+    import torch
+    import alea_b200
+    from alea_b200 import setup as S
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    rng = np.random.default_rng(a.seed)
+    catalog = []
+    for n in (13, 21, 29, 45):
+        for rs in (30.0, 40.0, 60.0):
+            for t in [(x, y) for x in TWIST_GRID for y in TWIST_GRID]:
+                catalog.append(("heg", n, rs, t))
+    catalog.append(("dipoles", 256, 0.0353, None))
+    picks, setups = [], {}
+    while len(picks) < a.serve_jobs:
+        kind, n, rs, t = catalog[rng.integers(len(catalog))]
+        key = (kind, n, rs, t)
+        if key not in setups:
+            try:
+                setups[key] = (S.heg2d_twisted(n, n, rs, t) if kind == "heg"
+                               else S.dipoles2d(n, rs, 1.0, 3.0, 0.0459))
+            except ValueError:       # this twist splits a shell at this N: not a valid job
+                setups[key] = None
+        if setups[key] is not None:
+            picks.append(key)
+    jobs = []
+    for i, key in enumerate(picks):
+        kind, n, rs, t = key
+        st = setups[key]
+        np_tot = st.desc["np"]
+        sweeps = -(-SERVE_SAMPLES // (SERVE_WALKERS * np_tot))
+        n_acc = 4
+        steps = -(-sweeps // (n_acc + 1))
+        tau = (0.5 * rs) ** 2 if kind == "heg" else 0.0003
+        pos = st.positions(a.seed + i, SERVE_WALKERS)
+        jobs.append((st, pos, steps, n_acc, tau, key))
+    arrivals = np.cumsum(rng.exponential(1.0 / a.serve_rate, size=len(jobs)))
+    srv = alea_b200.Server(max_running=a.serve_slots)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ids = []
+    for (st, pos, steps, n_acc, tau, key), t_arr in zip(jobs, arrivals):
+        delay = t0 + t_arr - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(st.desc, pos, 0, 1, n_acc, steps, 1, tau, seed=a.seed + len(ids)))
+    results = [srv.poll(i, timeout_ms=600000) for i in ids]
+    wall = time.perf_counter() - t0
+    srv.close()
+    ok = [r for r in results if r is not None and r.status == 0]
+    lat = np.array([r.latency_ms for r in ok])
+    moves = float(sum(r.result.n_moves for r in ok))
+    kinds = {}
+    for (st, pos, steps, n_acc, tau, key), r in zip(jobs, results):
+        label = f"heg N={2 * key[1]} rs={key[2]:g}" if key[0] == "heg" else "dipoles N=256"
+        kinds.setdefault(label, []).append(r.latency_ms if r is not None else None)
+    line = {
+        "metric": "serving: aggregate electron-moves/s, p50/p99 job latency", "value": moves / wall,
+        "unit": "moves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic: seeded uniform walkers per job, Poisson arrivals",
+        "config": {"workload": "serving mix: VMC jobs of 2^20 moves, 256 walkers, 2-D electron gas "
+                               "N in {26,42,58,90} x rs in {30,40,60} x 4x4 offset twists (complex) "
+                               "and 2-D dipolar bosons N=256",
+                   "jobs": len(jobs), "arrival_rate_per_s": a.serve_rate, "slots": a.serve_slots},
+        "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+        "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+        "mean_queue_ms": float(np.mean([r.queue_ms for r in ok])) if ok else None,
+        "completed": len(ok), "wall_s": wall,
+        "latency_by_kind_ms": {k: float(np.median([x for x in v if x is not None])) for k, v in kinds.items()},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def ctypes_ptr(t, _capi):
     import ctypes
     return ctypes.cast(ctypes.c_void_p(t.data_ptr()), _capi.c_dp)
@@ -432,6 +525,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         return reference_arm(a)
+    if a.serve:
+        return serve_arm(a)
     return gpu_arm(a)
 
 

@@ -53,7 +53,8 @@ enum {
     ALEA_ERR_UNSUPPORTED = 3,  /* valid, but outside what the kernels implement */
     ALEA_ERR_SINGULAR = 4,     /* a determinant became singular or nonfinite */
     ALEA_ERR_TIMEOUT = 5,      /* a bounded device wait ran out */
-    ALEA_ERR_NOMEM = 6         /* device allocation failed / capacity exceeded */
+    ALEA_ERR_NOMEM = 6,        /* device allocation failed / capacity exceeded */
+    ALEA_ERR_CANCELLED = 7     /* a served job was cancelled (alea_gpu_cancel) */
 };
 
 enum { ALEA_ORB_PLANE_WAVE = 0, ALEA_ORB_GAUSSIAN = 1, ALEA_ORB_TWISTED_PLANE_WAVE = 2 };
@@ -372,6 +373,15 @@ typedef struct alea_gpu_setup alea_gpu_setup;
  * Ewald tolerance ewald_tol (<= 0: 1e-6).  err receives a message on failure. */
 int alea_gpu_setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pade_a,
                          double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len);
+/* The same electron gas at twist (twist_x, twist_y) in units of the
+ * reciprocal vectors: twisted plane waves e^{i(k+θ)·r} filling the n lowest
+ * |k + θ| per spin, a complex determinant (fixed-phase DMC); an integer twist
+ * is Γ and gives the real determinant above.  ALEA_ERR_INVALID when a spin's
+ * count splits a degenerate |k + θ| shell (builders/slater.cpp:244-262,
+ * wavefunction/complex_orbital_set.h:278-343). */
+int alea_gpu_setup_heg2d_twisted(int n_up, int n_down, double rs, double pade_b, double pade_a,
+                                 double twist_x, double twist_y, double ewald_tol, alea_gpu_setup** out,
+                                 char* err, size_t err_len);
 /* 2-D Wigner crystal of nx × ny triangular sites (ny even), Gaussian
  * orbitals exp(-(gauss_c / rs²) |r - R|²), Drummond Jastrows with alpha0 and
  * cutoff cutoff_frac × the Wigner-Seitz radius (<= 0: 0.999), initial
@@ -398,6 +408,62 @@ const char* alea_gpu_setup_json(const alea_gpu_setup* s);
  * (src/qmc/app.cpp:56-112): one mt19937_64 seeded with `seed`. */
 int alea_gpu_setup_positions(const alea_gpu_setup* s, uint64_t seed, int nw, double* positions);
 void alea_gpu_setup_free(alea_gpu_setup* s);
+
+/* ───────────────────────── serving ─────────────────────────────────────
+ *
+ * No reference counterpart: the reference runs one input file per process.
+ * A server takes VMC / DMC jobs that differ in system, walkers and length,
+ * keeps each admitted job's walkers and inverses on the device in a context
+ * of its own (own CUDA stream, own random streams keyed by the job's seed),
+ * and runs up to max_running of them at once, so their kernels overlap on
+ * the device.  A job is admitted, in arrival order among those that fit,
+ * when its device footprint (≈ 2 × capacity × record bytes, the record being
+ * Σ_blocks 6 N_b² + 14 N + … doubles) fits the HBM budget left by the running
+ * ones; jobs that arrive while others run are admitted as slots and memory
+ * free up.  A job's result does not depend on what else runs: its arithmetic
+ * is that of alea_gpu_vmc_run / alea_gpu_dmc_run on its own context.
+ *
+ * Threads: any host thread may submit, poll or cancel; the server's worker
+ * threads own the contexts.  Borrowed pointers (system tables, positions)
+ * must stay valid until the job is done, failed or cancelled. */
+typedef struct alea_gpu_server alea_gpu_server;
+
+enum { ALEA_JOB_VMC = 0, ALEA_JOB_DMC = 1 };
+
+typedef struct {
+    const alea_gpu_system* system;   /* borrowed */
+    const double* positions;         /* AoS [w][p][d] initial walkers, borrowed */
+    int n_walkers;
+    int mode;                        /* ALEA_JOB_VMC or ALEA_JOB_DMC */
+    alea_gpu_run_config run;         /* as for alea_gpu_vmc_run / alea_gpu_dmc_run */
+} alea_gpu_job;
+
+typedef struct {
+    int status;                      /* ALEA_OK or the job's ALEA_ERR_* code */
+    alea_gpu_run_result result;
+    double queue_ms;                 /* submission to admission */
+    double run_ms;                   /* admission to completion */
+    double latency_ms;               /* submission to completion */
+    size_t footprint_bytes;          /* the admission estimate */
+} alea_gpu_job_result;
+
+/* hbm_budget_bytes = 0: 80% of the device memory free at creation;
+ * max_running >= 1 worker contexts. */
+int alea_gpu_server_create(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out);
+/* Queue a job; never blocks on the device.  ALEA_ERR_NOMEM when the job
+ * alone exceeds the budget. */
+int alea_gpu_submit_job(alea_gpu_server* s, const alea_gpu_job* job, uint64_t* job_id);
+/* Wait at most timeout_ms (0: do not wait) for a job: ALEA_OK with *out
+ * filled when it has finished (out->status tells how), ALEA_ERR_TIMEOUT when
+ * it is still queued or running, ALEA_ERR_INVALID for an unknown id.  A
+ * finished job's result stays readable until the server is destroyed. */
+int alea_gpu_poll(alea_gpu_server* s, uint64_t job_id, int timeout_ms, alea_gpu_job_result* out);
+/* Cancel a queued job at once, or a running one at its next step
+ * (status ALEA_ERR_CANCELLED); ALEA_ERR_INVALID for an unknown or finished id. */
+int alea_gpu_cancel(alea_gpu_server* s, uint64_t job_id);
+/* Cancel what is left, join the workers, free every context. */
+int alea_gpu_server_destroy(alea_gpu_server* s);
+const char* alea_gpu_server_last_error(const alea_gpu_server* s);
 
 #ifdef __cplusplus
 }

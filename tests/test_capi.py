@@ -41,12 +41,13 @@ def test_struct_layout_matches_header():
 #include <stdio.h>
 #include "alea_gpu.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(alea_gpu_system),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(alea_gpu_system),
          sizeof(alea_gpu_pair_term), sizeof(alea_gpu_orbitals), sizeof(alea_gpu_ewald),
          offsetof(alea_gpu_system, terms), offsetof(alea_gpu_system, ewald),
          offsetof(alea_gpu_system, coulomb), sizeof(alea_gpu_run_config),
          sizeof(alea_gpu_step_stats), sizeof(alea_gpu_run_result),
-         offsetof(alea_gpu_run_result, n_moves));
+         offsetof(alea_gpu_run_result, n_moves), sizeof(alea_gpu_job), offsetof(alea_gpu_job, run),
+         sizeof(alea_gpu_job_result), offsetof(alea_gpu_job_result, footprint_bytes));
   return 0;
 }
 """
@@ -60,7 +61,8 @@ int main(void) {
             ctypes.sizeof(_capi.Ewald), _capi.System.terms.offset, _capi.System.ewald.offset,
             _capi.System.coulomb.offset, ctypes.sizeof(_capi.RunConfig),
             ctypes.sizeof(_capi.StepStats), ctypes.sizeof(_capi.RunResult),
-            _capi.RunResult.n_moves.offset]
+            _capi.RunResult.n_moves.offset, ctypes.sizeof(_capi.Job), _capi.Job.run.offset,
+            ctypes.sizeof(_capi.JobResult), _capi.JobResult.footprint_bytes.offset]
     assert got == want
 
 
