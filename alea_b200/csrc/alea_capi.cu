@@ -12,6 +12,7 @@
 //   spread         src/numerics/statistics.cpp:297-315
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -200,6 +201,22 @@ int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
     } while (0)
 
 long round4(long x) { return (x + 3) & ~3L; }
+
+// The device's default memory pool keeps what contexts free (no release at
+// synchronisation points), so the next context's allocations are served from
+// it.  A setting of this process's runtime, not of the GPU.
+void keep_pool_warm(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    done[device] = true;
+}
 
 // e^x K0(x), e^x K1(x) on the host: the ascending series for x <= 2 (DLMF
 // 10.31.1-2), the standard library's K_nu times e^x up to x = 30, and the
@@ -866,8 +883,9 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         return fail(c, ALEA_ERR_UNSUPPORTED,
                     "walker state needs " + std::to_string(c->smem) + " bytes of shared memory (> 227 KB)");
     // upload the arena and patch pointers
-    CUDA_TRY(c, cudaMalloc(&c->arena, std::max<size_t>(ar.bytes.size(), 256)));
-    CUDA_TRY(c, cudaMemcpy(c->arena, ar.bytes.data(), ar.bytes.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMallocAsync(&c->arena, std::max<size_t>(ar.bytes.size(), 256), c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->arena, ar.bytes.data(), ar.bytes.size(), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));   // ar.bytes is freed on return
     for (const Patch& p : patches) *p.slot = static_cast<char*>(c->arena) + p.off;
     for (int t : ze_terms) s.terms[t].ze_cheb = bessel_dev;
     return ALEA_OK;
@@ -875,9 +893,9 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
 
 int ensure_streams(alea_gpu_ctx* c, int n) {
     if (n > c->streams_cap) {
-        if (c->streams) cudaFree(c->streams);
+        if (c->streams) cudaFreeAsync(c->streams, c->stream);
         c->streams = nullptr;
-        CUDA_TRY(c, cudaMalloc(&c->streams, sizeof(uint64_t) * 4 * static_cast<size_t>(n)));
+        CUDA_TRY(c, cudaMallocAsync(&c->streams, sizeof(uint64_t) * 4 * static_cast<size_t>(n), c->stream));
         c->streams_cap = n;
     }
     return ALEA_OK;
@@ -885,10 +903,10 @@ int ensure_streams(alea_gpu_ctx* c, int n) {
 
 int ensure_randoms(alea_gpu_ctx* c, int sweeps) {
     if (sweeps > c->rnd_sweeps) {
-        if (c->randoms) cudaFree(c->randoms);
+        if (c->randoms) cudaFreeAsync(c->randoms, c->stream);
         c->randoms = nullptr;
         const size_t n = static_cast<size_t>(sweeps) * c->sys.np * 3 * c->capacity;
-        CUDA_TRY(c, cudaMalloc(&c->randoms, n * 8));
+        CUDA_TRY(c, cudaMallocAsync(&c->randoms, n * 8, c->stream));
         c->rnd_sweeps = sweeps;
     }
     return ALEA_OK;
@@ -1060,29 +1078,38 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
         c->err = "cudaSetDevice failed";
         return bail(ALEA_ERR_CUDA);
     }
+    // Device memory is stream-ordered (cudaMallocAsync on the context's own
+    // stream, from the device's pool kept warm), so creating or destroying a
+    // context never waits for other contexts' work on the device.
+    keep_pool_warm(device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        c->err = "cudaStreamCreate failed";
+        return bail(ALEA_ERR_CUDA);
+    }
     if (int rc = build_system(c, sys)) return bail(rc);
     const DevSys& s = c->sys;
     const size_t recb = static_cast<size_t>(s.rec) * 8 * capacity;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&c->rec[0], recb) != cudaSuccess || cudaMalloc(&c->rec[1], recb) != cudaSuccess ||
-        cudaMalloc(&c->d_buf, static_cast<size_t>(std::max(s.np * 2, 8)) * 8 * capacity) != cudaSuccess ||
-        cudaMalloc(&c->d_sigma, static_cast<size_t>(s.np) * 2 * 8) != cudaSuccess ||
-        cudaMalloc(&c->d_src, sizeof(int) * static_cast<size_t>(capacity)) != cudaSuccess ||
-        cudaMalloc(&c->d_mask, static_cast<size_t>(capacity)) != cudaSuccess ||
+    cudaStream_t st = c->stream;
+    if (cudaMallocAsync(&c->rec[0], recb, st) != cudaSuccess || cudaMallocAsync(&c->rec[1], recb, st) != cudaSuccess ||
+        cudaMallocAsync(&c->d_buf, static_cast<size_t>(std::max(s.np * 2, 8)) * 8 * capacity, st) != cudaSuccess ||
+        cudaMallocAsync(&c->d_sigma, static_cast<size_t>(s.np) * 2 * 8, st) != cudaSuccess ||
+        cudaMallocAsync(&c->d_src, sizeof(int) * static_cast<size_t>(capacity), st) != cudaSuccess ||
+        cudaMallocAsync(&c->d_mask, static_cast<size_t>(capacity), st) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         c->err = "device allocation failed";
         return bail(ALEA_ERR_NOMEM);
     }
-    cudaMemset(c->rec[0], 0, recb);
-    cudaMemset(c->rec[1], 0, recb);
+    cudaMemsetAsync(c->rec[0], 0, recb, st);
+    cudaMemsetAsync(c->rec[1], 0, recb, st);
     // pair list i < j for the Ewald real-space sum
     std::vector<int2> pl;
     for (int i = 0; i < s.np; ++i)
         for (int j = i + 1; j < s.np; ++j) pl.push_back(make_int2(i, j));
     c->npair = static_cast<int>(pl.size());
     if (c->npair > 0) {
-        if (cudaMalloc(&c->pairs, pl.size() * sizeof(int2)) != cudaSuccess ||
-            cudaMemcpy(c->pairs, pl.data(), pl.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        if (cudaMallocAsync(&c->pairs, pl.size() * sizeof(int2), st) != cudaSuccess ||
+            cudaMemcpyAsync(c->pairs, pl.data(), pl.size() * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
             c->err = "device allocation failed";
             return bail(ALEA_ERR_NOMEM);
         }
@@ -1098,12 +1125,12 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
 
 int alea_gpu_destroy(alea_gpu_ctx* c) {
     if (!c) return ALEA_OK;
-    if (c->stream) cudaStreamSynchronize(c->stream);
     for (void* p : {static_cast<void*>(c->arena), static_cast<void*>(c->rec[0]), static_cast<void*>(c->rec[1]),
                     static_cast<void*>(c->randoms), static_cast<void*>(c->streams), static_cast<void*>(c->pairs),
                     static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
                     static_cast<void*>(c->d_mask)})
-        if (p) cudaFree(p);
+        if (p && c->stream) cudaFreeAsync(p, c->stream);
+    if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);

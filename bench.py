@@ -431,7 +431,7 @@ def gpu_arm(a):
 # ───────────────────────── serving mix ──────────────────────────────────
 
 SERVE_SAMPLES = 1 << 20          # electron moves per job
-SERVE_WALKERS = 256
+SERVE_WALKERS = 1024
 TWIST_GRID = [(i + 0.5) / 4.0 for i in range(4)]
 
 
@@ -502,7 +502,7 @@ def serve_arm(a):
         "metric": "serving: aggregate electron-moves/s, p50/p99 job latency", "value": moves / wall,
         "unit": "moves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
         "data": "synthetic: seeded uniform walkers per job, Poisson arrivals",
-        "config": {"workload": "serving mix: VMC jobs of 2^20 moves, 256 walkers, 2-D electron gas "
+        "config": {"workload": "serving mix: VMC jobs of 2^20 moves, 1024 walkers, 2-D electron gas "
                                "N in {26,42,58,90} x rs in {30,40,60} x 4x4 offset twists (complex) "
                                "and 2-D dipolar bosons N=256",
                    "jobs": len(jobs), "arrival_rate_per_s": a.serve_rate, "slots": a.serve_slots},
