@@ -226,6 +226,11 @@ class Walkers:
         except Exception:
             pass
 
+    def set_precision(self, precision: str) -> None:
+        """'fp64' (the drop-in) or 'fp32' (the FP32 form of the sweeps)."""
+        code = {"fp64": _capi.PRECISION_FP64, "fp32": _capi.PRECISION_FP32}[precision]
+        self._check(self.lib.alea_gpu_set_precision(self.ctx, code))
+
     def _check(self, rc: int):
         if rc != 0:
             raise AleaGpuError(rc, self.lib.alea_gpu_last_error(self.ctx).decode())

@@ -139,6 +139,7 @@ class JobResult(ctypes.Structure):
 
 
 JOB_VMC, JOB_DMC = 0, 1
+PRECISION_FP64, PRECISION_FP32 = 0, 1
 ERR_TIMEOUT, ERR_NOMEM, ERR_CANCELLED = 5, 6, 7
 
 
@@ -154,6 +155,7 @@ EXPORTS = [
     "alea_gpu_setup_charges2d", "alea_gpu_setup_dipoles2d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
     "alea_gpu_setup_free",
+    "alea_gpu_set_precision",
     "alea_gpu_server_create", "alea_gpu_submit_job", "alea_gpu_poll", "alea_gpu_cancel",
     "alea_gpu_server_destroy", "alea_gpu_server_last_error",
 ]
@@ -208,6 +210,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_setup_json": ([P], ctypes.c_char_p),
         "alea_gpu_setup_positions": ([P, ctypes.c_uint64, I, c_dp], I),
         "alea_gpu_setup_free": ([P], None),
+        "alea_gpu_set_precision": ([P, I], I),
         "alea_gpu_server_create": ([I, ctypes.c_size_t, I, ctypes.POINTER(P)], I),
         "alea_gpu_submit_job": ([P, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)], I),
         "alea_gpu_poll": ([P, ctypes.c_uint64, I, ctypes.POINTER(JobResult)], I),

@@ -1249,6 +1249,8 @@ int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_ps
 int alea_gpu_move(alea_gpu_ctx* c, int p, const double* new_pos, const uint8_t* accept, double* log_ratio,
                   double* phase, double* new_grad, double* new_lap) {
     if (!c || !new_pos) return ALEA_ERR_INVALID;
+    if (c->sys.f32)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "single moves run in FP64: set the precision back to FP64 first");
     const DevSys& s = c->sys;
     if (p < 0 || p >= s.np) return fail(c, ALEA_ERR_INVALID, "particle index out of range");
     cudaSetDevice(c->device);
@@ -1281,10 +1283,27 @@ int alea_gpu_move(alea_gpu_ctx* c, int p, const double* new_pos, const uint8_t* 
     return accept ? check_errors(c) : ALEA_OK;
 }
 
+int alea_gpu_set_precision(alea_gpu_ctx* c, int precision) {
+    if (!c) return ALEA_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (precision == ALEA_PRECISION_FP32) {
+        if (c->nt != 32 || !f32_sweep_eligible(c->sys))
+            return fail(c, ALEA_ERR_UNSUPPORTED,
+                        "the FP32 form takes real determinants and Pade/Drummond pair terms of at most 64 particles");
+        c->sys.f32 = 1;
+        return ALEA_OK;
+    }
+    if (precision != ALEA_PRECISION_FP64) return fail(c, ALEA_ERR_INVALID, "precision must be FP64 or FP32");
+    if (!c->sys.f32) return ALEA_OK;
+    c->sys.f32 = 0;
+    return c->nw > 0 ? launch_evaluate(c) : ALEA_OK;   // FP64 inverses and orbital rows again
+}
+
 int alea_gpu_measure(alea_gpu_ctx* c) {
     if (!c) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->nw == 0) return ALEA_OK;
+    if (c->sys.f32) return launch_evaluate(c);   // the FP32 form keeps no orbital rows to refresh from
     ++c->launches;
     CUDA_TRY(c, launch_measure(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));

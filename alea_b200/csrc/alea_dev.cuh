@@ -146,6 +146,7 @@ struct DevSys {
     // k-space tables)
     int f_pos, f_jg, f_jl, f_scal, f_nval, f_ngrad, f_nlap, f_col, f_rowp, f_misc, f_work, f_cn,
         f_sn, f_co, f_so, f_sg, f_sl, f_kg, f_kl, f_elwork, f_total;
+    int f32;                  // sweeps run the FP32 form (alea_gpu_set_precision)
     // ziggurat tables
     const uint64_t* zk;
     const double *zw, *zf;

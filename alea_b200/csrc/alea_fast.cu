@@ -26,307 +26,9 @@
 // same totals and takes the accept decision itself, so a move has no block
 // barrier.  The orbital rows of the next particle are fetched from HBM while
 // the current move runs, and a sweep's random numbers are read once per lane.
-#include "alea_walker.cuh"
+#include "alea_warp.cuh"
 
 namespace alea_gpu {
-
-namespace {
-
-// k-space contribution of one k to the gradient/Laplacian of a particle with
-// phase (c, sn) that sees the density (pr, pi) (kspace_pair_sum.cpp:76-97).
-__device__ __forceinline__ void kterm_r(double kx, double ky, double w, double c, double sn, double pr,
-                                        double pi, double self, double* acc) {
-    const double g = 2.0 * w * (c * pi - sn * pr);
-    const double l = 2.0 * w * (self - (c * pr + sn * pi));
-    acc[0] += kx * g;
-    acc[1] += ky * g;
-    acc[2] += kx * kx * l;
-    acc[3] += ky * ky * l;
-}
-
-// Orbital rows ∇D, ∇²D of particle p (its block's row), lane slot j = column
-// l + 32j; nothing for a particle outside every determinant.
-template <int S>
-__device__ __forceinline__ void fetch_rows(const DevSys& s, const double* grec, int p, double2 (&dg)[S],
-                                           double2 (&dl)[S]) {
-    const int b = block_of(s, p);
-    if (b < 0) return;
-    const DevBlock& B = s.blocks[b];
-    const int N = B.n, kr = p - B.first;
-    const double2* rg = reinterpret_cast<const double2*>(grec + B.oDg) + kr * N;
-    const double2* rl = reinterpret_cast<const double2*>(grec + B.oDl) + kr * N;
-#pragma unroll
-    for (int j = 0; j < S; ++j) {
-        const int m = static_cast<int>(threadIdx.x) + 32 * j;
-        if (m < N) {
-            dg[j] = __ldcg(rg + m);
-            dl[j] = __ldcg(rl + m);
-        }
-    }
-}
-
-// Orbital i of a real block at (x, y): value, gradient, diagonal second
-// derivatives (plane waves, orbital_set.h:436-474; Gaussians, :185-224).
-__device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int i, double x, double y,
-                                         double& val, double& gx, double& gy, double& lx, double& ly) {
-    if (B.type == 0) {
-        const double k0 = B.k[i * 2], k1 = B.k[i * 2 + 1];
-        double sn, c;
-        sincos(fma(k1, y, k0 * x), &sn, &c);
-        if (B.is_sin[i] != 0.0) {
-            val = sn;
-            gx = k0 * c;
-            gy = k1 * c;
-            lx = -k0 * k0 * sn;
-            ly = -k1 * k1 * sn;
-        } else {
-            val = c;
-            gx = -k0 * sn;
-            gy = -k1 * sn;
-            lx = -k0 * k0 * c;
-            ly = -k1 * k1 * c;
-        }
-    } else {
-        const double alpha = B.alphas[i];
-        double dx = x - B.centers[i * 2], dy = y - B.centers[i * 2 + 1];
-        min_image2(s, dx, dy);
-        const double phi = exp(-alpha * fma(dy, dy, dx * dx));
-        val = phi;
-        gx = phi * (-2.0 * alpha * dx);
-        gy = phi * (-2.0 * alpha * dy);
-        lx = phi * (4.0 * alpha * alpha * dx * dx - 2.0 * alpha);
-        ly = phi * (4.0 * alpha * alpha * dy * dy - 2.0 * alpha);
-    }
-}
-
-// A = D⁻¹ of an N x N block by pivoted Gauss-Jordan on one warp (first
-// maximum |pivot| of each column, as rebuild_inverse): lane l owns columns
-// l + 32j of the work copy m of D and of A.  The pivot is found with the
-// warp's integer max/min reductions on the bits of |x| (order-preserving for
-// non-negative doubles; NaNs never win, ties go to the lowest row) and its
-// value is broadcast from the lane that holds it, so no lane reads column k
-// while its owner swaps rows.  Leaves log|det D| in misc[M_LOGDET] and flags
-// a zero or nonfinite pivot in misc[M_ERR].
-template <int S>
-__device__ __forceinline__ void gj_rebuild_warp(double* A, double* m, double* col, const double* D, int N,
-                                                double* misc) {
-    const int lane = threadIdx.x;
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < S; ++j) {
-        const int c = lane + 32 * j;
-        if (c >= N) continue;
-        for (int r0 = 0; r0 < N; r0 += 8) {
-            double t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = (r0 + u < N) ? __ldcg(D + (r0 + u) * N + c) : 0.0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int r = r0 + u;
-                if (r < N) {
-                    m[r * N + c] = t[u];
-                    A[r * N + c] = (r == c) ? 1.0 : 0.0;
-                }
-            }
-        }
-    }
-    __syncwarp();
-    double pivots[S];
-#pragma unroll
-    for (int j = 0; j < S; ++j) pivots[j] = 1.0;
-    bool bad = false;
-    for (int k = 0; k < N; ++k) {
-        unsigned long long key = 0ull;
-        int br = N;
-        double bv = 0.0;
-        for (int r = k + lane; r < N; r += 32) {
-            const double x = m[r * N + k];
-            const unsigned long long kx =
-                isnan(x) ? 0ull : static_cast<unsigned long long>(__double_as_longlong(fabs(x))) + 1ull;
-            if (kx > key) {
-                key = kx;
-                br = r;
-                bv = x;
-            }
-        }
-        const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
-        const unsigned mhi = __reduce_max_sync(kAllLanes, hi);
-        const unsigned mlo = __reduce_max_sync(kAllLanes, hi == mhi ? lo : 0u);
-        const bool cand = hi == mhi && lo == mlo;
-        const unsigned prow = __reduce_min_sync(kAllLanes, cand ? static_cast<unsigned>(br) : 0xffffffffu);
-        const bool none = mhi == 0u && mlo == 0u;   // a column of NaNs has no pivot: flagged below
-        const int piv = none ? k : static_cast<int>(prow);
-        const unsigned owner = __ffs(__ballot_sync(kAllLanes, cand && br == piv && !none));
-        double diag = __shfl_sync(kAllLanes, bv, owner ? owner - 1 : 0);
-        if (none) diag = 0.0;
-        bad |= diag == 0.0 || !isfinite(diag);
-#pragma unroll
-        for (int j = 0; j < S; ++j)
-            if ((k >> 5) == j && lane == (k & 31)) pivots[j] = diag;
-        double pk[S], ak[S];
-#pragma unroll
-        for (int j = 0; j < S; ++j) {
-            const int c = lane + 32 * j;
-            pk[j] = ak[j] = 0.0;
-            if (c >= N) continue;
-            const double mk = m[k * N + c], mp = m[piv * N + c];
-            const double xk = A[k * N + c], xp = A[piv * N + c];
-            if (piv != k) {
-                m[piv * N + c] = mk;
-                A[piv * N + c] = xk;
-            }
-            pk[j] = (piv != k ? mp : mk) / diag;
-            ak[j] = (piv != k ? xp : xk) / diag;
-            m[k * N + c] = pk[j];
-            A[k * N + c] = ak[j];
-        }
-        __syncwarp();
-        for (int r = lane; r < N; r += 32) col[r] = m[r * N + k];
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < S; ++j) {
-            const int c = lane + 32 * j;
-            if (c >= N) continue;
-            for (int r0 = 0; r0 < N; r0 += 4) {
-                double f[4], x[4], y[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int r = r0 + u;
-                    const bool on = r < N && r != k;
-                    f[u] = on ? col[r] : 0.0;
-                    x[u] = on ? m[r * N + c] : 0.0;
-                    y[u] = on ? A[r * N + c] : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int r = r0 + u;
-                    if (r < N && r != k) {
-                        m[r * N + c] = x[u] - f[u] * pk[j];
-                        A[r * N + c] = y[u] - f[u] * ak[j];
-                    }
-                }
-            }
-        }
-        __syncwarp();
-    }
-    double logdet = 0.0;
-#pragma unroll
-    for (int j = 0; j < S; ++j)
-        if (lane + 32 * j < N) logdet += log(fabs(pivots[j]));
-    logdet = warp_sum(logdet);
-    if (lane == 0) {
-        misc[M_LOGDET] = logdet;
-        if (bad) misc[M_ERR] = 1.0;
-    }
-    __syncwarp();
-}
-
-// Shared-memory view of the one-warp layout (DevSys f_*).  The sg, sl, kg,
-// kl planes exist only in the local-energy phase (el = true), on top of the
-// move scratch; `work` is the move union or the local energy's tables.
-__device__ __forceinline__ Smem view_fast(const DevSys& s, double* sm, bool el) {
-    Smem v{};
-    v.pos = sm + s.f_pos;
-    v.jg = sm + s.f_jg;
-    v.jl = sm + s.f_jl;
-    v.scal = sm + s.f_scal;
-    v.rho = v.scal - s.o_scal + s.o_rho;
-    v.nval = sm + s.f_nval;
-    v.ngrad = sm + s.f_ngrad;
-    v.nlap = sm + s.f_nlap;
-    v.col = sm + s.f_col;
-    v.rowp = sm + s.f_rowp;
-    v.misc = sm + s.f_misc;
-    v.cn = sm + s.f_cn;
-    v.sn = sm + s.f_sn;
-    v.co = sm + s.f_co;
-    v.so = sm + s.f_so;
-    v.work = sm + (el ? s.f_elwork : s.f_work);
-    if (el) {
-        v.sg = sm + s.f_sg;
-        v.sl = sm + s.f_sl;
-        v.kg = sm + s.f_kg;
-        v.kl = sm + s.f_kl;
-    }
-    return v;
-}
-
-// n doubles (n even, both ends 16-byte aligned) between a record (global,
-// through L2 only: records stream through) and shared memory, by the warp.
-__device__ __forceinline__ void copy_in_warp(double* dst, const double* src, int n) {
-    const double2* s2 = reinterpret_cast<const double2*>(src);
-    double2* d2 = reinterpret_cast<double2*>(dst);
-    for (int i = threadIdx.x; i < n / 2; i += 32) d2[i] = __ldcg(s2 + i);
-}
-
-__device__ __forceinline__ void copy_out_warp(double* dst, const double* src, int n) {
-    const double2* s2 = reinterpret_cast<const double2*>(src);
-    double2* d2 = reinterpret_cast<double2*>(dst);
-    for (int i = threadIdx.x; i < n / 2; i += 32) __stcg(d2 + i, s2[i]);
-}
-
-// The record's positions, pair-Jastrow planes and [scalars, end of the hot
-// part) into the one-warp layout, and back.
-__device__ __forceinline__ void load_fast(const DevSys& s, const double* rec, double* sm) {
-    const int n2 = 2 * s.np;
-    copy_in_warp(sm + s.f_pos, rec + s.o_pos, n2);
-    copy_in_warp(sm + s.f_jg, rec + s.o_jg, n2);
-    copy_in_warp(sm + s.f_jl, rec + s.o_jl, n2);
-    copy_in_warp(sm + s.f_scal, rec + s.o_scal, s.hot - s.o_scal);
-    __syncwarp();
-}
-
-__device__ __forceinline__ void store_fast(const DevSys& s, double* rec, const double* sm) {
-    __syncwarp();
-    const int n2 = 2 * s.np;
-    copy_out_warp(rec + s.o_pos, sm + s.f_pos, n2);
-    copy_out_warp(rec + s.o_jg, sm + s.f_jg, n2);
-    copy_out_warp(rec + s.o_jl, sm + s.f_jl, n2);
-    copy_out_warp(rec + s.o_scal, sm + s.f_scal, s.hot - s.o_scal);
-    copy_out_warp(rec + s.o_sg, sm + s.f_sg, n2);
-    copy_out_warp(rec + s.o_sl, sm + s.f_sl, n2);
-    copy_out_warp(rec + s.o_kg, sm + s.f_kg, n2);
-    copy_out_warp(rec + s.o_kl, sm + s.f_kl, n2);
-}
-
-// The local energy after a sweep: every particle's derivatives refreshed
-// into the local-energy planes (zero for particles outside every determinant
-// or image sum, as in the record), then kinetic + Ewald + open pair
-// potentials.  Out of line: once per sweep.
-template <int S>
-__device__ __noinline__ double local_energy_warp(const DevSys& s, double* sm, const double* grec,
-                                                 const int2* pairs, int npair) {
-    const Smem v = view_fast(s, sm, true);
-    __syncwarp();
-    for (int i = threadIdx.x; i < 2 * s.np; i += 32) v.sg[i] = v.sl[i] = v.kg[i] = v.kl[i] = 0.0;
-    __syncwarp();
-    refresh_all<32, S>(s, v, grec);
-    return local_energy<32, S>(s, v, pairs, npair);
-}
-
-// A pair term's u, u', u'' for the one-warp sweep: without zero-energy terms
-// (ZE = false) only the inline Padé/Drummond forms are compiled, so the
-// move's pair stage makes no function call.
-template <bool ZE>
-__device__ __forceinline__ void radial_w(const DevTerm& T, double r, double& u, double& du, double& d2u) {
-    if constexpr (ZE)
-        radial(T, r, u, du, d2u);
-    else
-        radial_pd(T, r, u, du, d2u);
-}
-
-// Select slot p >> 5 of a per-lane register array and read it from lane
-// p & 31 (warp-uniform result).
-template <int S, class T>
-__device__ __forceinline__ T from_owner(const T (&x)[S], int p) {
-    T mine = x[0];
-#pragma unroll
-    for (int j = 1; j < S; ++j)
-        if ((p >> 5) == j) mine = x[j];
-    return __shfl_sync(kAllLanes, mine, p & 31);
-}
-
-}  // namespace
 
 template <int S, bool ZE>
 __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,

@@ -234,7 +234,8 @@ cudaError_t reserve_smem(size_t smem) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
         if (e != cudaSuccess) return e;
     }
-    const cudaError_t e = reserve_smem_fast(smem);
+    cudaError_t e = reserve_smem_fast(smem);
+    if (e == cudaSuccess) e = reserve_smem_f32(smem);
     if (e == cudaSuccess) reserved[dev] = smem;
     return e;
 }
@@ -261,6 +262,8 @@ cudaError_t launch_move(int nt, int nw, size_t smem, cudaStream_t st, const DevS
 cudaError_t launch_sweep(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
                          double* records, const double* randoms, long stride,
                          const SweepParams& prm, const int2* pairs, int npair) {
+    if (s.f32)   // the FP32 form keeps no FP64 orbital rows: no other sweep may run on its records
+        return launch_sweep_f32(nw, st, s, records, randoms, stride, prm, pairs, npair);
     if (nt == 32 && fast_sweep_eligible(s)) {
         const char* e = std::getenv("ALEA_GPU_SWEEP");
         if (e == nullptr || std::strcmp(e, "generic") != 0)

@@ -39,6 +39,13 @@ cudaError_t reserve_smem_fast(size_t smem);
 cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
                               const double* randoms, long stride, const SweepParams& prm, const int2* pairs,
                               int npair);
+// The FP32 form of the one-warp sweep (alea_fast32.cu), for the one-warp
+// sweep's systems without zero-energy terms; launch_sweep takes it whenever
+// DevSys::f32 is set.
+bool f32_sweep_eligible(const DevSys& s);
+cudaError_t reserve_smem_f32(size_t smem);
+cudaError_t launch_sweep_f32(int nw, cudaStream_t st, const DevSys& s, double* records, const double* randoms,
+                             long stride, const SweepParams& prm, const int2* pairs, int npair);
 __global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
                             int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
                             double zr, double* out, int crowd_mode);

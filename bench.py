@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--cpu-walkers", type=int, default=1024,
                     help="walker sample of the host-CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--serve", action="store_true",
                     help="serving mix instead of the DMC step: Poisson VMC jobs through alea_gpu_server")
     ap.add_argument("--serve-jobs", type=int, default=60)
@@ -332,12 +333,14 @@ def gpu_arm(a):
     moves = evals = 0
     sweep_ms = []
     sweep_walkers = []
+    energies = []
     for _ in range(a.steps):
         st, ms = loop.step()
         moves += st.n_proposed
         evals += st.n_walkers
         sweep_ms.append(ms)
         sweep_walkers.append(st.n_walkers)
+        energies.append(st.energy_sum / st.weight_sum)
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = g.launch_count() - l0
@@ -357,6 +360,43 @@ def gpu_arm(a):
     achieved = bytes_alg / t_sweep / 1e9
     per_walker = profiled_traffic_per_walker()
     traffic = per_walker * float(np.mean(sweep_walkers)) if per_walker else None
+
+    # ── the FP32 form on the same start: throughput and energy against FP64 ──
+    fp32 = None
+    if not a.no_fp32:
+        f = alea_b200.Walkers(desc, capacity=2 * nw + 2, device=local)
+        f.upload(setup.positions(seed, nw))
+        f.set_precision("fp32")
+        if a.pre > 0:
+            f.vmc_run(0, 1, a.pre, 1, VMC_TAU, nw, seed)
+        floop = DmcLoop(f, nw, seed)
+        for _ in range(a.warmup):
+            floop.step()
+        fstream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
+        torch.cuda.synchronize()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(fstream)
+        fmoves, fms, fen = 0, [], []
+        for _ in range(a.steps):
+            fst, fstep_ms = floop.step()
+            fmoves += fst.n_proposed
+            fms.append(fstep_ms)
+            fen.append(fst.energy_sum / fst.weight_sum)
+        f1.record(fstream)
+        torch.cuda.synchronize()
+        barrier()
+        fms_max = allreduce(f0.elapsed_time(f1), dist.ReduceOp.MAX if world > 1 else None)
+        fmoves_all = allreduce(float(fmoves), dist.ReduceOp.SUM if world > 1 else None)
+        e64, e32 = float(np.mean(energies)), float(np.mean(fen))
+        err = float(np.sqrt(np.var(energies) / max(len(energies) - 1, 1) + np.var(fen) / max(len(fen) - 1, 1)))
+        fp32 = {"value": fmoves_all / (fms_max * 1e-3), "unit": UNIT, "ms_per_step": fms_max / a.steps,
+                "sweep_ms_per_launch": float(np.mean(fms)),
+                "energy_per_particle": e32 / NP, "energy_per_particle_fp64": e64 / NP,
+                "bias_per_particle": (e32 - e64) / NP, "bias_error_per_particle": err / NP,
+                "note": "independent FP32 and FP64 walks from the same start, mean of the timed "
+                        "steps' mixed estimators; error from the step-to-step scatter"}
+        f.close()
 
     # ── end to end through the C ABI from pinned host buffers ──
     lib = _capi.load()
@@ -420,6 +460,7 @@ def gpu_arm(a):
             "gpu_launches": int(launches_all),
             "clocks": clk,
             "population": int(g.nw),
+            "fp32": fp32,
         }
         print(json.dumps(line), flush=True)
     g.close()

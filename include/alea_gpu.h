@@ -409,6 +409,23 @@ const char* alea_gpu_setup_json(const alea_gpu_setup* s);
 int alea_gpu_setup_positions(const alea_gpu_setup* s, uint64_t seed, int nw, double* positions);
 void alea_gpu_setup_free(alea_gpu_setup* s);
 
+/* ───────────────────────── precision ───────────────────────────────────
+ *
+ * No reference counterpart (the reference is FP64 throughout).  FP64 is the
+ * drop-in.  ALEA_PRECISION_FP32 makes the sweep entry points (vmc_step,
+ * dmc_advance, the runs, the allocation-free step) run the FP32 form: the
+ * inverses, orbitals, ratios, rank-one updates, pair-Jastrow radial terms and
+ * image-sum terms of every move in FP32 (angles reduced in FP64, sums in
+ * FP64); positions, the Jastrow gradient planes, ρ(k), the inverse
+ * recomputation every 64 updates (rows recomputed in FP64, Gauss-Jordan in
+ * FP64), log|det|, the local energy and the DMC weights in FP64.  For
+ * real plane-wave determinants with Padé or Drummond pair terms, ≤ 64
+ * particles (the electron gases); ALEA_ERR_UNSUPPORTED otherwise.  The FP32 form keeps no FP64
+ * orbital rows, so meanwhile alea_gpu_measure re-evaluates the walkers and
+ * alea_gpu_move is refused; setting FP64 again re-evaluates them. */
+enum { ALEA_PRECISION_FP64 = 0, ALEA_PRECISION_FP32 = 1 };
+int alea_gpu_set_precision(alea_gpu_ctx* ctx, int precision);
+
 /* ───────────────────────── serving ─────────────────────────────────────
  *
  * No reference counterpart: the reference runs one input file per process.
