@@ -77,18 +77,23 @@ __device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int
     }
 }
 
-// A = D⁻¹ of an N x N block by pivoted Gauss-Jordan on one warp (first
-// maximum |pivot| of each column, as rebuild_inverse): lane l owns columns
-// l + 32j of the work copy m of D and of A.  The pivot is found with the
-// warp's integer max/min reductions on the bits of |x| (order-preserving for
+// A = D⁻¹ of an N x N block by pivoted Gauss-Jordan on one warp, in place:
+// D is loaded into A's own storage and inverted there (the reference's pivot
+// rule, first maximum |pivot| of each column, on the same column values as
+// the augmented [D | I] form of rebuild_inverse; the row exchanges are undone
+// as column exchanges at the end).  Lane l owns columns l + 32j for the
+// row scaling and the elimination.  The pivot is found with the warp's
+// integer max/min reductions on the bits of |x| (order-preserving for
 // non-negative doubles; NaNs never win, ties go to the lowest row) and its
 // value is broadcast from the lane that holds it, so no lane reads column k
-// while its owner swaps rows.  Leaves log|det D| in misc[M_LOGDET] and flags
-// a zero or nonfinite pivot in misc[M_ERR].
+// while its owner swaps rows; row k is scaled by one reciprocal.  `mult`
+// (N doubles) and `perm` (N ints) are scratch.  Leaves log|det D| in
+// misc[M_LOGDET] and flags a zero or nonfinite pivot in misc[M_ERR].
 template <int S>
-__device__ __forceinline__ void gj_rebuild_warp(double* A, double* m, double* col, const double* D, int N,
-                                                double* misc) {
+__device__ __forceinline__ void gj_rebuild_warp(double* A, double* mult, double* perm_area, const double* D,
+                                                int N, double* misc) {
     const int lane = threadIdx.x;
+    int* perm = reinterpret_cast<int*>(perm_area);
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < S; ++j) {
@@ -99,13 +104,8 @@ __device__ __forceinline__ void gj_rebuild_warp(double* A, double* m, double* co
 #pragma unroll
             for (int u = 0; u < 8; ++u) t[u] = (r0 + u < N) ? __ldcg(D + (r0 + u) * N + c) : 0.0;
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int r = r0 + u;
-                if (r < N) {
-                    m[r * N + c] = t[u];
-                    A[r * N + c] = (r == c) ? 1.0 : 0.0;
-                }
-            }
+            for (int u = 0; u < 8; ++u)
+                if (r0 + u < N) A[(r0 + u) * N + c] = t[u];
         }
     }
     __syncwarp();
@@ -118,7 +118,7 @@ __device__ __forceinline__ void gj_rebuild_warp(double* A, double* m, double* co
         int br = N;
         double bv = 0.0;
         for (int r = k + lane; r < N; r += 32) {
-            const double x = m[r * N + k];
+            const double x = A[r * N + k];
             const unsigned long long kx =
                 isnan(x) ? 0ull : static_cast<unsigned long long>(__double_as_longlong(fabs(x))) + 1ull;
             if (kx > key) {
@@ -141,50 +141,58 @@ __device__ __forceinline__ void gj_rebuild_warp(double* A, double* m, double* co
 #pragma unroll
         for (int j = 0; j < S; ++j)
             if ((k >> 5) == j && lane == (k & 31)) pivots[j] = diag;
-        double pk[S], ak[S];
+        const double inv = __drcp_rn(diag);
+        // exchange rows k and piv; scale row k (its pivot entry becomes 1/diag)
+        double pk[S];
 #pragma unroll
         for (int j = 0; j < S; ++j) {
             const int c = lane + 32 * j;
-            pk[j] = ak[j] = 0.0;
+            pk[j] = 0.0;
             if (c >= N) continue;
-            const double mk = m[k * N + c], mp = m[piv * N + c];
             const double xk = A[k * N + c], xp = A[piv * N + c];
-            if (piv != k) {
-                m[piv * N + c] = mk;
-                A[piv * N + c] = xk;
-            }
-            pk[j] = (piv != k ? mp : mk) / diag;
-            ak[j] = (piv != k ? xp : xk) / diag;
-            m[k * N + c] = pk[j];
-            A[k * N + c] = ak[j];
+            if (piv != k) A[piv * N + c] = xk;
+            pk[j] = (c == k ? 1.0 : (piv != k ? xp : xk)) * inv;
+            A[k * N + c] = pk[j];
         }
+        if (lane == 0) perm[k] = piv;
         __syncwarp();
-        for (int r = lane; r < N; r += 32) col[r] = m[r * N + k];
+        // multipliers: column k of the other rows, which then starts from 0
+        for (int r = lane; r < N; r += 32) {
+            mult[r] = r == k ? 0.0 : A[r * N + k];
+            if (r != k) A[r * N + k] = 0.0;
+        }
         __syncwarp();
 #pragma unroll
         for (int j = 0; j < S; ++j) {
             const int c = lane + 32 * j;
             if (c >= N) continue;
             for (int r0 = 0; r0 < N; r0 += 4) {
-                double f[4], x[4], y[4];
+                double f[4], y[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int r = r0 + u;
                     const bool on = r < N && r != k;
-                    f[u] = on ? col[r] : 0.0;
-                    x[u] = on ? m[r * N + c] : 0.0;
+                    f[u] = on ? mult[r] : 0.0;
                     y[u] = on ? A[r * N + c] : 0.0;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int r = r0 + u;
-                    if (r < N && r != k) {
-                        m[r * N + c] = x[u] - f[u] * pk[j];
-                        A[r * N + c] = y[u] - f[u] * ak[j];
-                    }
+                    if (r < N && r != k) A[r * N + c] = y[u] - f[u] * pk[j];
                 }
             }
         }
+        __syncwarp();
+    }
+    // undo the row exchanges as column exchanges, last first
+    for (int k = N - 1; k >= 0; --k) {
+        const int pk = perm[k];
+        if (pk != k)
+            for (int r = lane; r < N; r += 32) {
+                const double t = A[r * N + k];
+                A[r * N + k] = A[r * N + pk];
+                A[r * N + pk] = t;
+            }
         __syncwarp();
     }
     double logdet = 0.0;
