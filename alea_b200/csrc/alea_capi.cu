@@ -836,7 +836,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     for (int d = 0; d < s.nbf; ++d) work = std::max(work, 4L * s.bf[d].n * s.bf[d].n + 8L * s.bf[d].n);
     work = std::max(work, 2L * s.enk);
     work = std::max(work, static_cast<long>(np) * 10);
-    work = std::max(work, 3L * s.ngroups * s.nkJ);   // one-warp k-space refresh: E_g(k), S_g(k)
+    work = std::max(work, 2L * s.ngroups * s.nkJ);   // one-warp k-space refresh: E_g(k)
     s.s_work = take(work);
     s.s_rad = s.s_work;
     s.s_total = static_cast<int>(m);
@@ -863,21 +863,24 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         s.f_col = ftake(s.maxN);
         s.f_rowp = ftake(s.maxN);
         s.f_work = static_cast<int>(f);
+        // the move union: the partners' and phases' changes (the FP64 sweep
+        // inverts in place); the FP32 form's FP64 rebuild also needs N² there
         const long changes = round4(4L * np) + 4 * round4(std::max(s.nkJ, 1));
         s.f_cn = s.f_work + static_cast<int>(round4(4L * np));
         s.f_sn = s.f_cn + static_cast<int>(round4(std::max(s.nkJ, 1)));
         s.f_co = s.f_sn + static_cast<int>(round4(std::max(s.nkJ, 1)));
         s.f_so = s.f_co + static_cast<int>(round4(std::max(s.nkJ, 1)));
-        f += std::max(round4(static_cast<long>(s.maxN) * s.maxN), changes);
-        const long moves_end = f;
+        const long moves_end = f + changes;
+        const long moves_end32 = f + std::max(round4(static_cast<long>(s.maxN) * s.maxN), changes);
         f = scratch;   // the local energy reuses the whole scratch area
         s.f_sg = ftake(np2);
         s.f_sl = ftake(np2);
         s.f_kg = ftake(np2);
         s.f_kl = ftake(np2);
         s.f_elwork = static_cast<int>(f);
-        f += round4(std::max({3L * s.ngroups * s.nkJ, 2L * s.enk, 1L}));
+        f += round4(std::max({2L * s.ngroups * s.nkJ, 2L * s.enk, 1L}));
         s.f_total = static_cast<int>(std::max(f, moves_end));
+        s.f_total32 = static_cast<int>(std::max(f, moves_end32));
     }
     if (c->smem > 227 * 1024)
         return fail(c, ALEA_ERR_UNSUPPORTED,

@@ -140,12 +140,13 @@ struct DevSys {
     // shared-memory layout of the one-warp sweep (doubles; f_total = 0 when a
     // system does not take it): positions and pair-Jastrow planes, the record
     // from the scalars to the end of the hot part, the misc slots, then one
-    // scratch area used by the moves (new orbital row, update vectors, and a union of the
-    // Gauss-Jordan work matrix with the partner and k-space changes) and,
-    // after the moves, by the local energy (sg, sl, kg, kl planes and the
-    // k-space tables)
+    // scratch area used by the moves (new orbital row, update vectors, and a
+    // union of the partner and k-space changes with, in the FP32 form, the
+    // FP64 rebuild's matrix) and, after the moves, by the local energy (sg,
+    // sl, kg, kl planes and the k-space tables)
     int f_pos, f_jg, f_jl, f_scal, f_nval, f_ngrad, f_nlap, f_col, f_rowp, f_misc, f_work, f_cn,
         f_sn, f_co, f_so, f_sg, f_sl, f_kg, f_kl, f_elwork, f_total;
+    int f_total32;            // the FP32 form's total: its FP64 rebuild needs N² in the move union
     int f32;                  // sweeps run the FP32 form (alea_gpu_set_precision)
     // ziggurat tables
     const uint64_t* zk;

@@ -211,10 +211,8 @@ __device__ void blocks_to_f64(const DevSys& s, const Smem& v) {
 
 // Full inverse recomputation of block b in FP64: the orbital rows at the
 // current positions (the moved particle's row at (mx, my)) into `m`, then
-// in-place Gauss-Jordan with the reference's pivot rule (first maximum
-// |pivot| of each column, found as in gj_rebuild_warp), the row exchanges
-// undone as column exchanges at the end; the inverse is rounded into the
-// FP32 block.  log|det| to misc[M_LOGDET], a bad pivot to misc[M_ERR]; the
+// the in-place warp Gauss-Jordan of the FP64 sweep (gj_invert_warp, the
+// reference's pivot rule); the inverse is rounded into the FP32 block.  log|det| to misc[M_LOGDET], a bad pivot to misc[M_ERR]; the
 // row sums of |inverse| come back as the lane's maximum.
 template <int S>
 __device__ double rebuild_f64(const DevSys& s, const Smem& v, int b, int moved, double mx, double my) {
@@ -223,7 +221,6 @@ __device__ double rebuild_f64(const DevSys& s, const Smem& v, int b, int moved, 
     const int lane = threadIdx.x;
     double* m = v.work;
     float* Af = reinterpret_cast<float*>(v.scal - s.o_scal + B.oA);
-    int* perm = reinterpret_cast<int*>(v.col);
     __syncwarp();
     for (int e = lane; e < N * N; e += 32) {
         const int r = e / N, c = e - r * N;
@@ -233,77 +230,7 @@ __device__ double rebuild_f64(const DevSys& s, const Smem& v, int b, int moved, 
         orbital2(s, B, c, x, y, val, gx, gy, lx, ly);
         m[e] = val;
     }
-    __syncwarp();
-    double logdet = 0.0;
-    bool bad = false;
-    for (int k = 0; k < N; ++k) {
-        unsigned long long key = 0ull;
-        int br = N;
-        double bv = 0.0;
-        for (int r = k + lane; r < N; r += 32) {
-            const double x = m[r * N + k];
-            const unsigned long long kx =
-                isnan(x) ? 0ull : static_cast<unsigned long long>(__double_as_longlong(fabs(x))) + 1ull;
-            if (kx > key) {
-                key = kx;
-                br = r;
-                bv = x;
-            }
-        }
-        const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
-        const unsigned mhi = __reduce_max_sync(kAllLanes, hi);
-        const unsigned mlo = __reduce_max_sync(kAllLanes, hi == mhi ? lo : 0u);
-        const bool cand = hi == mhi && lo == mlo;
-        const unsigned prow = __reduce_min_sync(kAllLanes, cand ? static_cast<unsigned>(br) : 0xffffffffu);
-        const bool none = mhi == 0u && mlo == 0u;
-        const int piv = none ? k : static_cast<int>(prow);
-        const unsigned owner = __ffs(__ballot_sync(kAllLanes, cand && br == piv && !none));
-        double diag = __shfl_sync(kAllLanes, bv, owner ? owner - 1 : 0);
-        if (none) diag = 0.0;
-        bad |= diag == 0.0 || !isfinite(diag);
-        if (lane == (k & 31)) logdet += log(fabs(diag));
-        const double inv = 1.0 / diag;
-        // exchange rows k and piv, then scale row k (its pivot becomes 1/diag)
-#pragma unroll
-        for (int j = 0; j < S; ++j) {
-            const int c = lane + 32 * j;
-            if (c >= N) continue;
-            const double xk = m[k * N + c], xp = m[piv * N + c];
-            if (piv != k) m[piv * N + c] = xk;
-            m[k * N + c] = (c == k ? 1.0 : (piv != k ? xp : xk)) * inv;
-        }
-        if (lane == 0) perm[k] = piv;
-        __syncwarp();
-        for (int r = lane; r < N; r += 32) {
-            v.rowp[r] = r == k ? 0.0 : m[r * N + k];   // multipliers (FP64 scratch)
-        }
-        __syncwarp();
-        for (int r = lane; r < N; r += 32)
-            if (r != k) m[r * N + k] = 0.0;
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < S; ++j) {
-            const int c = lane + 32 * j;
-            if (c >= N) continue;
-            const double pk = m[k * N + c];
-            for (int r = 0; r < N; ++r) {
-                if (r == k) continue;
-                m[r * N + c] -= v.rowp[r] * pk;
-            }
-        }
-        __syncwarp();
-    }
-    // undo the row exchanges as column exchanges, last first
-    for (int k = N - 1; k >= 0; --k) {
-        const int pk = perm[k];
-        if (pk != k)
-            for (int r = lane; r < N; r += 32) {
-                const double t = m[r * N + k];
-                m[r * N + k] = m[r * N + pk];
-                m[r * N + pk] = t;
-            }
-        __syncwarp();
-    }
+    gj_invert_warp<S>(m, v.rowp, v.col, N, v.misc);
     double rs = 0.0;
     for (int r = lane; r < N; r += 32) {
         double t = 0.0;
@@ -313,11 +240,6 @@ __device__ double rebuild_f64(const DevSys& s, const Smem& v, int b, int moved, 
             t += fabs(x);
         }
         rs = fmax(rs, t);
-    }
-    logdet = warp_sum(logdet);
-    if (lane == 0) {
-        v.misc[M_LOGDET] = logdet;
-        if (bad) v.misc[M_ERR] = 1.0;
     }
     __syncwarp();
     return rs;
@@ -899,7 +821,7 @@ cudaError_t reserve_smem_f32(size_t smem) {
 
 cudaError_t launch_sweep_f32(int nw, cudaStream_t st, const DevSys& s, double* records, const double* randoms,
                              long stride, const SweepParams& prm, const int2* pairs, int npair) {
-    sweep_f32_kernel<2><<<nw, 32, static_cast<size_t>(s.f_total) * 8, st>>>(s, records, nw, randoms, stride,
+    sweep_f32_kernel<2><<<nw, 32, static_cast<size_t>(s.f_total32) * 8, st>>>(s, records, nw, randoms, stride,
                                                                             prm, pairs, npair);
     return cudaGetLastError();
 }

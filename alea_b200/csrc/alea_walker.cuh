@@ -1055,15 +1055,16 @@ struct PhaseWalk {
 
 // k-space gradient and Laplacian of every particle (one warp): the image
 // terms' weights and the partner densities are folded per group into
-// E_g(k) = Σ_t w_t(k) ρ_{g'(t)}(k) and S_g(k) = Σ_{t same-group} w_t(k) in
-// `work`; lane slot i then walks the k list once with its own phase.
+// E_g(k) = Σ_t w_t(k) ρ_{g'(t)}(k) in `work`; the self weight
+// S_g(k) = Σ_{t same-group} w_t(k) is summed per lane from the weights.  Lane
+// slot i then walks the k list once with its own phase.
 template <int S>
 __device__ void kspace_refresh_warp(const DevSys& s, const Smem& v) {
     const int np = s.np, nk = s.nkJ, ng = s.ngroups;
-    double* E = v.work;   // [g][3][nk]: Re E, Im E, S
+    double* E = v.work;   // [g][2][nk]: Re E, Im E
     for (int e = threadIdx.x; e < ng * nk; e += 32) {
         const int g = e / nk, q = e - g * nk;
-        double er = 0.0, ei = 0.0, sw = 0.0;
+        double er = 0.0, ei = 0.0;
         for (int t = 0; t < s.nterms; ++t) {
             const DevTerm& T = s.terms[t];
             if (!T.image || !in_term(T, s.gfirst[g])) continue;
@@ -1072,21 +1073,24 @@ __device__ void kspace_refresh_warp(const DevSys& s, const Smem& v) {
             const double w = T.kw[q];
             er += w * v.rho[go * 2 * nk + q];
             ei += w * v.rho[go * 2 * nk + nk + q];
-            if (T.same0) sw += w;
         }
-        E[(g * 3 + 0) * nk + q] = er;
-        E[(g * 3 + 1) * nk + q] = ei;
-        E[(g * 3 + 2) * nk + q] = sw;
+        E[(g * 2 + 0) * nk + q] = er;
+        E[(g * 2 + 1) * nk + q] = ei;
     }
     __syncwarp();
     double th1[S], th2[S], e2r[S], e2i[S], c[S], sn[S], acc[S][4];
     int gi[S];
+    unsigned selfmask[S];   // same-group image terms of the slot's group: S_g(k) = Σ their w(k)
     bool on[S];
 #pragma unroll
     for (int j = 0; j < S; ++j) {
         const int i = threadIdx.x + 32 * j;
         on[j] = i < np && kspace_of(s, i);
         gi[j] = i < np ? s.group_of[i] : 0;
+        selfmask[j] = 0u;
+        for (int t = 0; t < s.nterms; ++t)
+            if (s.terms[t].image && s.terms[t].same0 && in_term(s.terms[t], s.gfirst[gi[j]]))
+                selfmask[j] |= 1u << t;
         const double x = i < np ? v.pos[i * 2] : 0.0, y = i < np ? v.pos[i * 2 + 1] : 0.0;
         th1[j] = s.recip[0] * x + s.recip[1] * y;
         th2[j] = s.recip[2] * x + s.recip[3] * y;
@@ -1102,8 +1106,10 @@ __device__ void kspace_refresh_warp(const DevSys& s, const Smem& v) {
 #pragma unroll
         for (int j = 0; j < S; ++j) {
             walk[j].next(m1, m2, th1[j], th2[j], e2r[j], e2i[j], c[j], sn[j]);
-            const double* Eg = E + gi[j] * 3 * nk;
-            const double er = Eg[q], ei = Eg[nk + q], sw = Eg[2 * nk + q];
+            const double* Eg = E + gi[j] * 2 * nk;
+            const double er = Eg[q], ei = Eg[nk + q];
+            double sw = 0.0;
+            for (unsigned bits = selfmask[j]; bits; bits &= bits - 1) sw += s.terms[__ffs(bits) - 1].kw[q];
             const double g = 2.0 * (c[j] * ei - sn[j] * er);
             const double l = 2.0 * (sw - (c[j] * er + sn[j] * ei));
             acc[j][0] += kx * g;

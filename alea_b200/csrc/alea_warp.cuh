@@ -90,24 +90,9 @@ __device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int
 // (N doubles) and `perm` (N ints) are scratch.  Leaves log|det D| in
 // misc[M_LOGDET] and flags a zero or nonfinite pivot in misc[M_ERR].
 template <int S>
-__device__ __forceinline__ void gj_rebuild_warp(double* A, double* mult, double* perm_area, const double* D,
-                                                int N, double* misc) {
+__device__ __forceinline__ void gj_invert_warp(double* A, double* mult, double* perm_area, int N, double* misc) {
     const int lane = threadIdx.x;
     int* perm = reinterpret_cast<int*>(perm_area);
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < S; ++j) {
-        const int c = lane + 32 * j;
-        if (c >= N) continue;
-        for (int r0 = 0; r0 < N; r0 += 8) {
-            double t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = (r0 + u < N) ? __ldcg(D + (r0 + u) * N + c) : 0.0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (r0 + u < N) A[(r0 + u) * N + c] = t[u];
-        }
-    }
     __syncwarp();
     double pivots[S];
 #pragma unroll
@@ -205,6 +190,29 @@ __device__ __forceinline__ void gj_rebuild_warp(double* A, double* mult, double*
         if (bad) misc[M_ERR] = 1.0;
     }
     __syncwarp();
+}
+
+// The same from the block's committed orbital rows D in the record: every
+// column's loads first, then the inversion in A's storage.
+template <int S>
+__device__ __forceinline__ void gj_rebuild_warp(double* A, double* mult, double* perm_area, const double* D,
+                                                int N, double* misc) {
+    const int lane = threadIdx.x;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const int c = lane + 32 * j;
+        if (c >= N) continue;
+        for (int r0 = 0; r0 < N; r0 += 8) {
+            double t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = (r0 + u < N) ? __ldcg(D + (r0 + u) * N + c) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (r0 + u < N) A[(r0 + u) * N + c] = t[u];
+        }
+    }
+    gj_invert_warp<S>(A, mult, perm_area, N, misc);
 }
 
 // Shared-memory view of the one-warp layout (DevSys f_*).  The sg, sl, kg,
