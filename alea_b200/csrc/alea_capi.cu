@@ -18,6 +18,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -178,6 +180,7 @@ struct alea_gpu_ctx {
     double last_ms = 0.0;
     std::vector<double> h_inv_mass;
     std::vector<double> h_w, h_el, h_ids, h_par, h_nacc, h_ncut;
+    double* h_stage = nullptr;     // pinned staging for the per-step scalar planes [8 * capacity]
     double next_id = 1.0;
     uint64_t h2d = 0, d2h = 0;     // bytes copied host->device / device->host
     uint64_t launches = 0;         // kernels launched by this context
@@ -201,6 +204,38 @@ int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
     } while (0)
 
 long round4(long x) { return (x + 3) & ~3L; }
+
+// Pinned host staging blocks, reused across contexts for the life of the
+// process: freeing pinned memory can synchronise the device, which would make
+// a finishing context wait for the others' work.
+std::mutex g_pinned_mu;
+std::multimap<size_t, void*> g_pinned_free;
+
+void* pinned_acquire(size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        auto it = g_pinned_free.lower_bound(bytes);
+        if (it != g_pinned_free.end()) {
+            void* p = it->second;
+            g_pinned_free.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    // round up so that blocks are reusable by contexts of similar size
+    size_t b = 1u << 16;
+    while (b < bytes) b <<= 1;
+    if (cudaMallocHost(&p, b) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void pinned_release(void* p, size_t bytes) {
+    if (!p) return;
+    size_t b = 1u << 16;
+    while (b < bytes) b <<= 1;
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free.emplace(b, p);
+}
 
 // The device's default memory pool keeps what contexts free (no release at
 // synchronisation points), so the next context's allocations are served from
@@ -939,14 +974,25 @@ int read_scalars(alea_gpu_ctx* c, int slot, std::vector<double>& out) {
     return ALEA_OK;
 }
 
-int write_scalars(alea_gpu_ctx* c, int slot, const std::vector<double>& in) {
-    if (c->nw == 0) return ALEA_OK;
-    CUDA_TRY(c, copy_in(c, c->d_buf, in.data(), 8 * c->nw));
-    ++c->launches;
-    from_soa_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
-                                                                c->sys.o_scal + slot, 1, c->d_buf);
-    CUDA_TRY(c, cudaGetLastError());
+// Several scalar slots of every walker in one transfer: plane k of `slots`
+// lands in out[k] (one copy and one synchronisation for all of them).
+int read_pack(alea_gpu_ctx* c, std::initializer_list<int> slots, std::initializer_list<std::vector<double>*> out) {
+    const int nw = c->nw;
+    int k = 0;
+    for (int slot : slots) {
+        ++c->launches;
+        scalar_kernel<<<(nw + 255) / 256, 256, 0, c->stream>>>(records(c), nw, c->sys.rec, c->sys.o_scal + slot,
+                                                                c->d_buf + static_cast<size_t>(k) * nw);
+        CUDA_TRY(c, cudaGetLastError());
+        ++k;
+    }
+    CUDA_TRY(c, copy_out(c, c->h_stage, c->d_buf, 8L * k * nw));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    k = 0;
+    for (std::vector<double>* v : out) {
+        v->assign(c->h_stage + static_cast<long>(k) * nw, c->h_stage + static_cast<long>(k + 1) * nw);
+        ++k;
+    }
     return ALEA_OK;
 }
 
@@ -970,7 +1016,7 @@ int launch_evaluate(alea_gpu_ctx* c) {
 
 // One sweep-kernel launch (VMC step or DMC advance) with its randoms.
 int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, double etrial, double eref,
-              double e_cut, double e_max) {
+              double e_cut, double e_max, bool check = true) {
     if (c->nw == 0) return ALEA_OK;
     if (c->n_streams < 1) return fail(c, ALEA_ERR_INVALID, "no random streams (alea_gpu_set_streams)");
     if (n_sub < 1) return fail(c, ALEA_ERR_INVALID, "n_substeps must be >= 1");
@@ -1002,7 +1048,7 @@ int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, doubl
     float ms = 0.f;
     CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     c->last_ms = ms;
-    return check_errors(c);
+    return check ? check_errors(c) : ALEA_OK;
 }
 
 // ───────────────────────── allocation-free VMC step ─────────────────────
@@ -1098,6 +1144,7 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
         cudaMallocAsync(&c->d_sigma, static_cast<size_t>(s.np) * 2 * 8, st) != cudaSuccess ||
         cudaMallocAsync(&c->d_src, sizeof(int) * static_cast<size_t>(capacity), st) != cudaSuccess ||
         cudaMallocAsync(&c->d_mask, static_cast<size_t>(capacity), st) != cudaSuccess ||
+        (c->h_stage = static_cast<double*>(pinned_acquire(64 * static_cast<size_t>(capacity)))) == nullptr ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         c->err = "device allocation failed";
         return bail(ALEA_ERR_NOMEM);
@@ -1134,6 +1181,7 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
                     static_cast<void*>(c->d_mask)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    pinned_release(c->h_stage, 64 * static_cast<size_t>(c->capacity));
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1417,13 +1465,18 @@ int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, a
 int alea_gpu_dmc_advance(alea_gpu_ctx* c, const alea_gpu_dmc_params* prm, alea_gpu_step_stats* out) {
     if (!c || !prm) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
-    if (int rc = run_sweep(c, 1, prm->n_substeps, prm->tau, 1, prm->e_trial, prm->e_ref, prm->e_cut, prm->e_max))
+    if (int rc = run_sweep(c, 1, prm->n_substeps, prm->tau, 1, prm->e_trial, prm->e_ref, prm->e_cut, prm->e_max,
+                           false))
         return rc;
-    if (int rc = read_scalars(c, S_WEIGHT, c->h_w)) return rc;
-    if (int rc = read_scalars(c, S_EL, c->h_el)) return rc;
+    // weights, energies, counters and error flags in one transfer
+    std::vector<double> err;
+    if (int rc = read_pack(c, {S_WEIGHT, S_EL, S_NACC, S_NCUT, S_ERR}, {&c->h_w, &c->h_el, &c->h_nacc, &c->h_ncut, &err}))
+        return rc;
+    for (int w = 0; w < c->nw; ++w)
+        if (err[w] != 0.0)
+            return fail(c, ALEA_ERR_SINGULAR,
+                        "walker " + std::to_string(w) + ": accepted determinant is singular or nonfinite");
     if (out) {
-        if (int rc = read_scalars(c, S_NACC, c->h_nacc)) return rc;
-        if (int rc = read_scalars(c, S_NCUT, c->h_ncut)) return rc;
         *out = alea_gpu_step_stats{};
         // Σ w E and Σ w per crowd, then over crowds (dmc.cpp:713-724)
         const int nw = c->nw;
@@ -1455,8 +1508,8 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
     cudaSetDevice(c->device);
     const int n = c->nw;
     if (n == 0) return ALEA_OK;
-    std::vector<double> w;
-    if (int rc = read_scalars(c, S_WEIGHT, w)) return rc;
+    std::vector<double> w, ids, par;
+    if (int rc = read_pack(c, {S_WEIGHT, S_ID, S_PARENT}, {&w, &ids, &par})) return rc;
     HostXo rng;
     std::memcpy(rng.s, state, 32);
     std::vector<int> src;
@@ -1496,12 +1549,11 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
     std::memcpy(state, rng.s, 32);
     if (static_cast<int>(src.size()) > c->capacity)
         return fail(c, ALEA_ERR_NOMEM, "branching exceeded the walker capacity");
-    // genealogy (walker_set.cpp:221-238)
-    std::vector<double> ids, par;
-    if (int rc = read_scalars(c, S_ID, ids)) return rc;
-    if (int rc = read_scalars(c, S_PARENT, par)) return rc;
+    // genealogy (walker_set.cpp:221-238): ids then parents, one plane each
     std::vector<char> seen(n, 0);
-    std::vector<double> nid(src.size()), npar(src.size());
+    std::vector<double> idpar(2 * src.size());
+    double* nid = idpar.data();
+    double* npar = idpar.data() + src.size();
     for (size_t j = 0; j < src.size(); ++j) {
         nid[j] = ids[src[j]];
         npar[j] = par[src[j]];
@@ -1514,7 +1566,11 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
         }
     }
     const int nn = static_cast<int>(src.size());
-    CUDA_TRY(c, copy_in(c, c->d_src, src.data(), sizeof(int) * nn));
+    // the maps through the pinned stage: ids and parents first, then src
+    double* st_idpar = c->h_stage;
+    int* st_src = reinterpret_cast<int*>(c->h_stage + 2 * static_cast<size_t>(nn));
+    std::memcpy(st_src, src.data(), sizeof(int) * nn);
+    CUDA_TRY(c, copy_in(c, c->d_src, st_src, sizeof(int) * nn));
     ++c->launches;
     gather_kernel<<<nn, 256, 0, c->stream>>>(c->rec[1 - c->cur], c->rec[c->cur], c->d_src, nn, c->sys.rec);
     CUDA_TRY(c, cudaGetLastError());
@@ -1524,8 +1580,13 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
     set_scalar_kernel<<<(nn + 255) / 256, 256, 0, c->stream>>>(records(c), nn, c->sys.rec,
                                                                 c->sys.o_scal + S_WEIGHT, 1.0);
     CUDA_TRY(c, cudaGetLastError());
-    if (int rc = write_scalars(c, S_ID, nid)) return rc;
-    if (int rc = write_scalars(c, S_PARENT, npar)) return rc;
+    std::memcpy(st_idpar, idpar.data(), 16L * nn);
+    CUDA_TRY(c, copy_in(c, c->d_buf, st_idpar, 16L * nn));
+    ++c->launches;
+    from_soa_kernel<<<(2 * nn + 255) / 256, 256, 0, c->stream>>>(records(c), nn, c->sys.rec, c->sys.o_scal + S_ID,
+                                                                  2, c->d_buf);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return ALEA_OK;
 }
 
