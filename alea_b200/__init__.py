@@ -18,6 +18,7 @@ from typing import Any, Dict, List, Optional, Sequence
 import numpy as np
 
 from . import _capi
+from . import estimators as _est
 from ._capi import load as _load
 
 __all__ = ["Walkers", "Server", "AleaGpuError", "pack_system", "STREAM_VMC", "STREAM_DMC", "STREAM_BRANCH"]
@@ -351,6 +352,78 @@ class Walkers:
         v = ctypes.c_double()
         self._check(self.lib.alea_gpu_last_kernel_ms(self.ctx, ctypes.byref(v)))
         return v.value
+
+    # ── estimators (include/alea_gpu.h, estimators) ────────────────────────
+    def add_estimator(self, kind: str, n_bins: int = 0, rmax: float = 0.0, per_particle: bool = False,
+                      kmax: float = 0.0) -> int:
+        """'gofr' (rmax, n_bins), 'density' (n_bins, rmax for an open cell,
+        per_particle) or 'sofk' (kmax); returns the estimator's id."""
+        spec = _capi.EstimatorSpec(_est.KINDS[kind], int(n_bins), float(rmax), 1 if per_particle else 0,
+                                   float(kmax))
+        i = ctypes.c_int()
+        self._check(self.lib.alea_gpu_add_estimator(self.ctx, ctypes.byref(spec), ctypes.byref(i)))
+        self._est_specs = getattr(self, "_est_specs", {})
+        self._est_specs[i.value] = dict(kind=kind, n_bins=int(n_bins), rmax=float(rmax),
+                                        per_particle=bool(per_particle), kmax=float(kmax))
+        return i.value
+
+    def clear_estimators(self) -> None:
+        self._check(self.lib.alea_gpu_clear_estimators(self.ctx))
+        self._est_specs = {}
+
+    def estimators_reset(self) -> None:
+        self._check(self.lib.alea_gpu_estimators_reset(self.ctx))
+
+    def estimators_start_block(self) -> None:
+        self._check(self.lib.alea_gpu_estimators_start_block(self.ctx))
+
+    def estimators_accumulate(self, weights: Optional[np.ndarray] = None, chains: int = 1) -> None:
+        """One measurement; weights [nw] (None: the walkers' own)."""
+        wp = None
+        if weights is not None:
+            w = np.ascontiguousarray(weights, dtype=np.float64)
+            wp = _dp(w)
+        self._check(self.lib.alea_gpu_estimators_accumulate(self.ctx, wp, int(chains)))
+
+    def estimators_stop_block(self) -> None:
+        self._check(self.lib.alea_gpu_estimators_stop_block(self.ctx))
+
+    def estimator_desc(self, i: int) -> _capi.EstimatorDesc:
+        d = _capi.EstimatorDesc()
+        self._check(self.lib.alea_gpu_estimator_info(self.ctx, int(i), ctypes.byref(d)))
+        return d
+
+    def estimator_blocks(self, i: int) -> np.ndarray:
+        """Block estimates [n_chains][n_blocks][block_width]."""
+        d = self.estimator_desc(i)
+        out = np.zeros(max(d.n_chains * d.n_blocks * d.block_width, 1))
+        self._check(self.lib.alea_gpu_estimator_blocks(self.ctx, int(i), _dp(out)))
+        return out[:d.n_chains * d.n_blocks * d.block_width].reshape(d.n_chains, d.n_blocks, d.block_width)
+
+    def estimator_kvectors(self, i: int) -> Dict[str, np.ndarray]:
+        d = self.estimator_desc(i)
+        nk, ns = d.n_k, d.n_shells
+        n1, n2, sh, cnt = (np.zeros(nk, np.int32), np.zeros(nk, np.int32), np.zeros(nk, np.int32),
+                           np.zeros(ns, np.int32))
+        kx, ky, sk = np.zeros(nk), np.zeros(nk), np.zeros(ns)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self._check(self.lib.alea_gpu_estimator_kvectors(
+            self.ctx, int(i), n1.ctypes.data_as(ip), n2.ctypes.data_as(ip), _dp(kx), _dp(ky),
+            sh.ctypes.data_as(ip), _dp(sk), cnt.ctypes.data_as(ip)))
+        return dict(n1=n1, n2=n2, kx=kx, ky=ky, shell_of=sh, shell_k=sk, shell_count=cnt)
+
+    def estimator_results(self, i: int) -> Dict[str, np.ndarray]:
+        """The estimator's named series (the reference's finalize())."""
+        spec = self._est_specs[i]
+        groups = self.desc["groups"]
+        d = self.estimator_desc(i)
+        chains = self.estimator_blocks(i)
+        flat = chains.reshape(-1, d.block_width)
+        if spec["kind"] == "gofr":
+            return _est.finalize_gofr(flat, groups, spec["rmax"], spec["n_bins"], d.volume)
+        if spec["kind"] == "density":
+            return _est.finalize_density(chains, groups, spec["n_bins"], spec["per_particle"])
+        return _est.finalize_sofk(flat, groups, self.estimator_kvectors(i))
 
     def _run(self, fn, n_eq, n_acc, n_steps, n_substeps, tau, streams, seed, drift=False,
              target=0, generations=10.0, alpha=2.0, n_blocks_out=0):

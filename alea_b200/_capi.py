@@ -138,6 +138,19 @@ class JobResult(ctypes.Structure):
                 ("footprint_bytes", ctypes.c_size_t)]
 
 
+class EstimatorSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("n_bins", ctypes.c_int), ("rmax", ctypes.c_double),
+                ("per_particle", ctypes.c_int), ("kmax", ctypes.c_double)]
+
+
+class EstimatorDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("block_width", ctypes.c_int), ("n_chains", ctypes.c_int),
+                ("n_blocks", ctypes.c_int), ("n_series", ctypes.c_int), ("n_bins", ctypes.c_int),
+                ("n_cells", ctypes.c_int), ("n_k", ctypes.c_int), ("n_shells", ctypes.c_int),
+                ("volume", ctypes.c_double), ("cell_volume", ctypes.c_double)]
+
+
+EST_GOFR, EST_DENSITY, EST_SOFK = 1, 2, 3
 JOB_VMC, JOB_DMC = 0, 1
 PRECISION_FP64, PRECISION_FP32 = 0, 1
 ERR_TIMEOUT, ERR_NOMEM, ERR_CANCELLED = 5, 6, 7
@@ -158,6 +171,9 @@ EXPORTS = [
     "alea_gpu_set_precision",
     "alea_gpu_server_create", "alea_gpu_submit_job", "alea_gpu_poll", "alea_gpu_cancel",
     "alea_gpu_server_destroy", "alea_gpu_server_last_error",
+    "alea_gpu_add_estimator", "alea_gpu_clear_estimators", "alea_gpu_estimators_reset",
+    "alea_gpu_estimators_start_block", "alea_gpu_estimators_accumulate", "alea_gpu_estimators_stop_block",
+    "alea_gpu_estimator_info", "alea_gpu_estimator_blocks", "alea_gpu_estimator_kvectors",
 ]
 
 _LIB = None
@@ -217,6 +233,15 @@ def load() -> ctypes.CDLL:
         "alea_gpu_cancel": ([P, ctypes.c_uint64], I),
         "alea_gpu_server_destroy": ([P], I),
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
+        "alea_gpu_add_estimator": ([P, ctypes.POINTER(EstimatorSpec), c_ip], I),
+        "alea_gpu_clear_estimators": ([P], I),
+        "alea_gpu_estimators_reset": ([P], I),
+        "alea_gpu_estimators_start_block": ([P], I),
+        "alea_gpu_estimators_accumulate": ([P, c_dp, I], I),
+        "alea_gpu_estimators_stop_block": ([P], I),
+        "alea_gpu_estimator_info": ([P, I, ctypes.POINTER(EstimatorDesc)], I),
+        "alea_gpu_estimator_blocks": ([P, I, c_dp], I),
+        "alea_gpu_estimator_kvectors": ([P, I, c_ip, c_ip, c_dp, c_dp, c_ip, c_dp, c_ip], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -26,6 +26,7 @@
 #include "../../include/alea_gpu.h"
 #include "alea_internal.h"
 #include "alea_dev.cuh"
+#include "alea_estimators.h"
 #include "alea_kernels.h"
 
 using namespace alea_gpu;
@@ -186,6 +187,7 @@ struct alea_gpu_ctx {
     uint64_t launches = 0;         // kernels launched by this context
     double* noalloc_scratch = nullptr;   // device address of g_noalloc_scratch on `device`
     const std::atomic<int>* cancel = nullptr;   // a server's cancel flag, read between steps
+    alea_gpu::EstimatorSet* est = nullptr;      // observable estimators (alea_gpu_add_estimator)
 };
 
 namespace {
@@ -1180,6 +1182,7 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
                     static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
                     static_cast<void*>(c->d_mask)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
+    if (c->stream) alea_gpu::est_free(c->est, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     pinned_release(c->h_stage, 64 * static_cast<size_t>(c->capacity));
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1615,6 +1618,95 @@ int alea_gpu_last_kernel_ms(const alea_gpu_ctx* c, double* ms) {
     return ALEA_OK;
 }
 
+// ───────────────────────── estimators ─────────────────────────────────
+
+int alea_gpu_add_estimator(alea_gpu_ctx* c, const alea_gpu_estimator_spec* spec, int* id) {
+    if (!c || !spec || !id) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    std::string err;
+    if (int rc = est_add(c->est, c->sys, *spec, c->stream, err, id)) return fail(c, rc, err);
+    return ALEA_OK;
+}
+
+int alea_gpu_clear_estimators(alea_gpu_ctx* c) {
+    if (!c) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    est_free(c->est, c->stream);
+    return ALEA_OK;
+}
+
+int alea_gpu_estimators_reset(alea_gpu_ctx* c) {
+    if (!c) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    std::string err;
+    if (int rc = est_reset(c->est, c->stream, err)) return fail(c, rc, err);
+    return ALEA_OK;
+}
+
+int alea_gpu_estimators_start_block(alea_gpu_ctx* c) {
+    if (!c) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    std::string err;
+    if (int rc = est_start_block(c->est, c->stream, err)) return fail(c, rc, err);
+    return ALEA_OK;
+}
+
+namespace {
+
+// One measurement of the context's estimators: weights on the host (copied
+// into the staging buffer), or the records' own (null), or all 1 (unit).
+int measure_estimators(alea_gpu_ctx* c, const double* weights, bool unit, int chains) {
+    if (est_count(c->est) == 0) return ALEA_OK;
+    const double* dw = nullptr;
+    if (weights && !unit) {
+        CUDA_TRY(c, copy_in(c, c->d_buf, weights, sizeof(double) * c->nw));
+        dw = c->d_buf;
+    }
+    std::string err;
+    if (int rc = est_accumulate(c->est, c->sys, records(c), c->nw, dw, unit, chains, c->pairs, c->npair, c->stream,
+                                err, &c->launches))
+        return fail(c, rc, err);
+    return ALEA_OK;
+}
+
+int close_estimator_block(alea_gpu_ctx* c) {
+    if (est_count(c->est) == 0) return ALEA_OK;
+    std::string err;
+    if (int rc = est_stop_block(c->est, c->stream, err, &c->d2h)) return fail(c, rc, err);
+    return ALEA_OK;
+}
+
+}  // namespace
+
+int alea_gpu_estimators_accumulate(alea_gpu_ctx* c, const double* weights, int n_chains) {
+    if (!c) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    if (c->nw == 0) return fail(c, ALEA_ERR_INVALID, "no walkers");
+    return measure_estimators(c, weights, false, n_chains);
+}
+
+int alea_gpu_estimators_stop_block(alea_gpu_ctx* c) {
+    if (!c) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    return close_estimator_block(c);
+}
+
+int alea_gpu_estimator_info(const alea_gpu_ctx* c, int id, alea_gpu_estimator_desc* out) {
+    if (!c) return ALEA_ERR_INVALID;
+    return est_info(c->est, id, out);
+}
+
+int alea_gpu_estimator_blocks(const alea_gpu_ctx* c, int id, double* blocks) {
+    if (!c) return ALEA_ERR_INVALID;
+    return est_blocks(c->est, id, blocks);
+}
+
+int alea_gpu_estimator_kvectors(const alea_gpu_ctx* c, int id, int* n1, int* n2, double* kx, double* ky,
+                                int* shell_of, double* shell_k, int* shell_count) {
+    if (!c) return ALEA_ERR_INVALID;
+    return est_kvectors(c->est, id, n1, n2, kx, ky, shell_of, shell_k, shell_count);
+}
+
 int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
                      double* block_energies) {
     if (!c || !cfg || !res) return ALEA_ERR_INVALID;
@@ -1628,8 +1720,12 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     double e_sum = 0, e2_sum = 0;
     int64_t n_tot = 0, acc = 0, prop = 0, all_moves = 0, all_evals = 0;
     const int base = nw / T, rem = nw % T;
+    std::string est_err;
+    if (int rc = est_reset(c->est, c->stream, est_err)) return fail(c, rc, est_err);
     for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
         const bool measure = b >= cfg->n_equilibration_blocks;
+        if (measure)
+            if (int rc = est_start_block(c->est, c->stream, est_err)) return fail(c, rc, est_err);
         std::vector<double> blk(T, 0.0);
         std::vector<int64_t> blk_n(T, 0);
         for (int st = 0; st < cfg->n_steps; ++st) {
@@ -1640,6 +1736,7 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             all_moves += s.n_proposed;
             all_evals += s.n_walkers;
             if (!measure) continue;
+            if (int rc = measure_estimators(c, nullptr, true, T)) return rc;
             std::vector<double> el;
             if (int rc = read_scalars(c, S_EL, el)) return rc;
             for (int t = 0; t < T; ++t) {
@@ -1655,8 +1752,10 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             acc += s.n_accepted;
             prop += s.n_proposed;
         }
-        if (measure)
+        if (measure) {
             for (int t = 0; t < T; ++t) chain[t].push_back(blk[t] / static_cast<double>(blk_n[t]));
+            if (int rc = close_estimator_block(c)) return rc;
+        }
     }
     for (int t = 0; t < T; ++t) blocks.insert(blocks.end(), chain[t].begin(), chain[t].end());
     double mean = 0.0, err = 0.0;
@@ -1718,9 +1817,13 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     refresh_spread(el);
     std::vector<double> blocks;
     int64_t acc = 0, prop = 0, all_evals = 0;
+    std::string est_err;
+    if (int rc = est_reset(c->est, c->stream, est_err)) return fail(c, rc, est_err);
     for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
         const bool measure = b >= cfg->n_equilibration_blocks;
         if (b == cfg->n_equilibration_blocks) eref_sum = eref_wsum = 0.0;
+        if (measure)
+            if (int rc = est_start_block(c->est, c->stream, est_err)) return fail(c, rc, est_err);
         double blk_e = 0.0, blk_w = 0.0;
         for (int st = 0; st < cfg->n_steps; ++st) {
             if (c->cancel && c->cancel->load(std::memory_order_relaxed))
@@ -1734,6 +1837,9 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             blk_e += s.energy_sum;
             blk_w += s.weight_sum;
             const double ens_e = s.weight_sum > 0.0 ? s.energy_sum / s.weight_sum : etrial;
+            // mixed estimator: the population before the branch, DMC weights
+            if (measure)
+                if (int rc = measure_estimators(c, nullptr, false, 1)) return rc;
             if (int rc = alea_gpu_dmc_branch(c, bstate, target)) return rc;
             if (measure) {
                 eref_sum += ens_e * s.weight_sum;
@@ -1745,8 +1851,10 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             if (s.weight_sum > 0.0)
                 etrial = eref - feedback * std::log(s.weight_sum / static_cast<double>(target));
         }
-        if (measure) blocks.push_back(blk_w > 0.0 ? blk_e / blk_w : 0.0);
-        else {
+        if (measure) {
+            blocks.push_back(blk_w > 0.0 ? blk_e / blk_w : 0.0);
+            if (int rc = close_estimator_block(c)) return rc;
+        } else {
             if (int rc = read_scalars(c, S_EL, el)) return rc;
             refresh_spread(el);
         }

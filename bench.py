@@ -65,6 +65,8 @@ def parse():
                     help="walker sample of the host-CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form measurement")
+    ap.add_argument("--no-estimators", action="store_true",
+                    help="skip the device-estimator (g(r), density, S(k)) measurement")
     ap.add_argument("--serve", action="store_true",
                     help="serving mix instead of the DMC step: Poisson VMC jobs through alea_gpu_server")
     ap.add_argument("--serve-jobs", type=int, default=60)
@@ -428,6 +430,32 @@ def gpu_arm(a):
            "h2d_bytes_per_step": int((h1 - h0) / a.steps), "d2h_bytes_per_step": int((d1 - d0) / a.steps),
            "path": "alea_gpu_upload_walkers + alea_gpu_dmc_run + alea_gpu_download_walkers, pinned host buffers"}
 
+    # ── device estimators on the same population: one measurement each step ──
+    est = None
+    if not a.no_estimators:
+        ws = float(desc["cell"]["ws_radius"])
+        b1 = float(np.hypot(*desc["cell"]["reciprocal"][:2]))
+        ids = [g.add_estimator("gofr", n_bins=110, rmax=ws),
+               g.add_estimator("density", n_bins=48, rmax=ws),
+               g.add_estimator("sofk", kmax=8.0 * b1)]
+        g.estimators_accumulate()          # first measurement allocates the running blocks
+        torch.cuda.synchronize()
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l_est = g.launch_count()
+        x0.record(stream)
+        for _ in range(a.steps):
+            g.estimators_accumulate()
+        x1.record(stream)
+        torch.cuda.synchronize()
+        est_ms = x0.elapsed_time(x1) / a.steps
+        est = {"ms_per_measurement": est_ms, "share_of_dmc_step": est_ms / (ms_max / a.steps),
+               "launches_per_measurement": (g.launch_count() - l_est) / a.steps,
+               "walkers": int(g.nw),
+               "estimators": f"gofr 110 bins to r = {ws:.1f}, density 48x48 per spin, "
+                             f"sofk n_k = {g.estimator_desc(ids[2]).n_k} (|k| <= 8 |b1|)",
+               "note": "every walker binned on the device; the host reads one block estimate per block"}
+        g.clear_estimators()
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -461,6 +489,7 @@ def gpu_arm(a):
             "clocks": clk,
             "population": int(g.nw),
             "fp32": fp32,
+            "estimators": est,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -335,7 +335,11 @@ typedef struct {
 
 /* Whole VMC / DMC runs, the reference drivers' loops with device sweeps.
  * block_energies (nullable) receives one mean per accumulation block (VMC:
- * one per block and stream chain, stream-major). */
+ * one per block and stream chain, stream-major).  The context's estimators
+ * (alea_gpu_add_estimator) start afresh and measure every accumulation step:
+ * VMC with one chain per random stream and unit weights (vmc.cpp:331-350),
+ * DMC on the whole population with the DMC weights before the branch
+ * (dmc.cpp:704-706, :792-801). */
 int alea_gpu_vmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
                      double* block_energies);
 int alea_gpu_dmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
@@ -355,6 +359,82 @@ int alea_gpu_transfer_bytes(const alea_gpu_ctx* ctx, uint64_t* h2d, uint64_t* d2
 /* Kernels this context has launched so far (instrumentation; no counterpart
  * in the reference). */
 int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
+
+/* ───────────────────────── estimators ──────────────────────────────────
+ *
+ * Observable estimators accumulated on the device from the walker records
+ * (the reference's Estimator, src/estimators/estimator.h:44-131, whose
+ * per-block lifecycle start_block → accumulate × n_steps → stop_block these
+ * calls keep): pair correlation g(r) (PairCorrelation,
+ * src/estimators/pair_correlation.cpp), the density grid (Density,
+ * src/estimators/density.cpp) and the structure factor S(k) with the group
+ * densities ρ_g(k) (StructureFactor, src/estimators/structure_factor.cpp).
+ * A measurement bins every walker's configuration on the device, so a run
+ * with estimators downloads nothing per step; a block's estimate (the array
+ * the reference's stop_block stores) is read back once per block.
+ *
+ * Chains: a measurement may split the walkers into n_chains contiguous even
+ * ranges, each with its own running block, as the reference's VMC keeps one
+ * estimator clone per thread (src/qmc/vmc.cpp:201-207, reduced at :381-387).
+ * Blocks are returned chain-major, the order in which the reference's
+ * collect() concatenates the clones' histories.
+ *
+ * Block estimates (block_width doubles each, W = Σ weights of the block):
+ *   gofr     [pair (a<=b)][bin]  histogram / W                (pair_correlation.cpp:143-160)
+ *   density  [series][cell]      histogram / (W · V_cell)     (density.cpp:153-188)
+ *   sofk     [pair][shell] S, then [group][k] Re ρ, then [group][k] Im ρ, each / W
+ *                                                             (structure_factor.cpp:133-163)
+ * Normalisation into g(r), errors and the named series are the host's
+ * (the reference's finalize()). */
+enum { ALEA_EST_GOFR = 1, ALEA_EST_DENSITY = 2, ALEA_EST_SOFK = 3 };
+
+typedef struct {
+    int kind;            /* ALEA_EST_* */
+    int n_bins;          /* gofr: radial bins; density: bins per axis */
+    double rmax;         /* gofr: range (at most the Wigner-Seitz inradius of a periodic cell);
+                          * density: half-width of the box of an open cell */
+    int per_particle;    /* density: one series per particle instead of per group */
+    double kmax;         /* sofk: |k| <= kmax (periodic 2-D cells) */
+} alea_gpu_estimator_spec;
+
+typedef struct {
+    int kind;
+    int block_width;     /* doubles per block estimate */
+    int n_chains;        /* chains of the current measurements (0 before the first) */
+    int n_blocks;        /* finished blocks per chain */
+    int n_series;        /* gofr, sofk: group pairs a <= b; density: groups or particles */
+    int n_bins;
+    int n_cells;         /* density: cells per series (n_bins^2) */
+    int n_k, n_shells;   /* sofk */
+    double volume;       /* cell area (0 for an open cell) */
+    double cell_volume;  /* density: area of one grid cell */
+} alea_gpu_estimator_desc;
+
+/* Add an estimator (ALEA_ERR_INVALID for a gofr range beyond the
+ * Wigner-Seitz inradius, S(k) on an open cell, or no k below kmax; the
+ * reference's constructors throw there). */
+int alea_gpu_add_estimator(alea_gpu_ctx* ctx, const alea_gpu_estimator_spec* spec, int* id);
+/* Remove every estimator. */
+int alea_gpu_clear_estimators(alea_gpu_ctx* ctx);
+/* Drop every estimator's finished blocks and running block and its chain
+ * count (a fresh clone of each). */
+int alea_gpu_estimators_reset(alea_gpu_ctx* ctx);
+/* Zero the running block of every estimator. */
+int alea_gpu_estimators_start_block(alea_gpu_ctx* ctx);
+/* One measurement of every estimator on the current walkers:
+ * Estimator::accumulate(configs, weights).  weights [nw] (host, borrowed;
+ * NULL: the walkers' own weights, 1 in VMC, the DMC weights between advance
+ * and branch).  n_chains (>= 1) must stay the same until the next reset. */
+int alea_gpu_estimators_accumulate(alea_gpu_ctx* ctx, const double* weights, int n_chains);
+/* Close the running block of every estimator on every chain. */
+int alea_gpu_estimators_stop_block(alea_gpu_ctx* ctx);
+int alea_gpu_estimator_info(const alea_gpu_ctx* ctx, int id, alea_gpu_estimator_desc* out);
+/* Finished block estimates, [n_chains][n_blocks][block_width]. */
+int alea_gpu_estimator_blocks(const alea_gpu_ctx* ctx, int id, double* blocks);
+/* The S(k) k set: k = n1 b1 + n2 b2 over the half space, sorted by |k|
+ * (ties in (n1, n2) order), shells of equal |k|; any pointer may be NULL. */
+int alea_gpu_estimator_kvectors(const alea_gpu_ctx* ctx, int id, int* n1, int* n2, double* kx, double* ky,
+                                int* shell_of, double* shell_k, int* shell_count);
 
 /* ── Host setup ─────────────────────────────────────────────────────────
  * Builds an alea_gpu_system (and its JSON description) for the systems the

@@ -2705,3 +2705,181 @@ int o_dmc(void* ps, double* walkers, long* nw_io, long capacity, int threads, ui
     free(rnd); free(scratch); free(tmpw); free(src); free(rngs);
     return 0;
 }
+
+/* ───────────────────────── estimators ───────────────────────────────────
+ * One measurement of the observable estimators on nw configurations, SoA
+ * positions [p*dim*nw + d*nw + w], configuration w weighted by wts[w]; the
+ * histograms and accumulators are added to (the caller zeroes them at a
+ * block start), *wsum receives += Σ_w wts[w] in walker order. */
+
+/* Triangular index of an unordered group pair
+ * (src/estimators/pair_correlation.cpp:88-93). */
+static long est_pair_id(long ga, long gb, long ng) {
+    if (gb < ga) { const long t = ga; ga = gb; gb = t; }
+    return ga * ng - ga * (ga - 1) / 2 + (gb - ga);
+}
+
+static int est_group_of(const sys_t* s, int p) {
+    for (int g = 0; g < s->ngroups; ++g)
+        if (p >= s->gfirst[g] && p < s->glast[g]) return g;
+    return 0;
+}
+
+/* PairCorrelation::accumulate (src/estimators/pair_correlation.cpp:99-127):
+ * pairs i < j in order, walkers innermost; the distance is the one the
+ * distance table holds after build_all (batched_distance_table.cpp:20-55):
+ * minimum image of r_i - r_j, squares summed over dimensions in order. */
+void o_est_gofr(void* ps, const double* pos, long nw, const double* wts, double rmax, int n_bins,
+                double* hist, double* wsum) {
+    const sys_t* s = (const sys_t*)ps;
+    const int np = s->np, dim = s->dim;
+    const double inv_delta = (double)n_bins / rmax;
+    for (int i = 0; i < np; ++i) {
+        const int gi = est_group_of(s, i);
+        for (int j = i + 1; j < np; ++j) {
+            double* h = hist + est_pair_id(gi, est_group_of(s, j), s->ngroups) * n_bins;
+            for (long w = 0; w < nw; ++w) {
+                double xi[3], xj[3], del[3];
+                for (int d = 0; d < dim; ++d) {
+                    xi[d] = pos[((long)i * dim + d) * nw + w];
+                    xj[d] = pos[((long)j * dim + d) * nw + w];
+                }
+                const double r = fold_dist(s, xi, xj, del);
+                if (r < rmax) {
+                    const size_t bin = (size_t)(r * inv_delta);
+                    if (bin < (size_t)n_bins) h[bin] += wts[w];
+                }
+            }
+        }
+    }
+    double t = 0.0;
+    for (long w = 0; w < nw; ++w) t += wts[w];
+    *wsum += t;
+}
+
+/* Density::accumulate (src/estimators/density.cpp:70-130): per group (or per
+ * particle when per_particle), a cell of the n_bins^dim grid per particle;
+ * periodic cells bin the fractional coordinates of the wrapped position,
+ * open ones the box [-rmax, rmax)^dim. */
+void o_est_density(void* ps, const double* pos, long nw, const double* wts, double rmax, int n_bins,
+                   int per_particle, double* hist, double* wsum) {
+    const sys_t* s = (const sys_t*)ps;
+    const int dim = s->dim;
+    size_t n_cells = 1;
+    for (int d = 0; d < dim; ++d) n_cells *= (size_t)n_bins;
+    const double two_rmax = 2.0 * rmax;
+    const double inv_delta = (double)n_bins / (2.0 * rmax);
+    const int nser = per_particle ? s->np : s->ngroups;
+    for (int g = 0; g < nser; ++g) {
+        double* h = hist + (size_t)g * n_cells;
+        const int first = per_particle ? g : s->gfirst[g];
+        const int last = per_particle ? g + 1 : s->glast[g];
+        for (int p = first; p < last; ++p) {
+            const double* base = pos + (long)p * dim * nw;
+            for (long w = 0; w < nw; ++w) {
+                size_t cell = 0;
+                if (s->periodic) {
+                    double r[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+                    for (int d = 0; d < dim; ++d) r[d] = base[d * nw + w];
+                    wrap(s, r);
+                    for (int i = 0; i < dim; ++i) {
+                        double acc = 0.0;
+                        for (int d = 0; d < dim; ++d) acc += s->ainv[i * dim + d] * r[d];
+                        f[i] = acc;
+                    }
+                    for (int d = 0; d < dim; ++d) {
+                        const double x = f[d] + 0.5;
+                        size_t b = (size_t)(x * (double)n_bins);
+                        if (b >= (size_t)n_bins) b = (size_t)n_bins - 1;
+                        cell = cell * (size_t)n_bins + b;
+                    }
+                    h[cell] += wts[w];
+                    continue;
+                }
+                int in_box = 1;
+                for (int d = 0; d < dim; ++d) {
+                    const double x = base[d * nw + w] + rmax;
+                    if (x < 0.0 || x >= two_rmax) {
+                        in_box = 0;
+                        break;
+                    }
+                    size_t b = (size_t)(x * inv_delta);
+                    if (b >= (size_t)n_bins) b = (size_t)n_bins - 1;
+                    cell = cell * (size_t)n_bins + b;
+                }
+                if (in_box) h[cell] += wts[w];
+            }
+        }
+    }
+    double t = 0.0;
+    for (long w = 0; w < nw; ++w) t += wts[w];
+    *wsum += t;
+}
+
+/* e^{inθ}, n = 0..m, by the recurrence of numerics::ReciprocalPhases::ladder
+ * (src/numerics/reciprocal_phases.h:62-76). */
+static void est_ladder(double theta, int m, double* re, double* im) {
+    const double c = cos(theta), sn = sin(theta);
+    re[0] = 1.0;
+    im[0] = 0.0;
+    for (int n = 1; n <= m; ++n) {
+        re[n] = re[n - 1] * c - im[n - 1] * sn;
+        im[n] = re[n - 1] * sn + im[n - 1] * c;
+    }
+}
+
+/* StructureFactor::accumulate (src/estimators/structure_factor.cpp:80-121):
+ * per walker the group densities ρ_g(k) = Σ_i e^{ik·r_i} (ReciprocalPhases,
+ * reciprocal_phases.h:41-58), then acc_re/acc_im += w ρ_g, and for every
+ * group pair a <= b acc_s += w (Re ρ_a Re ρ_b + Im ρ_a Im ρ_b). */
+void o_est_sofk(void* ps, const double* pos, long nw, const double* wts, int nk, const int* n1,
+                const int* n2, double* acc_s, double* acc_re, double* acc_im, double* wsum) {
+    const sys_t* s = (const sys_t*)ps;
+    const int ng = s->ngroups;
+    int m1 = 0, m2 = 0;
+    for (int k = 0; k < nk; ++k) {
+        if (abs(n1[k]) > m1) m1 = abs(n1[k]);
+        if (abs(n2[k]) > m2) m2 = abs(n2[k]);
+    }
+    const double b1x = s->recip[0], b1y = s->recip[1], b2x = s->recip[2], b2y = s->recip[3];
+    double* e1r = malloc(sizeof(double) * (m1 + 1));
+    double* e1i = malloc(sizeof(double) * (m1 + 1));
+    double* e2r = malloc(sizeof(double) * (m2 + 1));
+    double* e2i = malloc(sizeof(double) * (m2 + 1));
+    double* rr = malloc(sizeof(double) * ng * nk);
+    double* ri = malloc(sizeof(double) * ng * nk);
+    for (long w = 0; w < nw; ++w) {
+        const double wt = wts[w];
+        for (int g = 0; g < ng; ++g) {
+            double* re = rr + g * nk;
+            double* im = ri + g * nk;
+            for (int k = 0; k < nk; ++k) re[k] = im[k] = 0.0;
+            for (int i = s->gfirst[g]; i < s->glast[g]; ++i) {
+                const double x = pos[((long)i * 2 + 0) * nw + w], y = pos[((long)i * 2 + 1) * nw + w];
+                est_ladder(b1x * x + b1y * y, m1, e1r, e1i);
+                est_ladder(b2x * x + b2y * y, m2, e2r, e2i);
+                for (int k = 0; k < nk; ++k) {
+                    const int a = n1[k], b = n2[k];
+                    const double ar = e1r[abs(a)], ai = a < 0 ? -e1i[-a] : e1i[a];
+                    const double br = e2r[abs(b)], bi = b < 0 ? -e2i[-b] : e2i[b];
+                    const double c = ar * br - ai * bi;
+                    const double sn = ar * bi + ai * br;
+                    re[k] += c;
+                    im[k] += sn;
+                }
+            }
+            for (int k = 0; k < nk; ++k) {
+                acc_re[g * nk + k] += wt * re[k];
+                acc_im[g * nk + k] += wt * im[k];
+            }
+        }
+        int pid = 0;
+        for (int a = 0; a < ng; ++a)
+            for (int b = a; b < ng; ++b, ++pid) {
+                const double *ra = rr + a * nk, *ia = ri + a * nk, *rb = rr + b * nk, *ib = ri + b * nk;
+                for (int k = 0; k < nk; ++k) acc_s[pid * nk + k] += wt * (ra[k] * rb[k] + ia[k] * ib[k]);
+            }
+        *wsum += wt;
+    }
+    free(e1r); free(e1i); free(e2r); free(e2i); free(rr); free(ri);
+}

@@ -17,6 +17,10 @@
 //   MODE vmc    : run the reference VMC driver and print its trace
 //   MODE dmc    : run the reference DMC driver and print its trace
 //   MODE bench  : time DMC (or VMC, method=vmc) steps with all host threads
+//   MODE estimate : accumulate the estimators (gofr / density / sofk) over
+//                   fixed configurations with given weights, print their series
+// vmc and dmc attach the same estimators when gofr_bins, dens_bins or
+// sofk_kmax is given, and print the estimators' series of run_result().
 #include <omp.h>
 
 #include <chrono>
@@ -29,6 +33,9 @@
 #include <string>
 #include <vector>
 
+#include "estimators/density.h"
+#include "estimators/pair_correlation.h"
+#include "estimators/structure_factor.h"
 #include "hamiltonian/coulomb.h"
 #include "hamiltonian/ewald_term.h"
 #include "hamiltonian/inverse_power.h"
@@ -714,6 +721,33 @@ std::string fix_empty_keys(std::string s) {
     return out;
 }
 
+// The estimators named by the arguments, built as the reference's estimator
+// builders do: gofr (gofr_rmax, gofr_bins), density (dens_rmax, dens_bins,
+// dens_pp = one series per particle) and sofk (sofk_kmax).
+std::vector<std::unique_ptr<Estimator>> make_estimators(const Args& a, const System& s) {
+    std::vector<std::unique_ptr<Estimator>> e;
+    const std::span<const ParticleGroup> groups(s.groups);
+    if (geti(a, "gofr_bins", 0) > 0)
+        e.push_back(std::make_unique<PairCorrelation>(groups, s.dim, getd(a, "gofr_rmax", 1.0),
+                                                      static_cast<int>(geti(a, "gofr_bins", 0)), s.cell));
+    if (geti(a, "dens_bins", 0) > 0)
+        e.push_back(std::make_unique<Density>(groups, s.dim, getd(a, "dens_rmax", 1.0),
+                                              static_cast<int>(geti(a, "dens_bins", 0)),
+                                              geti(a, "dens_pp", 0) != 0, s.cell));
+    if (getd(a, "sofk_kmax", 0.0) > 0.0)
+        e.push_back(std::make_unique<StructureFactor>(groups, s.cell, getd(a, "sofk_kmax", 0.0)));
+    return e;
+}
+
+// Every series and scalar of a run result, under "estimators".
+void put_results(Json& j, const RunResult& r) {
+    j.key("estimators");
+    j.open('{');
+    for (const auto& [k, v] : r.series) j.arr(k, v);
+    for (const auto& [k, v] : r.scalars) j.kv(k, v);
+    j.close('}');
+}
+
 int run(const std::string& mode, const Args& a) {
     auto sys = build_system(a);
     const std::size_t nw = static_cast<std::size_t>(geti(a, "nw", 4));
@@ -777,7 +811,11 @@ int run(const std::string& mode, const Args& a) {
             auto& v = el[static_cast<std::size_t>(omp_get_thread_num())];
             for (double e : ws.local_energies()) v.push_back(e);
         });
+        auto ests = make_estimators(a, *sys);
+        const bool with_ests = !ests.empty();
+        if (with_ests) vmc.set_estimators(std::move(ests));
         vmc.run();
+        if (with_ests) put_results(out, vmc.run_result());
         out.kv("energy", vmc.energy());
         out.kv("energy_error", vmc.energy_error());
         out.kv("variance", vmc.energy_variance());
@@ -845,10 +883,14 @@ int run(const std::string& mode, const Args& a) {
                     ids.emplace_back(ws.ids().begin(), ws.ids().end());
                 }
             });
+            auto ests = make_estimators(a, *sys);
+            const bool with_ests = !ests.empty();
+            if (with_ests) dmc.set_estimators(std::move(ests));
             const auto t0 = std::chrono::steady_clock::now();
             dmc.run();
             const double wall =
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (with_ests) put_results(out, dmc.run_result());
             out.ki("threads", c.n_threads);
             out.kv("wall", wall);
             out.arr("stamps", stamps);
@@ -872,6 +914,39 @@ int run(const std::string& mode, const Args& a) {
                 out.arr("final_positions", dmc.final_configurations());
             }
         }
+    } else if (mode == "estimate") {
+        // acc blocks of `steps` configurations each: configuration (b, s) is a
+        // fresh App initialisation from init_seed + 1000 b + s, walker w
+        // weighted by 0.25 + 0.125 ((5w + 3s + b) mod 13).
+        const int n_blocks = static_cast<int>(geti(a, "acc", 2));
+        const int n_steps = static_cast<int>(geti(a, "steps", 3));
+        auto ests = make_estimators(a, *sys);
+        out.key("configurations");
+        out.open('[');
+        for (int b = 0; b < n_blocks; ++b) {
+            for (auto& e : ests) e->start_block();
+            for (int st = 0; st < n_steps; ++st) {
+                WalkerEnsemble e2(nw, sys->groups, sys->dim, sys->cell);
+                initialize(e2, *sys, init_seed + 1000 * static_cast<std::uint64_t>(b) +
+                                         static_cast<std::uint64_t>(st));
+                WalkerSet ws(nw, sys->np, sys->dim, sys->cell);
+                for (Walker& w : e2.walkers()) ws.add_walker(w);
+                ws.load_all();
+                std::vector<double> wt(nw);
+                for (std::size_t w = 0; w < nw; ++w)
+                    wt[w] = 0.25 + 0.125 * static_cast<double>((5 * w + 3 * st + b) % 13);
+                for (auto& e : ests) e->accumulate(ws, wt);
+                out.open('{');
+                out.arr("positions", ws.positions());
+                out.arr("weights", wt);
+                out.close('}');
+            }
+            for (auto& e : ests) e->stop_block();
+        }
+        out.close(']');
+        RunResult rr;
+        for (auto& e : ests) e->write_results(rr);
+        put_results(out, rr);
     } else {
         throw std::runtime_error("unknown mode " + mode);
     }

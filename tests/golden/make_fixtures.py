@@ -15,6 +15,11 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
   positions, acceptance;
 * ``dmc_<name>.json``    DMC::run with one crowd per walker: per-step
   populations, weights, energies, ids, final positions;
+* ``est_<name>.json``     the estimators (PairCorrelation, Density,
+  StructureFactor) accumulated over fixed configurations (fresh App
+  initialisations) with given weights: configurations, weights, series;
+* ``est_vmc_<name>.json`` / ``est_dmc_<name>.json`` the same estimators
+  attached to VMC::run / DMC::run (runs as in vmc_/dmc_<name>): series;
 * ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
   reduced here to accumulation-block energies, their mean and its reblocked
   standard error (the statistical reference for the device's DMC).
@@ -58,6 +63,20 @@ DMC = {
     "heg10bf": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
 }
 
+
+# Observable estimators (gofr / density / sofk), with the argument names of
+# ref_harness's estimator builder.
+EST = {
+    "heg10": dict(gofr_rmax=80.0, gofr_bins=20, dens_rmax=84.0, dens_bins=8, sofk_kmax=0.12),
+    "dipoles16": dict(gofr_rmax=0.13, gofr_bins=13, dens_rmax=0.14, dens_bins=4, dens_pp=1,
+                      sofk_kmax=60.0),
+}
+ESTIMATE = {
+    "heg10": dict(nw=6, acc=3, steps=2, init_seed=77),
+    "dipoles16": dict(nw=5, acc=2, steps=3, init_seed=78),
+}
+EST_VMC = {"heg10": "heg10", "dipoles16": "dipoles16"}
+EST_DMC = {"heg10": "heg10"}
 
 DMC_STAT = {
     "heg10": dict(nw=1024, seed=424242, eq=10, acc=50, steps=10, substeps=1, tau=0.5, threads=8),
@@ -106,6 +125,25 @@ def main(only=None):
         r["params"] = run
         r["system"] = name
         dump(f"dmc_{name}.json", r)
+    for name, run in ESTIMATE.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("estimate", **run, **EST[name], **SYSTEMS[name])
+        r["params"] = run
+        r["est"] = EST[name]
+        dump(f"est_{name}.json", r)
+    for name, key in EST_VMC.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("vmc", **VMC[key], **EST[name], **SYSTEMS[name])
+        dump(f"est_vmc_{name}.json", {"params": VMC[key], "est": EST[name], "estimators": r["estimators"],
+                                      "final_positions": r["final_positions"]})
+    for name, key in EST_DMC.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("dmc", **DMC[key], **EST[name], **SYSTEMS[name])
+        dump(f"est_dmc_{name}.json", {"params": DMC[key], "est": EST[name], "estimators": r["estimators"],
+                                      "walkers": r["walkers"], "final_positions": r["final_positions"]})
     for name, run in DMC_STAT.items():
         if only and name not in only:
             continue
