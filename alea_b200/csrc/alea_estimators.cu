@@ -480,8 +480,8 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const double* records, in
                    bool unit, int chains, const int2* pairs, int npair, cudaStream_t st, std::string& err,
                    uint64_t* launches) {
     if (!set || set->e.empty()) return ALEA_OK;
-    if (chains < 1 || chains > nw) {
-        err = "estimators: n_chains must be in [1, walkers]";
+    if (chains < 1 || chains > nw || chains > 65535) {
+        err = "estimators: n_chains must be in [1, min(walkers, 65535)]";
         return ALEA_ERR_INVALID;
     }
     if (set->chains == 0) {
