@@ -9,16 +9,17 @@
 // walkers into it.  Within a walker the lanes take 32 pairs (particles,
 // k-vectors) at a time; lanes that land in the same bin are counted with
 // match.any and their leader adds weight × count, so no two lanes of a warp
-// ever add to one address and a row's sums have a fixed order.  A second
-// kernel adds the rows of each chain in row order to the chain's running
-// block, so a measurement's result does not depend on scheduling; with unit
-// (or dyadic) weights every bin is an exact sum, bit-equal to the
-// reference's running sums.  The block's close (the reference's stop_block)
-// runs on the host once per block.
+// ever add to one address and a row's sums have a fixed order.  Two more
+// kernels add a chain's rows into its running block in a fixed order (slabs
+// of 64 rows, then the slabs in order), so a measurement's result does not
+// depend on scheduling; with unit (or dyadic) weights every bin is an exact
+// sum, bit-equal to the reference's running sums.  The block's close (the
+// reference's stop_block) runs on the host once per block.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "alea_estimators.h"
@@ -30,7 +31,7 @@ namespace {
 constexpr unsigned kAll = 0xffffffffu;
 constexpr size_t kPartBudget = size_t(32) << 20;   // bytes of per-row partial sums, all chains
 constexpr int kSmemRowDoubles = 5120;               // rows up to 40 KB are staged in shared memory
-constexpr int kRowsTarget = 148 * 16;               // warps in flight: 16 one-warp CTAs per SM
+constexpr int kRowsTarget = 148 * 32;               // warps in flight: 32 one-warp CTAs per SM
 
 struct EstLaunch {
     const double* rec;
@@ -95,40 +96,65 @@ __device__ __forceinline__ int pair_id(int ga, int gb, int ng) {
     return ga * ng - ga * (ga - 1) / 2 + (gb - ga);
 }
 
+// Group of particle p from the group ranges (kernel parameters, no load).
+__device__ __forceinline__ int group_at(const DevSys& s, int p) {
+    int g = 0;
+    for (int q = 0; q < s.ngroups; ++q)
+        if (p >= s.gfirst[q] && p < s.glast[q]) g = q;
+    return g;
+}
+
 // PairCorrelation::accumulate (pair_correlation.cpp:99-127): every pair i < j
 // at its minimum-image distance |r_i - r_j| (the distance table's value,
-// batched_distance_table.cpp:20-55), binned below rmax.
+// batched_distance_table.cpp:20-55), binned below rmax.  A walker's pairs are
+// first counted per bin (integer shared-memory atomics: exact, order-free);
+// then each bin with a count adds weight × count to the row once.  The pair
+// list is staged in shared memory when pairs_smem is set.
 __global__ void __launch_bounds__(32) gofr_kernel(const __grid_constant__ DevSys s, const EstLaunch L,
-                                                  const int2* __restrict__ pairs, int npair, double rmax,
-                                                  double inv_delta, int n_bins) {
+                                                  const int2* __restrict__ pairs, int npair, int pairs_smem,
+                                                  double rmax, double inv_delta, int n_bins) {
     extern __shared__ double sm[];
-    double* pos = sm;                                   // [np * 2]
-    double* row = row_of(L, sm + ((s.np * 2 + 1) & ~1));
+    const int width = L.width1 - 1;
+    double* pos = sm;                                           // [np * 2]
+    int* cnt = reinterpret_cast<int*>(pos + ((s.np * 2 + 1) & ~1));   // [width]
+    int2* spairs = reinterpret_cast<int2*>(cnt + ((width + 1) & ~1));
+    double* row = row_of(L, reinterpret_cast<double*>(spairs + (pairs_smem ? npair : 0)));
+    const int lane = threadIdx.x;
+    const int2* pt = pairs;
+    if (pairs_smem) {
+        for (int q = lane; q < npair; q += 32) spairs[q] = pairs[q];
+        pt = spairs;
+    }
+    for (int k = lane; k < width; k += 32) cnt[k] = 0;
     row_zero(L, row);
     int w0, w1;
     row_range(L, blockIdx.y, blockIdx.x, w0, w1);
-    const int lane = threadIdx.x;
     for (int w = w0; w < w1; ++w) {
         const double* r = L.rec + static_cast<long>(w) * L.stride + L.o_pos;
         for (int k = lane; k < s.np * 2; k += 32) pos[k] = r[k];
         const double wt = weight_of(L, w);
         __syncwarp();
-        for (int q0 = 0; q0 < npair; q0 += 32) {
-            const int q = q0 + lane;
-            int idx = -1;
-            if (q < npair) {
-                const int2 ij = pairs[q];
-                double dx, dy;
-                const double d = fold2(s, pos[ij.x * 2], pos[ij.x * 2 + 1], pos[ij.y * 2], pos[ij.y * 2 + 1], dx, dy);
-                if (d < rmax) {
-                    const unsigned long long bin = static_cast<unsigned long long>(d * inv_delta);
-                    if (bin < static_cast<unsigned long long>(n_bins))
-                        idx = pair_id(s.group_of[ij.x], s.group_of[ij.y], s.ngroups) * n_bins + static_cast<int>(bin);
-                }
+        for (int q = lane; q < npair; q += 32) {
+            const int2 ij = pt[q];
+            double dx, dy;
+            const double d = fold2(s, pos[ij.x * 2], pos[ij.x * 2 + 1], pos[ij.y * 2], pos[ij.y * 2 + 1], dx, dy);
+            if (d < rmax) {
+                const unsigned long long bin = static_cast<unsigned long long>(d * inv_delta);
+                if (bin < static_cast<unsigned long long>(n_bins))
+                    atomicAdd(cnt + pair_id(group_at(s, ij.x), group_at(s, ij.y), s.ngroups) * n_bins +
+                                  static_cast<int>(bin),
+                              1);
             }
-            add_binned(row, idx, wt);
         }
-        if (lane == 0) row[L.width1 - 1] += wt;
+        __syncwarp();
+        for (int k = lane; k < width; k += 32) {
+            const int c = cnt[k];
+            if (c) {
+                row[k] += wt * static_cast<double>(c);
+                cnt[k] = 0;
+            }
+        }
+        if (lane == 0) row[width] += wt;
         __syncwarp();
     }
     row_flush(L, row);
@@ -209,20 +235,62 @@ __device__ __forceinline__ void pick(const double* lad, int n, double& re, doubl
     im = n < 0 ? -lad[2 * a + 1] : lad[2 * a + 1];
 }
 
+// ρ(k) += Σ_q e^{ik·r_q} over the cnt particles whose ladders are in lad, for
+// this lane's NS k-vectors k = 32 (c0 + c) + lane; the NS sums are independent
+// chains, particles in order within each.
+template <int NS>
+__device__ __forceinline__ void rho_slots(const int* __restrict__ kn, int nk, int c0, const double* lad, int lw,
+                                          int m1, int cnt, double* re, double* im) {
+    const int lane = threadIdx.x;
+    int a[NS], b[NS];
+    double sr[NS], si[NS];
+#pragma unroll
+    for (int c = 0; c < NS; ++c) {
+        const int k = (c0 + c) * 32 + lane;
+        const bool in = k < nk;
+        a[c] = in ? kn[k] : 0;
+        b[c] = in ? kn[nk + k] : 0;
+        sr[c] = in ? re[k] : 0.0;
+        si[c] = in ? im[k] : 0.0;
+    }
+    for (int q = 0; q < cnt; ++q) {
+        const double* l1 = lad + q * lw;
+        const double* l2 = l1 + 2 * (m1 + 1);
+#pragma unroll
+        for (int c = 0; c < NS; ++c) {
+            double ar, ai, br, bi;
+            pick(l1, a[c], ar, ai);
+            pick(l2, b[c], br, bi);
+            sr[c] += ar * br - ai * bi;
+            si[c] += ar * bi + ai * br;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NS; ++c) {
+        const int k = (c0 + c) * 32 + lane;
+        if (k < nk) {
+            re[k] = sr[c];
+            im[k] = si[c];
+        }
+    }
+}
+
 // StructureFactor::accumulate (structure_factor.cpp:80-121): per walker the
-// group densities ρ_g(k) = Σ_{i∈g} e^{ik·r_i} from the two ladders of each
-// particle, then per k (one lane each) Re ρ_g, Im ρ_g and, for every group
-// pair a <= b, Re ρ_a Re ρ_b + Im ρ_a Im ρ_b, times the weight.
+// group densities ρ_g(k) = Σ_{i∈g} e^{ik·r_i}, then per k (one lane each)
+// Re ρ_g, Im ρ_g and, for every group pair a <= b, Re ρ_a Re ρ_b + Im ρ_a
+// Im ρ_b, times the weight.  A group's particles are taken 32 at a time: each
+// lane builds its particle's two ladders, then each lane sums its k-vectors
+// over the 32 particles in particle order.
 // Row: [pair][k] S sums, [group][k] Re ρ, [group][k] Im ρ, W.
 __global__ void __launch_bounds__(32) sofk_kernel(const __grid_constant__ DevSys s, const EstLaunch L,
                                                   const int* __restrict__ kn, int nk, int m1, int m2) {
     extern __shared__ double sm[];
     const int ng = s.ngroups, lane = threadIdx.x;
     const int npairs = ng * (ng + 1) / 2;
+    const int lw = 2 * (m1 + 1) + 2 * (m2 + 1);         // one particle's two ladders
     double* rho = sm;                                   // [ng][2][nk]
-    double* lad1 = rho + 2 * ng * nk;                   // [2 (m1 + 1)]
-    double* lad2 = lad1 + 2 * (m1 + 1);                 // [2 (m2 + 1)]
-    double* row = row_of(L, lad2 + 2 * (m2 + 1));
+    double* lad = rho + 2 * ng * nk;                    // [32][lw]
+    double* row = row_of(L, lad + 32 * lw);
     row_zero(L, row);
     int w0, w1;
     row_range(L, blockIdx.y, blockIdx.x, w0, w1);
@@ -233,18 +301,23 @@ __global__ void __launch_bounds__(32) sofk_kernel(const __grid_constant__ DevSys
         for (int g = 0; g < ng; ++g) {
             double* re = rho + 2 * g * nk;
             double* im = re + nk;
-            for (int i = s.gfirst[g]; i < s.glast[g]; ++i) {
-                const double x = r[i * 2], y = r[i * 2 + 1];
-                __syncwarp();   // the previous particle's ladders are read
-                if (lane == 0) ladder(s.recip[0] * x + s.recip[1] * y, m1, lad1);
-                if (lane == 1) ladder(s.recip[2] * x + s.recip[3] * y, m2, lad2);
+            for (int i0 = s.gfirst[g]; i0 < s.glast[g]; i0 += 32) {
+                const int cnt = min(32, s.glast[g] - i0);
+                __syncwarp();   // rho zeroed, the previous particles' ladders read
+                if (lane < cnt) {
+                    const double x = r[(i0 + lane) * 2], y = r[(i0 + lane) * 2 + 1];
+                    ladder(s.recip[0] * x + s.recip[1] * y, m1, lad + lane * lw);
+                    ladder(s.recip[2] * x + s.recip[3] * y, m2, lad + lane * lw + 2 * (m1 + 1));
+                }
                 __syncwarp();
-                for (int k = lane; k < nk; k += 32) {
-                    double ar, ai, br, bi;
-                    pick(lad1, kn[k], ar, ai);
-                    pick(lad2, kn[nk + k], br, bi);
-                    re[k] += ar * br - ai * bi;
-                    im[k] += ar * bi + ai * br;
+                const int slots = (nk + 31) / 32;
+                for (int c0 = 0; c0 < slots; c0 += 4) {
+                    switch (min(slots - c0, 4)) {
+                        case 1: rho_slots<1>(kn, nk, c0, lad, lw, m1, cnt, re, im); break;
+                        case 2: rho_slots<2>(kn, nk, c0, lad, lw, m1, cnt, re, im); break;
+                        case 3: rho_slots<3>(kn, nk, c0, lad, lw, m1, cnt, re, im); break;
+                        default: rho_slots<4>(kn, nk, c0, lad, lw, m1, cnt, re, im); break;
+                    }
                 }
             }
         }
@@ -267,18 +340,42 @@ __global__ void __launch_bounds__(32) sofk_kernel(const __grid_constant__ DevSys
     row_flush(L, row);
 }
 
-// acc[t][k] += Σ_r part[t][r][k], rows in order.
-__global__ void est_reduce_kernel(const double* __restrict__ part, int rows, int width1, int chains,
-                                  double* __restrict__ acc) {
-    const long n = static_cast<long>(chains) * width1;
-    for (long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; e < n;
-         e += static_cast<long>(gridDim.x) * blockDim.x) {
-        const long t = e / width1, k = e % width1;
-        const double* p = part + t * rows * width1 + k;
-        double sum = 0.0;
-        for (int q = 0; q < rows; ++q) sum += p[static_cast<long>(q) * width1];
-        acc[e] += sum;
+constexpr int kSlab = 64;   // rows summed by one CTA of the first reduction stage
+
+// First stage: slab j of chain t (rows [64 j, 64 j + 64)) summed per column.
+// Thread (warp v, lane l) takes column k = 32 x + l and adds rows
+// 64 j + v + 8 i in i order; the 8 warps' sums are added in warp order.
+__global__ void __launch_bounds__(256) est_slab_kernel(const double* __restrict__ part, int rows, int width1,
+                                                       int slabs, double* __restrict__ part2) {
+    __shared__ double red[8][32];
+    const int l = threadIdx.x & 31, v = threadIdx.x >> 5;
+    const int k = blockIdx.x * 32 + l, j = blockIdx.y, t = blockIdx.z;
+    double sum = 0.0;
+    if (k < width1) {
+        const double* p = part + static_cast<long>(t) * rows * width1 + k;
+        const int r1 = min(rows, (j + 1) * kSlab);
+#pragma unroll 4
+        for (int q = j * kSlab + v; q < r1; q += 8) sum += p[static_cast<long>(q) * width1];
     }
+    red[v][l] = sum;
+    __syncthreads();
+    if (v == 0 && k < width1) {
+        double a = red[0][l];
+        for (int q = 1; q < 8; ++q) a += red[q][l];
+        part2[(static_cast<long>(t) * slabs + j) * width1 + k] = a;
+    }
+}
+
+// Second stage: acc[t][k] += Σ_j part2[t][j][k], slabs in order.
+__global__ void est_sum_kernel(const double* __restrict__ part2, int slabs, int width1, int chains,
+                               double* __restrict__ acc) {
+    const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    if (e >= static_cast<long>(chains) * width1) return;
+    const long t = e / width1, k = e % width1;
+    const double* p = part2 + t * slabs * width1 + k;
+    double a = 0.0;
+    for (int j = 0; j < slabs; ++j) a += p[static_cast<long>(j) * width1];
+    acc[e] += a;
 }
 
 }  // namespace
@@ -303,8 +400,10 @@ struct DevEstimator {
 
 struct EstimatorSet {
     std::vector<DevEstimator> e;
-    double* d_part = nullptr;
+    double* d_part = nullptr;      // per-row sums of one measurement
     size_t part_bytes = 0;
+    double* d_part2 = nullptr;     // per-slab sums
+    size_t part2_bytes = 0;
     int chains = 0;
 };
 
@@ -447,6 +546,7 @@ void est_free(EstimatorSet*& set, cudaStream_t st) {
     if (!set) return;
     for (DevEstimator& d : set->e) free_one(d, st);
     if (set->d_part) cudaFreeAsync(set->d_part, st);
+    if (set->d_part2) cudaFreeAsync(set->d_part2, st);
     delete set;
     set = nullptr;
 }
@@ -506,15 +606,19 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const double* records, in
         const size_t per_row = sizeof(double) * width1;
         rows = static_cast<int>(std::max<size_t>(1, std::min<size_t>(rows, kPartBudget / (per_row * chains))));
         const size_t need = per_row * rows * chains;
-        if (need > set->part_bytes) {
-            if (set->d_part) cudaFreeAsync(set->d_part, st);
-            set->d_part = nullptr;
-            set->part_bytes = 0;
-            if (cudaMallocAsync(&set->d_part, need, st) != cudaSuccess) {
+        const int slabs = (rows + kSlab - 1) / kSlab;
+        const size_t need2 = per_row * slabs * chains;
+        for (auto [buf, have, want] : {std::tuple<double**, size_t*, size_t>{&set->d_part, &set->part_bytes, need},
+                                       {&set->d_part2, &set->part2_bytes, need2}}) {
+            if (want <= *have) continue;
+            if (*buf) cudaFreeAsync(*buf, st);
+            *buf = nullptr;
+            *have = 0;
+            if (cudaMallocAsync(buf, want, st) != cudaSuccess) {
                 err = "estimators: device allocation failed";
                 return ALEA_ERR_NOMEM;
             }
-            set->part_bytes = need;
+            *have = want;
         }
         EstLaunch L{};
         L.rec = records;
@@ -533,22 +637,30 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const double* records, in
         size_t smem = L.smem_row ? sizeof(double) * width1 : 0;
         const alea_gpu_estimator_spec& sp = d.spec;
         if (sp.kind == ALEA_EST_GOFR) {
-            smem += sizeof(double) * ((s.np * 2 + 1) & ~1);
-            gofr_kernel<<<grid, 32, smem, st>>>(s, L, pairs, npair, sp.rmax, d.inv_delta, sp.n_bins);
+            smem += sizeof(double) * ((s.np * 2 + 1) & ~1) + sizeof(int) * ((d.width + 1) & ~1);
+            if (smem > 48 * 1024) {
+                err = "gofr: too many bins for one warp's shared memory (" + std::to_string(d.width) + ")";
+                return ALEA_ERR_UNSUPPORTED;
+            }
+            const int pairs_smem = smem + sizeof(int2) * npair <= 40 * 1024 ? 1 : 0;
+            if (pairs_smem) smem += sizeof(int2) * npair;
+            gofr_kernel<<<grid, 32, smem, st>>>(s, L, pairs, npair, pairs_smem, sp.rmax, d.inv_delta, sp.n_bins);
         } else if (sp.kind == ALEA_EST_DENSITY) {
             density_kernel<<<grid, 32, smem, st>>>(s, L, sp.rmax, sp.n_bins, sp.per_particle ? 1 : 0);
         } else {
-            smem += sizeof(double) * (2 * s.ngroups * d.nk + 2 * (d.m1 + 1) + 2 * (d.m2 + 1));
+            smem += sizeof(double) * (2 * s.ngroups * d.nk + 32 * (2 * (d.m1 + 1) + 2 * (d.m2 + 1)));
             if (smem > 48 * 1024) {
                 err = "sofk: too many k-vectors for one warp's shared memory (n_k = " + std::to_string(d.nk) + ")";
                 return ALEA_ERR_UNSUPPORTED;
             }
             sofk_kernel<<<grid, 32, smem, st>>>(s, L, d.d_kn, d.nk, d.m1, d.m2);
         }
+        est_slab_kernel<<<dim3((width1 + 31) / 32, slabs, chains), 256, 0, st>>>(set->d_part, rows, width1, slabs,
+                                                                                set->d_part2);
         const long n = static_cast<long>(chains) * width1;
-        est_reduce_kernel<<<static_cast<int>(std::min<long>((n + 255) / 256, 148L * 8)), 256, 0, st>>>(
-            set->d_part, rows, width1, chains, d.d_acc);
-        if (launches) *launches += 2;
+        est_sum_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, st>>>(set->d_part2, slabs, width1, chains,
+                                                                         d.d_acc);
+        if (launches) *launches += 3;
         if (cudaGetLastError() != cudaSuccess) {
             err = "estimators: kernel launch failed";
             return ALEA_ERR_CUDA;

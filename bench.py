@@ -433,8 +433,10 @@ def gpu_arm(a):
     # ── device estimators on the same population: one measurement each step ──
     est = None
     if not a.no_estimators:
-        ws = float(desc["cell"]["ws_radius"])
-        b1 = float(np.hypot(*desc["cell"]["reciprocal"][:2]))
+        av = np.array(desc["cell"]["vectors"], dtype=float).reshape(2, 2)
+        ws = 0.5 * min(float(np.hypot(*(i * av[0] + j * av[1])))
+                       for i in range(-2, 3) for j in range(-2, 3) if i or j)
+        b1 = float(np.hypot(*(2.0 * np.pi * np.linalg.inv(av)[:, 0])))
         ids = [g.add_estimator("gofr", n_bins=110, rmax=ws),
                g.add_estimator("density", n_bins=48, rmax=ws),
                g.add_estimator("sofk", kmax=8.0 * b1)]
