@@ -353,6 +353,26 @@ class Walkers:
         self._check(self.lib.alea_gpu_last_kernel_ms(self.ctx, ctypes.byref(v)))
         return v.value
 
+    # ── configurations and carry-over ─────────────────────────────────────
+    def final_configurations(self) -> np.ndarray:
+        """AoS rows [w][p][d] of the current walkers (the checkpoint rows)."""
+        n = ctypes.c_int()
+        self._check(self.lib.alea_gpu_final_configurations(self.ctx, None, ctypes.byref(n)))
+        rows = np.zeros(max(n.value, 1) * self.np * self.dim)
+        self._check(self.lib.alea_gpu_final_configurations(self.ctx, _dp(rows), ctypes.byref(n)))
+        return rows[:n.value * self.np * self.dim].reshape(n.value, self.np, self.dim)
+
+    def seed_walker_rows(self, rows: np.ndarray, nw: int) -> None:
+        """nw walkers from AoS rows, walker w taking row w mod len(rows)."""
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(-1, self.np * self.dim))
+        self._check(self.lib.alea_gpu_seed_walker_rows(self.ctx, _dp(r), r.shape[0], int(nw)))
+
+    def carry_over(self, source: "Walkers", nw: int, keep_state: bool = False) -> None:
+        """Seed this context from `source`'s walkers on the device: positions
+        and a full evaluation, or (keep_state, same system) whole records."""
+        mode = _capi.CARRY_STATE if keep_state else _capi.CARRY_POSITIONS
+        self._check(self.lib.alea_gpu_carry_over(source.ctx, self.ctx, int(nw), mode))
+
     # ── estimators (include/alea_gpu.h, estimators) ────────────────────────
     def add_estimator(self, kind: str, n_bins: int = 0, rmax: float = 0.0, per_particle: bool = False,
                       kmax: float = 0.0) -> int:

@@ -151,6 +151,7 @@ class EstimatorDesc(ctypes.Structure):
 
 
 EST_GOFR, EST_DENSITY, EST_SOFK = 1, 2, 3
+CARRY_POSITIONS, CARRY_STATE = 0, 1
 JOB_VMC, JOB_DMC = 0, 1
 PRECISION_FP64, PRECISION_FP32 = 0, 1
 ERR_TIMEOUT, ERR_NOMEM, ERR_CANCELLED = 5, 6, 7
@@ -174,6 +175,7 @@ EXPORTS = [
     "alea_gpu_add_estimator", "alea_gpu_clear_estimators", "alea_gpu_estimators_reset",
     "alea_gpu_estimators_start_block", "alea_gpu_estimators_accumulate", "alea_gpu_estimators_stop_block",
     "alea_gpu_estimator_info", "alea_gpu_estimator_blocks", "alea_gpu_estimator_kvectors",
+    "alea_gpu_final_configurations", "alea_gpu_seed_walker_rows", "alea_gpu_carry_over",
 ]
 
 _LIB = None
@@ -233,6 +235,9 @@ def load() -> ctypes.CDLL:
         "alea_gpu_cancel": ([P, ctypes.c_uint64], I),
         "alea_gpu_server_destroy": ([P], I),
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
+        "alea_gpu_final_configurations": ([P, c_dp, c_ip], I),
+        "alea_gpu_seed_walker_rows": ([P, c_dp, I, I], I),
+        "alea_gpu_carry_over": ([P, P, I, I], I),
         "alea_gpu_add_estimator": ([P, ctypes.POINTER(EstimatorSpec), c_ip], I),
         "alea_gpu_clear_estimators": ([P], I),
         "alea_gpu_estimators_reset": ([P], I),

@@ -188,6 +188,7 @@ struct alea_gpu_ctx {
     double* noalloc_scratch = nullptr;   // device address of g_noalloc_scratch on `device`
     const std::atomic<int>* cancel = nullptr;   // a server's cancel flag, read between steps
     alea_gpu::EstimatorSet* est = nullptr;      // observable estimators (alea_gpu_add_estimator)
+    uint64_t fingerprint = 0;      // FNV-1a of the system's layout and tables (equal systems, equal records)
 };
 
 namespace {
@@ -922,6 +923,17 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     if (c->smem > 227 * 1024)
         return fail(c, ALEA_ERR_UNSUPPORTED,
                     "walker state needs " + std::to_string(c->smem) + " bytes of shared memory (> 227 KB)");
+    // fingerprint before the pointers are patched: layout, scalars and tables
+    {
+        uint64_t h = 1469598103934665603ULL;
+        auto mix = [&h](const void* p, size_t n) {
+            const unsigned char* b = static_cast<const unsigned char*>(p);
+            for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ULL;
+        };
+        mix(&s, sizeof s);
+        mix(ar.bytes.data(), ar.bytes.size());
+        c->fingerprint = h;
+    }
     // upload the arena and patch pointers
     CUDA_TRY(c, cudaMallocAsync(&c->arena, std::max<size_t>(ar.bytes.size(), 256), c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(c->arena, ar.bytes.data(), ar.bytes.size(), cudaMemcpyHostToDevice, c->stream));
@@ -1616,6 +1628,118 @@ int alea_gpu_last_kernel_ms(const alea_gpu_ctx* c, double* ms) {
     if (!c || !ms) return ALEA_ERR_INVALID;
     *ms = c->last_ms;
     return ALEA_OK;
+}
+
+// ───────────────────────── configurations / carry-over ────────────────
+
+namespace {
+
+// Fresh walkers from n_rows AoS rows already on c's device (walker w takes
+// row w mod n_rows): what alea_gpu_upload_walkers does with SoA positions.
+int fresh_walkers(alea_gpu_ctx* c, const double* d_rows, int n_rows, int nw) {
+    const DevSys& s = c->sys;
+    c->cur = 0;
+    c->nw = nw;
+    CUDA_TRY(c, cudaMemsetAsync(records(c), 0, static_cast<size_t>(s.rec) * 8 * nw, c->stream));
+    const long n = static_cast<long>(s.np) * 2 * nw;
+    ++c->launches;
+    from_rows_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_pos,
+                                                                              s.np * 2, d_rows, n_rows);
+    ++c->launches;
+    set_scalar_kernel<<<(nw + 255) / 256, 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_scal + S_WEIGHT, 1.0);
+    CUDA_TRY(c, cudaGetLastError());
+    c->next_id = 1.0;
+    return launch_evaluate(c);
+}
+
+}  // namespace
+
+int alea_gpu_final_configurations(alea_gpu_ctx* c, double* rows, int* nw) {
+    if (!c || !nw) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    *nw = c->nw;
+    if (!rows || c->nw == 0) return ALEA_OK;
+    const int n = c->sys.np * 2;
+    const long tot = static_cast<long>(n) * c->nw;
+    ++c->launches;
+    to_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
+                                                                              c->sys.o_pos, n, c->d_buf);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, copy_out(c, rows, c->d_buf, static_cast<size_t>(tot) * 8));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
+}
+
+int alea_gpu_seed_walker_rows(alea_gpu_ctx* c, const double* rows, int n_rows, int nw) {
+    if (!c) return ALEA_ERR_INVALID;
+    if (!rows || n_rows < 1) return fail(c, ALEA_ERR_INVALID, "seed_walker_rows: no configurations to seed from");
+    if (nw < 1 || nw > c->capacity) return fail(c, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const int used = std::min(n_rows, nw);
+    CUDA_TRY(c, copy_in(c, c->d_buf, rows, static_cast<size_t>(used) * c->sys.np * 2 * 8));
+    return fresh_walkers(c, c->d_buf, used, nw);
+}
+
+int alea_gpu_carry_over(alea_gpu_ctx* from, alea_gpu_ctx* to, int nw, int mode) {
+    if (!from || !to || from == to) return ALEA_ERR_INVALID;
+    if (mode != ALEA_CARRY_POSITIONS && mode != ALEA_CARRY_STATE)
+        return fail(to, ALEA_ERR_INVALID, "carry_over: unknown mode");
+    if (nw < 1 || nw > to->capacity) return fail(to, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
+    if (from->nw < 1) return fail(to, ALEA_ERR_INVALID, "carry_over: the source context has no walkers");
+    if (from->sys.np != to->sys.np) return fail(to, ALEA_ERR_INVALID, "carry_over: particle counts differ");
+    const int used = std::min(from->nw, nw);
+    const bool peer = from->device != to->device;
+    if (mode == ALEA_CARRY_STATE) {
+        if (from->fingerprint != to->fingerprint)
+            return fail(to, ALEA_ERR_INVALID,
+                        "carry_over: the contexts were created from different systems; carry positions instead");
+        if (from->sys.f32 != to->sys.f32)
+            return fail(to, ALEA_ERR_INVALID, "carry_over: the contexts run at different precisions");
+        const DevSys& s = to->sys;
+        CUDA_TRY(to, cudaSetDevice(from->device));
+        CUDA_TRY(to, cudaStreamSynchronize(from->stream));
+        const double* src = from->rec[from->cur];
+        CUDA_TRY(to, cudaSetDevice(to->device));
+        if (peer) {   // stage the used records in the destination's spare buffer
+            double* stage = to->rec[1 - to->cur];
+            CUDA_TRY(to, cudaMemcpyPeerAsync(stage, to->device, src, from->device,
+                                             static_cast<size_t>(used) * s.rec * 8, to->stream));
+            src = stage;
+        }
+        ++to->launches;
+        cycle_index_kernel<<<(nw + 255) / 256, 256, 0, to->stream>>>(to->d_src, nw, used);
+        ++to->launches;
+        gather_kernel<<<nw, 256, 0, to->stream>>>(to->rec[to->cur], src, to->d_src, nw, s.rec);
+        // a fresh ensemble: weight 1, no age, no ancestry, no displacement sums
+        to->launches += 6;
+        set_scalar_kernel<<<(nw + 255) / 256, 256, 0, to->stream>>>(to->rec[to->cur], nw, s.rec,
+                                                                     s.o_scal + S_WEIGHT, 1.0);
+        for (int slot : {S_RRP, S_RRA, S_AGE, S_ID, S_PARENT})
+            set_scalar_kernel<<<(nw + 255) / 256, 256, 0, to->stream>>>(to->rec[to->cur], nw, s.rec,
+                                                                         s.o_scal + slot, 0.0);
+        CUDA_TRY(to, cudaGetLastError());
+        CUDA_TRY(to, cudaStreamSynchronize(to->stream));
+        to->nw = nw;
+        to->next_id = 1.0;
+        return ALEA_OK;
+    }
+    // positions: the source's rows, then a full evaluation in the destination
+    CUDA_TRY(to, cudaSetDevice(from->device));
+    const int n = from->sys.np * 2;
+    const long tot = static_cast<long>(n) * used;
+    ++from->launches;
+    to_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, from->stream>>>(
+        from->rec[from->cur], used, from->sys.rec, from->sys.o_pos, n, from->d_buf);
+    CUDA_TRY(to, cudaGetLastError());
+    CUDA_TRY(to, cudaStreamSynchronize(from->stream));
+    CUDA_TRY(to, cudaSetDevice(to->device));
+    const double* rows = from->d_buf;
+    if (peer) {
+        CUDA_TRY(to, cudaMemcpyPeerAsync(to->d_buf, to->device, from->d_buf, from->device,
+                                         static_cast<size_t>(tot) * 8, to->stream));
+        rows = to->d_buf;
+    }
+    return fresh_walkers(to, rows, used, nw);
 }
 
 // ───────────────────────── estimators ─────────────────────────────────

@@ -333,6 +333,24 @@ __global__ void from_soa_kernel(double* records, int nw, long rec, int offset, i
     records[static_cast<long>(w) * rec + offset + i] = in[e];
 }
 
+__global__ void to_rows_kernel(const double* records, int nw, long rec, int offset, int n, double* out) {
+    const long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<long>(n) * nw) return;
+    const int w = static_cast<int>(e / n), i = static_cast<int>(e % n);
+    out[e] = records[static_cast<long>(w) * rec + offset + i];
+}
+__global__ void from_rows_kernel(double* records, int nw, long rec, int offset, int n, const double* rows,
+                                 int n_rows) {
+    const long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<long>(n) * nw) return;
+    const int w = static_cast<int>(e / n), i = static_cast<int>(e % n);
+    records[static_cast<long>(w) * rec + offset + i] = rows[static_cast<long>(w % n_rows) * n + i];
+}
+__global__ void cycle_index_kernel(int* idx, int nw, int n_src) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < nw) idx[w] = w % n_src;
+}
+
 __global__ void set_scalar_kernel(double* records, int nw, long rec, int offset, double value) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w < nw) records[static_cast<long>(w) * rec + offset] = value;

@@ -54,5 +54,12 @@ __global__ void scalar_kernel(const double* records, int nw, long rec, int offse
 __global__ void to_soa_kernel(const double* records, int nw, long rec, int offset, int n, double* out);
 __global__ void from_soa_kernel(double* records, int nw, long rec, int offset, int n, const double* in);
 __global__ void set_scalar_kernel(double* records, int nw, long rec, int offset, double value);
+// AoS rows [w][i] of the n doubles at `offset` of each record; the inverse
+// takes row w mod n_rows for walker w.
+__global__ void to_rows_kernel(const double* records, int nw, long rec, int offset, int n, double* out);
+__global__ void from_rows_kernel(double* records, int nw, long rec, int offset, int n, const double* rows,
+                                 int n_rows);
+// idx[w] = w mod n_src
+__global__ void cycle_index_kernel(int* idx, int nw, int n_src);
 
 }  // namespace alea_gpu

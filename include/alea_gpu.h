@@ -360,6 +360,43 @@ int alea_gpu_transfer_bytes(const alea_gpu_ctx* ctx, uint64_t* h2d, uint64_t* d2
  * in the reference). */
 int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
 
+/* ───────────────────────── configurations and carry-over ───────────────
+ *
+ * The walker population as the rows a checkpoint stores and the next driver
+ * is seeded from: AoS [w][p][d] (io::WalkerFile, src/io/walker_io.h:34-40).
+ * The reference hands configurations from one driver to the next through
+ * the host (carry_over_walkers, src/qmc/app.cpp:1078-1098); here the rows can
+ * stay in device memory, and a chain of stages on one system (VMC -> DMC tau1
+ * -> DMC tau2) can keep the walkers' whole state. */
+
+/* Final configurations, AoS rows [w][p][d] of n_particles x dim doubles per
+ * walker (Driver::final_configurations, src/qmc/vmc.h:63-67 and
+ * src/qmc/dmc.h:128-132; WalkerSet::append_configurations,
+ * src/population/walker_set.cpp:253-262).  *nw receives the walker count;
+ * rows may be NULL to ask for it. */
+int alea_gpu_final_configurations(alea_gpu_ctx* ctx, double* rows, int* nw);
+/* nw fresh walkers from n_rows AoS rows, walker w taking row w mod n_rows
+ * (seed_walker_rows, src/qmc/app.cpp:1068-1076: a checkpoint's rows or the
+ * previous driver's), wrapped and fully evaluated, weights 1: a driver's
+ * reload_configurations (src/qmc/driver.h:55-58).  The checkpoint's
+ * geometry and cell checks (app.cpp:834-866) are the host's. */
+int alea_gpu_seed_walker_rows(alea_gpu_ctx* ctx, const double* rows, int n_rows, int nw);
+
+enum { ALEA_CARRY_POSITIONS = 0, ALEA_CARRY_STATE = 1 };
+/* Carry `from`'s population into `to` (nw walkers, walker w from source
+ * walker w mod from's count) without a host round trip:
+ *   ALEA_CARRY_POSITIONS  positions only, then a full evaluation in `to`
+ *                         (the reference's semantics; any two systems with
+ *                         the same particle count);
+ *   ALEA_CARRY_STATE      the whole walker records (inverses, orbital rows,
+ *                         ρ(k), ln ψ, derivatives, E_L), so the next stage
+ *                         starts without re-evaluating; both contexts must be
+ *                         created from identical systems (same tables, same
+ *                         precision), else ALEA_ERR_INVALID.
+ * Either way the walkers restart as a fresh ensemble: weight 1, age 0, no
+ * ancestry.  The contexts may live on different devices (peer copy). */
+int alea_gpu_carry_over(alea_gpu_ctx* from, alea_gpu_ctx* to, int nw, int mode);
+
 /* ───────────────────────── estimators ──────────────────────────────────
  *
  * Observable estimators accumulated on the device from the walker records

@@ -17,6 +17,7 @@
 //   MODE vmc    : run the reference VMC driver and print its trace
 //   MODE dmc    : run the reference DMC driver and print its trace
 //   MODE bench  : time DMC (or VMC, method=vmc) steps with all host threads
+//   MODE chain  : VMC, then DMC seeded from VMC's final configurations
 //   MODE estimate : accumulate the estimators (gofr / density / sofk) over
 //                   fixed configurations with given weights, print their series
 // vmc and dmc attach the same estimators when gofr_bins, dens_bins or
@@ -914,6 +915,59 @@ int run(const std::string& mode, const Args& a) {
                 out.arr("final_positions", dmc.final_configurations());
             }
         }
+    } else if (mode == "chain") {
+        // VMC, then DMC seeded from VMC's final configurations the way
+        // carry_over_walkers / seed_walker_rows do it (app.cpp:1068-1098):
+        // a fresh ensemble of dmc_nw walkers, walker w on row w mod rows.
+        VMCConfig vc;
+        vc.n_equilibration_blocks = static_cast<int>(geti(a, "eq", 0));
+        vc.n_accumulation_blocks = static_cast<int>(geti(a, "acc", 1));
+        vc.n_steps = static_cast<int>(geti(a, "steps", 2));
+        vc.n_substeps = static_cast<int>(geti(a, "substeps", 1));
+        vc.tau = getd(a, "tau", 1.0);
+        vc.n_threads = static_cast<int>(nw);
+        vc.seed = seed;
+        put_positions(out, "initial_positions", ens);
+        VMC vmc(vc, ens, sys->psi, sys->ham);
+        vmc.run();
+        const std::vector<double> rows = vmc.final_configurations();
+        out.arr("vmc_final_positions", rows);
+        const std::size_t nw2 = static_cast<std::size_t>(geti(a, "dmc_nw", static_cast<long long>(nw)));
+        const std::size_t row = sys->np * sys->dim, n_rows = rows.size() / row;
+        WalkerEnsemble ens2(nw2, sys->groups, sys->dim, sys->cell);
+        {
+            std::size_t w = 0;
+            for (Walker& wk : ens2.walkers()) {
+                wk.set_positions(std::span<const double>(rows).subspan((w % n_rows) * row, row));
+                ++w;
+            }
+        }
+        DMCConfig dc;
+        dc.n_equilibration_blocks = static_cast<int>(geti(a, "dmc_eq", 0));
+        dc.n_accumulation_blocks = static_cast<int>(geti(a, "dmc_acc", 1));
+        dc.n_steps = static_cast<int>(geti(a, "dmc_steps", 3));
+        dc.n_substeps = 1;
+        dc.tau = getd(a, "dmc_tau", 0.5);
+        dc.n_threads = static_cast<int>(nw2);
+        dc.seed = static_cast<std::uint64_t>(geti(a, "dmc_seed", static_cast<long long>(seed) + 1));
+        dc.population_generations = getd(a, "generations", 10.0);
+        DMC dmc(dc, ens2, sys->psi, sys->ham);
+        std::vector<double> wsum, ewsum, nws;
+        dmc.set_measure_hook([&](const WalkerSet& ws, const TrialWavefunction&) {
+            nws.push_back(static_cast<double>(ws.num_walkers()));
+            double sw = 0.0, se = 0.0;
+            for (std::size_t w = 0; w < ws.num_walkers(); ++w) {
+                sw += ws.weights()[w];
+                se += ws.weights()[w] * ws.local_energies()[w];
+            }
+            wsum.push_back(sw);
+            ewsum.push_back(se);
+        });
+        dmc.run();
+        out.arr("walkers", nws);
+        out.arr("weight_sum", wsum);
+        out.arr("weighted_energy_sum", ewsum);
+        out.arr("final_positions", dmc.final_configurations());
     } else if (mode == "estimate") {
         // acc blocks of `steps` configurations each: configuration (b, s) is a
         // fresh App initialisation from init_seed + 1000 b + s, walker w

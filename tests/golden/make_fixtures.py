@@ -20,6 +20,8 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
   initialisations) with given weights: configurations, weights, series;
 * ``est_vmc_<name>.json`` / ``est_dmc_<name>.json`` the same estimators
   attached to VMC::run / DMC::run (runs as in vmc_/dmc_<name>): series;
+* ``chain_<name>.json``   a VMC::run whose final configurations seed a DMC::run
+  (carry_over_walkers): DMC populations and weighted energy sums per step;
 * ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
   reduced here to accumulation-block energies, their mean and its reblocked
   standard error (the statistical reference for the device's DMC).
@@ -78,6 +80,12 @@ ESTIMATE = {
 EST_VMC = {"heg10": "heg10", "dipoles16": "dipoles16"}
 EST_DMC = {"heg10": "heg10"}
 
+# VMC -> DMC stage chain: DMC seeded from VMC's final configurations.
+CHAIN = {
+    "heg10": dict(nw=6, seed=11, eq=1, acc=1, steps=2, substeps=2, tau=225.0, dmc_nw=8, dmc_eq=1,
+                  dmc_acc=2, dmc_steps=3, dmc_tau=2.0, dmc_seed=5),
+}
+
 DMC_STAT = {
     "heg10": dict(nw=1024, seed=424242, eq=10, acc=50, steps=10, substeps=1, tau=0.5, threads=8),
 }
@@ -100,6 +108,15 @@ def dump(name, obj):
     with open(os.path.join(HERE, name), "w") as f:
         json.dump(obj, f, separators=(",", ":"))
     print("wrote", name)
+
+
+def chain_fixtures(only=None):
+    for name, run in CHAIN.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("chain", **run, **SYSTEMS[name])
+        r["params"] = run
+        dump(f"chain_{name}.json", r)
 
 
 def main(only=None):
@@ -144,6 +161,7 @@ def main(only=None):
         r = run_ref_harness("dmc", **DMC[key], **EST[name], **SYSTEMS[name])
         dump(f"est_dmc_{name}.json", {"params": DMC[key], "est": EST[name], "estimators": r["estimators"],
                                       "walkers": r["walkers"], "final_positions": r["final_positions"]})
+    chain_fixtures(only)
     for name, run in DMC_STAT.items():
         if only and name not in only:
             continue
