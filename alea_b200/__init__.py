@@ -445,6 +445,62 @@ class Walkers:
             return _est.finalize_density(chains, groups, spec["n_bins"], spec["per_particle"])
         return _est.finalize_sofk(flat, groups, self.estimator_kvectors(i))
 
+    # ── forward walking (pure estimators of a DMC run) ─────────────────────
+    def set_forward_walking(self, lags: Sequence[float], interval: int = 1) -> None:
+        """Lags in imaginary time (strictly increasing; empty: off)."""
+        a = np.ascontiguousarray(np.asarray(lags, dtype=np.float64))
+        self._check(self.lib.alea_gpu_set_forward_walking(self.ctx, _dp(a) if a.size else None, int(a.size),
+                                                          int(interval)))
+        self._fw_specs = {i: {} for i in range(a.size)}
+
+    def add_fw_estimator(self, lag: int, kind: str, n_bins: int = 0, rmax: float = 0.0,
+                         per_particle: bool = False, kmax: float = 0.0) -> int:
+        spec = _capi.EstimatorSpec(_est.KINDS[kind], int(n_bins), float(rmax), 1 if per_particle else 0,
+                                   float(kmax))
+        i = ctypes.c_int()
+        self._check(self.lib.alea_gpu_add_fw_estimator(self.ctx, int(lag), ctypes.byref(spec), ctypes.byref(i)))
+        self._fw_specs[int(lag)][i.value] = dict(kind=kind, n_bins=int(n_bins), rmax=float(rmax),
+                                                 per_particle=bool(per_particle), kmax=float(kmax))
+        return i.value
+
+    def fw_result(self, lag: int) -> Dict[str, Any]:
+        """Pure potential energy of lag index `lag`: summary and block values."""
+        out = _capi.FwSummary()
+        self._check(self.lib.alea_gpu_fw_result(self.ctx, int(lag), ctypes.byref(out), None))
+        blocks = np.zeros(max(out.n_blocks, 1))
+        self._check(self.lib.alea_gpu_fw_result(self.ctx, int(lag), ctypes.byref(out), _dp(blocks)))
+        return dict(lag_time=out.lag_time, lag_steps=out.lag_steps, measurements=out.measurements,
+                    surviving_fraction=out.surviving_fraction, potential=out.potential,
+                    potential_error=out.potential_error, block_potentials=blocks[:out.n_blocks])
+
+    def fw_estimator_results(self, lag: int, i: int) -> Dict[str, np.ndarray]:
+        """Series of a pure estimator, keys labelled fw<lag> as the reference's
+        forward-walking builders label them (gofr_fw0_up_down, ...)."""
+        spec = self._fw_specs[int(lag)][i]
+        d = _capi.EstimatorDesc()
+        self._check(self.lib.alea_gpu_fw_estimator_info(self.ctx, int(lag), int(i), ctypes.byref(d)))
+        out = np.zeros(max(d.n_chains * d.n_blocks * d.block_width, 1))
+        self._check(self.lib.alea_gpu_fw_estimator_blocks(self.ctx, int(lag), int(i), _dp(out)))
+        chains = out[:d.n_chains * d.n_blocks * d.block_width].reshape(d.n_chains, d.n_blocks, d.block_width)
+        groups = self.desc["groups"]
+        flat = chains.reshape(-1, d.block_width)
+        if spec["kind"] == "gofr":
+            res = _est.finalize_gofr(flat, groups, spec["rmax"], spec["n_bins"], d.volume)
+        elif spec["kind"] == "density":
+            res = _est.finalize_density(chains, groups, spec["n_bins"], spec["per_particle"])
+        else:
+            nk, ns = d.n_k, d.n_shells
+            n1, n2, sh, cnt = (np.zeros(nk, np.int32), np.zeros(nk, np.int32), np.zeros(nk, np.int32),
+                               np.zeros(ns, np.int32))
+            kx, ky, sk = np.zeros(nk), np.zeros(nk), np.zeros(ns)
+            ip = ctypes.POINTER(ctypes.c_int)
+            self._check(self.lib.alea_gpu_fw_estimator_kvectors(
+                self.ctx, int(lag), int(i), n1.ctypes.data_as(ip), n2.ctypes.data_as(ip), _dp(kx), _dp(ky),
+                sh.ctypes.data_as(ip), _dp(sk), cnt.ctypes.data_as(ip)))
+            res = _est.finalize_sofk(flat, groups, dict(n1=n1, n2=n2, kx=kx, ky=ky, shell_of=sh, shell_k=sk,
+                                                        shell_count=cnt))
+        return _est.relabel(res, f"fw{int(lag)}")
+
     def _run(self, fn, n_eq, n_acc, n_steps, n_substeps, tau, streams, seed, drift=False,
              target=0, generations=10.0, alpha=2.0, n_blocks_out=0):
         cfg = _capi.RunConfig(n_eq, n_acc, n_steps, n_substeps, tau, 1 if drift else 0, streams,

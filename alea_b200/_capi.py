@@ -150,6 +150,12 @@ class EstimatorDesc(ctypes.Structure):
                 ("volume", ctypes.c_double), ("cell_volume", ctypes.c_double)]
 
 
+class FwSummary(ctypes.Structure):
+    _fields_ = [("lag_time", ctypes.c_double), ("lag_steps", ctypes.c_int), ("n_blocks", ctypes.c_int),
+                ("measurements", ctypes.c_int64), ("surviving_fraction", ctypes.c_double),
+                ("potential", ctypes.c_double), ("potential_error", ctypes.c_double)]
+
+
 EST_GOFR, EST_DENSITY, EST_SOFK = 1, 2, 3
 CARRY_POSITIONS, CARRY_STATE = 0, 1
 JOB_VMC, JOB_DMC = 0, 1
@@ -176,6 +182,8 @@ EXPORTS = [
     "alea_gpu_estimators_start_block", "alea_gpu_estimators_accumulate", "alea_gpu_estimators_stop_block",
     "alea_gpu_estimator_info", "alea_gpu_estimator_blocks", "alea_gpu_estimator_kvectors",
     "alea_gpu_final_configurations", "alea_gpu_seed_walker_rows", "alea_gpu_carry_over",
+    "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
+    "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
 ]
 
 _LIB = None
@@ -235,6 +243,12 @@ def load() -> ctypes.CDLL:
         "alea_gpu_cancel": ([P, ctypes.c_uint64], I),
         "alea_gpu_server_destroy": ([P], I),
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
+        "alea_gpu_set_forward_walking": ([P, c_dp, I, I], I),
+        "alea_gpu_add_fw_estimator": ([P, I, ctypes.POINTER(EstimatorSpec), c_ip], I),
+        "alea_gpu_fw_result": ([P, I, ctypes.POINTER(FwSummary), c_dp], I),
+        "alea_gpu_fw_estimator_info": ([P, I, I, ctypes.POINTER(EstimatorDesc)], I),
+        "alea_gpu_fw_estimator_blocks": ([P, I, I, c_dp], I),
+        "alea_gpu_fw_estimator_kvectors": ([P, I, I, c_ip, c_ip, c_dp, c_dp, c_ip, c_dp, c_ip], I),
         "alea_gpu_final_configurations": ([P, c_dp, c_ip], I),
         "alea_gpu_seed_walker_rows": ([P, c_dp, I, I], I),
         "alea_gpu_carry_over": ([P, P, I, I], I),

@@ -155,6 +155,35 @@ void reblock(const std::vector<double>& series, double& mean, double& err) {
 
 // ───────────────────────── context ──────────────────────────────────────
 
+// Forward walking (src/qmc/forward_walking.h): a ring of position snapshots
+// in device memory, the ancestry of every live walker in each snapshot on the
+// host (integers, carried through each branch's src map), per-lag pure
+// estimators and potential-energy block sums.
+struct FwSlot {
+    long step = -1;                // the step it was taken at; -1: unused
+    int nw = 0;
+    double* d_pos = nullptr;       // [capacity][np * 2]
+    std::vector<int> anc;          // [live walkers]: index into the snapshot
+};
+
+struct FwState {
+    std::vector<double> lags;      // imaginary times, as set
+    int interval = 1;
+    std::vector<alea_gpu::EstimatorSet*> est;   // per lag
+    // per run
+    std::vector<long> lag_steps;
+    double step_time = 0.0;
+    long first_measured = 0, first_snapshot = 0;
+    std::vector<FwSlot> slots;
+    std::vector<double> blk_wpot, blk_w;
+    std::vector<std::vector<double>> block_pot;
+    std::vector<int64_t> measurements;
+    std::vector<double> surviving;
+    int* d_idx = nullptr;          // kept ancestors [capacity]
+    double* d_kw = nullptr;        // their descendant weights
+    double* d_v = nullptr;         // their potentials
+};
+
 struct alea_gpu_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -189,6 +218,8 @@ struct alea_gpu_ctx {
     const std::atomic<int>* cancel = nullptr;   // a server's cancel flag, read between steps
     alea_gpu::EstimatorSet* est = nullptr;      // observable estimators (alea_gpu_add_estimator)
     uint64_t fingerprint = 0;      // FNV-1a of the system's layout and tables (equal systems, equal records)
+    std::vector<int> last_src;     // the last branch's map: new walker j copies old walker last_src[j]
+    FwState* fw = nullptr;         // forward walking (alea_gpu_set_forward_walking)
 };
 
 namespace {
@@ -1187,6 +1218,10 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
     return ALEA_OK;
 }
 
+namespace {
+void fw_free(alea_gpu_ctx* c);
+}  // namespace
+
 int alea_gpu_destroy(alea_gpu_ctx* c) {
     if (!c) return ALEA_OK;
     for (void* p : {static_cast<void*>(c->arena), static_cast<void*>(c->rec[0]), static_cast<void*>(c->rec[1]),
@@ -1195,6 +1230,7 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
                     static_cast<void*>(c->d_mask)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
     if (c->stream) alea_gpu::est_free(c->est, c->stream);
+    if (c->stream) fw_free(c);
     if (c->stream) cudaStreamSynchronize(c->stream);
     pinned_release(c->h_stage, 64 * static_cast<size_t>(c->capacity));
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1581,6 +1617,7 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
         }
     }
     const int nn = static_cast<int>(src.size());
+    c->last_src = src;
     // the maps through the pinned stage: ids and parents first, then src
     double* st_idpar = c->h_stage;
     int* st_src = reinterpret_cast<int*>(c->h_stage + 2 * static_cast<size_t>(nn));
@@ -1629,6 +1666,207 @@ int alea_gpu_last_kernel_ms(const alea_gpu_ctx* c, double* ms) {
     *ms = c->last_ms;
     return ALEA_OK;
 }
+
+// ───────────────────────── forward walking ─────────────────────────────
+
+namespace {
+
+void fw_free_run(alea_gpu_ctx* c) {
+    FwState* f = c->fw;
+    if (!f) return;
+    for (FwSlot& sl : f->slots)
+        if (sl.d_pos) cudaFreeAsync(sl.d_pos, c->stream);
+    f->slots.clear();
+    for (void* p : {static_cast<void*>(f->d_idx), static_cast<void*>(f->d_kw), static_cast<void*>(f->d_v)})
+        if (p) cudaFreeAsync(p, c->stream);
+    f->d_idx = nullptr;
+    f->d_kw = f->d_v = nullptr;
+}
+
+void fw_free(alea_gpu_ctx* c) {
+    if (!c->fw) return;
+    fw_free_run(c);
+    for (EstimatorSet*& e : c->fw->est) est_free(e, c->stream);
+    delete c->fw;
+    c->fw = nullptr;
+}
+
+// DMC::DMC's forward-walking checks and ForwardWalking::prepare
+// (src/qmc/dmc.cpp:102-138, :591-600; src/qmc/forward_walking.cpp:49-73):
+// lags in whole steps of τ·n_substeps, the largest inside the equilibration,
+// the interval dividing the steps per block; a ring of max_lag/interval + 1
+// snapshots of the population capacity.
+int fw_prepare(alea_gpu_ctx* c, const alea_gpu_run_config* cfg) {
+    FwState* f = c->fw;
+    if (!f) return ALEA_OK;
+    fw_free_run(c);
+    const double step_time = cfg->tau * static_cast<double>(cfg->n_substeps);
+    if (!(std::isfinite(step_time) && step_time > 0.0))
+        return fail(c, ALEA_ERR_INVALID, "dmc: forward walking needs time_step > 0 and sub_steps >= 1");
+    if (f->interval < 1 || cfg->n_steps <= 0 || cfg->n_steps % f->interval != 0)
+        return fail(c, ALEA_ERR_INVALID, "dmc: forward_walking interval (" + std::to_string(f->interval) +
+                                             ") must be >= 1 and divide steps_per_block (" +
+                                             std::to_string(cfg->n_steps) + ")");
+    f->lag_steps.clear();
+    for (double lag : f->lags) {
+        const double steps = lag / step_time, whole = std::round(steps);
+        if (std::abs(steps - whole) > 1e-9 * std::max(1.0, steps))
+            return fail(c, ALEA_ERR_INVALID, "dmc: forward_walking lag " + std::to_string(lag) +
+                                                 " is not a whole number of steps of time_step * sub_steps = " +
+                                                 std::to_string(step_time));
+        f->lag_steps.push_back(static_cast<long>(whole));
+    }
+    const long eq_steps = static_cast<long>(std::max(0, cfg->n_equilibration_blocks)) * cfg->n_steps;
+    const long max_lag = f->lag_steps.back();
+    if (max_lag > eq_steps)
+        return fail(c, ALEA_ERR_INVALID, "dmc: the largest forward_walking lag (" + std::to_string(max_lag) +
+                                             " steps) exceeds the equilibration (" + std::to_string(eq_steps) +
+                                             " steps): snapshots start that many steps before accumulation");
+    f->step_time = step_time;
+    f->first_measured = eq_steps;
+    f->first_snapshot = eq_steps - max_lag;
+    const size_t n = f->lags.size();
+    f->blk_wpot.assign(n, 0.0);
+    f->blk_w.assign(n, 0.0);
+    f->block_pot.assign(n, {});
+    f->measurements.assign(n, 0);
+    f->surviving.assign(n, 0.0);
+    f->slots.assign(static_cast<size_t>(max_lag / f->interval + 1), FwSlot{});
+    const size_t cap = static_cast<size_t>(c->capacity);
+    for (FwSlot& sl : f->slots)
+        if (cudaMallocAsync(&sl.d_pos, cap * c->sys.np * 2 * 8, c->stream) != cudaSuccess)
+            return fail(c, ALEA_ERR_NOMEM, "forward walking: snapshot allocation failed");
+    if (cudaMallocAsync(&f->d_idx, cap * sizeof(int), c->stream) != cudaSuccess ||
+        cudaMallocAsync(&f->d_kw, cap * 8, c->stream) != cudaSuccess ||
+        cudaMallocAsync(&f->d_v, cap * 8, c->stream) != cudaSuccess)
+        return fail(c, ALEA_ERR_NOMEM, "forward walking: allocation failed");
+    for (EstimatorSet* e : f->est) {
+        std::string err;
+        if (int rc = est_reset(e, c->stream, err)) return fail(c, rc, err);
+    }
+    return ALEA_OK;
+}
+
+bool fw_snapshot_step(const FwState* f, long step) {
+    return step >= f->first_snapshot && (step - f->first_snapshot) % f->interval == 0;
+}
+
+size_t fw_slot_of(const FwState* f, long step) {
+    return static_cast<size_t>((step - f->first_snapshot) / f->interval) % f->slots.size();
+}
+
+// ForwardWalking::measure (forward_walking.cpp:133-173): descendant weights
+// D[a] = Σ_{w: a(w)=a} W_w in walker order, the ancestors with D > 0 in
+// snapshot order measured with weights D: the lag's estimators and the
+// potential energy (Σ D V / Σ D into the block).
+int fw_measure(alea_gpu_ctx* c, size_t lag, const FwSlot& sl) {
+    FwState* f = c->fw;
+    std::vector<double> w;
+    if (int rc = read_scalars(c, S_WEIGHT, w)) return rc;
+    if (sl.anc.size() != w.size())
+        return fail(c, ALEA_ERR_INVALID, "forward walking: ancestry out of step with the population");
+    std::vector<double> dw(static_cast<size_t>(sl.nw), 0.0);
+    for (size_t i = 0; i < w.size(); ++i) dw[sl.anc[i]] += w[i];
+    std::vector<int> kept;
+    std::vector<double> kw;
+    for (int a = 0; a < sl.nw; ++a)
+        if (dw[a] > 0.0) {
+            kept.push_back(a);
+            kw.push_back(dw[a]);
+        }
+    if (kept.empty()) return ALEA_OK;
+    const int nk = static_cast<int>(kept.size());
+    CUDA_TRY(c, copy_in(c, f->d_idx, kept.data(), sizeof(int) * nk));
+    CUDA_TRY(c, copy_in(c, f->d_kw, kw.data(), 8L * nk));
+    ++c->launches;
+    CUDA_TRY(c, launch_potential(c->nt, nk, c->smem, c->stream, c->sys, sl.d_pos, f->d_idx, c->pairs, c->npair,
+                                 f->d_v));
+    const EstSource src{sl.d_pos, static_cast<long>(c->sys.np) * 2, 0, -1, f->d_idx, nk};
+    std::string err;
+    if (int rc = est_accumulate(f->est[lag], c->sys, src, f->d_kw, false, 1, c->pairs, c->npair, c->stream, err,
+                                &c->launches))
+        return fail(c, rc, err);
+    std::vector<double> v(static_cast<size_t>(nk));
+    CUDA_TRY(c, copy_out(c, v.data(), f->d_v, 8L * nk));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    double weighted = 0.0, total = 0.0;
+    for (int k = 0; k < nk; ++k) {
+        weighted += kw[k] * v[k];
+        total += kw[k];
+    }
+    f->blk_wpot[lag] += weighted;
+    f->blk_w[lag] += total;
+    ++f->measurements[lag];
+    f->surviving[lag] += static_cast<double>(nk) / static_cast<double>(sl.nw);
+    return ALEA_OK;
+}
+
+// ForwardWalking::observe (forward_walking.cpp:113-131): after the step's
+// moves and reweighting, before the branch.
+int fw_observe(alea_gpu_ctx* c, long step) {
+    FwState* f = c->fw;
+    if (!f) return ALEA_OK;
+    if (fw_snapshot_step(f, step)) {
+        FwSlot& sl = f->slots[fw_slot_of(f, step)];
+        sl.step = step;
+        sl.nw = c->nw;
+        const int n = c->sys.np * 2;
+        const long tot = static_cast<long>(n) * c->nw;
+        ++c->launches;
+        to_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
+                                                                                  c->sys.o_pos, n, sl.d_pos);
+        CUDA_TRY(c, cudaGetLastError());
+        sl.anc.resize(static_cast<size_t>(c->nw));
+        for (int i = 0; i < c->nw; ++i) sl.anc[i] = i;
+    }
+    if (step < f->first_measured) return ALEA_OK;
+    for (size_t i = 0; i < f->lag_steps.size(); ++i) {
+        const long taken = step - f->lag_steps[i];
+        if (taken < f->first_snapshot || !fw_snapshot_step(f, taken)) continue;
+        const FwSlot& sl = f->slots[fw_slot_of(f, taken)];
+        if (sl.step != taken) return fail(c, ALEA_ERR_INVALID, "forward walking: snapshot ring overwritten too early");
+        if (int rc = fw_measure(c, i, sl)) return rc;
+    }
+    return ALEA_OK;
+}
+
+// ForwardWalking::branch (forward_walking.cpp:175-182).
+void fw_branch(alea_gpu_ctx* c) {
+    if (!c->fw) return;
+    for (FwSlot& sl : c->fw->slots) {
+        if (sl.step < 0) continue;
+        std::vector<int> g(c->last_src.size());
+        for (size_t j = 0; j < g.size(); ++j) g[j] = sl.anc[c->last_src[j]];
+        sl.anc.swap(g);
+    }
+}
+
+int fw_start_block(alea_gpu_ctx* c) {
+    FwState* f = c->fw;
+    if (!f) return ALEA_OK;
+    std::fill(f->blk_wpot.begin(), f->blk_wpot.end(), 0.0);
+    std::fill(f->blk_w.begin(), f->blk_w.end(), 0.0);
+    for (EstimatorSet* e : f->est) {
+        std::string err;
+        if (int rc = est_start_block(e, c->stream, err)) return fail(c, rc, err);
+    }
+    return ALEA_OK;
+}
+
+int fw_stop_block(alea_gpu_ctx* c) {
+    FwState* f = c->fw;
+    if (!f) return ALEA_OK;
+    for (size_t i = 0; i < f->lags.size(); ++i) {
+        if (f->blk_w[i] > 0.0) f->block_pot[i].push_back(f->blk_wpot[i] / f->blk_w[i]);
+        std::string err;
+        // a lag with no measurement in the block (none possible) closes nothing
+        if (est_count(f->est[i]) > 0 && f->measurements[i] > 0)
+            if (int rc = est_stop_block(f->est[i], c->stream, err, &c->d2h)) return fail(c, rc, err);
+    }
+    return ALEA_OK;
+}
+
+}  // namespace
 
 // ───────────────────────── configurations / carry-over ────────────────
 
@@ -1787,8 +2025,9 @@ int measure_estimators(alea_gpu_ctx* c, const double* weights, bool unit, int ch
         dw = c->d_buf;
     }
     std::string err;
-    if (int rc = est_accumulate(c->est, c->sys, records(c), c->nw, dw, unit, chains, c->pairs, c->npair, c->stream,
-                                err, &c->launches))
+    const EstSource src{records(c), c->sys.rec, c->sys.o_pos, c->sys.o_scal + S_WEIGHT, nullptr, c->nw};
+    if (int rc = est_accumulate(c->est, c->sys, src, dw, unit, chains, c->pairs, c->npair, c->stream, err,
+                                &c->launches))
         return fail(c, rc, err);
     return ALEA_OK;
 }
@@ -1829,6 +2068,70 @@ int alea_gpu_estimator_kvectors(const alea_gpu_ctx* c, int id, int* n1, int* n2,
                                 int* shell_of, double* shell_k, int* shell_count) {
     if (!c) return ALEA_ERR_INVALID;
     return est_kvectors(c->est, id, n1, n2, kx, ky, shell_of, shell_k, shell_count);
+}
+
+// ───────────────────────── forward walking API ─────────────────────────
+
+int alea_gpu_set_forward_walking(alea_gpu_ctx* c, const double* lags, int n_lags, int interval) {
+    if (!c || n_lags < 0 || (n_lags > 0 && !lags)) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    fw_free(c);
+    if (n_lags == 0) return ALEA_OK;
+    if (interval < 1) return fail(c, ALEA_ERR_INVALID, "forward walking interval must be at least one step");
+    for (int i = 0; i < n_lags; ++i) {
+        if (!(std::isfinite(lags[i]) && lags[i] >= 0.0))
+            return fail(c, ALEA_ERR_INVALID, "dmc: forward_walking lags must be finite and >= 0");
+        if (i > 0 && !(lags[i] > lags[i - 1]))
+            return fail(c, ALEA_ERR_INVALID, "dmc: forward_walking lags must be strictly increasing");
+    }
+    c->fw = new FwState();
+    c->fw->lags.assign(lags, lags + n_lags);
+    c->fw->interval = interval;
+    c->fw->est.assign(static_cast<size_t>(n_lags), nullptr);
+    return ALEA_OK;
+}
+
+int alea_gpu_add_fw_estimator(alea_gpu_ctx* c, int lag, const alea_gpu_estimator_spec* spec, int* id) {
+    if (!c || !spec || !id) return ALEA_ERR_INVALID;
+    if (!c->fw || lag < 0 || lag >= static_cast<int>(c->fw->lags.size()))
+        return fail(c, ALEA_ERR_INVALID, "forward walking: no such lag (alea_gpu_set_forward_walking)");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    std::string err;
+    if (int rc = est_add(c->fw->est[lag], c->sys, *spec, c->stream, err, id)) return fail(c, rc, err);
+    return ALEA_OK;
+}
+
+int alea_gpu_fw_result(const alea_gpu_ctx* c, int lag, alea_gpu_fw_summary* out, double* block_potentials) {
+    if (!c || !out || !c->fw || lag < 0 || lag >= static_cast<int>(c->fw->lags.size())) return ALEA_ERR_INVALID;
+    const FwState* f = c->fw;
+    *out = alea_gpu_fw_summary{};
+    out->lag_time = f->lags[lag];
+    if (f->lag_steps.size() != f->lags.size()) return ALEA_OK;   // no run yet
+    out->lag_steps = static_cast<int>(f->lag_steps[lag]);
+    out->measurements = f->measurements[lag];
+    out->surviving_fraction =
+        f->measurements[lag] > 0 ? f->surviving[lag] / static_cast<double>(f->measurements[lag]) : 0.0;
+    const std::vector<double>& chain = f->block_pot[lag];
+    out->n_blocks = static_cast<int>(chain.size());
+    if (!chain.empty()) reblock(chain, out->potential, out->potential_error);
+    if (block_potentials) std::copy(chain.begin(), chain.end(), block_potentials);
+    return ALEA_OK;
+}
+
+int alea_gpu_fw_estimator_info(const alea_gpu_ctx* c, int lag, int id, alea_gpu_estimator_desc* out) {
+    if (!c || !c->fw || lag < 0 || lag >= static_cast<int>(c->fw->lags.size())) return ALEA_ERR_INVALID;
+    return est_info(c->fw->est[lag], id, out);
+}
+
+int alea_gpu_fw_estimator_blocks(const alea_gpu_ctx* c, int lag, int id, double* blocks) {
+    if (!c || !c->fw || lag < 0 || lag >= static_cast<int>(c->fw->lags.size())) return ALEA_ERR_INVALID;
+    return est_blocks(c->fw->est[lag], id, blocks);
+}
+
+int alea_gpu_fw_estimator_kvectors(const alea_gpu_ctx* c, int lag, int id, int* n1, int* n2, double* kx,
+                                   double* ky, int* shell_of, double* shell_k, int* shell_count) {
+    if (!c || !c->fw || lag < 0 || lag >= static_cast<int>(c->fw->lags.size())) return ALEA_ERR_INVALID;
+    return est_kvectors(c->fw->est[lag], id, n1, n2, kx, ky, shell_of, shell_k, shell_count);
 }
 
 int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
@@ -1943,11 +2246,15 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     int64_t acc = 0, prop = 0, all_evals = 0;
     std::string est_err;
     if (int rc = est_reset(c->est, c->stream, est_err)) return fail(c, rc, est_err);
+    if (int rc = fw_prepare(c, cfg)) return rc;
+    long step_index = 0;   // from the first equilibration step (forward walking's clock)
     for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
         const bool measure = b >= cfg->n_equilibration_blocks;
         if (b == cfg->n_equilibration_blocks) eref_sum = eref_wsum = 0.0;
-        if (measure)
+        if (measure) {
             if (int rc = est_start_block(c->est, c->stream, est_err)) return fail(c, rc, est_err);
+            if (int rc = fw_start_block(c)) return rc;
+        }
         double blk_e = 0.0, blk_w = 0.0;
         for (int st = 0; st < cfg->n_steps; ++st) {
             if (c->cancel && c->cancel->load(std::memory_order_relaxed))
@@ -1964,7 +2271,11 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             // mixed estimator: the population before the branch, DMC weights
             if (measure)
                 if (int rc = measure_estimators(c, nullptr, false, 1)) return rc;
+            // pure estimators: snapshots and lagged measurements, same weights
+            if (int rc = fw_observe(c, step_index)) return rc;
             if (int rc = alea_gpu_dmc_branch(c, bstate, target)) return rc;
+            fw_branch(c);
+            ++step_index;
             if (measure) {
                 eref_sum += ens_e * s.weight_sum;
                 eref_wsum += s.weight_sum;
@@ -1978,6 +2289,7 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
         if (measure) {
             blocks.push_back(blk_w > 0.0 ? blk_e / blk_w : 0.0);
             if (int rc = close_estimator_block(c)) return rc;
+            if (int rc = fw_stop_block(c)) return rc;
         } else {
             if (int rc = read_scalars(c, S_EL, el)) return rc;
             refresh_spread(el);

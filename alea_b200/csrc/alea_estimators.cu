@@ -34,10 +34,11 @@ constexpr int kSmemRowDoubles = 5120;               // rows up to 40 KB are stag
 constexpr int kRowsTarget = 148 * 32;               // warps in flight: 32 one-warp CTAs per SM
 
 struct EstLaunch {
-    const double* rec;
+    const double* rec;       // walker records or compact position rows
     long stride;
     int o_pos, o_w;
-    const double* weights;   // [nw], or null: the records' weights
+    const int* idx;          // configuration c is block idx[c] (null: c)
+    const double* weights;   // [nw], or null: the blocks' weights
     int unit;                // every weight 1
     int nw, chains, rows;
     double* part;            // [chains * rows][width1]
@@ -55,10 +56,12 @@ __device__ __forceinline__ void row_range(const EstLaunch& L, int t, int r, int&
     w1 = w0 + rb + (r < rr ? 1 : 0);
 }
 
+__device__ __forceinline__ long block_of_conf(const EstLaunch& L, int w) { return L.idx ? L.idx[w] : w; }
+
 __device__ __forceinline__ double weight_of(const EstLaunch& L, int w) {
     if (L.unit) return 1.0;
     if (L.weights) return L.weights[w];
-    return L.rec[static_cast<long>(w) * L.stride + L.o_w];
+    return L.rec[block_of_conf(L, w) * L.stride + L.o_w];
 }
 
 __device__ __forceinline__ double* row_of(const EstLaunch& L, double* smem_row) {
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(32) gofr_kernel(const __grid_constant__ DevSys
     int w0, w1;
     row_range(L, blockIdx.y, blockIdx.x, w0, w1);
     for (int w = w0; w < w1; ++w) {
-        const double* r = L.rec + static_cast<long>(w) * L.stride + L.o_pos;
+        const double* r = L.rec + block_of_conf(L, w) * L.stride + L.o_pos;
         for (int k = lane; k < s.np * 2; k += 32) pos[k] = r[k];
         const double wt = weight_of(L, w);
         __syncwarp();
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(32) density_kernel(const __grid_constant__ Dev
     const int n_cells = n_bins * n_bins;
     const double two_rmax = 2.0 * rmax, inv_delta = static_cast<double>(n_bins) / (2.0 * rmax);
     for (int w = w0; w < w1; ++w) {
-        const double* r = L.rec + static_cast<long>(w) * L.stride + L.o_pos;
+        const double* r = L.rec + block_of_conf(L, w) * L.stride + L.o_pos;
         const double wt = weight_of(L, w);
         for (int p0 = 0; p0 < s.np; p0 += 32) {
             const int p = p0 + lane;
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(32) sofk_kernel(const __grid_constant__ DevSys
     int w0, w1;
     row_range(L, blockIdx.y, blockIdx.x, w0, w1);
     for (int w = w0; w < w1; ++w) {
-        const double* r = L.rec + static_cast<long>(w) * L.stride + L.o_pos;
+        const double* r = L.rec + block_of_conf(L, w) * L.stride + L.o_pos;
         const double wt = weight_of(L, w);
         for (int k = lane; k < 2 * ng * nk; k += 32) rho[k] = 0.0;
         for (int g = 0; g < ng; ++g) {
@@ -576,10 +579,14 @@ int est_start_block(EstimatorSet* set, cudaStream_t st, std::string& err) {
     return ALEA_OK;
 }
 
-int est_accumulate(EstimatorSet* set, const DevSys& s, const double* records, int nw, const double* d_weights,
-                   bool unit, int chains, const int2* pairs, int npair, cudaStream_t st, std::string& err,
-                   uint64_t* launches) {
+int est_accumulate(EstimatorSet* set, const DevSys& s, const EstSource& src, const double* d_weights, bool unit,
+                   int chains, const int2* pairs, int npair, cudaStream_t st, std::string& err, uint64_t* launches) {
     if (!set || set->e.empty()) return ALEA_OK;
+    const int nw = src.n;
+    if (!unit && !d_weights && src.o_w < 0) {
+        err = "estimators: the configurations carry no weights";
+        return ALEA_ERR_INVALID;
+    }
     if (chains < 1 || chains > nw || chains > 65535) {
         err = "estimators: n_chains must be in [1, min(walkers, 65535)]";
         return ALEA_ERR_INVALID;
@@ -621,10 +628,11 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const double* records, in
             *have = want;
         }
         EstLaunch L{};
-        L.rec = records;
-        L.stride = s.rec;
-        L.o_pos = s.o_pos;
-        L.o_w = s.o_scal + S_WEIGHT;
+        L.rec = src.base;
+        L.stride = src.stride;
+        L.o_pos = src.o_pos;
+        L.o_w = src.o_w;
+        L.idx = src.idx;
         L.weights = d_weights;
         L.unit = unit ? 1 : 0;
         L.nw = nw;

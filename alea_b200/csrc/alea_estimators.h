@@ -22,11 +22,24 @@ void est_free(EstimatorSet*& set, cudaStream_t st);
 int est_count(const EstimatorSet* set);
 int est_reset(EstimatorSet* set, cudaStream_t st, std::string& err);
 int est_start_block(EstimatorSet* set, cudaStream_t st, std::string& err);
-// One measurement on nw records.  d_weights: device [nw] or null (the
-// records' weights); unit: every weight 1.  Adds the launches to *launches.
-int est_accumulate(EstimatorSet* set, const DevSys& s, const double* records, int nw, const double* d_weights,
-                   bool unit, int chains, const int2* pairs, int npair, cudaStream_t st, std::string& err,
-                   uint64_t* launches);
+// Where a measurement's configurations are: walker records (stride s.rec,
+// positions at s.o_pos, weight at s.o_scal + S_WEIGHT) or compact position
+// rows (stride np * 2, offset 0, no weight); configuration c of the
+// measurement is block idx[c] (idx null: block c).
+struct EstSource {
+    const double* base;
+    long stride;
+    int o_pos;
+    int o_w;              // -1: the blocks hold no weight
+    const int* idx;       // device [n] or null
+    int n;                // configurations measured
+};
+
+// One measurement of every estimator of the set.  d_weights: device [n] or
+// null (the blocks' own weights); unit: every weight 1.  Adds the launches to
+// *launches.
+int est_accumulate(EstimatorSet* set, const DevSys& s, const EstSource& src, const double* d_weights, bool unit,
+                   int chains, const int2* pairs, int npair, cudaStream_t st, std::string& err, uint64_t* launches);
 // Reads the running blocks back (adds the bytes to *d2h), stores the block
 // estimates, zeroes the running blocks.
 int est_stop_block(EstimatorSet* set, cudaStream_t st, std::string& err, uint64_t* d2h);

@@ -25,6 +25,28 @@ __global__ void __launch_bounds__(NT) evaluate_kernel(DevSys s, double* records,
     store_hot<NT>(s, rec, sm);
 }
 
+// Potential energy of stored configurations (Hamiltonian::evaluate_potential,
+// src/hamiltonian/hamiltonian_component.h:165-403): configuration c is
+// rows[idx[c]] (positions [np][2]); the local energy's potential terms with
+// zero derivative planes, so the kinetic part adds nothing.
+template <int NT>
+__global__ void __launch_bounds__(NT) potential_kernel(DevSys s, const double* rows, const int* idx, int n,
+                                                       const int2* pairs, int npair, double* out) {
+    extern __shared__ __align__(16) double sm[];
+    const int c = blockIdx.x;
+    if (c >= n) return;
+    const Smem v = view(s, sm);
+    const double* r = rows + static_cast<long>(idx[c]) * s.np * 2;
+    for (int i = threadIdx.x; i < s.np * 2; i += NT) {
+        v.pos[i] = r[i];
+        v.jg[i] = v.jl[i] = v.kg[i] = v.kl[i] = v.sg[i] = v.sl[i] = 0.0;
+        if (s.cplx) v.pg[i] = v.pl[i] = 0.0;
+    }
+    __syncthreads();
+    const double e = local_energy<NT>(s, v, pairs, npair);
+    if (threadIdx.x == 0) out[c] = e;
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) measure_kernel(DevSys s, double* records, int nw,
                                                      const int2* pairs, int npair) {
@@ -229,7 +251,9 @@ cudaError_t reserve_smem(size_t smem) {
         reinterpret_cast<const void*>(evaluate_kernel<64>), reinterpret_cast<const void*>(measure_kernel<64>),
         reinterpret_cast<const void*>(move_kernel<64>), reinterpret_cast<const void*>(sweep_kernel<64>),
         reinterpret_cast<const void*>(evaluate_kernel<128>), reinterpret_cast<const void*>(measure_kernel<128>),
-        reinterpret_cast<const void*>(move_kernel<128>), reinterpret_cast<const void*>(sweep_kernel<128>)};
+        reinterpret_cast<const void*>(move_kernel<128>), reinterpret_cast<const void*>(sweep_kernel<128>),
+        reinterpret_cast<const void*>(potential_kernel<32>), reinterpret_cast<const void*>(potential_kernel<64>),
+        reinterpret_cast<const void*>(potential_kernel<128>)};
     for (const void* k : kernels) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
         if (e != cudaSuccess) return e;
@@ -238,6 +262,13 @@ cudaError_t reserve_smem(size_t smem) {
     if (e == cudaSuccess) e = reserve_smem_f32(smem);
     if (e == cudaSuccess) reserved[dev] = smem;
     return e;
+}
+
+cudaError_t launch_potential(int nt, int n, size_t smem, cudaStream_t st, const DevSys& s, const double* rows,
+                             const int* idx, const int2* pairs, int npair, double* out) {
+    if (n < 1) return cudaSuccess;
+    ALEA_LAUNCH(nt, potential_kernel, n, smem, st, s, rows, idx, n, pairs, npair, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,

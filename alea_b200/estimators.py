@@ -140,3 +140,17 @@ def finalize_sofk(blocks: np.ndarray, groups, kvec: Dict[str, np.ndarray]) -> Di
             name = f"rhok_{groups[g]['name']}_{part}"
             out[name], out[name + "_error"] = m, e
     return out
+
+
+NAMESPACES = ("gofr", "density", "sofk", "rhok")
+
+
+def relabel(series: Dict[str, np.ndarray], label: str) -> Dict[str, np.ndarray]:
+    """Insert an output label after each key's namespace, as the reference's
+    Estimator::write_results does (src/estimators/estimator.h:110-131):
+    label "fw0" turns gofr_up_down into gofr_fw0_up_down."""
+    out = {}
+    for k, v in series.items():
+        ns = max((n for n in NAMESPACES if k == n or k.startswith(n + "_")), key=len, default=None)
+        out[k if ns is None else ns + "_" + label + k[len(ns):]] = v
+    return out

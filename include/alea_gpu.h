@@ -473,6 +473,42 @@ int alea_gpu_estimator_blocks(const alea_gpu_ctx* ctx, int id, double* blocks);
 int alea_gpu_estimator_kvectors(const alea_gpu_ctx* ctx, int id, int* n1, int* n2, double* kx, double* ky,
                                 int* shell_of, double* shell_k, int* shell_count);
 
+/* ───────────────────────── forward walking ─────────────────────────────
+ *
+ * Pure estimators of a DMC run (ForwardWalking, src/qmc/forward_walking.h:
+ * Casulleras & Boronat, PRB 52, 3654 (1995)): every `interval` steps the
+ * population's positions are stored (a snapshot, here in device memory); each
+ * live walker's ancestor in every snapshot is carried through the branches;
+ * at an accumulation step, for each lag T whose snapshot is T old, the
+ * ancestors are weighted by the weight their descendants carry now and
+ * measured: the potential energy (the pure potential; the pure kinetic energy
+ * is E − ⟨V⟩) and the lag's pure estimators.  alea_gpu_dmc_run runs it when
+ * set; the schedule follows DMC::DMC (src/qmc/dmc.cpp:102-138): lags are
+ * whole numbers of steps of τ·n_substeps, the largest at most the
+ * equilibration, interval divides n_steps — else the run fails with
+ * ALEA_ERR_INVALID.  Steps count from the first equilibration step; a run
+ * clears the previous results. */
+typedef struct {
+    double lag_time;              /* imaginary time T */
+    int lag_steps;                /* T in DMC steps */
+    int n_blocks;                 /* accumulation blocks with measurements */
+    int64_t measurements;
+    double surviving_fraction;    /* mean fraction of snapshot walkers with descendants */
+    double potential, potential_error;   /* pure ⟨V⟩ and its reblocked error */
+} alea_gpu_fw_summary;
+
+/* lags [n_lags] strictly increasing imaginary times (n_lags = 0: off). */
+int alea_gpu_set_forward_walking(alea_gpu_ctx* ctx, const double* lags, int n_lags, int interval);
+/* A pure estimator measured at lag index `lag` (the estimator kinds above). */
+int alea_gpu_add_fw_estimator(alea_gpu_ctx* ctx, int lag, const alea_gpu_estimator_spec* spec, int* id);
+/* Results of lag index `lag` after a run; block_potentials (nullable) gets
+ * one ⟨V⟩ per accumulation block (the reference's acc_block_potential_fw<i>). */
+int alea_gpu_fw_result(const alea_gpu_ctx* ctx, int lag, alea_gpu_fw_summary* out, double* block_potentials);
+int alea_gpu_fw_estimator_info(const alea_gpu_ctx* ctx, int lag, int id, alea_gpu_estimator_desc* out);
+int alea_gpu_fw_estimator_blocks(const alea_gpu_ctx* ctx, int lag, int id, double* blocks);
+int alea_gpu_fw_estimator_kvectors(const alea_gpu_ctx* ctx, int lag, int id, int* n1, int* n2, double* kx,
+                                   double* ky, int* shell_of, double* shell_k, int* shell_count);
+
 /* ── Host setup ─────────────────────────────────────────────────────────
  * Builds an alea_gpu_system (and its JSON description) for the systems the
  * reference's App assembles from a config, computing the same tables on the

@@ -863,8 +863,25 @@ int run(const std::string& mode, const Args& a) {
                 geti(a, "threads", bench ? host_threads : static_cast<long long>(nw)));
             c.seed = seed;
             c.population_generations = getd(a, "generations", 10.0);
+            // forward walking: fw_lags=t0,t1,... (imaginary times), fw_interval
+            const std::string fw = gets(a, "fw_lags", "");
+            for (std::size_t p0 = 0; p0 < fw.size();) {
+                const std::size_t p1 = std::min(fw.find(',', p0), fw.size());
+                c.forward_walking_lags.push_back(std::stod(fw.substr(p0, p1 - p0)));
+                p0 = p1 + 1;
+            }
+            c.forward_walking_interval = static_cast<std::size_t>(geti(a, "fw_interval", 1));
             if (!bench) put_positions(out, "initial_positions", ens);
             DMC dmc(c, ens, sys->psi, sys->ham);
+            if (!c.forward_walking_lags.empty()) {
+                // each lag: the same estimators, labelled fw<i> as the builders do
+                std::vector<std::vector<std::unique_ptr<Estimator>>> per_lag(c.forward_walking_lags.size());
+                for (std::size_t i = 0; i < per_lag.size(); ++i) {
+                    per_lag[i] = make_estimators(a, *sys);
+                    for (auto& e : per_lag[i]) e->set_output_label("fw" + std::to_string(i));
+                }
+                dmc.set_forward_walking_estimators(std::move(per_lag));
+            }
             std::vector<double> stamps, wsum, ewsum, nws;
             std::vector<std::vector<double>> el, wt, ids;
             dmc.set_measure_hook([&](const WalkerSet& ws, const TrialWavefunction&) {
@@ -891,7 +908,7 @@ int run(const std::string& mode, const Args& a) {
             dmc.run();
             const double wall =
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            if (with_ests) put_results(out, dmc.run_result());
+            if (with_ests || !c.forward_walking_lags.empty()) put_results(out, dmc.run_result());
             out.ki("threads", c.n_threads);
             out.kv("wall", wall);
             out.arr("stamps", stamps);

@@ -20,6 +20,8 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
   initialisations) with given weights: configurations, weights, series;
 * ``est_vmc_<name>.json`` / ``est_dmc_<name>.json`` the same estimators
   attached to VMC::run / DMC::run (runs as in vmc_/dmc_<name>): series;
+* ``fw_dmc_<name>.json``  a DMC::run with forward walking (pure potential energy
+  and pure estimators at three lags): the run result's series and scalars;
 * ``chain_<name>.json``   a VMC::run whose final configurations seed a DMC::run
   (carry_over_walkers): DMC populations and weighted energy sums per step;
 * ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
@@ -80,6 +82,9 @@ ESTIMATE = {
 EST_VMC = {"heg10": "heg10", "dipoles16": "dipoles16"}
 EST_DMC = {"heg10": "heg10"}
 
+# Forward walking (pure estimators) on a DMC run: lags in imaginary time.
+FW = {"heg10": dict(fw_lags="0,4,8", fw_interval=1)}
+
 # VMC -> DMC stage chain: DMC seeded from VMC's final configurations.
 CHAIN = {
     "heg10": dict(nw=6, seed=11, eq=1, acc=1, steps=2, substeps=2, tau=225.0, dmc_nw=8, dmc_eq=1,
@@ -108,6 +113,16 @@ def dump(name, obj):
     with open(os.path.join(HERE, name), "w") as f:
         json.dump(obj, f, separators=(",", ":"))
     print("wrote", name)
+
+
+def fw_fixtures(only=None):
+    for name, fw in FW.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("dmc", **DMC[name], **EST[name], **fw, **SYSTEMS[name])
+        dump(f"fw_dmc_{name}.json", {"params": DMC[name], "est": EST[name], "fw": fw,
+                                     "estimators": r["estimators"], "walkers": r["walkers"],
+                                     "initial_positions": r["initial_positions"]})
 
 
 def chain_fixtures(only=None):
@@ -162,6 +177,7 @@ def main(only=None):
         dump(f"est_dmc_{name}.json", {"params": DMC[key], "est": EST[name], "estimators": r["estimators"],
                                       "walkers": r["walkers"], "final_positions": r["final_positions"]})
     chain_fixtures(only)
+    fw_fixtures(only)
     for name, run in DMC_STAT.items():
         if only and name not in only:
             continue

@@ -58,7 +58,7 @@ def compare(out, ref, tol, skip=()):
             continue
         rv = np.array(ref[k], dtype=float)
         v = np.asarray(v, dtype=float)
-        if k.startswith("rhok") or k in ("sofk_kx", "sofk_ky", "sofk_shell"):
+        if k.startswith("rhok") or (k.startswith("sofk") and k.rsplit("_", 1)[-1] in ("kx", "ky", "shell")):
             a = by_k(v, out["sofk_kx"], out["sofk_ky"])
             b = by_k(rv, ref["sofk_kx"], ref["sofk_ky"])
             assert a.keys() == b.keys(), k
