@@ -122,6 +122,17 @@ def pack_system(desc: Dict[str, Any]):
                 T.kset.kx = _dp(f64(im["kx"]))
                 T.kset.ky = _dp(f64(im["ky"]))
                 T.kset.weight = _dp(f64(im["weight"]))
+            opts = t.get("opt", [])
+            T.n_opt = len(opts)
+            for q, o in enumerate(opts):
+                T.opt_index[q] = int(o["index"])
+                if im:
+                    T.opt_inf[q] = float(o["inf"])
+                    sp = o["spline"]
+                    S = T.opt_short_range[q]
+                    S.r_cut, S.inv_delta, S.n_knots = float(sp["r_cut"]), float(sp["inv_delta"]), int(sp["n_knots"])
+                    S.scaled = _dp(f64(sp["scaled"]))
+                    T.opt_weight[q] = _dp(f64(o["weight"]))
         elif kind == "zero_energy":
             T.kind = _capi.PAIR_ZERO_ENERGY
             T.n_pairs = 1
@@ -144,6 +155,10 @@ def pack_system(desc: Dict[str, Any]):
             T.n_coeffs = len(t["coeffs"])
             for k, v in enumerate(t["coeffs"]):
                 T.dcoeffs[k] = float(v)
+            opts = t.get("opt", [])
+            T.n_opt = len(opts)
+            for q, o in enumerate(opts):
+                T.opt_index[q] = int(o["index"])
     ew = desc.get("ewald")
     if ew:
         E = s.ewald
@@ -446,6 +461,16 @@ class Walkers:
         return _est.finalize_sofk(flat, groups, self.estimator_kvectors(i))
 
     # ── forward walking (pure estimators of a DMC run) ─────────────────────
+    def parameter_derivatives(self) -> np.ndarray:
+        """O_k = d ln psi / d p_k of the pair terms' optimisable parameters,
+        [n_params][nw]."""
+        n = ctypes.c_int()
+        self._check(self.lib.alea_gpu_parameter_derivatives(self.ctx, None, ctypes.byref(n)))
+        nw = self.nw
+        out = np.zeros(max(n.value * nw, 1))
+        self._check(self.lib.alea_gpu_parameter_derivatives(self.ctx, _dp(out), ctypes.byref(n)))
+        return out[:n.value * nw].reshape(n.value, nw)
+
     def set_forward_walking(self, lags: Sequence[float], interval: int = 1) -> None:
         """Lags in imaginary time (strictly increasing; empty: off)."""
         a = np.ascontiguousarray(np.asarray(lags, dtype=np.float64))

@@ -53,7 +53,9 @@ class PairTerm(ctypes.Structure):
                 ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int),
                 ("dcoeffs", ctypes.c_double * 16), ("ze_b", ctypes.c_double),
                 ("ze_exponent", ctypes.c_double), ("ze_matching_radius", ctypes.c_double),
-                ("ze_cutoff", ctypes.c_double)]
+                ("ze_cutoff", ctypes.c_double), ("n_opt", ctypes.c_int), ("opt_index", ctypes.c_int * 4),
+                ("opt_inf", ctypes.c_double * 4), ("opt_short_range", Spline * 4),
+                ("opt_weight", c_dp * 4)]
 
 
 class Ewald(ctypes.Structure):
@@ -182,6 +184,7 @@ EXPORTS = [
     "alea_gpu_estimators_start_block", "alea_gpu_estimators_accumulate", "alea_gpu_estimators_stop_block",
     "alea_gpu_estimator_info", "alea_gpu_estimator_blocks", "alea_gpu_estimator_kvectors",
     "alea_gpu_final_configurations", "alea_gpu_seed_walker_rows", "alea_gpu_carry_over",
+    "alea_gpu_parameter_derivatives",
     "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
     "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
 ]
@@ -243,6 +246,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_cancel": ([P, ctypes.c_uint64], I),
         "alea_gpu_server_destroy": ([P], I),
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
+        "alea_gpu_parameter_derivatives": ([P, c_dp, c_ip], I),
         "alea_gpu_set_forward_walking": ([P, c_dp, I, I], I),
         "alea_gpu_add_fw_estimator": ([P, I, ctypes.POINTER(EstimatorSpec), c_ip], I),
         "alea_gpu_fw_result": ([P, I, ctypes.POINTER(FwSummary), c_dp], I),

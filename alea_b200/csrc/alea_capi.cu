@@ -219,6 +219,9 @@ struct alea_gpu_ctx {
     alea_gpu::EstimatorSet* est = nullptr;      // observable estimators (alea_gpu_add_estimator)
     uint64_t fingerprint = 0;      // FNV-1a of the system's layout and tables (equal systems, equal records)
     std::vector<int> last_src;     // the last branch's map: new walker j copies old walker last_src[j]
+    std::vector<DevOpt> h_opt;     // optimisable parameters of the pair terms (device pointers patched)
+    DevOpt* d_opt = nullptr;
+    double* d_opt_out = nullptr;   // [n_opt][capacity]
     FwState* fw = nullptr;         // forward walking (alea_gpu_set_forward_walking)
 };
 
@@ -751,6 +754,38 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
             return fail(c, ALEA_ERR_INVALID, "unknown pair term");
         }
     }
+    // optimisable parameters of the pair terms (alea_gpu_parameter_derivatives)
+    c->h_opt.clear();
+    c->h_opt.reserve(static_cast<size_t>(kMaxTerms) * ALEA_GPU_MAX_OPT);
+    for (int t = 0; t < in->n_terms; ++t) {
+        const alea_gpu_pair_term& T = in->terms[t];
+        if (T.n_opt < 0 || T.n_opt > ALEA_GPU_MAX_OPT) return fail(c, ALEA_ERR_INVALID, "bad n_opt");
+        if (T.n_opt > 0 && T.kind == ALEA_PAIR_ZERO_ENERGY)
+            return fail(c, ALEA_ERR_UNSUPPORTED, "zero-energy terms have no optimisable parameters here");
+        for (int q = 0; q < T.n_opt; ++q) {
+            const int idx = T.opt_index[q];
+            const int limit = T.kind == ALEA_PAIR_PADE ? T.num_order + T.den_order : T.n_coeffs + 1;
+            if (idx < 0 || idx >= limit) return fail(c, ALEA_ERR_INVALID, "opt_index out of range");
+            c->h_opt.push_back(DevOpt{});
+            DevOpt& o = c->h_opt.back();
+            o.term = t;
+            o.index = idx;
+            if (T.kind == ALEA_PAIR_PADE && T.image_sum) {
+                const alea_gpu_spline& sp = T.opt_short_range[q];
+                if (!sp.scaled || sp.n_knots < 2 || !T.opt_weight[q])
+                    return fail(c, ALEA_ERR_INVALID, "an image-summed Padé parameter needs its breakup tables");
+                o.inf = T.opt_inf[q];
+                o.sp.r_cut = sp.r_cut;
+                o.sp.inv_delta = sp.inv_delta;
+                o.sp.n_knots = sp.n_knots;
+                put(sp.scaled, 3 * sp.n_knots * 8, reinterpret_cast<const void**>(&o.sp.scaled));
+                poly_tables.push_back(hermite_to_monomial(sp.scaled, sp.n_knots));
+                put(poly_tables.back().data(), poly_tables.back().size() * 8,
+                    reinterpret_cast<const void**>(&o.sp.poly));
+                put(T.opt_weight[q], T.kset.n_k * 8, reinterpret_cast<const void**>(&o.kw));
+            }
+        }
+    }
     // group-pair coupling masks, when every term's ranges are whole groups
     {
         auto group_at = [&](int f, int l) {
@@ -971,6 +1006,12 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));   // ar.bytes is freed on return
     for (const Patch& p : patches) *p.slot = static_cast<char*>(c->arena) + p.off;
     for (int t : ze_terms) s.terms[t].ze_cheb = bessel_dev;
+    if (!c->h_opt.empty()) {
+        CUDA_TRY(c, cudaMallocAsync(&c->d_opt, c->h_opt.size() * sizeof(DevOpt), c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_opt, c->h_opt.data(), c->h_opt.size() * sizeof(DevOpt),
+                                    cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
     return ALEA_OK;
 }
 
@@ -1227,7 +1268,7 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
     for (void* p : {static_cast<void*>(c->arena), static_cast<void*>(c->rec[0]), static_cast<void*>(c->rec[1]),
                     static_cast<void*>(c->randoms), static_cast<void*>(c->streams), static_cast<void*>(c->pairs),
                     static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
-                    static_cast<void*>(c->d_mask)})
+                    static_cast<void*>(c->d_mask), static_cast<void*>(c->d_opt), static_cast<void*>(c->d_opt_out)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
     if (c->stream) alea_gpu::est_free(c->est, c->stream);
     if (c->stream) fw_free(c);
@@ -2068,6 +2109,27 @@ int alea_gpu_estimator_kvectors(const alea_gpu_ctx* c, int id, int* n1, int* n2,
                                 int* shell_of, double* shell_k, int* shell_count) {
     if (!c) return ALEA_ERR_INVALID;
     return est_kvectors(c->est, id, n1, n2, kx, ky, shell_of, shell_k, shell_count);
+}
+
+// ───────────────────────── parameter derivatives ───────────────────────
+
+int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_params) {
+    if (!c || !n_params) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const int nopt = static_cast<int>(c->h_opt.size());
+    *n_params = nopt;
+    if (!derivs || nopt == 0 || c->nw == 0) return ALEA_OK;
+    if (c->sys.np > 256) return fail(c, ALEA_ERR_UNSUPPORTED, "parameter derivatives: more than 256 particles");
+    if (!c->d_opt_out) {
+        const size_t b = static_cast<size_t>(nopt) * c->capacity * 8;
+        if (cudaMallocAsync(&c->d_opt_out, b, c->stream) != cudaSuccess)
+            return fail(c, ALEA_ERR_NOMEM, "parameter derivatives: device allocation failed");
+    }
+    ++c->launches;
+    CUDA_TRY(c, launch_param_derivatives(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, c->d_opt_out));
+    CUDA_TRY(c, copy_out(c, derivs, c->d_opt_out, static_cast<size_t>(nopt) * c->nw * 8));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
 }
 
 // ───────────────────────── forward walking API ─────────────────────────

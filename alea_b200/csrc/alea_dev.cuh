@@ -57,6 +57,17 @@ struct DevTerm {
     const double* ze_cheb;
 };
 
+// One optimisable parameter of a pair term (alea_gpu_pair_term n_opt /
+// opt_index): the term, which coefficient, and for an image-summed Padé the
+// breakup of du/dp - inf (spline and k weights on the shared Jastrow k set).
+struct DevOpt {
+    int term;
+    int index;
+    double inf;
+    DevSpline sp;
+    const double* kw;
+};
+
 struct DevBlock {
     int first, last, n, type;  // type 0 plane waves, 1 Gaussians, 2 twisted plane waves
     const double* k;          // plane waves [n*dim]; twisted: q = k + θ

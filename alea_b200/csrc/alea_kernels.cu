@@ -25,6 +25,111 @@ __global__ void __launch_bounds__(NT) evaluate_kernel(DevSys s, double* records,
     store_hot<NT>(s, rec, sm);
 }
 
+// d u / d p of parameter `o` of its term at pair distance r: Padé
+// du/da_k = r^k / Q, du/db_k = -P r^k / Q^2 (pade_jastrow.cpp:208-213);
+// Drummond u = (r - L)^C (alpha_0 + alpha_1 r + sum_l alpha_l r^l) below L with
+// alpha_1 = Gamma / (-L)^C + alpha_0 C / L (drummond_jastrow.cpp:201-320).
+__device__ double dudp(const DevTerm& T, const DevOpt& o, double r) {
+    if (T.kind == 0) {
+        double P = 0.0, Q = 1.0, rk = 1.0;
+        for (int k = 0; k < T.nnum; ++k) {
+            rk *= r;
+            P = fma(T.coef[k], rk, P);
+        }
+        rk = 1.0;
+        for (int k = 0; k < T.nden; ++k) {
+            rk *= r;
+            Q = fma(T.coef[T.nnum + k], rk, Q);
+        }
+        if (o.index < T.nnum) {
+            double rp = 1.0;
+            for (int k = 0; k <= o.index; ++k) rp *= r;
+            return rp / Q;
+        }
+        double rp = 1.0;
+        for (int k = 0; k <= o.index - T.nnum; ++k) rp *= r;
+        return -P * rp / (Q * Q);
+    }
+    // Drummond
+    if (r >= T.L) return 0.0;
+    const double d = r - T.L;
+    double g = 1.0;   // (r - L)^C
+    for (int i = 0; i < T.C; ++i) g *= d;
+    const double C = static_cast<double>(T.C);
+    if (o.index == 0) return g * fma(C / T.L, r, 1.0);
+    if (o.index < T.ncoef) {
+        double rp = 1.0;
+        for (int k = 0; k <= o.index; ++k) rp *= r;   // alpha_{index+1} r^{index+1}
+        return g * rp;
+    }
+    // the cutoff L: d/dL of (r - L)^C P(r) with alpha_1(L)
+    double P = T.dc[0] + T.alpha1 * r, rp = r;
+    for (int k = 1; k < T.ncoef; ++k) {
+        rp *= r;
+        P = fma(T.dc[k], rp, P);
+    }
+    double gm1 = 1.0;
+    for (int i = 0; i + 1 < T.C; ++i) gm1 *= d;
+    double ipw = 1.0;
+    for (int i = 0; i < T.C + 1; ++i) ipw *= -T.L;
+    const double dalpha1 = T.gamma * C / ipw - T.dc[0] * C / (T.L * T.L);
+    return -C * gm1 * P + g * dalpha1 * r;
+}
+
+// O_q = d ln psi / d p_q of every optimisable parameter for one walker: the
+// pair sum of du/dp over the term's pairs (minus, for an image sum, the
+// breakup's long-range part and limit inside r_cut, zero outside) plus the
+// image sum's k-space part, sum_k w'_k |rho_a|^2 or 2 Re rho_a rho_b*
+// (kspace_pair_sum.cpp:109-122, :303-313).
+template <int NT>
+__global__ void __launch_bounds__(NT) param_kernel(DevSys s, const double* records, int nw, const DevOpt* opts,
+                                                   int nopt, double* out) {
+    __shared__ double pos[2 * 256];
+    __shared__ double red[NT];
+    const int w = blockIdx.x;
+    if (w >= nw || s.np > 256) return;
+    const double* rec = records + static_cast<long>(w) * s.rec;
+    for (int i = threadIdx.x; i < s.np * 2; i += NT) pos[i] = rec[s.o_pos + i];
+    __syncthreads();
+    for (int q = 0; q < nopt; ++q) {
+        const DevOpt& o = opts[q];
+        const DevTerm& T = s.terms[o.term];
+        double acc = 0.0;
+        for (int pp = 0; pp < T.npairs; ++pp) {
+            const int af = T.pairs[pp][0], al = T.pairs[pp][1], bf = T.pairs[pp][2], bl = T.pairs[pp][3];
+            const bool same = af == bf && al == bl;
+            const int na = al - af, nb = bl - bf;
+            const int tot = na * nb;
+            for (int e = threadIdx.x; e < tot; e += NT) {
+                const int i = af + e / nb, j = bf + e % nb;
+                if (same && j <= i) continue;
+                double del[3];
+                const double r = fold_dist(s, pos + i * 2, pos + j * 2, del);
+                double v = dudp(T, o, r);
+                if (T.image) v = r < o.sp.r_cut ? v - (o.inf + spline1(o.sp, r)) : 0.0;
+                acc += v;
+            }
+        }
+        if (T.image) {
+            const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+            const double* ra = rec + s.o_rho + 2 * ga * s.nkJ;
+            const double* rb = rec + s.o_rho + 2 * gb * s.nkJ;
+            for (int k = threadIdx.x; k < s.nkJ; k += NT) {
+                if (T.same0) acc += o.kw[k] * (ra[k] * ra[k] + ra[s.nkJ + k] * ra[s.nkJ + k]);
+                else acc += 2.0 * o.kw[k] * (ra[k] * rb[k] + ra[s.nkJ + k] * rb[s.nkJ + k]);
+            }
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int h = NT / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[static_cast<long>(q) * nw + w] = red[0];
+        __syncthreads();
+    }
+}
+
 // Potential energy of stored configurations (Hamiltonian::evaluate_potential,
 // src/hamiltonian/hamiltonian_component.h:165-403): configuration c is
 // rows[idx[c]] (positions [np][2]); the local energy's potential terms with
@@ -262,6 +367,13 @@ cudaError_t reserve_smem(size_t smem) {
     if (e == cudaSuccess) e = reserve_smem_f32(smem);
     if (e == cudaSuccess) reserved[dev] = smem;
     return e;
+}
+
+cudaError_t launch_param_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
+                                     const DevOpt* opts, int nopt, double* out) {
+    if (nw < 1 || nopt < 1) return cudaSuccess;
+    param_kernel<128><<<nw, 128, 0, st>>>(s, records, nw, opts, nopt, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_potential(int nt, int n, size_t smem, cudaStream_t st, const DevSys& s, const double* rows,

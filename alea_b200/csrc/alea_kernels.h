@@ -22,6 +22,9 @@ struct SweepParams {
 cudaError_t reserve_smem(size_t smem);
 cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const DevSys& s,
                             double* records, const int2* pairs, int npair);
+// d ln psi / d p of the nopt optimisable parameters for nw walkers, out [nopt][nw].
+cudaError_t launch_param_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
+                                     const DevOpt* opts, int nopt, double* out);
 // Potential energy of n stored configurations rows[idx[c]] into out[c].
 cudaError_t launch_potential(int nt, int n, size_t smem, cudaStream_t st, const DevSys& s, const double* rows,
                              const int* idx, const int2* pairs, int npair, double* out);

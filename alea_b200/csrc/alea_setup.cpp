@@ -899,6 +899,21 @@ void write_json(alea_gpu_setup* S, const std::string& kind, double ewald_self, d
             json_kset(j, T.kset);
             j.close('}');
         }
+        if (T.n_opt > 0) {
+            j.key("opt");
+            j.open('[');
+            for (int q = 0; q < T.n_opt; ++q) {
+                j.open('{');
+                j.kv("index", T.opt_index[q]);
+                if (T.image_sum) {
+                    j.kv("inf", T.opt_inf[q]);
+                    json_spline(j, "spline", T.opt_short_range[q]);
+                    j.arr("weight", std::vector<double>(T.opt_weight[q], T.opt_weight[q] + T.kset.n_k));
+                }
+                j.close('}');
+            }
+            j.close(']');
+        }
         j.close('}');
     }
     j.close(']');
@@ -1083,10 +1098,18 @@ static int setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pa
                 int same = -1;
                 for (int q = 0; q + 1 < y.n_terms; ++q)
                     if (y.terms[q].coeffs[0] == a1) same = q;
+                // the denominator b is the term's optimisable parameter (a_1 is
+                // fixed by the cusp): the breakup of du/db = -a_1 r^2 / Q^2 on the
+                // same options (src/wavefunction/pade_jastrow.cpp:214-248)
+                T.n_opt = 1;
+                T.opt_index[0] = 1;
                 if (same >= 0) {
                     T.short_range = y.terms[same].short_range;
                     T.u_inf = y.terms[same].u_inf;
                     T.kset = y.terms[same].kset;
+                    T.opt_inf[0] = y.terms[same].opt_inf[0];
+                    T.opt_short_range[0] = y.terms[same].opt_short_range[0];
+                    T.opt_weight[0] = y.terms[same].opt_weight[0];
                     continue;
                 }
                 double u_inf = 0.0;
@@ -1094,6 +1117,13 @@ static int setup_heg2d(int n_up, int n_down, double rs, double pade_b, double pa
                 set_spline(S, T.short_range, br);
                 T.u_inf = u_inf;
                 set_kset(S, T.kset, br);
+                double d_inf = 0.0;
+                const Breakup bp = pade_breakup(c, {0.0, -a1}, {2.0 * pade_b, pade_b * pade_b}, d_inf);
+                if (bp.weight.size() != br.weight.size())
+                    throw std::logic_error("heg2d: the parameter breakup's k set differs");
+                T.opt_inf[0] = d_inf;
+                set_spline(S, T.opt_short_range[0], bp);
+                T.opt_weight[0] = S->keep(bp.weight);
             }
         write_json(S, "heg", self, bg);
     } catch (const std::exception& e) {

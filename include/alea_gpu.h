@@ -65,6 +65,7 @@ enum { ALEA_PAIR_PADE = 0, ALEA_PAIR_DRUMMOND = 1, ALEA_PAIR_ZERO_ENERGY = 2 };
 #define ALEA_GPU_MAX_TERMS 8
 #define ALEA_GPU_MAX_PAIRS 4
 #define ALEA_GPU_MAX_COULOMB 8
+#define ALEA_GPU_MAX_OPT 4
 
 /* Quintic-Hermite long-range spline of the optimized breakup
  * (src/numerics/long_range_spline.h:41-48): 3 coefficients per knot, scaled
@@ -130,6 +131,19 @@ typedef struct {
     double ze_b;                            /* 2 mu C of the pair's C/r^p core */
     double ze_exponent;                     /* p > 2 */
     double ze_matching_radius, ze_cutoff;
+    /* The term's optimisable parameters, in the order of its Parameter list
+       (the linear method's, WavefunctionComponent::compute_parameter_derivatives,
+       src/wavefunction/wavefunction_component.h:165-171).  opt_index: Padé, the
+       index into coeffs (a_1..a_N, then b_1..b_M); Drummond, 0 = alpha_0,
+       i = alpha_{i+1} for 1 <= i < n_coeffs, n_coeffs = the cutoff L.  An
+       image-summed Padé also carries, per parameter, the breakup of
+       du/dp - its r -> infinity limit on the term's k set
+       (src/wavefunction/pade_jastrow.cpp:208-248). */
+    int n_opt;
+    int opt_index[ALEA_GPU_MAX_OPT];
+    double opt_inf[ALEA_GPU_MAX_OPT];
+    alea_gpu_spline opt_short_range[ALEA_GPU_MAX_OPT];
+    const double* opt_weight[ALEA_GPU_MAX_OPT];   /* [kset.n_k] */
 } alea_gpu_pair_term;
 
 /* 2-D Ewald sum of the Coulomb interaction (src/hamiltonian/ewald_term.h). */
@@ -359,6 +373,22 @@ int alea_gpu_transfer_bytes(const alea_gpu_ctx* ctx, uint64_t* h2d, uint64_t* d2
 /* Kernels this context has launched so far (instrumentation; no counterpart
  * in the reference). */
 int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
+
+/* ───────────────────────── parameter derivatives ───────────────────────
+ *
+ * O_k = d ln psi / d p_k of every optimisable parameter of the pair Jastrow
+ * terms (their n_opt / opt_index), for every walker: what the linear method
+ * samples (TrialWavefunction::compute_parameter_derivatives,
+ * src/wavefunction/trial_wavefunction.h:104-114; PadeJastrow,
+ * src/wavefunction/pade_jastrow.cpp:641-800 with its image sum,
+ * periodic_pair_sum.cpp:80-92 and kspace_pair_sum.cpp:303-313;
+ * DrummondJastrow, src/wavefunction/drummond_jastrow.cpp:201-320).
+ * derivs [n_params][nw] in term order, parameter order within a term;
+ * *n_params receives their number (derivs may be NULL to ask for it).  The
+ * walkers must be evaluated (after upload, a step or alea_gpu_measure).
+ * Orbital (Slater) and backflow parameters and the derivatives of the
+ * gradient and Laplacian are not computed here. */
+int alea_gpu_parameter_derivatives(alea_gpu_ctx* ctx, double* derivs, int* n_params);
 
 /* ───────────────────────── configurations and carry-over ───────────────
  *

@@ -234,6 +234,51 @@ void dump_pade_image_sum(Json& j, const SimulationCell& cell, const std::vector<
     j.close('}');
 }
 
+// The optimisable parameters' breakups of an image-summed Padé, with the
+// calls of PadeJastrow::build_image_sum (src/wavefunction/pade_jastrow.cpp:
+// 214-248): du/da_k = r^k/Q, du/db_k = -P r^k/Q^2, each split on the same
+// options.  free[i] marks parameter i of [a_1..a_N, b_1..b_M] as optimisable.
+void dump_pade_opt(Json& j, const SimulationCell& cell, const std::vector<double>& a,
+                   const std::vector<double>& b, const std::vector<bool>& free) {
+    const double rc = cell.ws_radius();
+    numerics::BreakupOptions opt{};
+    opt.k_continuum = 20.0 * 3.14159265358979323846 / rc;
+    opt.k_max = 300.0 / rc;
+    opt.n_continuum = 150;
+    opt.k_cut = 5.0 * std::min(std::hypot(cell.reciprocal()[0], cell.reciprocal()[1]),
+                               std::hypot(cell.reciprocal()[2], cell.reciprocal()[3]));
+    std::vector<double> q2(2 * b.size(), 0.0);
+    for (std::size_t jj = 0; jj < b.size(); ++jj) {
+        q2[jj] += 2.0 * b[jj];
+        for (std::size_t l = 0; l < b.size(); ++l) q2[jj + l + 1] += b[jj] * b[l];
+    }
+    j.key("opt");
+    j.open('[');
+    for (std::size_t i = 0; i < free.size(); ++i) {
+        if (!free[i]) continue;
+        std::vector<double> num, den;
+        if (i < a.size()) {
+            num.assign(i + 1, 0.0);
+            num[i] = 1.0;
+            den = b;
+        } else {
+            const std::size_t k = i - a.size() + 1;
+            num.assign(a.size() + k, 0.0);
+            for (std::size_t jj = 0; jj < a.size(); ++jj) num[jj + k] = -a[jj];
+            den = q2;
+        }
+        const numerics::LongRangeBreakup bp =
+            numerics::build_long_range_breakup(cell, numerics::pade_radial(num, den, rc), opt);
+        j.open('{');
+        j.ki("index", static_cast<long long>(i));
+        j.kv("inf", numerics::pade_limit(num, den));
+        dump_spline(j, "spline", bp.spline());
+        j.arr("weight", bp.weight());
+        j.close('}');
+    }
+    j.close(']');
+}
+
 // ── systems ─────────────────────────────────────────────────────────────────
 
 // 2D homogeneous electron gas: plane-wave determinants per spin, image-summed
@@ -397,6 +442,7 @@ std::unique_ptr<System> build_heg(const Args& a) {
             j.arr("a", std::vector<double>{a1});
             j.arr("b", std::vector<double>{bden});
             dump_pade_image_sum(j, s->cell, {a1}, {bden});
+            dump_pade_opt(j, s->cell, {a1}, {bden}, {false, true});
             j.close('}');
             s->psi.add_component(std::move(pj));
         }
@@ -788,6 +834,15 @@ int run(const std::string& mode, const Args& a) {
         out.key("component_log_psi");
         out.open('[');
         for (const auto& c : psi.components()) out.arr("", c->log_psi_c());
+        out.close(']');
+        // d ln psi_c / d p_k of every component's optimisable parameters
+        out.key("param_derivs");
+        out.open('[');
+        for (const auto& c : psi.components()) {
+            std::vector<double> d(c->num_optimizable_params() * nw);
+            if (!d.empty()) c->compute_parameter_derivatives(ws, d);
+            out.arr("", d);
+        }
         out.close(']');
         // Kinetic alone, to separate the potential.
         Hamiltonian kin;

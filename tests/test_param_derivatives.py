@@ -1,0 +1,50 @@
+"""d ln psi / d p of the pair Jastrows' optimisable parameters (the linear
+method's O_k), through the C ABI, against the compiled reference's
+compute_parameter_derivatives on the same walkers (eval fixtures: the
+reference's App walkers, seed 12345).
+
+The electron gases' image-summed Padé terms each carry one optimisable
+parameter (b; a_1 is fixed by the cusp): the short-range sum of du/db minus
+its breakup, plus the k-space part from each walker's rho(k).  Tolerance 1e-10
+relative to the largest |O_k|; after VMC steps (rho(k) updated move by move)
+the derivatives equal those of a fresh evaluation of the same positions.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+SYSTEMS = ["heg10", "heg42", "heg10t", "heg10bf"]
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_parameter_derivatives_match_reference(name):
+    import alea_b200
+    setup = golden(f"setup_{name}.json")
+    ev = golden(f"eval_{name}.json")
+    pos = np.array(ev["positions"])
+    g = alea_b200.Walkers(setup, capacity=8)
+    g.upload(pos)
+    got = g.parameter_derivatives()
+    # components: the determinant, then one Padé term per spin pair
+    want = np.concatenate([np.array(d).reshape(-1, len(pos)) for d in ev["param_derivs"][1:]])
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) <= 1e-10 * np.abs(want).max()
+
+
+def test_parameter_derivatives_follow_the_walk():
+    import alea_b200
+    setup = golden("setup_heg10.json")
+    pos = np.array(golden("eval_heg10.json")["positions"])
+    g = alea_b200.Walkers(setup, capacity=8)
+    g.upload(pos)
+    g.set_streams(9, alea_b200.STREAM_VMC, 4)
+    for _ in range(3):
+        g.vmc_step(225.0, 2)
+    moved = g.parameter_derivatives()
+    f = alea_b200.Walkers(setup, capacity=8)
+    f.upload(g.download()["positions"].reshape(len(pos), -1, 2))
+    fresh = f.parameter_derivatives()
+    assert np.max(np.abs(moved - fresh)) <= 1e-10 * np.abs(fresh).max()

@@ -97,6 +97,20 @@ def test_breakup_tables(case):
         assert d["ewald"]["self_energy"] == pytest.approx(g["ewald"]["self_energy"], rel=TABLE_RTOL)
 
 
+def test_parameter_breakup_tables(case):
+    """The optimisable Padé parameter (b) of each image-summed term: its
+    index, du/db's limit and the breakup of du/db - limit on the same k set
+    (PadeJastrow::build_image_sum, pade_jastrow.cpp:214-248)."""
+    name, s, ref = case
+    for mine, theirs in zip(s.desc.get("pade", []), ref.get("pade", [])):
+        assert len(mine.get("opt", [])) == len(theirs.get("opt", []))
+        for o, r in zip(mine.get("opt", []), theirs.get("opt", [])):
+            assert int(o["index"]) == int(r["index"])
+            assert abs(o["inf"] - r["inf"]) <= 1e-12 * abs(r["inf"])
+            _close(o["weight"], r["weight"], TABLE_RTOL)
+            _close(o["spline"]["scaled"], r["spline"]["scaled"], TABLE_RTOL)
+
+
 def test_local_energy_matches_reference_tables(case):
     from oracle import Oracle
     name, s, g = case
