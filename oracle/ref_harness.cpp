@@ -555,14 +555,30 @@ std::unique_ptr<System> build_crystal(const Args& a) {
         }
         const double R = ew.coulomb_cusp_residue(pairs[0].a, pairs[0].b);
         const double gamma = 2.0 * 0.5 * R / static_cast<double>(2 * (item == 0 ? 1 : 0) + 1);
-        std::vector<Parameter> params{Parameter{"p0", alpha0, true},
-                                      Parameter{"L", Lcut, true, true}};
+        // drummond_free=1: alpha_0, an alpha_2 term and L optimisable (the
+        // linear method's parameters); otherwise alpha_0 and L fixed
+        const bool dfree = geti(a, "drummond_free", 0) != 0;
+        const double alpha2 = getd(a, "alpha2", 0.0);
+        std::vector<Parameter> params{Parameter{"p0", alpha0, !dfree}};
+        if (dfree) params.push_back(Parameter{"p2", alpha2, false});
+        params.push_back(Parameter{"L", Lcut, !dfree, true});
         auto dj = std::make_unique<DrummondJastrow>(3, gamma, pairs, params);
         j.open('{');
         j.ki("C", 3);
         j.kv("gamma", gamma);
         j.kv("L", Lcut);
-        j.arr("coeffs", std::vector<double>{alpha0});
+        if (dfree) j.arr("coeffs", std::vector<double>{alpha0, alpha2});
+        else j.arr("coeffs", std::vector<double>{alpha0});
+        if (dfree) {
+            j.key("opt");
+            j.open('[');
+            for (int q = 0; q < 3; ++q) {
+                j.open('{');
+                j.ki("index", q);
+                j.close('}');
+            }
+            j.close(']');
+        }
         j.key("pairs");
         j.open('[');
         for (const auto& p : pairs)

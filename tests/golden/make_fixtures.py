@@ -47,6 +47,9 @@ SYSTEMS = {
     "dipoles16": dict(system="dipoles", n=16),
     "heg10t": dict(system="heg", nu=5, nd=5, rs=30, tx=0.25, ty=0.125),
     "heg10bf": dict(system="heg", nu=5, nd=5, rs=30, bf=1),
+    # the crystal with its Drummond alpha_0, an alpha_2 term and L optimisable
+    "crystal16p": dict(system="crystal", nx=4, ny=4, rs=40, drummond_free=1, alpha0=-2e-3,
+                       alpha2=3e-8),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),

@@ -5,7 +5,8 @@ reference's App walkers, seed 12345).
 
 The electron gases' image-summed Padé terms each carry one optimisable
 parameter (b; a_1 is fixed by the cusp): the short-range sum of du/db minus
-its breakup, plus the k-space part from each walker's rho(k).  Tolerance 1e-10
+its breakup, plus the k-space part from each walker's rho(k).  The crystal
+variant frees its Drummond alpha_0, an alpha_2 term and the cutoff L.  Tolerance 1e-10
 relative to the largest |O_k|; after VMC steps (rho(k) updated move by move)
 the derivatives equal those of a fresh evaluation of the same positions.
 """
@@ -16,7 +17,7 @@ from conftest import golden
 
 pytestmark = pytest.mark.gpu
 
-SYSTEMS = ["heg10", "heg42", "heg10t", "heg10bf"]
+SYSTEMS = ["heg10", "heg42", "heg10t", "heg10bf", "crystal16p"]
 
 
 @pytest.mark.parametrize("name", SYSTEMS)
@@ -28,8 +29,11 @@ def test_parameter_derivatives_match_reference(name):
     g = alea_b200.Walkers(setup, capacity=8)
     g.upload(pos)
     got = g.parameter_derivatives()
-    # components: the determinant, then one Padé term per spin pair
-    want = np.concatenate([np.array(d).reshape(-1, len(pos)) for d in ev["param_derivs"][1:]])
+    # components: the determinant(s), then the pair terms (Padé per spin pair,
+    # or the crystal's two Drummond items)
+    n_terms = len(setup.get("pade", [])) + len(setup.get("drummond", []))
+    terms = ev["param_derivs"][-n_terms:]
+    want = np.concatenate([np.array(d).reshape(-1, len(pos)) for d in terms])
     assert got.shape == want.shape
     assert np.max(np.abs(got - want)) <= 1e-10 * np.abs(want).max()
 
