@@ -471,6 +471,17 @@ class Walkers:
         self._check(self.lib.alea_gpu_parameter_derivatives(self.ctx, _dp(out), ctypes.byref(n)))
         return out[:n.value * nw].reshape(n.value, nw)
 
+    def parameter_gradient_derivatives(self):
+        """(dgrad, dlap), each [n_params][np*dim][nw]: the parameters'
+        derivatives of grad ln psi and of the per-dimension Laplacians."""
+        n = ctypes.c_int()
+        self._check(self.lib.alea_gpu_parameter_gradient_derivatives(self.ctx, None, None, ctypes.byref(n)))
+        nw, m = self.nw, self.np * self.dim
+        g, l = np.zeros(max(n.value * m * nw, 1)), np.zeros(max(n.value * m * nw, 1))
+        self._check(self.lib.alea_gpu_parameter_gradient_derivatives(self.ctx, _dp(g), _dp(l), ctypes.byref(n)))
+        k = n.value * m * nw
+        return g[:k].reshape(n.value, m, nw), l[:k].reshape(n.value, m, nw)
+
     def set_forward_walking(self, lags: Sequence[float], interval: int = 1) -> None:
         """Lags in imaginary time (strictly increasing; empty: off)."""
         a = np.ascontiguousarray(np.asarray(lags, dtype=np.float64))

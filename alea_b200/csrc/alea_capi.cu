@@ -222,6 +222,7 @@ struct alea_gpu_ctx {
     std::vector<DevOpt> h_opt;     // optimisable parameters of the pair terms (device pointers patched)
     DevOpt* d_opt = nullptr;
     double* d_opt_out = nullptr;   // [n_opt][capacity]
+    double* d_opt_grad = nullptr;  // [n_opt][np*2][capacity] x 2 (gradient, Laplacian)
     FwState* fw = nullptr;         // forward walking (alea_gpu_set_forward_walking)
 };
 
@@ -1268,7 +1269,8 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
     for (void* p : {static_cast<void*>(c->arena), static_cast<void*>(c->rec[0]), static_cast<void*>(c->rec[1]),
                     static_cast<void*>(c->randoms), static_cast<void*>(c->streams), static_cast<void*>(c->pairs),
                     static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
-                    static_cast<void*>(c->d_mask), static_cast<void*>(c->d_opt), static_cast<void*>(c->d_opt_out)})
+                    static_cast<void*>(c->d_mask), static_cast<void*>(c->d_opt), static_cast<void*>(c->d_opt_out),
+                    static_cast<void*>(c->d_opt_grad)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
     if (c->stream) alea_gpu::est_free(c->est, c->stream);
     if (c->stream) fw_free(c);
@@ -2128,6 +2130,29 @@ int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_param
     ++c->launches;
     CUDA_TRY(c, launch_param_derivatives(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, c->d_opt_out));
     CUDA_TRY(c, copy_out(c, derivs, c->d_opt_out, static_cast<size_t>(nopt) * c->nw * 8));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
+}
+
+int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, double* dlap, int* n_params) {
+    if (!c || !n_params) return ALEA_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const int nopt = static_cast<int>(c->h_opt.size());
+    *n_params = nopt;
+    if ((!dgrad && !dlap) || nopt == 0 || c->nw == 0) return ALEA_OK;
+    if (c->sys.np > 256) return fail(c, ALEA_ERR_UNSUPPORTED, "parameter derivatives: more than 256 particles");
+    const size_t cap = static_cast<size_t>(nopt) * c->sys.np * 2 * c->capacity;
+    if (!c->d_opt_grad && cudaMallocAsync(&c->d_opt_grad, 2 * cap * 8, c->stream) != cudaSuccess)
+        return fail(c, ALEA_ERR_NOMEM, "parameter derivatives: device allocation failed");
+    const size_t n = static_cast<size_t>(nopt) * c->sys.np * 2 * c->nw;
+    double* g = c->d_opt_grad;
+    double* l = c->d_opt_grad + cap;
+    CUDA_TRY(c, cudaMemsetAsync(g, 0, n * 8, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(l, 0, n * 8, c->stream));
+    ++c->launches;
+    CUDA_TRY(c, launch_param_grad_derivatives(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, g, l));
+    if (dgrad) CUDA_TRY(c, copy_out(c, dgrad, g, n * 8));
+    if (dlap) CUDA_TRY(c, copy_out(c, dlap, l, n * 8));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return ALEA_OK;
 }

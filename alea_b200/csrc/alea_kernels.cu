@@ -76,6 +76,180 @@ __device__ double dudp(const DevTerm& T, const DevOpt& o, double r) {
     return -C * gm1 * P + g * dalpha1 * r;
 }
 
+// d u / d p with its first and second r-derivatives (the same functions as
+// dudp): Padé by the quotient rule on N/D (N = r^k, D = Q for a_k;
+// N = -P r^k, D = Q^2 for b_k); Drummond by the product rule on
+// (r - L)^m times a polynomial.  Zero for a Drummond pair beyond L.
+__device__ void dudp3(const DevTerm& T, const DevOpt& o, double r, double& v, double& d1, double& d2) {
+    auto powi = [](double x, int n) {
+        double y = 1.0;
+        for (int i = 0; i < n; ++i) y *= x;
+        return n < 0 ? 0.0 : y;
+    };
+    if (T.kind == 0) {
+        double P = 0.0, P1 = 0.0, P2 = 0.0, Q = 1.0, Q1 = 0.0, Q2 = 0.0;
+        for (int k = 1; k <= T.nnum; ++k) {
+            const double a = T.coef[k - 1];
+            P += a * powi(r, k);
+            P1 += a * k * powi(r, k - 1);
+            P2 += a * k * (k - 1) * powi(r, k - 2);
+        }
+        for (int k = 1; k <= T.nden; ++k) {
+            const double b = T.coef[T.nnum + k - 1];
+            Q += b * powi(r, k);
+            Q1 += b * k * powi(r, k - 1);
+            Q2 += b * k * (k - 1) * powi(r, k - 2);
+        }
+        double N, N1, N2, D, D1, D2;
+        if (o.index < T.nnum) {
+            const int k = o.index + 1;
+            N = powi(r, k);
+            N1 = k * powi(r, k - 1);
+            N2 = k * (k - 1) * powi(r, k - 2);
+            D = Q;
+            D1 = Q1;
+            D2 = Q2;
+        } else {
+            const int k = o.index - T.nnum + 1;
+            const double rk = powi(r, k), rk1 = k * powi(r, k - 1), rk2 = k * (k - 1) * powi(r, k - 2);
+            N = -P * rk;
+            N1 = -(P1 * rk + P * rk1);
+            N2 = -(P2 * rk + 2.0 * P1 * rk1 + P * rk2);
+            D = Q * Q;
+            D1 = 2.0 * Q * Q1;
+            D2 = 2.0 * (Q1 * Q1 + Q * Q2);
+        }
+        v = N / D;
+        d1 = (N1 - v * D1) / D;
+        d2 = (N2 - 2.0 * d1 * D1 - v * D2) / D;
+        return;
+    }
+    v = d1 = d2 = 0.0;
+    if (r >= T.L) return;
+    const int C = T.C;
+    const double x = r - T.L;
+    // (r - L)^m and its two r-derivatives
+    auto g = [&](int m, double& g0, double& g1, double& g2) {
+        g0 = powi(x, m);
+        g1 = m * powi(x, m - 1);
+        g2 = m * (m - 1) * powi(x, m - 2);
+    };
+    auto product = [&](double a0, double a1, double a2, double b0, double b1, double b2, double s) {
+        v += s * a0 * b0;
+        d1 += s * (a1 * b0 + a0 * b1);
+        d2 += s * (a2 * b0 + 2.0 * a1 * b1 + a0 * b2);
+    };
+    double g0, g1, g2;
+    g(C, g0, g1, g2);
+    if (o.index == 0) {   // alpha_0, with alpha_1's dependence C / L
+        product(g0, g1, g2, 1.0 + C / T.L * r, C / T.L, 0.0, 1.0);
+        return;
+    }
+    if (o.index < T.ncoef) {   // alpha_l r^l, l = index + 1
+        const int l = o.index + 1;
+        product(g0, g1, g2, powi(r, l), l * powi(r, l - 1), l * (l - 1) * powi(r, l - 2), 1.0);
+        return;
+    }
+    // the cutoff L: -C (r - L)^{C-1} P(r) + (r - L)^C (d alpha_1 / dL) r
+    double P = T.dc[0] + T.alpha1 * r, P1 = T.alpha1, P2 = 0.0;
+    for (int k = 1; k < T.ncoef; ++k) {
+        const int l = k + 1;
+        P += T.dc[k] * powi(r, l);
+        P1 += T.dc[k] * l * powi(r, l - 1);
+        P2 += T.dc[k] * l * (l - 1) * powi(r, l - 2);
+    }
+    double h0, h1, h2;
+    g(C - 1, h0, h1, h2);
+    product(h0, h1, h2, P, P1, P2, -static_cast<double>(C));
+    const double ipw = powi(-T.L, C + 1);
+    const double dalpha1 = T.gamma * C / ipw - T.dc[0] * C / (T.L * T.L);
+    product(g0, g1, g2, r, 1.0, 0.0, dalpha1);
+}
+
+// d(grad ln psi)/dp_q and d(lap ln psi)/dp_q for one walker, each particle
+// on its own thread summing over its partners in the parameter's term
+// (PadeJastrow / DrummondJastrow::compute_parameter_gradient_derivatives,
+// pade_jastrow.cpp:806-880): with f1, f2 the r-derivatives of du/dp (minus the
+// image sum's long-range part inside r_cut), grad += f1 Δ/r and
+// lap += f2 (Δ/r)^2 + f1 (1 - (Δ/r)^2) / r; the image sum's k-space part
+// (kspace_pair_sum.cpp:91-107, :315-320) from the particle's phases and the
+// other side's rho(k).  Outputs [q][p*2 + d][nw]; other particles untouched.
+template <int NT>
+__global__ void __launch_bounds__(NT) param_grad_kernel(DevSys s, const double* records, int nw,
+                                                        const DevOpt* opts, int nopt, double* dgrad,
+                                                        double* dlap) {
+    __shared__ double pos[2 * 256];
+    const int w = blockIdx.x;
+    if (w >= nw || s.np > 256) return;
+    const double* rec = records + static_cast<long>(w) * s.rec;
+    for (int i = threadIdx.x; i < s.np * 2; i += NT) pos[i] = rec[s.o_pos + i];
+    __syncthreads();
+    const long plane = static_cast<long>(s.np) * 2 * nw;
+    for (int q = 0; q < nopt; ++q) {
+        const DevOpt& o = opts[q];
+        const DevTerm& T = s.terms[o.term];
+        for (int i = threadIdx.x; i < s.np; i += NT) {
+            double gx = 0.0, gy = 0.0, lx = 0.0, ly = 0.0;
+            bool touched = false;
+            for (int pp = 0; pp < T.npairs; ++pp) {
+                const int af = T.pairs[pp][0], al = T.pairs[pp][1], bf = T.pairs[pp][2], bl = T.pairs[pp][3];
+                const bool same = af == bf && al == bl;
+                const bool in_a = i >= af && i < al, in_b = i >= bf && i < bl;
+                for (int side = 0; side < 2; ++side) {
+                    if (side == 0 ? !in_a : (same || !in_b)) continue;
+                    touched = true;
+                    const int jf = side == 0 ? bf : af, jl = side == 0 ? bl : al;
+                    for (int j = jf; j < jl; ++j) {
+                        if (j == i) continue;
+                        double del[3];
+                        const double r = fold_dist(s, pos + i * 2, pos + j * 2, del);
+                        double v, f1, f2;
+                        dudp3(T, o, r, v, f1, f2);
+                        if (T.image) {
+                            if (r >= o.sp.r_cut) continue;
+                            double f, df, d2f;
+                            spline3(o.sp, r, f, df, d2f);
+                            f1 -= df;
+                            f2 -= d2f;
+                        }
+                        const double inv_r = 1.0 / r;
+                        const double ox = del[0] * inv_r, oy = del[1] * inv_r;
+                        gx += f1 * ox;
+                        gy += f1 * oy;
+                        lx += f2 * ox * ox + f1 * inv_r * (1.0 - ox * ox);
+                        ly += f2 * oy * oy + f1 * inv_r * (1.0 - oy * oy);
+                    }
+                }
+            }
+            if (T.image && touched) {
+                const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
+                const bool in_a = i >= T.pairs[0][0] && i < T.pairs[0][1];
+                const int go = T.same0 ? ga : (in_a ? gb : ga);
+                const double self = T.same0 ? 1.0 : 0.0;
+                const double* pr = rec + s.o_rho + 2 * go * s.nkJ;
+                const double* pi = pr + s.nkJ;
+                const double x = pos[i * 2], y = pos[i * 2 + 1];
+                for (int k = 0; k < s.nkJ; ++k) {
+                    double sn, c;
+                    sincos(s.kxJ[k] * x + s.kyJ[k] * y, &sn, &c);
+                    const double gk = 2.0 * o.kw[k] * (c * pi[k] - sn * pr[k]);
+                    const double lk = 2.0 * o.kw[k] * (self - (c * pr[k] + sn * pi[k]));
+                    gx += s.kxJ[k] * gk;
+                    gy += s.kyJ[k] * gk;
+                    lx += s.kx2J[k] * lk;
+                    ly += s.ky2J[k] * lk;
+                }
+            }
+            if (!touched) continue;
+            const long base = q * plane + static_cast<long>(i) * 2 * nw + w;
+            dgrad[base] = gx;
+            dgrad[base + nw] = gy;
+            dlap[base] = lx;
+            dlap[base + nw] = ly;
+        }
+    }
+}
+
 // O_q = d ln psi / d p_q of every optimisable parameter for one walker: the
 // pair sum of du/dp over the term's pairs (minus, for an image sum, the
 // breakup's long-range part and limit inside r_cut, zero outside) plus the
@@ -373,6 +547,13 @@ cudaError_t launch_param_derivatives(int nw, cudaStream_t st, const DevSys& s, c
                                      const DevOpt* opts, int nopt, double* out) {
     if (nw < 1 || nopt < 1) return cudaSuccess;
     param_kernel<128><<<nw, 128, 0, st>>>(s, records, nw, opts, nopt, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_param_grad_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
+                                          const DevOpt* opts, int nopt, double* dgrad, double* dlap) {
+    if (nw < 1 || nopt < 1) return cudaSuccess;
+    param_grad_kernel<64><<<nw, 64, 0, st>>>(s, records, nw, opts, nopt, dgrad, dlap);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,10 @@ cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const 
 // d ln psi / d p of the nopt optimisable parameters for nw walkers, out [nopt][nw].
 cudaError_t launch_param_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
                                      const DevOpt* opts, int nopt, double* out);
+// d(grad ln psi)/dp and d(lap ln psi)/dp of the nopt parameters, [nopt][np*2][nw]
+// each; entries of particles outside a parameter's term are left as they are.
+cudaError_t launch_param_grad_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
+                                          const DevOpt* opts, int nopt, double* dgrad, double* dlap);
 // Potential energy of n stored configurations rows[idx[c]] into out[c].
 cudaError_t launch_potential(int nt, int n, size_t smem, cudaStream_t st, const DevSys& s, const double* rows,
                              const int* idx, const int2* pairs, int npair, double* out);

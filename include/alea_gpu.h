@@ -386,9 +386,16 @@ int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
  * derivs [n_params][nw] in term order, parameter order within a term;
  * *n_params receives their number (derivs may be NULL to ask for it).  The
  * walkers must be evaluated (after upload, a step or alea_gpu_measure).
- * Orbital (Slater) and backflow parameters and the derivatives of the
- * gradient and Laplacian are not computed here. */
+ * Orbital (Slater) and backflow parameters are not computed here. */
 int alea_gpu_parameter_derivatives(alea_gpu_ctx* ctx, double* derivs, int* n_params);
+/* d(grad_d ln psi)/d p_k and d(lap_d ln psi)/d p_k of the same parameters,
+ * [n_params][n_particles * dim][nw] each (the gradient planes' layout per
+ * parameter): the curvature term of the linear method's Hbar
+ * (compute_parameter_gradient_derivatives,
+ * src/wavefunction/wavefunction_component.h:173-191; Padé
+ * src/wavefunction/pade_jastrow.cpp:806-880 with the image sum's
+ * kspace_pair_sum.cpp:315-320).  Either output may be NULL. */
+int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* ctx, double* dgrad, double* dlap, int* n_params);
 
 /* ───────────────────────── configurations and carry-over ───────────────
  *

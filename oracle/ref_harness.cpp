@@ -860,6 +860,22 @@ int run(const std::string& mode, const Args& a) {
             out.arr("", d);
         }
         out.close(']');
+        // d(grad_d ln psi_c)/d p_k and d(lap_d ln psi_c)/d p_k, [n_opt][np*dim*nw]
+        // per component (empty when the component does not supply them)
+        out.key("param_grad_derivs");
+        out.open('[');
+        for (const auto& c : psi.components()) {
+            const std::size_t n = c->num_optimizable_params() * sys->np * sys->dim * nw;
+            std::vector<double> dg(n), dl(n);
+            const bool ok = n > 0 && c->supports_parameter_gradient_derivatives() &&
+                            c->compute_parameter_gradient_derivatives(ws, dg, dl);
+            out.open('{');
+            out.ki("ok", ok ? 1 : 0);
+            out.arr("grad", ok ? dg : std::vector<double>{});
+            out.arr("lap", ok ? dl : std::vector<double>{});
+            out.close('}');
+        }
+        out.close(']');
         // Kinetic alone, to separate the potential.
         Hamiltonian kin;
         kin.add_component(std::make_unique<Kinetic>(sys->groups));

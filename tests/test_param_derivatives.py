@@ -52,3 +52,25 @@ def test_parameter_derivatives_follow_the_walk():
     f.upload(g.download()["positions"].reshape(len(pos), -1, 2))
     fresh = f.parameter_derivatives()
     assert np.max(np.abs(moved - fresh)) <= 1e-10 * np.abs(fresh).max()
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_parameter_gradient_derivatives_match_reference(name):
+    """d(grad ln psi)/dp and d(lap ln psi)/dp (the linear method's curvature
+    term) against compute_parameter_gradient_derivatives, 1e-9 relative."""
+    import alea_b200
+    setup = golden(f"setup_{name}.json")
+    ev = golden(f"eval_{name}.json")
+    pos = np.array(ev["positions"])
+    nw, m = len(pos), int(setup["np"]) * int(setup["dim"])
+    g = alea_b200.Walkers(setup, capacity=8)
+    g.upload(pos)
+    dg, dl = g.parameter_gradient_derivatives()
+    n_terms = len(setup.get("pade", [])) + len(setup.get("drummond", []))
+    terms = ev["param_grad_derivs"][-n_terms:]
+    assert all(t["ok"] for t in terms)
+    wg = np.concatenate([np.array(t["grad"]).reshape(-1, m, nw) for t in terms])
+    wl = np.concatenate([np.array(t["lap"]).reshape(-1, m, nw) for t in terms])
+    assert dg.shape == wg.shape and dl.shape == wl.shape
+    assert np.max(np.abs(dg - wg)) <= 1e-9 * np.abs(wg).max()
+    assert np.max(np.abs(dl - wl)) <= 1e-9 * np.abs(wl).max()
