@@ -23,6 +23,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/alea_gpu.h"
 #include "alea_internal.h"
 #include "alea_dev.cuh"
@@ -227,6 +229,16 @@ struct alea_gpu_ctx {
 };
 
 namespace {
+
+// NVTX range over one entry point's work (the phases of a step: sweep,
+// branch, estimators, uploads), visible to ncu's --nvtx filters and any
+// NVTX-aware tracer; no cost without one attached.
+struct Phase {
+    explicit Phase(const char* name) { nvtxRangePushA(name); }
+    ~Phase() { nvtxRangePop(); }
+    Phase(const Phase&) = delete;
+    Phase& operator=(const Phase&) = delete;
+};
 
 int fail(alea_gpu_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -1290,9 +1302,13 @@ int alea_gpu_num_walkers(const alea_gpu_ctx* c, int* nw) {
 }
 
 int alea_gpu_upload_walkers(alea_gpu_ctx* c, const double* positions, int nw) {
+    const Phase phase("alea.upload");
     if (!c) return ALEA_ERR_INVALID;
     if (nw < 1 || nw > c->capacity) return fail(c, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
     if (!positions) return fail(c, ALEA_ERR_INVALID, "null positions");
+    for (long i = 0, n = static_cast<long>(c->sys.np) * 2 * nw; i < n; ++i)
+        if (!std::isfinite(positions[i]))
+            return fail(c, ALEA_ERR_INVALID, "walker positions must be finite (entry " + std::to_string(i) + ")");
     cudaSetDevice(c->device);
     c->cur = 0;
     c->nw = nw;
@@ -1471,6 +1487,7 @@ int alea_gpu_set_streams(alea_gpu_ctx* c, uint64_t seed, uint64_t kind, int n) {
 }
 
 int alea_gpu_vmc_step(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out) {
+    const Phase phase("alea.vmc_step");
     if (!c || !prm) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     if (int rc = run_sweep(c, 0, prm->n_substeps, prm->tau, prm->use_drift, 0, 0, 0, 0)) return rc;
@@ -1557,6 +1574,7 @@ int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, a
 }
 
 int alea_gpu_dmc_advance(alea_gpu_ctx* c, const alea_gpu_dmc_params* prm, alea_gpu_step_stats* out) {
+    const Phase phase("alea.dmc_advance");
     if (!c || !prm) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     if (int rc = run_sweep(c, 1, prm->n_substeps, prm->tau, 1, prm->e_trial, prm->e_ref, prm->e_cut, prm->e_max,
@@ -1598,6 +1616,7 @@ int alea_gpu_dmc_advance(alea_gpu_ctx* c, const alea_gpu_dmc_params* prm, alea_g
 }
 
 int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
+    const Phase phase("alea.dmc_branch");
     if (!c || !state || target < 1) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     const int n = c->nw;
@@ -1849,6 +1868,7 @@ int fw_measure(alea_gpu_ctx* c, size_t lag, const FwSlot& sl) {
 int fw_observe(alea_gpu_ctx* c, long step) {
     FwState* f = c->fw;
     if (!f) return ALEA_OK;
+    const Phase phase("alea.forward_walking");
     if (fw_snapshot_step(f, step)) {
         FwSlot& sl = f->slots[fw_slot_of(f, step)];
         sl.step = step;
@@ -1957,6 +1977,9 @@ int alea_gpu_seed_walker_rows(alea_gpu_ctx* c, const double* rows, int n_rows, i
     if (nw < 1 || nw > c->capacity) return fail(c, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
     CUDA_TRY(c, cudaSetDevice(c->device));
     const int used = std::min(n_rows, nw);
+    for (long i = 0, n = static_cast<long>(used) * c->sys.np * 2; i < n; ++i)
+        if (!std::isfinite(rows[i]))
+            return fail(c, ALEA_ERR_INVALID, "configuration rows must be finite (entry " + std::to_string(i) + ")");
     CUDA_TRY(c, copy_in(c, c->d_buf, rows, static_cast<size_t>(used) * c->sys.np * 2 * 8));
     return fresh_walkers(c, c->d_buf, used, nw);
 }
@@ -2085,6 +2108,7 @@ int close_estimator_block(alea_gpu_ctx* c) {
 }  // namespace
 
 int alea_gpu_estimators_accumulate(alea_gpu_ctx* c, const double* weights, int n_chains) {
+    const Phase phase("alea.estimators");
     if (!c) return ALEA_ERR_INVALID;
     CUDA_TRY(c, cudaSetDevice(c->device));
     if (c->nw == 0) return fail(c, ALEA_ERR_INVALID, "no walkers");
@@ -2116,6 +2140,7 @@ int alea_gpu_estimator_kvectors(const alea_gpu_ctx* c, int id, int* n1, int* n2,
 // ───────────────────────── parameter derivatives ───────────────────────
 
 int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_params) {
+    const Phase phase("alea.param_derivs");
     if (!c || !n_params) return ALEA_ERR_INVALID;
     CUDA_TRY(c, cudaSetDevice(c->device));
     const int nopt = static_cast<int>(c->h_opt.size());
@@ -2223,6 +2248,7 @@ int alea_gpu_fw_estimator_kvectors(const alea_gpu_ctx* c, int lag, int id, int* 
 
 int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
                      double* block_energies) {
+    const Phase phase("alea.vmc_run");
     if (!c || !cfg || !res) return ALEA_ERR_INVALID;
     const auto t0 = std::chrono::steady_clock::now();
     const int nw = c->nw;
@@ -2290,6 +2316,7 @@ int alea_gpu_vmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
 
 int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
                      double* block_energies) {
+    const Phase phase("alea.dmc_run");
     if (!c || !cfg || !res) return ALEA_ERR_INVALID;
     const auto t0 = std::chrono::steady_clock::now();
     const int target = cfg->target_walkers > 0 ? cfg->target_walkers : c->nw;

@@ -231,7 +231,11 @@ const char* alea_gpu_last_error(const alea_gpu_ctx* ctx);
 int alea_gpu_abi_version(void);
 
 /* Positions of nw walkers, SoA [p*dim*nw + d*nw + w]; they are wrapped into
- * the cell and fully evaluated (ψ, derivatives, E_L).  Weights reset to 1. */
+ * the cell and fully evaluated (ψ, derivatives, E_L).  Weights reset to 1.
+ * ALEA_ERR_INVALID for a nonfinite position (nothing is launched);
+ * ALEA_ERR_SINGULAR when a walker's determinant is singular (coincident
+ * same-spin particles, say), as the reference's evaluation throws
+ * (src/wavefunction/slater_determinant.cpp:927-928). */
 int alea_gpu_upload_walkers(alea_gpu_ctx* ctx, const double* positions, int nw);
 int alea_gpu_evaluate(alea_gpu_ctx* ctx);
 int alea_gpu_num_walkers(const alea_gpu_ctx* ctx, int* nw);
