@@ -87,6 +87,7 @@ def pack_system(desc: Dict[str, Any]):
             B.type = _capi.ORB_GAUSSIAN
             B.centers = _dp(f64(b["centers"]))
             B.alphas = _dp(f64(b["alphas"]))
+            B.opt_alpha = int(b.get("opt_alpha", 0))
     terms = []
     for p in desc.get("pade", []):
         terms.append(("pade", p))

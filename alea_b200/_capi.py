@@ -41,7 +41,8 @@ class Group(ctypes.Structure):
 
 class Orbitals(ctypes.Structure):
     _fields_ = [("first", ctypes.c_int), ("last", ctypes.c_int), ("type", ctypes.c_int),
-                ("k", c_dp), ("is_sin", c_ip), ("centers", c_dp), ("alphas", c_dp)]
+                ("k", c_dp), ("is_sin", c_ip), ("centers", c_dp), ("alphas", c_dp),
+                ("opt_alpha", ctypes.c_int)]
 
 
 class PairTerm(ctypes.Structure):

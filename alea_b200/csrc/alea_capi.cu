@@ -225,6 +225,8 @@ struct alea_gpu_ctx {
     DevOpt* d_opt = nullptr;
     double* d_opt_out = nullptr;   // [n_opt][capacity]
     double* d_opt_grad = nullptr;  // [n_opt][np*2][capacity] x 2 (gradient, Laplacian)
+    double* d_opt_scratch = nullptr;   // Gaussian-width derivatives: 3 maxN^2 per CTA
+    int orbital_opts = 0;          // kind-1 (Gaussian width) parameters among h_opt
     FwState* fw = nullptr;         // forward walking (alea_gpu_set_forward_walking)
 };
 
@@ -769,7 +771,19 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     }
     // optimisable parameters of the pair terms (alea_gpu_parameter_derivatives)
     c->h_opt.clear();
-    c->h_opt.reserve(static_cast<size_t>(kMaxTerms) * ALEA_GPU_MAX_OPT);
+    c->h_opt.reserve(static_cast<size_t>(kMaxTerms) * ALEA_GPU_MAX_OPT + kMaxBlocks);
+    for (int b = 0; b < in->n_blocks; ++b) {
+        const alea_gpu_orbitals& O = in->blocks[b];
+        if (!O.opt_alpha) continue;
+        const int n = O.last - O.first;
+        bool uniform = O.type == ALEA_ORB_GAUSSIAN && n > 0;
+        for (int i = 1; uniform && i < n; ++i) uniform = O.alphas[i] == O.alphas[0];
+        if (!uniform)
+            return fail(c, ALEA_ERR_INVALID, "opt_alpha needs a Gaussian block of one shared width");
+        c->h_opt.push_back(DevOpt{});
+        c->h_opt.back().kind = 1;
+        c->h_opt.back().term = b;
+    }
     for (int t = 0; t < in->n_terms; ++t) {
         const alea_gpu_pair_term& T = in->terms[t];
         if (T.n_opt < 0 || T.n_opt > ALEA_GPU_MAX_OPT) return fail(c, ALEA_ERR_INVALID, "bad n_opt");
@@ -1019,6 +1033,8 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));   // ar.bytes is freed on return
     for (const Patch& p : patches) *p.slot = static_cast<char*>(c->arena) + p.off;
     for (int t : ze_terms) s.terms[t].ze_cheb = bessel_dev;
+    c->orbital_opts = 0;
+    for (const DevOpt& o : c->h_opt) c->orbital_opts += o.kind == 1;
     if (!c->h_opt.empty()) {
         CUDA_TRY(c, cudaMallocAsync(&c->d_opt, c->h_opt.size() * sizeof(DevOpt), c->stream));
         CUDA_TRY(c, cudaMemcpyAsync(c->d_opt, c->h_opt.data(), c->h_opt.size() * sizeof(DevOpt),
@@ -1282,7 +1298,7 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
                     static_cast<void*>(c->randoms), static_cast<void*>(c->streams), static_cast<void*>(c->pairs),
                     static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
                     static_cast<void*>(c->d_mask), static_cast<void*>(c->d_opt), static_cast<void*>(c->d_opt_out),
-                    static_cast<void*>(c->d_opt_grad)})
+                    static_cast<void*>(c->d_opt_grad), static_cast<void*>(c->d_opt_scratch)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
     if (c->stream) alea_gpu::est_free(c->est, c->stream);
     if (c->stream) fw_free(c);
@@ -2139,6 +2155,27 @@ int alea_gpu_estimator_kvectors(const alea_gpu_ctx* c, int id, int* n1, int* n2,
 
 // ───────────────────────── parameter derivatives ───────────────────────
 
+namespace {
+
+constexpr int kOrbitalGrid = 148 * 4;   // CTAs of the Gaussian-width kernel (walkers grid-strided)
+
+int orbital_param_derivatives(alea_gpu_ctx* c, double* out, double* dgrad, double* dlap) {
+    if (c->orbital_opts == 0) return ALEA_OK;
+    const int grid = std::min(c->nw, kOrbitalGrid);
+    if (!c->d_opt_scratch) {
+        const size_t b = static_cast<size_t>(kOrbitalGrid) * 3 * c->sys.maxN * c->sys.maxN * 8;
+        if (cudaMallocAsync(&c->d_opt_scratch, b, c->stream) != cudaSuccess)
+            return fail(c, ALEA_ERR_NOMEM, "parameter derivatives: device allocation failed");
+    }
+    ++c->launches;
+    CUDA_TRY(c, launch_orbital_param_derivatives(c->nw, grid, c->stream, c->sys, records(c), c->d_opt,
+                                                 static_cast<int>(c->h_opt.size()), out, dgrad, dlap,
+                                                 c->d_opt_scratch));
+    return ALEA_OK;
+}
+
+}  // namespace
+
 int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_params) {
     const Phase phase("alea.param_derivs");
     if (!c || !n_params) return ALEA_ERR_INVALID;
@@ -2154,6 +2191,7 @@ int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_param
     }
     ++c->launches;
     CUDA_TRY(c, launch_param_derivatives(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, c->d_opt_out));
+    if (int rc = orbital_param_derivatives(c, c->d_opt_out, nullptr, nullptr)) return rc;
     CUDA_TRY(c, copy_out(c, derivs, c->d_opt_out, static_cast<size_t>(nopt) * c->nw * 8));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return ALEA_OK;
@@ -2176,6 +2214,7 @@ int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, doub
     CUDA_TRY(c, cudaMemsetAsync(l, 0, n * 8, c->stream));
     ++c->launches;
     CUDA_TRY(c, launch_param_grad_derivatives(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, g, l));
+    if (int rc = orbital_param_derivatives(c, nullptr, g, l)) return rc;
     if (dgrad) CUDA_TRY(c, copy_out(c, dgrad, g, n * 8));
     if (dlap) CUDA_TRY(c, copy_out(c, dlap, l, n * 8));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));

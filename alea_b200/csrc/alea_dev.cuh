@@ -57,10 +57,12 @@ struct DevTerm {
     const double* ze_cheb;
 };
 
-// One optimisable parameter of a pair term (alea_gpu_pair_term n_opt /
-// opt_index): the term, which coefficient, and for an image-summed Padé the
-// breakup of du/dp - inf (spline and k weights on the shared Jastrow k set).
+// One optimisable parameter: a pair term's coefficient (alea_gpu_pair_term
+// n_opt / opt_index: the term, which coefficient, and for an image-summed
+// Padé the breakup of du/dp - inf, spline and k weights on the shared Jastrow
+// k set), or the shared width of a Gaussian orbital block (opt_alpha).
 struct DevOpt {
+    int kind;       // 0: a pair term's coefficient; 1: the shared width of Gaussian block `term`
     int term;
     int index;
     double inf;

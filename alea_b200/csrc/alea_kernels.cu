@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(NT) param_grad_kernel(DevSys s, const double* 
     const long plane = static_cast<long>(s.np) * 2 * nw;
     for (int q = 0; q < nopt; ++q) {
         const DevOpt& o = opts[q];
+        if (o.kind != 0) continue;   // orbital widths: orbital_param_kernel
         const DevTerm& T = s.terms[o.term];
         for (int i = threadIdx.x; i < s.np; i += NT) {
             double gx = 0.0, gy = 0.0, lx = 0.0, ly = 0.0;
@@ -267,6 +268,7 @@ __global__ void __launch_bounds__(NT) param_kernel(DevSys s, const double* recor
     __syncthreads();
     for (int q = 0; q < nopt; ++q) {
         const DevOpt& o = opts[q];
+        if (o.kind != 0) continue;   // orbital widths: orbital_param_kernel
         const DevTerm& T = s.terms[o.term];
         double acc = 0.0;
         for (int pp = 0; pp < T.npairs; ++pp) {
@@ -301,6 +303,95 @@ __global__ void __launch_bounds__(NT) param_kernel(DevSys s, const double* recor
         }
         if (threadIdx.x == 0) out[static_cast<long>(q) * nw + w] = red[0];
         __syncthreads();
+    }
+}
+
+// The shared width alpha of a Gaussian orbital block (kind-1 parameters), for
+// the walkers blockIdx.x, blockIdx.x + gridDim.x, ...; scratch holds three
+// N x N matrices per CTA.  With D_{c,a} = phi_a(r_c), phi = exp(-alpha |Δ|^2)
+// at the minimum image Δ = r_c - R_a, and A = D^-1 (A[m N + c]):
+//   O       = sum_{c,a} A_{a,c} dD_{c,a},  dD = d phi / d alpha = -|Δ|^2 phi
+//   dA      = -A dD A
+//   dG_d(j) = sum_m dA_{m,j} d_d phi_m(r_j) + A_{m,j} d_alpha d_d phi_m(r_j)
+//   dL_d(j) = sum_m dA_{m,j} d2_d phi_m(r_j) + A_{m,j} d_alpha d2_d phi_m(r_j) - 2 G_d(j) dG_d(j)
+// (slater_determinant.cpp:98-157, :159-250; orbital_set.h:250-286).
+template <int NT>
+__global__ void __launch_bounds__(NT) orbital_param_kernel(DevSys s, const double* records, int nw,
+                                                           const DevOpt* opts, int nopt, double* out,
+                                                           double* dgrad, double* dlap, double* scratch) {
+    __shared__ double red[NT];
+    const long n2 = static_cast<long>(s.maxN) * s.maxN;
+    double* dD = scratch + blockIdx.x * 3 * n2;
+    double* Y = dD + n2;
+    double* dA = Y + n2;
+    const long plane = static_cast<long>(s.np) * 2 * nw;
+    for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+        const double* rec = records + static_cast<long>(w) * s.rec;
+        const double* pos = rec + s.o_pos;
+        for (int q = 0; q < nopt; ++q) {
+            const DevOpt& o = opts[q];
+            if (o.kind != 1) continue;
+            const DevBlock& B = s.blocks[o.term];
+            const int N = B.n;
+            const double* A = rec + B.oA;
+            const double al = B.alphas[0];
+            double acc = 0.0;
+            for (int e = threadIdx.x; e < N * N; e += NT) {
+                const int c = e / N, a = e % N;
+                double del[3] = {pos[(B.first + c) * 2] - B.centers[a * 2],
+                                 pos[(B.first + c) * 2 + 1] - B.centers[a * 2 + 1], 0.0};
+                min_image(s, del);
+                const double r2 = del[0] * del[0] + del[1] * del[1];
+                dD[e] = -r2 * exp(-al * r2);
+                acc += A[a * N + c] * dD[e];
+            }
+            red[threadIdx.x] = acc;
+            __syncthreads();
+            for (int h = NT / 2; h > 0; h >>= 1) {
+                if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0 && out) out[static_cast<long>(q) * nw + w] = red[0];
+            __syncthreads();
+            if (!dgrad && !dlap) continue;
+            for (int e = threadIdx.x; e < N * N; e += NT) {   // Y = dD A
+                const int c = e / N, j = e % N;
+                double t = 0.0;
+                for (int a = 0; a < N; ++a) t = fma(dD[c * N + a], A[a * N + j], t);
+                Y[e] = t;
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < N * N; e += NT) {   // dA = -A Y
+                const int m = e / N, j = e % N;
+                double t = 0.0;
+                for (int c = 0; c < N; ++c) t = fma(A[m * N + c], Y[c * N + j], t);
+                dA[e] = -t;
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < N * 2; e += NT) {
+                const int j = e / 2, d = e % 2;
+                const int particle = B.first + j;
+                const double xj = pos[particle * 2], yj = pos[particle * 2 + 1];
+                double dG = 0.0, dL = 0.0;
+                for (int m = 0; m < N; ++m) {
+                    double del[3] = {xj - B.centers[m * 2], yj - B.centers[m * 2 + 1], 0.0};
+                    min_image(s, del);
+                    const double r2 = del[0] * del[0] + del[1] * del[1];
+                    const double phi = exp(-al * r2), dd = del[d];
+                    const double g = -2.0 * al * dd * phi;
+                    const double l = (4.0 * al * al * dd * dd - 2.0 * al) * phi;
+                    const double dg = -2.0 * dd * phi * (1.0 - al * r2);
+                    const double dl = phi * (8.0 * al * dd * dd - 2.0 - r2 * (4.0 * al * al * dd * dd - 2.0 * al));
+                    const double a = A[m * N + j], da = dA[m * N + j];
+                    dG += da * g + a * dg;
+                    dL += da * l + a * dl;
+                }
+                const long idx = q * plane + (static_cast<long>(particle) * 2 + d) * nw + w;
+                if (dgrad) dgrad[idx] = dG;
+                if (dlap) dlap[idx] = dL - 2.0 * rec[s.o_sg + particle * 2 + d] * dG;
+            }
+            __syncthreads();
+        }
     }
 }
 
@@ -547,6 +638,14 @@ cudaError_t launch_param_derivatives(int nw, cudaStream_t st, const DevSys& s, c
                                      const DevOpt* opts, int nopt, double* out) {
     if (nw < 1 || nopt < 1) return cudaSuccess;
     param_kernel<128><<<nw, 128, 0, st>>>(s, records, nw, opts, nopt, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_orbital_param_derivatives(int nw, int grid, cudaStream_t st, const DevSys& s,
+                                            const double* records, const DevOpt* opts, int nopt, double* out,
+                                            double* dgrad, double* dlap, double* scratch) {
+    if (nw < 1 || nopt < 1) return cudaSuccess;
+    orbital_param_kernel<128><<<grid, 128, 0, st>>>(s, records, nw, opts, nopt, out, dgrad, dlap, scratch);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,12 @@ cudaError_t launch_evaluate(int nt, int nw, size_t smem, cudaStream_t st, const 
 // d ln psi / d p of the nopt optimisable parameters for nw walkers, out [nopt][nw].
 cudaError_t launch_param_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
                                      const DevOpt* opts, int nopt, double* out);
+// The Gaussian-width parameters (kind 1) of the same list: out [nopt][nw] and,
+// when dgrad/dlap are given, their rows of the curvature planes; scratch holds
+// 3 maxN^2 doubles per CTA of the grid.
+cudaError_t launch_orbital_param_derivatives(int nw, int grid, cudaStream_t st, const DevSys& s,
+                                            const double* records, const DevOpt* opts, int nopt, double* out,
+                                            double* dgrad, double* dlap, double* scratch);
 // d(grad ln psi)/dp and d(lap ln psi)/dp of the nopt parameters, [nopt][np*2][nw]
 // each; entries of particles outside a parameter's term are left as they are.
 cudaError_t launch_param_grad_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,

@@ -106,6 +106,8 @@ typedef struct {
     const int* is_sin;        /* plane waves: [n], nonzero = sine */
     const double* centers;    /* Gaussians: [n * dim] */
     const double* alphas;     /* Gaussians: [n] */
+    int opt_alpha;            /* Gaussians of one shared width: that width is an optimisable
+                                 parameter (GaussianOrbitalSet, src/wavefunction/orbital_set.h:226-286) */
 } alea_gpu_orbitals;
 
 /* A pair Jastrow: Padé u = Σ a_k r^k / (1 + Σ b_k r^k) on one group pair,
@@ -380,17 +382,20 @@ int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
 
 /* ───────────────────────── parameter derivatives ───────────────────────
  *
- * O_k = d ln psi / d p_k of every optimisable parameter of the pair Jastrow
- * terms (their n_opt / opt_index), for every walker: what the linear method
+ * O_k = d ln psi / d p_k of every optimisable parameter — the shared widths
+ * of Gaussian orbital blocks (opt_alpha), then the pair Jastrow terms' (their
+ * n_opt / opt_index) — for every walker: what the linear method
  * samples (TrialWavefunction::compute_parameter_derivatives,
  * src/wavefunction/trial_wavefunction.h:104-114; PadeJastrow,
  * src/wavefunction/pade_jastrow.cpp:641-800 with its image sum,
  * periodic_pair_sum.cpp:80-92 and kspace_pair_sum.cpp:303-313;
  * DrummondJastrow, src/wavefunction/drummond_jastrow.cpp:201-320).
- * derivs [n_params][nw] in term order, parameter order within a term;
+ * (SlaterDeterminant, src/wavefunction/slater_determinant.cpp:98-157 and,
+ * for the curvature term below, :159-250).
+ * derivs [n_params][nw]: blocks, then terms, parameter order within a term;
  * *n_params receives their number (derivs may be NULL to ask for it).  The
  * walkers must be evaluated (after upload, a step or alea_gpu_measure).
- * Orbital (Slater) and backflow parameters are not computed here. */
+ * Backflow parameters are not computed here. */
 int alea_gpu_parameter_derivatives(alea_gpu_ctx* ctx, double* derivs, int* n_params);
 /* d(grad_d ln psi)/d p_k and d(lap_d ln psi)/d p_k of the same parameters,
  * [n_params][n_particles * dim][nw] each (the gradient planes' layout per

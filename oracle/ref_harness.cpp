@@ -534,12 +534,18 @@ std::unique_ptr<System> build_crystal(const Args& a) {
         j.ks("type", "gaussian");
         j.arr("centers", cen);
         j.arr("alphas", al);
+        if (geti(a, "gauss_free", 0) != 0) j.ki("opt_alpha", 1);
         j.close('}');
         blocks.push_back({g.first, g.last,
                           std::make_unique<GaussianOrbitalSet>(2, cen, al, s->cell)});
     }
     j.close(']');
-    s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
+    auto slater = std::make_unique<SlaterDeterminant>(std::move(blocks));
+    // gauss_free=1: each block's shared Gaussian width optimisable (the
+    // config layer's opt-in; fixed by default, orbital_set.h:232-241)
+    if (geti(a, "gauss_free", 0) != 0)
+        for (Parameter& p : slater->parameters()) p.is_fixed = false;
+    s->psi.add_component(std::move(slater));
 
     // Drummond: same-spin pairs (l = 1) in one item, opposite spins (l = 0) in another.
     const double Lcut = getd(a, "cutoff", 0.999 * s->cell.ws_radius());

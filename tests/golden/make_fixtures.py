@@ -49,7 +49,7 @@ SYSTEMS = {
     "heg10bf": dict(system="heg", nu=5, nd=5, rs=30, bf=1),
     # the crystal with its Drummond alpha_0, an alpha_2 term and L optimisable
     "crystal16p": dict(system="crystal", nx=4, ny=4, rs=40, drummond_free=1, alpha0=-2e-3,
-                       alpha2=3e-8),
+                       alpha2=3e-8, gauss_free=1),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
@@ -77,12 +77,13 @@ EST = {
     "heg10": dict(gofr_rmax=80.0, gofr_bins=20, dens_rmax=84.0, dens_bins=8, sofk_kmax=0.12),
     "dipoles16": dict(gofr_rmax=0.13, gofr_bins=13, dens_rmax=0.14, dens_bins=4, dens_pp=1,
                       sofk_kmax=60.0),
+    "crystal16": dict(gofr_rmax=130.0, gofr_bins=26, dens_rmax=200.0, dens_bins=10, sofk_kmax=0.05),
 }
 ESTIMATE = {
     "heg10": dict(nw=6, acc=3, steps=2, init_seed=77),
     "dipoles16": dict(nw=5, acc=2, steps=3, init_seed=78),
 }
-EST_VMC = {"heg10": "heg10", "dipoles16": "dipoles16"}
+EST_VMC = {"heg10": "heg10", "dipoles16": "dipoles16", "crystal16": "crystal16"}
 EST_DMC = {"heg10": "heg10"}
 
 # Forward walking (pure estimators) on a DMC run: lags in imaginary time.

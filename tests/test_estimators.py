@@ -174,7 +174,7 @@ def test_device_blocks_match_oracle(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", SYSTEMS)
+@pytest.mark.parametrize("name", SYSTEMS + ["crystal16"])
 def test_vmc_run_estimators_match_reference(name):
     """VMC::run with the estimators attached, one stream (and estimator
     clone) per walker: symmetric-Metropolis positions are bit-identical, so
@@ -240,3 +240,54 @@ def test_estimator_errors():
     g.estimators_accumulate(chains=1)
     g.estimators_stop_block()
     assert g.estimator_desc(0).n_blocks == 1
+
+
+@pytest.mark.gpu
+def test_ragged_chains_match_per_chain_oracle():
+    """Chains that do not divide the population (10 walkers in 3 chains of
+    4, 3, 3, VMC's even split): every chain's block equals the oracle run on
+    that chain's walkers alone, bit for bit (dyadic weights)."""
+    import alea_b200
+    name = "heg10"
+    r = golden(f"est_{name}.json")
+    setup = golden(f"setup_{name}.json")
+    confs = r["configurations"]
+    npart = int(setup["np"])
+    pos = np.concatenate([np.array(c["positions"]).reshape(npart * 2, -1).T for c in confs[:2]])[:10]
+    wts = np.concatenate([np.array(c["weights"]) for c in confs[:2]])[:10]
+    g = alea_b200.Walkers(setup, capacity=10)
+    g.upload(pos.reshape(10, npart, 2))
+    gid = g.add_estimator("gofr", n_bins=20, rmax=80.0)
+    did = g.add_estimator("density", n_bins=8, rmax=84.0)
+    g.estimators_accumulate(wts, chains=3)
+    g.estimators_stop_block()
+    o = Oracle(setup)
+    starts = [0, 4, 7, 10]
+    for t in range(3):
+        sl = slice(starts[t], starts[t + 1])
+        soa = np.ascontiguousarray(g.download()["positions"][sl].T)
+        og, od = OE.Gofr(o, 80.0, 20), OE.Density(o, 84.0, 8)
+        for e in (og, od):
+            e.accumulate(soa, wts[sl])
+            e.stop_block()
+        assert np.array_equal(g.estimator_blocks(gid)[t, 0], og.history[0])
+        assert np.array_equal(g.estimator_blocks(did)[t, 0], od.history[0])
+
+
+@pytest.mark.gpu
+def test_estimator_size_limits_are_refused():
+    import alea_b200
+    setup = golden("setup_heg10.json")
+    g = alea_b200.Walkers(setup, capacity=8)
+    g.upload(np.array(golden("eval_heg10.json")["positions"]))
+    g.add_estimator("gofr", n_bins=6000, rmax=80.0)        # counters beyond one warp's shared memory
+    with pytest.raises(alea_b200.AleaGpuError) as e:
+        g.estimators_accumulate()
+    assert e.value.code == 3
+    g.clear_estimators()
+    with pytest.raises(alea_b200.AleaGpuError):
+        g.add_estimator("density", n_bins=5000)              # more than 4096 bins per axis
+    g.add_estimator("gofr", n_bins=1, rmax=80.0)             # the smallest histogram
+    g.estimators_accumulate()
+    g.estimators_stop_block()
+    assert g.estimator_blocks(0).shape == (1, 1, 3)

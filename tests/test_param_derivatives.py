@@ -6,7 +6,9 @@ reference's App walkers, seed 12345).
 The electron gases' image-summed Padé terms each carry one optimisable
 parameter (b; a_1 is fixed by the cusp): the short-range sum of du/db minus
 its breakup, plus the k-space part from each walker's rho(k).  The crystal
-variant frees its Drummond alpha_0, an alpha_2 term and the cutoff L.  Tolerance 1e-10
+variant frees its Drummond alpha_0, an alpha_2 term and the cutoff L, and
+each Gaussian block's shared width (d ln det/d alpha = Tr(A dD), and
+dA = -A dD A for the curvature term).  Tolerance 1e-10
 relative to the largest |O_k|; after VMC steps (rho(k) updated move by move)
 the derivatives equal those of a fresh evaluation of the same positions.
 """
@@ -20,6 +22,15 @@ pytestmark = pytest.mark.gpu
 SYSTEMS = ["heg10", "heg42", "heg10t", "heg10bf", "crystal16p"]
 
 
+def ours(setup, components):
+    """The reference's components whose parameters this library computes, in
+    its order: the determinant when a Gaussian block's width is free, then
+    the pair terms (Padé per spin pair, or the crystal's Drummond items)."""
+    n_terms = len(setup.get("pade", [])) + len(setup.get("drummond", []))
+    det = [components[0]] if any(b.get("opt_alpha") for b in setup.get("slater", [])) else []
+    return det + components[-n_terms:]
+
+
 @pytest.mark.parametrize("name", SYSTEMS)
 def test_parameter_derivatives_match_reference(name):
     import alea_b200
@@ -29,11 +40,7 @@ def test_parameter_derivatives_match_reference(name):
     g = alea_b200.Walkers(setup, capacity=8)
     g.upload(pos)
     got = g.parameter_derivatives()
-    # components: the determinant(s), then the pair terms (Padé per spin pair,
-    # or the crystal's two Drummond items)
-    n_terms = len(setup.get("pade", [])) + len(setup.get("drummond", []))
-    terms = ev["param_derivs"][-n_terms:]
-    want = np.concatenate([np.array(d).reshape(-1, len(pos)) for d in terms])
+    want = np.concatenate([np.array(d).reshape(-1, len(pos)) for d in ours(setup, ev["param_derivs"])])
     assert got.shape == want.shape
     assert np.max(np.abs(got - want)) <= 1e-10 * np.abs(want).max()
 
@@ -66,8 +73,7 @@ def test_parameter_gradient_derivatives_match_reference(name):
     g = alea_b200.Walkers(setup, capacity=8)
     g.upload(pos)
     dg, dl = g.parameter_gradient_derivatives()
-    n_terms = len(setup.get("pade", [])) + len(setup.get("drummond", []))
-    terms = ev["param_grad_derivs"][-n_terms:]
+    terms = ours(setup, ev["param_grad_derivs"])
     assert all(t["ok"] for t in terms)
     wg = np.concatenate([np.array(t["grad"]).reshape(-1, m, nw) for t in terms])
     wl = np.concatenate([np.array(t["lap"]).reshape(-1, m, nw) for t in terms])
