@@ -294,21 +294,15 @@ def gpu_arm(a):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def allreduce(x, op):
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=op)
-        return float(t.item())
+    from alea_b200.replicas import Replicas, replica_seed
+    reps = Replicas(dist if world > 1 else None, dev)
+    barrier = reps.barrier
 
     nw = a.walkers
     setup = S.heg2d(N_UP, N_DOWN, RS, PADE_B)
     desc = setup.desc
     b_move, b_eval, n_kj, n_ke = work_per_unit(desc)
-    seed = a.seed + 7919 * rank
+    seed = replica_seed(a.seed, rank)
     g = alea_b200.Walkers(desc, capacity=2 * nw + 2, device=local)
     g.upload(setup.positions(seed, nw))
     # untimed VMC pre-equilibration from the uniform start
@@ -349,10 +343,10 @@ def gpu_arm(a):
     clk = clocks.stop()
     barrier()
     ms = ev0.elapsed_time(ev1)
-    ms_max = allreduce(ms, dist.ReduceOp.MAX if world > 1 else None)
-    moves_all = allreduce(float(moves), dist.ReduceOp.SUM if world > 1 else None)
-    evals_all = allreduce(float(evals), dist.ReduceOp.SUM if world > 1 else None)
-    launches_all = allreduce(float(launches), dist.ReduceOp.SUM if world > 1 else None)
+    ms_max = reps.max(ms)
+    moves_all = reps.sum(float(moves))
+    evals_all = reps.sum(float(evals))
+    launches_all = reps.sum(float(launches))
     value = moves_all / (ms_max * 1e-3)
 
     # roofline of the sweep kernel (the dominant launch)
@@ -388,8 +382,8 @@ def gpu_arm(a):
         f1.record(fstream)
         torch.cuda.synchronize()
         barrier()
-        fms_max = allreduce(f0.elapsed_time(f1), dist.ReduceOp.MAX if world > 1 else None)
-        fmoves_all = allreduce(float(fmoves), dist.ReduceOp.SUM if world > 1 else None)
+        fms_max = reps.max(f0.elapsed_time(f1))
+        fmoves_all = reps.sum(float(fmoves))
         e64, e32 = float(np.mean(energies)), float(np.mean(fen))
         err = float(np.sqrt(np.var(energies) / max(len(energies) - 1, 1) + np.var(fen) / max(len(fen) - 1, 1)))
         fp32 = {"value": fmoves_all / (fms_max * 1e-3), "unit": UNIT, "ms_per_step": fms_max / a.steps,
@@ -424,8 +418,8 @@ def gpu_arm(a):
     torch.cuda.synchronize()
     barrier()
     h1, d1 = g.transfer_bytes()
-    e_ms = allreduce(e0.elapsed_time(e1), dist.ReduceOp.MAX if world > 1 else None)
-    e_moves = allreduce(float(res.n_moves), dist.ReduceOp.SUM if world > 1 else None)
+    e_ms = reps.max(e0.elapsed_time(e1))
+    e_moves = reps.sum(float(res.n_moves))
     e2e = {"value": e_moves / (e_ms * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": int((h1 - h0) / a.steps), "d2h_bytes_per_step": int((d1 - d0) / a.steps),
            "path": "alea_gpu_upload_walkers + alea_gpu_dmc_run + alea_gpu_download_walkers, pinned host buffers"}
