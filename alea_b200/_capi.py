@@ -185,7 +185,7 @@ EXPORTS = [
     "alea_gpu_estimators_start_block", "alea_gpu_estimators_accumulate", "alea_gpu_estimators_stop_block",
     "alea_gpu_estimator_info", "alea_gpu_estimator_blocks", "alea_gpu_estimator_kvectors",
     "alea_gpu_final_configurations", "alea_gpu_seed_walker_rows", "alea_gpu_carry_over",
-    "alea_gpu_parameter_derivatives", "alea_gpu_parameter_gradient_derivatives",
+    "alea_gpu_parameter_derivatives", "alea_gpu_parameter_gradient_derivatives", "alea_gpu_measure_fp64_peak",
     "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
     "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
 ]
@@ -248,6 +248,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_server_destroy": ([P], I),
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
         "alea_gpu_parameter_derivatives": ([P, c_dp, c_ip], I),
+        "alea_gpu_measure_fp64_peak": ([I, c_dp], I),
         "alea_gpu_parameter_gradient_derivatives": ([P, c_dp, c_dp, c_ip], I),
         "alea_gpu_set_forward_walking": ([P, c_dp, I, I], I),
         "alea_gpu_add_fw_estimator": ([P, I, ctypes.POINTER(EstimatorSpec), c_ip], I),

@@ -1733,6 +1733,12 @@ int alea_gpu_transfer_bytes(const alea_gpu_ctx* c, uint64_t* h2d, uint64_t* d2h)
     return ALEA_OK;
 }
 
+int alea_gpu_measure_fp64_peak(int device, double* tflops) {
+    if (!tflops) return ALEA_ERR_INVALID;
+    *tflops = 0.0;
+    return measure_fp64_peak(device, tflops) == cudaSuccess ? ALEA_OK : ALEA_ERR_CUDA;
+}
+
 int alea_gpu_launch_count(const alea_gpu_ctx* c, uint64_t* launches) {
     if (!c || !launches) return ALEA_ERR_INVALID;
     *launches = c->launches;

@@ -395,6 +395,23 @@ __global__ void __launch_bounds__(NT) orbital_param_kernel(DevSys s, const doubl
     }
 }
 
+// FP64 CUDA-core peak probe: every thread runs 8 independent FMA chains of
+// `iters` steps (no memory traffic); out gets a sum so the work is kept.
+__global__ void __launch_bounds__(256) fp64_fma_kernel(int iters, double* out) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
+    const double m = 0.999999999, c = 1e-12;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], m, c);
+    }
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += a[k];
+    if (t == 12345.678) out[0] = t;   // never true; keeps the chains live
+}
+
 // Potential energy of stored configurations (Hamiltonian::evaluate_potential,
 // src/hamiltonian/hamiltonian_component.h:165-403): configuration c is
 // rows[idx[c]] (positions [np][2]); the local energy's potential terms with
@@ -654,6 +671,39 @@ cudaError_t launch_param_grad_derivatives(int nw, cudaStream_t st, const DevSys&
     if (nw < 1 || nopt < 1) return cudaSuccess;
     param_grad_kernel<64><<<nw, 64, 0, st>>>(s, records, nw, opts, nopt, dgrad, dlap);
     return cudaGetLastError();
+}
+
+cudaError_t measure_fp64_peak(int device, double* tflops) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaStream_t st;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    double* out = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    e = cudaMallocAsync(&out, sizeof(double), st);
+    const int grid = sms * 8, iters = 1 << 14;
+    double best = 0.0;
+    for (int rep = 0; e == cudaSuccess && rep < 4; ++rep) {   // the first launch warms up
+        cudaEventRecord(e0, st);
+        fp64_fma_kernel<<<grid, 256, 0, st>>>(iters, out);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * 8.0 * iters * grid * 256.0;
+        if (rep > 0 && ms > 0.0f) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    if (out) cudaFreeAsync(out, st);
+    cudaStreamSynchronize(st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    *tflops = best;
+    return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
 cudaError_t launch_potential(int nt, int n, size_t smem, cudaStream_t st, const DevSys& s, const double* rows,

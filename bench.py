@@ -26,6 +26,7 @@ from the reference sources) on the host cores on a bounded walker sample.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -167,6 +168,19 @@ def profiled_traffic_per_walker():
 
 
 # ───────────────────────── reference (host CPU) arm ─────────────────────
+
+def profiled_fp64_flops_per_move():
+    """FP64 flops per move of the sweep kernel from the committed ncu summary
+    (a `fp64_flops_per_move:` line), or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "sweep_dmc_heg42.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("fp64_flops_per_move:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
 
 def host_threads():
     try:
@@ -356,6 +370,17 @@ def gpu_arm(a):
     achieved = bytes_alg / t_sweep / 1e9
     per_walker = profiled_traffic_per_walker()
     traffic = per_walker * float(np.mean(sweep_walkers)) if per_walker else None
+    # the sweep's binding roof: FP64 CUDA-core throughput (measured FMA loop)
+    fpm = profiled_fp64_flops_per_move()
+    fp64_peak = ctypes.c_double(0.0)
+    _capi.load().alea_gpu_measure_fp64_peak(local, ctypes.byref(fp64_peak))
+    roof64 = None
+    if fpm and fp64_peak.value > 0.0:
+        ach64 = fpm * moves / t_sweep / 1e12
+        roof64 = {"bound": "fp64", "achieved": ach64, "peak": fp64_peak.value, "unit": "TFLOP/s",
+                  "frac": ach64 / fp64_peak.value, "flops_per_move": fpm,
+                  "peak_kind": "measured: FP64 FMA loop on this GPU (alea_gpu_measure_fp64_peak)",
+                  "kernel": "sweep_fast_kernel (one-warp DMC sweep)"}
 
     # ── the FP32 form on the same start: throughput and energy against FP64 ──
     fp32 = None
@@ -479,6 +504,7 @@ def gpu_arm(a):
                          "bytes_per_move": b_move, "bytes_per_eval": b_eval,
                          "sweep_ms_per_launch": float(np.mean(sweep_ms)),
                          "sweep_share_of_step": t_sweep / (ms * 1e-3)},
+            "roofline_fp64": roof64,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches_all),

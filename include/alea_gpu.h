@@ -379,6 +379,10 @@ int alea_gpu_transfer_bytes(const alea_gpu_ctx* ctx, uint64_t* h2d, uint64_t* d2
 /* Kernels this context has launched so far (instrumentation; no counterpart
  * in the reference). */
 int alea_gpu_launch_count(const alea_gpu_ctx* ctx, uint64_t* launches);
+/* Measured FP64 CUDA-core FMA throughput of a device in TFLOP/s (a
+ * register-only loop of independent FMAs over every SM; instrumentation, no
+ * counterpart in the reference): the roof of the FP64-latency-bound sweep. */
+int alea_gpu_measure_fp64_peak(int device, double* tflops);
 
 /* ───────────────────────── parameter derivatives ───────────────────────
  *
