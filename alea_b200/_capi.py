@@ -186,6 +186,8 @@ EXPORTS = [
     "alea_gpu_estimator_info", "alea_gpu_estimator_blocks", "alea_gpu_estimator_kvectors",
     "alea_gpu_final_configurations", "alea_gpu_seed_walker_rows", "alea_gpu_carry_over",
     "alea_gpu_parameter_derivatives", "alea_gpu_parameter_gradient_derivatives", "alea_gpu_measure_fp64_peak",
+    "alea_gpu_propose", "alea_gpu_ratio", "alea_gpu_commit", "alea_gpu_local_energy", "alea_gpu_set_rng_streams",
+    "alea_gpu_vmc_steps", "alea_gpu_dmc_steps",
     "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
     "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
 ]
@@ -249,6 +251,14 @@ def load() -> ctypes.CDLL:
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
         "alea_gpu_parameter_derivatives": ([P, c_dp, c_ip], I),
         "alea_gpu_measure_fp64_peak": ([I, c_dp], I),
+        "alea_gpu_propose": ([P, I, c_dp], I),
+        "alea_gpu_ratio": ([P, I, c_dp, c_dp, c_dp, c_dp], I),
+        "alea_gpu_commit": ([P, I, ctypes.POINTER(ctypes.c_uint8)], I),
+        "alea_gpu_local_energy": ([P, c_dp], I),
+        "alea_gpu_set_rng_streams": ([P, ctypes.c_uint64, ctypes.c_uint64, I], I),
+        "alea_gpu_vmc_steps": ([P, ctypes.POINTER(VmcParams), I, ctypes.POINTER(StepStats)], I),
+        "alea_gpu_dmc_steps": ([P, ctypes.POINTER(DmcParams), I, ctypes.POINTER(ctypes.c_uint64), I,
+                                ctypes.POINTER(StepStats)], I),
         "alea_gpu_parameter_gradient_derivatives": ([P, c_dp, c_dp, c_ip], I),
         "alea_gpu_set_forward_walking": ([P, c_dp, I, I], I),
         "alea_gpu_add_fw_estimator": ([P, I, ctypes.POINTER(EstimatorSpec), c_ip], I),

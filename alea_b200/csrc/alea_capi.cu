@@ -228,6 +228,8 @@ struct alea_gpu_ctx {
     double* d_opt_scratch = nullptr;   // Gaussian-width derivatives: 3 maxN^2 per CTA
     int orbital_opts = 0;          // kind-1 (Gaussian width) parameters among h_opt
     FwState* fw = nullptr;         // forward walking (alea_gpu_set_forward_walking)
+    int prop_p = -1;               // alea_gpu_propose: the proposed particle and its positions [dim*nw]
+    std::vector<double> prop_pos;
 };
 
 namespace {
@@ -1476,6 +1478,43 @@ int alea_gpu_set_precision(alea_gpu_ctx* c, int precision) {
     return c->nw > 0 ? launch_evaluate(c) : ALEA_OK;   // FP64 inverses and orbital rows again
 }
 
+// The reference's split of a move (ParticleBatch::propose_move_batch,
+// WavefunctionComponent::ratio_batch, commit), each step alea_gpu_move's
+// arithmetic: the proposal is kept on the host until committed.
+int alea_gpu_propose(alea_gpu_ctx* c, int p, const double* new_pos) {
+    if (!c || !new_pos) return ALEA_ERR_INVALID;
+    if (p < 0 || p >= c->sys.np) return fail(c, ALEA_ERR_INVALID, "particle index out of range");
+    c->prop_p = p;
+    c->prop_pos.assign(new_pos, new_pos + 2L * c->nw);
+    return ALEA_OK;
+}
+
+int alea_gpu_ratio(alea_gpu_ctx* c, int p, double* log_ratio, double* phase, double* new_grad, double* new_lap) {
+    if (!c) return ALEA_ERR_INVALID;
+    if (p != c->prop_p || c->prop_pos.size() != 2u * c->nw)
+        return fail(c, ALEA_ERR_INVALID, "ratio: no proposal of this particle (alea_gpu_propose)");
+    return alea_gpu_move(c, p, c->prop_pos.data(), nullptr, log_ratio, phase, new_grad, new_lap);
+}
+
+int alea_gpu_commit(alea_gpu_ctx* c, int p, const uint8_t* mask) {
+    if (!c || !mask) return ALEA_ERR_INVALID;
+    if (p != c->prop_p || c->prop_pos.size() != 2u * c->nw)
+        return fail(c, ALEA_ERR_INVALID, "commit: no proposal of this particle (alea_gpu_propose)");
+    const int rc = alea_gpu_move(c, p, c->prop_pos.data(), mask, nullptr, nullptr, nullptr, nullptr);
+    c->prop_p = -1;
+    c->prop_pos.clear();
+    return rc;
+}
+
+int alea_gpu_local_energy(alea_gpu_ctx* c, double* el) {
+    if (!c || !el) return ALEA_ERR_INVALID;
+    if (int rc = alea_gpu_measure(c)) return rc;
+    std::vector<double> v;
+    if (int rc = read_scalars(c, S_EL, v)) return rc;
+    std::copy(v.begin(), v.end(), el);
+    return ALEA_OK;
+}
+
 int alea_gpu_measure(alea_gpu_ctx* c) {
     if (!c) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
@@ -1484,6 +1523,47 @@ int alea_gpu_measure(alea_gpu_ctx* c) {
     ++c->launches;
     CUDA_TRY(c, launch_measure(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return ALEA_OK;
+}
+
+int alea_gpu_set_rng_streams(alea_gpu_ctx* c, uint64_t stage_seed, uint64_t stream_kind, int n_streams) {
+    return alea_gpu_set_streams(c, stage_seed, stream_kind, n_streams);
+}
+
+int alea_gpu_vmc_steps(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, int n_steps, alea_gpu_step_stats* out) {
+    if (!c || !prm || n_steps < 0) return ALEA_ERR_INVALID;
+    alea_gpu_step_stats tot{};
+    for (int i = 0; i < n_steps; ++i) {
+        alea_gpu_step_stats st{};
+        if (int rc = alea_gpu_vmc_step(c, prm, &st)) return rc;
+        tot.energy_sum += st.energy_sum;
+        tot.energy_sq_sum += st.energy_sq_sum;
+        tot.weight_sum += st.weight_sum;
+        tot.n_accepted += st.n_accepted;
+        tot.n_proposed += st.n_proposed;
+        tot.n_walkers = st.n_walkers;
+    }
+    if (out) *out = tot;
+    return ALEA_OK;
+}
+
+int alea_gpu_dmc_steps(alea_gpu_ctx* c, const alea_gpu_dmc_params* prm, int n_steps, uint64_t* branch_state,
+                       int target, alea_gpu_step_stats* out) {
+    if (!c || !prm || !branch_state || n_steps < 0) return ALEA_ERR_INVALID;
+    alea_gpu_step_stats tot{};
+    for (int i = 0; i < n_steps; ++i) {
+        alea_gpu_step_stats st{};
+        if (int rc = alea_gpu_dmc_advance(c, prm, &st)) return rc;
+        if (int rc = alea_gpu_dmc_branch(c, branch_state, target)) return rc;
+        tot.energy_sum += st.energy_sum;
+        tot.energy_sq_sum += st.energy_sq_sum;
+        tot.weight_sum += st.weight_sum;
+        tot.n_accepted += st.n_accepted;
+        tot.n_proposed += st.n_proposed;
+        tot.n_cut += st.n_cut;
+        tot.n_walkers = c->nw;
+    }
+    if (out) *out = tot;
     return ALEA_OK;
 }
 

@@ -262,6 +262,20 @@ int alea_gpu_move(alea_gpu_ctx* ctx, int p, const double* new_pos, const uint8_t
                   double* log_ratio, double* phase, double* new_grad, double* new_lap);
 /* Refresh every derivative and recompute E_L (before reading them after moves). */
 int alea_gpu_measure(alea_gpu_ctx* ctx);
+/* The same move in the reference's three steps (ParticleBatch::
+ * propose_move_batch, src/population/particle_batch.cpp:43-57;
+ * WavefunctionComponent::ratio_batch and the masked commit,
+ * src/wavefunction/wavefunction_component.h:82-110): propose keeps particle
+ * p's new positions [d*nw + w]; ratio returns what alea_gpu_move returns for
+ * them; commit applies them to the walkers with mask[w] != 0 and drops the
+ * proposal.  ALEA_ERR_INVALID when ratio/commit name another particle than
+ * the pending proposal. */
+int alea_gpu_propose(alea_gpu_ctx* ctx, int p, const double* new_pos);
+int alea_gpu_ratio(alea_gpu_ctx* ctx, int p, double* log_ratio, double* phase, double* new_grad, double* new_lap);
+int alea_gpu_commit(alea_gpu_ctx* ctx, int p, const uint8_t* mask);
+/* Refresh and E_L of every walker into el [nw] (Hamiltonian::evaluate_batch
+ * after TrialWavefunction::refresh_derivatives). */
+int alea_gpu_local_energy(alea_gpu_ctx* ctx, double* el);
 
 /* Random streams: stream t starts from xoshiro256++ seeded with
  * stream_seed(seed, kind, t) (src/numerics/random.h:52-56). */
@@ -269,6 +283,8 @@ int alea_gpu_measure(alea_gpu_ctx* ctx);
 #define ALEA_STREAM_DMC 0x646d632d74687264ULL   /* "dmc-thrd" */
 #define ALEA_STREAM_BRANCH 0x646d632d62726368ULL /* "dmc-brch" */
 int alea_gpu_set_streams(alea_gpu_ctx* ctx, uint64_t seed, uint64_t kind, int n_streams);
+/* The same, under the name of the fused-driver contract. */
+int alea_gpu_set_rng_streams(alea_gpu_ctx* ctx, uint64_t stage_seed, uint64_t stream_kind, int n_streams);
 
 typedef struct {
     double tau;
@@ -290,6 +306,8 @@ typedef struct {
  * walkers are split over the streams in contiguous even ranges, as VMC's
  * threads are (src/qmc/vmc.cpp:45-61). */
 int alea_gpu_vmc_step(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out);
+/* n_steps VMC steps, statistics summed over the steps (n_walkers: the last). */
+int alea_gpu_vmc_steps(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, int n_steps, alea_gpu_step_stats* out);
 
 /* The same VMC step as alea_gpu_vmc_step, allocating nothing (no counterpart
  * in the reference).  For callers that must not allocate device memory once
@@ -331,6 +349,12 @@ int alea_gpu_dmc_advance(alea_gpu_ctx* ctx, const alea_gpu_dmc_params* prm, alea
  * multiplicities floor(w + U), clipping to [target/5 + 1, 2 target + 1],
  * walker state gathered, weights reset to 1. */
 int alea_gpu_dmc_branch(alea_gpu_ctx* ctx, uint64_t* state, int target);
+/* n_steps DMC steps (advance, then branch on `branch_state`) at the fixed
+ * population-control state of prm; the caller updates E_T between calls as
+ * PopulationControl::update does (src/qmc/population_control.cpp:56-103), or
+ * runs alea_gpu_dmc_run, which does.  Statistics summed over the steps. */
+int alea_gpu_dmc_steps(alea_gpu_ctx* ctx, const alea_gpu_dmc_params* prm, int n_steps, uint64_t* branch_state,
+                       int target, alea_gpu_step_stats* out);
 
 typedef struct {
     int n_equilibration_blocks, n_accumulation_blocks, n_steps, n_substeps;

@@ -264,3 +264,46 @@ def test_one_warp_sweep_matches_generic_sweep(name, monkeypatch):
     assert rel(d_f["local_energy"], d_g["local_energy"]) < 1e-10
     assert rel(d_f["log_psi"], d_g["log_psi"], floor=1.0) < 1e-10
     assert rel(d_f["weights"], d_g["weights"]) < 1e-10
+
+
+def test_split_move_and_multi_step_entry_points_equal_the_fused_ones():
+    """alea_gpu_propose / ratio / commit give alea_gpu_move's results bit for
+    bit; alea_gpu_local_energy is measure + E_L; vmc_steps / dmc_steps equal
+    their step loops (same streams, same walkers)."""
+    import ctypes
+    import alea_b200
+    from alea_b200 import _capi
+    setup = golden("setup_heg10.json")
+    pos = np.array(golden("eval_heg10.json")["positions"])
+    nw = pos.shape[0]
+    a, b = walkers(setup, 8), walkers(setup, 8)
+    a.upload(pos)
+    b.upload(pos)
+    lib = _capi.load()
+    dp = lambda x: x.ctypes.data_as(_capi.c_dp)
+    rng = np.random.default_rng(5)
+    for p in (0, 7, 3):
+        new = np.ascontiguousarray((a.download()["positions"].reshape(nw, -1, 2)[:, p, :] +
+                                    rng.normal(0, 8.0, (nw, 2))).T)
+        acc = np.array([1, 0, 1, 1], dtype=np.uint8)
+        lr_a, ph_a, g_a, l_a = a.move(p, new.T, acc)
+        lr_b, ph_b = np.zeros(nw), np.zeros(nw)
+        g_b, l_b = np.zeros(2 * nw), np.zeros(2 * nw)
+        assert lib.alea_gpu_propose(b.ctx, p, dp(new)) == 0
+        assert lib.alea_gpu_ratio(b.ctx, p, dp(lr_b), dp(ph_b), dp(g_b), dp(l_b)) == 0
+        assert lib.alea_gpu_commit(b.ctx, p, acc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))) == 0
+        assert np.array_equal(lr_a, lr_b) and np.array_equal(ph_a, ph_b)
+        assert np.array_equal(g_a, g_b.reshape(2, nw).T) and np.array_equal(l_a, l_b.reshape(2, nw).T)
+        assert lib.alea_gpu_commit(b.ctx, p, acc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))) != 0
+    el = np.zeros(nw)
+    assert lib.alea_gpu_local_energy(b.ctx, dp(el)) == 0
+    a.measure()
+    assert np.array_equal(el, a.download()["local_energy"])
+    for g in (a, b):
+        g.set_streams(4, alea_b200.STREAM_VMC, nw)
+    tot = [a.vmc_step(225.0, 1) for _ in range(3)]
+    st = _capi.StepStats()
+    prm = _capi.VmcParams(225.0, 1, 0)
+    assert lib.alea_gpu_vmc_steps(b.ctx, ctypes.byref(prm), 3, ctypes.byref(st)) == 0
+    assert st.n_accepted == sum(t.n_accepted for t in tot)
+    assert np.array_equal(a.download()["positions"], b.download()["positions"])
