@@ -383,6 +383,18 @@ class Walkers:
         r = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(-1, self.np * self.dim))
         self._check(self.lib.alea_gpu_seed_walker_rows(self.ctx, _dp(r), r.shape[0], int(nw)))
 
+    def set_checkpoint_hook(self, fn) -> None:
+        """fn(walkers, tag, blocks_done) at dmc_run's milestones ("eq", "a25",
+        "a50", "a75"); it may read self.final_configurations().  None: off."""
+        if fn is None:
+            self._ckpt = None
+            self._check(self.lib.alea_gpu_set_checkpoint_hook(self.ctx, _capi.CHECKPOINT_FN(), None))
+            return
+        def hook(_user, _ctx, tag, done):
+            fn(self, tag.decode(), int(done))
+        self._ckpt = _capi.CHECKPOINT_FN(hook)   # kept alive with the context
+        self._check(self.lib.alea_gpu_set_checkpoint_hook(self.ctx, self._ckpt, None))
+
     def carry_over(self, source: "Walkers", nw: int, keep_state: bool = False) -> None:
         """Seed this context from `source`'s walkers on the device: positions
         and a full evaluation, or (keep_state, same system) whole records."""

@@ -160,6 +160,7 @@ class FwSummary(ctypes.Structure):
 
 
 EST_GOFR, EST_DENSITY, EST_SOFK = 1, 2, 3
+CHECKPOINT_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int)
 CARRY_POSITIONS, CARRY_STATE = 0, 1
 JOB_VMC, JOB_DMC = 0, 1
 PRECISION_FP64, PRECISION_FP32 = 0, 1
@@ -187,7 +188,7 @@ EXPORTS = [
     "alea_gpu_final_configurations", "alea_gpu_seed_walker_rows", "alea_gpu_carry_over",
     "alea_gpu_parameter_derivatives", "alea_gpu_parameter_gradient_derivatives", "alea_gpu_measure_fp64_peak",
     "alea_gpu_propose", "alea_gpu_ratio", "alea_gpu_commit", "alea_gpu_local_energy", "alea_gpu_set_rng_streams",
-    "alea_gpu_vmc_steps", "alea_gpu_dmc_steps",
+    "alea_gpu_vmc_steps", "alea_gpu_dmc_steps", "alea_gpu_set_checkpoint_hook",
     "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
     "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
 ]
@@ -251,6 +252,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_server_last_error": ([P], ctypes.c_char_p),
         "alea_gpu_parameter_derivatives": ([P, c_dp, c_ip], I),
         "alea_gpu_measure_fp64_peak": ([I, c_dp], I),
+        "alea_gpu_set_checkpoint_hook": ([P, CHECKPOINT_FN, P], I),
         "alea_gpu_propose": ([P, I, c_dp], I),
         "alea_gpu_ratio": ([P, I, c_dp, c_dp, c_dp, c_dp], I),
         "alea_gpu_commit": ([P, I, ctypes.POINTER(ctypes.c_uint8)], I),

@@ -228,6 +228,8 @@ struct alea_gpu_ctx {
     double* d_opt_scratch = nullptr;   // Gaussian-width derivatives: 3 maxN^2 per CTA
     int orbital_opts = 0;          // kind-1 (Gaussian width) parameters among h_opt
     FwState* fw = nullptr;         // forward walking (alea_gpu_set_forward_walking)
+    alea_gpu_checkpoint_fn ckpt_fn = nullptr;   // DMC milestone hook and its argument
+    void* ckpt_user = nullptr;
     int prop_p = -1;               // alea_gpu_propose: the proposed particle and its positions [dim*nw]
     std::vector<double> prop_pos;
 };
@@ -2057,6 +2059,13 @@ int fresh_walkers(alea_gpu_ctx* c, const double* d_rows, int n_rows, int nw) {
 
 }  // namespace
 
+int alea_gpu_set_checkpoint_hook(alea_gpu_ctx* c, alea_gpu_checkpoint_fn fn, void* user) {
+    if (!c) return ALEA_ERR_INVALID;
+    c->ckpt_fn = fn;
+    c->ckpt_user = user;
+    return ALEA_OK;
+}
+
 int alea_gpu_final_configurations(alea_gpu_ctx* c, double* rows, int* nw) {
     if (!c || !nw) return ALEA_ERR_INVALID;
     CUDA_TRY(c, cudaSetDevice(c->device));
@@ -2489,7 +2498,11 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
     long step_index = 0;   // from the first equilibration step (forward walking's clock)
     for (int b = 0; b < cfg->n_equilibration_blocks + cfg->n_accumulation_blocks; ++b) {
         const bool measure = b >= cfg->n_equilibration_blocks;
-        if (b == cfg->n_equilibration_blocks) eref_sum = eref_wsum = 0.0;
+        if (b == cfg->n_equilibration_blocks) {
+            eref_sum = eref_wsum = 0.0;
+            // milestone: the equilibrated population (dmc.cpp:776-779)
+            if (c->ckpt_fn) c->ckpt_fn(c->ckpt_user, c, "eq", 0);
+        }
         if (measure) {
             if (int rc = est_start_block(c->est, c->stream, est_err)) return fail(c, rc, est_err);
             if (int rc = fw_start_block(c)) return rc;
@@ -2529,6 +2542,16 @@ int alea_gpu_dmc_run(alea_gpu_ctx* c, const alea_gpu_run_config* cfg, alea_gpu_r
             blocks.push_back(blk_w > 0.0 ? blk_e / blk_w : 0.0);
             if (int rc = close_estimator_block(c)) return rc;
             if (int rc = fw_stop_block(c)) return rc;
+            // quarter milestones (dmc.cpp:810-821): integer quarters, each once
+            if (c->ckpt_fn) {
+                const int n_acc = cfg->n_accumulation_blocks, done = b - cfg->n_equilibration_blocks + 1;
+                if (done == n_acc / 4)
+                    c->ckpt_fn(c->ckpt_user, c, "a25", done);
+                else if (done == n_acc / 2 && n_acc / 2 > n_acc / 4)
+                    c->ckpt_fn(c->ckpt_user, c, "a50", done);
+                else if (done == 3 * n_acc / 4 && 3 * n_acc / 4 > n_acc / 2)
+                    c->ckpt_fn(c->ckpt_user, c, "a75", done);
+            }
         } else {
             if (int rc = read_scalars(c, S_EL, el)) return rc;
             refresh_spread(el);

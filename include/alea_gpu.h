@@ -456,6 +456,16 @@ int alea_gpu_final_configurations(alea_gpu_ctx* ctx, double* rows, int* nw);
  * geometry and cell checks (app.cpp:834-866) are the host's. */
 int alea_gpu_seed_walker_rows(alea_gpu_ctx* ctx, const double* rows, int n_rows, int nw);
 
+/* Milestone checkpoints of alea_gpu_dmc_run (DMC::set_checkpoint_hook,
+ * src/qmc/dmc.h:150-165; called at src/qmc/dmc.cpp:779 and :810-821): after
+ * equilibration (tag "eq", blocks_done 0) and after 25/50/75% of the
+ * accumulation blocks ("a25"/"a50"/"a75", integer quarters, each tag at most
+ * once), between blocks.  The hook may call alea_gpu_final_configurations on
+ * the context to write a snapshot (the reference's App writes
+ * "<walkers_out>.<tag>.h5", app.cpp:885-911).  fn NULL: no hook. */
+typedef void (*alea_gpu_checkpoint_fn)(void* user, alea_gpu_ctx* ctx, const char* tag, int blocks_done);
+int alea_gpu_set_checkpoint_hook(alea_gpu_ctx* ctx, alea_gpu_checkpoint_fn fn, void* user);
+
 enum { ALEA_CARRY_POSITIONS = 0, ALEA_CARRY_STATE = 1 };
 /* Carry `from`'s population into `to` (nw walkers, walker w from source
  * walker w mod from's count) without a host round trip:

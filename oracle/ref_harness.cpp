@@ -966,6 +966,19 @@ int run(const std::string& mode, const Args& a) {
             c.forward_walking_interval = static_cast<std::size_t>(geti(a, "fw_interval", 1));
             if (!bench) put_positions(out, "initial_positions", ens);
             DMC dmc(c, ens, sys->psi, sys->ham);
+            // ckpt=1: the milestone checkpoint hook's calls (DMC::run's eq /
+            // a25 / a50 / a75 snapshots): tag, blocks done, SoA positions
+            Json ck;
+            ck.open('[');
+            if (geti(a, "ckpt", 0) != 0)
+                dmc.set_checkpoint_hook([&ck](const WalkerSet& ws, std::string_view tag, int done) {
+                    ck.open('{');
+                    ck.ks("tag", std::string(tag));
+                    ck.ki("blocks_done", done);
+                    ck.ki("nw", static_cast<long long>(ws.num_walkers()));
+                    ck.arr("positions", ws.positions());
+                    ck.close('}');
+                });
             if (!c.forward_walking_lags.empty()) {
                 // each lag: the same estimators, labelled fw<i> as the builders do
                 std::vector<std::vector<std::unique_ptr<Estimator>>> per_lag(c.forward_walking_lags.size());
@@ -1002,6 +1015,12 @@ int run(const std::string& mode, const Args& a) {
             const double wall =
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             if (with_ests || !c.forward_walking_lags.empty()) put_results(out, dmc.run_result());
+            ck.close(']');
+            if (geti(a, "ckpt", 0) != 0) {
+                out.key("checkpoints");
+                out.s += ck.s;
+                out.first = false;
+            }
             out.ki("threads", c.n_threads);
             out.kv("wall", wall);
             out.arr("stamps", stamps);

@@ -22,6 +22,8 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
   attached to VMC::run / DMC::run (runs as in vmc_/dmc_<name>): series;
 * ``fw_dmc_<name>.json``  a DMC::run with forward walking (pure potential energy
   and pure estimators at three lags): the run result's series and scalars;
+* ``ckpt_dmc_<name>.json`` a DMC::run's milestone checkpoint calls (eq, a25,
+  a50, a75): tag, blocks done, the population's positions;
 * ``chain_<name>.json``   a VMC::run whose final configurations seed a DMC::run
   (carry_over_walkers): DMC populations and weighted energy sums per step;
 * ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
@@ -119,6 +121,18 @@ def dump(name, obj):
     print("wrote", name)
 
 
+CKPT = {"heg10": dict(nw=8, seed=5, eq=1, acc=4, steps=3, substeps=1, tau=2.0, ckpt=1)}
+
+
+def ckpt_fixtures(only=None):
+    for name, run in CKPT.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("dmc", **run, **SYSTEMS[name])
+        dump(f"ckpt_dmc_{name}.json", {"params": run, "checkpoints": r["checkpoints"],
+                                       "initial_positions": r["initial_positions"]})
+
+
 def fw_fixtures(only=None):
     for name, fw in FW.items():
         if only and name not in only:
@@ -182,6 +196,7 @@ def main(only=None):
                                       "walkers": r["walkers"], "final_positions": r["final_positions"]})
     chain_fixtures(only)
     fw_fixtures(only)
+    ckpt_fixtures(only)
     for name, run in DMC_STAT.items():
         if only and name not in only:
             continue

@@ -119,3 +119,35 @@ def test_carry_over_state_keeps_records():
         o.carry_over(a, 4, keep_state=True)
     o.carry_over(a, 4)
     assert o.nw == 4
+
+
+@pytest.mark.gpu
+def test_dmc_milestone_checkpoints_match_reference(tmp_path):
+    """alea_gpu_dmc_run's checkpoint hook fires where DMC::run's does (eq,
+    a25, a50, a75), with the same population; the hook writes a checkpoint
+    file per milestone as the reference's App does (wk.<tag>.*)."""
+    import alea_b200
+    from alea_b200 import checkpoint as C
+    ref = golden("ckpt_dmc_heg10.json")
+    p = ref["params"]
+    setup = golden("setup_heg10.json")
+    nw = p["nw"]
+    g = alea_b200.Walkers(setup, capacity=4 * nw + 4)
+    g.upload(np.array(ref["initial_positions"]))
+    seen = []
+
+    def hook(w, tag, done):
+        rows = w.final_configurations()
+        seen.append((tag, done, rows))
+        C.write_walkers(str(tmp_path / f"wk.{tag}.npz"), rows, lattice=setup["cell"]["vectors"], tag=tag,
+                        blocks_done=done)
+
+    g.set_checkpoint_hook(hook)
+    g.dmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], nw, p["seed"], target=nw)
+    assert [(t, d) for t, d, _ in seen] == [(c["tag"], c["blocks_done"]) for c in ref["checkpoints"]]
+    for (tag, done, rows), c in zip(seen, ref["checkpoints"]):
+        want = np.array(c["positions"]).reshape(-1, c["nw"]).T.reshape(c["nw"], -1, 2)
+        assert rows.shape == want.shape
+        assert np.max(np.abs(rows - want)) < 1e-9 * np.abs(want).max()
+        wf = C.read_walkers(str(tmp_path / f"wk.{tag}.npz"))
+        assert wf["tag"] == tag and wf["blocks_done"] == done and np.array_equal(wf["positions"], rows)
