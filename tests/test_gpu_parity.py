@@ -307,3 +307,31 @@ def test_split_move_and_multi_step_entry_points_equal_the_fused_ones():
     assert lib.alea_gpu_vmc_steps(b.ctx, ctypes.byref(prm), 3, ctypes.byref(st)) == 0
     assert st.n_accepted == sum(t.n_accepted for t in tot)
     assert np.array_equal(a.download()["positions"], b.download()["positions"])
+
+
+def test_dmc_steps_equal_the_advance_branch_loop():
+    import ctypes
+    import alea_b200
+    from alea_b200 import _capi
+    setup = golden("setup_heg10.json")
+    pos = np.array(golden("eval_heg10.json")["positions"])
+    nw = pos.shape[0]
+    a, b = walkers(setup, 4 * nw + 4), walkers(setup, 4 * nw + 4)
+    lib = _capi.load()
+    for g in (a, b):
+        g.upload(pos)
+        assert lib.alea_gpu_set_rng_streams(g.ctx, ctypes.c_uint64(8), ctypes.c_uint64(alea_b200.STREAM_DMC), nw) == 0
+    el0 = float(np.mean(a.download()["local_energy"]))
+    prm = _capi.DmcParams(2.0, 1, el0, el0, np.inf, np.inf)
+    sa = np.array([1, 2, 3, 4], dtype=np.uint64)
+    sb = sa.copy()
+    tot = 0
+    for _ in range(3):
+        st = a.dmc_advance(2.0, 1, el0, el0, np.inf, np.inf)
+        a.dmc_branch(sa, nw)
+        tot += st.n_accepted
+    st = _capi.StepStats()
+    assert lib.alea_gpu_dmc_steps(b.ctx, ctypes.byref(prm), 3, sb.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                  nw, ctypes.byref(st)) == 0
+    assert st.n_accepted == tot and st.n_walkers == a.nw and np.array_equal(sa, sb)
+    assert np.array_equal(a.download()["positions"], b.download()["positions"])
