@@ -213,6 +213,11 @@ def pack_system(desc: Dict[str, Any]):
             C.n_coeffs = len(ch["coeffs"])
             for k, v in enumerate(ch["coeffs"]):
                 C.coeffs[k] = float(v)
+            C.zero_slope = int(ch.get("zero_slope", 0))
+            opt = ch.get("opt_index", [])
+            C.n_opt = len(opt)
+            for q, v in enumerate(opt):
+                C.opt_index[q] = int(v)
     return s, keep
 
 

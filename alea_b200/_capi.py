@@ -22,6 +22,7 @@ STREAM_BRANCH = 0x646D632D62726368
 
 c_dp = ctypes.POINTER(ctypes.c_double)
 c_ip = ctypes.POINTER(ctypes.c_int)
+MAX_OPT = 4   # ALEA_GPU_MAX_OPT
 
 
 class Spline(ctypes.Structure):
@@ -54,7 +55,7 @@ class PairTerm(ctypes.Structure):
                 ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int),
                 ("dcoeffs", ctypes.c_double * 16), ("ze_b", ctypes.c_double),
                 ("ze_exponent", ctypes.c_double), ("ze_matching_radius", ctypes.c_double),
-                ("ze_cutoff", ctypes.c_double), ("n_opt", ctypes.c_int), ("opt_index", ctypes.c_int * 4),
+                ("ze_cutoff", ctypes.c_double), ("n_opt", ctypes.c_int), ("opt_index", ctypes.c_int * MAX_OPT),
                 ("opt_inf", ctypes.c_double * 4), ("opt_short_range", Spline * 4),
                 ("opt_weight", c_dp * 4)]
 
@@ -78,7 +79,8 @@ class InversePower(ctypes.Structure):
 
 class BackflowChannel(ctypes.Structure):
     _fields_ = [("source_first", ctypes.c_int), ("source_last", ctypes.c_int), ("C", ctypes.c_int),
-                ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int), ("coeffs", ctypes.c_double * 16)]
+                ("L", ctypes.c_double), ("n_coeffs", ctypes.c_int), ("coeffs", ctypes.c_double * 16),
+                ("zero_slope", ctypes.c_int), ("n_opt", ctypes.c_int), ("opt_index", ctypes.c_int * MAX_OPT)]
 
 
 class Backflow(ctypes.Structure):

@@ -775,7 +775,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     }
     // optimisable parameters of the pair terms (alea_gpu_parameter_derivatives)
     c->h_opt.clear();
-    c->h_opt.reserve(static_cast<size_t>(kMaxTerms) * ALEA_GPU_MAX_OPT + kMaxBlocks);
+    c->h_opt.reserve(static_cast<size_t>(kMaxTerms + 8) * ALEA_GPU_MAX_OPT + kMaxBlocks);
     for (int b = 0; b < in->n_blocks; ++b) {
         const alea_gpu_orbitals& O = in->blocks[b];
         if (!O.opt_alpha) continue;
@@ -788,6 +788,28 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         c->h_opt.back().kind = 1;
         c->h_opt.back().term = b;
     }
+    // backflow channels' parameters, BackflowFunction's order [c_0, (c_1), c_2.., L]
+    // (backflow_function.h:111-135) mapped to a coefficient index or -1 for L
+    for (int d = 0; d < in->n_backflow; ++d)
+        for (int q = 0; q < in->backflow[d].n_channels; ++q) {
+            const alea_gpu_backflow_channel& C = in->backflow[d].channels[q];
+            const int zs = C.zero_slope ? 1 : 0;
+            if (C.n_opt < 0 || C.n_opt > ALEA_GPU_MAX_OPT || (zs && C.n_coeffs < 2))
+                return fail(c, ALEA_ERR_INVALID, "bad backflow n_opt / zero_slope");
+            const int n_par = C.n_coeffs - zs + 1;
+            for (int u = 0; u < C.n_opt; ++u) {
+                const int slot = C.opt_index[u];
+                if (slot < 0 || slot >= n_par || (u > 0 && slot <= C.opt_index[u - 1]))
+                    return fail(c, ALEA_ERR_INVALID, "backflow opt_index out of range or not ascending");
+                c->h_opt.push_back(DevOpt{});
+                DevOpt& o = c->h_opt.back();
+                o.kind = 2;
+                o.term = d;
+                o.ch = q;
+                o.zs = zs;
+                o.index = slot == n_par - 1 ? -1 : (zs && slot >= 1 ? slot + 1 : slot);
+            }
+        }
     for (int t = 0; t < in->n_terms; ++t) {
         const alea_gpu_pair_term& T = in->terms[t];
         if (T.n_opt < 0 || T.n_opt > ALEA_GPU_MAX_OPT) return fail(c, ALEA_ERR_INVALID, "bad n_opt");
@@ -2298,6 +2320,9 @@ int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, doub
     const int nopt = static_cast<int>(c->h_opt.size());
     *n_params = nopt;
     if ((!dgrad && !dlap) || nopt == 0 || c->nw == 0) return ALEA_OK;
+    for (const DevOpt& o : c->h_opt)
+        if (o.kind == 2)
+            return fail(c, ALEA_ERR_UNSUPPORTED, "curvature terms of backflow parameters are not built");
     if (c->sys.np > 256) return fail(c, ALEA_ERR_UNSUPPORTED, "parameter derivatives: more than 256 particles");
     const size_t cap = static_cast<size_t>(nopt) * c->sys.np * 2 * c->capacity;
     if (!c->d_opt_grad && cudaMallocAsync(&c->d_opt_grad, 2 * cap * 8, c->stream) != cudaSuccess)

@@ -60,11 +60,15 @@ struct DevTerm {
 // One optimisable parameter: a pair term's coefficient (alea_gpu_pair_term
 // n_opt / opt_index: the term, which coefficient, and for an image-summed
 // Padé the breakup of du/dp - inf, spline and k weights on the shared Jastrow
-// k set), or the shared width of a Gaussian orbital block (opt_alpha).
+// k set), the shared width of a Gaussian orbital block (opt_alpha), or a
+// backflow channel's parameter (kind 2: determinant `term`, channel `ch`,
+// `index` the coefficient k of c_0..c_N or -1 for the cutoff L, `zs` set when
+// the channel derives c_1 = C c_0 / L).
 struct DevOpt {
-    int kind;       // 0: a pair term's coefficient; 1: the shared width of Gaussian block `term`
+    int kind;       // 0: a pair term's coefficient; 1: the shared width of Gaussian block `term`; 2: backflow
     int term;
     int index;
+    int ch, zs;
     double inf;
     DevSpline sp;
     const double* kw;

@@ -252,6 +252,30 @@ __global__ void __launch_bounds__(NT) param_grad_kernel(DevSys s, const double* 
 }
 
 // O_q = d ln psi / d p_q of every optimisable parameter for one walker: the
+// ∂η/∂p at r of one backflow parameter (BackflowFunction::parameter_derivatives,
+// backflow_function.h:111-135): k >= 0 the coefficient c_k, ∂η/∂c_k = f r^k
+// with f = (1 - r/L)^C (plus f C r/L for c_0 when c_1 = C c_0/L, zs); k = -1
+// the cutoff, ∂η/∂L = C t^{C-1} r/L² P(r) (minus f C c_0 r/L² when zs).
+__device__ __forceinline__ double bf_eta_dparam(const DevBFCh& C, int k, int zs, double r) {
+    if (r >= C.L) return 0.0;
+    const double t = 1.0 - r / C.L;
+    double tc1 = 1.0;
+    for (int i = 0; i < C.C - 1; ++i) tc1 *= t;
+    const double f = tc1 * t;
+    if (k >= 0) {
+        double rk = 1.0;
+        for (int i = 0; i < k; ++i) rk *= r;
+        double v = f * rk;
+        if (zs && k == 0) v += f * static_cast<double>(C.C) * r / C.L;
+        return v;
+    }
+    double P = 0.0;
+    for (int i = C.nc - 1; i >= 0; --i) P = P * r + C.c[i];
+    double v = static_cast<double>(C.C) * tc1 * r / (C.L * C.L) * P;
+    if (zs) v -= f * static_cast<double>(C.C) * C.c[0] * r / (C.L * C.L);
+    return v;
+}
+
 // pair sum of du/dp over the term's pairs (minus, for an image sum, the
 // breakup's long-range part and limit inside r_cut, zero outside) plus the
 // image sum's k-space part, sum_k w'_k |rho_a|^2 or 2 Re rho_a rho_b*
@@ -268,10 +292,27 @@ __global__ void __launch_bounds__(NT) param_kernel(DevSys s, const double* recor
     __syncthreads();
     for (int q = 0; q < nopt; ++q) {
         const DevOpt& o = opts[q];
-        if (o.kind != 0) continue;   // orbital widths: orbital_param_kernel
-        const DevTerm& T = s.terms[o.term];
+        if (o.kind == 1) continue;   // orbital widths: orbital_param_kernel
         double acc = 0.0;
-        for (int pp = 0; pp < T.npairs; ++pp) {
+        if (o.kind == 2) {
+            // Σ_P Σ_j (F_P · r_Pj) ∂η(r_Pj)/∂p over the channel's sources j ≠ P
+            // (BackflowTransformation::parameter_derivatives,
+            // backflow_transformation.cpp:284-312; F_P the committed row of F)
+            const DevBF& D = s.bf[o.term];
+            const DevBFCh& C = D.ch[o.ch];
+            const double* F = rec + D.oF;
+            const int ns = C.sl - C.sf;
+            for (int e = threadIdx.x; e < D.n * ns; e += NT) {
+                const int t = e / ns, j = C.sf + e % ns, P = D.first + t;
+                if (j == P) continue;
+                double del[3];
+                const double r = fold_dist(s, pos + P * 2, pos + j * 2, del);
+                if (r >= C.L) continue;
+                acc += (F[t * 2] * del[0] + F[t * 2 + 1] * del[1]) * bf_eta_dparam(C, o.index, o.zs, r);
+            }
+        }
+        const DevTerm& T = s.terms[o.kind == 0 ? o.term : 0];
+        for (int pp = 0; o.kind == 0 && pp < T.npairs; ++pp) {
             const int af = T.pairs[pp][0], al = T.pairs[pp][1], bf = T.pairs[pp][2], bl = T.pairs[pp][3];
             const bool same = af == bf && al == bl;
             const int na = al - af, nb = bl - bf;
@@ -286,7 +327,7 @@ __global__ void __launch_bounds__(NT) param_kernel(DevSys s, const double* recor
                 acc += v;
             }
         }
-        if (T.image) {
+        if (o.kind == 0 && T.image) {
             const int ga = s.group_of[T.pairs[0][0]], gb = s.group_of[T.pairs[0][2]];
             const double* ra = rec + s.o_rho + 2 * ga * s.nkJ;
             const double* rb = rec + s.o_rho + 2 * gb * s.nkJ;

@@ -175,13 +175,19 @@ typedef struct {
 /* One backflow channel: the particles [source_first, source_last) displace
  * every row of the determinant by η(r) r, η = (1 - r/L)^C Σ_k c_k r^k for
  * r < L (src/wavefunction/backflow_function.h:11-37; coeffs are c_0..c_N with
- * a like-spin channel's c_1 = C c_0 / L already filled in). */
+ * a like-spin channel's c_1 = C c_0 / L already filled in).
+ * zero_slope marks that derived c_1; n_opt / opt_index name the channel's
+ * optimisable parameters in BackflowFunction's order [c_0, (c_1 unless
+ * zero_slope), c_2.., L] (backflow_function.h:111-135), ascending. */
 typedef struct {
     int source_first, source_last;
     int C;
     double L;
     int n_coeffs;
     double coeffs[16];
+    int zero_slope;
+    int n_opt;
+    int opt_index[ALEA_GPU_MAX_OPT];
 } alea_gpu_backflow_channel;
 
 /* A backflow Slater determinant over the rows [first, last) of one spin group

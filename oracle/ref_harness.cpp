@@ -383,6 +383,12 @@ std::unique_ptr<System> build_heg(const Args& a) {
                 j.ki("C", 3);
                 j.arr("coeffs", full);
                 j.kv("L", L);
+                // free parameters in BackflowFunction's order [c_0, (c_1), .., L]
+                j.ki("zero_slope", hi == gi ? 1 : 0);
+                std::vector<double> opt;
+                for (std::size_t q = 0; q < ch.params.size(); ++q)
+                    if (!ch.params[q].is_fixed) opt.push_back(static_cast<double>(q));
+                j.arr("opt_index", opt);
                 j.close('}');
                 chans.push_back(std::move(ch));
             }

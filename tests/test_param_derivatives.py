@@ -8,7 +8,9 @@ parameter (b; a_1 is fixed by the cusp): the short-range sum of du/db minus
 its breakup, plus the k-space part from each walker's rho(k).  The crystal
 variant frees its Drummond alpha_0, an alpha_2 term and the cutoff L, and
 each Gaussian block's shared width (d ln det/d alpha = Tr(A dD), and
-dA = -A dD A for the curvature term).  Tolerance 1e-10
+dA = -A dD A for the curvature term).  The backflow gas frees each channel's
+c_0 (and the unlike-spin c_1): O = Σ_P Σ_j (F_P · r_Pj) dη(r_Pj)/dp with the
+committed F = A^T ∇φ(x); its curvature terms are refused.  Tolerance 1e-10
 relative to the largest |O_k|; after VMC steps (rho(k) updated move by move)
 the derivatives equal those of a fresh evaluation of the same positions.
 """
@@ -24,10 +26,14 @@ SYSTEMS = ["heg10", "heg42", "heg10t", "heg10bf", "crystal16p"]
 
 def ours(setup, components):
     """The reference's components whose parameters this library computes, in
-    its order: the determinant when a Gaussian block's width is free, then
-    the pair terms (Padé per spin pair, or the crystal's Drummond items)."""
+    its order: the backflow determinants with free channel parameters, or the
+    determinant when a Gaussian block's width is free, then the pair terms
+    (Padé per spin pair, or the crystal's Drummond items)."""
     n_terms = len(setup.get("pade", [])) + len(setup.get("drummond", []))
-    det = [components[0]] if any(b.get("opt_alpha") for b in setup.get("slater", [])) else []
+    bf = setup.get("backflow", [])
+    det = [components[d] for d, b in enumerate(bf) if any(ch.get("opt_index") for ch in b["channels"])]
+    if any(b.get("opt_alpha") for b in setup.get("slater", [])):
+        det = [components[0]]
     return det + components[-n_terms:]
 
 
@@ -72,6 +78,11 @@ def test_parameter_gradient_derivatives_match_reference(name):
     nw, m = len(pos), int(setup["np"]) * int(setup["dim"])
     g = alea_b200.Walkers(setup, capacity=8)
     g.upload(pos)
+    if "backflow" in setup:
+        with pytest.raises(alea_b200.AleaGpuError) as e:
+            g.parameter_gradient_derivatives()
+        assert e.value.code == 3                     # backflow curvature terms: not built
+        return
     dg, dl = g.parameter_gradient_derivatives()
     terms = ours(setup, ev["param_grad_derivs"])
     assert all(t["ok"] for t in terms)
