@@ -1,6 +1,8 @@
 """The C-ABI library builds, loads and exports every symbol include/alea_gpu.h
 declares; host-side validation errors come back as status codes (CPU only)."""
 import ctypes
+import subprocess
+import tempfile
 import os
 import re
 
@@ -74,3 +76,36 @@ def test_create_reports_errors_without_crashing():
     assert rc != 0
     assert lib.alea_gpu_last_error(None)
     assert not ctx.value
+
+
+def test_every_struct_field_matches_the_header():
+    """Every ctypes mirror of an alea_gpu.h struct has the C size and, field by
+    field, the C offset (a probe compiled with gcc against the header)."""
+    from alea_b200 import _capi
+    pairs = [("alea_gpu_spline", _capi.Spline), ("alea_gpu_kset", _capi.KSet), ("alea_gpu_group", _capi.Group),
+             ("alea_gpu_orbitals", _capi.Orbitals), ("alea_gpu_pair_term", _capi.PairTerm),
+             ("alea_gpu_ewald", _capi.Ewald), ("alea_gpu_coulomb", _capi.Coulomb),
+             ("alea_gpu_inverse_power", _capi.InversePower),
+             ("alea_gpu_backflow_channel", _capi.BackflowChannel), ("alea_gpu_backflow", _capi.Backflow),
+             ("alea_gpu_system", _capi.System), ("alea_gpu_vmc_params", _capi.VmcParams),
+             ("alea_gpu_step_stats", _capi.StepStats), ("alea_gpu_dmc_params", _capi.DmcParams),
+             ("alea_gpu_run_config", _capi.RunConfig), ("alea_gpu_run_result", _capi.RunResult),
+             ("alea_gpu_job", _capi.Job), ("alea_gpu_job_result", _capi.JobResult),
+             ("alea_gpu_estimator_spec", _capi.EstimatorSpec), ("alea_gpu_estimator_desc", _capi.EstimatorDesc),
+             ("alea_gpu_fw_summary", _capi.FwSummary)]
+    lines, want = [], []
+    for cname, cls in pairs:
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        want.append(ctypes.sizeof(cls))
+        for f in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {f[0]}));')
+            want.append(getattr(cls, f[0]).offset)
+    src = "#include <stddef.h>\n#include <stdio.h>\n#include \"alea_gpu.h\"\nint main(void) {\n" + \
+          "\n".join(lines) + "\n  return 0;\n}\n"
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "layout.c")
+        exe = os.path.join(d, "layout")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        got = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
+    assert got == want
