@@ -291,3 +291,27 @@ def test_estimator_size_limits_are_refused():
     g.estimators_accumulate()
     g.estimators_stop_block()
     assert g.estimator_blocks(0).shape == (1, 1, 3)
+
+
+@pytest.mark.gpu
+def test_per_particle_density_sums_to_group_density():
+    """On a DMC run (non-dyadic weights, population changing at every
+    branch) the per-particle series of each group add up to the group's
+    density series, block by block (1e-12): the per-particle grids and the
+    group grids bin the same walkers with the same weights."""
+    import alea_b200
+    setup = golden("setup_heg10.json")
+    ref = golden("dmc_heg10.json")
+    nw = len(ref["initial_positions"])
+    g = alea_b200.Walkers(setup, capacity=4 * nw + 4)
+    g.upload(np.array(ref["initial_positions"]))
+    grp = g.add_estimator("density", n_bins=8, rmax=84.0)
+    per = g.add_estimator("density", n_bins=8, rmax=84.0, per_particle=True)
+    g.dmc_run(1, 3, 4, 1, 2.0, nw, 7, target=nw)
+    a, b = g.estimator_blocks(grp), g.estimator_blocks(per)
+    n_cells = 64
+    assert a.shape[:2] == b.shape[:2] and a.shape[1] == 3
+    for q, G in enumerate(setup["groups"]):
+        want = a[..., q * n_cells:(q + 1) * n_cells]
+        got = sum(b[..., p * n_cells:(p + 1) * n_cells] for p in range(G["first"], G["last"]))
+        assert np.max(np.abs(got - want)) <= 1e-12 * np.abs(want).max()
