@@ -690,6 +690,24 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const EstSource& src, con
         *have = want;
         return true;
     };
+    // one binning launch's view of the source: `rows` walker ranges per chain,
+    // each writing a row of `width1` sums into the scratch
+    auto launch_of = [&](int rows, int width1) {
+        EstLaunch L{};
+        L.rec = src.base;
+        L.stride = src.stride;
+        L.o_pos = src.o_pos;
+        L.o_w = src.o_w;
+        L.idx = src.idx;
+        L.weights = d_weights;
+        L.unit = unit ? 1 : 0;
+        L.nw = nw;
+        L.chains = chains;
+        L.rows = rows;
+        L.part = set->d_part;
+        L.width1 = width1;
+        return L;
+    };
     for (DevEstimator& d : set->e) {
         const int width1 = d.width + 1;
         const int cells1 = d.n_cells + 1;
@@ -704,19 +722,7 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const EstSource& src, con
                 err = "estimators: device allocation failed";
                 return ALEA_ERR_NOMEM;
             }
-            EstLaunch L{};
-            L.rec = src.base;
-            L.stride = src.stride;
-            L.o_pos = src.o_pos;
-            L.o_w = src.o_w;
-            L.idx = src.idx;
-            L.weights = d_weights;
-            L.unit = unit ? 1 : 0;
-            L.nw = nw;
-            L.chains = chains;
-            L.rows = ranges;
-            L.part = set->d_part;
-            L.width1 = cells1;
+            const EstLaunch L = launch_of(ranges, cells1);
             density_pp_kernel<<<dim3(ranges, s.np, chains), 32, sizeof(double) * cells1, st>>>(s, L, d.spec.rmax,
                                                                                               d.spec.n_bins);
             const long n = static_cast<long>(chains) * s.np * cells1;
@@ -739,19 +745,7 @@ int est_accumulate(EstimatorSet* set, const DevSys& s, const EstSource& src, con
             err = "estimators: device allocation failed";
             return ALEA_ERR_NOMEM;
         }
-        EstLaunch L{};
-        L.rec = src.base;
-        L.stride = src.stride;
-        L.o_pos = src.o_pos;
-        L.o_w = src.o_w;
-        L.idx = src.idx;
-        L.weights = d_weights;
-        L.unit = unit ? 1 : 0;
-        L.nw = nw;
-        L.chains = chains;
-        L.rows = rows;
-        L.part = set->d_part;
-        L.width1 = width1;
+        EstLaunch L = launch_of(rows, width1);
         L.smem_row = width1 <= kSmemRowDoubles ? 1 : 0;
         const dim3 grid(rows, chains);
         size_t smem = L.smem_row ? sizeof(double) * width1 : 0;
