@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--no-estimators", action="store_true",
                     help="skip the device-estimator (g(r), density, S(k)) measurement")
+    ap.add_argument("--density-per-particle", action="store_true",
+                    help="measure the density per particle (one 48x48 grid each) instead of per spin")
     ap.add_argument("--serve", action="store_true",
                     help="serving mix instead of the DMC step: Poisson VMC jobs through alea_gpu_server")
     ap.add_argument("--serve-jobs", type=int, default=60)
@@ -457,7 +459,7 @@ def gpu_arm(a):
                        for i in range(-2, 3) for j in range(-2, 3) if i or j)
         b1 = float(np.hypot(*(2.0 * np.pi * np.linalg.inv(av)[:, 0])))
         ids = [g.add_estimator("gofr", n_bins=110, rmax=ws),
-               g.add_estimator("density", n_bins=48, rmax=ws),
+               g.add_estimator("density", n_bins=48, rmax=ws, per_particle=a.density_per_particle),
                g.add_estimator("sofk", kmax=8.0 * b1)]
         g.estimators_accumulate()          # first measurement allocates the running blocks
         torch.cuda.synchronize()
@@ -472,7 +474,8 @@ def gpu_arm(a):
         est = {"ms_per_measurement": est_ms, "share_of_dmc_step": est_ms / (ms_max / a.steps),
                "launches_per_measurement": (g.launch_count() - l_est) / a.steps,
                "walkers": int(g.nw),
-               "estimators": f"gofr 110 bins to r = {ws:.1f}, density 48x48 per spin, "
+               "estimators": f"gofr 110 bins to r = {ws:.1f}, density 48x48 per "
+                             f"{'particle' if a.density_per_particle else 'spin'}, "
                              f"sofk n_k = {g.estimator_desc(ids[2]).n_k} (|k| <= 8 |b1|)",
                "note": "every walker binned on the device; the host reads one block estimate per block"}
         g.clear_estimators()
