@@ -5,17 +5,11 @@
 //   cell             lattice from r_s and N (src/qmc/app.cpp:288-336)
 //   plane waves      closed reciprocal shells (src/wavefunction/orbital_set.h:575-665)
 //   cusps            Kato Γ = 2 μ R / (2ℓ + d − 1) (src/builders/jastrow.cpp:48-98)
-//   Ewald            optimized breakup of 1/r (src/numerics/ewald_breakup.cpp:205-276)
+//   Ewald            optimized breakup of 1/r (alea_breakup.cpp; the reference's
+//                    src/numerics/ewald_breakup.cpp:205-276 fits the same χ²)
 //   Padé image sum   u − u∞ split by the same breakup with the Jastrow options
-//                    (src/wavefunction/periodic_pair_sum.cpp:21-60) and the tail
-//                    transform of the Padé (src/numerics/pair_radial.cpp)
+//                    (src/wavefunction/periodic_pair_sum.cpp:21-60)
 //   initial walkers  App::initialize_positions (src/qmc/app.cpp:56-112)
-//
-// The breakup is Natoli & Ceperley, J. Comput. Phys. 117, 171 (1995): a
-// locally piecewise quintic Hermite basis on [0, r_c] whose coefficients are
-// fitted, by Householder QR on the weighted rectangular system, so that the
-// long-range part's transform vanishes above k_cut (lattice shells up to
-// k_continuum, the 2-D density of states (A/2π) k dk beyond).
 #include <algorithm>
 #include <mutex>
 #include <map>
@@ -34,431 +28,12 @@
 #include <vector>
 
 #include "../../include/alea_gpu.h"
+#include "alea_breakup.h"
 
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 2.0 * kPi;
-
-// ───────────────────────── special functions, quadrature ────────────────
-
-// J0: the standard library below x = 40, Hankel's asymptotic expansion
-// (Abramowitz & Stegun 9.2.5, four terms of P and Q) above.
-double bessel_j0(double x) {
-    if (x < 40.0) return std::cyl_bessel_j(0.0, x);
-    const double z = 1.0 / x, z2 = z * z;
-    // a_k from a_k = a_{k-1} (μ − (2k−1)²)/(8k) at μ = 0
-    double a[9];
-    a[0] = 1.0;
-    for (int k = 1; k < 9; ++k) a[k] = a[k - 1] * (0.0 - (2.0 * k - 1) * (2.0 * k - 1)) / (8.0 * k);
-    const double p = a[0] - a[2] * z2 + a[4] * z2 * z2 - a[6] * z2 * z2 * z2 + a[8] * z2 * z2 * z2 * z2;
-    const double q = z * (a[1] - a[3] * z2 + a[5] * z2 * z2 - a[7] * z2 * z2 * z2);
-    const double w = x - 0.25 * kPi;
-    return std::sqrt(2.0 / (kPi * x)) * (p * std::cos(w) - q * std::sin(w));
-}
-
-// 20-point Gauss-Legendre nodes and weights (the positive half).
-const double kGx[10] = {0.0765265211334973, 0.2277858511416451, 0.3737060887154195,
-                        0.5108670019508271, 0.6360536807265150, 0.7463319064601508,
-                        0.8391169718222188, 0.9122344282513259, 0.9639719272779138,
-                        0.9931285991850949};
-const double kGw[10] = {0.1527533871307258, 0.1491729864726037, 0.1420961093183820,
-                        0.1316886384491766, 0.1181945319615184, 0.1019301198172404,
-                        0.0832767415767048, 0.0626720483341091, 0.0406014298003869,
-                        0.0176140071391521};
-
-template <class F>
-double gauss20(F&& f, double a, double b) {
-    const double c = 0.5 * (a + b), h = 0.5 * (b - a);
-    double s = 0.0;
-    for (int i = 0; i < 10; ++i) s += kGw[i] * (f(c + h * kGx[i]) + f(c - h * kGx[i]));
-    return s * h;
-}
-template <class F>
-double gauss20_panels(F&& f, double a, double b, int np) {
-    np = std::max(np, 1);
-    const double h = (b - a) / np;
-    double s = 0.0;
-    for (int i = 0; i < np; ++i) s += gauss20(f, a + i * h, a + (i + 1) * h);
-    return s;
-}
-// panels of about one radian of J0(kr)'s phase
-template <class F>
-double panel_integral(F&& f, double a, double b, double k) {
-    return gauss20_panels(f, a, b, std::clamp(1 + static_cast<int>(k * (b - a)), 1, 4000));
-}
-
-// ───────────────────────── LPQHI basis ──────────────────────────────────
-
-struct Lpqhi {
-    int n_knots = 0;
-    double rc = 0.0, delta = 0.0;
-    static constexpr double S[3][6] = {{1, 0, 0, -10, 15, -6}, {0, 1, 0, -6, 8, -3}, {0, 0, 0.5, -1.5, 1.5, -0.5}};
-    static constexpr double mirror[3] = {1, -1, 1};
-    Lpqhi() = default;
-    Lpqhi(int n, double r) : n_knots(n), rc(r), delta(r / (n - 1)) {}
-    int size() const { return 3 * n_knots; }
-    double lo(int n) const { return std::max(0.0, delta * (n / 3 - 1)); }
-    double hi(int n) const { return std::min(rc, delta * (n / 3 + 1)); }
-    double knot(int i) const { return delta * i; }
-    double h(int n, double r) const {
-        const int i = n / 3, a = n - 3 * i;
-        const double rb = delta * i;
-        if (r < delta * (i - 1) || r > hi(n)) return 0.0;
-        const bool left = r <= rb;
-        const double x = left ? (rb - r) / delta : (r - rb) / delta;
-        double p = 0.0;
-        for (int m = 5; m >= 0; --m) p = p * x + S[a][m];
-        const double s = std::pow(delta, a) * p;
-        return left ? mirror[a] * s : s;
-    }
-};
-
-// body(i) for i in [0, n) on the host's hardware threads (rows of the fit
-// are independent; each writes only its own outputs).
-template <class F>
-void parallel_for(size_t n, F&& body) {
-    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t nt = std::min<size_t>(hw, std::max<size_t>(1, n / 4));
-    if (nt <= 1) {
-        for (size_t i = 0; i < n; ++i) body(i);
-        return;
-    }
-    std::atomic<size_t> next{0};
-    std::vector<std::thread> pool;
-    for (size_t t = 0; t < nt; ++t)
-        pool.emplace_back([&] {
-            for (size_t i; (i = next.fetch_add(1)) < n;) body(i);
-        });
-    for (auto& th : pool) th.join();
-}
-
-struct Radial {
-    std::function<double(double)> value, d1, d2, fourier, tail;
-};
-
-struct BreakupOptions {
-    int n_knots = 20;
-    double k_cut = 0.0, k_continuum = 0.0, k_max = 0.0;
-    int n_continuum = 400;
-};
-
-struct Breakup {
-    Lpqhi basis;
-    std::vector<double> coefs, kx, ky, weight, scaled;
-    std::vector<int> n1, n2;
-    double k_cut = 0.0, residual = 0.0, condition = 0.0, long_range_zero = 0.0, sr_k0 = 0.0;
-};
-
-double basis_transform(const Lpqhi& b, int n, double k) {
-    const int i = n / 3;
-    const double lo = b.lo(n), mid = b.knot(i), hi = b.hi(n);
-    auto f = [&](double r) { return r * bessel_j0(k * r) * b.h(n, r); };
-    double s = 0.0;
-    if (mid > lo) s += panel_integral(f, lo, mid, k);
-    if (hi > mid) s += panel_integral(f, mid, hi, k);
-    return kTwoPi * s;
-}
-
-// Σ over halving panels [b/2, b] from r_c down to 1e-14 r_c of ∫ g.
-template <class G>
-double halving(G&& g, double rc, double k) {
-    double s = 0.0, b = rc;
-    for (int j = 0; j < 60 && b > 1e-14 * rc; ++j) {
-        const double a = 0.5 * b;
-        s += panel_integral(g, a, b, k);
-        b = a;
-    }
-    return s;
-}
-
-// X(k) = −∫_{r > r_c} f e^{−ik·r} d²r
-double fit_target(const Radial& f, double rc, double k) {
-    if (f.tail) return -f.tail(k);
-    const double inner = halving([&](double r) { return r * bessel_j0(k * r) * f.value(r); }, rc, k);
-    return -f.fourier(k) + kTwoPi * inner;
-}
-
-Breakup build_breakup(const double* b, double area, double rc, const Radial& f, const BreakupOptions& opt) {
-    Breakup out;
-    out.basis = Lpqhi(opt.n_knots, rc);
-    const double b1x = b[0], b1y = b[1], b2x = b[2], b2y = b[3];
-    const double b_min = std::min(std::hypot(b1x, b1y), std::hypot(b2x, b2y));
-    const double k_cut = opt.k_cut > 0.0 ? opt.k_cut : 8.0 * b_min;
-    const double k_cont = opt.k_continuum > 0.0 ? opt.k_continuum : 60.0 * kPi / rc;
-    const double k_max = opt.k_max > 0.0 ? opt.k_max : 6000.0 / rc;
-    if (!(k_cut < k_cont && k_cont < k_max)) throw std::invalid_argument("breakup: need k_cut < k_continuum < k_max");
-    out.k_cut = k_cut;
-    // fit rows: exact shells up to k_continuum, then the continuum tail
-    std::vector<double> kf, kw;
-    {
-        const int nmax = static_cast<int>(std::ceil(k_cont / b_min)) + 1;
-        std::vector<double> raw;
-        for (int i = -nmax; i <= nmax; ++i)
-            for (int j = -nmax; j <= nmax; ++j) {
-                if (i == 0 && j == 0) continue;
-                const double k = std::hypot(i * b1x + j * b2x, i * b1y + j * b2y);
-                if (k > k_cut && k <= k_cont) raw.push_back(k);
-            }
-        std::sort(raw.begin(), raw.end());
-        for (size_t a = 0; a < raw.size();) {
-            size_t z = a;
-            while (z < raw.size() && raw[z] - raw[a] < 1e-9 * b_min) ++z;
-            kf.push_back(raw[a]);
-            kw.push_back(static_cast<double>(z - a));
-            a = z;
-        }
-        const double lo = std::log(k_cont), hi = std::log(k_max), dl = (hi - lo) / opt.n_continuum;
-        for (int i = 0; i < opt.n_continuum; ++i) {
-            const double k = std::exp(lo + (i + 0.5) * dl);
-            kf.push_back(k);
-            kw.push_back(area * k * (k * dl) / kTwoPi);
-        }
-    }
-    const int nb = out.basis.size(), nfree = nb - 3;
-    out.coefs.assign(nb, 0.0);
-    out.coefs[nb - 3] = f.value(rc);
-    out.coefs[nb - 2] = f.d1(rc);
-    out.coefs[nb - 1] = f.d2(rc);
-    const size_t nr = kf.size();
-    std::vector<double> cnk(nr * nb), target(nr);
-    parallel_for(nr, [&](size_t r) {
-        for (int n = 0; n < nb; ++n) cnk[r * nb + n] = basis_transform(out.basis, n, kf[r]);
-        double x = fit_target(f, rc, kf[r]);
-        for (int n = nfree; n < nb; ++n) x -= out.coefs[n] * cnk[r * nb + n];
-        target[r] = x;
-    });
-    // weighted least squares by Householder QR
-    std::vector<double> d(nr * nfree), y(nr), diag(nfree, 0.0);
-    for (size_t r = 0; r < nr; ++r) {
-        const double sw = std::sqrt(kw[r]);
-        for (int n = 0; n < nfree; ++n) d[r * nfree + n] = sw * cnk[r * nb + n];
-        y[r] = sw * target[r];
-    }
-    for (int j = 0; j < nfree; ++j) {
-        double norm2 = 0.0;
-        for (size_t r = j; r < nr; ++r) norm2 += d[r * nfree + j] * d[r * nfree + j];
-        const double norm = std::sqrt(norm2);
-        if (norm < 1e-300) continue;
-        const double head = d[static_cast<size_t>(j) * nfree + j];
-        const double alpha = head > 0.0 ? -norm : norm;
-        const double v0 = head - alpha;
-        const double vn2 = norm2 - head * head + v0 * v0;
-        if (vn2 < 1e-300) {
-            diag[j] = alpha;
-            continue;
-        }
-        d[static_cast<size_t>(j) * nfree + j] = v0;
-        for (int c = j + 1; c < nfree; ++c) {
-            double dot = 0.0;
-            for (size_t r = j; r < nr; ++r) dot += d[r * nfree + j] * d[r * nfree + c];
-            const double s = 2.0 * dot / vn2;
-            for (size_t r = j; r < nr; ++r) d[r * nfree + c] -= s * d[r * nfree + j];
-        }
-        double dot = 0.0;
-        for (size_t r = j; r < nr; ++r) dot += d[r * nfree + j] * y[r];
-        const double s = 2.0 * dot / vn2;
-        for (size_t r = j; r < nr; ++r) y[r] -= s * d[r * nfree + j];
-        diag[j] = alpha;
-    }
-    for (int i = nfree - 1; i >= 0; --i) {
-        double s = y[i];
-        for (int j = i + 1; j < nfree; ++j) s -= d[static_cast<size_t>(i) * nfree + j] * out.coefs[j];
-        out.coefs[i] = std::abs(diag[i]) > 1e-300 ? s / diag[i] : 0.0;
-    }
-    {
-        double hi = 0.0, lo = 1e300;
-        for (int i = 0; i < nfree; ++i) {
-            const double a = std::abs(diag[i]);
-            hi = std::max(hi, a);
-            if (a > 1e-300) lo = std::min(lo, a);
-        }
-        out.condition = lo < 1e299 ? hi / lo : 0.0;
-    }
-    out.scaled.resize(nb);
-    for (int n = 0; n < nb; ++n) out.scaled[n] = out.coefs[n] * std::pow(out.basis.delta, n % 3);
-    out.long_range_zero = out.coefs[0];
-    {
-        double integral = kTwoPi * halving([&](double r) { return r * f.value(r); }, rc, 0.0);
-        for (int n = 0; n < nb; ++n) integral -= out.coefs[n] * basis_transform(out.basis, n, 0.0);
-        out.sr_k0 = integral / area;
-    }
-    for (size_t r = 0; r < nr; ++r) {
-        if (kf[r] > k_cont) continue;
-        double resid = target[r];
-        for (int n = 0; n < nfree; ++n) resid -= out.coefs[n] * cnk[r * nb + n];
-        out.residual = std::max(out.residual, std::abs(resid));
-    }
-    // retained half-space vectors and weights f̃_long(k)/A
-    const int nmax = static_cast<int>(std::ceil(k_cut / b_min)) + 1;
-    for (int i = -nmax; i <= nmax; ++i)
-        for (int j = -nmax; j <= nmax; ++j) {
-            if (i < 0 || (i == 0 && j <= 0)) continue;
-            const double kx = i * b1x + j * b2x, ky = i * b1y + j * b2y;
-            const double k = std::hypot(kx, ky);
-            if (k > k_cut || k == 0.0) continue;
-            double fs = 0.0;
-            for (int n = 0; n < nb; ++n) fs += out.coefs[n] * basis_transform(out.basis, n, k);
-            out.kx.push_back(kx);
-            out.ky.push_back(ky);
-            out.weight.push_back((-fit_target(f, rc, k) + fs) / area);
-            out.n1.push_back(i);
-            out.n2.push_back(j);
-        }
-    return out;
-}
-
-// ───────────────────────── Padé radial function ─────────────────────────
-
-// u = P/Q, P = Σ a_k r^k, Q = 1 + Σ b_k r^k, with u' and u''.
-struct Rational {
-    std::vector<double> a, b;
-    void eval(double r, double& u, double& du, double& d2u) const {
-        double p = 0, dp = 0, d2p = 0, q = 1, dq = 0, d2q = 0;
-        for (size_t i = 0; i < a.size(); ++i) {
-            const double k = static_cast<double>(i + 1);
-            p += a[i] * std::pow(r, k);
-            dp += k * a[i] * std::pow(r, k - 1);
-            if (i >= 1) d2p += k * (k - 1) * a[i] * std::pow(r, k - 2);
-        }
-        for (size_t i = 0; i < b.size(); ++i) {
-            const double k = static_cast<double>(i + 1);
-            q += b[i] * std::pow(r, k);
-            dq += k * b[i] * std::pow(r, k - 1);
-            if (i >= 1) d2q += k * (k - 1) * b[i] * std::pow(r, k - 2);
-        }
-        u = p / q;
-        du = (dp - u * dq) / q;
-        d2u = (d2p - 2.0 * du * dq - u * d2q) / q;
-    }
-};
-
-// u(1/x) = A(x)/B(x) as the power series Σ e_j x^j (N ≤ M).
-std::vector<double> large_r_series(const Rational& f, int n) {
-    const size_t M = f.b.size();
-    std::vector<double> A(M + 1, 0.0), B(M + 1, 0.0), e(n, 0.0);
-    for (size_t k = 1; k <= f.a.size(); ++k) A[M - k] += f.a[k - 1];
-    B[M] = 1.0;
-    for (size_t k = 1; k <= M; ++k) B[M - k] += f.b[k - 1];
-    for (int j = 0; j < n; ++j) {
-        double s = j <= static_cast<int>(M) ? A[j] : 0.0;
-        for (int i = 1; i <= j && i <= static_cast<int>(M); ++i) s -= B[i] * e[j - i];
-        e[j] = s / B[0];
-    }
-    return e;
-}
-
-// Largest |root| of 1 + Σ b_k r^k (Durand-Kerner on the monic form).
-double pole_radius(const std::vector<double>& b) {
-    const size_t M = b.size();
-    if (M == 0) return 0.0;
-    std::vector<double> c(M);
-    c[0] = 1.0 / b.back();
-    for (size_t j = 1; j < M; ++j) c[j] = b[j - 1] / b.back();
-    std::vector<std::complex<double>> z(M);
-    for (size_t i = 0; i < M; ++i) z[i] = std::pow(std::complex<double>(0.4, 0.9), static_cast<double>(i));
-    for (int it = 0; it < 500; ++it) {
-        double change = 0.0;
-        for (size_t i = 0; i < M; ++i) {
-            std::complex<double> p = 1.0;
-            for (size_t j = M; j-- > 0;) p = p * z[i] + c[j];
-            std::complex<double> den = 1.0;
-            for (size_t l = 0; l < M; ++l)
-                if (l != i) den *= z[i] - z[l];
-            const std::complex<double> dz = p / den;
-            z[i] -= dz;
-            change = std::max(change, std::abs(dz));
-        }
-        if (change < 1e-14) break;
-    }
-    double r = 0.0;
-    for (const auto& zi : z) r = std::max(r, std::abs(zi));
-    return r;
-}
-
-double smooth_window(double r, double lo, double hi) {
-    if (r <= lo) return 1.0;
-    if (r >= hi) return 0.0;
-    const double t = (r - lo) / (hi - lo);
-    const double p = std::exp(-1.0 / (1.0 - t)), q = std::exp(-1.0 / t);
-    return p / (p + q);
-}
-
-// f = u − u∞ for the breakup, with tail(k) = 2π ∫_{r_c}^∞ r J0(kr) f dr from
-// an analytic large-r model (Σ_n d_n (r² + s²)^{−n/2}, whose 2-D Hankel
-// transforms are Bessel K functions, Gradshteyn & Ryzhik 6.565.4) plus the
-// numerically integrated remainder.
-Radial pade_radial(std::vector<double> a, std::vector<double> b, double rc, double& u_inf) {
-    while (!a.empty() && a.back() == 0.0) a.pop_back();
-    while (!b.empty() && b.back() == 0.0) b.pop_back();
-    if (a.size() > b.size())
-        throw std::invalid_argument("padé: numerator of higher order than the denominator has no image sum");
-    for (int i = 0; i <= 4000; ++i) {
-        const double r = 1e-6 * std::pow(1e14, i / 4000.0);
-        double q = 1.0;
-        for (size_t k = 0; k < b.size(); ++k) q += b[k] * std::pow(r, static_cast<double>(k + 1));
-        if (q <= 0.0) throw std::invalid_argument("padé: the denominator vanishes at some r > 0");
-    }
-    auto f = std::make_shared<const Rational>(Rational{a, b});
-    constexpr int kTerms = 16;
-    const std::vector<double> e = large_r_series(*f, kTerms + 1);
-    u_inf = e[0];
-    const double uinf = u_inf;
-    Radial out;
-    out.value = [f, uinf](double r) { double u, d1, d2; f->eval(r, u, d1, d2); return u - uinf; };
-    out.d1 = [f](double r) { double u, d1, d2; f->eval(r, u, d1, d2); return d1; };
-    out.d2 = [f](double r) { double u, d1, d2; f->eval(r, u, d1, d2); return d2; };
-    const double s = std::max(0.5 * rc, 2.0 * pole_radius(b));
-    std::vector<double> d(kTerms + 1, 0.0);
-    for (int m = 1; m <= kTerms; ++m) {
-        double v = e[m];
-        for (int n = m - 2; n >= 1; n -= 2) {
-            const int i = (m - n) / 2;
-            double c = 1.0;   // binomial C(−n/2, i)
-            for (int t = 0; t < i; ++t) c *= (-0.5 * n - t) / (t + 1);
-            v -= d[n] * c * std::pow(s, m - n);
-        }
-        d[m] = v;
-    }
-    auto model = [d, s](double r) {
-        const double w = 1.0 / std::sqrt(r * r + s * s);
-        double acc = 0.0;
-        for (int n = kTerms; n >= 1; --n) acc = w * (d[n] + acc);
-        return acc;
-    };
-    auto remainder = [f, uinf, model](double r) {
-        double u, d1, d2;
-        f->eval(r, u, d1, d2);
-        return u - uinf - model(r);
-    };
-    const double scale = std::max(std::abs(out.value(rc)) * rc * rc, 1e-300);
-    const double far = 64.0 * std::max(rc, s);
-    double R = 2.0 * rc;
-    while (R < far && std::abs(remainder(R)) * R * R > 1e-12 * scale) R *= 1.2;
-    out.tail = [d, s, model, remainder, rc, R](double k) {
-        const double ks = k * s;
-        double total = 0.0;
-        for (int n = 1; n <= kTerms; ++n) {
-            if (d[n] == 0.0) continue;
-            const double mu = 0.5 * n - 1.0;
-            total += d[n] * std::pow(k / s, mu) * std::cyl_bessel_k(std::abs(mu), ks) /
-                     (std::pow(2.0, mu) * std::tgamma(mu + 1.0));
-        }
-        const int n_in = 1 + static_cast<int>(k * rc + 4.0 * rc / s);
-        total -= gauss20_panels([&](double r) { return r * bessel_j0(k * r) * model(r); }, 0.0, rc, n_in);
-        total += gauss20_panels(
-            [&](double r) { return r * bessel_j0(k * r) * remainder(r) * smooth_window(r, rc, 2.0 * rc); },
-            rc, 2.0 * rc, 40 + static_cast<int>(k * rc));
-        if (k * rc < 100.0)
-            total += gauss20_panels(
-                [&](double r) {
-                    return r * bessel_j0(k * r) * remainder(r) * (1.0 - smooth_window(r, rc, 2.0 * rc));
-                },
-                rc, R, 40 + static_cast<int>(k * (R - rc) + 8.0 * (R - rc) / rc));
-        return kTwoPi * total;
-    };
-    return out;
-}
 
 // ───────────────────────── cell, shells ─────────────────────────────────
 
@@ -732,19 +307,30 @@ struct alea_gpu_setup {
 
 namespace {
 
+using Breakup = alea_breakup::Result;
+
 void set_spline(alea_gpu_setup* S, alea_gpu_spline& sp, const Breakup& br) {
-    sp.r_cut = br.basis.rc;
-    sp.inv_delta = 1.0 / br.basis.delta;
-    sp.n_knots = br.basis.n_knots;
+    sp.r_cut = br.rc;
+    sp.inv_delta = 1.0 / br.delta;
+    sp.n_knots = br.n_knots;
     sp.scaled = S->keep(br.scaled);
 }
 void set_kset(alea_gpu_setup* S, alea_gpu_kset& ks, const Breakup& br) {
     ks.n_k = static_cast<int>(br.weight.size());
-    ks.n1 = S->keepi(br.n1);
-    ks.n2 = S->keepi(br.n2);
-    ks.kx = S->keep(br.kx);
-    ks.ky = S->keep(br.ky);
+    ks.n1 = S->keepi(br.n[0]);
+    ks.n2 = S->keepi(br.n[1]);
+    ks.kx = S->keep(br.kvec[0]);
+    ks.ky = S->keep(br.kvec[1]);
     ks.weight = S->keep(br.weight);
+}
+
+alea_breakup::Lattice lattice_of(const Cell& c) {
+    alea_breakup::Lattice lat;
+    lat.dim = 2;
+    std::copy(c.a, c.a + 4, lat.a);
+    std::copy(c.b, c.b + 4, lat.b);
+    lat.volume = c.area;
+    return lat;
 }
 
 // Coulomb 1/(ε r) Ewald tables (n_knots auto-tuned, default k set).
@@ -760,17 +346,16 @@ std::vector<double> breakup_key(const Cell& c, double kind, std::initializer_lis
     return key;
 }
 
+// The knot count is the smallest of 12, 16, 20, 24 whose fit misfit on the
+// lattice shells is below `tol`.  The fit targets leave out r < r_c 2⁻⁴⁷ as
+// the reference's do (src/numerics/long_range_breakup.cpp fit_target), so
+// that the tables, and the local energies to 1e-10, are the reference's.
 Breakup ewald_breakup_uncached(const Cell& c, double tol) {
-    Radial f;
-    f.value = [](double r) { return 1.0 / r; };
-    f.fourier = [](double k) { return kTwoPi / k; };
-    f.d1 = [](double r) { return -1.0 / (r * r); };
-    f.d2 = [](double r) { return 2.0 / (r * r * r); };
-    Breakup br;
+    const auto f = alea_breakup::coulomb(std::ldexp(1.0, -47));
     for (int nk : {12, 16, 20, 24}) {
-        BreakupOptions opt;
+        alea_breakup::Options opt;
         opt.n_knots = nk;
-        br = build_breakup(c.b, c.area, c.ws, f, opt);
+        Breakup br = alea_breakup::optimize(lattice_of(c), c.ws, *f, opt);
         if (br.residual < tol) return br;
     }
     throw std::runtime_error("ewald: the breakup did not reach the requested tolerance");
@@ -803,13 +388,14 @@ Breakup pade_breakup(const Cell& c, const std::vector<double>& a, const std::vec
             return it->second;
         }
     }
-    const Radial f = pade_radial(a, b, c.ws, u_inf);
-    BreakupOptions opt;
+    const auto f = alea_breakup::rational(a, b, &u_inf);
+    // the Jastrow's options: a shorter continuum and k_cut = 5 |b|_min
+    alea_breakup::Options opt;
     opt.k_continuum = 20.0 * kPi / c.ws;
     opt.k_max = 300.0 / c.ws;
     opt.n_continuum = 150;
     opt.k_cut = 5.0 * std::min(std::hypot(c.b[0], c.b[1]), std::hypot(c.b[2], c.b[3]));
-    Breakup br = build_breakup(c.b, c.area, c.ws, f, opt);
+    Breakup br = alea_breakup::optimize(lattice_of(c), c.ws, *f, opt);
     std::lock_guard<std::mutex> lk(g_breakup_mu);
     g_breakups[key] = br;
     g_breakup_uinf[key] = u_inf;
@@ -1018,7 +604,7 @@ void add_ewald(alea_gpu_setup* S, const Cell& c, double tol, double& self, doubl
         Q += y.groups[g].charge * n;
     }
     self = -0.5 * br.long_range_zero * q2;
-    bg = -0.5 * Q * Q * br.sr_k0;
+    bg = -0.5 * Q * Q * br.short_range_k0;
     y.ewald.constant = self + bg;
 }
 
