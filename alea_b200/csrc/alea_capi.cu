@@ -1236,6 +1236,13 @@ __global__ void __launch_bounds__(256) noalloc_stats_kernel(const double* record
     if (threadIdx.x < 4) out[threadIdx.x] = red[threadIdx.x][0];
 }
 
+// sqrt(τ/m) per coordinate from the device's inverse-mass table (the host's
+// IEEE product and square root, so equal to what alea_gpu_vmc_step stages).
+__global__ void sigma_kernel(double* sigma, const double* inv_mass, int n, double tau) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sigma[i] = sqrt(tau * inv_mass[i]);
+}
+
 }  // namespace
 
 // ───────────────────────── C ABI ────────────────────────────────────────
@@ -1647,13 +1654,11 @@ int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, a
         CUDA_TRY(c, cudaGetSymbolAddress(&p, g_noalloc_scratch));
         c->noalloc_scratch = static_cast<double*>(p);
     }
-    if (prm->tau != c->sigma_tau) {   // sqrt(τ/m) per coordinate, staged from the stack
-        double sg[2 * 1024];
-        const size_t n = c->h_inv_mass.size();
-        if (n > sizeof sg / sizeof sg[0]) return fail(c, ALEA_ERR_UNSUPPORTED, "too many particles");
-        for (size_t i = 0; i < n; ++i) sg[i] = std::sqrt(prm->tau * c->h_inv_mass[i]);
-        CUDA_TRY(c, copy_in(c, c->d_sigma, sg, n * 8));
-        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (prm->tau != c->sigma_tau) {   // sqrt(τ/m) per coordinate, computed on the device
+        const int n = static_cast<int>(c->h_inv_mass.size());
+        ++c->launches;
+        sigma_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(c->d_sigma, c->sys.inv_mass, n, prm->tau);
+        CUDA_TRY(c, cudaGetLastError());
         c->sigma_tau = prm->tau;
     }
     double* rnd = c->noalloc_scratch;
@@ -1672,14 +1677,19 @@ int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, a
     sp.tau = prm->tau;
     sp.sigma = c->d_sigma;
     ++c->launches;
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
     CUDA_TRY(c, launch_sweep(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), rnd, stride, sp, c->pairs,
                              c->npair));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     ++c->launches;
     noalloc_stats_kernel<<<1, 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec, c->sys.o_scal, stats);
     CUDA_TRY(c, cudaGetLastError());
     double h[4];
     CUDA_TRY(c, copy_out(c, h, stats, sizeof h));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
     if (h[3] != 0.0) return fail(c, ALEA_ERR_SINGULAR, "a walker's accepted determinant is singular or nonfinite");
     if (out) {
         *out = alea_gpu_step_stats{};
@@ -1779,9 +1789,11 @@ int alea_gpu_dmc_branch(alea_gpu_ctx* c, uint64_t* state, int target) {
         const size_t i = static_cast<size_t>(rng.uniform() * static_cast<double>(src.size()));
         src.push_back(src[i]);
     }
-    std::memcpy(state, rng.s, 32);
+    // a refused branch leaves the caller's stream where it was, so a retry
+    // with more capacity draws the same multiplicities
     if (static_cast<int>(src.size()) > c->capacity)
         return fail(c, ALEA_ERR_NOMEM, "branching exceeded the walker capacity");
+    std::memcpy(state, rng.s, 32);
     // genealogy (walker_set.cpp:221-238): ids then parents, one plane each
     std::vector<char> seen(n, 0);
     std::vector<double> idpar(2 * src.size());

@@ -104,8 +104,10 @@ struct alea_gpu_server {
             rc = sp.mode == ALEA_JOB_DMC ? alea_gpu_dmc_run(ctx, &sp.run, &r, nullptr)
                                          : alea_gpu_vmc_run(ctx, &sp.run, &r, nullptr);
         if (rc == ALEA_OK && j->cancel.load()) rc = ALEA_ERR_CANCELLED;
-        finish(j, rc, rc == ALEA_OK ? &r : nullptr);
+        // the context's memory goes back to the device before the job's bytes
+        // go back to the budget, so the next admission cannot overcommit
         if (ctx) alea_gpu_destroy(ctx);
+        finish(j, rc, rc == ALEA_OK ? &r : nullptr);
     }
 
     void worker() {
@@ -180,6 +182,7 @@ int alea_gpu_poll(alea_gpu_server* s, uint64_t job_id, int timeout_ms, alea_gpu_
         s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return j->done; });
     if (!j->done) return ALEA_ERR_TIMEOUT;
     *out = j->res;
+    s->jobs.erase(it);   // a finished job's result is handed out once
     return ALEA_OK;
 }
 

@@ -335,7 +335,8 @@ int alea_gpu_vmc_steps(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, int n_
  *     reading it, so nothing in it needs to start at zero.
  *   - alea_gpu_set_streams must have been called (that call may allocate).
  * Results equal alea_gpu_vmc_step's: same kernels, same random numbers;
- * the energy sums are reduced on the device (rounding order differs). */
+ * the energy sums are reduced on the device (rounding order differs).
+ * alea_gpu_last_kernel_ms reports the step's sweep, as after a VMC step. */
 #define ALEA_GPU_NOALLOC_RANDOMS 1048576
 int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* ctx, const alea_gpu_vmc_params* prm, alea_gpu_step_stats* out);
 
@@ -716,7 +717,8 @@ int alea_gpu_submit_job(alea_gpu_server* s, const alea_gpu_job* job, uint64_t* j
 /* Wait at most timeout_ms (0: do not wait) for a job: ALEA_OK with *out
  * filled when it has finished (out->status tells how), ALEA_ERR_TIMEOUT when
  * it is still queued or running, ALEA_ERR_INVALID for an unknown id.  A
- * finished job's result stays readable until the server is destroyed. */
+ * finished job's result is handed out once: the poll that returns it drops
+ * the job, and later polls of its id return ALEA_ERR_INVALID. */
 int alea_gpu_poll(alea_gpu_server* s, uint64_t job_id, int timeout_ms, alea_gpu_job_result* out);
 /* Cancel a queued job at once, or a running one at its next step
  * (status ALEA_ERR_CANCELLED); ALEA_ERR_INVALID for an unknown or finished id. */

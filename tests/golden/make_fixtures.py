@@ -28,7 +28,10 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
   (carry_over_walkers): DMC populations and weighted energy sums per step;
 * ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
   reduced here to accumulation-block energies, their mean and its reblocked
-  standard error (the statistical reference for the device's DMC).
+  standard error (the statistical reference for the device's DMC);
+* ``vmc_<name>_crowd.json`` / ``dmc_<name>_crowd.json`` VMC::run / DMC::run
+  with fewer threads than walkers: each thread's stream serves a contiguous
+  range of walkers (VMC's per-thread clones, DMC's crowds).
 """
 from __future__ import annotations
 
@@ -49,6 +52,8 @@ SYSTEMS = {
     "dipoles16": dict(system="dipoles", n=16),
     "heg10t": dict(system="heg", nu=5, nd=5, rs=30, tx=0.25, ty=0.125),
     "heg10bf": dict(system="heg", nu=5, nd=5, rs=30, bf=1),
+    # the 10 x 12 Wigner crystal (120 electrons, 60 per spin) at r_s = 40
+    "crystal120": dict(system="crystal", nx=10, ny=12, rs=40),
     # the crystal with its Drummond alpha_0, an alpha_2 term and L optimisable
     "crystal16p": dict(system="crystal", nx=4, ny=4, rs=40, drummond_free=1, alpha0=-2e-3,
                        alpha2=3e-8, gauss_free=1),
@@ -63,6 +68,7 @@ VMC = {
     "heg10t_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
     "heg10bf": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=225.0),
     "heg10bf_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
+    "crystal120": dict(nw=4, seed=19, eq=0, acc=1, steps=2, substeps=1, tau=400.0),
 }
 DMC = {
     "exciton": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.05),
@@ -70,7 +76,12 @@ DMC = {
     "dipoles16": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=1e-5),
     "heg10t": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
     "heg10bf": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
+    "heg42": dict(nw=16, seed=5, eq=1, acc=2, steps=3, substeps=1, tau=0.5),
 }
+
+# Fewer threads (streams, crowds) than walkers: contiguous walker ranges.
+VMC_CROWD = {"heg42": dict(nw=64, seed=11, eq=1, acc=2, steps=2, substeps=1, tau=225.0, threads=4)}
+DMC_CROWD = {"heg42": dict(nw=32, seed=5, eq=1, acc=2, steps=3, substeps=1, tau=0.5, threads=4)}
 
 
 # Observable estimators (gofr / density / sofk), with the argument names of
@@ -99,6 +110,7 @@ CHAIN = {
 
 DMC_STAT = {
     "heg10": dict(nw=1024, seed=424242, eq=10, acc=50, steps=10, substeps=1, tau=0.5, threads=8),
+    "heg42": dict(nw=1024, seed=424243, eq=10, acc=40, steps=10, substeps=1, tau=0.5, threads=8),
 }
 
 
@@ -141,6 +153,23 @@ def fw_fixtures(only=None):
         dump(f"fw_dmc_{name}.json", {"params": DMC[name], "est": EST[name], "fw": fw,
                                      "estimators": r["estimators"], "walkers": r["walkers"],
                                      "initial_positions": r["initial_positions"]})
+
+
+def crowd_fixtures(only=None):
+    for name, run in VMC_CROWD.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("vmc", **run, **SYSTEMS[name])
+        r["params"] = run
+        r["system"] = name
+        dump(f"vmc_{name}_crowd.json", r)
+    for name, run in DMC_CROWD.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("dmc", **run, **SYSTEMS[name])
+        r["params"] = run
+        r["system"] = name
+        dump(f"dmc_{name}_crowd.json", r)
 
 
 def chain_fixtures(only=None):
@@ -194,6 +223,7 @@ def main(only=None):
         r = run_ref_harness("dmc", **DMC[key], **EST[name], **SYSTEMS[name])
         dump(f"est_dmc_{name}.json", {"params": DMC[key], "est": EST[name], "estimators": r["estimators"],
                                       "walkers": r["walkers"], "final_positions": r["final_positions"]})
+    crowd_fixtures(only)
     chain_fixtures(only)
     fw_fixtures(only)
     ckpt_fixtures(only)

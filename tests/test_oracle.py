@@ -12,7 +12,7 @@ from conftest import golden
 from oracle import Oracle
 from oracle.oracle import S_EL, S_LOGPSI, load_oracle_lib
 
-SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t", "heg10bf"]
+SYSTEMS = ["exciton", "heg10", "crystal16", "heg42", "dipoles16", "heg10t", "heg10bf", "crystal120"]
 
 
 def rel(a, b):
@@ -70,17 +70,23 @@ def test_oracle_evaluate_matches_reference(name):
 
 
 @pytest.mark.parametrize("name", ["exciton", "heg10", "heg10_drift", "crystal16", "dipoles16",
-                                  "heg10t", "heg10t_drift", "heg10bf", "heg10bf_drift"])
+                                  "heg10t", "heg10t_drift", "heg10bf", "heg10bf_drift", "crystal120",
+                                  "heg42_crowd"])
 def test_oracle_vmc_matches_reference(name):
     r = golden(f"vmc_{name}.json")
     p = r["params"]
     o = Oracle(golden(f"setup_{r['system']}.json"))
     o.init(np.array(r["initial_positions"]))
-    el, st = o.vmc(p["nw"], p["seed"], p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"],
+    T = p.get("threads", p["nw"])
+    el, st = o.vmc(T, p["seed"], p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"],
                    drift=bool(p.get("drift", 0)))
     n_eq_steps = p["eq"] * p["steps"]
-    ref_el = np.array(r["thread_local_energy"])          # [walker][accumulation step]
-    assert rel(el[n_eq_steps:].T, ref_el) < 1e-10
+    # thread t's list: its contiguous walkers' E_L, step after step
+    nw = p["nw"]
+    lo = [t * (nw // T) + min(t, nw % T) for t in range(T + 1)]
+    mine = [el[n_eq_steps:, lo[t]:lo[t + 1]].ravel() for t in range(T)]
+    for t in range(T):
+        assert rel(mine[t], r["thread_local_energy"][t]) < 1e-10
     assert st[0] / st[1] == pytest.approx(r["acceptance"], abs=0, rel=1e-15)
     fp = np.array(r["final_positions"]).reshape(p["nw"], -1)
     if p.get("drift", 0):
@@ -90,13 +96,14 @@ def test_oracle_vmc_matches_reference(name):
         assert np.array_equal(o.pos()[: p["nw"]], fp)
 
 
-@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t", "heg10bf"])
+@pytest.mark.parametrize("name", ["exciton", "heg10", "dipoles16", "heg10t", "heg10bf", "heg42",
+                                  "heg42_crowd"])
 def test_oracle_dmc_matches_reference(name):
     r = golden(f"dmc_{name}.json")
     p = r["params"]
-    o = Oracle(golden(f"setup_{name}.json"))
+    o = Oracle(golden(f"setup_{r['system']}.json"))
     o.init(np.array(r["initial_positions"]), capacity=4 * p["nw"] + 4)
-    tr = o.dmc(p["nw"], p["seed"], p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"],
+    tr = o.dmc(p.get("threads", p["nw"]), p["seed"], p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"],
                target=p["nw"])
     n_eq_steps = p["eq"] * p["steps"]
     pops_ref = [len(x) for x in r["local_energy"]]

@@ -20,21 +20,26 @@ E_L_RTOL = 1e-10
 SUM_RTOL = 1e-12
 
 
-def _pair():
+def _pair(name="heg10", precision="fp64"):
     import alea_b200
-    setup = golden("setup_heg10.json")
-    pos = np.array(golden("eval_heg10.json")["positions"])
+    setup = golden(f"setup_{name}.json")
+    pos = np.array(golden(f"eval_{name}.json")["positions"])
     nw = pos.shape[0]
     a = alea_b200.Walkers(setup, capacity=nw)
     b = alea_b200.Walkers(setup, capacity=nw)
     for g in (a, b):
         g.upload(pos)
+        if precision != "fp64":
+            g.set_precision(precision)
         g.set_streams(5, alea_b200.STREAM_VMC, nw)
     return a, b
 
 
-def test_noalloc_step_matches_vmc_step_twice():
-    a, b = _pair()
+# the one-warp FP64 sweep, its FP32 form, and the generic CTA sweep (the
+# backflow determinant), each stepped through both entry points
+@pytest.mark.parametrize("name,precision", [("heg10", "fp64"), ("heg10", "fp32"), ("heg10bf", "fp64")])
+def test_noalloc_step_matches_vmc_step_twice(name, precision):
+    a, b = _pair(name, precision)
     for call, (tau, n_sub, drift) in enumerate([(225.0, 2, False), (100.0, 1, True)]):
         sa = a.vmc_step(tau, n_sub, drift)
         sb = b.vmc_step_noalloc(tau, n_sub, drift)
@@ -45,6 +50,7 @@ def test_noalloc_step_matches_vmc_step_twice():
         assert sb.n_proposed == sa.n_proposed and sb.n_walkers == sa.n_walkers
         assert sb.energy_sum == pytest.approx(sa.energy_sum, rel=SUM_RTOL)
         assert sb.energy_sq_sum == pytest.approx(sa.energy_sq_sum, rel=SUM_RTOL)
+        assert b.last_kernel_ms() > 0.0      # the sweep of this call was timed
     a.close()
     b.close()
 
