@@ -128,3 +128,25 @@ def test_twisted_builder_evaluates_like_the_oracle():
     ph = g.download_phase()
     assert np.max(np.abs(ph["phase_grad"] - o.phase_grad()[:4])) < 1e-10 * max(1.0, np.abs(o.phase_grad()).max())
     g.close()
+
+
+@pytest.mark.gpu
+def test_budget_of_one_job_runs_jobs_one_after_another():
+    """A server whose memory budget holds exactly one job's footprint: two
+    jobs in a row both run (the second is admitted only once the first's
+    context has released its memory) and a polled job is forgotten."""
+    import alea_b200
+    st, mode, tau = _jobs()[0]
+    pos = st.positions(5, 64)
+    probe = alea_b200.Server(max_running=1)
+    r = probe.poll(probe.submit(st.desc, pos, 0, 1, 1, 1, 1, tau, seed=1), timeout_ms=60000)
+    probe.close()
+    assert r is not None and r.status == 0 and r.footprint_bytes > 0
+    srv = alea_b200.Server(hbm_budget_bytes=int(r.footprint_bytes), max_running=2)
+    ids = [srv.submit(st.desc, pos, 0, 1, 2, 2, 1, tau, seed=2 + k) for k in range(2)]
+    res = [srv.poll(i, timeout_ms=60000) for i in ids]
+    assert all(x is not None and x.status == 0 for x in res)
+    assert res[1].queue_ms >= res[0].run_ms * 0.5       # it waited for the first to finish
+    with pytest.raises(alea_b200.AleaGpuError):
+        srv.poll(ids[0], timeout_ms=0)                  # handed out once
+    srv.close()
