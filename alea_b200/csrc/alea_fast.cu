@@ -382,6 +382,7 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                 double2* Dl = reinterpret_cast<double2*>(rec + B.oDl) + jrow * N;
                 double* rabs = v.scal - s.o_scal + B.orabs;
                 const double R = acc[0];
+                const double inv_r = 1.0 / R;
                 __syncwarp();   // the new orbital row v.nval
 #pragma unroll 1
                 for (int c = lane; c < N; c += 32) {
@@ -393,7 +394,7 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
                     }
                     if (m < N) pa += v.nval[m] * A[m * N + c];
                     v.rowp[c] = (pa + pb) - (c == jrow ? 1.0 : 0.0);
-                    v.col[c] = A[c * N + jrow] / R;   // factor of row c of the update
+                    v.col[c] = A[c * N + jrow] * inv_r;   // factor of row c of the update
                     __stcg(D + jrow * N + c, v.nval[c]);
                     __stcg(Dg + c, make_double2(v.ngrad[c * 2], v.ngrad[c * 2 + 1]));
                     __stcg(Dl + c, make_double2(v.nlap[c * 2], v.nlap[c * 2 + 1]));

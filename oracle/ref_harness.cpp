@@ -20,6 +20,11 @@
 //   MODE chain  : VMC, then DMC seeded from VMC's final configurations
 //   MODE estimate : accumulate the estimators (gofr / density / sofk) over
 //                   fixed configurations with given weights, print their series
+//   MODE gpu_pair : (ref_harness_gpu only, built with the reference-side GPU
+//                   drivers of alea_b200/adapter) the reference's VMC or DMC
+//                   (method=vmc|dmc) and GpuVMC / GpuDMC on copies of the same
+//                   ensemble, the system flattened by alea::gpu::pack_system
+//                   from the objects built here; both traces printed
 // vmc and dmc attach the same estimators when gofr_bins, dens_bins or
 // sofk_kmax is given, and print the estimators' series of run_result().
 #include <omp.h>
@@ -60,6 +65,10 @@
 #include "wavefunction/slater_determinant.h"
 #include "wavefunction/trial_wavefunction.h"
 #include "wavefunction/zero_energy_jastrow.h"
+
+#ifdef ALEA_GPU_DRIVER
+#include "../alea_b200/adapter/alea_gpu_driver.h"
+#endif
 
 using namespace alea;
 
@@ -165,6 +174,9 @@ struct System {
     std::vector<double> anchors;         // [np*dim] crystal sites per particle
     double jitter = 0.0;
     Json setup;                          // system description
+#ifdef ALEA_GPU_DRIVER
+    std::vector<gpu::PadeTermSpec> pade_specs;   // what pack_system cannot read off a PadeJastrow
+#endif
 };
 
 void dump_cell(Json& j, const SimulationCell& c) {
@@ -442,6 +454,9 @@ std::unique_ptr<System> build_heg(const Args& a) {
                                           Parameter{"pade_0", bden, false}};
             auto pj = std::make_unique<PadeJastrow>(1, 1, A, B, params);
             pj->sum_over_images(s->cell);
+#ifdef ALEA_GPU_DRIVER
+            s->pade_specs.push_back({pj.get(), A, B, 1, 1});
+#endif
             j.open('{');
             j.arr("ga", std::vector<double>{double(A.first), double(A.last)});
             j.arr("gb", std::vector<double>{double(B.first), double(B.last)});
@@ -1103,6 +1118,63 @@ int run(const std::string& mode, const Args& a) {
         out.arr("weight_sum", wsum);
         out.arr("weighted_energy_sum", ewsum);
         out.arr("final_positions", dmc.final_configurations());
+#ifdef ALEA_GPU_DRIVER
+    } else if (mode == "gpu_pair") {
+        const std::string method = gets(a, "method", "dmc");
+        const gpu::PackedSystem packed = gpu::pack_system(ens, sys->psi, sys->ham, sys->pade_specs);
+        WalkerEnsemble ens_gpu = ens;
+        put_positions(out, "initial_positions", ens);
+        const int threads = static_cast<int>(geti(a, "threads", static_cast<long long>(nw)));
+        if (method == "vmc") {
+            VMCConfig c;
+            c.n_equilibration_blocks = static_cast<int>(geti(a, "eq", 0));
+            c.n_accumulation_blocks = static_cast<int>(geti(a, "acc", 2));
+            c.n_steps = static_cast<int>(geti(a, "steps", 3));
+            c.n_substeps = static_cast<int>(geti(a, "substeps", 1));
+            c.tau = getd(a, "tau", 1.0);
+            c.n_threads = threads;
+            c.seed = seed;
+            VMC ref(c, ens, sys->psi, sys->ham);
+            ref.run();
+            gpu::GpuVMC dev(c, ens_gpu, packed);
+            dev.run();
+            out.arr("ref_block_energies", ref.block_energies());
+            out.arr("gpu_block_energies", dev.block_energies());
+            out.kv("ref_energy", ref.energy());
+            out.kv("gpu_energy", dev.energy());
+            out.kv("ref_acceptance", ref.acceptance_ratio());
+            out.kv("gpu_acceptance", dev.acceptance_ratio());
+            out.arr("ref_final_positions", ref.final_configurations());
+            out.arr("gpu_final_positions", dev.final_configurations());
+            out.ks("gpu_summary", dev.summary());
+        } else {
+            DMCConfig c;
+            c.n_equilibration_blocks = static_cast<int>(geti(a, "eq", 0));
+            c.n_accumulation_blocks = static_cast<int>(geti(a, "acc", 1));
+            c.n_steps = static_cast<int>(geti(a, "steps", 3));
+            c.n_substeps = static_cast<int>(geti(a, "substeps", 1));
+            c.tau = getd(a, "tau", 0.5);
+            c.n_threads = threads;
+            c.seed = seed;
+            c.population_generations = getd(a, "generations", 10.0);
+            DMC ref(c, ens, sys->psi, sys->ham);
+            ref.run();
+            gpu::GpuDMC dev(c, ens_gpu, packed);
+            dev.run();
+            out.arr("ref_block_energies", ref.block_energies());
+            out.arr("gpu_block_energies", dev.block_energies());
+            out.kv("ref_energy", ref.energy());
+            out.kv("gpu_energy", dev.energy());
+            out.kv("ref_energy_error", ref.energy_error());
+            out.kv("gpu_energy_error", dev.energy_error());
+            out.arr("ref_final_positions", ref.final_configurations());
+            out.arr("gpu_final_positions", dev.final_configurations());
+            out.ks("gpu_summary", dev.summary());
+            const RunResult rr = dev.run_result();
+            out.ks("gpu_method", rr.method);
+            out.ki("gpu_result_scalars", static_cast<long long>(rr.scalars.size()));
+        }
+#endif
     } else if (mode == "estimate") {
         // acc blocks of `steps` configurations each: configuration (b, s) is a
         // fresh App initialisation from init_seed + 1000 b + s, walker w
