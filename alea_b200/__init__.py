@@ -575,6 +575,27 @@ class Walkers:
                          streams, seed, target=target, generations=generations, n_blocks_out=n_acc)
 
 
+def vmc_run_packed(walkers: Sequence["Walkers"], runs: Sequence[Dict[str, Any]]):
+    """alea_gpu_vmc_run_packed: the VMC runs of several contexts, every step
+    one packed sweep launch for all of them.  runs[i] holds vmc_run's
+    arguments for walkers[i] (n_eq, n_acc, n_steps, n_substeps, tau, streams,
+    seed, drift).  Returns [(RunResult, status)]."""
+    lib = _load()
+    n = len(walkers)
+    ctxs = (ctypes.c_void_p * n)(*[w.ctx for w in walkers])
+    cfgs = (_capi.RunConfig * n)()
+    for i, r in enumerate(runs):
+        cfgs[i] = _capi.RunConfig(r["n_eq"], r["n_acc"], r["n_steps"], r["n_substeps"], r["tau"],
+                                  1 if r.get("drift") else 0, r["streams"], ctypes.c_uint64(r["seed"]), 0,
+                                  10.0, 2.0)
+    res = (_capi.RunResult * n)()
+    st = (ctypes.c_int * n)()
+    rc = lib.alea_gpu_vmc_run_packed(ctxs, n, cfgs, res, st)
+    if rc != 0:
+        raise AleaGpuError(rc, lib.alea_gpu_last_error(None).decode())
+    return [(res[i], st[i]) for i in range(n)]
+
+
 class Server:
     """Serving front end over alea_gpu_server (include/alea_gpu.h, serving):
     jobs are queued, admitted by device-memory footprint and run

@@ -193,6 +193,7 @@ EXPORTS = [
     "alea_gpu_vmc_steps", "alea_gpu_dmc_steps", "alea_gpu_set_checkpoint_hook",
     "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
     "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
+    "alea_gpu_vmc_run_packed",
 ]
 
 _LIB = None
@@ -226,6 +227,8 @@ def load() -> ctypes.CDLL:
         "alea_gpu_dmc_advance": ([P, ctypes.POINTER(DmcParams), ctypes.POINTER(StepStats)], I),
         "alea_gpu_dmc_branch": ([P, ctypes.POINTER(ctypes.c_uint64), I], I),
         "alea_gpu_vmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),
+        "alea_gpu_vmc_run_packed": ([ctypes.POINTER(P), I, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult),
+                                     ctypes.POINTER(I)], I),
         "alea_gpu_dmc_run": ([P, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult), c_dp], I),
         "alea_gpu_last_kernel_ms": ([P, c_dp], I),
         "alea_gpu_stream": ([P, ctypes.POINTER(P)], I),

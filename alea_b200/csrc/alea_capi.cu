@@ -232,6 +232,7 @@ struct alea_gpu_ctx {
     void* ckpt_user = nullptr;
     int prop_p = -1;               // alea_gpu_propose: the proposed particle and its positions [dim*nw]
     std::vector<double> prop_pos;
+    DevSys* d_sys = nullptr;       // device copy of sys for packed launches (alea_gpu_vmc_run_packed)
 };
 
 namespace {
@@ -1331,7 +1332,8 @@ int alea_gpu_destroy(alea_gpu_ctx* c) {
                     static_cast<void*>(c->randoms), static_cast<void*>(c->streams), static_cast<void*>(c->pairs),
                     static_cast<void*>(c->d_buf), static_cast<void*>(c->d_sigma), static_cast<void*>(c->d_src),
                     static_cast<void*>(c->d_mask), static_cast<void*>(c->d_opt), static_cast<void*>(c->d_opt_out),
-                    static_cast<void*>(c->d_opt_grad), static_cast<void*>(c->d_opt_scratch)})
+                    static_cast<void*>(c->d_opt_grad), static_cast<void*>(c->d_opt_scratch),
+                    static_cast<void*>(c->d_sys)})
         if (p && c->stream) cudaFreeAsync(p, c->stream);
     if (c->stream) alea_gpu::est_free(c->est, c->stream);
     if (c->stream) fw_free(c);
@@ -1866,6 +1868,556 @@ int alea_gpu_last_kernel_ms(const alea_gpu_ctx* c, double* ms) {
     *ms = c->last_ms;
     return ALEA_OK;
 }
+
+}  // extern "C"
+
+// ───────────────────────── packed VMC runs ──────────────────────────────
+//
+// Several contexts' VMC runs stepped together: every step draws each run's
+// random numbers and then sweeps the walkers of all runs in one launch per
+// sweep body (the one-warp body for the runs that take it, the generic
+// 32-thread body for the others), with each run's own system, records and
+// parameters (BatchJob).  Per-chain E_L sums of each run reduce on the device
+// in walker order and come back in one copy per step, so a run's blocks,
+// energy, error and acceptance are those of alea_gpu_vmc_run on its own
+// context.  The launch shape of each body (one CTA per walker, or persistent
+// CTAs over a work counter, as many as the occupancy calculator allows) is
+// picked by timing both on the first steps (PackedTuner); once a step's set
+// of runs repeats, the step is captured into a CUDA graph and replayed until
+// a run joins or leaves.
+
+namespace {
+
+// A packed run's per-step sums, in alea_gpu_vmc_run's order and rounding:
+// state = [step, block, blk[T] (running block sums), e_sum, e2_sum] persists
+// on the device across steps.  One thread adds every walker's E_L in walker
+// order to its chain's block sum and, in accumulation blocks, to the running
+// Σ E_L and Σ E_L² (no contraction, as the host sums); the block sums reset
+// when a block starts.  Other threads sum the accepted moves and the largest
+// |error flag|.  out = [blk[T], e_sum, e2_sum, Σ accepted, max |error|].
+__global__ void run_sums_kernel(const double* records, int nw, long rec, int o_scal, int T, int n_steps,
+                                int n_eq, double* state, double* out) {
+    if (threadIdx.x == 0) {
+        double* blk = state + 2;
+        const int step = static_cast<int>(state[0]), block = static_cast<int>(state[1]);
+        if (step == 0)
+            for (int t = 0; t < T; ++t) blk[t] = 0.0;
+        const bool measure = block >= n_eq;
+        double e = state[2 + T], e2 = state[3 + T];
+        const int base = nw / T, rem = nw % T;
+        for (int t = 0; t < T; ++t) {
+            const int w0 = t * base + min(t, rem), cnt = base + (t < rem ? 1 : 0);
+            double b = blk[t];
+            for (int w = w0; w < w0 + cnt; ++w) {
+                const double el = records[static_cast<size_t>(w) * rec + o_scal + S_EL];
+                b = __dadd_rn(b, el);
+                if (measure) {
+                    e = __dadd_rn(e, el);
+                    e2 = __dadd_rn(e2, __dmul_rn(el, el));
+                }
+            }
+            blk[t] = b;
+            out[t] = b;
+        }
+        state[2 + T] = e;
+        state[3 + T] = e2;
+        out[T] = e;
+        out[T + 1] = e2;
+        const int next = step + 1 == n_steps ? 0 : step + 1;
+        state[0] = next;
+        if (next == 0) state[1] = block + 1;
+    }
+    __shared__ double red[2][256];
+    double na = 0.0, er = 0.0;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+        const double* r = records + static_cast<size_t>(w) * rec + o_scal;
+        na += r[S_NACC];
+        er = fmax(er, fabs(r[S_ERR]));
+    }
+    red[0][threadIdx.x] = na;
+    red[1][threadIdx.x] = er;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + h];
+            red[1][threadIdx.x] = fmax(red[1][threadIdx.x], red[1][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[T + 2] = red[0][0];
+        out[T + 3] = red[1][0];
+    }
+}
+
+// Launch shapes of the packed bodies: for each body (0 one-warp, 1 generic)
+// the measured time per walker-sweep of shape 0 (one CTA per walker) and
+// shape 1 (persistent CTAs); the faster one is kept for the device's
+// lifetime (every packed run of the process shares the table).
+struct PackedTuner {
+    std::mutex mu;
+    double ms_per_walker[64][2][2] = {};
+    int samples[64][2][2] = {};
+    int choice(int dev, int body) {
+        std::lock_guard<std::mutex> lk(mu);
+        for (int shape = 0; shape < 2; ++shape)
+            if (samples[dev][body][shape] < 2) return shape;   // still measuring
+        return ms_per_walker[dev][body][1] < ms_per_walker[dev][body][0] ? 1 : 0;
+    }
+    bool settled(int dev, int body) {
+        std::lock_guard<std::mutex> lk(mu);
+        return samples[dev][body][0] >= 2 && samples[dev][body][1] >= 2;
+    }
+    void record(int dev, int body, int shape, double ms_per_w) {
+        std::lock_guard<std::mutex> lk(mu);
+        int& n = samples[dev][body][shape];
+        double& m = ms_per_walker[dev][body][shape];
+        m = (m * n + ms_per_w) / (n + 1);
+        ++n;
+    }
+};
+PackedTuner g_packed_tuner;
+
+struct PackedRunState {
+    alea_gpu_ctx* c = nullptr;
+    alea_gpu_run_config cfg{};
+    int T = 1;
+    int block = 0, step = 0;
+    bool fast = false;
+    size_t smem = 0;
+    size_t stats_off = 0;
+    double* d_state = nullptr;     // run_sums_kernel's [step, block, blk[T], e_sum, e2_sum]
+    std::vector<std::vector<double>> chain;
+    std::vector<double> blk;
+    std::vector<int64_t> blk_n;
+    double e_sum = 0.0, e2_sum = 0.0;
+    int64_t n_tot = 0, acc = 0, prop = 0, moves = 0, evals = 0;
+    std::chrono::steady_clock::time_point t0;
+    bool done = false;
+    int status = ALEA_OK;
+    alea_gpu_run_result res{};
+    std::vector<double> blocks;
+};
+
+}  // namespace
+
+struct alea_gpu_packed {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<PackedRunState> runs;
+    bool dirty = true;
+    BatchJob* d_jobs = nullptr;
+    BatchJob* h_jobs = nullptr;   // pinned
+    int jobs_cap = 0;
+    double* d_stats = nullptr;
+    double* h_stats = nullptr;    // pinned
+    size_t stats_cap = 0;
+    int* d_next = nullptr;
+    int n_fast = 0, n_gen = 0, total_fast = 0, total_gen = 0;
+    size_t smem_fast = 0, smem_gen = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_shapes[2] = {-1, -1};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::string err;
+    uint64_t launches = 0;
+};
+
+namespace {
+
+int pfail(alea_gpu_packed* P, int code, const std::string& msg) {
+    P->err = msg;
+    return code;
+}
+
+#define PCUDA(P, expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return pfail((P), ALEA_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void packed_drop_graph(alea_gpu_packed* P) {
+    if (P->graph) cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+}
+
+// Job tables, stats slots and the shared-memory reservation of the runs still
+// going, after one joined or left.
+int packed_rebuild(alea_gpu_packed* P) {
+    packed_drop_graph(P);
+    std::vector<BatchJob> fast, gen;
+    size_t stats = 0;
+    P->smem_fast = P->smem_gen = 0;
+    for (PackedRunState& r : P->runs) {
+        if (r.done) continue;
+        alea_gpu_ctx* c = r.c;
+        if (int rc = ensure_randoms(c, r.cfg.n_substeps)) return pfail(P, rc, c->err);
+        if (int rc = set_sigma(c, r.cfg.tau)) return pfail(P, rc, c->err);
+        if (!c->d_sys) PCUDA(P, cudaMallocAsync(&c->d_sys, sizeof(DevSys), c->stream));
+        if (!r.d_state) {
+            PCUDA(P, cudaMallocAsync(&r.d_state, 8 * (static_cast<size_t>(r.T) + 4), P->stream));
+            PCUDA(P, cudaMemsetAsync(r.d_state, 0, 8 * (static_cast<size_t>(r.T) + 4), P->stream));
+        }
+        PCUDA(P, cudaMemcpyAsync(c->d_sys, &c->sys, sizeof(DevSys), cudaMemcpyHostToDevice, c->stream));
+        PCUDA(P, cudaStreamSynchronize(c->stream));
+        BatchJob j{};
+        j.sys = c->d_sys;
+        j.records = records(c);
+        j.randoms = c->randoms;
+        j.stride = c->nw;
+        j.prm.mode = 0;
+        j.prm.n_sub = r.cfg.n_substeps;
+        j.prm.drift = r.cfg.use_drift;
+        j.prm.tau = r.cfg.tau;
+        j.prm.sigma = c->d_sigma;
+        j.pairs = c->pairs;
+        j.npair = c->npair;
+        j.nw = c->nw;
+        auto& list = r.fast ? fast : gen;
+        int& total = r.fast ? P->total_fast : P->total_gen;
+        if (list.empty()) total = 0;
+        j.first = total;
+        total += c->nw;
+        list.push_back(j);
+        (r.fast ? P->smem_fast : P->smem_gen) = std::max(r.fast ? P->smem_fast : P->smem_gen, r.smem);
+        r.stats_off = stats;
+        stats += static_cast<size_t>(r.T) + 4;
+    }
+    P->n_fast = static_cast<int>(fast.size());
+    P->n_gen = static_cast<int>(gen.size());
+    if (fast.empty()) P->total_fast = 0;
+    if (gen.empty()) P->total_gen = 0;
+    const int need = P->n_fast + P->n_gen;
+    if (need > P->jobs_cap) {
+        if (P->d_jobs) cudaFreeAsync(P->d_jobs, P->stream);
+        if (P->h_jobs) cudaFreeHost(P->h_jobs);
+        P->d_jobs = nullptr;
+        P->h_jobs = nullptr;
+        const int cap = std::max(need, 2 * P->jobs_cap);
+        PCUDA(P, cudaMallocAsync(&P->d_jobs, sizeof(BatchJob) * cap, P->stream));
+        PCUDA(P, cudaMallocHost(&P->h_jobs, sizeof(BatchJob) * cap));
+        P->jobs_cap = cap;
+    }
+    if (stats > P->stats_cap) {
+        if (P->d_stats) cudaFreeAsync(P->d_stats, P->stream);
+        if (P->h_stats) cudaFreeHost(P->h_stats);
+        P->d_stats = nullptr;
+        P->h_stats = nullptr;
+        const size_t cap = std::max(stats, 2 * P->stats_cap);
+        PCUDA(P, cudaMallocAsync(&P->d_stats, 8 * cap, P->stream));
+        PCUDA(P, cudaMallocHost(&P->h_stats, 8 * cap));
+        P->stats_cap = cap;
+    }
+    if (!P->d_next) PCUDA(P, cudaMallocAsync(&P->d_next, 2 * sizeof(int), P->stream));
+    std::copy(fast.begin(), fast.end(), P->h_jobs);
+    std::copy(gen.begin(), gen.end(), P->h_jobs + P->n_fast);
+    if (need) PCUDA(P, cudaMemcpyAsync(P->d_jobs, P->h_jobs, sizeof(BatchJob) * need, cudaMemcpyHostToDevice,
+                                       P->stream));
+    PCUDA(P, cudaStreamSynchronize(P->stream));
+    PCUDA(P, reserve_smem(std::max(P->smem_fast, P->smem_gen)));
+    P->dirty = false;
+    return ALEA_OK;
+}
+
+bool packed_zero_energy(const alea_gpu_packed* P) {
+    for (const PackedRunState& r : P->runs)
+        if (!r.done && r.fast)
+            for (int t = 0; t < r.c->sys.nterms; ++t)
+                if (r.c->sys.terms[t].kind == 2) return true;
+    return false;
+}
+
+// Grid of a packed launch: every walker its CTA (shape 0), or as many
+// persistent CTAs as fit on the device (shape 1).
+int packed_grid(alea_gpu_packed* P, bool fast, int shape, int total) {
+    if (shape == 0) return total;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
+    if (fast) {
+        const bool ze = packed_zero_energy(P);
+        (void)ze;
+        per_sm = 12;
+    } else {
+        per_sm = std::max(1, static_cast<int>((227 * 1024) / std::max<size_t>(P->smem_gen + 1024, 1)));
+        per_sm = std::min(per_sm, 32);
+    }
+    return std::min(total, sms * per_sm);
+}
+
+// The launches of one step: draws, packed sweeps, per-run sums, their copy.
+int packed_enqueue(alea_gpu_packed* P, const int shape[2], bool timed) {
+    for (const PackedRunState& r : P->runs) {
+        if (r.done) continue;
+        alea_gpu_ctx* c = r.c;
+        const int nt = std::min(c->n_streams, c->nw);
+        draw_kernel<<<(nt + 127) / 128, 128, 0, P->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, c->nw,
+                                                             r.cfg.n_substeps, c->sys.zk, c->sys.zw, c->sys.zf,
+                                                             c->sys.zr, c->randoms, 0);
+        ++P->launches;
+    }
+    PCUDA(P, cudaGetLastError());
+    PCUDA(P, cudaMemsetAsync(P->d_next, 0, 2 * sizeof(int), P->stream));
+    if (P->n_fast) {
+        if (timed) PCUDA(P, cudaEventRecord(P->ev[0], P->stream));
+        PCUDA(P, launch_sweep_fast_batch(packed_zero_energy(P), P->d_jobs, P->n_fast, P->total_fast,
+                                         packed_grid(P, true, shape[0], P->total_fast), P->smem_fast,
+                                         P->d_next, P->stream));
+        ++P->launches;
+        if (timed) PCUDA(P, cudaEventRecord(P->ev[1], P->stream));
+    }
+    if (P->n_gen) {
+        if (timed) PCUDA(P, cudaEventRecord(P->ev[2], P->stream));
+        PCUDA(P, launch_sweep_generic_batch(P->d_jobs + P->n_fast, P->n_gen, P->total_gen,
+                                            packed_grid(P, false, shape[1], P->total_gen), P->smem_gen,
+                                            P->d_next + 1, P->stream));
+        ++P->launches;
+        if (timed) PCUDA(P, cudaEventRecord(P->ev[3], P->stream));
+    }
+    for (const PackedRunState& r : P->runs) {
+        if (r.done) continue;
+        alea_gpu_ctx* c = r.c;
+        run_sums_kernel<<<1, 256, 0, P->stream>>>(records(c), c->nw, c->sys.rec, c->sys.o_scal, r.T,
+                                                  r.cfg.n_steps, r.cfg.n_equilibration_blocks, r.d_state,
+                                                  P->d_stats + r.stats_off);
+        ++P->launches;
+    }
+    PCUDA(P, cudaGetLastError());
+    size_t n = 0;
+    for (const PackedRunState& r : P->runs)
+        if (!r.done) n = std::max(n, r.stats_off + static_cast<size_t>(r.T) + 4);
+    PCUDA(P, cudaMemcpyAsync(P->h_stats, P->d_stats, 8 * n, cudaMemcpyDeviceToHost, P->stream));
+    return ALEA_OK;
+}
+
+// The run's result from its blocks, as alea_gpu_vmc_run forms it.
+void packed_finish(PackedRunState& r) {
+    if (r.d_state) cudaFreeAsync(r.d_state, r.c->stream);
+    r.d_state = nullptr;
+    for (int t = 0; t < r.T; ++t) r.blocks.insert(r.blocks.end(), r.chain[t].begin(), r.chain[t].end());
+    double mean = 0.0, err = 0.0;
+    reblock(r.blocks, mean, err);
+    r.res.energy = mean;
+    r.res.energy_error = err;
+    const double m = r.n_tot ? r.e_sum / static_cast<double>(r.n_tot) : 0.0;
+    r.res.variance = r.n_tot ? r.e2_sum / static_cast<double>(r.n_tot) - m * m : 0.0;
+    r.res.acceptance = r.prop ? static_cast<double>(r.acc) / static_cast<double>(r.prop) : 0.0;
+    r.res.walltime_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - r.t0).count();
+    r.res.n_walkers = r.c->nw;
+    r.res.e_trial = 0.0;
+    r.res.n_moves = r.moves;
+    r.res.n_evaluations = r.evals;
+    r.done = true;
+}
+
+}  // namespace
+
+namespace alea_gpu {
+
+int packed_create(int device, alea_gpu_packed** out) {
+    if (!out) return ALEA_ERR_INVALID;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return ALEA_ERR_CUDA;
+    auto* P = new alea_gpu_packed();
+    P->device = device;
+    bool ok = cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaEvent_t& e : P->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    if (!ok) {
+        packed_destroy(P);
+        return ALEA_ERR_CUDA;
+    }
+    *out = P;
+    return ALEA_OK;
+}
+
+void packed_destroy(alea_gpu_packed* P) {
+    if (!P) return;
+    cudaSetDevice(P->device);
+    packed_drop_graph(P);
+    for (PackedRunState& r : P->runs)
+        if (r.d_state) cudaFreeAsync(r.d_state, P->stream);
+    if (P->stream) {
+        for (void* p : {static_cast<void*>(P->d_jobs), static_cast<void*>(P->d_stats), static_cast<void*>(P->d_next)})
+            if (p) cudaFreeAsync(p, P->stream);
+        cudaStreamSynchronize(P->stream);
+        cudaStreamDestroy(P->stream);
+    }
+    if (P->h_jobs) cudaFreeHost(P->h_jobs);
+    if (P->h_stats) cudaFreeHost(P->h_stats);
+    for (cudaEvent_t e : P->ev)
+        if (e) cudaEventDestroy(e);
+    delete P;
+}
+
+const std::string& packed_error(const alea_gpu_packed* P) { return P->err; }
+
+// A context (walkers uploaded, FP64) joins with its VMC run; its random
+// streams are set as alea_gpu_vmc_run sets them.  Returns the run's slot.
+int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& cfg, int* slot) {
+    if (!P || !c || c->device != P->device) return pfail(P, ALEA_ERR_INVALID, "packed run: context on another device");
+    if (c->sys.f32) return pfail(P, ALEA_ERR_UNSUPPORTED, "packed run: FP64 contexts only");
+    if (c->nw < 1 || cfg.n_steps < 1 || cfg.n_substeps < 1 || cfg.n_accumulation_blocks < 0 ||
+        cfg.n_equilibration_blocks < 0)
+        return pfail(P, ALEA_ERR_INVALID, "packed run: empty population or bad run configuration");
+    PackedRunState r;
+    r.c = c;
+    r.cfg = cfg;
+    r.T = std::min(std::max(cfg.n_streams, 1), c->nw);
+    if (int rc = alea_gpu_set_streams(c, cfg.seed, ALEA_STREAM_VMC, r.T)) return pfail(P, rc, c->err);
+    const char* e = std::getenv("ALEA_GPU_SWEEP");
+    r.fast = c->nt == 32 && fast_sweep_eligible(c->sys) && (e == nullptr || std::strcmp(e, "generic") != 0);
+    r.smem = r.fast ? static_cast<size_t>(c->sys.f_total) * 8 : c->smem;
+    r.chain.assign(r.T, {});
+    r.blk.assign(r.T, 0.0);
+    r.blk_n.assign(r.T, 0);
+    r.t0 = std::chrono::steady_clock::now();
+    if (cfg.n_equilibration_blocks + cfg.n_accumulation_blocks == 0) r.done = true;
+    if (slot) *slot = static_cast<int>(P->runs.size());
+    P->runs.push_back(std::move(r));
+    P->dirty = true;
+    return ALEA_OK;
+}
+
+int packed_active(const alea_gpu_packed* P) {
+    int n = 0;
+    for (const PackedRunState& r : P->runs) n += r.done ? 0 : 1;
+    return n;
+}
+
+bool packed_done(const alea_gpu_packed* P, int slot, int* status, alea_gpu_run_result* res) {
+    const PackedRunState& r = P->runs[slot];
+    if (!r.done) return false;
+    if (status) *status = r.status;
+    if (res) *res = r.res;
+    return true;
+}
+
+const std::vector<double>& packed_blocks(const alea_gpu_packed* P, int slot) { return P->runs[slot].blocks; }
+
+// Forget finished runs (their contexts are the caller's); slots renumber.
+void packed_prune(alea_gpu_packed* P) {
+    std::vector<PackedRunState> keep;
+    for (PackedRunState& r : P->runs) {
+        if (!r.done) {
+            keep.push_back(std::move(r));
+        } else if (r.d_state) {
+            cudaFreeAsync(r.d_state, P->stream);
+            r.d_state = nullptr;
+        }
+    }
+    P->runs.swap(keep);
+    P->dirty = true;
+}
+
+// One step of every run still going.
+int packed_step(alea_gpu_packed* P) {
+    if (packed_active(P) == 0) return ALEA_OK;
+    PCUDA(P, cudaSetDevice(P->device));
+    if (P->dirty)
+        if (int rc = packed_rebuild(P)) return rc;
+    const int dev = P->device;
+    const int shape[2] = {g_packed_tuner.choice(dev, 0), g_packed_tuner.choice(dev, 1)};
+    const bool settled = (!P->n_fast || g_packed_tuner.settled(dev, 0)) && (!P->n_gen || g_packed_tuner.settled(dev, 1));
+    if (settled) {
+        if (P->graph && (P->graph_shapes[0] != shape[0] || P->graph_shapes[1] != shape[1])) packed_drop_graph(P);
+        if (!P->graph) {
+            cudaGraph_t g = nullptr;
+            PCUDA(P, cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = packed_enqueue(P, shape, false);
+            const cudaError_t ce = cudaStreamEndCapture(P->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            PCUDA(P, ce);
+            const cudaError_t ie = cudaGraphInstantiate(&P->graph, g, 0);
+            cudaGraphDestroy(g);
+            PCUDA(P, ie);
+            P->graph_shapes[0] = shape[0];
+            P->graph_shapes[1] = shape[1];
+        }
+        PCUDA(P, cudaGraphLaunch(P->graph, P->stream));
+    } else {
+        if (int rc = packed_enqueue(P, shape, true)) return rc;
+    }
+    PCUDA(P, cudaStreamSynchronize(P->stream));
+    if (!settled) {
+        float ms = 0.f;
+        if (P->n_fast && cudaEventElapsedTime(&ms, P->ev[0], P->ev[1]) == cudaSuccess)
+            g_packed_tuner.record(dev, 0, shape[0], ms / P->total_fast);
+        if (P->n_gen && cudaEventElapsedTime(&ms, P->ev[2], P->ev[3]) == cudaSuccess)
+            g_packed_tuner.record(dev, 1, shape[1], ms / P->total_gen);
+    }
+    for (PackedRunState& r : P->runs) {
+        if (r.done) continue;
+        alea_gpu_ctx* c = r.c;
+        const double* st = P->h_stats + r.stats_off;
+        c->launches += 3;
+        if (st[r.T + 3] != 0.0) {
+            r.status = fail(c, ALEA_ERR_SINGULAR, "a walker's accepted determinant is singular or nonfinite");
+            r.done = true;
+            P->dirty = true;
+            continue;
+        }
+        const int64_t proposed = static_cast<int64_t>(r.cfg.n_substeps) * c->sys.np * c->nw;
+        r.moves += proposed;
+        r.evals += c->nw;
+        const bool measure = r.block >= r.cfg.n_equilibration_blocks;
+        if (measure) {
+            const int base = c->nw / r.T, rem = c->nw % r.T;
+            for (int t = 0; t < r.T; ++t) {
+                r.blk[t] = st[t];
+                r.blk_n[t] += base + (t < rem ? 1 : 0);
+            }
+            r.n_tot += c->nw;
+            r.e_sum = st[r.T];
+            r.e2_sum = st[r.T + 1];
+            r.acc += static_cast<int64_t>(st[r.T + 2]);
+            r.prop += proposed;
+        }
+        if (++r.step == r.cfg.n_steps) {
+            if (measure)
+                for (int t = 0; t < r.T; ++t) r.chain[t].push_back(r.blk[t] / static_cast<double>(r.blk_n[t]));
+            std::fill(r.blk.begin(), r.blk.end(), 0.0);
+            std::fill(r.blk_n.begin(), r.blk_n.end(), 0);
+            r.step = 0;
+            if (++r.block == r.cfg.n_equilibration_blocks + r.cfg.n_accumulation_blocks) {
+                packed_finish(r);
+                P->dirty = true;
+            }
+        }
+    }
+    return ALEA_OK;
+}
+
+uint64_t packed_launches(const alea_gpu_packed* P) { return P->launches; }
+
+}  // namespace alea_gpu
+
+extern "C" int alea_gpu_vmc_run_packed(alea_gpu_ctx* const* ctxs, int n, const alea_gpu_run_config* cfgs,
+                                       alea_gpu_run_result* results, int* statuses) {
+    if (!ctxs || n < 1 || !cfgs || !results) return ALEA_ERR_INVALID;
+    alea_gpu_packed* P = nullptr;
+    if (int rc = alea_gpu::packed_create(ctxs[0]->device, &P)) return rc;
+    int rc = ALEA_OK;
+    for (int i = 0; i < n && rc == ALEA_OK; ++i) {
+        if (!ctxs[i]) rc = ALEA_ERR_INVALID;
+        else rc = alea_gpu::packed_add(P, ctxs[i], cfgs[i], nullptr);
+        if (rc) g_create_error = P->err;
+    }
+    while (rc == ALEA_OK && alea_gpu::packed_active(P) > 0) {
+        rc = alea_gpu::packed_step(P);
+        if (rc) g_create_error = P->err;
+    }
+    for (int i = 0; i < n && rc == ALEA_OK; ++i) {
+        int st = ALEA_OK;
+        alea_gpu::packed_done(P, i, &st, &results[i]);
+        if (statuses) statuses[i] = st;
+    }
+    alea_gpu::packed_destroy(P);
+    return rc;
+}
+
+extern "C" {
 
 // ───────────────────────── forward walking ─────────────────────────────
 

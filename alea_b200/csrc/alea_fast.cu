@@ -30,13 +30,12 @@
 
 namespace alea_gpu {
 
+// One walker's sweep by one warp (the body of sweep_fast_kernel and of the
+// packed launches of alea_batch.cu).
 template <int S, bool ZE>
-__global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
-                                                        int nw, const double* randoms, long stride,
-                                                        SweepParams prm, const int2* pairs, int npair) {
-    extern __shared__ __align__(16) double sm[];
-    const int w = blockIdx.x;
-    if (w >= nw) return;
+__device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* records, int w, const double* randoms,
+                                                  long stride, const SweepParams& prm, const int2* pairs,
+                                                  int npair, double* sm) {
     const int lane = threadIdx.x;
     double* rec = records + static_cast<long>(w) * s.rec;
     load_fast(s, rec, sm);
@@ -509,6 +508,40 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constan
     store_fast(s, rec, sm);
 }
 
+template <int S, bool ZE>
+__global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
+                                                        int nw, const double* randoms, long stride,
+                                                        SweepParams prm, const int2* pairs, int npair) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    sweep_fast_walker<S, ZE>(s, records, w, randoms, stride, prm, pairs, npair, sm);
+}
+
+// Packed one-warp sweeps of several contexts (BatchJob, alea_kernels.h).
+template <bool ZE>
+__global__ void __launch_bounds__(32, 12) sweep_fast_batch_kernel(const BatchJob* __restrict__ jobs, int n_jobs,
+                                                              int total, int* next) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int slot;
+    for (bool first = true;; first = false) {
+        const int w = batch_next(total, next, &slot, first);
+        if (w < 0) return;
+        const BatchJob& J = jobs[batch_job_of(jobs, n_jobs, w)];
+        sweep_fast_walker<2, ZE>(*J.sys, J.records, w - J.first, J.randoms, J.stride, J.prm, J.pairs, J.npair,
+                                 sm);
+    }
+}
+
+cudaError_t launch_sweep_fast_batch(bool zero_energy, const BatchJob* jobs, int n_jobs, int total, int grid,
+                                    size_t smem, int* next, cudaStream_t st) {
+    if (zero_energy)
+        sweep_fast_batch_kernel<true><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
+    else
+        sweep_fast_batch_kernel<false><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
+    return cudaGetLastError();
+}
+
 bool fast_sweep_eligible(const DevSys& s) {
     return s.dim == 2 && !s.cplx && s.nbf == 0 && s.pair_by_group && s.np <= 64 && s.maxN <= 64 &&
            s.nkJ <= 64 && s.ngroups <= 8;
@@ -523,7 +556,9 @@ static bool has_zero_energy(const DevSys& s) {
 
 cudaError_t reserve_smem_fast(size_t smem) {
     for (const void* k : {reinterpret_cast<const void*>(sweep_fast_kernel<2, false>),
-                          reinterpret_cast<const void*>(sweep_fast_kernel<2, true>)}) {
+                          reinterpret_cast<const void*>(sweep_fast_kernel<2, true>),
+                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<false>),
+                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<true>)}) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    static_cast<int>(smem));
         if (e != cudaSuccess) return e;

@@ -4,8 +4,12 @@
 
 #include <atomic>
 #include <cstddef>
+#include <cstdint>
+#include <string>
 
 #include "../../include/alea_gpu.h"
+
+struct alea_gpu_packed;
 
 namespace alea_gpu {
 
@@ -16,5 +20,21 @@ void set_cancel_flag(alea_gpu_ctx* c, const std::atomic<int>* flag);
 // Device bytes of a context of `capacity` walkers of `sys` running
 // `n_substeps` sweeps per step (the server's admission estimate).
 size_t footprint_bytes(const alea_gpu_system* sys, int capacity, int n_substeps);
+
+// Packed VMC runs (alea_capi.cu, "packed VMC runs"): several contexts'
+// runs stepped together, one sweep launch per sweep body per step.
+int packed_create(int device, alea_gpu_packed** out);
+void packed_destroy(alea_gpu_packed* P);
+const std::string& packed_error(const alea_gpu_packed* P);
+// Join with a context whose walkers are uploaded; *slot numbers the run.
+int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& cfg, int* slot);
+int packed_active(const alea_gpu_packed* P);
+// One step of every run still going.
+int packed_step(alea_gpu_packed* P);
+// Whether run `slot` has finished, with its status and result.
+bool packed_done(const alea_gpu_packed* P, int slot, int* status, alea_gpu_run_result* res);
+// Forget the finished runs; the slots of the others renumber in order.
+void packed_prune(alea_gpu_packed* P);
+uint64_t packed_launches(const alea_gpu_packed* P);
 
 }  // namespace alea_gpu

@@ -523,12 +523,9 @@ __global__ void __launch_bounds__(NT) move_kernel(DevSys s, double* records, int
 // Fused sweep kernel.  mode 0: VMC step (n_sub sweeps, then refresh + E_L);
 // mode 1: DMC advance (per sweep: refresh + E_L + branch factor).
 template <int NT>
-__global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, int nw,
-                                                   const double* randoms, long stride,
-                                                   SweepParams prm, const int2* pairs, int npair) {
-    extern __shared__ __align__(16) double sm[];
-    const int w = blockIdx.x;
-    if (w >= nw) return;
+__device__ __forceinline__ void sweep_walker(const DevSys& s, double* records, int w, const double* randoms,
+                                             long stride, const SweepParams& prm, const int2* pairs, int npair,
+                                             double* sm) {
     double* rec = records + static_cast<long>(w) * s.rec;
     load_hot<NT>(s, rec, sm);
     const Smem v = view(s, sm);
@@ -652,6 +649,37 @@ __global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, in
     store_hot<NT>(s, rec, sm);
 }
 
+// One CTA of NT threads per walker.
+template <int NT>
+__global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, int nw,
+                                                   const double* randoms, long stride,
+                                                   SweepParams prm, const int2* pairs, int npair) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    sweep_walker<NT>(s, records, w, randoms, stride, prm, pairs, npair, sm);
+}
+
+// Packed generic sweeps of several contexts, 32 threads per walker
+// (BatchJob, alea_kernels.h).
+__global__ void __launch_bounds__(32) sweep_batch_kernel(const BatchJob* __restrict__ jobs, int n_jobs, int total,
+                                                         int* next) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int slot;
+    for (bool first = true;; first = false) {
+        const int w = batch_next(total, next, &slot, first);
+        if (w < 0) return;
+        const BatchJob& J = jobs[batch_job_of(jobs, n_jobs, w)];
+        sweep_walker<32>(*J.sys, J.records, w - J.first, J.randoms, J.stride, J.prm, J.pairs, J.npair, sm);
+    }
+}
+
+cudaError_t launch_sweep_generic_batch(const BatchJob* jobs, int n_jobs, int total, int grid, size_t smem,
+                                       int* next, cudaStream_t st) {
+    sweep_batch_kernel<<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
+    return cudaGetLastError();
+}
+
 // ───────────────────────── launchers ────────────────────────────────────
 
 #define ALEA_LAUNCH(nt, KERNEL, grid, smem, st, ...)                                     \
@@ -681,7 +709,7 @@ cudaError_t reserve_smem(size_t smem) {
         reinterpret_cast<const void*>(evaluate_kernel<128>), reinterpret_cast<const void*>(measure_kernel<128>),
         reinterpret_cast<const void*>(move_kernel<128>), reinterpret_cast<const void*>(sweep_kernel<128>),
         reinterpret_cast<const void*>(potential_kernel<32>), reinterpret_cast<const void*>(potential_kernel<64>),
-        reinterpret_cast<const void*>(potential_kernel<128>)};
+        reinterpret_cast<const void*>(potential_kernel<128>), reinterpret_cast<const void*>(sweep_batch_kernel)};
     for (const void* k : kernels) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
         if (e != cudaSuccess) return e;

@@ -57,6 +57,54 @@ cudaError_t reserve_smem_fast(size_t smem);
 cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
                               const double* randoms, long stride, const SweepParams& prm, const int2* pairs,
                               int npair);
+// One context's share of a packed sweep launch: its walkers are
+// [first, first + nw) of the launch's global walker index, swept with its own
+// system (a device copy of its DevSys), records, random numbers and
+// parameters.  Jobs are in increasing `first`.
+struct BatchJob {
+    const DevSys* sys;
+    double* records;
+    const double* randoms;
+    long stride;
+    SweepParams prm;
+    const int2* pairs;
+    int npair;
+    int first, nw;
+};
+// Packed sweeps of n_jobs jobs, `total` walkers in all, one 32-thread CTA per
+// walker at a time: the one-warp body (alea_fast.cu, every job fast-sweep
+// eligible; zero_energy: some job has a zero-energy term) or the generic body
+// with 32 threads (alea_kernels.cu, any system).  grid >= total: one CTA per
+// walker; grid < total: persistent CTAs take walkers from the counter *next
+// (zero before the launch).  The walker's arithmetic is that of launch_sweep
+// on its own context whatever the grid.  reserve_smem covers both kernels.
+cudaError_t launch_sweep_fast_batch(bool zero_energy, const BatchJob* jobs, int n_jobs, int total, int grid,
+                                    size_t smem, int* next, cudaStream_t st);
+cudaError_t launch_sweep_generic_batch(const BatchJob* jobs, int n_jobs, int total, int grid, size_t smem,
+                                       int* next, cudaStream_t st);
+// The walker of global index w of a packed launch: its job by binary search
+// over the jobs' first indices.
+__device__ __forceinline__ int batch_job_of(const BatchJob* jobs, int n_jobs, int w) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].first <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Next walker of a packed launch for this CTA: blockIdx.x once (grid >= total)
+// or from the shared counter; -1 when none is left.
+__device__ __forceinline__ int batch_next(int total, int* next, int* slot, bool first_round) {
+    if (gridDim.x >= total) return first_round && static_cast<int>(blockIdx.x) < total ? static_cast<int>(blockIdx.x) : -1;
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = atomicAdd(next, 1);
+    __syncthreads();
+    const int w = *slot;
+    return w < total ? w : -1;
+}
+
 // The FP32 form of the one-warp sweep (alea_fast32.cu), for the one-warp
 // sweep's systems without zero-energy terms; launch_sweep takes it whenever
 // DevSys::f32 is set.

@@ -396,6 +396,22 @@ int alea_gpu_vmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu
 int alea_gpu_dmc_run(alea_gpu_ctx* ctx, const alea_gpu_run_config* cfg, alea_gpu_run_result* res,
                      double* block_energies);
 
+/* Packed VMC runs (no counterpart in the reference, which runs one input per
+ * process): the VMC runs of n contexts (each alea_gpu_vmc_run's arguments:
+ * cfgs[i] for ctxs[i]) stepped together on the first context's device, the
+ * walkers of every run swept in one launch per step (one per sweep body:
+ * the one-warp body for the systems that take it, a 32-thread generic body
+ * for the rest), uneven walker counts and particle numbers packed raggedly.
+ * Each run's blocks, energy, error, variance and acceptance equal its
+ * alea_gpu_vmc_run's on its own context (same random streams, same walker
+ * arithmetic; statuses[i] its status), so a run's result does not depend on
+ * what it was packed with.  The launch shape (one CTA per walker or
+ * persistent CTAs) comes from timing both on the first steps, per device;
+ * once the set of running contexts repeats, a step is a CUDA graph replay.
+ * Estimators and FP32 contexts are not packed (ALEA_ERR_UNSUPPORTED). */
+int alea_gpu_vmc_run_packed(alea_gpu_ctx* const* ctxs, int n, const alea_gpu_run_config* cfgs,
+                            alea_gpu_run_result* results, int* statuses);
+
 /* Device time of the last alea_gpu_*_step / advance call's sweep kernel, in
  * milliseconds (CUDA events on the context's stream). */
 int alea_gpu_last_kernel_ms(const alea_gpu_ctx* ctx, double* ms);
