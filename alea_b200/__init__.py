@@ -599,14 +599,16 @@ def vmc_run_packed(walkers: Sequence["Walkers"], runs: Sequence[Dict[str, Any]])
 class Server:
     """Serving front end over alea_gpu_server (include/alea_gpu.h, serving):
     jobs are queued, admitted by device-memory footprint and run
-    ``max_running`` at a time, each on its own context and stream.  The
+    ``max_running`` at a time, each on its own context and stream (packed:
+    VMC jobs step together in packed launches, alea_gpu_server_create_packed).  The
     packed system tables and positions of a job are kept alive here until
     the job has finished."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_running: int = 8):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_running: int = 8, packed: bool = False):
         self.lib = _load()
         h = ctypes.c_void_p()
-        rc = self.lib.alea_gpu_server_create(device, int(hbm_budget_bytes), int(max_running), ctypes.byref(h))
+        create = self.lib.alea_gpu_server_create_packed if packed else self.lib.alea_gpu_server_create
+        rc = create(device, int(hbm_budget_bytes), int(max_running), ctypes.byref(h))
         if rc != 0:
             raise AleaGpuError(rc, "alea_gpu_server_create failed")
         self.h = h

@@ -193,7 +193,7 @@ EXPORTS = [
     "alea_gpu_vmc_steps", "alea_gpu_dmc_steps", "alea_gpu_set_checkpoint_hook",
     "alea_gpu_set_forward_walking", "alea_gpu_add_fw_estimator", "alea_gpu_fw_result",
     "alea_gpu_fw_estimator_info", "alea_gpu_fw_estimator_blocks", "alea_gpu_fw_estimator_kvectors",
-    "alea_gpu_vmc_run_packed",
+    "alea_gpu_vmc_run_packed", "alea_gpu_server_create_packed",
 ]
 
 _LIB = None
@@ -250,6 +250,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_setup_free": ([P], None),
         "alea_gpu_set_precision": ([P, I], I),
         "alea_gpu_server_create": ([I, ctypes.c_size_t, I, ctypes.POINTER(P)], I),
+        "alea_gpu_server_create_packed": ([I, ctypes.c_size_t, I, ctypes.POINTER(P)], I),
         "alea_gpu_submit_job": ([P, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)], I),
         "alea_gpu_poll": ([P, ctypes.c_uint64, I, ctypes.POINTER(JobResult)], I),
         "alea_gpu_cancel": ([P, ctypes.c_uint64], I),

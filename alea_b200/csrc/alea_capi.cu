@@ -1950,14 +1950,15 @@ __global__ void run_sums_kernel(const double* records, int nw, long rec, int o_s
     }
 }
 
-// Launch shapes of the packed bodies: for each body (0 one-warp, 1 generic)
+// Launch shapes of the packed bodies: for each body class (0 one-warp, 1-3
+// generic of 32, 64, 128 threads)
 // the measured time per walker-sweep of shape 0 (one CTA per walker) and
 // shape 1 (persistent CTAs); the faster one is kept for the device's
 // lifetime (every packed run of the process shares the table).
 struct PackedTuner {
     std::mutex mu;
-    double ms_per_walker[64][2][2] = {};
-    int samples[64][2][2] = {};
+    double ms_per_walker[64][4][2] = {};
+    int samples[64][4][2] = {};
     int choice(int dev, int body) {
         std::lock_guard<std::mutex> lk(mu);
         for (int shape = 0; shape < 2; ++shape)
@@ -1983,7 +1984,7 @@ struct PackedRunState {
     alea_gpu_run_config cfg{};
     int T = 1;
     int block = 0, step = 0;
-    bool fast = false;
+    int cls = 0;                   // body class: 0 one-warp, 1-3 generic of 32, 64, 128 threads
     size_t smem = 0;
     size_t stats_off = 0;
     double* d_state = nullptr;     // run_sums_kernel's [step, block, blk[T], e_sum, e2_sum]
@@ -2012,12 +2013,14 @@ struct alea_gpu_packed {
     double* d_stats = nullptr;
     double* h_stats = nullptr;    // pinned
     size_t stats_cap = 0;
-    int* d_next = nullptr;
-    int n_fast = 0, n_gen = 0, total_fast = 0, total_gen = 0;
-    size_t smem_fast = 0, smem_gen = 0;
+    int* d_next = nullptr;         // one work counter per class
+    int n_jobs[4] = {0, 0, 0, 0}, job0[4] = {0, 0, 0, 0}, total[4] = {0, 0, 0, 0};
+    size_t smem[4] = {0, 0, 0, 0};
+    cudaStream_t cls_stream[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t graph = nullptr;
-    int graph_shapes[2] = {-1, -1};
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int graph_shapes[4] = {-1, -1, -1, -1};
+    cudaEvent_t ev[8] = {};
     std::string err;
     uint64_t launches = 0;
 };
@@ -2045,20 +2048,20 @@ void packed_drop_graph(alea_gpu_packed* P) {
 // going, after one joined or left.
 int packed_rebuild(alea_gpu_packed* P) {
     packed_drop_graph(P);
-    std::vector<BatchJob> fast, gen;
+    std::vector<BatchJob> lists[4];
     size_t stats = 0;
-    P->smem_fast = P->smem_gen = 0;
+    for (int k = 0; k < 4; ++k) P->smem[k] = 0, P->total[k] = 0;
     for (PackedRunState& r : P->runs) {
         if (r.done) continue;
         alea_gpu_ctx* c = r.c;
         if (int rc = ensure_randoms(c, r.cfg.n_substeps)) return pfail(P, rc, c->err);
         if (int rc = set_sigma(c, r.cfg.tau)) return pfail(P, rc, c->err);
         if (!c->d_sys) PCUDA(P, cudaMallocAsync(&c->d_sys, sizeof(DevSys), c->stream));
-        if (!r.d_state) {
-            PCUDA(P, cudaMallocAsync(&r.d_state, 8 * (static_cast<size_t>(r.T) + 4), P->stream));
-            PCUDA(P, cudaMemsetAsync(r.d_state, 0, 8 * (static_cast<size_t>(r.T) + 4), P->stream));
-        }
         PCUDA(P, cudaMemcpyAsync(c->d_sys, &c->sys, sizeof(DevSys), cudaMemcpyHostToDevice, c->stream));
+        if (!r.d_state) {
+            PCUDA(P, cudaMallocAsync(&r.d_state, 8 * (static_cast<size_t>(r.T) + 4), c->stream));
+            PCUDA(P, cudaMemsetAsync(r.d_state, 0, 8 * (static_cast<size_t>(r.T) + 4), c->stream));
+        }
         PCUDA(P, cudaStreamSynchronize(c->stream));
         BatchJob j{};
         j.sys = c->d_sys;
@@ -2073,21 +2076,19 @@ int packed_rebuild(alea_gpu_packed* P) {
         j.pairs = c->pairs;
         j.npair = c->npair;
         j.nw = c->nw;
-        auto& list = r.fast ? fast : gen;
-        int& total = r.fast ? P->total_fast : P->total_gen;
-        if (list.empty()) total = 0;
-        j.first = total;
-        total += c->nw;
-        list.push_back(j);
-        (r.fast ? P->smem_fast : P->smem_gen) = std::max(r.fast ? P->smem_fast : P->smem_gen, r.smem);
+        j.first = P->total[r.cls];
+        P->total[r.cls] += c->nw;
+        lists[r.cls].push_back(j);
+        P->smem[r.cls] = std::max(P->smem[r.cls], r.smem);
         r.stats_off = stats;
         stats += static_cast<size_t>(r.T) + 4;
     }
-    P->n_fast = static_cast<int>(fast.size());
-    P->n_gen = static_cast<int>(gen.size());
-    if (fast.empty()) P->total_fast = 0;
-    if (gen.empty()) P->total_gen = 0;
-    const int need = P->n_fast + P->n_gen;
+    int need = 0;
+    for (int k = 0; k < 4; ++k) {
+        P->job0[k] = need;
+        P->n_jobs[k] = static_cast<int>(lists[k].size());
+        need += P->n_jobs[k];
+    }
     if (need > P->jobs_cap) {
         if (P->d_jobs) cudaFreeAsync(P->d_jobs, P->stream);
         if (P->h_jobs) cudaFreeHost(P->h_jobs);
@@ -2108,44 +2109,39 @@ int packed_rebuild(alea_gpu_packed* P) {
         PCUDA(P, cudaMallocHost(&P->h_stats, 8 * cap));
         P->stats_cap = cap;
     }
-    if (!P->d_next) PCUDA(P, cudaMallocAsync(&P->d_next, 2 * sizeof(int), P->stream));
-    std::copy(fast.begin(), fast.end(), P->h_jobs);
-    std::copy(gen.begin(), gen.end(), P->h_jobs + P->n_fast);
+    if (!P->d_next) PCUDA(P, cudaMallocAsync(&P->d_next, 4 * sizeof(int), P->stream));
+    for (int k = 0; k < 4; ++k) std::copy(lists[k].begin(), lists[k].end(), P->h_jobs + P->job0[k]);
     if (need) PCUDA(P, cudaMemcpyAsync(P->d_jobs, P->h_jobs, sizeof(BatchJob) * need, cudaMemcpyHostToDevice,
                                        P->stream));
     PCUDA(P, cudaStreamSynchronize(P->stream));
-    PCUDA(P, reserve_smem(std::max(P->smem_fast, P->smem_gen)));
+    PCUDA(P, reserve_smem(std::max({P->smem[0], P->smem[1], P->smem[2], P->smem[3]})));
     P->dirty = false;
     return ALEA_OK;
 }
 
 bool packed_zero_energy(const alea_gpu_packed* P) {
     for (const PackedRunState& r : P->runs)
-        if (!r.done && r.fast)
+        if (!r.done && r.cls == 0)
             for (int t = 0; t < r.c->sys.nterms; ++t)
                 if (r.c->sys.terms[t].kind == 2) return true;
     return false;
 }
 
-// Grid of a packed launch: every walker its CTA (shape 0), or as many
-// persistent CTAs as fit on the device (shape 1).
-int packed_grid(alea_gpu_packed* P, bool fast, int shape, int total) {
+// Grid of a packed launch of class k: every walker its CTA (shape 0), or as
+// many persistent CTAs as are resident on the device at once (shape 1).
+int packed_grid(alea_gpu_packed* P, int k, int shape) {
+    const int total = P->total[k];
     if (shape == 0) return total;
-    int sms = 148, per_sm = 1;
+    int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
-    if (fast) {
-        const bool ze = packed_zero_energy(P);
-        (void)ze;
-        per_sm = 12;
-    } else {
-        per_sm = std::max(1, static_cast<int>((227 * 1024) / std::max<size_t>(P->smem_gen + 1024, 1)));
-        per_sm = std::min(per_sm, 32);
-    }
-    return std::min(total, sms * per_sm);
+    const int per_sm = k == 0 ? 12 : batch_ctas_per_sm(16 << k, P->smem[k]);
+    return std::max(1, std::min(total, sms * per_sm));
 }
 
-// The launches of one step: draws, packed sweeps, per-run sums, their copy.
-int packed_enqueue(alea_gpu_packed* P, const int shape[2], bool timed) {
+// The launches of one step: draws, then the classes' packed sweeps on their
+// own streams (forked from and joined back into the engine's stream, so they
+// run side by side), then the per-run sums and their copy.
+int packed_enqueue(alea_gpu_packed* P, const int shape[4], bool timed) {
     for (const PackedRunState& r : P->runs) {
         if (r.done) continue;
         alea_gpu_ctx* c = r.c;
@@ -2156,22 +2152,24 @@ int packed_enqueue(alea_gpu_packed* P, const int shape[2], bool timed) {
         ++P->launches;
     }
     PCUDA(P, cudaGetLastError());
-    PCUDA(P, cudaMemsetAsync(P->d_next, 0, 2 * sizeof(int), P->stream));
-    if (P->n_fast) {
-        if (timed) PCUDA(P, cudaEventRecord(P->ev[0], P->stream));
-        PCUDA(P, launch_sweep_fast_batch(packed_zero_energy(P), P->d_jobs, P->n_fast, P->total_fast,
-                                         packed_grid(P, true, shape[0], P->total_fast), P->smem_fast,
-                                         P->d_next, P->stream));
+    PCUDA(P, cudaMemsetAsync(P->d_next, 0, 4 * sizeof(int), P->stream));
+    PCUDA(P, cudaEventRecord(P->fork, P->stream));
+    for (int k = 0; k < 4; ++k) {
+        if (!P->n_jobs[k]) continue;
+        cudaStream_t st = P->cls_stream[k];
+        PCUDA(P, cudaStreamWaitEvent(st, P->fork, 0));
+        if (timed) PCUDA(P, cudaEventRecord(P->ev[2 * k], st));
+        const BatchJob* jobs = P->d_jobs + P->job0[k];
+        if (k == 0)
+            PCUDA(P, launch_sweep_fast_batch(packed_zero_energy(P), jobs, P->n_jobs[0], P->total[0],
+                                             packed_grid(P, 0, shape[0]), P->smem[0], P->d_next, st));
+        else
+            PCUDA(P, launch_sweep_generic_batch(16 << k, jobs, P->n_jobs[k], P->total[k],
+                                                packed_grid(P, k, shape[k]), P->smem[k], P->d_next + k, st));
         ++P->launches;
-        if (timed) PCUDA(P, cudaEventRecord(P->ev[1], P->stream));
-    }
-    if (P->n_gen) {
-        if (timed) PCUDA(P, cudaEventRecord(P->ev[2], P->stream));
-        PCUDA(P, launch_sweep_generic_batch(P->d_jobs + P->n_fast, P->n_gen, P->total_gen,
-                                            packed_grid(P, false, shape[1], P->total_gen), P->smem_gen,
-                                            P->d_next + 1, P->stream));
-        ++P->launches;
-        if (timed) PCUDA(P, cudaEventRecord(P->ev[3], P->stream));
+        if (timed) PCUDA(P, cudaEventRecord(P->ev[2 * k + 1], st));
+        PCUDA(P, cudaEventRecord(P->join[k], st));
+        PCUDA(P, cudaStreamWaitEvent(P->stream, P->join[k], 0));
     }
     for (const PackedRunState& r : P->runs) {
         if (r.done) continue;
@@ -2220,7 +2218,10 @@ int packed_create(int device, alea_gpu_packed** out) {
     auto* P = new alea_gpu_packed();
     P->device = device;
     bool ok = cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaStream_t& st : P->cls_stream) ok = ok && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
     for (cudaEvent_t& e : P->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (cudaEvent_t& e : P->join) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         packed_destroy(P);
         return ALEA_ERR_CUDA;
@@ -2245,6 +2246,11 @@ void packed_destroy(alea_gpu_packed* P) {
     if (P->h_stats) cudaFreeHost(P->h_stats);
     for (cudaEvent_t e : P->ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : P->join)
+        if (e) cudaEventDestroy(e);
+    if (P->fork) cudaEventDestroy(P->fork);
+    for (cudaStream_t st : P->cls_stream)
+        if (st) cudaStreamDestroy(st);
     delete P;
 }
 
@@ -2264,8 +2270,9 @@ int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& c
     r.T = std::min(std::max(cfg.n_streams, 1), c->nw);
     if (int rc = alea_gpu_set_streams(c, cfg.seed, ALEA_STREAM_VMC, r.T)) return pfail(P, rc, c->err);
     const char* e = std::getenv("ALEA_GPU_SWEEP");
-    r.fast = c->nt == 32 && fast_sweep_eligible(c->sys) && (e == nullptr || std::strcmp(e, "generic") != 0);
-    r.smem = r.fast ? static_cast<size_t>(c->sys.f_total) * 8 : c->smem;
+    const bool fast = c->nt == 32 && fast_sweep_eligible(c->sys) && (e == nullptr || std::strcmp(e, "generic") != 0);
+    r.cls = fast ? 0 : c->nt == 32 ? 1 : c->nt == 64 ? 2 : 3;
+    r.smem = fast ? static_cast<size_t>(c->sys.f_total) * 8 : c->smem;
     r.chain.assign(r.T, {});
     r.blk.assign(r.T, 0.0);
     r.blk_n.assign(r.T, 0);
@@ -2293,6 +2300,15 @@ bool packed_done(const alea_gpu_packed* P, int slot, int* status, alea_gpu_run_r
 
 const std::vector<double>& packed_blocks(const alea_gpu_packed* P, int slot) { return P->runs[slot].blocks; }
 
+// Stop run `slot` before its next step (status ALEA_ERR_CANCELLED).
+void packed_cancel(alea_gpu_packed* P, int slot) {
+    PackedRunState& r = P->runs[slot];
+    if (r.done) return;
+    r.status = ALEA_ERR_CANCELLED;
+    r.done = true;
+    P->dirty = true;
+}
+
 // Forget finished runs (their contexts are the caller's); slots renumber.
 void packed_prune(alea_gpu_packed* P) {
     std::vector<PackedRunState> keep;
@@ -2315,10 +2331,16 @@ int packed_step(alea_gpu_packed* P) {
     if (P->dirty)
         if (int rc = packed_rebuild(P)) return rc;
     const int dev = P->device;
-    const int shape[2] = {g_packed_tuner.choice(dev, 0), g_packed_tuner.choice(dev, 1)};
-    const bool settled = (!P->n_fast || g_packed_tuner.settled(dev, 0)) && (!P->n_gen || g_packed_tuner.settled(dev, 1));
+    int shape[4];
+    bool settled = true;
+    for (int k = 0; k < 4; ++k) {
+        shape[k] = g_packed_tuner.choice(dev, k);
+        if (P->n_jobs[k] && !g_packed_tuner.settled(dev, k)) settled = false;
+    }
     if (settled) {
-        if (P->graph && (P->graph_shapes[0] != shape[0] || P->graph_shapes[1] != shape[1])) packed_drop_graph(P);
+        bool same = P->graph != nullptr;
+        for (int k = 0; k < 4 && same; ++k) same = P->graph_shapes[k] == shape[k];
+        if (!same) packed_drop_graph(P);
         if (!P->graph) {
             cudaGraph_t g = nullptr;
             PCUDA(P, cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
@@ -2332,8 +2354,7 @@ int packed_step(alea_gpu_packed* P) {
             const cudaError_t ie = cudaGraphInstantiate(&P->graph, g, 0);
             cudaGraphDestroy(g);
             PCUDA(P, ie);
-            P->graph_shapes[0] = shape[0];
-            P->graph_shapes[1] = shape[1];
+            for (int k = 0; k < 4; ++k) P->graph_shapes[k] = shape[k];
         }
         PCUDA(P, cudaGraphLaunch(P->graph, P->stream));
     } else {
@@ -2341,11 +2362,11 @@ int packed_step(alea_gpu_packed* P) {
     }
     PCUDA(P, cudaStreamSynchronize(P->stream));
     if (!settled) {
-        float ms = 0.f;
-        if (P->n_fast && cudaEventElapsedTime(&ms, P->ev[0], P->ev[1]) == cudaSuccess)
-            g_packed_tuner.record(dev, 0, shape[0], ms / P->total_fast);
-        if (P->n_gen && cudaEventElapsedTime(&ms, P->ev[2], P->ev[3]) == cudaSuccess)
-            g_packed_tuner.record(dev, 1, shape[1], ms / P->total_gen);
+        for (int k = 0; k < 4; ++k) {
+            float ms = 0.f;
+            if (P->n_jobs[k] && cudaEventElapsedTime(&ms, P->ev[2 * k], P->ev[2 * k + 1]) == cudaSuccess)
+                g_packed_tuner.record(dev, k, shape[k], ms / P->total[k]);
+        }
     }
     for (PackedRunState& r : P->runs) {
         if (r.done) continue;

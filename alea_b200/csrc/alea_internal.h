@@ -33,6 +33,8 @@ int packed_active(const alea_gpu_packed* P);
 int packed_step(alea_gpu_packed* P);
 // Whether run `slot` has finished, with its status and result.
 bool packed_done(const alea_gpu_packed* P, int slot, int* status, alea_gpu_run_result* res);
+// Stop run `slot` before its next step (status ALEA_ERR_CANCELLED).
+void packed_cancel(alea_gpu_packed* P, int slot);
 // Forget the finished runs; the slots of the others renumber in order.
 void packed_prune(alea_gpu_packed* P);
 uint64_t packed_launches(const alea_gpu_packed* P);

@@ -662,7 +662,8 @@ __global__ void __launch_bounds__(NT) sweep_kernel(DevSys s, double* records, in
 
 // Packed generic sweeps of several contexts, 32 threads per walker
 // (BatchJob, alea_kernels.h).
-__global__ void __launch_bounds__(32) sweep_batch_kernel(const BatchJob* __restrict__ jobs, int n_jobs, int total,
+template <int NT>
+__global__ void __launch_bounds__(NT) sweep_batch_kernel(const BatchJob* __restrict__ jobs, int n_jobs, int total,
                                                          int* next) {
     extern __shared__ __align__(16) double sm[];
     __shared__ int slot;
@@ -670,14 +671,8 @@ __global__ void __launch_bounds__(32) sweep_batch_kernel(const BatchJob* __restr
         const int w = batch_next(total, next, &slot, first);
         if (w < 0) return;
         const BatchJob& J = jobs[batch_job_of(jobs, n_jobs, w)];
-        sweep_walker<32>(*J.sys, J.records, w - J.first, J.randoms, J.stride, J.prm, J.pairs, J.npair, sm);
+        sweep_walker<NT>(*J.sys, J.records, w - J.first, J.randoms, J.stride, J.prm, J.pairs, J.npair, sm);
     }
-}
-
-cudaError_t launch_sweep_generic_batch(const BatchJob* jobs, int n_jobs, int total, int grid, size_t smem,
-                                       int* next, cudaStream_t st) {
-    sweep_batch_kernel<<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
-    return cudaGetLastError();
 }
 
 // ───────────────────────── launchers ────────────────────────────────────
@@ -709,7 +704,8 @@ cudaError_t reserve_smem(size_t smem) {
         reinterpret_cast<const void*>(evaluate_kernel<128>), reinterpret_cast<const void*>(measure_kernel<128>),
         reinterpret_cast<const void*>(move_kernel<128>), reinterpret_cast<const void*>(sweep_kernel<128>),
         reinterpret_cast<const void*>(potential_kernel<32>), reinterpret_cast<const void*>(potential_kernel<64>),
-        reinterpret_cast<const void*>(potential_kernel<128>), reinterpret_cast<const void*>(sweep_batch_kernel)};
+        reinterpret_cast<const void*>(potential_kernel<128>), reinterpret_cast<const void*>(sweep_batch_kernel<32>),
+        reinterpret_cast<const void*>(sweep_batch_kernel<64>), reinterpret_cast<const void*>(sweep_batch_kernel<128>)};
     for (const void* k : kernels) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
         if (e != cudaSuccess) return e;
@@ -814,6 +810,21 @@ cudaError_t launch_sweep(int nt, int nw, size_t smem, cudaStream_t st, const Dev
     ALEA_LAUNCH(nt, sweep_kernel, nw, smem, st, s, records, nw, randoms, stride, prm, pairs, npair);
     return cudaGetLastError();
 }
+cudaError_t launch_sweep_generic_batch(int nt, const BatchJob* jobs, int n_jobs, int total, int grid, size_t smem,
+                                       int* next, cudaStream_t st) {
+    ALEA_LAUNCH(nt, sweep_batch_kernel, grid, smem, st, jobs, n_jobs, total, next);
+    return cudaGetLastError();
+}
+
+int batch_ctas_per_sm(int nt, size_t smem) {
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+    if (nt == 32) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_batch_kernel<32>, 32, smem);
+    else if (nt == 64) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_batch_kernel<64>, 64, smem);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_batch_kernel<128>, 128, smem);
+    return e == cudaSuccess ? std::max(n, 1) : 1;
+}
+
 #undef ALEA_LAUNCH
 
 // One sweep's (or several sweeps') random numbers per stream: stream t fills

@@ -2,6 +2,12 @@
 // walker contexts.  No reference counterpart: the reference runs one input
 // per process.
 //
+// A packed server (alea_gpu_server_create_packed) steps every admitted VMC
+// job together: one scheduler thread admits queued VMC jobs between steps
+// as memory frees up, gives each its context and runs all of them through
+// the packed engine (alea_capi.cu, "packed VMC runs"), one sweep launch per
+// step for all jobs' walkers; DMC jobs still take worker contexts.
+//
 // Each admitted job gets its own alea_gpu_ctx (own CUDA stream, own device
 // records, own random streams keyed by the job's seed) on one of max_running
 // worker threads, so several jobs' kernels are in flight on the device at
@@ -46,10 +52,21 @@ struct Job {
     Clock::time_point t_submit, t_admit;
 };
 
+// A job's AoS walkers [w][p][d] as the SoA planes alea_gpu_upload_walkers
+// reads, [p*dim*nw + d*nw + w].
+std::vector<double> soa_of(const alea_gpu_job& j) {
+    const int row = j.system->n_particles * j.system->dim, nw = j.n_walkers;
+    std::vector<double> soa(static_cast<size_t>(row) * nw);
+    for (int w = 0; w < nw; ++w)
+        for (int i = 0; i < row; ++i) soa[static_cast<size_t>(i) * nw + w] = j.positions[static_cast<size_t>(w) * row + i];
+    return soa;
+}
+
 }  // namespace
 
 struct alea_gpu_server {
     int device = 0;
+    bool packed = false;           // VMC jobs go to the packing scheduler
     size_t budget = 0, in_use = 0;
     int max_running = 1;
     std::mutex mu;
@@ -61,13 +78,80 @@ struct alea_gpu_server {
     std::vector<std::thread> workers;
     std::string err;
 
-    // First queued job that fits the budget left (caller holds mu).
-    Job* admissible() {
+    // First queued job that fits the budget left (caller holds mu); a packed
+    // server's workers take DMC jobs only, its scheduler VMC jobs only.
+    Job* admissible(bool vmc_packer = false) {
         for (uint64_t id : queue) {
             Job* j = jobs[id].get();
+            if (packed && (j->spec.mode == ALEA_JOB_VMC) != vmc_packer) continue;
             if (j->bytes <= budget - std::min(budget, in_use)) return j;
         }
         return nullptr;
+    }
+
+    void admit(Job* j) {   // caller holds mu
+        queue.erase(std::find(queue.begin(), queue.end(), j->id));
+        in_use += j->bytes;
+        j->running = true;
+        j->t_admit = Clock::now();
+    }
+
+    // The packing scheduler: admitted VMC jobs step together.
+    void packer() {
+        cudaSetDevice(device);
+        alea_gpu_packed* P = nullptr;
+        const int prc = alea_gpu::packed_create(device, &P);
+        std::vector<std::pair<Job*, alea_gpu_ctx*>> slots;   // in the engine's run order
+        for (;;) {
+            std::vector<Job*> fresh;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                if (slots.empty())
+                    cv_work.wait(lk, [&] { return stop || admissible(true) != nullptr; });
+                if (stop && slots.empty()) break;
+                if (!stop)
+                    while (Job* j = admissible(true)) {
+                        admit(j);
+                        fresh.push_back(j);
+                    }
+            }
+            for (Job* j : fresh) {
+                alea_gpu_ctx* ctx = nullptr;
+                int rc = prc != ALEA_OK ? prc : j->cancel.load() ? ALEA_ERR_CANCELLED : ALEA_OK;
+                if (rc == ALEA_OK) rc = alea_gpu_create(j->spec.system, device, j->capacity, &ctx);
+                if (rc == ALEA_OK) rc = alea_gpu_upload_walkers(ctx, soa_of(j->spec).data(), j->spec.n_walkers);
+                if (rc == ALEA_OK) rc = alea_gpu::packed_add(P, ctx, j->spec.run, nullptr);
+                if (rc != ALEA_OK) {
+                    if (ctx) alea_gpu_destroy(ctx);
+                    finish(j, rc, nullptr);
+                    continue;
+                }
+                slots.emplace_back(j, ctx);
+            }
+            if (slots.empty()) continue;
+            for (size_t i = 0; i < slots.size(); ++i)
+                if (slots[i].first->cancel.load()) alea_gpu::packed_cancel(P, static_cast<int>(i));
+            const int rc = alea_gpu::packed_step(P);
+            std::vector<std::pair<Job*, alea_gpu_ctx*>> keep;
+            for (size_t i = 0; i < slots.size(); ++i) {
+                int status = ALEA_OK;
+                alea_gpu_run_result r{};
+                const bool done = alea_gpu::packed_done(P, static_cast<int>(i), &status, &r);
+                if (!done && rc == ALEA_OK) {
+                    keep.push_back(slots[i]);
+                    continue;
+                }
+                if (!done) {
+                    status = rc;
+                    alea_gpu::packed_cancel(P, static_cast<int>(i));
+                }
+                alea_gpu_destroy(slots[i].second);
+                finish(slots[i].first, status, status == ALEA_OK ? &r : nullptr);
+            }
+            if (keep.size() != slots.size()) alea_gpu::packed_prune(P);
+            slots.swap(keep);
+        }
+        alea_gpu::packed_destroy(P);
     }
 
     void finish(Job* j, int status, const alea_gpu_run_result* r) {
@@ -98,7 +182,7 @@ struct alea_gpu_server {
         if (rc == ALEA_OK) rc = alea_gpu_create(sp.system, device, j->capacity, &ctx);
         if (rc == ALEA_OK) {
             alea_gpu::set_cancel_flag(ctx, &j->cancel);
-            rc = alea_gpu_upload_walkers(ctx, sp.positions, sp.n_walkers);
+            rc = alea_gpu_upload_walkers(ctx, soa_of(sp).data(), sp.n_walkers);
         }
         if (rc == ALEA_OK)
             rc = sp.mode == ALEA_JOB_DMC ? alea_gpu_dmc_run(ctx, &sp.run, &r, nullptr)
@@ -119,10 +203,7 @@ struct alea_gpu_server {
                 cv_work.wait(lk, [&] { return stop || admissible() != nullptr; });
                 if (stop) return;
                 j = admissible();
-                queue.erase(std::find(queue.begin(), queue.end(), j->id));
-                in_use += j->bytes;
-                j->running = true;
-                j->t_admit = Clock::now();
+                admit(j);
             }
             run(j);
         }
@@ -131,7 +212,8 @@ struct alea_gpu_server {
 
 extern "C" {
 
-int alea_gpu_server_create(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out) {
+static int server_create(int device, size_t hbm_budget_bytes, int max_running, bool packed,
+                         alea_gpu_server** out) {
     if (!out || max_running < 1) return ALEA_ERR_INVALID;
     *out = nullptr;
     int n_dev = 0;
@@ -143,9 +225,19 @@ int alea_gpu_server_create(int device, size_t hbm_budget_bytes, int max_running,
     s->device = device;
     s->budget = hbm_budget_bytes ? std::min(hbm_budget_bytes, free_b) : free_b / 10 * 8;
     s->max_running = max_running;
+    s->packed = packed;
     for (int i = 0; i < max_running; ++i) s->workers.emplace_back([s] { s->worker(); });
+    if (packed) s->workers.emplace_back([s] { s->packer(); });
     *out = s;
     return ALEA_OK;
+}
+
+int alea_gpu_server_create(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out) {
+    return server_create(device, hbm_budget_bytes, max_running, false, out);
+}
+
+int alea_gpu_server_create_packed(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out) {
+    return server_create(device, hbm_budget_bytes, max_running, true, out);
 }
 
 int alea_gpu_submit_job(alea_gpu_server* s, const alea_gpu_job* job, uint64_t* job_id) {
@@ -168,7 +260,7 @@ int alea_gpu_submit_job(alea_gpu_server* s, const alea_gpu_job* job, uint64_t* j
     *job_id = j->id;
     s->queue.push_back(j->id);
     s->jobs[j->id] = std::move(j);
-    s->cv_work.notify_one();
+    s->cv_work.notify_all();   // a packed server's workers and scheduler wait on different jobs
     return ALEA_OK;
 }
 

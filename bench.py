@@ -74,7 +74,11 @@ def parse():
                     help="serving mix instead of the DMC step: Poisson VMC jobs through alea_gpu_server")
     ap.add_argument("--serve-jobs", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=50.0, help="arrivals per second")
-    ap.add_argument("--serve-slots", type=int, default=8, help="jobs running at once")
+    ap.add_argument("--serve-slots", type=int, default=8, help="DMC jobs running at once (worker contexts)")
+    ap.add_argument("--serve-unpacked", action="store_true",
+                    help="one context and launch stream per job instead of the packed scheduler")
+    ap.add_argument("--serve-bench-jobs", type=int, default=24,
+                    help="jobs of the serving sub-object of the default line (0: none)")
     return ap.parse_args()
 
 
@@ -480,6 +484,14 @@ def gpu_arm(a):
                "note": "every walker binned on the device; the host reads one block estimate per block"}
         g.clear_estimators()
 
+    # ── the serving mix through the packed server (config 5), rank 0 only ──
+    serving = None
+    if rank == 0 and world == 1 and a.serve_bench_jobs > 0:
+        serving = run_serving(a, a.serve_bench_jobs, packed=True)
+        unpacked = run_serving(a, a.serve_bench_jobs, packed=False)
+        serving["unpacked"] = {k: unpacked[k] for k in ("value", "p50_ms", "p99_ms", "mean_queue_ms",
+                                                        "mean_run_ms", "wall_s")}
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -515,6 +527,7 @@ def gpu_arm(a):
             "population": int(g.nw),
             "fp32": fp32,
             "estimators": est,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -530,38 +543,44 @@ SERVE_WALKERS = 1024
 TWIST_GRID = [(i + 0.5) / 4.0 for i in range(4)]
 
 
-def serve_arm(a):
+def run_serving(a, n_jobs, packed=True, rate=None, slots=None):
     """The serving mix of the workload list: VMC jobs of 2^20 moves each,
-    arriving Poisson at --serve-rate, drawn uniformly from the 2-D electron gas
-    (N = 26, 42, 58, 90 at rs = 30, 40, 60, each at one of the 4x4 offset
-    twists that does not split a shell: complex determinants) and 2-D dipolar
-    bosons (N = 256, C/r^3, zero-energy Jastrow).  Every job runs through
-    alea_gpu_submit_job / alea_gpu_poll on one server; latency is submission
-    to completion.  One JSON line: aggregate moves/s, p50/p99 latency."""
+    arriving Poisson at `rate`, half from the 2-D electron gas (N = 26, 42,
+    58, 90 at rs = 30, 40, 60, each at one of the 4x4 offset twists that does
+    not split a shell: complex determinants) and half from the 2-D dipolar
+    bosons (N = 256, C/r^3, zero-energy Jastrow).  Every job goes through
+    alea_gpu_submit_job / alea_gpu_poll on one server (packed: every admitted
+    VMC job steps in the same sweep launches); latency is submission to
+    completion.  Returns the summary dict."""
     import torch
     import alea_b200
     from alea_b200 import setup as S
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py: no CUDA device")
+    rate = a.serve_rate if rate is None else rate
+    slots = a.serve_slots if slots is None else slots
     rng = np.random.default_rng(a.seed)
-    catalog = []
-    for n in (13, 21, 29, 45):
-        for rs in (30.0, 40.0, 60.0):
-            for t in [(x, y) for x in TWIST_GRID for y in TWIST_GRID]:
-                catalog.append(("heg", n, rs, t))
-    catalog.append(("dipoles", 256, 0.0353, None))
+    heg = [(n, rs, (x, y)) for n in (13, 21, 29, 45) for rs in (30.0, 40.0, 60.0)
+           for x in TWIST_GRID for y in TWIST_GRID]
     picks, setups = [], {}
-    while len(picks) < a.serve_jobs:
-        kind, n, rs, t = catalog[rng.integers(len(catalog))]
-        key = (kind, n, rs, t)
+    def setup_of(key):
         if key not in setups:
             try:
-                setups[key] = (S.heg2d_twisted(n, n, rs, t) if kind == "heg"
-                               else S.dipoles2d(n, rs, 1.0, 3.0, 0.0459))
+                setups[key] = (S.heg2d_twisted(key[1], key[1], key[2], key[3]) if key[0] == "heg"
+                               else S.dipoles2d(256, 0.0353, 1.0, 3.0, 0.0459))
             except ValueError:       # this twist splits a shell at this N: not a valid job
                 setups[key] = None
-        if setups[key] is not None:
-            picks.append(key)
+        return setups[key]
+
+    while len(picks) < n_jobs:
+        if rng.random() < 0.5:       # the family first, 50/50; then a valid member of it
+            while True:
+                n, rs, t = heg[rng.integers(len(heg))]
+                key = ("heg", n, rs, t)
+                if setup_of(key) is not None:
+                    break
+        else:
+            key = ("dipoles", 256, 0.0353, None)
+            setup_of(key)
+        picks.append(key)
     jobs = []
     for i, key in enumerate(picks):
         kind, n, rs, t = key
@@ -573,8 +592,8 @@ def serve_arm(a):
         tau = (0.5 * rs) ** 2 if kind == "heg" else 0.0003
         pos = st.positions(a.seed + i, SERVE_WALKERS)
         jobs.append((st, pos, steps, n_acc, tau, key))
-    arrivals = np.cumsum(rng.exponential(1.0 / a.serve_rate, size=len(jobs)))
-    srv = alea_b200.Server(max_running=a.serve_slots)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(jobs)))
+    srv = alea_b200.Server(max_running=slots, packed=packed)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ids = []
@@ -593,20 +612,37 @@ def serve_arm(a):
     for (st, pos, steps, n_acc, tau, key), r in zip(jobs, results):
         label = f"heg N={2 * key[1]} rs={key[2]:g}" if key[0] == "heg" else "dipoles N=256"
         kinds.setdefault(label, []).append(r.latency_ms if r is not None else None)
-    line = {
-        "metric": "serving: aggregate electron-moves/s, p50/p99 job latency", "value": moves / wall,
-        "unit": "moves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
-        "data": "synthetic: seeded uniform walkers per job, Poisson arrivals",
-        "config": {"workload": "serving mix: VMC jobs of 2^20 moves, 1024 walkers, 2-D electron gas "
-                               "N in {26,42,58,90} x rs in {30,40,60} x 4x4 offset twists (complex) "
-                               "and 2-D dipolar bosons N=256",
-                   "jobs": len(jobs), "arrival_rate_per_s": a.serve_rate, "slots": a.serve_slots},
+    return {
+        "value": moves / wall, "unit": "moves/s",
         "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
         "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
         "mean_queue_ms": float(np.mean([r.queue_ms for r in ok])) if ok else None,
-        "completed": len(ok), "wall_s": wall,
+        "mean_run_ms": float(np.mean([r.run_ms for r in ok])) if ok else None,
+        "requested_moves_per_s": float(rate * SERVE_SAMPLES),
+        "jobs": len(jobs), "completed": len(ok), "wall_s": wall, "arrival_rate_per_s": rate,
+        "dipole_jobs": sum(1 for k in picks if k[0] == "dipoles"),
+        "packed": bool(packed), "slots": slots,
         "latency_by_kind_ms": {k: float(np.median([x for x in v if x is not None])) for k, v in kinds.items()},
     }
+
+
+def serve_arm(a):
+    """--serve: the serving mix alone, one JSON line."""
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    r = run_serving(a, a.serve_jobs, packed=not a.serve_unpacked)
+    line = {
+        "metric": "serving: aggregate electron-moves/s, p50/p99 job latency", "value": r.pop("value"),
+        "unit": r.pop("unit"), "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic: seeded uniform walkers per job, Poisson arrivals",
+        "config": {"workload": "serving mix: VMC jobs of 2^20 moves, 1024 walkers; half 2-D electron gas "
+                               "N in {26,42,58,90} x rs in {30,40,60} x 4x4 offset twists (complex), "
+                               "half 2-D dipolar bosons N=256",
+                   "jobs": r["jobs"], "arrival_rate_per_s": r["arrival_rate_per_s"], "slots": r["slots"],
+                   "packed": r["packed"]},
+    }
+    line.update(r)
     print(json.dumps(line), flush=True)
     return 0
 

@@ -150,3 +150,51 @@ def test_budget_of_one_job_runs_jobs_one_after_another():
     with pytest.raises(alea_b200.AleaGpuError):
         srv.poll(ids[0], timeout_ms=0)                  # handed out once
     srv.close()
+
+
+@pytest.mark.gpu
+def test_packed_server_job_is_the_same_alone_in_a_mix_and_as_its_own_run():
+    """A packed server steps every admitted VMC job together (one sweep launch
+    per step for all of them): each job's result is bit for bit the same
+    alone, in a mix of four kinds (plane-wave, twisted, dipolar and Gaussian
+    systems, different walker counts) and as alea_gpu_vmc_run on its own
+    context; a queued job can still be cancelled."""
+    import alea_b200
+    from alea_b200 import _capi
+    heg = S.heg2d(5, 5, 30.0)
+    tw = S.heg2d_twisted(5, 5, 30.0, (0.125, 0.125))
+    dip = S.dipoles2d(16, 10.0)
+    jobs = [(heg, 64, 225.0), (tw, 48, 225.0), (dip, 40, 0.0003), (heg, 24, 100.0)]
+
+    def submit(srv, k):
+        st, nw, tau = jobs[k]
+        return srv.submit(st.desc, st.positions(300 + k, nw), 0, 1, 3, 2 + k, 1, tau, seed=17 + k,
+                          n_streams=max(1, nw // 4))
+
+    alone = []
+    for k in range(len(jobs)):
+        srv = alea_b200.Server(max_running=1, packed=True)
+        r = srv.poll(submit(srv, k), timeout_ms=120000)
+        assert r is not None and r.status == 0
+        alone.append(r.result)
+        srv.close()
+        st, nw, tau = jobs[k]
+        g = alea_b200.Walkers(st.desc, capacity=nw)
+        g.upload(st.positions(300 + k, nw))
+        own, _ = g.vmc_run(1, 3, 2 + k, 1, tau, max(1, nw // 4), 17 + k)
+        assert own.energy == r.result.energy and own.energy_error == r.result.energy_error
+        assert own.acceptance == r.result.acceptance and own.n_moves == r.result.n_moves
+        g.close()
+    srv = alea_b200.Server(max_running=1, packed=True)
+    ids = [submit(srv, k % len(jobs)) for k in range(2 * len(jobs))]
+    extra = submit(srv, 0)
+    srv.cancel(extra)
+    got = [srv.poll(i, timeout_ms=120000) for i in ids]
+    r_extra = srv.poll(extra, timeout_ms=120000)
+    srv.close()
+    assert r_extra is not None and r_extra.status in (0, _capi.ERR_CANCELLED)
+    for k, r in enumerate(got):
+        assert r is not None and r.status == 0
+        a = alone[k % len(jobs)]
+        assert r.result.energy == a.energy and r.result.energy_error == a.energy_error
+        assert r.result.acceptance == a.acceptance and r.result.n_moves == a.n_moves
