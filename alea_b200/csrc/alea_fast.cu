@@ -400,8 +400,13 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
                 }
                 const double upd = bs[1] + 1.0;
                 const double old_log = bs[0];
-                bool rebuild = upd >= 64.0 || !isfinite(R) || fabs(R) < 1e-5 || bs[2] > 1e8 ||
-                               fabs(R) <= 1e4 * kEps * acc[1];
+                // the reference's triggers; the routine refresh after 64 updates
+                // (no other trigger, N <= 24) is the update followed by one
+                // Newton-Schulz step on the tensor cores instead of Gauss-Jordan
+                const bool trigger = !isfinite(R) || fabs(R) < 1e-5 || bs[2] > 1e8 ||
+                                     fabs(R) <= 1e4 * kEps * acc[1];
+                const bool refresh = !trigger && upd >= 64.0 && N <= 24;
+                bool rebuild = trigger || (upd >= 64.0 && !refresh);
                 __syncwarp();
                 if (lane == 0) {
                     bs[1] = upd;
@@ -440,7 +445,12 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
                 for (int a = lane; a < N; a += 32) rd_max = fmax(rd_max, rabs[a]);
                 rd_max = warp_max(rd_max);
                 double cond = rebuild ? 0.0 : rd_max * warp_max(rs_max);
-                const bool cond_rebuild = !rebuild && (!isfinite(cond) || cond > 1e8);
+                bool cond_rebuild = !rebuild && (!isfinite(cond) || cond > 1e8);
+                bool refreshed = false;
+                if (refresh && !cond_rebuild) {
+                    if (ns_refresh_warp(A, D, N) < 1e-6) refreshed = true;
+                    else cond_rebuild = true;   // too far from D⁻¹: recompute by Gauss-Jordan
+                }
                 if (__builtin_expect(rebuild || cond_rebuild, 0)) {
                     gj_rebuild_warp<S>(A, v.work, v.col, D, N, v.misc);
                     if (rebuild) {
@@ -463,6 +473,7 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
                         if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
                     } else {
                         bs[0] = old_log + log(fabs(R));
+                        if (refreshed) bs[1] = 0.0;
                     }
                     v.scal[S_LOGPSI] += bs[0] - old_log;
                 }

@@ -77,6 +77,97 @@ __device__ __forceinline__ void orbital2(const DevSys& s, const DevBlock& B, int
     }
 }
 
+// D (8x8) += A (8x4, row-major) B (4x8, column-major) on the FP64 tensor
+// cores (mma.sync m8n8k4 .f64).  Lane l = 4g + t holds a = A[g][t],
+// b = B[t][g] and d = D[g][2t], D[g][2t + 1].
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+
+// One Newton-Schulz step X <- X (2I - D X) of an inverse X (shared memory,
+// row-major, stride N) against the block's orbital rows D (the record, row
+// major), N <= 24, on the FP64 tensor cores: T = D X as 3 x 3 tiles of 8 x 8
+// in registers, Y = 2I - T, then X Y tile row by tile row, each written back
+// over the rows of X it was made from.  The residual of X after a run of
+// Sherman-Morrison updates is ~1e-13, so one step leaves X = D⁻¹ to
+// rounding, the inverse the Gauss-Jordan recomputation would give.  Returns
+// max |T - I| (X untouched when it is not below 1e-6: the caller then
+// recomputes by Gauss-Jordan).
+__device__ double ns_refresh_warp(double* X, const double* D, int N) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int nb = (N + 7) >> 3;
+    double y[3][3][2];
+#pragma unroll
+    for (int mt = 0; mt < 3; ++mt) {
+        // this tile row's D fragments, all loads in flight before the products
+        double a[6];
+#pragma unroll
+        for (int kt = 0; kt < 6; ++kt) {
+            const int ar = mt * 8 + g, ac = kt * 4 + t;
+            a[kt] = (mt < nb && ar < N && ac < N) ? D[ar * N + ac] : 0.0;
+        }
+#pragma unroll
+        for (int nt = 0; nt < 3; ++nt) {
+            y[mt][nt][0] = y[mt][nt][1] = 0.0;
+            if (mt >= nb || nt >= nb) continue;
+#pragma unroll
+            for (int kt = 0; kt < 6; ++kt) {
+                if (kt * 4 >= N) break;
+                const int br = kt * 4 + t, bc = nt * 8 + g;
+                const double b = (br < N && bc < N) ? X[br * N + bc] : 0.0;
+                dmma_m8n8k4(y[mt][nt], a[kt], b);
+            }
+        }
+    }
+    double res = 0.0;
+#pragma unroll
+    for (int mt = 0; mt < 3; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 3; ++nt)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int row = mt * 8 + g, col = nt * 8 + 2 * t + i;
+                const bool in = row < N && col < N;
+                const double id = row == col ? 1.0 : 0.0;
+                if (in) res = fmax(res, fabs(y[mt][nt][i] - id));
+                y[mt][nt][i] = in ? 2.0 * id - y[mt][nt][i] : 0.0;
+            }
+    res = warp_max(res);
+    if (!(res < 1e-6)) return res;
+#pragma unroll
+    for (int mt = 0; mt < 3; ++mt) {
+        if (mt >= nb) break;
+        double o[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+        for (int nt = 0; nt < 3; ++nt) {
+            if (nt >= nb) continue;
+#pragma unroll
+            for (int kt = 0; kt < 6; ++kt) {
+                if (kt * 4 >= N) break;
+                const int ar = mt * 8 + g, ac = kt * 4 + t;
+                const double a = (ar < N && ac < N) ? X[ar * N + ac] : 0.0;
+                // Y[kt*4 + t][nt*8 + g] from the lane holding it in its C fragment
+                const int src = ((kt & 1) * 4 + t) * 4 + (g >> 1);
+                const double b0 = __shfl_sync(kAllLanes, y[kt >> 1][nt][0], src);
+                const double b1 = __shfl_sync(kAllLanes, y[kt >> 1][nt][1], src);
+                dmma_m8n8k4(o[nt], a, (g & 1) ? b1 : b0);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int nt = 0; nt < 3; ++nt)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int row = mt * 8 + g, col = nt * 8 + 2 * t + i;
+                if (nt < nb && row < N && col < N) X[row * N + col] = o[nt][i];
+            }
+        __syncwarp();
+    }
+    return res;
+}
+
 // A = D⁻¹ of an N x N block by pivoted Gauss-Jordan on one warp, in place:
 // D is loaded into A's own storage and inverted there (the reference's pivot
 // rule, first maximum |pivot| of each column, on the same column values as
