@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=8, help="DMC jobs running at once (worker contexts)")
     ap.add_argument("--serve-unpacked", action="store_true",
                     help="one context and launch stream per job instead of the packed scheduler")
+    ap.add_argument("--vmc-blocks", type=int, default=100,
+                    help="blocks of 50 sweeps of the VMC sub-object (512 walkers; 0: none)")
     ap.add_argument("--serve-bench-jobs", type=int, default=24,
                     help="jobs of the serving sub-object of the default line (0: none)")
     return ap.parse_args()
@@ -493,6 +495,30 @@ def gpu_arm(a):
                "note": "every walker binned on the device; the host reads one block estimate per block"}
         g.clear_estimators()
 
+    # ── the VMC benchmark (config 1): 512 walkers, 100 blocks x 50 sweeps ──
+    vmc_c1 = None
+    if a.vmc_blocks > 0:
+        v = alea_b200.Walkers(desc, capacity=512, device=local)
+        v.upload(setup.positions(seed + 7, 512))
+        vstream = torch.cuda.ExternalStream(v.stream_handle(), device=dev)
+        torch.cuda.synchronize()
+        barrier()
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        v0.record(vstream)
+        vres, _ = v.vmc_run(0, a.vmc_blocks, 10, 5, VMC_TAU, 8, seed + 8)
+        v1.record(vstream)
+        torch.cuda.synchronize()
+        barrier()
+        vms = reps.max(v0.elapsed_time(v1))
+        vmc_c1 = {"value": reps.sum(float(vres.n_moves)) / (vms * 1e-3), "unit": UNIT,
+                  "el_evals_per_s": reps.sum(float(vres.n_evaluations)) / (vms * 1e-3),
+                  "walkers": 512, "blocks": a.vmc_blocks, "sweeps_per_block": 50,
+                  "energy_per_particle": vres.energy / NP, "error_per_particle": vres.energy_error / NP,
+                  "acceptance": vres.acceptance, "seconds": vms * 1e-3,
+                  "note": "VMC of the same system, Metropolis step 0.5 rs, 8 random streams, from a uniform "
+                          "start (no equilibration blocks: the first blocks are in the mean)"}
+        v.close()
+
     # ── the serving mix through the packed server (config 5), rank 0 only ──
     serving = None
     if rank == 0 and world == 1 and a.serve_bench_jobs > 0:
@@ -537,6 +563,7 @@ def gpu_arm(a):
             "fp32": fp32,
             "estimators": est,
             "serving": serving,
+            "vmc_c1": vmc_c1,
         }
         print(json.dumps(line), flush=True)
     g.close()

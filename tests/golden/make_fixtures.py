@@ -29,6 +29,8 @@ components and setup-time breakups) run through oracle/_ref/ref_harness:
 * ``dmcstat_<name>.json`` a long DMC::run on 8 crowds: per-step Σw and ΣwE_L,
   reduced here to accumulation-block energies, their mean and its reblocked
   standard error (the statistical reference for the device's DMC);
+* ``vmcstat_<name>.json`` a VMC::run of the VMC benchmark's shape (512
+  walkers, 8 threads): block energies, their reblocked mean and error;
 * ``vmc_<name>_crowd.json`` / ``dmc_<name>_crowd.json`` VMC::run / DMC::run
   with fewer threads than walkers: each thread's stream serves a contiguous
   range of walkers (VMC's per-thread clones, DMC's crowds).
@@ -106,6 +108,12 @@ FW = {"heg10": dict(fw_lags="0,4,8", fw_interval=1)}
 CHAIN = {
     "heg10": dict(nw=6, seed=11, eq=1, acc=1, steps=2, substeps=2, tau=225.0, dmc_nw=8, dmc_eq=1,
                   dmc_acc=2, dmc_steps=3, dmc_tau=2.0, dmc_seed=5),
+}
+
+# the VMC benchmark's system and walker count (512 walkers, Metropolis step
+# 0.5 rs): block energies for the statistical comparison of the device's VMC
+VMC_STAT = {
+    "heg42": dict(nw=512, seed=515151, eq=2, acc=24, steps=10, substeps=5, tau=225.0, threads=8),
 }
 
 DMC_STAT = {
@@ -227,6 +235,13 @@ def main(only=None):
     chain_fixtures(only)
     fw_fixtures(only)
     ckpt_fixtures(only)
+    for name, run in VMC_STAT.items():
+        if only and name not in only:
+            continue
+        r = run_ref_harness("vmc", **run, **SYSTEMS[name])
+        mean, err = reblock(r["block_energies"])
+        dump(f"vmcstat_{name}.json", {"params": run, "system": name, "block_energies": r["block_energies"],
+                                      "energy": mean, "energy_error": err, "acceptance": r["acceptance"]})
     for name, run in DMC_STAT.items():
         if only and name not in only:
             continue

@@ -149,3 +149,21 @@ def test_heg42_dmc_energy_agrees_with_reference_statistically():
     assert res.energy_error > 0 and abs(res.energy - ref["energy"]) < 2.0 * sigma, \
         (res.energy, res.energy_error, ref["energy"], ref["energy_error"])
     g.close()
+
+
+def test_heg42_vmc_energy_agrees_with_reference_statistically():
+    """The VMC benchmark's shape (512 walkers, 8 streams, Metropolis step
+    0.5 r_s, 5 sweeps per step): the device's VMC energy from an independent
+    start and seed against the compiled reference's VMC::run, within 2
+    combined standard errors."""
+    from alea_b200 import setup as S
+    ref = golden("vmcstat_heg42.json")
+    p = ref["params"]
+    g = walkers(golden("setup_heg42.json"), p["nw"])
+    g.upload(S.heg2d(21, 21, 30.0).positions(5151, p["nw"]))
+    res, blocks = g.vmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], p["threads"], 5152)
+    sigma = float(np.hypot(res.energy_error, ref["energy_error"]))
+    assert res.energy_error > 0 and abs(res.energy - ref["energy"]) < 2.0 * sigma, \
+        (res.energy, res.energy_error, ref["energy"], ref["energy_error"])
+    assert abs(res.acceptance - ref["acceptance"]) < 0.02
+    g.close()
