@@ -87,6 +87,15 @@ def charges2d(lattice, counts, charges, ewald_tol: float = 1e-6) -> Setup:
                  cnt.ctypes.data_as(_capi.c_ip), q.ctypes.data_as(_capi.c_dp), ewald_tol)
 
 
+def ewald3d(lattice, ewald_tol: float = 1e-6) -> Setup:
+    """The 3-D Coulomb Ewald tables of a periodic cell (rows of `lattice`, 3x3):
+    host tables only, in `desc["ewald"]` (the walker kernels are 2-D)."""
+    lat = np.ascontiguousarray(np.asarray(lattice, dtype=np.float64).ravel())
+    if lat.size != 9:
+        raise ValueError("ewald3d: lattice needs 9 numbers")
+    return _make("alea_gpu_setup_ewald3d", lat.ctypes.data_as(_capi.c_dp), ewald_tol)
+
+
 def dipoles2d(n: int, rs: float, strength: float = 1.0, exponent: float = 3.0,
               matching_radius: float = 0.0459) -> Setup:
     """2-D dipolar bosons: zero-energy Jastrow, C/r^p with its continuum tail."""

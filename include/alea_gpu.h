@@ -655,6 +655,15 @@ int alea_gpu_setup_crystal2d(int nx, int ny, double rs, double gauss_c, double a
  * energy (src/hamiltonian/ewald_term.cpp:368-612). */
 int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* counts, const double* charges,
                              double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len);
+/* The 3-D Coulomb Ewald tables of a periodic cell (no counterpart in the
+ * reference, which refuses 3-D Ewald: src/numerics/ewald_breakup.cpp:211-213):
+ * rows a_i of `lattice` (9 numbers), the optimized breakup of 1/r with the
+ * 3-D radial kernel, r_c the Wigner-Seitz inradius.  Host tables only, in
+ * alea_gpu_setup_json (the spline, half-space k-vectors with weights f̃_l/V,
+ * f_l(0), f̃_s(0)/V); the walker kernels are two-dimensional and
+ * alea_gpu_create refuses this setup's system. */
+int alea_gpu_setup_ewald3d(const double* lattice, double ewald_tol, alea_gpu_setup** out, char* err,
+                           size_t err_len);
 /* 2-D dipolar bosons: n of mass 1 in a hexagonal cell at density rs, C/r^p
  * (strength, exponent) with its continuum tail, and the zero-energy Jastrow
  * with the given matching radius, cut off at the Wigner-Seitz inradius. */
