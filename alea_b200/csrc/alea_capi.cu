@@ -1015,11 +1015,11 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
         s.f_scal = ftake(s.hot - s.o_scal);
         s.f_misc = ftake(8);   // the error flag lives through the whole sweep
         const long scratch = f;
-        s.f_nval = ftake(s.maxN);
+        s.f_nval = ftake(cf * s.maxN);
         s.f_ngrad = ftake(2L * s.maxN);
         s.f_nlap = ftake(2L * s.maxN);
-        s.f_col = ftake(s.maxN);
-        s.f_rowp = ftake(s.maxN);
+        s.f_col = ftake(cf * s.maxN);
+        s.f_rowp = ftake(cf * s.maxN);
         s.f_work = static_cast<int>(f);
         // the move union: the partners' and phases' changes (the FP64 sweep
         // inverts in place); the FP32 form's FP64 rebuild also needs N² there
@@ -1950,15 +1950,19 @@ __global__ void run_sums_kernel(const double* records, int nw, long rec, int o_s
     }
 }
 
-// Launch shapes of the packed bodies: for each body class (0 one-warp, 1-3
-// generic of 32, 64, 128 threads)
+// Body classes of a packed step: 0 the one-warp sweep of real determinants,
+// 1-3 the generic sweep of 32, 64, 128 threads, 4 the one-warp sweep of
+// complex determinants.  Each class is one launch on its own stream.
+constexpr int kClasses = 5;
+
+// Launch shapes of the packed bodies: for each body class
 // the measured time per walker-sweep of shape 0 (one CTA per walker) and
 // shape 1 (persistent CTAs); the faster one is kept for the device's
 // lifetime (every packed run of the process shares the table).
 struct PackedTuner {
     std::mutex mu;
-    double ms_per_walker[64][4][2] = {};
-    int samples[64][4][2] = {};
+    double ms_per_walker[64][kClasses][2] = {};
+    int samples[64][kClasses][2] = {};
     int choice(int dev, int body) {
         std::lock_guard<std::mutex> lk(mu);
         for (int shape = 0; shape < 2; ++shape)
@@ -1984,7 +1988,7 @@ struct PackedRunState {
     alea_gpu_run_config cfg{};
     int T = 1;
     int block = 0, step = 0;
-    int cls = 0;                   // body class: 0 one-warp, 1-3 generic of 32, 64, 128 threads
+    int cls = 0;                   // body class (kClasses)
     size_t smem = 0;
     size_t stats_off = 0;
     double* d_state = nullptr;     // run_sums_kernel's [step, block, blk[T], e_sum, e2_sum]
@@ -2014,13 +2018,13 @@ struct alea_gpu_packed {
     double* h_stats = nullptr;    // pinned
     size_t stats_cap = 0;
     int* d_next = nullptr;         // one work counter per class
-    int n_jobs[4] = {0, 0, 0, 0}, job0[4] = {0, 0, 0, 0}, total[4] = {0, 0, 0, 0};
-    size_t smem[4] = {0, 0, 0, 0};
-    cudaStream_t cls_stream[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
+    int n_jobs[kClasses] = {}, job0[kClasses] = {}, total[kClasses] = {};
+    size_t smem[kClasses] = {};
+    cudaStream_t cls_stream[kClasses] = {};
+    cudaEvent_t fork = nullptr, join[kClasses] = {};
     cudaGraphExec_t graph = nullptr;
-    int graph_shapes[4] = {-1, -1, -1, -1};
-    cudaEvent_t ev[8] = {};
+    int graph_shapes[kClasses] = {-1, -1, -1, -1, -1};
+    cudaEvent_t ev[2 * kClasses] = {};
     std::string err;
     uint64_t launches = 0;
 };
@@ -2048,9 +2052,9 @@ void packed_drop_graph(alea_gpu_packed* P) {
 // going, after one joined or left.
 int packed_rebuild(alea_gpu_packed* P) {
     packed_drop_graph(P);
-    std::vector<BatchJob> lists[4];
+    std::vector<BatchJob> lists[kClasses];
     size_t stats = 0;
-    for (int k = 0; k < 4; ++k) P->smem[k] = 0, P->total[k] = 0;
+    for (int k = 0; k < kClasses; ++k) P->smem[k] = 0, P->total[k] = 0;
     for (PackedRunState& r : P->runs) {
         if (r.done) continue;
         alea_gpu_ctx* c = r.c;
@@ -2084,7 +2088,7 @@ int packed_rebuild(alea_gpu_packed* P) {
         stats += static_cast<size_t>(r.T) + 4;
     }
     int need = 0;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kClasses; ++k) {
         P->job0[k] = need;
         P->n_jobs[k] = static_cast<int>(lists[k].size());
         need += P->n_jobs[k];
@@ -2109,12 +2113,12 @@ int packed_rebuild(alea_gpu_packed* P) {
         PCUDA(P, cudaMallocHost(&P->h_stats, 8 * cap));
         P->stats_cap = cap;
     }
-    if (!P->d_next) PCUDA(P, cudaMallocAsync(&P->d_next, 4 * sizeof(int), P->stream));
-    for (int k = 0; k < 4; ++k) std::copy(lists[k].begin(), lists[k].end(), P->h_jobs + P->job0[k]);
+    if (!P->d_next) PCUDA(P, cudaMallocAsync(&P->d_next, kClasses * sizeof(int), P->stream));
+    for (int k = 0; k < kClasses; ++k) std::copy(lists[k].begin(), lists[k].end(), P->h_jobs + P->job0[k]);
     if (need) PCUDA(P, cudaMemcpyAsync(P->d_jobs, P->h_jobs, sizeof(BatchJob) * need, cudaMemcpyHostToDevice,
                                        P->stream));
     PCUDA(P, cudaStreamSynchronize(P->stream));
-    PCUDA(P, reserve_smem(std::max({P->smem[0], P->smem[1], P->smem[2], P->smem[3]})));
+    PCUDA(P, reserve_smem(*std::max_element(P->smem, P->smem + kClasses)));
     P->dirty = false;
     return ALEA_OK;
 }
@@ -2134,14 +2138,15 @@ int packed_grid(alea_gpu_packed* P, int k, int shape) {
     if (shape == 0) return total;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
-    const int per_sm = k == 0 ? 12 : batch_ctas_per_sm(16 << k, P->smem[k]);
+    const int per_sm = (k == 0 || k == 4) ? fast_batch_ctas_per_sm(k == 4, P->smem[k])
+                                          : batch_ctas_per_sm(16 << k, P->smem[k]);
     return std::max(1, std::min(total, sms * per_sm));
 }
 
 // The launches of one step: draws, then the classes' packed sweeps on their
 // own streams (forked from and joined back into the engine's stream, so they
 // run side by side), then the per-run sums and their copy.
-int packed_enqueue(alea_gpu_packed* P, const int shape[4], bool timed) {
+int packed_enqueue(alea_gpu_packed* P, const int shape[kClasses], bool timed) {
     for (const PackedRunState& r : P->runs) {
         if (r.done) continue;
         alea_gpu_ctx* c = r.c;
@@ -2152,17 +2157,18 @@ int packed_enqueue(alea_gpu_packed* P, const int shape[4], bool timed) {
         ++P->launches;
     }
     PCUDA(P, cudaGetLastError());
-    PCUDA(P, cudaMemsetAsync(P->d_next, 0, 4 * sizeof(int), P->stream));
+    PCUDA(P, cudaMemsetAsync(P->d_next, 0, kClasses * sizeof(int), P->stream));
     PCUDA(P, cudaEventRecord(P->fork, P->stream));
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kClasses; ++k) {
         if (!P->n_jobs[k]) continue;
         cudaStream_t st = P->cls_stream[k];
         PCUDA(P, cudaStreamWaitEvent(st, P->fork, 0));
         if (timed) PCUDA(P, cudaEventRecord(P->ev[2 * k], st));
         const BatchJob* jobs = P->d_jobs + P->job0[k];
-        if (k == 0)
-            PCUDA(P, launch_sweep_fast_batch(packed_zero_energy(P), jobs, P->n_jobs[0], P->total[0],
-                                             packed_grid(P, 0, shape[0]), P->smem[0], P->d_next, st));
+        if (k == 0 || k == 4)
+            PCUDA(P, launch_sweep_fast_batch(k == 0 && packed_zero_energy(P), k == 4, jobs, P->n_jobs[k],
+                                             P->total[k], packed_grid(P, k, shape[k]), P->smem[k], P->d_next + k,
+                                             st));
         else
             PCUDA(P, launch_sweep_generic_batch(16 << k, jobs, P->n_jobs[k], P->total[k],
                                                 packed_grid(P, k, shape[k]), P->smem[k], P->d_next + k, st));
@@ -2271,7 +2277,7 @@ int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& c
     if (int rc = alea_gpu_set_streams(c, cfg.seed, ALEA_STREAM_VMC, r.T)) return pfail(P, rc, c->err);
     const char* e = std::getenv("ALEA_GPU_SWEEP");
     const bool fast = c->nt == 32 && fast_sweep_eligible(c->sys) && (e == nullptr || std::strcmp(e, "generic") != 0);
-    r.cls = fast ? 0 : c->nt == 32 ? 1 : c->nt == 64 ? 2 : 3;
+    r.cls = fast ? (c->sys.cplx ? 4 : 0) : c->nt == 32 ? 1 : c->nt == 64 ? 2 : 3;
     r.smem = fast ? static_cast<size_t>(c->sys.f_total) * 8 : c->smem;
     r.chain.assign(r.T, {});
     r.blk.assign(r.T, 0.0);
@@ -2331,15 +2337,15 @@ int packed_step(alea_gpu_packed* P) {
     if (P->dirty)
         if (int rc = packed_rebuild(P)) return rc;
     const int dev = P->device;
-    int shape[4];
+    int shape[kClasses];
     bool settled = true;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kClasses; ++k) {
         shape[k] = g_packed_tuner.choice(dev, k);
         if (P->n_jobs[k] && !g_packed_tuner.settled(dev, k)) settled = false;
     }
     if (settled) {
         bool same = P->graph != nullptr;
-        for (int k = 0; k < 4 && same; ++k) same = P->graph_shapes[k] == shape[k];
+        for (int k = 0; k < kClasses && same; ++k) same = P->graph_shapes[k] == shape[k];
         if (!same) packed_drop_graph(P);
         if (!P->graph) {
             cudaGraph_t g = nullptr;
@@ -2354,7 +2360,7 @@ int packed_step(alea_gpu_packed* P) {
             const cudaError_t ie = cudaGraphInstantiate(&P->graph, g, 0);
             cudaGraphDestroy(g);
             PCUDA(P, ie);
-            for (int k = 0; k < 4; ++k) P->graph_shapes[k] = shape[k];
+            for (int k = 0; k < kClasses; ++k) P->graph_shapes[k] = shape[k];
         }
         PCUDA(P, cudaGraphLaunch(P->graph, P->stream));
     } else {
@@ -2362,7 +2368,7 @@ int packed_step(alea_gpu_packed* P) {
     }
     PCUDA(P, cudaStreamSynchronize(P->stream));
     if (!settled) {
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kClasses; ++k) {
             float ms = 0.f;
             if (P->n_jobs[k] && cudaEventElapsedTime(&ms, P->ev[2 * k], P->ev[2 * k + 1]) == cudaSuccess)
                 g_packed_tuner.record(dev, k, shape[k], ms / P->total[k]);

@@ -31,8 +31,13 @@
 namespace alea_gpu {
 
 // One walker's sweep by one warp (the body of sweep_fast_kernel and of the
-// packed launches of alea_batch.cu).
-template <int S, bool ZE>
+// packed launches).  C: the determinants are complex (twisted plane waves,
+// complex_slater_determinant.cpp:154-256): orbital values are recomputed
+// from the positions (one sincos per orbital) instead of read from stored
+// rows, the inverse is re | im, the update is the complex rank-one form and
+// the refresh after 64 updates a complex Gauss-Jordan; the fixed-phase DMC
+// accept has no node gate.
+template <int S, bool ZE, bool C>
 __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* records, int w, const double* randoms,
                                                   long stride, const SweepParams& prm, const int2* pairs,
                                                   int npair, double* sm) {
@@ -95,7 +100,7 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
         double2 dg[S], dl[S];
 #pragma unroll
         for (int j = 0; j < S; ++j) dg[j] = dl[j] = make_double2(0.0, 0.0);
-        if (drift) fetch_rows<S>(s, rec, 0, dg, dl);
+        if (!C && drift) fetch_rows<S>(s, rec, 0, dg, dl);
         for (int p = 0; p < np; ++p) {
             const int gp = from_owner<S>(kgrp, p);
             const int b = block_of(s, p);
@@ -106,7 +111,22 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
             double sgp0 = 0.0, sgp1 = 0.0, kgp0 = 0.0, kgp1 = 0.0;
             if (drift) {
                 double ra[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                if (b >= 0) {
+                if (C && b >= 0) {
+                    // Re Σ_m A[m][kr] ∇φ_m(r_p), ∇φ = i q φ
+                    const DevBlock& B = s.blocks[b];
+                    const int N = B.n, kr = p - B.first;
+                    const double* Ar = v.scal - s.o_scal + B.oA;
+                    const double* Ai = Ar + ((N * N + 3) & ~3);
+#pragma unroll 1
+                    for (int m = lane; m < N; m += 32) {
+                        const double qx = B.k[m * 2], qy = B.k[m * 2 + 1];
+                        double sn, cs;
+                        sincos(fma(qy, py, qx * px), &sn, &cs);
+                        const double ti = Ar[m * N + kr] * sn + Ai[m * N + kr] * cs;
+                        ra[0] += -qx * ti;
+                        ra[1] += -qy * ti;
+                    }
+                } else if (b >= 0) {
                     const DevBlock& B = s.blocks[b];
                     const int N = B.n, kr = p - B.first;
                     const double* A = v.scal - s.o_scal + B.oA;
@@ -121,7 +141,7 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
                         ra[3] += a * dl[j].y;
                     }
                 }
-                if (p + 1 < np) fetch_rows<S>(s, rec, p + 1, dg, dl);
+                if (!C && p + 1 < np) fetch_rows<S>(s, rec, p + 1, dg, dl);
                 if (ks) {
 #pragma unroll 1
                     for (int q = lane; q < nk; q += 32) {
@@ -173,11 +193,33 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
             }
             // ── ratio ──
             // acc: 0 R, 1 Σ|A φ|, 2-3 Σ A ∇φ, 4-5 Σ A ∂²φ, 6 log J, 7-8 pair ∇,
-            // 9-10 pair ∂², 11-12 k-space ∇, 13-14 k-space ∂², 15 Σ|φ(r')|
+            // 9-10 pair ∂², 11-12 k-space ∇, 13-14 k-space ∂², 15 Σ|φ(r')|;
+            // complex: 0-1 Re, Im R, 2-3 Re Σ A ∇φ, 4-5 Im Σ A ∇φ
             double acc[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) acc[i] = 0.0;
-            if (b >= 0) {
+            if (C && b >= 0) {
+                const DevBlock& B = s.blocks[b];
+                const int N = B.n, jrow = p - B.first;
+                const double* Ar = v.scal - s.o_scal + B.oA;
+                const double* Ai = Ar + ((N * N + 3) & ~3);
+#pragma unroll 1
+                for (int m = lane; m < N; m += 32) {
+                    const double qx = B.k[m * 2], qy = B.k[m * 2 + 1];
+                    double sn, cs;
+                    sincos(fma(qy, ny, qx * nx), &sn, &cs);
+                    v.nval[m] = cs;
+                    v.nval[N + m] = sn;
+                    const double ar = Ar[m * N + jrow], ai = Ai[m * N + jrow];
+                    const double tr = ar * cs - ai * sn, ti = ar * sn + ai * cs;
+                    acc[0] += tr;
+                    acc[1] += ti;
+                    acc[2] += -qx * ti;
+                    acc[3] += -qy * ti;
+                    acc[4] += qx * tr;
+                    acc[5] += qy * tr;
+                }
+            } else if (b >= 0) {
                 const DevBlock& B = s.blocks[b];
                 const int N = B.n, jrow = p - B.first;
                 const double* A = v.scal - s.o_scal + B.oA;
@@ -307,7 +349,15 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
             }
             warp_allsum<16>(acc);
             double logr = acc[6], phase = 0.0, logdr = 0.0, sgx = 0.0, sgy = 0.0;
-            if (b >= 0) {
+            if (C && b >= 0) {
+                // |R| and Re(Σ A ∇φ / R); the phase of R moves no fixed-phase decision
+                const double rr = acc[0], ri = acc[1];
+                const double a2 = rr * rr + ri * ri;
+                logdr = log(fmax(sqrt(a2), 1e-300));
+                const double ir = a2 > 0.0 ? rr / a2 : 0.0, ii = a2 > 0.0 ? -ri / a2 : 0.0;
+                sgx = acc[2] * ir - acc[4] * ii;
+                sgy = acc[3] * ir - acc[5] * ii;
+            } else if (b >= 0) {
                 const double R = acc[0];
                 logdr = log(fmax(fabs(R), 1e-300));
                 if (R < 0.0) phase = kPi;
@@ -371,7 +421,65 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
                     mr[nk + q] += v.sn[q];
                 }
             }
-            if (b >= 0) {
+            if (C && b >= 0) {
+                // complex Sherman-Morrison: A -= (A[:, j] / R) ⊗ (φ(r')ᵀ A - e_j),
+                // Gauss-Jordan from the positions after 64 updates or at a
+                // small or nonfinite ratio (the generic sweep's triggers)
+                const DevBlock& B = s.blocks[b];
+                const int N = B.n, jrow = p - B.first;
+                double* Ar = v.scal - s.o_scal + B.oA;
+                double* Ai = Ar + ((N * N + 3) & ~3);
+                double* bs = v.scal + S_BLOCK0 + 3 * b;
+                const double rr = acc[0], ri = acc[1];
+                const double a2 = rr * rr + ri * ri;
+                const double ir = rr / a2, ii = -ri / a2;
+                const double* nr = v.nval;
+                const double* ni = v.nval + N;
+                __syncwarp();   // the new orbital row v.nval
+#pragma unroll 1
+                for (int c = lane; c < N; c += 32) {
+                    double pr = 0.0, pi = 0.0;
+                    for (int m = 0; m < N; ++m) {
+                        const double xr = nr[m], xi = ni[m], ar = Ar[m * N + c], ai = Ai[m * N + c];
+                        pr += xr * ar - xi * ai;
+                        pi += xr * ai + xi * ar;
+                    }
+                    v.rowp[c] = pr - (c == jrow ? 1.0 : 0.0);
+                    v.rowp[N + c] = pi;
+                    const double cr = Ar[c * N + jrow], ci = Ai[c * N + jrow];
+                    v.col[c] = cr * ir - ci * ii;
+                    v.col[N + c] = cr * ii + ci * ir;
+                }
+                const double upd = bs[1] + 1.0;
+                const double old_log = bs[0];
+                const bool rebuild = upd >= 64.0 || !isfinite(a2) || sqrt(a2) < 1e-5;
+                __syncwarp();
+                if (!rebuild) {
+#pragma unroll 1
+                    for (int a = lane; a < N; a += 32) {
+                        const double fr = v.col[a], fi = v.col[N + a];
+                        for (int c = 0; c < N; ++c) {
+                            const double qr = v.rowp[c], qi = v.rowp[N + c];
+                            Ar[a * N + c] -= fr * qr - fi * qi;
+                            Ai[a * N + c] -= fr * qi + fi * qr;
+                        }
+                    }
+                } else {
+                    cgj_rebuild_warp<S>(B, v.pos, p, nx, ny, Ar, Ai, v.work, v.col, v.misc);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    if (rebuild) {
+                        bs[0] = v.misc[M_LOGDET];
+                        bs[1] = 0.0;
+                        if (v.misc[M_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+                    } else {
+                        bs[0] = old_log + logdr;
+                        bs[1] = upd;
+                    }
+                    v.scal[S_LOGPSI] += bs[0] - old_log;
+                }
+            } else if (b >= 0) {
                 const DevBlock& B = s.blocks[b];
                 const int N = B.n, jrow = p - B.first;
                 double* A = v.scal - s.o_scal + B.oA;
@@ -478,13 +586,29 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
                     v.scal[S_LOGPSI] += bs[0] - old_log;
                 }
             }
+            double wx = nx, wy = ny;
+            wrap2(s, wx, wy);
+            if (C && b >= 0 && (wx != nx || wy != ny)) {
+                // wrapping moved p by a lattice vector Δ, and every twisted
+                // orbital by the same phase e^{iq·Δ}: A's column of p is
+                // re-gauged by e^{-iq·Δ} to stay the inverse at the stored positions
+                const DevBlock& B = s.blocks[b];
+                const int N = B.n, jrow = p - B.first;
+                double* Ar = v.scal - s.o_scal + B.oA;
+                double* Ai = Ar + ((N * N + 3) & ~3);
+                double sa, ca;
+                sincos(fma(B.k[1], wy - ny, B.k[0] * (wx - nx)), &sa, &ca);
+                for (int m = lane; m < N; m += 32) {
+                    const double ar = Ar[m * N + jrow], ai = Ai[m * N + jrow];
+                    Ar[m * N + jrow] = ar * ca + ai * sa;
+                    Ai[m * N + jrow] = ai * ca - ar * sa;
+                }
+            }
             if (lane == 0) {
                 v.jg[p * 2 + 0] = acc[7];
                 v.jg[p * 2 + 1] = acc[8];
                 v.jl[p * 2 + 0] = acc[9];
                 v.jl[p * 2 + 1] = acc[10];
-                double wx = nx, wy = ny;
-                wrap2(s, wx, wy);
                 v.pos[p * 2 + 0] = wx;
                 v.pos[p * 2 + 1] = wy;
                 v.scal[S_LOGPSI] += logr - logdr;
@@ -519,18 +643,19 @@ __device__ __forceinline__ void sweep_fast_walker(const DevSys& s, double* recor
     store_fast(s, rec, sm);
 }
 
-template <int S, bool ZE>
+template <int S, bool ZE, bool C>
 __global__ void __launch_bounds__(32, 12) sweep_fast_kernel(const __grid_constant__ DevSys s, double* records,
                                                         int nw, const double* randoms, long stride,
                                                         SweepParams prm, const int2* pairs, int npair) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
     if (w >= nw) return;
-    sweep_fast_walker<S, ZE>(s, records, w, randoms, stride, prm, pairs, npair, sm);
+    sweep_fast_walker<S, ZE, C>(s, records, w, randoms, stride, prm, pairs, npair, sm);
 }
 
-// Packed one-warp sweeps of several contexts (BatchJob, alea_kernels.h).
-template <bool ZE>
+// Packed one-warp sweeps of several contexts (BatchJob, alea_kernels.h),
+// all real (C = false) or all complex.
+template <bool ZE, bool C>
 __global__ void __launch_bounds__(32, 12) sweep_fast_batch_kernel(const BatchJob* __restrict__ jobs, int n_jobs,
                                                               int total, int* next) {
     extern __shared__ __align__(16) double sm[];
@@ -539,23 +664,29 @@ __global__ void __launch_bounds__(32, 12) sweep_fast_batch_kernel(const BatchJob
         const int w = batch_next(total, next, &slot, first);
         if (w < 0) return;
         const BatchJob& J = jobs[batch_job_of(jobs, n_jobs, w)];
-        sweep_fast_walker<2, ZE>(*J.sys, J.records, w - J.first, J.randoms, J.stride, J.prm, J.pairs, J.npair,
-                                 sm);
+        sweep_fast_walker<2, ZE, C>(*J.sys, J.records, w - J.first, J.randoms, J.stride, J.prm, J.pairs, J.npair,
+                                    sm);
     }
 }
 
-cudaError_t launch_sweep_fast_batch(bool zero_energy, const BatchJob* jobs, int n_jobs, int total, int grid,
-                                    size_t smem, int* next, cudaStream_t st) {
-    if (zero_energy)
-        sweep_fast_batch_kernel<true><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
+cudaError_t launch_sweep_fast_batch(bool zero_energy, bool complex_det, const BatchJob* jobs, int n_jobs, int total,
+                                    int grid, size_t smem, int* next, cudaStream_t st) {
+    if (complex_det)
+        sweep_fast_batch_kernel<false, true><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
+    else if (zero_energy)
+        sweep_fast_batch_kernel<true, false><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
     else
-        sweep_fast_batch_kernel<false><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
+        sweep_fast_batch_kernel<false, false><<<grid, 32, smem, st>>>(jobs, n_jobs, total, next);
     return cudaGetLastError();
 }
 
-bool fast_sweep_eligible(const DevSys& s) {
-    return s.dim == 2 && !s.cplx && s.nbf == 0 && s.pair_by_group && s.np <= 64 && s.maxN <= 64 &&
-           s.nkJ <= 64 && s.ngroups <= 8;
+int fast_batch_ctas_per_sm(bool complex_det, size_t smem) {
+    int n = 0;
+    const cudaError_t e =
+        complex_det ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_fast_batch_kernel<false, true>, 32, smem)
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_fast_batch_kernel<false, false>, 32,
+                                                                    smem);
+    return e == cudaSuccess ? std::max(n, 1) : 1;
 }
 
 // Does the system have a zero-energy pair term (the out-of-line radial form)?
@@ -565,11 +696,20 @@ static bool has_zero_energy(const DevSys& s) {
     return false;
 }
 
+// Complex determinants take the one-warp sweep without zero-energy pair
+// terms (no such system is built; the form is not compiled).
+bool fast_sweep_eligible(const DevSys& s) {
+    return s.dim == 2 && s.nbf == 0 && s.pair_by_group && s.np <= 64 && s.maxN <= 64 && s.nkJ <= 64 &&
+           s.ngroups <= 8 && !(s.cplx && has_zero_energy(s));
+}
+
 cudaError_t reserve_smem_fast(size_t smem) {
-    for (const void* k : {reinterpret_cast<const void*>(sweep_fast_kernel<2, false>),
-                          reinterpret_cast<const void*>(sweep_fast_kernel<2, true>),
-                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<false>),
-                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<true>)}) {
+    for (const void* k : {reinterpret_cast<const void*>(sweep_fast_kernel<2, false, false>),
+                          reinterpret_cast<const void*>(sweep_fast_kernel<2, true, false>),
+                          reinterpret_cast<const void*>(sweep_fast_kernel<2, false, true>),
+                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<false, false>),
+                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<true, false>),
+                          reinterpret_cast<const void*>(sweep_fast_batch_kernel<false, true>)}) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    static_cast<int>(smem));
         if (e != cudaSuccess) return e;
@@ -582,10 +722,13 @@ cudaError_t launch_sweep_fast(int nw, size_t smem, cudaStream_t st, const DevSys
                               int npair) {
     (void)smem;
     const size_t bytes = static_cast<size_t>(s.f_total) * 8;
-    if (has_zero_energy(s))
-        sweep_fast_kernel<2, true><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
+    if (s.cplx)
+        sweep_fast_kernel<2, false, true><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
+    else if (has_zero_energy(s))
+        sweep_fast_kernel<2, true, false><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
     else
-        sweep_fast_kernel<2, false><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs, npair);
+        sweep_fast_kernel<2, false, false><<<nw, 32, bytes, st>>>(s, records, nw, randoms, stride, prm, pairs,
+                                                                  npair);
     return cudaGetLastError();
 }
 

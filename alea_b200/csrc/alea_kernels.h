@@ -73,18 +73,21 @@ struct BatchJob {
 };
 // Packed sweeps of n_jobs jobs, `total` walkers in all, one 32-thread CTA per
 // walker at a time: the one-warp body (alea_fast.cu, every job fast-sweep
-// eligible; zero_energy: some job has a zero-energy term) or the generic body
+// eligible; zero_energy: some job has a zero-energy term; complex_det: every
+// job's determinants are complex, none otherwise) or the generic body
 // with nt threads per walker (alea_kernels.cu, any system; each job packed
 // with the contexts of its own thread count).  grid >= total: one CTA per
 // walker; grid < total: persistent CTAs take walkers from the counter *next
 // (zero before the launch).  The walker's arithmetic is that of launch_sweep
 // on its own context whatever the grid.  reserve_smem covers both kernels.
-cudaError_t launch_sweep_fast_batch(bool zero_energy, const BatchJob* jobs, int n_jobs, int total, int grid,
-                                    size_t smem, int* next, cudaStream_t st);
+cudaError_t launch_sweep_fast_batch(bool zero_energy, bool complex_det, const BatchJob* jobs, int n_jobs, int total,
+                                    int grid, size_t smem, int* next, cudaStream_t st);
 cudaError_t launch_sweep_generic_batch(int nt, const BatchJob* jobs, int n_jobs, int total, int grid, size_t smem,
                                        int* next, cudaStream_t st);
 // Resident CTAs per SM of the generic packed kernel of nt threads at `smem`.
 int batch_ctas_per_sm(int nt, size_t smem);
+// Resident CTAs per SM of the packed one-warp kernel (real or complex form).
+int fast_batch_ctas_per_sm(bool complex_det, size_t smem);
 // The walker of global index w of a packed launch: its job by binary search
 // over the jobs' first indices.
 __device__ __forceinline__ int batch_job_of(const BatchJob* jobs, int n_jobs, int w) {

@@ -1215,7 +1215,8 @@ template <int NT, int S = 0>
 __device__ void refresh_all(const DevSys& s, const Smem& v, const double* grec) {
     const int np = s.np;
     if constexpr (S > 0) {
-        for (int b = 0; b < s.nblocks; ++b) {
+        if (s.cplx) c_refresh_all<32>(s, v);   // complex rows from the positions, one particle per lane
+        for (int b = 0; b < (s.cplx ? 0 : s.nblocks); ++b) {
             const DevBlock& B = s.blocks[b];
             const int N = B.n;
             const double* A = v.scal - s.o_scal + B.oA;

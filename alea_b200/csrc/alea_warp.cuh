@@ -306,6 +306,125 @@ __device__ __forceinline__ void gj_rebuild_warp(double* A, double* mult, double*
     gj_invert_warp<S>(A, mult, perm_area, N, misc);
 }
 
+// A = D⁻¹ of a twisted plane-wave block, D[r][c] = φ_c(x_r) recomputed from
+// the positions (the particle `moved` at (mx, my)), by pivoted complex
+// Gauss-Jordan on one warp in A's own storage (re plane Ar, im plane Ai,
+// row-major, stride N).  The pivot of column k is the first row of largest
+// |x|² at or below k, the rule of c_gj_rebuild; row k is scaled by
+// (re, im) of 1/diag, the other rows lose their multiple of it, and the row
+// exchanges are undone as column exchanges at the end.  Lane l owns columns
+// l + 32j.  log|det D| accumulates pivot by pivot (0.5 ln|d|²) into
+// misc[M_LOGDET]; a zero or nonfinite pivot is flagged in misc[M_ERR].
+// `mult` (2N doubles) and `perm_area` (N ints) are scratch.
+template <int S>
+__device__ __noinline__ void cgj_rebuild_warp(const DevBlock& B, const double* pos, int moved, double mx, double my,
+                                              double* Ar, double* Ai, double* mult, double* perm_area,
+                                              double* misc) {
+    const int lane = threadIdx.x, N = B.n;
+    int* perm = reinterpret_cast<int*>(perm_area);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const int c = lane + 32 * j;
+        if (c >= N) continue;
+        const double kx = B.k[c * 2], ky = B.k[c * 2 + 1];
+        for (int r = 0; r < N; ++r) {
+            const int part = B.first + r;
+            const double x = part == moved ? mx : pos[part * 2];
+            const double y = part == moved ? my : pos[part * 2 + 1];
+            double sn, cs;
+            sincos(fma(ky, y, kx * x), &sn, &cs);
+            Ar[r * N + c] = cs;
+            Ai[r * N + c] = sn;
+        }
+    }
+    __syncwarp();
+    double logdet = 0.0;
+    bool bad = false;
+    for (int k = 0; k < N; ++k) {
+        double best = -1.0;
+        int bi = N;
+        for (int r = k + lane; r < N; r += 32) {
+            const double xr = Ar[r * N + k], xi = Ai[r * N + k];
+            const double a = xr * xr + xi * xi;
+            if (a > best) {
+                best = a;
+                bi = r;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(kAllLanes, best, o);
+            const int oi = __shfl_xor_sync(kAllLanes, bi, o);
+            if (ob > best || (ob == best && oi < bi)) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        const int piv = bi >= N ? k : bi;   // a column of NaNs has no pivot: flagged
+        bad |= !(best > 0.0) || !isfinite(best);
+        logdet += 0.5 * log(best);
+        const double dr = Ar[piv * N + k], di = Ai[piv * N + k];
+        const double dd = dr * dr + di * di;
+        const double ir = dr / dd, ii = -di / dd;
+        __syncwarp();   // every lane has the pivot before rows move
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            const int c = lane + 32 * j;
+            if (c >= N) continue;
+            double xr = Ar[piv * N + c], xi = Ai[piv * N + c];
+            if (piv != k) {
+                Ar[piv * N + c] = Ar[k * N + c];
+                Ai[piv * N + c] = Ai[k * N + c];
+            }
+            if (c == k) {   // the inverse's column takes the place of column k
+                xr = 1.0;
+                xi = 0.0;
+            }
+            Ar[k * N + c] = xr * ir - xi * ii;
+            Ai[k * N + c] = xr * ii + xi * ir;
+        }
+        if (lane == 0) perm[k] = piv;
+        __syncwarp();
+        for (int r = lane; r < N; r += 32) {
+            mult[r] = r == k ? 0.0 : Ar[r * N + k];
+            mult[N + r] = r == k ? 0.0 : Ai[r * N + k];
+            if (r != k) Ar[r * N + k] = Ai[r * N + k] = 0.0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            const int c = lane + 32 * j;
+            if (c >= N) continue;
+            const double qr = Ar[k * N + c], qi = Ai[k * N + c];
+            for (int r = 0; r < N; ++r) {
+                if (r == k) continue;
+                const double fr = mult[r], fi = mult[N + r];
+                Ar[r * N + c] -= fr * qr - fi * qi;
+                Ai[r * N + c] -= fr * qi + fi * qr;
+            }
+        }
+        __syncwarp();
+    }
+    for (int k = N - 1; k >= 0; --k) {
+        const int pk = perm[k];
+        if (pk != k)
+            for (int r = lane; r < N; r += 32) {
+                double t = Ar[r * N + k];
+                Ar[r * N + k] = Ar[r * N + pk];
+                Ar[r * N + pk] = t;
+                t = Ai[r * N + k];
+                Ai[r * N + k] = Ai[r * N + pk];
+                Ai[r * N + pk] = t;
+            }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        misc[M_LOGDET] = logdet;
+        if (bad) misc[M_ERR] = 1.0;
+    }
+    __syncwarp();
+}
+
 // Shared-memory view of the one-warp layout (DevSys f_*).  The sg, sl, kg,
 // kl planes exist only in the local-energy phase (el = true), on top of the
 // move scratch; `work` is the move union or the local energy's tables.
@@ -327,6 +446,10 @@ __device__ __forceinline__ Smem view_fast(const DevSys& s, double* sm, bool el) 
     v.co = sm + s.f_co;
     v.so = sm + s.f_so;
     v.work = sm + (el ? s.f_elwork : s.f_work);
+    if (s.cplx) {   // phase planes of a complex ψ: in the hot part
+        v.pg = v.scal - s.o_scal + s.o_pg;
+        v.pl = v.scal - s.o_scal + s.o_pl;
+    }
     if (el) {
         v.sg = sm + s.f_sg;
         v.sl = sm + s.f_sl;

@@ -226,19 +226,31 @@ def test_free_twisted_determinant_kinetic_energy_on_device():
     assert np.max(np.abs(g.download()["local_energy"] - exact)) < 1e-12 * abs(exact) + 1e-15
 
 
+def _twisted42(nw):
+    """The 21 + 21 electron gas at r_s = 30 and twist (1/8, 3/8): a complex
+    determinant of the serving mix's size, with walkers from its own sampler."""
+    from alea_b200 import setup as S
+    st = S.heg2d_twisted(21, 21, 30.0, (0.125, 0.375))
+    return st.desc, st.positions(4242, nw)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["heg42", "crystal16", "dipoles16"])
+@pytest.mark.parametrize("name", ["heg42", "crystal16", "dipoles16", "heg10t", "heg42t"])
 def test_one_warp_sweep_matches_generic_sweep(name, monkeypatch):
-    """The one-warp sweep (taken by 32-thread walkers of real determinants)
-    and the generic CTA sweep (ALEA_GPU_SWEEP=generic) on the same walkers
-    and random streams: VMC positions bit for bit; after drift VMC and DMC
-    advances, positions to 1e-9 and E_L, weights, ln ψ to 1e-10."""
+    """The one-warp sweep (taken by 32-thread walkers of at most 64
+    particles, real or complex determinants) and the generic CTA sweep
+    (ALEA_GPU_SWEEP=generic) on the same walkers and random streams: VMC
+    positions bit for bit; after drift VMC and DMC advances, positions to
+    1e-9 and E_L, Im E_L, weights, ln ψ to 1e-10."""
     import alea_b200
-    setup = golden(f"setup_{name}.json")
-    pos = np.array(golden(f"eval_{name}.json")["positions"])
+    if name == "heg42t":
+        setup, pos = _twisted42(64)
+    else:
+        setup = golden(f"setup_{name}.json")
+        pos = np.array(golden(f"eval_{name}.json")["positions"])
     nw = pos.shape[0]
-    tau = {"heg42": 225.0, "crystal16": 400.0, "dipoles16": 0.0003}[name]
-    dtau = {"heg42": 0.5, "crystal16": 1.0, "dipoles16": 1e-5}[name]
+    tau = {"heg42": 225.0, "crystal16": 400.0, "dipoles16": 0.0003, "heg10t": 225.0, "heg42t": 225.0}[name]
+    dtau = {"heg42": 0.5, "crystal16": 1.0, "dipoles16": 1e-5, "heg10t": 0.5, "heg42t": 0.5}[name]
     out = []
     for mode in ("generic", "fast"):
         if mode == "generic":
@@ -256,12 +268,19 @@ def test_one_warp_sweep_matches_generic_sweep(name, monkeypatch):
         e0 = float(np.mean(el))
         g.dmc_advance(dtau, 1, e0, e0, 10.0, 15.0)
         g.dmc_advance(dtau, 1, e0, e0, 10.0, 15.0)
-        out.append((vmc_pos, g.download()))
+        d = g.download()
+        if name.endswith("t"):
+            d.update(g.download_phase())
+        out.append((vmc_pos, d))
         g.close()
     (vp_g, d_g), (vp_f, d_f) = out
     assert np.array_equal(vp_g, vp_f)
     assert np.max(np.abs(d_f["positions"] - d_g["positions"])) < 1e-9 * np.abs(d_g["positions"]).max()
     assert rel(d_f["local_energy"], d_g["local_energy"]) < 1e-10
+    if name.endswith("t"):
+        scale = np.abs(d_g["local_energy"]).max()
+        assert np.max(np.abs(d_f["local_energy_imag"] - d_g["local_energy_imag"])) < 1e-10 * scale
+        assert np.max(np.abs(d_f["phase_grad"] - d_g["phase_grad"])) < 1e-9 * np.abs(d_g["phase_grad"]).max()
     assert rel(d_f["log_psi"], d_g["log_psi"], floor=1.0) < 1e-10
     assert rel(d_f["weights"], d_g["weights"]) < 1e-10
 

@@ -11,8 +11,8 @@ from conftest import golden
 
 pytestmark = pytest.mark.gpu
 
-# system, walkers, tau: one-warp body (real determinants, bosons) and the
-# generic body (twisted = complex, backflow)
+# system, walkers, tau: the one-warp bodies (real determinants, bosons;
+# twisted = complex determinants) and the generic body (backflow)
 MIX = [("heg10", 64, 225.0), ("crystal16", 40, 400.0), ("dipoles16", 24, 0.0003),
        ("heg10t", 48, 225.0), ("heg10bf", 32, 225.0)]
 
