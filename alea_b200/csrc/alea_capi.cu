@@ -2911,10 +2911,17 @@ int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, doub
     const int nopt = static_cast<int>(c->h_opt.size());
     *n_params = nopt;
     if ((!dgrad && !dlap) || nopt == 0 || c->nw == 0) return ALEA_OK;
+    bool backflow = false;
     for (const DevOpt& o : c->h_opt)
-        if (o.kind == 2)
-            return fail(c, ALEA_ERR_UNSUPPORTED, "curvature terms of backflow parameters are not built");
+        if (o.kind == 2) {
+            backflow = true;
+            // η'' jumps at L when C = 2: the reference reports no curvature term there
+            if (c->sys.bf[o.term].ch[o.ch].C < 3)
+                return fail(c, ALEA_ERR_UNSUPPORTED, "curvature terms of a backflow channel with truncation C < 3");
+        }
     if (c->sys.np > 256) return fail(c, ALEA_ERR_UNSUPPORTED, "parameter derivatives: more than 256 particles");
+    if (backflow && bf_curvature_smem(c->sys) > 227 * 1024)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "backflow curvature terms: the block needs more than 227 KB of shared memory");
     const size_t cap = static_cast<size_t>(nopt) * c->sys.np * 2 * c->capacity;
     if (!c->d_opt_grad && cudaMallocAsync(&c->d_opt_grad, 2 * cap * 8, c->stream) != cudaSuccess)
         return fail(c, ALEA_ERR_NOMEM, "parameter derivatives: device allocation failed");
@@ -2925,6 +2932,10 @@ int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, doub
     CUDA_TRY(c, cudaMemsetAsync(l, 0, n * 8, c->stream));
     ++c->launches;
     CUDA_TRY(c, launch_param_grad_derivatives(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, g, l));
+    if (backflow) {
+        ++c->launches;
+        CUDA_TRY(c, launch_bf_curvature(c->nw, c->stream, c->sys, records(c), c->d_opt, nopt, g, l));
+    }
     if (int rc = orbital_param_derivatives(c, nullptr, g, l)) return rc;
     if (dgrad) CUDA_TRY(c, copy_out(c, dgrad, g, n * 8));
     if (dlap) CUDA_TRY(c, copy_out(c, dlap, l, n * 8));

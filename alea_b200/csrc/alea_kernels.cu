@@ -276,6 +276,332 @@ __device__ __forceinline__ double bf_eta_dparam(const DevBFCh& C, int k, int zs,
     return v;
 }
 
+// ∂η/∂p, ∂η'/∂p and ∂η''/∂p at r of one backflow parameter (k >= 0 the
+// coefficient c_k, k = -1 the cutoff; zs: c_1 = C c_0/L), zero beyond L
+// (BackflowFunction::parameter_derivatives, backflow_function.h:137-196;
+// the channel's truncation C >= 3).  With t = 1 - r/L and f = t^C, a
+// coefficient multiplies b(r) = r^k (plus C r/L for c_0 when zs):
+// (f b, f'b + f b', f''b + 2f'b' + f b'').  The cutoff moves f by
+// g = ∂f/∂L = (C/L²) r t^{C-1} and, when zs, c_1 by a = -C c_0/L².
+__device__ void bf_eta_dparam3(const DevBFCh& C, int k, int zs, double r, double& de, double& d1, double& d2) {
+    de = d1 = d2 = 0.0;
+    if (r >= C.L) return;
+    const double Cd = static_cast<double>(C.C), L = C.L;
+    const double t = 1.0 - r / L;
+    double tc3 = 1.0;
+    for (int i = 0; i < C.C - 3; ++i) tc3 *= t;
+    const double tc2 = tc3 * t, tc1 = tc2 * t, f = tc1 * t;
+    const double fp = -Cd / L * tc1, fpp = Cd * (Cd - 1.0) / (L * L) * tc2;
+    if (k >= 0) {
+        double b = 1.0, b1 = 0.0, b2 = 0.0;   // r^k, k r^{k-1}, k(k-1) r^{k-2}
+        for (int i = 0; i < k; ++i) {
+            b2 = b2 * r + 2.0 * b1;
+            b1 = b1 * r + b;
+            b *= r;
+        }
+        if (zs && k == 0) {
+            b += Cd * r / L;
+            b1 += Cd / L;
+        }
+        de = f * b;
+        d1 = fp * b + f * b1;
+        d2 = fpp * b + 2.0 * fp * b1 + f * b2;
+        return;
+    }
+    double P = 0.0, Pp = 0.0, Ppp = 0.0;
+    for (int i = C.nc - 1; i >= 0; --i) {
+        Ppp = Ppp * r + 2.0 * Pp;
+        Pp = Pp * r + P;
+        P = P * r + C.c[i];
+    }
+    const double pre = Cd / (L * L);
+    const double g = pre * r * tc1;
+    const double g1 = pre * (tc1 - (Cd - 1.0) * (r / L) * tc2);
+    const double g2 = Cd * (Cd - 1.0) / (L * L * L) * (-2.0 * tc2 + (Cd - 2.0) * (r / L) * tc3);
+    const double a = zs ? -Cd * C.c[0] / (L * L) : 0.0;
+    de = g * P + f * a * r;
+    d1 = g1 * P + g * Pp + fp * a * r + f * a;
+    d2 = g2 * P + 2.0 * g1 * Pp + g * Ppp + fpp * a * r + 2.0 * fp * a;
+}
+
+// The pair tensors B = e δ + e1 r̂ r̂ᵀ r and S_{αβ} = ∂²_β [e r_α] of a radial
+// function with values (e, e1, e2) at the displacement del (|del| = r > 0):
+// the same forms as bf_pair's, here for the parameter derivative of η.
+__device__ __forceinline__ void bf_tensors(double e, double e1, double e2, const double* del, double r, double* B,
+                                           double* S) {
+    const double inv_r = r > 0.0 ? 1.0 / r : 0.0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            B[a * 2 + b] = (a == b ? e : 0.0) + e1 * del[a] * del[b] * inv_r;
+            const double rb2 = del[b] * del[b] * inv_r * inv_r;
+            S[a * 2 + b] = (a == b ? 2.0 * e1 * del[b] * inv_r : 0.0) + del[a] * (e2 * rb2 + e1 * inv_r * (1.0 - rb2));
+        }
+}
+
+// Orbital m of a backflow determinant at x: value, gradient, Hessian
+// [a*2 + b] and the Hessian's derivative along u, hu[a*2 + b] =
+// Σ_c ∂_a∂_b∂_c φ u_c (OrbitalSet::evaluate_third_derivatives contracted
+// with u).  Plane waves: ∂_a∂_b∂_c φ = -k_a k_b k_c φ' (φ' = -sin or cos);
+// Gaussians e^{-α d²}: [4α²(δ_ac d_b + δ_bc d_a + δ_ab d_c) - 8α³ d_a d_b d_c] φ.
+__device__ void bf_orbital3(const DevSys& s, const DevBF& D, int m, const double* x, const double* u, double* g,
+                            double* h, double* hu) {
+    if (D.type == 0) {
+        const double kx = D.k[m * 2], ky = D.k[m * 2 + 1];
+        double sn, c;
+        sincos(kx * x[0] + ky * x[1], &sn, &c);
+        const bool is_s = D.is_sin[m] != 0.0;
+        const double v = is_s ? sn : c, dv = is_s ? c : -sn;
+        const double k2[2] = {kx, ky};
+        const double ku = kx * u[0] + ky * u[1];
+        g[0] = kx * dv;
+        g[1] = ky * dv;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                h[a * 2 + b] = -k2[a] * k2[b] * v;
+                hu[a * 2 + b] = -k2[a] * k2[b] * dv * ku;
+            }
+    } else {
+        const double al = D.alphas[m];
+        double del[3] = {x[0] - D.centers[m * 2], x[1] - D.centers[m * 2 + 1], 0.0};
+        min_image(s, del);
+        const double phi = exp(-al * (del[0] * del[0] + del[1] * del[1]));
+        const double du = del[0] * u[0] + del[1] * u[1];
+        g[0] = -2.0 * al * del[0] * phi;
+        g[1] = -2.0 * al * del[1] * phi;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                const double dab = a == b ? 1.0 : 0.0;
+                h[a * 2 + b] = (4.0 * al * al * del[a] * del[b] - 2.0 * al * dab) * phi;
+                hu[a * 2 + b] = (4.0 * al * al * (u[a] * del[b] + u[b] * del[a] + dab * du) -
+                                 8.0 * al * al * al * del[a] * del[b] * du) *
+                                phi;
+            }
+    }
+}
+
+// ∂(∇ ln|D|)/∂p and ∂(∇² ln|D|)/∂p of a backflow determinant for every
+// optimisable channel parameter p of it, one CTA per walker, each parameter
+// in turn (BackflowSlaterDeterminant::compute_parameter_gradient_derivatives
+// and tangent_derivatives, backflow_slater_determinant.cpp:754-958).  The
+// parameter moves the quasi-coordinates by ẋ_t = Σ_j ∂η(r_tj)/∂p r_tj, so
+// with M[r][m] = φ_m(x_r) and A = M⁻¹ (committed):
+//   Ṁ[r][m] = ∇φ_m(x_r)·ẋ_r,  Ȧ = -A Ṁ A,
+//   Ḟ_iα = Σ_m Ȧ_mi ∂_αφ_m(x_i) + A_mi ∇∂_αφ_m(x_i)·ẋ_i,  Ṫ_i and Ġ^α alike,
+// and for every affected particle k and direction β, with v, v̇ the Jacobian
+// column of (k, β) and its parameter derivative (the pair tensors of ∂η/∂p,
+// no identity part):
+//   ∂_p ∂_kβ ln|D| = Σ_t Ḟ_t·v_t + F_t·v̇_t,
+//   ∂_p ∂²_kβ ln|D| = Σ_t (Ḟ_t·S_t + F_t·Ṡ_t + 2 v̇_tᵀ T_t v_t + v_tᵀ Ṫ_t v_t)
+//                    - 2 Σ_jr U̇_jr U_rj,   U_jr = Σ_α v_rα G^α_jr.
+// Shared memory (doubles): 2 np + 20 N² + 22 N.  Outputs [q][p*2 + d][nw]
+// for the backflow parameters q; other particles are left as they are.
+template <int NT>
+__global__ void __launch_bounds__(NT) bf_curvature_kernel(DevSys s, const double* records, int nw,
+                                                          const DevOpt* opts, int nopt, double* dgrad,
+                                                          double* dlap) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[(NT / 32) * 4 + 4];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    const int np = s.np;
+    const double* rec = records + static_cast<long>(w) * s.rec;
+    double* pos = sm;
+    for (int i = threadIdx.x; i < np * 2; i += NT) pos[i] = rec[s.o_pos + i];
+    const long plane = static_cast<long>(np) * 2 * nw;
+    for (int q = 0; q < nopt; ++q) {
+        const DevOpt& o = opts[q];
+        if (o.kind != 2) continue;
+        const DevBF& D = s.bf[o.term];
+        const DevBFCh& Cq = D.ch[o.ch];
+        const int N = D.n, NN = N * N;
+        double* x = pos + 2 * np;
+        double* xd = x + 2 * N;
+        double* A = xd + 2 * N;
+        double* Ad = A + NN;
+        double* Pm = Ad + NN;
+        double* Gr = Pm + NN;     // ∇φ_m(x_r)       [(r*N + m)*2 + α]
+        double* Hs = Gr + 2 * NN; // ∇∇φ_m(x_r)      [(r*N + m)*4 + αγ]
+        double* Md = Hs + 4 * NN; // Ṁ[r][m]
+        double* gd = Md + NN;     // (∇φ_m)˙(x_r)    [(r*N + m)*2 + α]
+        double* hd = gd + 2 * NN; // (∇∇φ_m)˙(x_r)   [(r*N + m)*4 + αγ]
+        double* G = hd + 4 * NN;  // G^α[j][r]       [α*NN + j*N + r]
+        double* Gd = G + 2 * NN;
+        double* T = Gd + 2 * NN;  // T_i [i*4 + αγ]
+        double* Td = T + 4 * N;
+        double* Fd = Td + 4 * N;  // Ḟ_i [i*2 + α]
+        double* V = Fd + 2 * N;   // Jacobian column [β*2N + t*2 + α]
+        double* Vd = V + 4 * N;
+        const double* F = rec + D.oF;
+        __syncthreads();
+        for (int t = threadIdx.x; t < N; t += NT) {
+            const int P = D.first + t;
+            bf_row_x(s, D, pos, -1, nullptr, P, x + t * 2);
+            double u0 = 0.0, u1 = 0.0;
+            for (int j = Cq.sf; j < Cq.sl; ++j) {
+                if (j == P) continue;
+                double del[3] = {pos[P * 2] - pos[j * 2], pos[P * 2 + 1] - pos[j * 2 + 1], 0.0};
+                min_image(s, del);
+                const double r = sqrt(del[0] * del[0] + del[1] * del[1]);
+                if (r >= Cq.L) continue;
+                double de, d1, d2;
+                bf_eta_dparam3(Cq, o.index, o.zs, r, de, d1, d2);
+                u0 += de * del[0];
+                u1 += de * del[1];
+            }
+            xd[t * 2] = u0;
+            xd[t * 2 + 1] = u1;
+        }
+        for (int i = threadIdx.x; i < NN; i += NT) A[i] = rec[D.oA + i];
+        __syncthreads();
+        for (int e = threadIdx.x; e < NN; e += NT) {
+            const int r = e / N, m = e % N;
+            double g[2], h[4], hu[4];
+            const double* u = xd + r * 2;
+            bf_orbital3(s, D, m, x + r * 2, u, g, h, hu);
+            Gr[e * 2] = g[0];
+            Gr[e * 2 + 1] = g[1];
+            Md[e] = g[0] * u[0] + g[1] * u[1];
+            for (int a = 0; a < 2; ++a) {
+                gd[e * 2 + a] = h[a * 2] * u[0] + h[a * 2 + 1] * u[1];
+                for (int b = 0; b < 2; ++b) {
+                    Hs[e * 4 + a * 2 + b] = h[a * 2 + b];
+                    hd[e * 4 + a * 2 + b] = hu[a * 2 + b];
+                }
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < NN; e += NT) {   // Pm = A Ṁ
+            const int m = e / N, mp = e % N;
+            double acc = 0.0;
+            for (int r = 0; r < N; ++r) acc += A[m * N + r] * Md[r * N + mp];
+            Pm[e] = acc;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < NN; e += NT) {   // Ȧ = -Pm A
+            const int m = e / N, r = e % N;
+            double acc = 0.0;
+            for (int mp = 0; mp < N; ++mp) acc += Pm[m * N + mp] * A[mp * N + r];
+            Ad[e] = -acc;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < N; i += NT) {
+            double f[2] = {0, 0}, tt[4] = {0, 0, 0, 0}, td[4] = {0, 0, 0, 0};
+            for (int m = 0; m < N; ++m) {
+                const double a = A[m * N + i], ad = Ad[m * N + i];
+                const int e = i * N + m;
+                for (int al = 0; al < 2; ++al) f[al] += ad * Gr[e * 2 + al] + a * gd[e * 2 + al];
+                for (int ag = 0; ag < 4; ++ag) {
+                    tt[ag] += a * Hs[e * 4 + ag];
+                    td[ag] += ad * Hs[e * 4 + ag] + a * hd[e * 4 + ag];
+                }
+            }
+            Fd[i * 2] = f[0];
+            Fd[i * 2 + 1] = f[1];
+            for (int ag = 0; ag < 4; ++ag) {
+                T[i * 4 + ag] = tt[ag];
+                Td[i * 4 + ag] = td[ag];
+            }
+        }
+        for (int e = threadIdx.x; e < NN; e += NT) {
+            const int j = e / N, r = e % N;
+            double g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;
+            for (int m = 0; m < N; ++m) {
+                const double a = A[m * N + j], ad = Ad[m * N + j];
+                const int f = r * N + m;
+                g0 += a * Gr[f * 2];
+                g1 += a * Gr[f * 2 + 1];
+                h0 += ad * Gr[f * 2] + a * gd[f * 2];
+                h1 += ad * Gr[f * 2 + 1] + a * gd[f * 2 + 1];
+            }
+            G[e] = g0;
+            G[NN + e] = g1;
+            Gd[e] = h0;
+            Gd[NN + e] = h1;
+        }
+        __syncthreads();
+        for (int k = 0; k < np; ++k) {
+            if (!bf_affects(D, k)) continue;
+            const int tk = (k >= D.first && k < D.last) ? k - D.first : -1;
+            // acc: 0-1 ∂_p of the gradient (β = 0, 1), 2-3 of the Laplacian
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int t = threadIdx.x; t < N; t += NT) {
+                double vt[2][2] = {{0, 0}, {0, 0}}, vd[2][2] = {{0, 0}, {0, 0}};
+                const int P = D.first + t;
+                const double* Ft = F + t * 2;
+                const double* Fdt = Fd + t * 2;
+                for (int c = 0; c < D.nch; ++c) {
+                    const DevBFCh& Ch = D.ch[c];
+                    const bool own = t == tk;
+                    if (!own && (k < Ch.sf || k >= Ch.sl)) continue;
+                    for (int j = own ? Ch.sf : k; j < (own ? Ch.sl : k + 1); ++j) {
+                        if (own && j == k) continue;
+                        const double* ri = own ? pos + k * 2 : pos + P * 2;
+                        const double* rj = own ? pos + j * 2 : pos + k * 2;
+                        double unused[2] = {0, 0}, B[4], S[4];
+                        if (!bf_pair(s, Ch, ri, rj, 1.0, unused, B, S)) continue;
+                        const double sg = own ? 1.0 : -1.0;
+                        for (int be = 0; be < 2; ++be)
+                            for (int a = 0; a < 2; ++a) {
+                                vt[be][a] += sg * B[a * 2 + be];
+                                acc[2 + be] += Fdt[a] * S[a * 2 + be];
+                            }
+                        if (c != o.ch) continue;
+                        double del[3] = {ri[0] - rj[0], ri[1] - rj[1], 0.0};
+                        min_image(s, del);
+                        const double r = sqrt(del[0] * del[0] + del[1] * del[1]);
+                        double de, d1, d2, Bd[4], Sd[4];
+                        bf_eta_dparam3(Ch, o.index, o.zs, r, de, d1, d2);
+                        bf_tensors(de, d1, d2, del, r, Bd, Sd);
+                        for (int be = 0; be < 2; ++be)
+                            for (int a = 0; a < 2; ++a) {
+                                vd[be][a] += sg * Bd[a * 2 + be];
+                                acc[2 + be] += Ft[a] * Sd[a * 2 + be];
+                            }
+                    }
+                }
+                if (t == tk) {
+                    vt[0][0] += 1.0;
+                    vt[1][1] += 1.0;
+                }
+                for (int be = 0; be < 2; ++be) {
+                    V[be * 2 * N + t * 2] = vt[be][0];
+                    V[be * 2 * N + t * 2 + 1] = vt[be][1];
+                    Vd[be * 2 * N + t * 2] = vd[be][0];
+                    Vd[be * 2 * N + t * 2 + 1] = vd[be][1];
+                    acc[be] += Fdt[0] * vt[be][0] + Fdt[1] * vt[be][1] + Ft[0] * vd[be][0] + Ft[1] * vd[be][1];
+                    const double* Tt = T + t * 4;
+                    const double* Tdt = Td + t * 4;
+                    for (int a = 0; a < 2; ++a)
+                        for (int g = 0; g < 2; ++g)
+                            acc[2 + be] += 2.0 * vd[be][a] * Tt[a * 2 + g] * vt[be][g] +
+                                           vt[be][a] * Tdt[a * 2 + g] * vt[be][g];
+                }
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < NN; e += NT) {
+                const int j = e / N, r = e % N;
+                for (int be = 0; be < 2; ++be) {
+                    const double* Vb = V + be * 2 * N;
+                    const double* Vdb = Vd + be * 2 * N;
+                    const double urj = Vb[j * 2] * G[r * N + j] + Vb[j * 2 + 1] * G[NN + r * N + j];
+                    const double udjr = Vdb[r * 2] * G[e] + Vdb[r * 2 + 1] * G[NN + e] + Vb[r * 2] * Gd[e] +
+                                        Vb[r * 2 + 1] * Gd[NN + e];
+                    acc[2 + be] -= 2.0 * udjr * urj;
+                }
+            }
+            block_sum<NT>(acc, red);
+            if (threadIdx.x == 0) {
+                const long base = q * plane + static_cast<long>(k) * 2 * nw + w;
+                dgrad[base] = acc[0];
+                dgrad[base + nw] = acc[1];
+                dlap[base] = acc[2];
+                dlap[base + nw] = acc[3];
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // pair sum of du/dp over the term's pairs (minus, for an image sum, the
 // breakup's long-range part and limit inside r_cut, zero outside) plus the
 // image sum's k-space part, sum_k w'_k |rho_a|^2 or 2 Re rho_a rho_b*
@@ -735,6 +1061,25 @@ cudaError_t launch_param_grad_derivatives(int nw, cudaStream_t st, const DevSys&
                                           const DevOpt* opts, int nopt, double* dgrad, double* dlap) {
     if (nw < 1 || nopt < 1) return cudaSuccess;
     param_grad_kernel<64><<<nw, 64, 0, st>>>(s, records, nw, opts, nopt, dgrad, dlap);
+    return cudaGetLastError();
+}
+
+size_t bf_curvature_smem(const DevSys& s) {
+    int n = 0;
+    for (int d = 0; d < s.nbf; ++d) n = std::max(n, s.bf[d].n);
+    // positions 2 np; A, Ȧ, A Ṁ, Ṁ (N² each), ∇φ, ∇φ˙, G, Ġ (2N²), ∇∇φ, ∇∇φ˙ (4N²);
+    // x, ẋ, Ḟ (2N), T, Ṫ, the two Jacobian columns and their derivatives (4N)
+    return 8 * (2 * static_cast<size_t>(s.np) + 20 * static_cast<size_t>(n) * n + 22 * static_cast<size_t>(n));
+}
+
+cudaError_t launch_bf_curvature(int nw, cudaStream_t st, const DevSys& s, const double* records, const DevOpt* opts,
+                                int nopt, double* dgrad, double* dlap) {
+    if (nw < 1 || nopt < 1 || s.nbf < 1) return cudaSuccess;
+    const size_t smem = bf_curvature_smem(s);
+    const cudaError_t e = cudaFuncSetAttribute(bf_curvature_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    bf_curvature_kernel<128><<<nw, 128, smem, st>>>(s, records, nw, opts, nopt, dgrad, dlap);
     return cudaGetLastError();
 }
 

@@ -35,6 +35,11 @@ cudaError_t launch_orbital_param_derivatives(int nw, int grid, cudaStream_t st, 
 // each; entries of particles outside a parameter's term are left as they are.
 cudaError_t launch_param_grad_derivatives(int nw, cudaStream_t st, const DevSys& s, const double* records,
                                           const DevOpt* opts, int nopt, double* dgrad, double* dlap);
+// The backflow channels' parameters' curvature terms (one CTA per walker)
+// and the dynamic shared memory that kernel takes.
+size_t bf_curvature_smem(const DevSys& s);
+cudaError_t launch_bf_curvature(int nw, cudaStream_t st, const DevSys& s, const double* records, const DevOpt* opts,
+                                int nopt, double* dgrad, double* dlap);
 // Measured FP64 FMA throughput of `device` in TFLOP/s (a register-only loop).
 cudaError_t measure_fp64_peak(int device, double* tflops);
 // Potential energy of n stored configurations rows[idx[c]] into out[c].

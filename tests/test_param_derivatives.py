@@ -10,7 +10,9 @@ variant frees its Drummond alpha_0, an alpha_2 term and the cutoff L, and
 each Gaussian block's shared width (d ln det/d alpha = Tr(A dD), and
 dA = -A dD A for the curvature term).  The backflow gas frees each channel's
 c_0 (and the unlike-spin c_1): O = Σ_P Σ_j (F_P · r_Pj) dη(r_Pj)/dp with the
-committed F = A^T ∇φ(x); its curvature terms are refused.  Tolerance 1e-10
+committed F = A^T ∇φ(x); its curvature terms follow the quasi-coordinates'
+parameter tangent through A, F, T, G and the Jacobian columns (a channel of
+truncation C < 3 is refused, as the reference reports none).  Tolerance 1e-10
 relative to the largest |O_k|; after VMC steps (rho(k) updated move by move)
 the derivatives equal those of a fresh evaluation of the same positions.
 """
@@ -78,11 +80,6 @@ def test_parameter_gradient_derivatives_match_reference(name):
     nw, m = len(pos), int(setup["np"]) * int(setup["dim"])
     g = alea_b200.Walkers(setup, capacity=8)
     g.upload(pos)
-    if "backflow" in setup:
-        with pytest.raises(alea_b200.AleaGpuError) as e:
-            g.parameter_gradient_derivatives()
-        assert e.value.code == 3                     # backflow curvature terms: not built
-        return
     dg, dl = g.parameter_gradient_derivatives()
     terms = ours(setup, ev["param_grad_derivs"])
     assert all(t["ok"] for t in terms)
@@ -91,3 +88,22 @@ def test_parameter_gradient_derivatives_match_reference(name):
     assert dg.shape == wg.shape and dl.shape == wl.shape
     assert np.max(np.abs(dg - wg)) <= 1e-9 * np.abs(wg).max()
     assert np.max(np.abs(dl - wl)) <= 1e-9 * np.abs(wl).max()
+
+
+def test_backflow_curvature_refused_below_truncation_three():
+    """A channel with C = 2 (η'' jumps at L): no curvature term, as in the
+    reference (supports_parameter_gradient_derivatives is false there)."""
+    import copy
+    import alea_b200
+    setup = copy.deepcopy(golden("setup_heg10bf.json"))
+    for b in setup["backflow"]:
+        for ch in b["channels"]:
+            ch["C"] = 2
+            if ch.get("zero_slope"):
+                ch["coeffs"][1] = 2.0 * ch["coeffs"][0] / ch["L"]
+    g = alea_b200.Walkers(setup, capacity=8)
+    g.upload(np.array(golden("eval_heg10bf.json")["positions"]))
+    with pytest.raises(alea_b200.AleaGpuError) as e:
+        g.parameter_gradient_derivatives()
+    assert e.value.code == 3
+    g.close()
