@@ -110,3 +110,33 @@ def exciton2d(L_init: float = 1.0) -> Setup:
     if rc != 0:
         raise ValueError(f"alea_gpu_setup_exciton2d failed ({rc})")
     return Setup(h)
+
+
+def with_backflow(desc: dict, c0_like: float = 0.3, c0_unlike: float = 0.2, c1_unlike: float = 0.002,
+                  C: int = 3, cutoff: float = 0.0) -> dict:
+    """A copy of a plane-wave system description whose determinants become
+    backflow determinants (BackflowSlaterDeterminant with the
+    transformation of backflow_transformation.h): each block is displaced by
+    every block, through η(r) = (1 - r/L)^C (c_0 + c_1 r), like-spin channels
+    with zero slope at the origin (c_1 = C c_0/L, only c_0 free) and
+    unlike-spin channels with c_0 and c_1 free.  The cutoff defaults to the
+    cell's Wigner-Seitz inradius, the largest the reference allows."""
+    import copy
+    out = copy.deepcopy(desc)
+    blocks = out.pop("slater")
+    if any(b.get("type") != "plane_wave" for b in blocks):
+        raise ValueError("with_backflow: plane-wave determinants only")
+    v = np.asarray(out["cell"]["vectors"], float).reshape(2, 2)
+    L = cutoff or 0.5 * min(np.linalg.norm(v[0]), np.linalg.norm(v[1]), np.linalg.norm(v[0] + v[1]),
+                            np.linalg.norm(v[0] - v[1]))
+    out["backflow"] = []
+    for b in blocks:
+        chans = []
+        for src in blocks:
+            like = src["first"] == b["first"]
+            chans.append({"source_first": src["first"], "source_last": src["last"], "C": C,
+                          "coeffs": [c0_like, C * c0_like / L] if like else [c0_unlike, c1_unlike],
+                          "L": L, "zero_slope": 1 if like else 0, "opt_index": [0] if like else [0, 1]})
+        out["backflow"].append({"first": b["first"], "last": b["last"], "type": "plane_wave", "k": b["k"],
+                                "is_sin": b["is_sin"], "channels": chans})
+    return out

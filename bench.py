@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=8, help="DMC jobs running at once (worker contexts)")
     ap.add_argument("--serve-unpacked", action="store_true",
                     help="one context and launch stream per job instead of the packed scheduler")
+    ap.add_argument("--no-other-systems", dest="other_systems", action="store_false",
+                    help="skip the twisted and backflow variants of the gas")
     ap.add_argument("--vmc-blocks", type=int, default=100,
                     help="blocks of 50 sweeps of the VMC sub-object (512 walkers; 0: none)")
     ap.add_argument("--serve-bench-jobs", type=int, default=24,
@@ -519,6 +521,47 @@ def gpu_arm(a):
                           "start (no equilibration blocks: the first blocks are in the mean)"}
         v.close()
 
+    # ── other trial functions of the same gas, VMC sweeps timed on the device ──
+    def vmc_sweeps(d, pos, n_walkers, steps, tau):
+        v = alea_b200.Walkers(d, capacity=n_walkers, device=local)
+        v.upload(pos)
+        v.set_streams(seed + 11, alea_b200.STREAM_VMC, n_walkers)
+        vs = torch.cuda.ExternalStream(v.stream_handle(), device=dev)
+        for _ in range(max(a.warmup, 3)):
+            v.vmc_step(tau, 1, False)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(vs)
+        acc = 0
+        for _ in range(steps):
+            acc += v.vmc_step(tau, 1, False).n_accepted
+        e1.record(vs)
+        torch.cuda.synchronize()
+        barrier()
+        t = reps.max(e0.elapsed_time(e1)) * 1e-3
+        n = n_walkers * int(d["np"]) * steps
+        out = {"value": reps.sum(float(n)) / t, "unit": UNIT, "walkers": n_walkers, "sweeps": steps,
+               "ms_per_sweep": t * 1e3 / steps, "acceptance": acc / n,
+               "energy_per_particle": float(np.mean(v.download()["local_energy"])) / int(d["np"])}
+        v.close()
+        return out
+
+    others = None
+    if a.other_systems:
+        from alea_b200 import setup as S
+        tw = S.heg2d_twisted(21, 21, RS, (0.125, 0.125))
+        others = {
+            "twisted_heg42": dict(vmc_sweeps(tw.desc, tw.positions(seed + 12, nw), nw, 5, VMC_TAU),
+                                  sweep="one-warp complex sweep",
+                                  system="N=42 rs=30 at twist (1/8, 1/8): complex determinant"),
+            "backflow_heg42": dict(vmc_sweeps(S.with_backflow(desc), setup.positions(seed + 13, 2048), 2048, 3,
+                                              VMC_TAU),
+                                   sweep="generic CTA sweep, one pivoted Gauss-Jordan per determinant per move",
+                                   system="N=42 rs=30 with backflow determinants (C=3, L at the inradius)"),
+        }
+        tw.close()
+
     # ── the serving mix through the packed server (config 5), rank 0 only ──
     serving = None
     if rank == 0 and world == 1 and a.serve_bench_jobs > 0:
@@ -564,6 +607,7 @@ def gpu_arm(a):
             "estimators": est,
             "serving": serving,
             "vmc_c1": vmc_c1,
+            "other_systems": others,
         }
         print(json.dumps(line), flush=True)
     g.close()

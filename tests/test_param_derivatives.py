@@ -107,3 +107,44 @@ def test_backflow_curvature_refused_below_truncation_three():
         g.parameter_gradient_derivatives()
     assert e.value.code == 3
     g.close()
+
+
+def test_backflow_curvature_matches_finite_differences_at_42():
+    """The benchmark gas (21 + 21 electrons, r_s = 30) with backflow
+    determinants: each free channel parameter's d(grad ln psi)/dp and
+    d(lap ln psi)/dp against central differences of the evaluated
+    derivatives at p +- h (h = 1e-5 |p|; the Jastrow does not depend on p),
+    1e-6 relative to the largest entry."""
+    import copy
+    import alea_b200
+    from alea_b200 import setup as S
+    base = S.heg2d(21, 21, 30.0)
+    desc = S.with_backflow(base.desc)
+    pos = base.positions(31, 4)
+    g = alea_b200.Walkers(desc, capacity=4)
+    g.upload(pos)
+    dg, dl = g.parameter_gradient_derivatives()
+    g.close()
+    q = 0
+    for d, blk in enumerate(desc["backflow"]):
+        for c, ch in enumerate(blk["channels"]):
+            for slot in ch["opt_index"]:
+                h = 1e-5 * abs(ch["coeffs"][slot])
+                side = []
+                for sgn in (1.0, -1.0):
+                    e = copy.deepcopy(desc)
+                    cc = e["backflow"][d]["channels"][c]
+                    cc["coeffs"][slot] += sgn * h            # c_0 (zero slope: c_1 follows) or c_1
+                    if cc["zero_slope"]:
+                        cc["coeffs"][1] = cc["C"] * cc["coeffs"][0] / cc["L"]
+                    w = alea_b200.Walkers(e, capacity=4)
+                    w.upload(pos)
+                    o = w.download()
+                    side.append((o["grad"].T, o["lap"].T))
+                    w.close()
+                fg = (side[0][0] - side[1][0]) / (2 * h)
+                fl = (side[0][1] - side[1][1]) / (2 * h)
+                assert np.max(np.abs(dg[q] - fg)) <= 1e-6 * np.abs(fg).max(), (d, c, slot)
+                assert np.max(np.abs(dl[q] - fl)) <= 1e-6 * np.abs(fl).max(), (d, c, slot)
+                q += 1
+    assert q == 6

@@ -178,3 +178,15 @@ def test_ewald_reproduces_square_madelung_constant():
     moved[0, 3] -= 2 * 2.0
     o.init(moved)
     assert -2.0 * o.measure(0) / 4.0 == pytest.approx(M, abs=1e-12)
+
+
+def test_with_backflow_builds_the_reference_apps_backflow_gas():
+    """with_backflow on the 5 + 5 gas gives the reference App's backflow
+    description of that system (channels, truncation, zero slope, cutoff at
+    the inradius, free parameters) as recorded in the heg10bf fixture."""
+    import json
+    from alea_b200 import setup as S
+    from conftest import golden
+    d = S.with_backflow(S.heg2d(5, 5, 30.0).desc)
+    assert json.dumps(d["backflow"]) == json.dumps(golden("setup_heg10bf.json")["backflow"])
+    assert "slater" not in d
