@@ -1001,7 +1001,7 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     c->smem = static_cast<size_t>(s.s_total) * 8;
     // the one-warp sweep's layout (see DevSys)
     s.f_total = 0;
-    if (fast_sweep_eligible(s)) {
+    if (fast_sweep_eligible(s) || boson_sweep_eligible(s)) {
         const long np2 = 2L * np;
         long f = 0;
         auto ftake = [&](long n) {
@@ -1314,8 +1314,10 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
         }
     }
     c->nt = pick_threads(s);
-    if (reserve_smem(c->smem) != cudaSuccess) {
-        c->err = "cannot reserve " + std::to_string(c->smem) + " bytes of shared memory";
+    // the one-warp layouts (f_total) are launched at their own size
+    const size_t reserve = std::max(c->smem, static_cast<size_t>(s.f_total) * 8);
+    if (reserve_smem(reserve) != cudaSuccess) {
+        c->err = "cannot reserve " + std::to_string(reserve) + " bytes of shared memory";
         return bail(ALEA_ERR_UNSUPPORTED);
     }
     *out = c;
@@ -1950,10 +1952,11 @@ __global__ void run_sums_kernel(const double* records, int nw, long rec, int o_s
     }
 }
 
-// Body classes of a packed step: 0 the one-warp sweep of real determinants,
-// 1-3 the generic sweep of 32, 64, 128 threads, 4 the one-warp sweep of
-// complex determinants.  Each class is one launch on its own stream.
-constexpr int kClasses = 5;
+// Body classes of a packed step (kPackedClasses): 0 the one-warp sweep of
+// real determinants, 1-3 the generic sweep of 32, 64, 128 threads, 4 the
+// one-warp sweep of complex determinants, 5 the one-warp Jastrow-only sweep
+// of up to 256 particles.  Each class is one launch on its own stream.
+constexpr int kClasses = alea_gpu::kPackedClasses;
 
 // Launch shapes of the packed bodies: for each body class
 // the measured time per walker-sweep of shape 0 (one CTA per walker) and
@@ -2023,7 +2026,7 @@ struct alea_gpu_packed {
     cudaStream_t cls_stream[kClasses] = {};
     cudaEvent_t fork = nullptr, join[kClasses] = {};
     cudaGraphExec_t graph = nullptr;
-    int graph_shapes[kClasses] = {-1, -1, -1, -1, -1};
+    int graph_shapes[kClasses] = {-1, -1, -1, -1, -1, -1};
     cudaEvent_t ev[2 * kClasses] = {};
     std::string err;
     uint64_t launches = 0;
@@ -2123,9 +2126,9 @@ int packed_rebuild(alea_gpu_packed* P) {
     return ALEA_OK;
 }
 
-bool packed_zero_energy(const alea_gpu_packed* P) {
+bool packed_zero_energy(const alea_gpu_packed* P, int cls) {
     for (const PackedRunState& r : P->runs)
-        if (!r.done && r.cls == 0)
+        if (!r.done && r.cls == cls)
             for (int t = 0; t < r.c->sys.nterms; ++t)
                 if (r.c->sys.terms[t].kind == 2) return true;
     return false;
@@ -2138,8 +2141,9 @@ int packed_grid(alea_gpu_packed* P, int k, int shape) {
     if (shape == 0) return total;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
-    const int per_sm = (k == 0 || k == 4) ? fast_batch_ctas_per_sm(k == 4, P->smem[k])
-                                          : batch_ctas_per_sm(16 << k, P->smem[k]);
+    const int per_sm = k == 5                ? boson_batch_ctas_per_sm(P->smem[k])
+                       : (k == 0 || k == 4) ? fast_batch_ctas_per_sm(k == 4, P->smem[k])
+                                            : batch_ctas_per_sm(16 << k, P->smem[k]);
     return std::max(1, std::min(total, sms * per_sm));
 }
 
@@ -2165,8 +2169,11 @@ int packed_enqueue(alea_gpu_packed* P, const int shape[kClasses], bool timed) {
         PCUDA(P, cudaStreamWaitEvent(st, P->fork, 0));
         if (timed) PCUDA(P, cudaEventRecord(P->ev[2 * k], st));
         const BatchJob* jobs = P->d_jobs + P->job0[k];
-        if (k == 0 || k == 4)
-            PCUDA(P, launch_sweep_fast_batch(k == 0 && packed_zero_energy(P), k == 4, jobs, P->n_jobs[k],
+        if (k == 5)
+            PCUDA(P, launch_sweep_boson_batch(packed_zero_energy(P, 5), jobs, P->n_jobs[k], P->total[k],
+                                              packed_grid(P, k, shape[k]), P->smem[k], P->d_next + k, st));
+        else if (k == 0 || k == 4)
+            PCUDA(P, launch_sweep_fast_batch(k == 0 && packed_zero_energy(P, 0), k == 4, jobs, P->n_jobs[k],
                                              P->total[k], packed_grid(P, k, shape[k]), P->smem[k], P->d_next + k,
                                              st));
         else
@@ -2262,6 +2269,14 @@ void packed_destroy(alea_gpu_packed* P) {
 
 const std::string& packed_error(const alea_gpu_packed* P) { return P->err; }
 
+int packed_class(const alea_gpu_ctx* c) {
+    const char* e = std::getenv("ALEA_GPU_SWEEP");
+    const bool one_warp = e == nullptr || std::strcmp(e, "generic") != 0;
+    if (one_warp && c->nt == 32 && fast_sweep_eligible(c->sys)) return c->sys.cplx ? 4 : 0;
+    if (one_warp && boson_sweep_eligible(c->sys)) return 5;
+    return c->nt == 32 ? 1 : c->nt == 64 ? 2 : 3;
+}
+
 // A context (walkers uploaded, FP64) joins with its VMC run; its random
 // streams are set as alea_gpu_vmc_run sets them.  Returns the run's slot.
 int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& cfg, int* slot) {
@@ -2275,9 +2290,8 @@ int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& c
     r.cfg = cfg;
     r.T = std::min(std::max(cfg.n_streams, 1), c->nw);
     if (int rc = alea_gpu_set_streams(c, cfg.seed, ALEA_STREAM_VMC, r.T)) return pfail(P, rc, c->err);
-    const char* e = std::getenv("ALEA_GPU_SWEEP");
-    const bool fast = c->nt == 32 && fast_sweep_eligible(c->sys) && (e == nullptr || std::strcmp(e, "generic") != 0);
-    r.cls = fast ? (c->sys.cplx ? 4 : 0) : c->nt == 32 ? 1 : c->nt == 64 ? 2 : 3;
+    r.cls = packed_class(c);
+    const bool fast = r.cls == 0 || r.cls == 4 || r.cls == 5;
     r.smem = fast ? static_cast<size_t>(c->sys.f_total) * 8 : c->smem;
     r.chain.assign(r.T, {});
     r.blk.assign(r.T, 0.0);

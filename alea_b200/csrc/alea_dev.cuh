@@ -385,8 +385,8 @@ static __device__ __noinline__ void radial_zero_energy(double r, double ze_s, do
                                                 double ze_rc, double ze_c3, double ze_logc1,
                                                 double ze_logc2, const double* ze_cheb, double& u,
                                                 double& du, double& d2u) {
-    if (r < ze_rm) {   // ln[C1 K0(κ r^-s)]
-        const double x = ze_kappa * pow(r, -ze_s);
+    if (r < ze_rm) {   // ln[C1 K0(κ r^-s)]; s = 1/2 (1/r³ dipoles) without pow
+        const double x = ze_kappa * (ze_s == 0.5 ? 1.0 / sqrt(r) : pow(r, -ze_s));
         double k0e, k1e;
         bessel_k01e(ze_cheb, x, k0e, k1e);
         const double q = k1e / k0e;
@@ -468,6 +468,17 @@ __device__ __forceinline__ void radial_pd(const DevTerm& T, double r, double& u,
 __device__ __forceinline__ void radial(const DevTerm& T, double r, double& u, double& du,
                                        double& d2u) {
     if (T.kind == 2) {
+        if (r >= T.ze_rm) {   // the tail, inline (the Bessel form below r_m is the rare call)
+            const double rr = fmin(r, T.ze_rc);
+            const double inv_r = 1.0 / rr;
+            const double inv_c = 1.0 / (2.0 * T.ze_rc - rr);
+            const double m = (r < T.ze_rc) ? 1.0 : 0.0;
+            const double a = T.ze_c3;
+            u = m * (T.ze_logc2 - a * inv_r - a * inv_c);
+            du = m * (a * inv_r * inv_r - a * inv_c * inv_c);
+            d2u = m * (-2.0 * a * inv_r * inv_r * inv_r - 2.0 * a * inv_c * inv_c * inv_c);
+            return;
+        }
         radial_zero_energy(r, T.ze_s, T.ze_kappa, T.ze_rm, T.ze_rc, T.ze_c3, T.ze_logc1, T.ze_logc2,
                            T.ze_cheb, u, du, d2u);
         return;

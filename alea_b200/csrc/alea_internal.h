@@ -26,6 +26,11 @@ size_t footprint_bytes(const alea_gpu_system* sys, int capacity, int n_substeps)
 int packed_create(int device, alea_gpu_packed** out);
 void packed_destroy(alea_gpu_packed* P);
 const std::string& packed_error(const alea_gpu_packed* P);
+// Body classes of the packed sweeps and the class of a context's walkers
+// (0 one-warp real, 1-3 generic of 32, 64, 128 threads, 4 one-warp complex,
+// 5 one-warp Jastrow-only).
+constexpr int kPackedClasses = 6;
+int packed_class(const alea_gpu_ctx* c);
 // Join with a context whose walkers are uploaded; *slot numbers the run.
 int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& cfg, int* slot);
 int packed_active(const alea_gpu_packed* P);

@@ -1037,6 +1037,7 @@ cudaError_t reserve_smem(size_t smem) {
         if (e != cudaSuccess) return e;
     }
     cudaError_t e = reserve_smem_fast(smem);
+    if (e == cudaSuccess) e = reserve_smem_boson(smem);
     if (e == cudaSuccess) e = reserve_smem_f32(smem);
     if (e == cudaSuccess) reserved[dev] = smem;
     return e;
@@ -1076,9 +1077,20 @@ cudaError_t launch_bf_curvature(int nw, cudaStream_t st, const DevSys& s, const 
                                 int nopt, double* dgrad, double* dlap) {
     if (nw < 1 || nopt < 1 || s.nbf < 1) return cudaSuccess;
     const size_t smem = bf_curvature_smem(s);
-    const cudaError_t e = cudaFuncSetAttribute(bf_curvature_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
+    {   // raised only, so a context on another thread never sees its reservation shrink
+        static std::mutex mu;
+        static size_t reserved[64] = {};
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        std::lock_guard<std::mutex> lk(mu);
+        if (smem > reserved[dev]) {
+            const cudaError_t e = cudaFuncSetAttribute(bf_curvature_kernel<128>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(smem));
+            if (e != cudaSuccess) return e;
+            reserved[dev] = smem;
+        }
+    }
     bf_curvature_kernel<128><<<nw, 128, smem, st>>>(s, records, nw, opts, nopt, dgrad, dlap);
     return cudaGetLastError();
 }
@@ -1147,11 +1159,12 @@ cudaError_t launch_sweep(int nt, int nw, size_t smem, cudaStream_t st, const Dev
                          const SweepParams& prm, const int2* pairs, int npair) {
     if (s.f32)   // the FP32 form keeps no FP64 orbital rows: no other sweep may run on its records
         return launch_sweep_f32(nw, st, s, records, randoms, stride, prm, pairs, npair);
-    if (nt == 32 && fast_sweep_eligible(s)) {
-        const char* e = std::getenv("ALEA_GPU_SWEEP");
-        if (e == nullptr || std::strcmp(e, "generic") != 0)
-            return launch_sweep_fast(nw, smem, st, s, records, randoms, stride, prm, pairs, npair);
-    }
+    const char* e = std::getenv("ALEA_GPU_SWEEP");
+    const bool one_warp = e == nullptr || std::strcmp(e, "generic") != 0;
+    if (one_warp && nt == 32 && fast_sweep_eligible(s))
+        return launch_sweep_fast(nw, smem, st, s, records, randoms, stride, prm, pairs, npair);
+    if (one_warp && boson_sweep_eligible(s))
+        return launch_sweep_boson(nw, st, s, records, randoms, stride, prm, pairs, npair);
     ALEA_LAUNCH(nt, sweep_kernel, nw, smem, st, s, records, nw, randoms, stride, prm, pairs, npair);
     return cudaGetLastError();
 }

@@ -93,6 +93,16 @@ cudaError_t launch_sweep_generic_batch(int nt, const BatchJob* jobs, int n_jobs,
 int batch_ctas_per_sm(int nt, size_t smem);
 // Resident CTAs per SM of the packed one-warp kernel (real or complex form).
 int fast_batch_ctas_per_sm(bool complex_det, size_t smem);
+// The one-warp Jastrow-only sweep (alea_boson.cu): no determinant, no image
+// sum, group-wise pair terms, 65 to 256 particles, in the one-warp layout.
+// launch_sweep takes it for any thread count unless ALEA_GPU_SWEEP=generic.
+bool boson_sweep_eligible(const DevSys& s);
+cudaError_t reserve_smem_boson(size_t smem);
+cudaError_t launch_sweep_boson(int nw, cudaStream_t st, const DevSys& s, double* records, const double* randoms,
+                               long stride, const SweepParams& prm, const int2* pairs, int npair);
+cudaError_t launch_sweep_boson_batch(bool zero_energy, const BatchJob* jobs, int n_jobs, int total, int grid,
+                                     size_t smem, int* next, cudaStream_t st);
+int boson_batch_ctas_per_sm(size_t smem);
 // The walker of global index w of a packed launch: its job by binary search
 // over the jobs' first indices.
 __device__ __forceinline__ int batch_job_of(const BatchJob* jobs, int n_jobs, int w) {

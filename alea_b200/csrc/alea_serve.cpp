@@ -2,11 +2,14 @@
 // walker contexts.  No reference counterpart: the reference runs one input
 // per process.
 //
-// A packed server (alea_gpu_server_create_packed) steps every admitted VMC
-// job together: one scheduler thread admits queued VMC jobs between steps
-// as memory frees up, gives each its context and runs all of them through
-// the packed engine (alea_capi.cu, "packed VMC runs"), one sweep launch per
-// step for all jobs' walkers; DMC jobs still take worker contexts.
+// A packed server (alea_gpu_server_create_packed) steps the admitted VMC
+// jobs together by sweep body: preparer threads admit queued VMC jobs as
+// memory frees up and build each one's context (system tables, walkers,
+// first evaluation), and one packing thread per body class runs its jobs
+// through its own packed engine (alea_capi.cu, "packed VMC runs"), one sweep
+// launch per step for all of that class's walkers.  The classes step
+// independently, so a class of cheap sweeps is not held to the pace of a
+// class of expensive ones; DMC jobs still take worker contexts.
 //
 // Each admitted job gets its own alea_gpu_ctx (own CUDA stream, own device
 // records, own random streams keyed by the job's seed) on one of max_running
@@ -77,6 +80,10 @@ struct alea_gpu_server {
     bool stop = false;
     std::vector<std::thread> workers;
     std::string err;
+    // packed: contexts built by the preparers, by body class, for the packers
+    std::deque<std::pair<Job*, alea_gpu_ctx*>> ready[alea_gpu::kPackedClasses];
+    int preparing = 0;
+    std::condition_variable cv_ready;
 
     // First queued job that fits the budget left (caller holds mu); a packed
     // server's workers take DMC jobs only, its scheduler VMC jobs only.
@@ -96,37 +103,63 @@ struct alea_gpu_server {
         j->t_admit = Clock::now();
     }
 
-    // The packing scheduler: admitted VMC jobs step together.
-    void packer() {
+    // A preparer: admits a queued VMC job, builds its context and hands it to
+    // the packer of its body class.
+    void preparer() {
+        cudaSetDevice(device);
+        for (;;) {
+            Job* j = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stop || admissible(true) != nullptr; });
+                if (stop) return;
+                j = admissible(true);
+                admit(j);
+                ++preparing;
+            }
+            alea_gpu_ctx* ctx = nullptr;
+            int rc = j->cancel.load() ? ALEA_ERR_CANCELLED : ALEA_OK;
+            if (rc == ALEA_OK) rc = alea_gpu_create(j->spec.system, device, j->capacity, &ctx);
+            if (rc == ALEA_OK) rc = alea_gpu_upload_walkers(ctx, soa_of(j->spec).data(), j->spec.n_walkers);
+            if (rc != ALEA_OK && ctx) {
+                alea_gpu_destroy(ctx);
+                ctx = nullptr;
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (rc == ALEA_OK) ready[alea_gpu::packed_class(ctx)].emplace_back(j, ctx);
+                --preparing;
+            }
+            if (rc != ALEA_OK) finish(j, rc, nullptr);
+            cv_ready.notify_all();
+        }
+    }
+
+    // The packer of body class `cls`: its prepared jobs step together.
+    void packer(int cls) {
         cudaSetDevice(device);
         alea_gpu_packed* P = nullptr;
         const int prc = alea_gpu::packed_create(device, &P);
         std::vector<std::pair<Job*, alea_gpu_ctx*>> slots;   // in the engine's run order
         for (;;) {
-            std::vector<Job*> fresh;
+            std::vector<std::pair<Job*, alea_gpu_ctx*>> fresh;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                if (slots.empty())
-                    cv_work.wait(lk, [&] { return stop || admissible(true) != nullptr; });
-                if (stop && slots.empty()) break;
-                if (!stop)
-                    while (Job* j = admissible(true)) {
-                        admit(j);
-                        fresh.push_back(j);
-                    }
+                const auto drained = [&] { return stop && preparing == 0 && ready[cls].empty(); };
+                if (slots.empty()) cv_ready.wait(lk, [&] { return drained() || !ready[cls].empty(); });
+                if (slots.empty() && drained()) break;
+                for (; !ready[cls].empty(); ready[cls].pop_front()) fresh.push_back(ready[cls].front());
             }
-            for (Job* j : fresh) {
-                alea_gpu_ctx* ctx = nullptr;
+            for (auto& jc : fresh) {
+                Job* j = jc.first;
                 int rc = prc != ALEA_OK ? prc : j->cancel.load() ? ALEA_ERR_CANCELLED : ALEA_OK;
-                if (rc == ALEA_OK) rc = alea_gpu_create(j->spec.system, device, j->capacity, &ctx);
-                if (rc == ALEA_OK) rc = alea_gpu_upload_walkers(ctx, soa_of(j->spec).data(), j->spec.n_walkers);
-                if (rc == ALEA_OK) rc = alea_gpu::packed_add(P, ctx, j->spec.run, nullptr);
+                if (rc == ALEA_OK) rc = alea_gpu::packed_add(P, jc.second, j->spec.run, nullptr);
                 if (rc != ALEA_OK) {
-                    if (ctx) alea_gpu_destroy(ctx);
+                    alea_gpu_destroy(jc.second);
                     finish(j, rc, nullptr);
                     continue;
                 }
-                slots.emplace_back(j, ctx);
+                slots.push_back(jc);
             }
             if (slots.empty()) continue;
             for (size_t i = 0; i < slots.size(); ++i)
@@ -227,7 +260,10 @@ static int server_create(int device, size_t hbm_budget_bytes, int max_running, b
     s->max_running = max_running;
     s->packed = packed;
     for (int i = 0; i < max_running; ++i) s->workers.emplace_back([s] { s->worker(); });
-    if (packed) s->workers.emplace_back([s] { s->packer(); });
+    if (packed) {
+        for (int i = 0; i < 2; ++i) s->workers.emplace_back([s] { s->preparer(); });
+        for (int k = 0; k < alea_gpu::kPackedClasses; ++k) s->workers.emplace_back([s, k] { s->packer(k); });
+    }
     *out = s;
     return ALEA_OK;
 }
@@ -304,6 +340,7 @@ int alea_gpu_server_destroy(alea_gpu_server* s) {
         for (uint64_t id : s->queue) queued.push_back(s->jobs[id].get());
         s->queue.clear();
         s->cv_work.notify_all();
+        s->cv_ready.notify_all();
     }
     for (Job* j : queued) s->finish(j, ALEA_ERR_CANCELLED, nullptr);
     for (std::thread& t : s->workers) t.join();

@@ -62,8 +62,10 @@ def parse():
     ap.add_argument("--walkers", type=int, default=16384)
     ap.add_argument("--pre", type=int, default=20, help="untimed VMC pre-equilibration steps")
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--cpu-walkers", type=int, default=1024,
+    ap.add_argument("--cpu-walkers", type=int, default=4096,
                     help="walker sample of the host-CPU baseline")
+    ap.add_argument("--cpu-steps", type=int, default=40,
+                    help="timed DMC steps of the host-CPU baseline (about 10 s of the reference's work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--no-estimators", action="store_true",
@@ -573,7 +575,7 @@ def gpu_arm(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
-            v, info = run_reference_cpu(min(nw, a.cpu_walkers), 3, 1, a.seed)
+            v, info = run_reference_cpu(min(nw, a.cpu_walkers), a.cpu_steps, 1, a.seed)
             cpu = dict(value=v, unit=UNIT, **info)
         except Exception as exc:   # reported, never substituted for the GPU number
             cpu = {"value": None, "unit": UNIT, "error": str(exc)[:200]}

@@ -737,11 +737,14 @@ typedef struct {
  * max_running >= 1 worker contexts. */
 int alea_gpu_server_create(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out);
 /* The same server with its VMC jobs packed (no counterpart in the reference):
- * one scheduler thread admits queued VMC jobs between steps as the budget
- * frees up and steps every admitted VMC job together, all their walkers in
- * one sweep launch per step (alea_gpu_vmc_run_packed); a job's result equals
- * its alea_gpu_vmc_run on its own context whatever else runs.  DMC jobs take
- * the max_running worker contexts as in alea_gpu_server_create. */
+ * two preparer threads admit queued VMC jobs as the budget frees up and
+ * build their contexts; one packing thread per sweep body (one-warp real or
+ * complex, generic of 32, 64 or 128 threads) steps its admitted jobs
+ * together, all their walkers in one sweep launch per step
+ * (alea_gpu_vmc_run_packed), independently of the other bodies; a job's
+ * result equals its alea_gpu_vmc_run on its own context whatever else runs.
+ * DMC jobs take the max_running worker contexts as in
+ * alea_gpu_server_create. */
 int alea_gpu_server_create_packed(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out);
 /* Queue a job; never blocks on the device.  ALEA_ERR_NOMEM when the job
  * alone exceeds the budget. */

@@ -234,23 +234,35 @@ def _twisted42(nw):
     return st.desc, st.positions(4242, nw)
 
 
+def _dipoles256(nw):
+    """256 dipolar bosons of the serving mix (Jastrow-only, one-warp body
+    for 65 to 256 particles)."""
+    from alea_b200 import setup as S
+    st = S.dipoles2d(256, 0.0353, 1.0, 3.0, 0.0459)
+    return st.desc, st.positions(4242, nw)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["heg42", "crystal16", "dipoles16", "heg10t", "heg42t"])
+@pytest.mark.parametrize("name", ["heg42", "crystal16", "dipoles16", "heg10t", "heg42t", "dipoles256"])
 def test_one_warp_sweep_matches_generic_sweep(name, monkeypatch):
-    """The one-warp sweep (taken by 32-thread walkers of at most 64
-    particles, real or complex determinants) and the generic CTA sweep
+    """The one-warp sweeps (taken by 32-thread walkers of at most 64
+    particles, real or complex determinants, and by Jastrow-only systems of
+    65 to 256 particles) and the generic CTA sweep
     (ALEA_GPU_SWEEP=generic) on the same walkers and random streams: VMC
     positions bit for bit; after drift VMC and DMC advances, positions to
     1e-9 and E_L, Im E_L, weights, ln ψ to 1e-10."""
     import alea_b200
     if name == "heg42t":
         setup, pos = _twisted42(64)
+    elif name == "dipoles256":
+        setup, pos = _dipoles256(32)
     else:
         setup = golden(f"setup_{name}.json")
         pos = np.array(golden(f"eval_{name}.json")["positions"])
     nw = pos.shape[0]
-    tau = {"heg42": 225.0, "crystal16": 400.0, "dipoles16": 0.0003, "heg10t": 225.0, "heg42t": 225.0}[name]
-    dtau = {"heg42": 0.5, "crystal16": 1.0, "dipoles16": 1e-5, "heg10t": 0.5, "heg42t": 0.5}[name]
+    tau = {"heg42": 225.0, "crystal16": 400.0, "dipoles16": 0.0003, "heg10t": 225.0, "heg42t": 225.0,
+           "dipoles256": 0.0003}[name]
+    dtau = {"heg42": 0.5, "crystal16": 1.0, "dipoles16": 1e-5, "heg10t": 0.5, "heg42t": 0.5, "dipoles256": 1e-5}[name]
     out = []
     for mode in ("generic", "fast"):
         if mode == "generic":

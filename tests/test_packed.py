@@ -85,3 +85,34 @@ def test_packed_runs_of_uneven_length():
             _same(res, want)
         for g in gs:
             g.close()
+
+
+def test_packed_jastrow_only_body_with_the_others():
+    """The one-warp Jastrow-only body (256 dipolar bosons) packed beside the
+    real and complex one-warp bodies: each run equals its own vmc_run."""
+    import alea_b200
+    from alea_b200 import setup as S
+    dip = S.dipoles2d(256, 0.0353, 1.0, 3.0, 0.0459)
+    dpos = dip.positions(71, 24)
+
+    def dipoles():
+        g = alea_b200.Walkers(dip.desc, capacity=len(dpos))
+        g.upload(dpos)
+        return g
+
+    makers = [dipoles, lambda: _walkers("heg10", MIX[0][1]), lambda: _walkers("heg10t", MIX[3][1])]
+    runs = [dict(n_eq=1, n_acc=2, n_steps=1, n_substeps=1, tau=0.0003, streams=3, seed=500), _run(0), _run(3)]
+    alone = []
+    for make, r in zip(makers, runs):
+        g = make()
+        res, _ = g.vmc_run(r["n_eq"], r["n_acc"], r["n_steps"], r["n_substeps"], r["tau"], r["streams"], r["seed"])
+        alone.append(res)
+        g.close()
+    gs = [make() for make in makers]
+    packed = alea_b200.vmc_run_packed(gs, runs)
+    for (res, status), want in zip(packed, alone):
+        assert status == 0
+        _same(res, want)
+    for g in gs:
+        g.close()
+    dip.close()
