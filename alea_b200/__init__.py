@@ -178,6 +178,9 @@ def pack_system(desc: Dict[str, Any]):
         E.kset.kx = _dp(f64(ew["kx"]))
         E.kset.ky = _dp(f64(ew["ky"]))
         E.kset.weight = _dp(f64(ew["weight"]))
+        if "kz" in ew:   # a 3-D cell
+            E.kset.n3 = _ip(i32(ew["n3"]))
+            E.kset.kz = _dp(f64(ew["kz"]))
     cl = desc.get("coulomb", [])
     s.n_coulomb = len(cl)
     for i, c in enumerate(cl):

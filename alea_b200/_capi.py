@@ -32,7 +32,7 @@ class Spline(ctypes.Structure):
 
 class KSet(ctypes.Structure):
     _fields_ = [("n_k", ctypes.c_int), ("n1", c_ip), ("n2", c_ip), ("kx", c_dp),
-                ("ky", c_dp), ("weight", c_dp)]
+                ("ky", c_dp), ("weight", c_dp), ("n3", c_ip), ("kz", c_dp)]
 
 
 class Group(ctypes.Structure):
@@ -178,7 +178,7 @@ EXPORTS = [
     "alea_gpu_launch_count", "alea_gpu_vmc_step_noalloc", "alea_gpu_download_phase",
     "alea_gpu_setup_heg2d", "alea_gpu_setup_heg2d_twisted", "alea_gpu_setup_crystal2d",
     "alea_gpu_setup_exciton2d",
-    "alea_gpu_setup_charges2d", "alea_gpu_setup_dipoles2d", "alea_gpu_setup_ewald3d",
+    "alea_gpu_setup_charges2d", "alea_gpu_setup_dipoles2d", "alea_gpu_setup_ewald3d", "alea_gpu_setup_heg3d",
     "alea_gpu_setup_system", "alea_gpu_setup_json", "alea_gpu_setup_positions",
     "alea_gpu_setup_free",
     "alea_gpu_set_precision",
@@ -245,6 +245,7 @@ def load() -> ctypes.CDLL:
         "alea_gpu_setup_charges2d": ([c_dp, I, c_ip, c_dp, D, ctypes.POINTER(P), ctypes.c_char_p,
                                       ctypes.c_size_t], I),
         "alea_gpu_setup_ewald3d": ([c_dp, D, ctypes.POINTER(P), ctypes.c_char_p, ctypes.c_size_t], I),
+        "alea_gpu_setup_heg3d": ([I, I, D, D, D, D, D, D, ctypes.POINTER(P), ctypes.c_char_p, ctypes.c_size_t], I),
         "alea_gpu_setup_system": ([P], ctypes.POINTER(System)),
         "alea_gpu_setup_json": ([P], ctypes.c_char_p),
         "alea_gpu_setup_positions": ([P, ctypes.c_uint64, I, c_dp], I),

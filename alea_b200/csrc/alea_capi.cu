@@ -523,11 +523,14 @@ struct Arena {
     }
 };
 
+int build_system3(alea_gpu_ctx* c, const alea_gpu_system* in);
+
 int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     DevSys& s = c->sys;
     s = DevSys{};
     if (!in) return fail(c, ALEA_ERR_INVALID, "null system");
-    if (in->dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "the walker kernels implement dim = 2");
+    if (in->dim == 3) return build_system3(c, in);
+    if (in->dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "the walker kernels implement dim = 2 and dim = 3");
     const int np = in->n_particles;
     if (np < 1 || np > 1024) return fail(c, ALEA_ERR_INVALID, "n_particles must be in [1, 1024]");
     s.dim = 2;
@@ -1071,6 +1074,273 @@ int build_system(alea_gpu_ctx* c, const alea_gpu_system* in) {
     return ALEA_OK;
 }
 
+// Three-dimensional systems, run by the walker kernels of alea_bf3d.cu: a
+// periodic cell whose lattice rows lie along the axes (the orthorhombic fold)
+// or an open one; backflow determinants, or plain determinants taken as
+// backflow determinants without channels (plane waves or Gaussians, at most
+// two); Drummond or minimum-image Padé pair terms; the 3-D Ewald sum (a k
+// set with kz) and open Coulomb terms.  Every walker's state is hot.
+int build_system3(alea_gpu_ctx* c, const alea_gpu_system* in) {
+    DevSys& s = c->sys;
+    const int np = in->n_particles;
+    if (np < 1 || np > 256) return fail(c, ALEA_ERR_INVALID, "a three-dimensional system has 1..256 particles");
+    s.dim = 3;
+    s.np = np;
+    s.periodic = in->periodic;
+    s.ortho = 1;
+    if (s.periodic) {
+        for (int i = 0; i < 3; ++i)
+            for (int d = 0; d < 3; ++d)
+                if (i != d && in->lattice[i * 3 + d] != 0.0)
+                    return fail(c, ALEA_ERR_UNSUPPORTED,
+                                "three-dimensional cells must be orthorhombic with rows along the axes");
+        for (int d = 0; d < 3; ++d) {
+            s.box[d] = std::abs(in->lattice[d * 3 + d]);
+            if (!(s.box[d] > 0.0) || !std::isfinite(s.box[d]))
+                return fail(c, ALEA_ERR_INVALID, "lattice vectors are singular");
+            s.inv_box[d] = 1.0 / s.box[d];
+        }
+    }
+    Arena ar;
+    struct Patch { size_t off; const void** slot; };
+    std::vector<Patch> patches;
+    auto put = [&](const void* p, size_t n, const void** slot) { patches.push_back({ar.add(p, n), slot}); };
+    if (in->n_groups < 1 || in->n_groups > kMaxGroups) return fail(c, ALEA_ERR_INVALID, "bad n_groups");
+    s.ngroups = in->n_groups;
+    std::vector<double> inv_mass(np * 3, 0.0), charge(np, 0.0);
+    std::vector<int> group_of(np, -1);
+    for (int g = 0; g < in->n_groups; ++g) {
+        const alea_gpu_group& G = in->groups[g];
+        if (G.first < 0 || G.last > np || G.first >= G.last)
+            return fail(c, ALEA_ERR_INVALID, "group range out of bounds");
+        s.gfirst[g] = G.first;
+        s.glast[g] = G.last;
+        s.gcharge[g] = G.charge;
+        for (int i = G.first; i < G.last; ++i) {
+            if (group_of[i] >= 0) return fail(c, ALEA_ERR_INVALID, "groups overlap");
+            group_of[i] = g;
+            charge[i] = G.charge;
+            for (int d = 0; d < 3; ++d) inv_mass[i * 3 + d] = G.inv_mass[d];
+        }
+    }
+    for (int i = 0; i < np; ++i)
+        if (group_of[i] < 0) return fail(c, ALEA_ERR_INVALID, "a particle belongs to no group");
+    c->h_inv_mass = inv_mass;
+    put(inv_mass.data(), inv_mass.size() * 8, reinterpret_cast<const void**>(&s.inv_mass));
+    put(charge.data(), charge.size() * 8, reinterpret_cast<const void**>(&s.charge));
+    put(group_of.data(), group_of.size() * 4, reinterpret_cast<const void**>(&s.group_of));
+    long o = 0;
+    s.o_pos = o; o += np * 3;
+    s.o_jg = o; o += np * 3;
+    s.o_jl = o; o += np * 3;
+    s.o_kg = o; o += np * 3;
+    s.o_kl = o; o += np * 3;
+    s.o_sg = o; o += np * 3;
+    s.o_sl = o; o += np * 3;
+    s.o_scal = o; o += S_NSCAL;
+    s.cplx = 0;
+    s.o_pg = s.o_pl = static_cast<int>(o);
+    s.nblocks = 0;
+    if (in->n_blocks > 0 && in->n_backflow > 0)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "backflow determinants cannot be mixed with plain blocks");
+    const int ndet = in->n_backflow > 0 ? in->n_backflow : in->n_blocks;
+    if (ndet < 0 || ndet > 2) return fail(c, ALEA_ERR_UNSUPPORTED, "a three-dimensional system has at most two determinants");
+    s.nbf = ndet;
+    s.maxN = 1;
+    std::vector<double> sin_flags[2];
+    for (int d = 0; d < ndet; ++d) {
+        DevBF& D = s.bf[d];
+        const bool bf = in->n_backflow > 0;
+        const alea_gpu_backflow* F = bf ? &in->backflow[d] : nullptr;
+        const alea_gpu_orbitals* B = bf ? nullptr : &in->blocks[d];
+        D.first = bf ? F->first : B->first;
+        D.last = bf ? F->last : B->last;
+        D.n = D.last - D.first;
+        D.type = bf ? F->type : B->type;
+        if (D.n < 1 || D.n > 32 || D.first < 0 || D.last > np)
+            return fail(c, ALEA_ERR_UNSUPPORTED, "three-dimensional determinants must have 1..32 rows");
+        s.maxN = std::max(s.maxN, D.n);
+        const double* k = bf ? F->k : B->k;
+        const int* is_sin = bf ? F->is_sin : B->is_sin;
+        const double* centers = bf ? F->centers : B->centers;
+        const double* alphas = bf ? F->alphas : B->alphas;
+        if (D.type == ALEA_ORB_PLANE_WAVE) {
+            if (!k || !is_sin) return fail(c, ALEA_ERR_INVALID, "plane-wave determinant without tables");
+            put(k, D.n * 3 * 8, reinterpret_cast<const void**>(&D.k));
+            sin_flags[d].resize(D.n);
+            for (int i = 0; i < D.n; ++i) sin_flags[d][i] = is_sin[i] ? 1.0 : 0.0;
+            put(sin_flags[d].data(), D.n * 8, reinterpret_cast<const void**>(&D.is_sin));
+        } else if (D.type == ALEA_ORB_GAUSSIAN) {
+            if (!centers || !alphas) return fail(c, ALEA_ERR_INVALID, "Gaussian determinant without tables");
+            put(centers, D.n * 3 * 8, reinterpret_cast<const void**>(&D.centers));
+            put(alphas, D.n * 8, reinterpret_cast<const void**>(&D.alphas));
+        } else {
+            return fail(c, ALEA_ERR_UNSUPPORTED, "three-dimensional orbitals must be plane waves or Gaussians");
+        }
+        D.nch = 0;
+        if (bf) {
+            if (F->n_channels < 1 || F->n_channels > 4) return fail(c, ALEA_ERR_INVALID, "bad backflow channels");
+            D.nch = F->n_channels;
+            for (int q = 0; q < D.nch; ++q) {
+                const alea_gpu_backflow_channel& C = F->channels[q];
+                DevBFCh& E = D.ch[q];
+                if (C.source_first < 0 || C.source_last > np || C.source_first >= C.source_last || C.C < 2 ||
+                    !(C.L > 0.0) || C.n_coeffs < 1 || C.n_coeffs > 16)
+                    return fail(c, ALEA_ERR_INVALID, "bad backflow channel");
+                if (s.periodic && C.L > 0.5 * std::min({s.box[0], s.box[1], s.box[2]}))
+                    return fail(c, ALEA_ERR_INVALID, "a backflow cutoff exceeds half the cell");
+                E.sf = C.source_first;
+                E.sl = C.source_last;
+                E.C = C.C;
+                E.L = C.L;
+                E.nc = C.n_coeffs;
+                for (int q2 = 0; q2 < E.nc; ++q2) E.c[q2] = C.coeffs[q2];
+            }
+        }
+        D.oX = static_cast<int>(o); o += round4(3 * D.n);
+        D.oA = static_cast<int>(o); o += round4(D.n * D.n);
+        D.oF = static_cast<int>(o); o += round4(3 * D.n);
+        D.oLS = static_cast<int>(o); o += 4;
+    }
+    if (in->n_terms < 0 || in->n_terms > kMaxTerms) return fail(c, ALEA_ERR_INVALID, "bad n_terms");
+    s.nterms = in->n_terms;
+    for (int t = 0; t < in->n_terms; ++t) {
+        const alea_gpu_pair_term& T = in->terms[t];
+        DevTerm& D = s.terms[t];
+        D.kind = T.kind;
+        D.npairs = T.n_pairs;
+        if (T.n_pairs < 1 || T.n_pairs > ALEA_GPU_MAX_PAIRS) return fail(c, ALEA_ERR_INVALID, "bad n_pairs");
+        for (int q = 0; q < T.n_pairs; ++q)
+            for (int k = 0; k < 4; ++k) {
+                D.pairs[q][k] = T.pairs[q][k];
+                if (T.pairs[q][k] < 0 || T.pairs[q][k] > np)
+                    return fail(c, ALEA_ERR_INVALID, "pair range out of bounds");
+            }
+        D.same0 = T.pairs[0][0] == T.pairs[0][2] && T.pairs[0][1] == T.pairs[0][3];
+        if (T.kind == ALEA_PAIR_PADE) {
+            if (T.image_sum) return fail(c, ALEA_ERR_UNSUPPORTED, "three-dimensional Padé terms are minimum-image only");
+            if (T.num_order + T.den_order > 16 || T.num_order < 0 || T.den_order < 0)
+                return fail(c, ALEA_ERR_INVALID, "Padé order too large");
+            D.nnum = T.num_order;
+            D.nden = T.den_order;
+            for (int k = 0; k < D.nnum + D.nden; ++k) D.coef[k] = T.coeffs[k];
+            D.image = 0;
+        } else if (T.kind == ALEA_PAIR_DRUMMOND) {
+            if (T.C < 2 || T.n_coeffs < 1 || T.n_coeffs > 16) return fail(c, ALEA_ERR_INVALID, "bad Drummond term");
+            D.C = T.C;
+            D.gamma = T.gamma;
+            D.L = T.L;
+            D.ncoef = T.n_coeffs;
+            for (int k = 0; k < T.n_coeffs; ++k) D.dc[k] = T.dcoeffs[k];
+            double ipw = 1.0;
+            for (int i = 0; i < T.C; ++i) ipw *= -T.L;
+            D.alpha1 = T.gamma / ipw + D.dc[0] * static_cast<double>(T.C) / T.L;
+        } else {
+            return fail(c, ALEA_ERR_UNSUPPORTED, "three-dimensional pair terms are Padé or Drummond");
+        }
+    }
+    c->h_opt.clear();
+    s.pair_by_group = 0;
+    s.nkJ = 0;
+    s.o_rho = static_cast<int>(o);
+    s.hot = static_cast<int>(round4(o));
+    s.rec = s.hot;
+    std::vector<std::vector<double>> poly_tables;
+    std::vector<double> ek3;
+    s.ewald = in->ewald.enabled;
+    if (s.ewald) {
+        const alea_gpu_ewald& E = in->ewald;
+        const alea_gpu_kset& K = E.kset;
+        if (!s.periodic) return fail(c, ALEA_ERR_INVALID, "Ewald in an open cell");
+        if (!E.long_range.scaled || E.long_range.n_knots < 2 || K.n_k < 0 ||
+            (K.n_k > 0 && (!K.kx || !K.ky || !K.kz || !K.weight)))
+            return fail(c, ALEA_ERR_INVALID, "bad 3-D Ewald tables (the k set needs kz)");
+        s.esp.r_cut = E.long_range.r_cut;
+        s.esp.inv_delta = E.long_range.inv_delta;
+        s.esp.n_knots = E.long_range.n_knots;
+        put(E.long_range.scaled, 3 * E.long_range.n_knots * 8, reinterpret_cast<const void**>(&s.esp.scaled));
+        poly_tables.push_back(hermite_to_monomial(E.long_range.scaled, E.long_range.n_knots));
+        put(poly_tables.back().data(), poly_tables.back().size() * 8, reinterpret_cast<const void**>(&s.esp.poly));
+        s.e_rcut = E.r_cut;
+        s.e_inv_eps = E.inv_eps;
+        s.e_const = E.constant;
+        s.enk = K.n_k;
+        for (int k = 0; k < K.n_k; ++k) {
+            ek3.push_back(K.kx[k]);
+            ek3.push_back(K.ky[k]);
+            ek3.push_back(K.kz[k]);
+        }
+        if (s.enk > 0) {
+            put(ek3.data(), ek3.size() * 8, reinterpret_cast<const void**>(&s.ek3));
+            put(K.weight, 8 * s.enk, reinterpret_cast<const void**>(&s.ew));
+        }
+    }
+    if (in->n_coulomb < 0 || in->n_coulomb > kMaxCoulomb) return fail(c, ALEA_ERR_INVALID, "bad n_coulomb");
+    s.ncoul = in->n_coulomb;
+    for (int k = 0; k < s.ncoul; ++k) {
+        const alea_gpu_coulomb& C = in->coulomb[k];
+        s.coul[k][0] = C.a_first;
+        s.coul[k][1] = C.a_last;
+        s.coul[k][2] = C.b_first;
+        s.coul[k][3] = C.b_last;
+        s.coul_coef[k] = C.coef;
+    }
+    if (in->n_inverse_power != 0)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "three-dimensional systems take no inverse-power terms");
+    s.nip = 0;
+    s.ip_tail = 0.0;
+    const Ziggurat z = make_ziggurat();
+    put(z.k, sizeof z.k, reinterpret_cast<const void**>(&s.zk));
+    put(z.w, sizeof z.w, reinterpret_cast<const void**>(&s.zw));
+    put(z.f, sizeof z.f, reinterpret_cast<const void**>(&s.zf));
+    s.zr = z.r;
+    // shared memory after the hot part (alea_bf3d.cu's view3)
+    long m = s.hot;
+    auto take = [&](long n) {
+        const long at = m;
+        m += round4(std::max(n, 1L));
+        return static_cast<int>(at);
+    };
+    s.t_newpos = take(4);
+    s.t_misc = take(32);
+    s.t_red = take(96);
+    s.t_col = take(s.maxN);
+    s.t_work = static_cast<int>(m);
+    for (int d = 0; d < s.nbf; ++d) {
+        DevBF& D = s.bf[d];
+        D.pX = take(3 * D.n);
+        D.pA = take(D.n * D.n);
+        D.pF = take(3 * D.n);
+        D.pM = take(8);
+    }
+    s.t_mwork = static_cast<int>(m);
+    const long N = s.maxN;
+    // the move's work per determinant: ∇φ rows (3N²), multipliers and row exchanges (2N)
+    const long total = std::max(s.t_mwork + s.nbf * round4(3 * N * N + 2 * N), s.t_work + round4(8 * N * N + 18 * N));
+    s.t_total = static_cast<int>(total);
+    s.f_total = 0;
+    c->smem = static_cast<size_t>(total) * 8;
+    if (c->smem > 227 * 1024)
+        return fail(c, ALEA_ERR_UNSUPPORTED,
+                    "walker state needs " + std::to_string(c->smem) + " bytes of shared memory (> 227 KB)");
+    {
+        uint64_t h = 1469598103934665603ULL;
+        auto mix = [&h](const void* p, size_t n) {
+            const unsigned char* b = static_cast<const unsigned char*>(p);
+            for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ULL;
+        };
+        mix(&s, sizeof s);
+        mix(ar.bytes.data(), ar.bytes.size());
+        c->fingerprint = h;
+    }
+    CUDA_TRY(c, cudaMallocAsync(&c->arena, std::max<size_t>(ar.bytes.size(), 256), c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->arena, ar.bytes.data(), ar.bytes.size(), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (const Patch& p : patches) *p.slot = static_cast<char*>(c->arena) + p.off;
+    c->orbital_opts = 0;
+    return ALEA_OK;
+}
+
 int ensure_streams(alea_gpu_ctx* c, int n) {
     if (n > c->streams_cap) {
         if (c->streams) cudaFreeAsync(c->streams, c->stream);
@@ -1085,7 +1355,7 @@ int ensure_randoms(alea_gpu_ctx* c, int sweeps) {
     if (sweeps > c->rnd_sweeps) {
         if (c->randoms) cudaFreeAsync(c->randoms, c->stream);
         c->randoms = nullptr;
-        const size_t n = static_cast<size_t>(sweeps) * c->sys.np * 3 * c->capacity;
+        const size_t n = static_cast<size_t>(sweeps) * c->sys.np * (c->sys.dim + 1) * c->capacity;
         CUDA_TRY(c, cudaMallocAsync(&c->randoms, n * 8, c->stream));
         c->rnd_sweeps = sweeps;
     }
@@ -1151,7 +1421,10 @@ int check_errors(alea_gpu_ctx* c) {
 int launch_evaluate(alea_gpu_ctx* c) {
     if (c->nw == 0) return ALEA_OK;
     ++c->launches;
-    CUDA_TRY(c, launch_evaluate(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
+    if (c->sys.dim == 3)
+        CUDA_TRY(c, launch_evaluate3(c->nw, c->smem, c->stream, c->sys, records(c)));
+    else
+        CUDA_TRY(c, launch_evaluate(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_errors(c);
 }
@@ -1169,7 +1442,7 @@ int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, doubl
     ++c->launches;
     draw_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, stride,
                                                          n_sub, c->sys.zk, c->sys.zw, c->sys.zf, c->sys.zr,
-                                                         c->randoms, 0);
+                                                         c->randoms, c->sys.dim);
     CUDA_TRY(c, cudaGetLastError());
     SweepParams prm{};
     prm.mode = mode;
@@ -1183,8 +1456,11 @@ int run_sweep(alea_gpu_ctx* c, int mode, int n_sub, double tau, int drift, doubl
     prm.e_max = e_max;
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
     ++c->launches;
-    CUDA_TRY(c, launch_sweep(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->randoms, stride, prm,
-                             c->pairs, c->npair));
+    if (c->sys.dim == 3)
+        CUDA_TRY(c, launch_sweep3(c->nw, c->smem, c->stream, c->sys, records(c), c->randoms, stride, prm));
+    else
+        CUDA_TRY(c, launch_sweep(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->randoms, stride, prm,
+                                 c->pairs, c->npair));
     CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     float ms = 0.f;
@@ -1289,8 +1565,8 @@ int alea_gpu_create(const alea_gpu_system* sys, int device, int capacity, alea_g
     const size_t recb = static_cast<size_t>(s.rec) * 8 * capacity;
     cudaStream_t st = c->stream;
     if (cudaMallocAsync(&c->rec[0], recb, st) != cudaSuccess || cudaMallocAsync(&c->rec[1], recb, st) != cudaSuccess ||
-        cudaMallocAsync(&c->d_buf, static_cast<size_t>(std::max(s.np * 2, 8)) * 8 * capacity, st) != cudaSuccess ||
-        cudaMallocAsync(&c->d_sigma, static_cast<size_t>(s.np) * 2 * 8, st) != cudaSuccess ||
+        cudaMallocAsync(&c->d_buf, static_cast<size_t>(std::max(s.np * s.dim, 8)) * 8 * capacity, st) != cudaSuccess ||
+        cudaMallocAsync(&c->d_sigma, static_cast<size_t>(s.np) * s.dim * 8, st) != cudaSuccess ||
         cudaMallocAsync(&c->d_src, sizeof(int) * static_cast<size_t>(capacity), st) != cudaSuccess ||
         cudaMallocAsync(&c->d_mask, static_cast<size_t>(capacity), st) != cudaSuccess ||
         (c->h_stage = static_cast<double*>(pinned_acquire(64 * static_cast<size_t>(capacity)))) == nullptr ||
@@ -1359,7 +1635,7 @@ int alea_gpu_upload_walkers(alea_gpu_ctx* c, const double* positions, int nw) {
     if (!c) return ALEA_ERR_INVALID;
     if (nw < 1 || nw > c->capacity) return fail(c, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
     if (!positions) return fail(c, ALEA_ERR_INVALID, "null positions");
-    for (long i = 0, n = static_cast<long>(c->sys.np) * 2 * nw; i < n; ++i)
+    for (long i = 0, n = static_cast<long>(c->sys.np) * c->sys.dim * nw; i < n; ++i)
         if (!std::isfinite(positions[i]))
             return fail(c, ALEA_ERR_INVALID, "walker positions must be finite (entry " + std::to_string(i) + ")");
     cudaSetDevice(c->device);
@@ -1367,11 +1643,11 @@ int alea_gpu_upload_walkers(alea_gpu_ctx* c, const double* positions, int nw) {
     c->nw = nw;
     const DevSys& s = c->sys;
     CUDA_TRY(c, cudaMemsetAsync(records(c), 0, static_cast<size_t>(s.rec) * 8 * nw, c->stream));
-    CUDA_TRY(c, copy_in(c, c->d_buf, positions, static_cast<size_t>(s.np) * 2 * nw * 8));
-    const long n = static_cast<long>(s.np) * 2 * nw;
+    CUDA_TRY(c, copy_in(c, c->d_buf, positions, static_cast<size_t>(s.np) * s.dim * nw * 8));
+    const long n = static_cast<long>(s.np) * s.dim * nw;
     ++c->launches;
     from_soa_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_pos,
-                                                                             s.np * 2, c->d_buf);
+                                                                             s.np * s.dim, c->d_buf);
     ++c->launches;
     set_scalar_kernel<<<(nw + 255) / 256, 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_scal + S_WEIGHT, 1.0);
     CUDA_TRY(c, cudaGetLastError());
@@ -1420,11 +1696,11 @@ int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_ps
     const DevSys& s = c->sys;
     const int nw = c->nw;
     if (nw == 0) return ALEA_OK;
-    const long n = static_cast<long>(s.np) * 2 * nw;
+    const long n = static_cast<long>(s.np) * s.dim * nw;
     const int grid = static_cast<int>((n + 255) / 256);
     auto plane = [&](int off, double* dst) -> int {
         ++c->launches;
-        to_soa_kernel<<<grid, 256, 0, c->stream>>>(records(c), nw, s.rec, off, s.np * 2, c->d_buf);
+        to_soa_kernel<<<grid, 256, 0, c->stream>>>(records(c), nw, s.rec, off, s.np * s.dim, c->d_buf);
         CUDA_TRY(c, cudaGetLastError());
         CUDA_TRY(c, copy_out(c, dst, c->d_buf, n * 8));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1463,6 +1739,7 @@ int alea_gpu_download_walkers(alea_gpu_ctx* c, double* positions, double* log_ps
 int alea_gpu_move(alea_gpu_ctx* c, int p, const double* new_pos, const uint8_t* accept, double* log_ratio,
                   double* phase, double* new_grad, double* new_lap) {
     if (!c || !new_pos) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_move: two-dimensional systems only");
     if (c->sys.f32)
         return fail(c, ALEA_ERR_UNSUPPORTED, "single moves run in FP64: set the precision back to FP64 first");
     const DevSys& s = c->sys;
@@ -1499,6 +1776,8 @@ int alea_gpu_move(alea_gpu_ctx* c, int p, const double* new_pos, const uint8_t* 
 
 int alea_gpu_set_precision(alea_gpu_ctx* c, int precision) {
     if (!c) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2 && precision == ALEA_PRECISION_FP32)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "the FP32 form runs two-dimensional systems only");
     cudaSetDevice(c->device);
     if (precision == ALEA_PRECISION_FP32) {
         if (c->nt != 32 || !f32_sweep_eligible(c->sys))
@@ -1518,6 +1797,7 @@ int alea_gpu_set_precision(alea_gpu_ctx* c, int precision) {
 // arithmetic: the proposal is kept on the host until committed.
 int alea_gpu_propose(alea_gpu_ctx* c, int p, const double* new_pos) {
     if (!c || !new_pos) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_propose: two-dimensional systems only");
     if (p < 0 || p >= c->sys.np) return fail(c, ALEA_ERR_INVALID, "particle index out of range");
     c->prop_p = p;
     c->prop_pos.assign(new_pos, new_pos + 2L * c->nw);
@@ -1554,7 +1834,8 @@ int alea_gpu_measure(alea_gpu_ctx* c) {
     if (!c) return ALEA_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->nw == 0) return ALEA_OK;
-    if (c->sys.f32) return launch_evaluate(c);   // the FP32 form keeps no orbital rows to refresh from
+    // the FP32 form keeps no orbital rows to refresh from; a 3-D walker is evaluated anew
+    if (c->sys.f32 || c->sys.dim == 3) return launch_evaluate(c);
     ++c->launches;
     CUDA_TRY(c, launch_measure(c->nt, c->nw, c->smem, c->stream, c->sys, records(c), c->pairs, c->npair));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1648,6 +1929,8 @@ int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, a
     }
     if (c->n_streams < 1) return fail(c, ALEA_ERR_INVALID, "no random streams (alea_gpu_set_streams)");
     if (prm->n_substeps < 1) return fail(c, ALEA_ERR_INVALID, "n_substeps must be >= 1");
+    if (c->sys.dim != 2)
+        return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_vmc_step_noalloc: two-dimensional systems only");
     const size_t need = static_cast<size_t>(prm->n_substeps) * c->sys.np * 3 * c->nw;
     if (need > kNoAllocRandoms)
         return fail(c, ALEA_ERR_INVALID,
@@ -1672,7 +1955,7 @@ int alea_gpu_vmc_step_noalloc(alea_gpu_ctx* c, const alea_gpu_vmc_params* prm, a
     ++c->launches;
     draw_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, stride,
                                                          prm->n_substeps, c->sys.zk, c->sys.zw, c->sys.zf,
-                                                         c->sys.zr, rnd, 0);
+                                                         c->sys.zr, rnd, c->sys.dim);
     CUDA_TRY(c, cudaGetLastError());
     SweepParams sp{};
     sp.mode = 0;
@@ -2157,7 +2440,7 @@ int packed_enqueue(alea_gpu_packed* P, const int shape[kClasses], bool timed) {
         const int nt = std::min(c->n_streams, c->nw);
         draw_kernel<<<(nt + 127) / 128, 128, 0, P->stream>>>(c->streams, c->n_streams, c->nw, c->sys.np, c->nw,
                                                              r.cfg.n_substeps, c->sys.zk, c->sys.zw, c->sys.zf,
-                                                             c->sys.zr, c->randoms, 0);
+                                                             c->sys.zr, c->randoms, c->sys.dim);
         ++P->launches;
     }
     PCUDA(P, cudaGetLastError());
@@ -2282,6 +2565,7 @@ int packed_class(const alea_gpu_ctx* c) {
 int packed_add(alea_gpu_packed* P, alea_gpu_ctx* c, const alea_gpu_run_config& cfg, int* slot) {
     if (!P || !c || c->device != P->device) return pfail(P, ALEA_ERR_INVALID, "packed run: context on another device");
     if (c->sys.f32) return pfail(P, ALEA_ERR_UNSUPPORTED, "packed run: FP64 contexts only");
+    if (c->sys.dim != 2) return pfail(P, ALEA_ERR_UNSUPPORTED, "packed run: two-dimensional systems only");
     if (c->nw < 1 || cfg.n_steps < 1 || cfg.n_substeps < 1 || cfg.n_accumulation_blocks < 0 ||
         cfg.n_equilibration_blocks < 0)
         return pfail(P, ALEA_ERR_INVALID, "packed run: empty population or bad run configuration");
@@ -2673,10 +2957,10 @@ int fresh_walkers(alea_gpu_ctx* c, const double* d_rows, int n_rows, int nw) {
     c->cur = 0;
     c->nw = nw;
     CUDA_TRY(c, cudaMemsetAsync(records(c), 0, static_cast<size_t>(s.rec) * 8 * nw, c->stream));
-    const long n = static_cast<long>(s.np) * 2 * nw;
+    const long n = static_cast<long>(s.np) * s.dim * nw;
     ++c->launches;
     from_rows_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_pos,
-                                                                              s.np * 2, d_rows, n_rows);
+                                                                              s.np * s.dim, d_rows, n_rows);
     ++c->launches;
     set_scalar_kernel<<<(nw + 255) / 256, 256, 0, c->stream>>>(records(c), nw, s.rec, s.o_scal + S_WEIGHT, 1.0);
     CUDA_TRY(c, cudaGetLastError());
@@ -2698,7 +2982,7 @@ int alea_gpu_final_configurations(alea_gpu_ctx* c, double* rows, int* nw) {
     CUDA_TRY(c, cudaSetDevice(c->device));
     *nw = c->nw;
     if (!rows || c->nw == 0) return ALEA_OK;
-    const int n = c->sys.np * 2;
+    const int n = c->sys.np * c->sys.dim;
     const long tot = static_cast<long>(n) * c->nw;
     ++c->launches;
     to_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, c->stream>>>(records(c), c->nw, c->sys.rec,
@@ -2715,10 +2999,10 @@ int alea_gpu_seed_walker_rows(alea_gpu_ctx* c, const double* rows, int n_rows, i
     if (nw < 1 || nw > c->capacity) return fail(c, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
     CUDA_TRY(c, cudaSetDevice(c->device));
     const int used = std::min(n_rows, nw);
-    for (long i = 0, n = static_cast<long>(used) * c->sys.np * 2; i < n; ++i)
+    for (long i = 0, n = static_cast<long>(used) * c->sys.np * c->sys.dim; i < n; ++i)
         if (!std::isfinite(rows[i]))
             return fail(c, ALEA_ERR_INVALID, "configuration rows must be finite (entry " + std::to_string(i) + ")");
-    CUDA_TRY(c, copy_in(c, c->d_buf, rows, static_cast<size_t>(used) * c->sys.np * 2 * 8));
+    CUDA_TRY(c, copy_in(c, c->d_buf, rows, static_cast<size_t>(used) * c->sys.np * c->sys.dim * 8));
     return fresh_walkers(c, c->d_buf, used, nw);
 }
 
@@ -2728,7 +3012,8 @@ int alea_gpu_carry_over(alea_gpu_ctx* from, alea_gpu_ctx* to, int nw, int mode) 
         return fail(to, ALEA_ERR_INVALID, "carry_over: unknown mode");
     if (nw < 1 || nw > to->capacity) return fail(to, ALEA_ERR_NOMEM, "walker count exceeds the capacity");
     if (from->nw < 1) return fail(to, ALEA_ERR_INVALID, "carry_over: the source context has no walkers");
-    if (from->sys.np != to->sys.np) return fail(to, ALEA_ERR_INVALID, "carry_over: particle counts differ");
+    if (from->sys.np != to->sys.np || from->sys.dim != to->sys.dim)
+        return fail(to, ALEA_ERR_INVALID, "carry_over: particle counts or dimensions differ");
     const int used = std::min(from->nw, nw);
     const bool peer = from->device != to->device;
     if (mode == ALEA_CARRY_STATE) {
@@ -2767,7 +3052,7 @@ int alea_gpu_carry_over(alea_gpu_ctx* from, alea_gpu_ctx* to, int nw, int mode) 
     }
     // positions: the source's rows, then a full evaluation in the destination
     CUDA_TRY(to, cudaSetDevice(from->device));
-    const int n = from->sys.np * 2;
+    const int n = from->sys.np * from->sys.dim;
     const long tot = static_cast<long>(n) * used;
     ++from->launches;
     to_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, from->stream>>>(
@@ -2788,6 +3073,7 @@ int alea_gpu_carry_over(alea_gpu_ctx* from, alea_gpu_ctx* to, int nw, int mode) 
 
 int alea_gpu_add_estimator(alea_gpu_ctx* c, const alea_gpu_estimator_spec* spec, int* id) {
     if (!c || !spec || !id) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_add_estimator: two-dimensional systems only");
     CUDA_TRY(c, cudaSetDevice(c->device));
     std::string err;
     if (int rc = est_add(c->est, c->sys, *spec, c->stream, err, id)) return fail(c, rc, err);
@@ -2901,6 +3187,7 @@ int orbital_param_derivatives(alea_gpu_ctx* c, double* out, double* dgrad, doubl
 int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_params) {
     const Phase phase("alea.param_derivs");
     if (!c || !n_params) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_parameter_derivatives: two-dimensional systems only");
     CUDA_TRY(c, cudaSetDevice(c->device));
     const int nopt = static_cast<int>(c->h_opt.size());
     *n_params = nopt;
@@ -2921,6 +3208,7 @@ int alea_gpu_parameter_derivatives(alea_gpu_ctx* c, double* derivs, int* n_param
 
 int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, double* dlap, int* n_params) {
     if (!c || !n_params) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_parameter_gradient_derivatives: two-dimensional systems only");
     CUDA_TRY(c, cudaSetDevice(c->device));
     const int nopt = static_cast<int>(c->h_opt.size());
     *n_params = nopt;
@@ -2961,6 +3249,7 @@ int alea_gpu_parameter_gradient_derivatives(alea_gpu_ctx* c, double* dgrad, doub
 
 int alea_gpu_set_forward_walking(alea_gpu_ctx* c, const double* lags, int n_lags, int interval) {
     if (!c || n_lags < 0 || (n_lags > 0 && !lags)) return ALEA_ERR_INVALID;
+    if (c->sys.dim != 2) return fail(c, ALEA_ERR_UNSUPPORTED, "alea_gpu_set_forward_walking: two-dimensional systems only");
     CUDA_TRY(c, cudaSetDevice(c->device));
     fw_free(c);
     if (n_lags == 0) return ALEA_OK;

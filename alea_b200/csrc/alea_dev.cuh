@@ -165,6 +165,14 @@ struct DevSys {
         f_sn, f_co, f_so, f_sg, f_sl, f_kg, f_kl, f_elwork, f_total;
     int f_total32;            // the FP32 form's total: its FP64 rebuild needs N² in the move union
     int f32;                  // sweeps run the FP32 form (alea_gpu_set_precision)
+    // three-dimensional walkers (alea_bf3d.cu): Ewald k-vectors [3*enk]
+    // (kx, ky, kz per vector) and the shared-memory layout after the hot
+    // part: proposal, misc slots, reduction area, pivot column, the pending
+    // determinants of a proposal, then the move's work area (new matrix and
+    // orbital rows); the refresh's tables reuse the area from the pending
+    // determinants on (t_work)
+    const double* ek3;
+    int t_newpos, t_misc, t_red, t_col, t_work, t_mwork, t_total;
     // ziggurat tables
     const uint64_t* zk;
     const double *zw, *zf;

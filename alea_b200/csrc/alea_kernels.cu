@@ -1191,21 +1191,20 @@ int batch_ctas_per_sm(int nt, size_t smem) {
 // out[(sweep*np + p)*(dim+1)*stride + d*stride + w].
 __global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
                             int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
-                            double zr, double* out, int crowd_mode) {
+                            double zr, double* out, int dim) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int n_active = n_streams < nw ? n_streams : nw;
     if (t >= n_active) return;
     const long base = nw / n_active, rem = nw % n_active;
     const long w0 = t * base + (t < rem ? t : rem);
     const long cnt = base + (t < rem ? 1 : 0);
-    (void)crowd_mode;
     Xo r{states[t * 4 + 0], states[t * 4 + 1], states[t * 4 + 2], states[t * 4 + 3]};
     for (int sw = 0; sw < n_sweeps; ++sw)
         for (int p = 0; p < np; ++p) {
-            double* row = out + (static_cast<long>(sw) * np + p) * 3 * stride;
-            for (int d = 0; d < 2; ++d)
+            double* row = out + (static_cast<long>(sw) * np + p) * (dim + 1) * stride;
+            for (int d = 0; d < dim; ++d)
                 for (long w = w0; w < w0 + cnt; ++w) row[d * stride + w] = xo_gaussian(r, zk, zw, zf, zr);
-            for (long w = w0; w < w0 + cnt; ++w) row[2 * stride + w] = xo_uniform(r);
+            for (long w = w0; w < w0 + cnt; ++w) row[dim * stride + w] = xo_uniform(r);
         }
     states[t * 4 + 0] = r.s0;
     states[t * 4 + 1] = r.s1;

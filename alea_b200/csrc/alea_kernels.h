@@ -133,9 +133,17 @@ bool f32_sweep_eligible(const DevSys& s);
 cudaError_t reserve_smem_f32(size_t smem);
 cudaError_t launch_sweep_f32(int nw, cudaStream_t st, const DevSys& s, double* records, const double* randoms,
                              long stride, const SweepParams& prm, const int2* pairs, int npair);
+// One thread per random stream: its crowd's randoms of n_sweeps sweeps, per
+// particle `dim` Gaussians then one uniform, [(sweep·np + p)·(dim+1)·stride +
+// d·stride + w] (src/qmc/sweep_blocking.h:39-48).
 __global__ void draw_kernel(uint64_t* states, int n_streams, int nw, int np, long stride,
                             int n_sweeps, const uint64_t* zk, const double* zw, const double* zf,
-                            double zr, double* out, int crowd_mode);
+                            double zr, double* out, int dim);
+// The three-dimensional walker kernels (alea_bf3d.cu): evaluation and the
+// VMC/DMC sweep, one CTA of 128 threads per walker, smem bytes each.
+cudaError_t launch_evaluate3(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records);
+cudaError_t launch_sweep3(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
+                          const double* randoms, long stride, const SweepParams& prm);
 __global__ void gather_kernel(double* dst, const double* src, const int* src_idx, int n, long rec);
 __global__ void scalar_kernel(const double* records, int nw, long rec, int offset, double* out);
 __global__ void to_soa_kernel(const double* records, int nw, long rec, int offset, int n, double* out);

@@ -11,6 +11,7 @@
 //                    (src/wavefunction/periodic_pair_sum.cpp:21-60)
 //   initial walkers  App::initialize_positions (src/qmc/app.cpp:56-112)
 #include <algorithm>
+#include <array>
 #include <mutex>
 #include <map>
 #include <atomic>
@@ -855,60 +856,120 @@ int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* cou
 // half-space k-vectors n1 n2 n3, kx ky kz with their weights, f_l(0) and
 // f̃_s(0)/V); the walker kernels are two-dimensional.  No counterpart in the
 // reference, which refuses 3-D Ewald (src/numerics/ewald_breakup.cpp:211-213).
+}  // extern "C"
+
+namespace {
+
+// The optimized breakup of 1/r in a 3-D cell (rows a_i of `lattice`): the
+// 3-D radial kernel, r_c the Wigner-Seitz inradius, the knot ladder 20, 24.
+// In 3-D the misfit on the discrete shells understates the energy's error
+// (the neglected tail grows with the k² density of vectors): 12 knots pass a
+// 1e-10 shell tolerance yet leave 2e-7 in the CsCl Madelung constant, 20
+// knots 7e-9.  The ladder starts at 20.
+Breakup ewald3d_breakup(const double* lattice, double ewald_tol, double& rc, double& volume) {
+    if (!lattice) throw std::invalid_argument("ewald3d: no lattice");
+    alea_breakup::Lattice lat;
+    lat.dim = 3;
+    std::copy(lattice, lattice + 9, lat.a);
+    const double* a = lat.a;
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    if (det == 0.0 || !std::isfinite(det)) throw std::invalid_argument("ewald3d: singular lattice vectors");
+    lat.volume = std::abs(det);
+    // b_i · a_j = 2π δ_ij: b = 2π (Aᵀ)⁻¹, rows b_i
+    const double inv[9] = {(a[4] * a[8] - a[5] * a[7]) / det, (a[2] * a[7] - a[1] * a[8]) / det,
+                           (a[1] * a[5] - a[2] * a[4]) / det, (a[5] * a[6] - a[3] * a[8]) / det,
+                           (a[0] * a[8] - a[2] * a[6]) / det, (a[2] * a[3] - a[0] * a[5]) / det,
+                           (a[3] * a[7] - a[4] * a[6]) / det, (a[1] * a[6] - a[0] * a[7]) / det,
+                           (a[0] * a[4] - a[1] * a[3]) / det};
+    for (int i = 0; i < 3; ++i)
+        for (int d = 0; d < 3; ++d) lat.b[i * 3 + d] = kTwoPi * inv[d * 3 + i];
+    double shortest2 = 0.0;
+    for (int n0 = -2; n0 <= 2; ++n0)
+        for (int n1 = -2; n1 <= 2; ++n1)
+            for (int n2 = -2; n2 <= 2; ++n2) {
+                if (!n0 && !n1 && !n2) continue;
+                double r2 = 0.0;
+                for (int d = 0; d < 3; ++d) {
+                    const double x = n0 * a[d] + n1 * a[3 + d] + n2 * a[6 + d];
+                    r2 += x * x;
+                }
+                if (shortest2 == 0.0 || r2 < shortest2) shortest2 = r2;
+            }
+    rc = 0.5 * std::sqrt(shortest2);
+    volume = lat.volume;
+    const double tol = ewald_tol > 0.0 ? ewald_tol : 1e-6;
+    const auto f = alea_breakup::coulomb();
+    for (int nk : {20, 24}) {
+        alea_breakup::Options opt;
+        opt.n_knots = nk;
+        Breakup br = alea_breakup::optimize(lat, rc, *f, opt);
+        if (br.residual < tol) return br;
+    }
+    throw std::runtime_error("ewald3d: the breakup did not reach the requested tolerance");
+}
+
+void json_ewald3d(Json& j, double rc, const Breakup& br) {
+    j.key("ewald");
+    j.open('{');
+    j.kv("r_cut", rc);
+    j.key("spline");
+    j.open('{');
+    j.kv("r_cut", br.rc);
+    j.kv("inv_delta", 1.0 / br.delta);
+    j.kv("n_knots", br.n_knots);
+    j.arr("scaled", br.scaled);
+    j.close('}');
+    j.arr("n1", br.n[0]);
+    j.arr("n2", br.n[1]);
+    j.arr("n3", br.n[2]);
+    j.arr("kx", br.kvec[0]);
+    j.arr("ky", br.kvec[1]);
+    j.arr("kz", br.kvec[2]);
+    j.arr("weight", br.weight);
+    j.kv("v_long_zero", br.long_range_zero);
+    j.kv("sr_k0", br.short_range_k0);
+    j.kv("residual", br.residual);
+}
+
+// Real 3-D plane waves of the lowest shells of a cubic cell of side L: k =
+// 2π n / L with n sorted by |n|², then lexicographically; k = 0 gives
+// cos(0), every other ±n pair is represented by the n whose first nonzero
+// component is positive and gives cos then sin.
+void plane_waves_3d(double L, int n, std::vector<double>& k, std::vector<int>& is_sin) {
+    std::vector<std::array<int, 4>> cand;
+    for (int a = -4; a <= 4; ++a)
+        for (int b = -4; b <= 4; ++b)
+            for (int c = -4; c <= 4; ++c) {
+                const int first = a != 0 ? a : (b != 0 ? b : c);
+                if (first < 0) continue;
+                cand.push_back({a * a + b * b + c * c, a, b, c});
+            }
+    std::sort(cand.begin(), cand.end());
+    k.clear();
+    is_sin.clear();
+    for (const auto& q : cand) {
+        if (static_cast<int>(is_sin.size()) >= n) break;
+        for (int s = 0; s < (q[0] == 0 ? 1 : 2) && static_cast<int>(is_sin.size()) < n; ++s) {
+            for (int d = 0; d < 3; ++d) k.push_back(kTwoPi * q[1 + d] / L);
+            is_sin.push_back(s);
+        }
+    }
+    if (static_cast<int>(is_sin.size()) != n) throw std::invalid_argument("heg3d: too many electrons per spin");
+}
+
+}  // namespace
+
+extern "C" {
+
 int alea_gpu_setup_ewald3d(const double* lattice, double ewald_tol, alea_gpu_setup** out, char* err,
                            size_t err_len) {
     if (!out) return ALEA_ERR_INVALID;
     *out = nullptr;
     auto* S = new alea_gpu_setup();
     try {
-        if (!lattice) throw std::invalid_argument("ewald3d: no lattice");
-        alea_breakup::Lattice lat;
-        lat.dim = 3;
-        std::copy(lattice, lattice + 9, lat.a);
-        const double* a = lat.a;
-        const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
-                           a[2] * (a[3] * a[7] - a[4] * a[6]);
-        if (det == 0.0 || !std::isfinite(det)) throw std::invalid_argument("ewald3d: singular lattice vectors");
-        lat.volume = std::abs(det);
-        // b_i · a_j = 2π δ_ij: b = 2π (Aᵀ)⁻¹, rows b_i
-        const double inv[9] = {(a[4] * a[8] - a[5] * a[7]) / det, (a[2] * a[7] - a[1] * a[8]) / det,
-                               (a[1] * a[5] - a[2] * a[4]) / det, (a[5] * a[6] - a[3] * a[8]) / det,
-                               (a[0] * a[8] - a[2] * a[6]) / det, (a[2] * a[3] - a[0] * a[5]) / det,
-                               (a[3] * a[7] - a[4] * a[6]) / det, (a[1] * a[6] - a[0] * a[7]) / det,
-                               (a[0] * a[4] - a[1] * a[3]) / det};
-        for (int i = 0; i < 3; ++i)
-            for (int d = 0; d < 3; ++d) lat.b[i * 3 + d] = kTwoPi * inv[d * 3 + i];
-        double shortest2 = 0.0;
-        for (int n0 = -2; n0 <= 2; ++n0)
-            for (int n1 = -2; n1 <= 2; ++n1)
-                for (int n2 = -2; n2 <= 2; ++n2) {
-                    if (!n0 && !n1 && !n2) continue;
-                    double r2 = 0.0;
-                    for (int d = 0; d < 3; ++d) {
-                        const double x = n0 * a[d] + n1 * a[3 + d] + n2 * a[6 + d];
-                        r2 += x * x;
-                    }
-                    if (shortest2 == 0.0 || r2 < shortest2) shortest2 = r2;
-                }
-        const double rc = 0.5 * std::sqrt(shortest2);
-        const double tol = ewald_tol > 0.0 ? ewald_tol : 1e-6;
-        const auto f = alea_breakup::coulomb();
-        Breakup br;
-        bool ok = false;
-        // In 3-D the misfit on the discrete shells understates the energy's
-        // error (the neglected tail grows with the k² density of vectors): 12
-        // knots pass a 1e-10 shell tolerance yet leave 2e-7 in the CsCl
-        // Madelung constant, 20 knots 7e-9.  The ladder starts at 20.
-        for (int nk : {20, 24}) {
-            alea_breakup::Options opt;
-            opt.n_knots = nk;
-            br = alea_breakup::optimize(lat, rc, *f, opt);
-            if (br.residual < tol) {
-                ok = true;
-                break;
-            }
-        }
-        if (!ok) throw std::runtime_error("ewald3d: the breakup did not reach the requested tolerance");
+        double rc = 0.0, volume = 0.0;
+        const Breakup br = ewald3d_breakup(lattice, ewald_tol, rc, volume);
         S->sys.dim = 3;
         S->sys.periodic = 1;
         Json j;
@@ -918,28 +979,187 @@ int alea_gpu_setup_ewald3d(const double* lattice, double ewald_tol, alea_gpu_set
         j.key("cell");
         j.open('{');
         j.arr("vectors", std::vector<double>(lattice, lattice + 9));
-        j.kv("volume", lat.volume);
+        j.kv("volume", volume);
         j.close('}');
-        j.key("ewald");
-        j.open('{');
-        j.kv("r_cut", rc);
-        j.key("spline");
-        j.open('{');
-        j.kv("r_cut", br.rc);
-        j.kv("inv_delta", 1.0 / br.delta);
-        j.kv("n_knots", br.n_knots);
-        j.arr("scaled", br.scaled);
+        json_ewald3d(j, rc, br);
         j.close('}');
-        j.arr("n1", br.n[0]);
-        j.arr("n2", br.n[1]);
-        j.arr("n3", br.n[2]);
-        j.arr("kx", br.kvec[0]);
-        j.arr("ky", br.kvec[1]);
-        j.arr("kz", br.kvec[2]);
-        j.arr("weight", br.weight);
-        j.kv("v_long_zero", br.long_range_zero);
-        j.kv("sr_k0", br.short_range_k0);
-        j.kv("residual", br.residual);
+        j.close('}');
+        S->json = j.s;
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        delete S;
+        return ALEA_ERR_INVALID;
+    }
+    *out = S;
+    return ALEA_OK;
+}
+
+// 3-D electron gas with backflow: n_up + n_down electrons in a cubic cell of
+// volume N 4π r_s³ / 3, one backflow determinant of real plane waves per spin
+// (plane_waves_3d; every spin must close its shell), channels from the own
+// spin (c_0 = bf_like, c_1 = 3 c_0 / L: zero slope) and the other spin
+// (c_0 = bf_unlike, c_1 = 0), C = 3, L = bf_cut (<= 0: half the side);
+// Drummond Jastrows (C = 3, the 3-D Kato cusps 1/2 and 1/4, alpha0, cutoff
+// 0.999 × half the side) on the like-spin pairs and the unlike pair; the 3-D
+// Ewald sum.  Initial walkers: uniform.
+int alea_gpu_setup_heg3d(int n_up, int n_down, double rs, double bf_like, double bf_unlike, double bf_cut,
+                         double alpha0, double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len) {
+    if (!out) return ALEA_ERR_INVALID;
+    *out = nullptr;
+    auto* S = new alea_gpu_setup();
+    try {
+        if (n_up < 1 || n_down < 1 || n_up > 64 || n_down > 64 || !(rs > 0.0))
+            throw std::invalid_argument("heg3d: need 1..64 electrons per spin and rs > 0");
+        alea_gpu_system& y = S->sys;
+        const int np = n_up + n_down;
+        const double L = rs * std::cbrt(4.0 * kPi * np / 3.0);
+        y.dim = 3;
+        y.n_particles = np;
+        y.periodic = 1;
+        const double lat[9] = {L, 0, 0, 0, L, 0, 0, 0, L};
+        std::copy(lat, lat + 9, y.lattice);
+        for (int g = 0; g < 2; ++g) {
+            alea_gpu_group& G = y.groups[y.n_groups++];
+            G.first = g == 0 ? 0 : n_up;
+            G.last = g == 0 ? n_up : np;
+            G.charge = -1.0;
+            G.inv_mass[0] = G.inv_mass[1] = G.inv_mass[2] = 1.0;
+        }
+        const double Lb = bf_cut > 0.0 ? bf_cut : 0.5 * L;
+        if (Lb > 0.5 * L) throw std::invalid_argument("heg3d: the backflow cutoff exceeds half the cell");
+        y.n_backflow = 2;
+        for (int g = 0; g < 2; ++g) {
+            alea_gpu_backflow& F = y.backflow[g];
+            F.first = y.groups[g].first;
+            F.last = y.groups[g].last;
+            F.type = ALEA_ORB_PLANE_WAVE;
+            std::vector<double> k;
+            std::vector<int> is_sin;
+            plane_waves_3d(L, F.last - F.first, k, is_sin);
+            F.k = S->keep(k);
+            F.is_sin = S->keepi(is_sin);
+            F.n_channels = 2;
+            for (int h = 0; h < 2; ++h) {
+                alea_gpu_backflow_channel& C = F.channels[h];
+                C.source_first = y.groups[h].first;
+                C.source_last = y.groups[h].last;
+                C.C = 3;
+                C.L = Lb;
+                C.n_coeffs = 2;
+                C.coeffs[0] = h == g ? bf_like : bf_unlike;
+                C.coeffs[1] = h == g ? 3.0 * bf_like / Lb : 0.0;
+                C.zero_slope = h == g ? 1 : 0;
+            }
+        }
+        const double Lj = 0.999 * 0.5 * L;
+        y.n_terms = 2;
+        for (int t = 0; t < 2; ++t) {
+            alea_gpu_pair_term& T = y.terms[t];
+            T.kind = ALEA_PAIR_DRUMMOND;
+            if (t == 0) {
+                T.n_pairs = 2;
+                const int pr[2][4] = {{0, n_up, 0, n_up}, {n_up, np, n_up, np}};
+                for (int q = 0; q < 2; ++q)
+                    for (int c = 0; c < 4; ++c) T.pairs[q][c] = pr[q][c];
+                T.gamma = 0.25;
+            } else {
+                T.n_pairs = 1;
+                const int pr[4] = {0, n_up, n_up, np};
+                for (int c = 0; c < 4; ++c) T.pairs[0][c] = pr[c];
+                T.gamma = 0.5;
+            }
+            T.C = 3;
+            T.L = Lj;
+            T.n_coeffs = 1;
+            T.dcoeffs[0] = alpha0;
+        }
+        double rc = 0.0, volume = 0.0;
+        const Breakup br = ewald3d_breakup(lat, ewald_tol, rc, volume);
+        alea_gpu_ewald& E = y.ewald;
+        E.enabled = 1;
+        E.r_cut = rc;
+        E.inv_eps = 1.0;
+        set_spline(S, E.long_range, br);
+        E.kset.n_k = static_cast<int>(br.weight.size());
+        E.kset.n1 = S->keepi(br.n[0]);
+        E.kset.n2 = S->keepi(br.n[1]);
+        E.kset.n3 = S->keepi(br.n[2]);
+        E.kset.kx = S->keep(br.kvec[0]);
+        E.kset.ky = S->keep(br.kvec[1]);
+        E.kset.kz = S->keep(br.kvec[2]);
+        E.kset.weight = S->keep(br.weight);
+        const double self = -0.5 * br.long_range_zero * np, bg = -0.5 * double(np) * np * br.short_range_k0;
+        E.constant = self + bg;
+        Json j;
+        j.open('{');
+        j.ks("kind", "heg3d");
+        j.kv("dim", 3);
+        j.kv("np", np);
+        j.key("cell");
+        j.open('{');
+        j.kv("periodic", 1);
+        j.kv("dim", 3);
+        j.arr("vectors", std::vector<double>(lat, lat + 9));
+        j.close('}');
+        j.key("groups");
+        j.open('[');
+        for (int g = 0; g < 2; ++g) {
+            j.open('{');
+            j.kv("first", y.groups[g].first);
+            j.kv("last", y.groups[g].last);
+            j.kv("charge", -1.0);
+            j.arr("inv_mass", std::vector<double>{1.0, 1.0, 1.0});
+            j.close('}');
+        }
+        j.close(']');
+        j.key("backflow");
+        j.open('[');
+        for (int g = 0; g < 2; ++g) {
+            const alea_gpu_backflow& F = y.backflow[g];
+            const int n = F.last - F.first;
+            j.open('{');
+            j.kv("first", F.first);
+            j.kv("last", F.last);
+            j.ks("type", "plane_wave");
+            j.arr("k", std::vector<double>(F.k, F.k + 3 * n));
+            j.arr("is_sin", std::vector<int>(F.is_sin, F.is_sin + n));
+            j.key("channels");
+            j.open('[');
+            for (int h = 0; h < 2; ++h) {
+                const alea_gpu_backflow_channel& C = F.channels[h];
+                j.open('{');
+                j.kv("source_first", C.source_first);
+                j.kv("source_last", C.source_last);
+                j.kv("C", C.C);
+                j.arr("coeffs", std::vector<double>(C.coeffs, C.coeffs + C.n_coeffs));
+                j.kv("L", C.L);
+                j.kv("zero_slope", C.zero_slope);
+                j.close('}');
+            }
+            j.close(']');
+            j.close('}');
+        }
+        j.close(']');
+        j.key("drummond");
+        j.open('[');
+        for (int t = 0; t < 2; ++t) {
+            const alea_gpu_pair_term& T = y.terms[t];
+            j.open('{');
+            j.kv("C", T.C);
+            j.kv("gamma", T.gamma);
+            j.kv("L", T.L);
+            j.arr("coeffs", std::vector<double>{alpha0});
+            j.key("pairs");
+            j.open('[');
+            for (int q = 0; q < T.n_pairs; ++q) j.arr("", std::vector<int>(T.pairs[q], T.pairs[q] + 4));
+            j.close(']');
+            j.close('}');
+        }
+        j.close(']');
+        json_ewald3d(j, rc, br);
+        j.kv("inv_eps", 1.0);
+        j.kv("self_energy", self);
+        j.kv("background_energy", bg);
         j.close('}');
         j.close('}');
         S->json = j.s;
@@ -1053,22 +1273,22 @@ int alea_gpu_setup_positions(const alea_gpu_setup* S, uint64_t seed, int nw, dou
     std::mt19937_64 eng(seed);
     std::uniform_real_distribution<double> uni(0.0, 1.0);
     std::normal_distribution<double> gau(0.0, 1.0);
-    const int np = y.n_particles;
+    const int np = y.n_particles, dim = y.dim;
     for (int w = 0; w < nw; ++w)
         for (int p = 0; p < np; ++p) {
-            double* r = positions + (static_cast<size_t>(w) * np + p) * 2;
+            double* r = positions + (static_cast<size_t>(w) * np + p) * dim;
             if (!S->anchors.empty()) {
-                for (int d = 0; d < 2; ++d) r[d] = std::fma(S->jitter, gau(eng), S->anchors[p * 2 + d]);
+                for (int d = 0; d < dim; ++d) r[d] = std::fma(S->jitter, gau(eng), S->anchors[p * dim + d]);
             } else if (y.periodic) {
-                double f[2];
-                for (int i = 0; i < 2; ++i) f[i] = std::fma(1.0, uni(eng), -0.5);
-                for (int d = 0; d < 2; ++d) {
+                double f[3];
+                for (int i = 0; i < dim; ++i) f[i] = std::fma(1.0, uni(eng), -0.5);
+                for (int d = 0; d < dim; ++d) {
                     double acc = 0.0;
-                    for (int i = 0; i < 2; ++i) acc = std::fma(f[i], y.lattice[i * 2 + d], acc);
+                    for (int i = 0; i < dim; ++i) acc = std::fma(f[i], y.lattice[i * dim + d], acc);
                     r[d] = acc;
                 }
             } else {
-                for (int d = 0; d < 2; ++d) r[d] = std::fma(S->open_L, uni(eng), -0.5 * S->open_L);
+                for (int d = 0; d < dim; ++d) r[d] = std::fma(S->open_L, uni(eng), -0.5 * S->open_L);
             }
         }
     return ALEA_OK;

@@ -96,6 +96,13 @@ def ewald3d(lattice, ewald_tol: float = 1e-6) -> Setup:
     return _make("alea_gpu_setup_ewald3d", lat.ctypes.data_as(_capi.c_dp), ewald_tol)
 
 
+def heg3d(n_up: int, n_down: int, rs: float, bf_like: float = 0.1, bf_unlike: float = 0.1,
+          bf_cut: float = 0.0, alpha0: float = 0.0, ewald_tol: float = 1e-6) -> Setup:
+    """3-D electron gas with backflow determinants, Drummond Jastrows and the
+    3-D Ewald sum (alea_gpu_setup_heg3d)."""
+    return _make("alea_gpu_setup_heg3d", n_up, n_down, rs, bf_like, bf_unlike, bf_cut, alpha0, ewald_tol)
+
+
 def dipoles2d(n: int, rs: float, strength: float = 1.0, exponent: float = 3.0,
               matching_radius: float = 0.0459) -> Setup:
     """2-D dipolar bosons: zero-energy Jastrow, C/r^p with its continuum tail."""

@@ -563,6 +563,14 @@ def gpu_arm(a):
                                    system="N=42 rs=30 with backflow determinants (C=3, L at the inradius)"),
         }
         tw.close()
+        # the fourth configuration: the 3-D backflow gas, 54 electrons at r_s = 5, 3-D Ewald, 4096 walkers
+        g3 = S.heg3d(27, 27, 5.0)
+        others["backflow_heg54_3d"] = dict(
+            vmc_sweeps(g3.desc, g3.positions(seed + 14, 4096), 4096, 2, 1.0),
+            sweep="3-D CTA sweep (alea_bf3d.cu), one pivoted Gauss-Jordan per determinant per move",
+            system="3-D electron gas N=54 (27+27) rs=5, backflow determinants of plane waves (C=3, c0=0.1, "
+                   "L = half the cell side), Drummond Jastrows, 3-D Ewald (%d k-vectors)" % len(g3.desc["ewald"]["weight"]))
+        g3.close()
 
     # ── the serving mix through the packed server (config 5), rank 0 only ──
     serving = None

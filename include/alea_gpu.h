@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define ALEA_GPU_ABI_VERSION 1
+#define ALEA_GPU_ABI_VERSION 2
 
 enum {
     ALEA_OK = 0,
@@ -77,8 +77,9 @@ typedef struct {
     const double* scaled; /* [3 * n_knots] */
 } alea_gpu_spline;
 
-/* Half-space reciprocal vectors k = n1 b1 + n2 b2 with their weights
- * (src/numerics/ewald_breakup.h:73-77). */
+/* Half-space reciprocal vectors k = n1 b1 + n2 b2 (+ n3 b3 in 3-D) with their
+ * weights (src/numerics/ewald_breakup.h:73-77).  n3 and kz are read only in
+ * a 3-D system (NULL otherwise). */
 typedef struct {
     int n_k;
     const int* n1;
@@ -86,6 +87,8 @@ typedef struct {
     const double* kx;
     const double* ky;
     const double* weight;
+    const int* n3;
+    const double* kz;
 } alea_gpu_kset;
 
 typedef struct {
@@ -207,7 +210,9 @@ typedef struct {
 } alea_gpu_backflow;
 
 typedef struct {
-    int dim;                      /* 2 (3 for open cells) */
+    int dim;                      /* 2, or 3: orthorhombic or open cells, backflow or plain
+                                     determinants, Drummond / minimum-image Padé terms,
+                                     3-D Ewald (kset.kz), open Coulomb */
     int n_particles;
     int periodic;
     double lattice[9];            /* reduced lattice vectors, row-major [i*dim + d]
@@ -660,10 +665,23 @@ int alea_gpu_setup_charges2d(const double* lattice, int n_groups, const int* cou
  * rows a_i of `lattice` (9 numbers), the optimized breakup of 1/r with the
  * 3-D radial kernel, r_c the Wigner-Seitz inradius.  Host tables only, in
  * alea_gpu_setup_json (the spline, half-space k-vectors with weights f̃_l/V,
- * f_l(0), f̃_s(0)/V); the walker kernels are two-dimensional and
- * alea_gpu_create refuses this setup's system. */
+ * f_l(0), f̃_s(0)/V).  The system of a 3-D electron gas that uses these
+ * tables is alea_gpu_setup_heg3d's. */
 int alea_gpu_setup_ewald3d(const double* lattice, double ewald_tol, alea_gpu_setup** out, char* err,
                            size_t err_len);
+/* 3-D electron gas with backflow (no counterpart among the reference's
+ * builders, which refuse 3-D plane-wave shells and 3-D Ewald; its backflow
+ * determinant, BackflowSlaterDeterminant, src/wavefunction/
+ * backflow_slater_determinant.h:15-80, is dimension-generic): n_up + n_down
+ * electrons in a cubic cell of volume N 4π rs³/3, one backflow determinant of
+ * real plane waves per spin (k = 2π n/L by |n|², then lexicographic n, k = 0
+ * first, cos then sin per ±n), channels from the own spin (c_0 = bf_like,
+ * c_1 = 3 c_0/L) and the other spin (c_0 = bf_unlike), C = 3, L = bf_cut
+ * (<= 0: half the side); Drummond Jastrows (C = 3, the 3-D Kato cusps 1/2 and
+ * 1/4, alpha0, cutoff 0.999 × half the side); the 3-D Ewald sum of
+ * alea_gpu_setup_ewald3d. */
+int alea_gpu_setup_heg3d(int n_up, int n_down, double rs, double bf_like, double bf_unlike, double bf_cut,
+                         double alpha0, double ewald_tol, alea_gpu_setup** out, char* err, size_t err_len);
 /* 2-D dipolar bosons: n of mass 1 in a hexagonal cell at density rs, C/r^p
  * (strength, exponent) with its continuum tail, and the zero-energy Jastrow
  * with the given matching radius, cut off at the Wigner-Seitz inradius. */

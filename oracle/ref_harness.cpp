@@ -25,10 +25,14 @@
 //                   (method=vmc|dmc) and GpuVMC / GpuDMC on copies of the same
 //                   ensemble, the system flattened by alea::gpu::pack_system
 //                   from the objects built here; both traces printed
+// Every mode takes pos_file=PATH (whitespace-separated AoS positions of the nw
+// walkers) in place of the seeded initialisation.
 // vmc and dmc attach the same estimators when gofr_bins, dens_bins or
 // sofk_kmax is given, and print the estimators' series of run_result().
 #include <omp.h>
 
+#include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -749,9 +753,188 @@ std::unique_ptr<System> build_dipoles(const Args& a) {
     return s;
 }
 
+// Real 3-D plane waves of the lowest shells of a cubic cell of side L: k = 2π n / L
+// with n sorted by |n|², then lexicographically; k = 0 gives cos(0), every other
+// ±n pair is represented by the n whose first nonzero component is positive and
+// gives cos then sin.  The reference builds no 3-D shells
+// (src/wavefunction/orbital_set.h:581-584), so this list is the harness's own;
+// the device reads it from the setup dump.
+void plane_waves_3d(double L, std::size_t n, std::vector<double>& k, std::vector<char>& is_sin) {
+    const double pi = 3.14159265358979323846;
+    std::vector<std::array<int, 4>> cand;   // |n|², n
+    for (int a = -4; a <= 4; ++a)
+        for (int b = -4; b <= 4; ++b)
+            for (int c = -4; c <= 4; ++c) {
+                const int first = a != 0 ? a : (b != 0 ? b : c);
+                if (first < 0) continue;
+                cand.push_back({a * a + b * b + c * c, a, b, c});
+            }
+    std::sort(cand.begin(), cand.end());
+    k.clear();
+    is_sin.clear();
+    for (const auto& q : cand) {
+        if (is_sin.size() >= n) break;
+        const double kv[3] = {2 * pi * q[1] / L, 2 * pi * q[2] / L, 2 * pi * q[3] / L};
+        for (int s = 0; s < (q[0] == 0 ? 1 : 2) && is_sin.size() < n; ++s) {
+            k.insert(k.end(), kv, kv + 3);
+            is_sin.push_back(static_cast<char>(s));
+        }
+    }
+    if (is_sin.size() != n) throw std::runtime_error("plane_waves_3d: shell table too small");
+}
+
+// 3-D electron gas with backflow: cubic cell at density rs, one backflow
+// determinant of plane waves per spin (channels as build_heg's: the own group
+// with c_1 derived, the other group with c_0, c_1; C = 3; L = bf_L or half the
+// cell side), Drummond Jastrows (C = 3, Kato cusps 1/2 for opposite and 1/4
+// for like spins in 3-D, scaled by cusp, cutoff 0.999 R_WS), kinetic energy
+// only: the reference has no 3-D Coulomb sum (src/numerics/ewald_breakup.cpp:211-213).
+// bf=0 leaves plain plane-wave determinants instead.
+std::unique_ptr<System> build_heg3d(const Args& a) {
+    auto s = std::make_unique<System>();
+    s->kind = "heg3d";
+    const std::size_t nu = static_cast<std::size_t>(geti(a, "nu", 27));
+    const std::size_t nd = static_cast<std::size_t>(geti(a, "nd", 27));
+    const double rs = getd(a, "rs", 5.0);
+    const double pi = 3.14159265358979323846;
+    s->dim = 3;
+    s->np = nu + nd;
+    const double L = rs * std::cbrt(4.0 * pi * static_cast<double>(s->np) / 3.0);
+    const std::vector<double> vec{L, 0.0, 0.0, 0.0, L, 0.0, 0.0, 0.0, L};
+    s->cell = SimulationCell(3, vec);
+    s->groups.push_back(make_group("up", 0, nu, -1.0, 3));
+    if (nd > 0) s->groups.push_back(make_group("down", nu, nd, -1.0, 3));
+    s->ham.add_component(std::make_unique<Kinetic>(s->groups));
+
+    Json& j = s->setup;
+    j.open('{');
+    j.ks("kind", "heg3d");
+    j.ki("dim", 3);
+    j.ki("np", static_cast<long long>(s->np));
+    dump_cell(j, s->cell);
+    dump_groups(j, s->groups);
+
+    const bool backflow = geti(a, "bf", 1) != 0;
+    if (backflow) {
+        const double c_like = getd(a, "bf_like", 0.1);
+        const double c_un0 = getd(a, "bf_un0", 0.1), c_un1 = getd(a, "bf_un1", 0.0);
+        const double Lb = getd(a, "bf_L", 0.5 * L);
+        j.key("backflow");
+        j.open('[');
+        for (std::size_t gi = 0; gi < s->groups.size(); ++gi) {
+            const ParticleGroup& g = s->groups[gi];
+            std::vector<double> kv;
+            std::vector<char> is_sin;
+            plane_waves_3d(L, g.size(), kv, is_sin);
+            j.open('{');
+            j.ki("first", static_cast<long long>(g.first));
+            j.ki("last", static_cast<long long>(g.last));
+            j.ks("type", "plane_wave");
+            j.arr("k", kv);
+            j.arr("is_sin", std::vector<double>(is_sin.begin(), is_sin.end()));
+            std::vector<BackflowSlaterDeterminant::Channel> chans;
+            j.key("channels");
+            j.open('[');
+            for (std::size_t hi = 0; hi < s->groups.size(); ++hi) {
+                const ParticleGroup& h = s->groups[hi];
+                BackflowSlaterDeterminant::Channel ch;
+                ch.source_first = h.first;
+                ch.source_last = h.last;
+                ch.truncation = 3;
+                std::vector<double> full;
+                if (hi == gi) {
+                    ch.params = {Parameter{"", c_like, false}, Parameter{"", Lb, true}};
+                    full = {c_like, 3.0 * c_like / Lb};
+                } else {
+                    ch.params = {Parameter{"", c_un0, false}, Parameter{"", c_un1, false},
+                                 Parameter{"", Lb, true}};
+                    full = {c_un0, c_un1};
+                }
+                j.open('{');
+                j.ki("source_first", static_cast<long long>(h.first));
+                j.ki("source_last", static_cast<long long>(h.last));
+                j.ki("C", 3);
+                j.arr("coeffs", full);
+                j.kv("L", Lb);
+                j.ki("zero_slope", hi == gi ? 1 : 0);
+                std::vector<double> opt;
+                for (std::size_t q = 0; q < ch.params.size(); ++q)
+                    if (!ch.params[q].is_fixed) opt.push_back(static_cast<double>(q));
+                j.arr("opt_index", opt);
+                j.close('}');
+                chans.push_back(std::move(ch));
+            }
+            j.close(']');
+            j.close('}');
+            std::vector<BackflowSlaterDeterminant::Block> bb;
+            bb.push_back({g.first, g.last, std::make_unique<PlaneWaveOrbitalSet>(3, kv, is_sin)});
+            s->psi.add_component(std::make_unique<BackflowSlaterDeterminant>(
+                std::move(bb), std::move(chans), s->cell));
+        }
+        j.close(']');
+    } else {
+        std::vector<SlaterDeterminant::Block> blocks;
+        j.key("slater");
+        j.open('[');
+        for (const ParticleGroup& g : s->groups) {
+            std::vector<double> kv;
+            std::vector<char> is_sin;
+            plane_waves_3d(L, g.size(), kv, is_sin);
+            j.open('{');
+            j.ki("first", static_cast<long long>(g.first));
+            j.ki("last", static_cast<long long>(g.last));
+            j.ks("type", "plane_wave");
+            j.arr("k", kv);
+            j.arr("is_sin", std::vector<double>(is_sin.begin(), is_sin.end()));
+            j.close('}');
+            blocks.push_back({g.first, g.last, std::make_unique<PlaneWaveOrbitalSet>(3, kv, is_sin)});
+        }
+        j.close(']');
+        s->psi.add_component(std::make_unique<SlaterDeterminant>(std::move(blocks)));
+    }
+
+    const double alpha0 = getd(a, "alpha0", 0.0);
+    if (geti(a, "jastrow", 1) != 0 && nd > 0) {
+        const double Lcut = getd(a, "cutoff", 0.999 * s->cell.ws_radius());
+        j.key("drummond");
+        j.open('[');
+        for (int item = 0; item < 2; ++item) {
+            std::vector<JastrowGroupPair> pairs;
+            if (item == 0) {
+                pairs.push_back({s->groups[0], s->groups[0]});
+                pairs.push_back({s->groups[1], s->groups[1]});
+            } else {
+                pairs.push_back({s->groups[0], s->groups[1]});
+            }
+            // 2 μ R / (2l + d - 1) with μ = 1/2, R = 1, d = 3; cusp=0 gives a smooth
+            // Jastrow (the kinetic-only Hamiltonian then has no 1/r local energy)
+            const double gamma = getd(a, "cusp", 1.0) / static_cast<double>(2 * (item == 0 ? 1 : 0) + 2);
+            std::vector<Parameter> params{Parameter{"p0", alpha0, true}, Parameter{"L", Lcut, true, true}};
+            auto dj = std::make_unique<DrummondJastrow>(3, gamma, pairs, params);
+            j.open('{');
+            j.ki("C", 3);
+            j.kv("gamma", gamma);
+            j.kv("L", Lcut);
+            j.arr("coeffs", std::vector<double>{alpha0});
+            j.key("pairs");
+            j.open('[');
+            for (const auto& p : pairs)
+                j.arr("", std::vector<double>{double(p.a.first), double(p.a.last),
+                                              double(p.b.first), double(p.b.last)});
+            j.close(']');
+            j.close('}');
+            s->psi.add_component(std::move(dj));
+        }
+        j.close(']');
+    }
+    j.close('}');
+    return s;
+}
+
 std::unique_ptr<System> build_system(const Args& a) {
     const std::string k = gets(a, "system", "heg");
     if (k == "heg") return build_heg(a);
+    if (k == "heg3d") return build_heg3d(a);
     if (k == "crystal") return build_crystal(a);
     if (k == "exciton") return build_exciton(a);
     if (k == "dipoles") return build_dipoles(a);
@@ -850,6 +1033,18 @@ int run(const std::string& mode, const Args& a) {
     }
     WalkerEnsemble ens(nw, sys->groups, sys->dim, sys->cell);
     initialize(ens, *sys, init_seed);
+    // pos_file=PATH: the walkers' positions instead, whitespace-separated AoS [w][p][d]
+    if (const std::string pf = gets(a, "pos_file", ""); !pf.empty()) {
+        std::FILE* f = std::fopen(pf.c_str(), "r");
+        if (!f) throw std::runtime_error("cannot open " + pf);
+        std::vector<double> pos(sys->np * sys->dim);
+        for (Walker& w : ens.walkers()) {
+            for (double& x : pos)
+                if (std::fscanf(f, "%lf", &x) != 1) throw std::runtime_error("short pos_file " + pf);
+            w.set_positions(pos);
+        }
+        std::fclose(f);
+    }
 
     Json out;
     out.open('{');

@@ -59,6 +59,17 @@ SYSTEMS = {
     # the crystal with its Drummond alpha_0, an alpha_2 term and L optimisable
     "crystal16p": dict(system="crystal", nx=4, ny=4, rs=40, drummond_free=1, alpha0=-2e-3,
                        alpha2=3e-8, gauss_free=1),
+    # 3-D electron gases (the reference's backflow determinant, Drummond
+    # Jastrow and kinetic energy in a cubic cell, plane waves passed
+    # directly): the 54-electron backflow gas at r_s = 5, a 14-electron one,
+    # and the 54-electron plain plane-wave determinant without a Jastrow
+    "heg54bf3d": dict(system="heg3d", nu=27, nd=27, rs=5, alpha0=-0.01),
+    "heg14bf3d": dict(system="heg3d", nu=7, nd=7, rs=5, alpha0=-0.01, bf_un1=0.02),
+    "heg54pw3d": dict(system="heg3d", nu=27, nd=27, rs=5, bf=0, jastrow=0),
+    # the same gases with cusp-free Jastrows, for DMC: with the kinetic energy
+    # alone a Coulomb cusp leaves an unbalanced 1/r local energy
+    "heg14bf3ds": dict(system="heg3d", nu=7, nd=7, rs=5, alpha0=-0.01, bf_un1=0.02, cusp=0),
+    "heg54bf3ds": dict(system="heg3d", nu=27, nd=27, rs=5, alpha0=-0.01, cusp=0),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
@@ -71,6 +82,10 @@ VMC = {
     "heg10bf": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=225.0),
     "heg10bf_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=225.0, drift=1),
     "crystal120": dict(nw=4, seed=19, eq=0, acc=1, steps=2, substeps=1, tau=400.0),
+    "heg54bf3d": dict(nw=4, seed=11, eq=0, acc=1, steps=2, substeps=1, tau=4.0),
+    "heg14bf3d": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=4.0),
+    "heg14bf3d_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=1.0, drift=1),
+    "heg54pw3d": dict(nw=4, seed=11, eq=0, acc=1, steps=2, substeps=1, tau=4.0),
 }
 DMC = {
     "exciton": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.05),
@@ -79,6 +94,8 @@ DMC = {
     "heg10t": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
     "heg10bf": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=2.0),
     "heg42": dict(nw=16, seed=5, eq=1, acc=2, steps=3, substeps=1, tau=0.5),
+    "heg14bf3ds": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.005),
+    "heg54bf3ds": dict(nw=8, seed=5, eq=1, acc=1, steps=2, substeps=1, tau=0.005),
 }
 
 # Fewer threads (streams, crowds) than walkers: contiguous walker ranges.
@@ -189,11 +206,17 @@ def chain_fixtures(only=None):
         dump(f"chain_{name}.json", r)
 
 
+# systems that serve only DMC fixtures (no evaluation fixture)
+NO_EVAL = {"heg14bf3ds", "heg54bf3ds"}
+
+
 def main(only=None):
     for name, args in SYSTEMS.items():
         if only and name not in only:
             continue
         dump(f"setup_{name}.json", run_ref_harness("setup", **args))
+        if name in NO_EVAL:
+            continue
         ev = run_ref_harness("eval", nw=4, seed=12345, **args)
         ev.pop("mode", None)
         dump(f"eval_{name}.json", ev)

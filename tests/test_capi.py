@@ -30,7 +30,7 @@ def test_library_loads_and_exports_every_symbol():
     for name in header_functions():
         assert hasattr(lib, name), name
     assert set(_capi.EXPORTS) >= set(header_functions())
-    assert lib.alea_gpu_abi_version() == 1
+    assert lib.alea_gpu_abi_version() == 2
 
 
 def test_struct_layout_matches_header():

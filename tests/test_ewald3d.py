@@ -3,7 +3,7 @@ breakup with the 3-D radial kernel; the reference refuses 3-D Ewald) against
 the known answers of cubic crystals: the Madelung constants of rock salt
 (NaCl, 1.747564594633) and caesium chloride (CsCl, 1.762674773070), from
 E = Σ_{i<j} q_i q_j [1/r − f_l(r)] (minimum image, r < r_c) + Σ_k w_k |ρ(k)|²
-− ½ f_l(0) Σ q_i², evaluated here from the tables alone, to 5e-8 (the
+− ½ f_l(0) Σ q_i², evaluated from the tables alone (oracle/ewald3d.py), to 5e-8 (the
 breakup's 20 knots leave ~1e-8; the reference's 2-D known answer is held to
 1e-6).
 """
@@ -11,42 +11,11 @@ import numpy as np
 import pytest
 
 from alea_b200 import setup as S
-
-
-def _hermite(t):
-    u = 1.0 - t
-    return np.array([u ** 3 * (1 + 3 * t + 6 * t * t), t * u ** 3 * (1 + 3 * t), 0.5 * t * t * u ** 3])
-
-
-def _f_long(sp, r):
-    """The breakup's quintic Hermite long-range part at r < r_c."""
-    s = np.array(sp["scaled"]).reshape(-1, 3)
-    x = r * sp["inv_delta"]
-    i = min(int(x), sp["n_knots"] - 2)
-    t = x - i
-    hl, hr = _hermite(t), _hermite(1.0 - t)
-    return float(s[i] @ hl + s[i + 1] @ (hr * np.array([1.0, -1.0, 1.0])))
+from oracle import ewald3d
 
 
 def _energy(lattice, pos, q, e):
-    lat = np.asarray(lattice, float).reshape(3, 3)
-    inv = np.linalg.inv(lat)
-    rc = e["r_cut"]
-    er = 0.0
-    for i in range(len(q)):
-        for j in range(i + 1, len(q)):
-            d = pos[i] - pos[j]
-            f = d @ inv
-            d = (f - np.rint(f)) @ lat
-            r = float(np.linalg.norm(d))
-            if r < rc:
-                er += q[i] * q[j] * (1.0 / r - _f_long(e["spline"], r))
-    k = np.stack([e["kx"], e["ky"], e["kz"]], axis=1)
-    rho = np.exp(1j * pos @ k.T).T @ q
-    ek = float(np.sum(np.array(e["weight"]) * np.abs(rho) ** 2))
-    self_ = -0.5 * e["v_long_zero"] * float(np.sum(q * q))
-    bg = -0.5 * float(np.sum(q)) ** 2 * e["sr_k0"]
-    return er + ek + self_ + bg
+    return ewald3d.energy(lattice, pos, q, e)
 
 
 @pytest.fixture(scope="module")

@@ -1,0 +1,197 @@
+"""Three-dimensional walkers (alea_bf3d.cu): the backflow electron gas of the
+benchmark's fourth configuration (54 electrons, r_s = 5) and smaller gases,
+against the compiled reference's own dimension-generic components and drivers
+(BackflowSlaterDeterminant, DrummondJastrow, Kinetic, VMC::run, DMC::run,
+fixtures from tests/golden/make_fixtures.py; the reference builds no 3-D
+plane-wave shells and has no 3-D Ewald, so its systems carry the plane waves
+directly and the kinetic energy alone).  The 3-D Ewald energy is checked
+against the oracle's restatement (oracle/ewald3d.py, pinned by Madelung
+constants).
+
+Known answer: a determinant of plane waves without Jastrow or backflow has
+E_L = Σ_k k²/2 exactly.
+
+The DMC runs use cusp-free Jastrows (Drummond with Γ = 0): with the
+kinetic energy alone, a Coulomb cusp leaves an unbalanced 1/r local energy
+whose weights overflow within a step.
+
+Tolerances: ln|psi| differences, gradients, Laplacians and E_L 1e-10
+relative (1e-9 for Laplacians); Metropolis VMC positions bit for bit;
+drift-move positions 1e-9; DMC block energies 1e-10 and identical
+populations.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+
+def rel(a, b, floor=1e-12):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
+# ─────────────────────────── CPU: fixtures and host setup ──────────────────
+
+
+def test_plane_wave_kinetic_known_answer_in_reference_fixture():
+    """The reference's own E_L of the plain 54-electron plane-wave
+    determinant (no Jastrow, no backflow) is Σ k²/2 for every walker."""
+    s = golden("setup_heg54pw3d.json")
+    ev = golden("eval_heg54pw3d.json")
+    k2 = sum(float(np.sum(np.array(b["k"]) ** 2)) for b in s["slater"])
+    assert np.allclose(ev["local_energy"], 0.5 * k2, rtol=1e-12, atol=0)
+    assert np.allclose(ev["kinetic"], 0.5 * k2, rtol=1e-12, atol=0)
+
+
+def test_host_setup_matches_reference_system():
+    """alea_gpu_setup_heg3d builds the fixture's system: the same cubic cell,
+    plane waves (shell order, cos/sin), backflow channels and Drummond terms;
+    its 3-D Ewald tables meet the Madelung-pinned energy formula."""
+    from alea_b200 import setup as S
+    ref = golden("setup_heg54bf3d.json")
+    st = S.heg3d(27, 27, 5.0, bf_like=0.1, bf_unlike=0.1, alpha0=-0.01)
+    d = st.desc
+    assert np.allclose(d["cell"]["vectors"], ref["cell"]["vectors"], rtol=1e-15)
+    for a, b in zip(d["backflow"], ref["backflow"]):
+        assert (a["first"], a["last"]) == (b["first"], b["last"])
+        assert np.allclose(a["k"], b["k"], rtol=0, atol=1e-15)
+        assert list(map(int, a["is_sin"])) == list(map(int, b["is_sin"]))
+        for ca, cb in zip(a["channels"], b["channels"]):
+            assert (ca["source_first"], ca["source_last"], ca["C"]) == (cb["source_first"], cb["source_last"], cb["C"])
+            assert np.allclose(ca["coeffs"], cb["coeffs"], rtol=1e-15)
+            assert ca["L"] == pytest.approx(cb["L"], rel=1e-15)
+    for a, b in zip(d["drummond"], ref["drummond"]):
+        assert (a["C"], a["gamma"]) == (b["C"], b["gamma"])
+        assert a["L"] == pytest.approx(b["L"], rel=1e-15)
+        assert [list(map(int, p)) for p in a["pairs"]] == [list(map(int, p)) for p in b["pairs"]]
+    # the constant of the sum: self and background energies of 54 unit charges
+    e = d["ewald"]
+    assert e["self_energy"] == pytest.approx(-0.5 * e["v_long_zero"] * 54, rel=1e-15)
+    assert e["background_energy"] == pytest.approx(-0.5 * 54 ** 2 * e["sr_k0"], rel=1e-15)
+    pos = st.positions(7, 3)
+    assert pos.shape == (3, 54, 3)
+    L = d["cell"]["vectors"][0]
+    assert np.all(np.abs(pos) <= 0.5 * L)
+    st.close()
+
+
+# ─────────────────────────── GPU: against the reference ────────────────────
+
+
+def walkers(desc, capacity):
+    import alea_b200
+    return alea_b200.Walkers(desc, capacity=capacity)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["heg54bf3d", "heg14bf3d", "heg54pw3d"])
+def test_evaluate_matches_reference(name):
+    setup = golden(f"setup_{name}.json")
+    ev = golden(f"eval_{name}.json")
+    pos = np.array(ev["positions"])
+    g = walkers(setup, len(pos))
+    g.upload(pos)
+    d = g.download()
+    nw, n = len(pos), setup["np"] * 3
+    assert rel(d["local_energy"], ev["local_energy"]) < 1e-10
+    lp, lr = d["log_psi"], np.array(ev["log_psi"])
+    assert np.max(np.abs((lp - lp[0]) - (lr - lr[0]))) < 1e-10 * max(1.0, np.abs(lr).max())
+    gr = np.array(ev["grad"]).reshape(n, nw).T
+    assert np.max(np.abs(d["grad"] - gr)) < 1e-10 * max(1.0, np.abs(gr).max())
+    lr_ = np.array(ev["lap"]).reshape(n, nw).T
+    assert np.max(np.abs(d["lap"] - lr_)) < 1e-9 * max(1.0, np.abs(lr_).max())
+    if name == "heg54pw3d":
+        k2 = sum(float(np.sum(np.array(b["k"]) ** 2)) for b in setup["slater"])
+        assert np.allclose(d["local_energy"], 0.5 * k2, rtol=1e-12, atol=0)
+    g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["heg54bf3d", "heg14bf3d", "heg14bf3d_drift", "heg54pw3d"])
+def test_vmc_matches_reference(name):
+    r = golden(f"vmc_{name}.json")
+    p = r["params"]
+    g = walkers(golden(f"setup_{r['system']}.json"), p["nw"])
+    g.upload(np.array(r["initial_positions"]))
+    res, blocks = g.vmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], p["nw"], p["seed"],
+                            drift=bool(p.get("drift", 0)))
+    fin = np.array(r["final_positions"]).reshape(p["nw"], -1)
+    got = g.download()["positions"]
+    if p.get("drift", 0):
+        assert np.max(np.abs(got - fin)) < 1e-9 * np.abs(fin).max()
+    else:
+        assert np.array_equal(got, fin)
+    assert res.acceptance == pytest.approx(r["acceptance"], rel=1e-15)
+    assert rel(blocks, r["block_energies"]) < 1e-10
+    g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["heg14bf3ds", "heg54bf3ds"])
+def test_dmc_matches_reference(name):
+    r = golden(f"dmc_{name}.json")
+    p = r["params"]
+    nw = p["nw"]
+    g = walkers(golden(f"setup_{name}.json"), 4 * nw + 4)
+    g.upload(np.array(r["initial_positions"]))
+    res, blocks = g.dmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], nw, p["seed"], target=nw)
+    ws = np.array(r["weight_sum"])            # the accumulation steps' sums
+    we = np.array(r["weighted_energy_sum"])
+    want = [we[b * p["steps"]:(b + 1) * p["steps"]].sum() / ws[b * p["steps"]:(b + 1) * p["steps"]].sum()
+            for b in range(p["acc"])]
+    assert rel(blocks, want) < 1e-10
+    fin = np.array(r["final_positions"]).reshape(-1, golden(f"setup_{name}.json")["np"] * 3)
+    assert g.nw == fin.shape[0]
+    assert np.max(np.abs(g.download()["positions"] - fin)) < 1e-9 * np.abs(fin).max()
+    g.close()
+
+
+@pytest.mark.gpu
+def test_ewald_potential_matches_oracle():
+    """The benchmark system with its 3-D Ewald sum: E_L minus the same
+    walkers' E_L without it is the oracle's electrostatic energy."""
+    from alea_b200 import setup as S
+    from oracle import ewald3d
+    st = S.heg3d(27, 27, 5.0)
+    d = st.desc
+    pos = st.positions(11, 4)
+    full = walkers(d, 4)
+    full.upload(pos)
+    e_full = full.download()["local_energy"]
+    bare = dict(d)
+    bare.pop("ewald")
+    kin = walkers(bare, 4)
+    kin.upload(pos)
+    e_kin = kin.download()["local_energy"]
+    q = np.full(54, -1.0)
+    want = [ewald3d.energy(d["cell"]["vectors"], pos[w].reshape(54, 3), q, d["ewald"]) for w in range(4)]
+    assert rel(e_full - e_kin, want) < 1e-10
+    full.close()
+    kin.close()
+    st.close()
+
+
+@pytest.mark.gpu
+def test_benchmark_population_dmc_step():
+    """The fourth configuration's shape: 4096 walkers of the 54-electron
+    backflow gas with 3-D Ewald, a VMC step and a DMC advance + branch; every
+    energy finite, the population within the clip window."""
+    import alea_b200
+    from alea_b200 import setup as S
+    nw = 4096
+    st = S.heg3d(27, 27, 5.0)
+    g = walkers(st.desc, 2 * nw + 2)
+    g.upload(st.positions(2025, nw))
+    g.set_streams(3, alea_b200.STREAM_VMC, nw)
+    g.vmc_step(1.0, 1, False)
+    e = g.download()["local_energy"]
+    assert np.all(np.isfinite(e))
+    g.set_streams(5, alea_b200.STREAM_DMC, nw)
+    et = float(np.mean(e))
+    st_ = g.dmc_advance(0.02, 1, et, et, 1e30, 1e30)
+    assert np.isfinite(st_.energy_sum)
+    g.dmc_branch(np.array([1, 2, 3, 4], dtype=np.uint64), nw)
+    assert nw // 5 + 1 <= g.nw <= 2 * nw + 1
+    g.close()
+    st.close()
