@@ -160,13 +160,16 @@ __device__ __forceinline__ bool in_sources(const DevBFCh& C, int k) { return k >
 // reductions on the bits of |x| (order-preserving for non-negative doubles;
 // a NaN never wins); row k is scaled by 1/pivot, the other rows lose their
 // multiple of it (multipliers in `mult`), and the row exchanges (`perm`) are
-// undone as column exchanges at the end.  No block barrier: two warps invert
-// two determinants at once.
+// undone as column exchanges at the end.  |det| accumulates as a mantissa
+// and a binary exponent (one log at the end).  No block barrier: two warps
+// invert two determinants at once.  (A register-resident form, a column per
+// lane with the multipliers broadcast by shuffles, ran 2.3x slower here.)
 __device__ void gj_warp_signed(double* A, int N, double* mult, int* perm, double* out) {
     const unsigned all = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     __syncwarp();
-    double logdet = 0.0, sign = 1.0;
+    double mant = 1.0, sign = 1.0;   // |det| = mant · 2^ex, one log at the end
+    int ex = 0;
     bool bad = false;
     for (int k = 0; k < N; ++k) {
         double x = 0.0;
@@ -185,7 +188,9 @@ __device__ void gj_warp_signed(double* A, int N, double* mult, int* perm, double
         double diag = __shfl_sync(all, x, piv);
         if (none) diag = 0.0;
         bad |= diag == 0.0 || !isfinite(diag);
-        logdet += log(fabs(diag));
+        int e1 = 0, e2 = 0;
+        mant = frexp(mant * frexp(fabs(diag), &e1), &e2);
+        ex += e1 + e2;
         if (diag < 0.0) sign = -sign;
         if (piv != k) sign = -sign;
         const double inv = 1.0 / diag;
@@ -228,7 +233,7 @@ __device__ void gj_warp_signed(double* A, int N, double* mult, int* perm, double
         __syncwarp();
     }
     if (lane == 0) {
-        out[0] = logdet;
+        out[0] = log(mant) + ex * 0.69314718055994530942;
         out[1] = sign;
         out[2] = bad ? 0.0 : 1.0;
     }
