@@ -28,7 +28,7 @@
 // log|det M'| are kept pending and committed on acceptance.  The local energy's
 // refresh rebuilds x from the positions and every particle's ∇ and
 // per-dimension ∂² ln|D| from the committed A and F: T = Aᵀ∂∂φ, G^a = Aᵀ∂_aφ
-// and the Jacobian columns ∂x_t/∂r_k^β (ln|D|'s Laplacian is
+// (three N×N×N products on the FP64 tensor cores) and the Jacobian columns ∂x_t/∂r_k^β (ln|D|'s Laplacian is
 // Σ F·∂²x + Σ v v T − tr((G·v)²)).
 //
 // Record of a 3-D walker (doubles): positions, Jastrow ∇/∂², two zero planes
@@ -36,7 +36,7 @@
 // ∇/∂², the scalars, then per determinant x (3N), A (N²), F (3N) and
 // (log|det|, sign).  All of it is hot: it is staged in shared memory for the
 // whole sweep.
-#include "alea_walker.cuh"
+#include "alea_warp.cuh"
 
 namespace alea_gpu {
 
@@ -419,13 +419,31 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
             F[t * 3 + a] = acc;
         }
     }
-    // G^a[j][r] = Σ_m A[m][j] ∂_a φ_m(x_r);  T_t^{ab} = Σ_m A[m][t] ∂_a∂_b φ_m(x_t)
-    for (int e = threadIdx.x; e < 3 * N * N; e += NT) {
-        const int a = e / (N * N), jr = e % (N * N), j = jr / N, r = jr % N;
-        double acc = 0.0;
-        for (int m = 0; m < N; ++m) acc = fma(A[m * N + j], R[(r * N + m) * 4 + 1 + a], acc);
-        G[a * N * N + jr] = acc;
+    // G^a = Aᵀ (∂_a Φ)ᵀ, G^a[j][r] = Σ_m A[m][j] ∂_a φ_m(x_r): three N×N×N products
+    // on the FP64 tensor cores, 8×8 output tiles dealt to the warps, k in
+    // slabs of 4 (mma.sync m8n8k4 .f64; lane 4g + t holds P[g][t], Q[t][g]
+    // and C[g][2t..2t+1] of a tile, zero-padded beyond N)
+    {
+        const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3, warp = threadIdx.x >> 5;
+        const int nt = (N + 7) >> 3, nk = (N + 3) >> 2;
+        for (int job = warp; job < 3 * nt * nt; job += NT / 32) {
+            const int a = job / (nt * nt), jt = (job / nt) % nt, rt = job % nt;
+            const int j = jt * 8 + g, r = rt * 8 + g;
+            double c[2] = {0.0, 0.0};
+            for (int kt = 0; kt < nk; ++kt) {
+                const int m = kt * 4 + tq;
+                const double pa = (j < N && m < N) ? A[m * N + j] : 0.0;
+                const double qb = (r < N && m < N) ? R[(r * N + m) * 4 + 1 + a] : 0.0;
+                dmma_m8n8k4(c, pa, qb);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int rc = rt * 8 + 2 * tq + i;
+                if (j < N && rc < N) G[a * N * N + j * N + rc] = c[i];
+            }
+        }
     }
+    // T_t^{ab} = Σ_m A[m][t] ∂_a∂_b φ_m(x_t)
     for (int e = threadIdx.x; e < 6 * N; e += NT) {
         const int t = e / 6, q = e % 6;
         const int a = q < 3 ? q : (q == 3 ? 0 : (q == 4 ? 0 : 1));

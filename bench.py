@@ -232,6 +232,26 @@ def run_reference_cpu(nw: int, steps: int, warmup: int, seed: int):
                                   "sample": f"{nw} walkers x {steps} DMC steps, oracle restatement"}
 
 
+def reference_vmc_3d(nw: int, steps: int, seed: int):
+    """The compiled reference's VMC of the 3-D backflow gas on the host cores
+    (its own BackflowSlaterDeterminant, Drummond Jastrow and drivers; kinetic
+    energy only, since it has no 3-D Ewald sum): moves/s over `steps` sweeps
+    after one untimed sweep, or None without the compiled reference."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return None
+    threads = host_threads()
+    args = [harness, "bench", "method=vmc", "system=heg3d", "nu=27", "nd=27", "rs=5", "alpha0=-0.01",
+            f"nw={nw}", f"steps={steps + 1}", "tau=1.0", f"seed={seed}", f"threads={threads}"]
+    out = subprocess.run(args, capture_output=True, text=True, check=True,
+                         env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+    d = json.loads(out.stdout)
+    dt = float(np.sum(np.diff(np.array(d["stamps"]))[-steps:]))
+    return {"value": nw * 54 * steps / dt, "unit": UNIT, "kind": "reference", "cores": int(d["threads"]),
+            "sample": f"{nw} walkers x {steps} VMC sweeps after 1 untimed, same trial function, "
+                      "kinetic energy only (the reference has no 3-D Ewald)"}
+
+
 def reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -567,10 +587,12 @@ def gpu_arm(a):
         g3 = S.heg3d(27, 27, 5.0)
         others["backflow_heg54_3d"] = dict(
             vmc_sweeps(g3.desc, g3.positions(seed + 14, 4096), 4096, 2, 1.0),
-            sweep="3-D CTA sweep (alea_bf3d.cu), one pivoted Gauss-Jordan per determinant per move",
+            sweep="3-D CTA sweep (alea_bf3d.cu), one warp Gauss-Jordan per spin determinant per move",
             system="3-D electron gas N=54 (27+27) rs=5, backflow determinants of plane waves (C=3, c0=0.1, "
                    "L = half the cell side), Drummond Jastrows, 3-D Ewald (%d k-vectors)" % len(g3.desc["ewald"]["weight"]))
         g3.close()
+        if rank == 0:
+            others["backflow_heg54_3d"]["cpu_reference"] = reference_vmc_3d(256, 3, seed)
 
     # ── the serving mix through the packed server (config 5), rank 0 only ──
     serving = None

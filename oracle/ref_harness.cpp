@@ -931,10 +931,102 @@ std::unique_ptr<System> build_heg3d(const Args& a) {
     return s;
 }
 
+// Open 3-D cell, the shape of the reference's own 3-D backflow test
+// (tests/test_backflow_slater.cpp:198-214): three like-spin particles [0, 3)
+// in Gaussian orbitals of one shared width, displaced by each other (zero
+// slope, c_0 = 0.2, c_2 = -0.04, L = 2.4) and by two holes [3, 5) (c_0 =
+// -0.12, c_1 = 0.08, c_2 = 0.03, L = 2.8); a Padé Jastrow a r/(1 + b r)
+// between the particles and the holes; kinetic energy and the open Coulomb
+// attraction between the two groups.  Initial positions uniform in [-L/2, L/2)³.
+std::unique_ptr<System> build_gauss3d(const Args& a) {
+    auto s = std::make_unique<System>();
+    s->kind = "gauss3d";
+    s->dim = 3;
+    s->np = 5;
+    s->cell = SimulationCell(3);
+    s->L_open = getd(a, "L", 2.0);
+    s->groups.push_back(make_group("particles", 0, 3, -1.0, 3));
+    s->groups.push_back(make_group("holes", 3, 2, 1.0, 3));
+    s->ham.add_component(std::make_unique<Kinetic>(s->groups));
+    s->ham.add_component(std::make_unique<CoulombTerm>(s->groups[0], s->groups[1], 1.0));
+    const std::vector<double> centers{-0.9, 0.1, 0.2, 0.8, 0.3, -0.4, 0.1, -0.8, 0.6};
+    const std::vector<double> alphas{0.5, 0.5, 0.5};
+    Json& j = s->setup;
+    j.open('{');
+    j.ks("kind", "gauss3d");
+    j.ki("dim", 3);
+    j.ki("np", 5);
+    dump_cell(j, s->cell);
+    dump_groups(j, s->groups);
+    const double c0 = 0.2, L1 = 2.4;
+    std::vector<BackflowSlaterDeterminant::Channel> chans(2);
+    chans[0].source_first = 0;
+    chans[0].source_last = 3;
+    chans[0].truncation = 3;
+    chans[0].params = {Parameter{"", c0, false}, Parameter{"", -0.04, false}, Parameter{"", L1, true}};
+    chans[1].source_first = 3;
+    chans[1].source_last = 5;
+    chans[1].truncation = 3;
+    chans[1].params = {Parameter{"", -0.12, false}, Parameter{"", 0.08, false}, Parameter{"", 0.03, false},
+                       Parameter{"", 2.8, true}};
+    j.key("backflow");
+    j.open('[');
+    j.open('{');
+    j.ki("first", 0);
+    j.ki("last", 3);
+    j.ks("type", "gaussian");
+    j.arr("centers", centers);
+    j.arr("alphas", alphas);
+    j.key("channels");
+    j.open('[');
+    const std::vector<std::vector<double>> full{{c0, 3.0 * c0 / L1, -0.04}, {-0.12, 0.08, 0.03}};
+    const double Ls[2] = {L1, 2.8};
+    for (int q = 0; q < 2; ++q) {
+        j.open('{');
+        j.ki("source_first", static_cast<long long>(chans[q].source_first));
+        j.ki("source_last", static_cast<long long>(chans[q].source_last));
+        j.ki("C", 3);
+        j.arr("coeffs", full[q]);
+        j.kv("L", Ls[q]);
+        j.ki("zero_slope", q == 0 ? 1 : 0);
+        j.close('}');
+    }
+    j.close(']');
+    j.close('}');
+    j.close(']');
+    std::vector<BackflowSlaterDeterminant::Block> bb;
+    bb.push_back({0, 3, std::make_unique<GaussianOrbitalSet>(3, centers, alphas)});
+    s->psi.add_component(std::make_unique<BackflowSlaterDeterminant>(std::move(bb), std::move(chans), s->cell));
+    const double pa = getd(a, "pade_a", -0.3), pb = getd(a, "pade_b", 0.5);
+    std::vector<Parameter> params{Parameter{"a1", pa, true}, Parameter{"pade_0", pb, true}};
+    s->psi.add_component(std::make_unique<PadeJastrow>(1, 1, s->groups[0], s->groups[1], params));
+    j.key("pade");
+    j.open('[');
+    j.open('{');
+    j.arr("ga", std::vector<double>{0, 3});
+    j.arr("gb", std::vector<double>{3, 5});
+    j.arr("a", std::vector<double>{pa});
+    j.arr("b", std::vector<double>{pb});
+    j.close('}');
+    j.close(']');
+    j.key("coulomb");
+    j.open('[');
+    j.open('{');
+    j.arr("ga", std::vector<double>{0, 3});
+    j.arr("gb", std::vector<double>{3, 5});
+    j.kv("coef", -1.0);
+    j.close('}');
+    j.close(']');
+    j.kv("L_open", s->L_open);
+    j.close('}');
+    return s;
+}
+
 std::unique_ptr<System> build_system(const Args& a) {
     const std::string k = gets(a, "system", "heg");
     if (k == "heg") return build_heg(a);
     if (k == "heg3d") return build_heg3d(a);
+    if (k == "gauss3d") return build_gauss3d(a);
     if (k == "crystal") return build_crystal(a);
     if (k == "exciton") return build_exciton(a);
     if (k == "dipoles") return build_dipoles(a);

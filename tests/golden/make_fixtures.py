@@ -70,6 +70,9 @@ SYSTEMS = {
     # alone a Coulomb cusp leaves an unbalanced 1/r local energy
     "heg14bf3ds": dict(system="heg3d", nu=7, nd=7, rs=5, alpha0=-0.01, bf_un1=0.02, cusp=0),
     "heg54bf3ds": dict(system="heg3d", nu=27, nd=27, rs=5, alpha0=-0.01, cusp=0),
+    # open 3-D cell, the reference's own 3-D backflow test shape: Gaussian
+    # orbitals, two backflow channels, a Padé Jastrow and open Coulomb
+    "gauss3d": dict(system="gauss3d"),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
@@ -86,6 +89,8 @@ VMC = {
     "heg14bf3d": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=4.0),
     "heg14bf3d_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=1.0, drift=1),
     "heg54pw3d": dict(nw=4, seed=11, eq=0, acc=1, steps=2, substeps=1, tau=4.0),
+    "gauss3d": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.1),
+    "gauss3d_drift": dict(nw=6, seed=13, eq=1, acc=2, steps=3, substeps=1, tau=0.05, drift=1),
 }
 DMC = {
     "exciton": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.05),
@@ -96,6 +101,7 @@ DMC = {
     "heg42": dict(nw=16, seed=5, eq=1, acc=2, steps=3, substeps=1, tau=0.5),
     "heg14bf3ds": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.005),
     "heg54bf3ds": dict(nw=8, seed=5, eq=1, acc=1, steps=2, substeps=1, tau=0.005),
+    "gauss3d": dict(nw=8, seed=5, eq=1, acc=2, steps=4, substeps=2, tau=0.01),
 }
 
 # Fewer threads (streams, crowds) than walkers: contiguous walker ranges.

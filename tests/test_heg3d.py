@@ -1,7 +1,10 @@
 """Three-dimensional walkers (alea_bf3d.cu): the backflow electron gas of the
 benchmark's fourth configuration (54 electrons, r_s = 5) and smaller gases,
-against the compiled reference's own dimension-generic components and drivers
-(BackflowSlaterDeterminant, DrummondJastrow, Kinetic, VMC::run, DMC::run,
+and the open 3-D cell of the reference's own 3-D backflow test (Gaussian
+orbitals, two backflow channels, a Padé Jastrow, open Coulomb), against the
+compiled reference's own dimension-generic components and drivers
+(BackflowSlaterDeterminant, DrummondJastrow, PadeJastrow, Kinetic,
+CoulombTerm, VMC::run, DMC::run,
 fixtures from tests/golden/make_fixtures.py; the reference builds no 3-D
 plane-wave shells and has no 3-D Ewald, so its systems carry the plane waves
 directly and the kinetic energy alone).  The 3-D Ewald energy is checked
@@ -42,6 +45,16 @@ def test_plane_wave_kinetic_known_answer_in_reference_fixture():
     k2 = sum(float(np.sum(np.array(b["k"]) ** 2)) for b in s["slater"])
     assert np.allclose(ev["local_energy"], 0.5 * k2, rtol=1e-12, atol=0)
     assert np.allclose(ev["kinetic"], 0.5 * k2, rtol=1e-12, atol=0)
+
+
+def test_open_gaussian_fixture_potential():
+    """The open 3-D fixture's E_L minus its kinetic part is the open Coulomb
+    attraction between the three particles and the two holes."""
+    ev = golden("eval_gauss3d.json")
+    for w, pos in enumerate(ev["positions"]):
+        x = np.array(pos).reshape(5, 3)
+        v = sum(-1.0 / np.linalg.norm(x[i] - x[j]) for i in range(3) for j in range(3, 5))
+        assert ev["local_energy"][w] - ev["kinetic"][w] == pytest.approx(v, rel=1e-12)
 
 
 def test_host_setup_matches_reference_system():
@@ -85,7 +98,7 @@ def walkers(desc, capacity):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["heg54bf3d", "heg14bf3d", "heg54pw3d"])
+@pytest.mark.parametrize("name", ["heg54bf3d", "heg14bf3d", "heg54pw3d", "gauss3d"])
 def test_evaluate_matches_reference(name):
     setup = golden(f"setup_{name}.json")
     ev = golden(f"eval_{name}.json")
@@ -108,7 +121,8 @@ def test_evaluate_matches_reference(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["heg54bf3d", "heg14bf3d", "heg14bf3d_drift", "heg54pw3d"])
+@pytest.mark.parametrize("name", ["heg54bf3d", "heg14bf3d", "heg14bf3d_drift", "heg54pw3d", "gauss3d",
+                                  "gauss3d_drift"])
 def test_vmc_matches_reference(name):
     r = golden(f"vmc_{name}.json")
     p = r["params"]
@@ -128,7 +142,7 @@ def test_vmc_matches_reference(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["heg14bf3ds", "heg54bf3ds"])
+@pytest.mark.parametrize("name", ["heg14bf3ds", "heg54bf3ds", "gauss3d"])
 def test_dmc_matches_reference(name):
     r = golden(f"dmc_{name}.json")
     p = r["params"]
