@@ -35,7 +35,7 @@
 // (the k-space planes of the 2-D layout, read by the download), determinant
 // ∇/∂², the scalars, then per determinant x (3N), A (N²), F (3N) and
 // (log|det|, sign).  All of it is hot: it is staged in shared memory for the
-// whole sweep.
+// whole sweep, in and out as one bulk copy each.
 #include "alea_warp.cuh"
 
 namespace alea_gpu {
@@ -47,7 +47,7 @@ constexpr int kNT3 = 128;
 // misc slots of the 3-D kernels
 enum : int {
     T_LOGR = 0, T_SIGN, T_ACC, T_ERR, T_U, T_SCF, T_GO /* 3 */ = 6, T_GN /* 3 */ = 9, T_LS /* 3 */ = 12,
-    T_BAD = 15
+    T_BAD = 15, T_JG /* 3: p's new Jastrow gradient */ = 16, T_JL /* 3: and Laplacian */ = 19
 };
 
 struct V3 {
@@ -348,8 +348,8 @@ __device__ double jastrow_all(const DevSys& s, const V3& v) {
 // added into sg/sl, from the committed A and F (refresh_walker); with
 // `invert`, A, F and (log|det|, sign) are first computed anew by pivoted
 // Gauss-Jordan (evaluate_batch).  Work area: M (N²), orbital rows
-// [(t·N + m)·4 + (φ, ∂x, ∂y, ∂z)] (4N²), G^a[j][r] (3N²), T (6N),
-// Jacobian columns (9N), their rows' F·∂²x (3N).
+// [(t·N + m)·4 + (φ, ∂x, ∂y, ∂z)] (4N²), G^a[j][r] (3N²), T (6N), the x
+// rebuild's slice sums (12N; 48N for the per-particle warps when N < 12).
 template <int NT>
 __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, bool invert) {
     const DevBF& D = s.bf[d];
@@ -363,7 +363,6 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
     double* G = R + 4 * N * N;
     double* T = G + 3 * N * N;
     double* J = T + 6 * N;
-    double* FS = J + 9 * N;
     __syncthreads();
     {   // x from the positions: row t's source sums in 4 slices (one thread per
         // row and slice, partial sums in J's area), then added in slice order
@@ -463,17 +462,25 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
         const int q = a == b ? a : (a == 0 ? (b == 1 ? 3 : 4) : 5);
         return T[t * 6 + q];
     };
-    for (int k = 0; k < np; ++k) {
+    // Every particle k's derivatives, one warp per particle (k = warp, warp +
+    // NT/32, ...): no block barrier inside.  Each warp's Jacobian columns and
+    // their F·∂²x rows (12N) live in R's area, free once G and T are formed,
+    // or from J on when R is smaller than 48N (N < 12: the host sizes the
+    // area for it).
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* Jw = (N >= 12 ? R : J) + warp * 12 * N;   // [β][t·3 + a] (9N), then F·∂²x [β][t] (3N)
+    double* FSw = Jw + 9 * N;
+    for (int k = warp; k < np; k += NT / 32) {
         bool hit = k >= D.first && k < D.last;
         for (int c = 0; c < D.nch && !hit; ++c) hit = in_sources(D.ch[c], k);
         if (!hit) continue;
         const double* rk = v.pos + k * 3;
         const int tk = (k >= D.first && k < D.last) ? k - D.first : -1;
-        // k's own row: Σ_j B(r_kj) and Σ_j F_k·S(r_kj) over the sources, spread over the CTA
+        // k's own row: Σ_j B(r_kj) and Σ_j F_k·S(r_kj) over the sources, over the warp
         double own[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (tk >= 0) {
             const double* Fk = F + tk * 3;
-            for (int j = threadIdx.x; j < np; j += NT) {
+            for (int j = lane; j < np; j += 32) {
                 if (j == k) continue;
                 for (int c = 0; c < D.nch; ++c) {
                     if (!in_sources(D.ch[c], j)) continue;
@@ -488,10 +495,11 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
                         }
                 }
             }
-            block_sum<NT>(own, v.red);
+#pragma unroll
+            for (int q = 0; q < 12; ++q) own[q] = warp_sum(own[q]);
         }
-        // Jacobian columns J[β][t·3 + a] = ∂x_t^a/∂r_k^β and F_t·∂²x_t/∂(r_k^β)² per row, FS[β][t]
-        for (int t = threadIdx.x; t < N; t += NT) {
+        // Jacobian columns Jw[β][t·3 + a] = ∂x_t^a/∂r_k^β and F_t·∂²x_t/∂(r_k^β)², lane = row
+        for (int t = lane; t < N; t += 32) {
             double vj[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, fs[3] = {0, 0, 0};
             const double* Ft = F + t * 3;
             if (t == tk) {
@@ -516,18 +524,18 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
                 }
             }
 #pragma unroll
-            for (int b = 0; b < 3; ++b)
+            for (int b = 0; b < 3; ++b) {
 #pragma unroll
-                for (int a = 0; a < 3; ++a) J[b * 3 * N + t * 3 + a] = vj[b * 3 + a];
-#pragma unroll
-            for (int b = 0; b < 3; ++b) FS[b * N + t] = fs[b];
+                for (int a = 0; a < 3; ++a) Jw[b * 3 * N + t * 3 + a] = vj[b * 3 + a];
+                FSw[b * N + t] = fs[b];
+            }
         }
-        __syncthreads();
-        // ∂_k ln|D|^β = Σ_t F_t·J_β;  ∂²: Σ F·S + Σ_t J T J - Σ_{j,r} U_jr U_rj, U = Σ_a G^a J^a
+        __syncwarp();
+        // ∂_k ln|D|^β = Σ_t F_t·J_β;  ∂²: Σ F·∂²x + Σ_t J T J - Σ_{j,r} U_jr U_rj, U = Σ_a G^a J^a
         double acc[6] = {0, 0, 0, 0, 0, 0};
-        for (int e = threadIdx.x; e < 3 * N; e += NT) {
+        for (int e = lane; e < 3 * N; e += 32) {
             const int b = e / N, t = e % N;
-            const double* vt = J + b * 3 * N + t * 3;
+            const double* vt = Jw + b * 3 * N + t * 3;
             double gg = 0.0, tt = 0.0;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -536,11 +544,11 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
                 for (int c = 0; c < 3; ++c) tt += vt[a] * vt[c] * Tab(t, a, c);
             }
             acc[b] += gg;
-            acc[3 + b] += tt + FS[b * N + t];
+            acc[3 + b] += tt + FSw[b * N + t];
         }
-        for (int e = threadIdx.x; e < 3 * N * N; e += NT) {
+        for (int e = lane; e < 3 * N * N; e += 32) {
             const int b = e / (N * N), jr = e % (N * N), j = jr / N, r = jr % N;
-            const double* vb = J + b * 3 * N;
+            const double* vb = Jw + b * 3 * N;
             double u1 = 0.0, u2 = 0.0;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -549,15 +557,17 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
             }
             acc[3 + b] -= u1 * u2;
         }
-        block_sum<NT>(acc, v.red);
-        if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
+        if (lane == 0)
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 v.sg[k * 3 + b] += acc[b];
                 v.sl[k * 3 + b] += acc[3 + b];
             }
-        __syncthreads();
+        __syncwarp();
     }
+    __syncthreads();
 }
 
 // ───────────────────────── local energy ─────────────────────────────────
@@ -644,13 +654,40 @@ __device__ __forceinline__ bool bf_touches(const DevBF& D, int k) {
     return false;
 }
 
+// The pair terms' change of ln J when p moves to v.newpos, for the partner
+// j, and the partner's share of p's new Jastrow gradient and per-dimension
+// Laplacian: acc[0] += Δu, acc[1..3] += u'(r') r̂', acc[4..6] += u'' r̂_d² +
+// u'/r (1 - r̂_d²).
+__device__ __forceinline__ void jastrow_pair_change(const DevSys& s, const V3& v, int p, int j, double* acc) {
+    for (int t = 0; t < s.nterms; ++t) {
+        const DevTerm& T = s.terms[t];
+        if (!any_term_couples(T, p, j)) continue;
+        double del[3], u, du, d2u;
+        const double ro = dist3(s, v.pos + p * 3, v.pos + j * 3, del);
+        radial(T, ro, u, du, d2u);
+        acc[0] -= u;
+        const double rn = dist3(s, v.newpos, v.pos + j * 3, del);
+        radial(T, rn, u, du, d2u);
+        acc[0] += u;
+        const double ir = 1.0 / rn;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double dor = del[d] * ir;
+            acc[1 + d] += du * dor;
+            acc[4 + d] += d2u * dor * dor + du * ir * (1.0 - dor * dor);
+        }
+    }
+}
+
 // The proposal of p for every determinant it touches: pending x', A', F',
 // (log|det|', sign', regular) in each one's pending area; with `grad`, the
 // determinants' part of p's new gradient is added to misc[T_GN..].  The
 // phases run over the CTA for all touched determinants together, the
 // inversions on one warp per determinant (warp d inverts determinant d).
 // Move work area per determinant: ∇φ rows [(t·N + m)·3 + a] (3N²), the
-// Gauss-Jordan multipliers (N) and row exchanges (N ints).
+// Gauss-Jordan multipliers (N) and row exchanges (N ints).  While warps 0
+// and 1 invert, warps 2 and 3 form the Jastrow ratio and p's new Jastrow
+// gradient into misc (with fewer warps ratio3 forms them first).
 template <int NT>
 __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool grad) {
     const int np = s.np, nb = s.nbf, W = s.maxN;
@@ -717,8 +754,29 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
         const DevBF& D = s.bf[warp];
         double* mult = v.mwork + warp * mstride + 3L * D.n * D.n;
         gj_warp_signed(sm + D.pA, D.n, mult, reinterpret_cast<int*>(mult + D.n), sm + D.pM);
+    } else if (NT >= 128 && warp >= 2) {
+        // meanwhile warps 2 and 3: the Jastrow ratio and p's new Jastrow
+        // gradient and Laplacian, each warp's partial sums to v.red[64 + 8·(warp - 2)..]
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int j = threadIdx.x - 64; j < np; j += 64) {
+            if (j == p) continue;
+            jastrow_pair_change(s, v, p, j, acc);
+        }
+#pragma unroll
+        for (int q = 0; q < 7; ++q) acc[q] = warp_sum(acc[q]);
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int q = 0; q < 7; ++q) v.red[64 + 8 * (warp - 2) + q] = acc[q];
     }
     __syncthreads();
+    if (NT >= 128 && threadIdx.x == 0) {
+        v.misc[T_LOGR] = v.red[64] + v.red[72];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v.misc[T_JG + d] = v.misc[T_GN + d] = v.red[65 + d] + v.red[73 + d];
+            v.misc[T_JL + d] = v.red[68 + d] + v.red[76 + d];
+        }
+    }
     // F'_t = Σ_m A'[m][t] ∇φ_m(x'_t)
     for (int e = threadIdx.x; e < nb * W * 3; e += NT) {
         const int d = e / (W * 3), ta = e % (W * 3), t = ta / 3, a = ta % 3;
@@ -751,35 +809,22 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
 // proposal in v.newpos.
 template <int NT>
 __device__ void ratio3(const DevSys& s, const V3& v, double* sm, int p, bool grad) {
-    const int np = s.np;
-    // Jastrow: Δu and the Jastrow part of p's new gradient
-    double acc[4] = {0, 0, 0, 0};
-    for (int j = threadIdx.x; j < np; j += NT) {
-        if (j == p) continue;
-        for (int t = 0; t < s.nterms; ++t) {
-            const DevTerm& T = s.terms[t];
-            if (!any_term_couples(T, p, j)) continue;
-            double del[3], u, du, d2u;
-            const double ro = dist3(s, v.pos + p * 3, v.pos + j * 3, del);
-            radial(T, ro, u, du, d2u);
-            acc[0] -= u;
-            const double rn = dist3(s, v.newpos, v.pos + j * 3, del);
-            radial(T, rn, u, du, d2u);
-            acc[0] += u;
-            const double ir = 1.0 / rn;
-            acc[1] += du * del[0] * ir;
-            acc[2] += du * del[1] * ir;
-            acc[3] += du * del[2] * ir;
-        }
-    }
-    block_sum<NT>(acc, v.red);
     if (threadIdx.x == 0) {
-        v.misc[T_LOGR] = acc[0];
         v.misc[T_SIGN] = 1.0;
         v.misc[T_BAD] = 0.0;
-        v.misc[T_GN] = acc[1];
-        v.misc[T_GN + 1] = acc[2];
-        v.misc[T_GN + 2] = acc[3];
+    }
+    if constexpr (NT < 128) {   // no spare warps during the inversions: the Jastrow first
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int j = threadIdx.x; j < s.np; j += NT)
+            if (j != p) jastrow_pair_change(s, v, p, j, acc);
+        block_sum<NT>(acc, v.red);
+        if (threadIdx.x == 0) {
+            v.misc[T_LOGR] = acc[0];
+            for (int d = 0; d < 3; ++d) {
+                v.misc[T_JG + d] = v.misc[T_GN + d] = acc[1 + d];
+                v.misc[T_JL + d] = acc[4 + d];
+            }
+        }
     }
     __syncthreads();
     propose3<NT>(s, v, sm, p, grad);
@@ -832,31 +877,12 @@ __device__ void commit3(const DevSys& s, const V3& v, double* sm, int p) {
                 v.jl[j * 3 + d] += dl[d];
             }
     }
-    // p's own planes from its new partners
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int j = threadIdx.x; j < np; j += NT) {
-        if (j == p) continue;
-        for (int t = 0; t < s.nterms; ++t) {
-            const DevTerm& T = s.terms[t];
-            if (!any_term_couples(T, p, j)) continue;
-            double del[3], u, du, d2u;
-            const double r = dist3(s, v.newpos, v.pos + j * 3, del);
-            radial(T, r, u, du, d2u);
-            const double ir = 1.0 / r;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double dor = del[d] * ir;
-                acc[d] += du * dor;
-                acc[3 + d] += d2u * dor * dor + du * ir * (1.0 - dor * dor);
-            }
-        }
-    }
-    block_sum<NT>(acc, v.red);
+    // p's own planes: the proposal's sums over its new partners
     if (threadIdx.x == 0)
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            v.jg[p * 3 + d] = acc[d];
-            v.jl[p * 3 + d] = acc[3 + d];
+            v.jg[p * 3 + d] = v.misc[T_JG + d];
+            v.jl[p * 3 + d] = v.misc[T_JL + d];
         }
     for (int d = 0; d < s.nbf; ++d) {
         const DevBF& D = s.bf[d];
@@ -905,6 +931,65 @@ __device__ void refresh_particle3(const DevSys& s, const V3& v, double* sm, int 
     __syncthreads();
 }
 
+// ───────────────────────── record staging ───────────────────────────────
+//
+// A walker's record is contiguous and all of it is hot, so it moves between
+// HBM and shared memory as one bulk copy of the tensor-memory-access engine
+// (cp.async.bulk, no tensor map): thread 0 arms an mbarrier with the byte
+// count and issues the load; every thread waits on the barrier's phase, the
+// wait bounded (about a second) so that a copy that never lands sets the
+// walker's error flag instead of hanging the kernel.  The store back is a
+// bulk copy of the staged record after the generic-proxy writes are fenced
+// for the async proxy.  Record strides and the hot size are multiples of 32
+// bytes, the shared base of 16: the alignment both copies need.
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// true when the record landed; false after the bounded wait ran out
+__device__ bool stage_in(const double* rec, double* sm, unsigned bytes, unsigned long long* bar) {
+    const unsigned b = smem_addr(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(smem_addr(sm)), "l"(rec), "r"(bytes), "r"(b)
+                     : "memory");
+    }
+    auto wait = [b](long limit) {
+        unsigned done = 0;
+        for (long it = 0; it < limit && !done; ++it)
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+                : "=r"(done)
+                : "r"(b)
+                : "memory");
+        return done != 0;
+    };
+    if (__syncthreads_and(wait(1L << 24))) return true;
+    wait(1L << 24);   // the copy still in flight: a second bounded wait before the CTA leaves
+    __syncthreads();
+    return false;
+}
+
+__device__ void stage_out(double* rec, const double* sm, unsigned bytes) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(rec), "r"(smem_addr(sm)),
+                     "r"(bytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+}
+
 // ───────────────────────── kernels ──────────────────────────────────────
 
 template <int NT>
@@ -913,15 +998,18 @@ __global__ void __launch_bounds__(NT) evaluate3_kernel(DevSys s, double* records
     const int w = blockIdx.x;
     if (w >= nw) return;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot<NT>(s, rec, sm);
+    __shared__ unsigned long long bar;
+    if (!stage_in(rec, sm, static_cast<unsigned>(s.hot) * 8u, &bar)) {
+        if (threadIdx.x == 0) rec[s.o_scal + S_ERR] = 2.0;   // the record never landed
+        return;
+    }
     const V3 v = view3(s, sm);
     if (threadIdx.x == 0) v.misc[T_ERR] = 0.0;
     for (int i = threadIdx.x; i < s.np; i += NT) wrap_pos(s, v.pos + i * 3);
     __syncthreads();
     refresh_walker3<NT>(s, v, sm, true);
     if (threadIdx.x == 0) v.scal[S_ERR] = v.misc[T_ERR];
-    __syncthreads();
-    store_hot<NT>(s, rec, sm);
+    stage_out(rec, sm, static_cast<unsigned>(s.hot) * 8u);
 }
 
 template <int NT>
@@ -931,7 +1019,11 @@ __global__ void __launch_bounds__(NT) sweep3_kernel(DevSys s, double* records, i
     const int w = blockIdx.x;
     if (w >= nw) return;
     double* rec = records + static_cast<long>(w) * s.rec;
-    load_hot<NT>(s, rec, sm);
+    __shared__ unsigned long long bar;
+    if (!stage_in(rec, sm, static_cast<unsigned>(s.hot) * 8u, &bar)) {
+        if (threadIdx.x == 0) rec[s.o_scal + S_ERR] = 2.0;   // the record never landed
+        return;
+    }
     const V3 v = view3(s, sm);
     const int np = s.np;
     const bool dmc = prm.mode == 1;
@@ -1048,8 +1140,7 @@ __global__ void __launch_bounds__(NT) sweep3_kernel(DevSys s, double* records, i
         if (dmc && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
         if (v.misc[T_ERR] != 0.0) v.scal[S_ERR] = 1.0;
     }
-    __syncthreads();
-    store_hot<NT>(s, rec, sm);
+    stage_out(rec, sm, static_cast<unsigned>(s.hot) * 8u);
 }
 
 }  // namespace

@@ -209,3 +209,92 @@ def test_benchmark_population_dmc_step():
     assert nw // 5 + 1 <= g.nw <= 2 * nw + 1
     g.close()
     st.close()
+
+
+# ─────────────────────────── GPU: what 3-D contexts refuse, rows in 3-D ─────
+
+UNSUPPORTED = 3   # ALEA_ERR_UNSUPPORTED
+
+
+def _small3d():
+    return golden("setup_heg14bf3d.json"), np.array(golden("eval_heg14bf3d.json")["positions"])
+
+
+@pytest.mark.gpu
+def test_refused_three_dimensional_systems():
+    """A 3-D cell must be orthorhombic along the axes, a 3-D determinant has
+    at most 32 rows, and 3-D Padé terms are minimum-image only."""
+    import copy
+    import alea_b200
+    setup, _ = _small3d()
+    skew = copy.deepcopy(setup)
+    v = list(skew["cell"]["vectors"])
+    v[1] = 0.5 * v[0]
+    skew["cell"]["vectors"] = v
+    with pytest.raises(alea_b200.AleaGpuError, match="orthorhombic") as e:
+        walkers(skew, 4)
+    assert e.value.code == UNSUPPORTED
+    pw = golden("setup_heg54pw3d.json")
+    big = copy.deepcopy(pw)
+    b = big["slater"][0]
+    b["last"] = b["first"] + 33
+    b["k"] = list(b["k"]) + [0.0] * (6 * 3)
+    b["is_sin"] = list(b["is_sin"]) + [0] * 6
+    big["slater"][1]["first"] = 33
+    big["np"] = 33 + 27
+    big["groups"][0]["last"] = 33
+    big["groups"][1]["first"], big["groups"][1]["last"] = 33, 60
+    big["slater"][1]["last"] = 60
+    with pytest.raises(alea_b200.AleaGpuError, match="1..32 rows") as e:
+        walkers(big, 4)
+    assert e.value.code == UNSUPPORTED
+    pade = copy.deepcopy(golden("setup_gauss3d.json"))
+    pade["pade"][0]["image_sum"] = {"spline": {"r_cut": 1.0, "inv_delta": 1.0, "n_knots": 2, "scaled": [0.0] * 6},
+                                    "u_inf": 0.0, "n1": [1], "n2": [0], "kx": [1.0], "ky": [0.0], "weight": [0.0]}
+    with pytest.raises(alea_b200.AleaGpuError) as e:
+        walkers(pade, 4)
+    assert e.value.code in (1, UNSUPPORTED)   # an image sum in an open cell is invalid either way
+
+
+@pytest.mark.gpu
+def test_two_dimensional_entry_points_refuse_3d_contexts():
+    """Single moves, the FP32 form, the allocation-free step, estimators,
+    forward walking and parameter derivatives answer ALEA_ERR_UNSUPPORTED for
+    a 3-D context, which then still steps."""
+    import alea_b200
+    setup, pos = _small3d()
+    g = walkers(setup, len(pos))
+    g.upload(pos)
+    g.set_streams(5, alea_b200.STREAM_VMC, len(pos))
+    calls = [lambda: g.move(0, pos.reshape(len(pos), -1, 3)[:, 0, :]),
+             lambda: g.set_precision("fp32"),
+             lambda: g.vmc_step_noalloc(1.0, 1, False),
+             lambda: g.add_estimator("gofr", n_bins=8, rmax=1.0),
+             lambda: g.set_forward_walking([1.0]),
+             lambda: g.parameter_derivatives()]
+    for call in calls:
+        with pytest.raises(alea_b200.AleaGpuError) as e:
+            call()
+        assert e.value.code == UNSUPPORTED
+    st = g.vmc_step(1.0, 1, False)
+    assert st.n_walkers == len(pos) and np.all(np.isfinite(g.download()["local_energy"]))
+    g.close()
+
+
+@pytest.mark.gpu
+def test_configuration_rows_round_trip_in_3d():
+    """final_configurations gives AoS rows [w][p][3]; seeding a second
+    context with them reproduces the positions and local energies."""
+    setup, pos = _small3d()
+    a = walkers(setup, len(pos))
+    a.upload(pos)
+    rows = a.final_configurations()
+    assert rows.shape == (len(pos), setup["np"], 3)
+    np.testing.assert_array_equal(rows.reshape(len(pos), -1), a.download()["positions"])
+    b = walkers(setup, len(pos))
+    b.seed_walker_rows(rows, len(pos))
+    da, db = a.download(), b.download()
+    np.testing.assert_array_equal(db["positions"], da["positions"])
+    np.testing.assert_array_equal(db["local_energy"], da["local_energy"])
+    a.close()
+    b.close()
