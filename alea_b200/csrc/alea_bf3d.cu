@@ -698,41 +698,60 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
         touched[d] = bf_touches(s.bf[d], p);
         if (p >= s.bf[d].first && p < s.bf[d].last) dp = d;
     }
-    // p's own row: r_p' + Σ_c Σ_j η(r_pj') r_pj' over the sources, by the CTA
-    if (dp >= 0) {
+    // p's own row, r_p' + Σ_c Σ_j η(r_pj') r_pj' over the sources, on the last
+    // warp, while the others shift the rows that p displaces (the committed x
+    // moved by p's old and new pair terms)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NW = NT / 32;
+    const bool own_warp = NW > 1 && dp >= 0 && warp == NW - 1;
+    if (own_warp) {
         const DevBF& D = s.bf[dp];
         double acc[3] = {0.0, 0.0, 0.0};
-        for (int j = threadIdx.x; j < np; j += NT) {
+        for (int j = lane; j < np; j += 32) {
             if (j == p) continue;
             for (int c = 0; c < D.nch; ++c)
                 if (in_sources(D.ch[c], j)) bf3_pair(s, D.ch[c], v.newpos, v.pos + j * 3, 1.0, acc, nullptr, nullptr);
         }
-        block_sum<NT>(acc, v.red);
-        if (threadIdx.x == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[a] = warp_sum(acc[a]);
+        if (lane == 0) {
             double* px = sm + D.pX + (p - D.first) * 3;
             px[0] = v.newpos[0] + acc[0];
             px[1] = v.newpos[1] + acc[1];
             px[2] = v.newpos[2] + acc[2];
         }
-    }
-    // the rows p displaces: the committed x shifted by p's old and new pair terms
-    for (int e = threadIdx.x; e < nb * W; e += NT) {
-        const int d = e / W, t = e % W;
-        const DevBF& D = s.bf[d];
-        const int P = D.first + t;
-        if (!touched[d] || t >= D.n || P == p) continue;
-        const double* x = sm + D.oX;
-        double xt[3] = {x[t * 3], x[t * 3 + 1], x[t * 3 + 2]};
-        for (int c = 0; c < D.nch; ++c) {
-            if (!in_sources(D.ch[c], p)) continue;
-            bf3_pair(s, D.ch[c], v.pos + P * 3, v.newpos, 1.0, xt, nullptr, nullptr);
-            bf3_pair(s, D.ch[c], v.pos + P * 3, v.pos + p * 3, -1.0, xt, nullptr, nullptr);
+    } else if (NW == 1 && dp >= 0 && threadIdx.x == 0) {   // a one-warp CTA: serially
+        const DevBF& D = s.bf[dp];
+        double xt[3] = {v.newpos[0], v.newpos[1], v.newpos[2]};
+        for (int j = 0; j < np; ++j) {
+            if (j == p) continue;
+            for (int c = 0; c < D.nch; ++c)
+                if (in_sources(D.ch[c], j)) bf3_pair(s, D.ch[c], v.newpos, v.pos + j * 3, 1.0, xt, nullptr, nullptr);
         }
-        double* px = sm + D.pX + t * 3;
+        double* px = sm + D.pX + (p - D.first) * 3;
         px[0] = xt[0];
         px[1] = xt[1];
         px[2] = xt[2];
     }
+    const int shifters = (NW > 1 && dp >= 0) ? NT - 32 : NT;
+    if (!own_warp)
+        for (int e = threadIdx.x; e < nb * W; e += shifters) {
+            const int d = e / W, t = e % W;
+            const DevBF& D = s.bf[d];
+            const int P = D.first + t;
+            if (!touched[d] || t >= D.n || P == p) continue;
+            const double* x = sm + D.oX;
+            double xt[3] = {x[t * 3], x[t * 3 + 1], x[t * 3 + 2]};
+            for (int c = 0; c < D.nch; ++c) {
+                if (!in_sources(D.ch[c], p)) continue;
+                bf3_pair(s, D.ch[c], v.pos + P * 3, v.newpos, 1.0, xt, nullptr, nullptr);
+                bf3_pair(s, D.ch[c], v.pos + P * 3, v.pos + p * 3, -1.0, xt, nullptr, nullptr);
+            }
+            double* px = sm + D.pX + t * 3;
+            px[0] = xt[0];
+            px[1] = xt[1];
+            px[2] = xt[2];
+        }
     __syncthreads();
     // the new matrices (values into A's pending storage, inverted there) and ∇φ rows
     for (int e = threadIdx.x; e < nb * W * W; e += NT) {
@@ -749,7 +768,6 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
         r[2] = g[2];
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5;
     if (warp < nb && touched[warp]) {
         const DevBF& D = s.bf[warp];
         double* mult = v.mwork + warp * mstride + 3L * D.n * D.n;
@@ -1013,7 +1031,7 @@ __global__ void __launch_bounds__(NT) evaluate3_kernel(DevSys s, double* records
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) sweep3_kernel(DevSys s, double* records, int nw, const double* randoms,
+__global__ void __launch_bounds__(NT, 3) sweep3_kernel(DevSys s, double* records, int nw, const double* randoms,
                                                     long stride, SweepParams prm) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
