@@ -3522,6 +3522,22 @@ void set_cancel_flag(alea_gpu_ctx* c, const std::atomic<int>* flag) {
 size_t footprint_bytes(const alea_gpu_system* sys, int capacity, int n_substeps) {
     if (!sys || capacity < 1) return 0;
     const long np = sys->n_particles;
+    if (sys->dim == 3) {   // build_system3's record: 7 planes of 3N, scalars, per determinant x, A, F, (ln|det|, sign)
+        long rec = 21 * np + S_NSCAL;
+        const int ndet = sys->n_backflow > 0 ? sys->n_backflow : sys->n_blocks;
+        for (int d = 0; d < ndet; ++d) {
+            const long n = sys->n_backflow > 0 ? sys->backflow[d].last - sys->backflow[d].first
+                                               : sys->blocks[d].last - sys->blocks[d].first;
+            rec += 2 * round4(3 * n) + round4(n * n) + 4;
+        }
+        rec = round4(rec);
+        const size_t cap = static_cast<size_t>(capacity);
+        size_t bytes = 2 * cap * static_cast<size_t>(rec) * 8;
+        bytes += cap * static_cast<size_t>(std::max<long>(3 * np, 8)) * 8 + cap * 5;
+        bytes += static_cast<size_t>(std::max(n_substeps, 1)) * static_cast<size_t>(np) * 4 * cap * 8;
+        bytes += static_cast<size_t>(np) * static_cast<size_t>(np) * 4 + (1u << 20);
+        return bytes;
+    }
     bool cplx = false;
     for (int b = 0; b < sys->n_blocks; ++b) cplx |= sys->blocks[b].type == ALEA_ORB_TWISTED_PLANE_WAVE;
     long rec = 14 * np + S_NSCAL + (cplx ? 4 * np : 0);

@@ -298,3 +298,28 @@ def test_configuration_rows_round_trip_in_3d():
     np.testing.assert_array_equal(db["local_energy"], da["local_energy"])
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_served_3d_job_equals_its_own_run():
+    """A 3-D VMC job through the serving queue (per-job contexts, footprint
+    admission) gives its own alea_gpu_vmc_run result bit for bit beside a
+    2-D job."""
+    import alea_b200
+    setup, pos = _small3d()
+    nw = len(pos)
+    g = walkers(setup, nw)
+    g.upload(pos)
+    own, _ = g.vmc_run(1, 2, 3, 1, 1.0, nw, 77)
+    g.close()
+    srv = alea_b200.Server(max_running=2)
+    two = golden("setup_heg10.json")
+    other = srv.submit(two, np.array(golden("eval_heg10.json")["positions"]), 0, 1, 2, 3, 1, 225.0, seed=5)
+    jid = srv.submit(setup, pos, 0, 1, 2, 3, 1, 1.0, seed=77)
+    r = srv.poll(jid, timeout_ms=120000)
+    assert r is not None and r.status == 0
+    assert r.result.energy == own.energy and r.result.energy_error == own.energy_error
+    assert r.result.acceptance == own.acceptance and r.result.n_moves == own.n_moves
+    assert r.footprint_bytes > 0
+    assert srv.poll(other, timeout_ms=120000).status == 0
+    srv.close()
