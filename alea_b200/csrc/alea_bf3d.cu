@@ -687,11 +687,13 @@ __device__ __forceinline__ void jastrow_pair_change(const DevSys& s, const V3& v
 // Move work area per determinant: ∇φ rows [(t·N + m)·3 + a] (3N²), the
 // Gauss-Jordan multipliers (N) and row exchanges (N ints).  While warps 0
 // and 1 invert, warps 2 and 3 form the Jastrow ratio and p's new Jastrow
-// gradient into misc (with fewer warps ratio3 forms them first).
+// gradient into misc (with fewer warps ratio3 forms them first).  The ∇φ
+// rows are not kept (the moves' layout fits four walkers per SM): F'
+// evaluates them again, two lanes per row.
 template <int NT>
 __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool grad) {
     const int np = s.np, nb = s.nbf, W = s.maxN;
-    const long mstride = (3L * W * W + 2L * W + 3) & ~3L;
+    const long mstride = (2L * W + 3) & ~3L;
     bool touched[2] = {false, false};
     int dp = -1;
     for (int d = 0; d < nb; ++d) {
@@ -762,15 +764,11 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
         double val, g[3];
         bf3_orbital(s, D, m, sm + D.pX + t * 3, val, g);
         sm[D.pA + t * N + m] = val;
-        double* r = v.mwork + d * mstride + (t * N + m) * 3;
-        r[0] = g[0];
-        r[1] = g[1];
-        r[2] = g[2];
     }
     __syncthreads();
     if (warp < nb && touched[warp]) {
         const DevBF& D = s.bf[warp];
-        double* mult = v.mwork + warp * mstride + 3L * D.n * D.n;
+        double* mult = v.mwork + warp * mstride;
         gj_warp_signed(sm + D.pA, D.n, mult, reinterpret_cast<int*>(mult + D.n), sm + D.pM);
     } else if (NT >= 128 && warp >= 2) {
         // meanwhile warps 2 and 3: the Jastrow ratio and p's new Jastrow
@@ -796,16 +794,35 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
         }
     }
     // F'_t = Σ_m A'[m][t] ∇φ_m(x'_t)
-    for (int e = threadIdx.x; e < nb * W * 3; e += NT) {
-        const int d = e / (W * 3), ta = e % (W * 3), t = ta / 3, a = ta % 3;
-        const DevBF& D = s.bf[d];
-        if (!touched[d] || t >= D.n || sm[D.pM + 2] == 0.0) continue;
-        const int N = D.n;
-        const double* pa = sm + D.pA;
-        const double* R = v.mwork + d * mstride;
-        double acc = 0.0;
-        for (int m = 0; m < N; ++m) acc = fma(pa[m * N + t], R[(t * N + m) * 3 + a], acc);
-        sm[D.pF + t * 3 + a] = acc;
+    // lanes 2i and 2i + 1 take the even and odd orbitals of one row; every
+    // lane of the warp takes part in the pair's shuffle
+    for (int base = 0; base < nb * W * 2; base += NT) {
+        const int e = base + threadIdx.x, h = e & 1, dt = e >> 1, d = dt / W, t = dt % W;
+        const DevBF* Dp = d < nb ? &s.bf[d] : nullptr;
+        const bool on = e < nb * W * 2 && touched[d] && t < Dp->n && sm[Dp->pM + 2] != 0.0;
+        double acc[3] = {0.0, 0.0, 0.0};
+        if (on) {
+            const DevBF& D = *Dp;
+            const int N = D.n;
+            const double* pa = sm + D.pA;
+            const double* xt = sm + D.pX + t * 3;
+            for (int m = h; m < N; m += 2) {
+                double val, g[3];
+                bf3_orbital(s, D, m, xt, val, g);
+                const double am = pa[m * N + t];
+                acc[0] = fma(am, g[0], acc[0]);
+                acc[1] = fma(am, g[1], acc[1]);
+                acc[2] = fma(am, g[2], acc[2]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], 1);
+        if (on && h == 0) {
+            double* pf = sm + Dp->pF + t * 3;
+            pf[0] = acc[0];
+            pf[1] = acc[1];
+            pf[2] = acc[2];
+        }
     }
     __syncthreads();
     if (grad)
@@ -1030,9 +1047,13 @@ __global__ void __launch_bounds__(NT) evaluate3_kernel(DevSys s, double* records
     stage_out(rec, sm, static_cast<unsigned>(s.hot) * 8u);
 }
 
+// The moves of prm.n_sub sweeps, in the moves' shared-memory layout (four
+// walkers per SM); the host follows each DMC sweep, or a VMC step's sweeps,
+// with refresh3_kernel (derivatives, E_L, branch factor).  `first` marks a
+// step's first launch: its scalars start there.
 template <int NT>
-__global__ void __launch_bounds__(NT, 3) sweep3_kernel(DevSys s, double* records, int nw, const double* randoms,
-                                                    long stride, SweepParams prm) {
+__global__ void __launch_bounds__(NT, 4) sweep3_kernel(DevSys s, double* records, int nw, const double* randoms,
+                                                       long stride, SweepParams prm, int first) {
     extern __shared__ __align__(16) double sm[];
     const int w = blockIdx.x;
     if (w >= nw) return;
@@ -1046,7 +1067,7 @@ __global__ void __launch_bounds__(NT, 3) sweep3_kernel(DevSys s, double* records
     const int np = s.np;
     const bool dmc = prm.mode == 1;
     const bool drift = dmc || prm.drift != 0;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && first) {
         v.scal[S_NACC] = 0.0;
         v.scal[S_NCUT] = 0.0;
         if (dmc) {
@@ -1055,8 +1076,8 @@ __global__ void __launch_bounds__(NT, 3) sweep3_kernel(DevSys s, double* records
             v.scal[S_WEIGHT] = 1.0;
             v.scal[S_EPREV] = v.scal[S_EL];
         }
-        v.misc[T_ERR] = 0.0;
     }
+    if (threadIdx.x == 0) v.misc[T_ERR] = 0.0;
     __syncthreads();
     for (int sub = 0; sub < prm.n_sub; ++sub) {
         const double* rnd = randoms + static_cast<long>(sub) * np * 4 * stride;
@@ -1137,25 +1158,45 @@ __global__ void __launch_bounds__(NT, 3) sweep3_kernel(DevSys s, double* records
             __syncthreads();
             if (v.misc[T_ACC] != 0.0) commit3<NT>(s, v, sm, p);
         }
-        if (dmc || sub == prm.n_sub - 1) {
-            refresh_walker3<NT>(s, v, sm, false);
-            if (threadIdx.x == 0 && dmc) {
-                const double enew = v.scal[S_EL], eold = v.scal[S_EPREV];
-                double half_tau = 0.5 * prm.tau;
-                const double x = fmax(prm.eref - enew, prm.eref - eold);
-                if (x > prm.e_max)
-                    half_tau = 0.0;
-                else if (x > prm.e_cut)
-                    half_tau *= 1.0 - (x - prm.e_cut) / (prm.e_max - prm.e_cut);
-                v.scal[S_WEIGHT] *= exp(half_tau * (2.0 * prm.etrial - enew - eold));
-                if (x > prm.e_cut) v.scal[S_NCUT] += 1.0;
-                v.scal[S_EPREV] = enew;
-            }
-            __syncthreads();
-        }
     }
+    if (threadIdx.x == 0 && v.misc[T_ERR] != 0.0) v.scal[S_ERR] = 1.0;
+    stage_out(rec, sm, static_cast<unsigned>(s.hot) * 8u);
+}
+
+// After a moves-only launch: every particle's derivatives from the committed
+// state, ln ψ and E_L; in DMC the branch factor of the sweep, and after the
+// step's last sweep the age (the fused kernel's end of a sweep).
+template <int NT>
+__global__ void __launch_bounds__(NT, 3) refresh3_kernel(DevSys s, double* records, int nw, SweepParams prm,
+                                                        int last) {
+    extern __shared__ __align__(16) double sm[];
+    const int w = blockIdx.x;
+    if (w >= nw) return;
+    double* rec = records + static_cast<long>(w) * s.rec;
+    __shared__ unsigned long long bar;
+    if (!stage_in(rec, sm, static_cast<unsigned>(s.hot) * 8u, &bar)) {
+        if (threadIdx.x == 0) rec[s.o_scal + S_ERR] = 2.0;   // the record never landed
+        return;
+    }
+    const V3 v = view3(s, sm);
+    const bool dmc = prm.mode == 1;
+    if (threadIdx.x == 0) v.misc[T_ERR] = 0.0;
+    __syncthreads();
+    refresh_walker3<NT>(s, v, sm, false);
     if (threadIdx.x == 0) {
-        if (dmc && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
+        if (dmc) {
+            const double enew = v.scal[S_EL], eold = v.scal[S_EPREV];
+            double half_tau = 0.5 * prm.tau;
+            const double x = fmax(prm.eref - enew, prm.eref - eold);
+            if (x > prm.e_max)
+                half_tau = 0.0;
+            else if (x > prm.e_cut)
+                half_tau *= 1.0 - (x - prm.e_cut) / (prm.e_max - prm.e_cut);
+            v.scal[S_WEIGHT] *= exp(half_tau * (2.0 * prm.etrial - enew - eold));
+            if (x > prm.e_cut) v.scal[S_NCUT] += 1.0;
+            v.scal[S_EPREV] = enew;
+            if (last && prm.tau > 0.0) v.scal[S_AGE] = v.scal[S_RRP] > 0.0 ? 0.0 : v.scal[S_AGE] + 1.0;
+        }
         if (v.misc[T_ERR] != 0.0) v.scal[S_ERR] = 1.0;
     }
     stage_out(rec, sm, static_cast<unsigned>(s.hot) * 8u);
@@ -1171,12 +1212,27 @@ cudaError_t launch_evaluate3(int nw, size_t smem, cudaStream_t st, const DevSys&
     return cudaGetLastError();
 }
 
+// The moves run as their own launches (four walkers per SM in the moves'
+// layout, s.t_mtotal doubles) followed by refresh3_kernel (the full layout):
+// one moves launch for a VMC step's sweeps, one pair per DMC sweep.
 cudaError_t launch_sweep3(int nw, size_t smem, cudaStream_t st, const DevSys& s, double* records,
                           const double* randoms, long stride, const SweepParams& prm) {
-    const cudaError_t e = cudaFuncSetAttribute(sweep3_kernel<kNT3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(smem));
+    const size_t msmem = static_cast<size_t>(s.t_mtotal) * 8;
+    cudaError_t e = cudaFuncSetAttribute(sweep3_kernel<kNT3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(msmem));
     if (e != cudaSuccess) return e;
-    sweep3_kernel<kNT3><<<nw, kNT3, smem, st>>>(s, records, nw, randoms, stride, prm);
+    e = cudaFuncSetAttribute(refresh3_kernel<kNT3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const bool dmc = prm.mode == 1;
+    const int launches = dmc ? prm.n_sub : 1;
+    for (int l = 0; l < launches; ++l) {
+        SweepParams mp = prm;
+        mp.n_sub = dmc ? 1 : prm.n_sub;
+        const double* rnd = randoms + static_cast<long>(dmc ? l : 0) * s.np * 4 * stride;
+        sweep3_kernel<kNT3><<<nw, kNT3, msmem, st>>>(s, records, nw, rnd, stride, mp, l == 0 ? 1 : 0);
+        refresh3_kernel<kNT3><<<nw, kNT3, smem, st>>>(s, records, nw, prm, l == launches - 1 ? 1 : 0);
+    }
     return cudaGetLastError();
 }
 

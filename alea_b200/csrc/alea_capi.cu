@@ -1315,10 +1315,12 @@ int build_system3(alea_gpu_ctx* c, const alea_gpu_system* in) {
     }
     s.t_mwork = static_cast<int>(m);
     const long N = s.maxN;
-    // the move's work per determinant: ∇φ rows (3N²), multipliers and row exchanges (2N)
-    // the refresh's: M, orbital rows, G, T, slice sums (48N for the per-particle warps when N < 12)
+    // the moves' layout ends with each determinant's Gauss-Jordan multipliers and
+    // row exchanges (2N); the refresh's work area (from t_work): M, orbital rows,
+    // G, T, slice sums (48N for the per-particle warps when N < 12)
+    s.t_mtotal = static_cast<int>(s.t_mwork + s.nbf * round4(2 * N));
     const long refresh = 8 * N * N + 18 * N + (N < 12 ? 36 * N : 0);
-    const long total = std::max(s.t_mwork + s.nbf * round4(3 * N * N + 2 * N), s.t_work + round4(refresh));
+    const long total = std::max(static_cast<long>(s.t_mtotal), s.t_work + round4(refresh));
     s.t_total = static_cast<int>(total);
     s.f_total = 0;
     c->smem = static_cast<size_t>(total) * 8;

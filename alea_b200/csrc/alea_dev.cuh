@@ -168,11 +168,13 @@ struct DevSys {
     // three-dimensional walkers (alea_bf3d.cu): Ewald k-vectors [3*enk]
     // (kx, ky, kz per vector) and the shared-memory layout after the hot
     // part: proposal, misc slots, reduction area, pivot column, the pending
-    // determinants of a proposal, then the move's work area (new matrix and
-    // orbital rows); the refresh's tables reuse the area from the pending
-    // determinants on (t_work)
+    // determinants of a proposal, then the move's work area (each
+    // determinant's Gauss-Jordan multipliers and row exchanges; the moves'
+    // layout ends there, at t_mtotal); the refresh's tables reuse the area
+    // from the pending determinants on (t_work, up to t_total)
     const double* ek3;
     int t_newpos, t_misc, t_red, t_col, t_work, t_mwork, t_total;
+    int t_mtotal;
     // ziggurat tables
     const uint64_t* zk;
     const double *zw, *zf;
