@@ -86,11 +86,13 @@ struct alea_gpu_server {
     std::condition_variable cv_ready;
 
     // First queued job that fits the budget left (caller holds mu); a packed
-    // server's workers take DMC jobs only, its scheduler VMC jobs only.
+    // server's scheduler takes the VMC jobs of two-dimensional systems (what
+    // the packed sweeps run), its workers every other job.
     Job* admissible(bool vmc_packer = false) {
         for (uint64_t id : queue) {
             Job* j = jobs[id].get();
-            if (packed && (j->spec.mode == ALEA_JOB_VMC) != vmc_packer) continue;
+            const bool packs = j->spec.mode == ALEA_JOB_VMC && j->spec.system->dim == 2;
+            if (packed && packs != vmc_packer) continue;
             if (j->bytes <= budget - std::min(budget, in_use)) return j;
         }
         return nullptr;

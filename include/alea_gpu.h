@@ -761,7 +761,8 @@ int alea_gpu_server_create(int device, size_t hbm_budget_bytes, int max_running,
  * together, all their walkers in one sweep launch per step
  * (alea_gpu_vmc_run_packed), independently of the other bodies; a job's
  * result equals its alea_gpu_vmc_run on its own context whatever else runs.
- * DMC jobs take the max_running worker contexts as in
+ * DMC jobs, and the VMC jobs of three-dimensional systems (the packed sweeps
+ * are two-dimensional), take the max_running worker contexts as in
  * alea_gpu_server_create. */
 int alea_gpu_server_create_packed(int device, size_t hbm_budget_bytes, int max_running, alea_gpu_server** out);
 /* Queue a job; never blocks on the device.  ALEA_ERR_NOMEM when the job

@@ -323,3 +323,10 @@ def test_served_3d_job_equals_its_own_run():
     assert r.footprint_bytes > 0
     assert srv.poll(other, timeout_ms=120000).status == 0
     srv.close()
+    # a packing server runs it on a context of its own (the packed sweeps are two-dimensional)
+    srv = alea_b200.Server(max_running=2, packed=True)
+    jid = srv.submit(setup, pos, 0, 1, 2, 3, 1, 1.0, seed=77)
+    r = srv.poll(jid, timeout_ms=120000)
+    assert r is not None and r.status == 0
+    assert r.result.energy == own.energy and r.result.n_moves == own.n_moves
+    srv.close()
