@@ -25,17 +25,19 @@
 // anew and inverted by pivoted Gauss-Jordan (its ratio is det M'/det M, no
 // rank-one update applies), one warp per determinant so that the two spins'
 // determinants invert at once; the inverse A', F' = A'ᵀ∇φ(x') and
-// log|det M'| are kept pending and committed on acceptance.  The local energy's
-// refresh rebuilds x from the positions and every particle's ∇ and
-// per-dimension ∂² ln|D| from the committed A and F: T = Aᵀ∂∂φ, G^a = Aᵀ∂_aφ
-// (three N×N×N products on the FP64 tensor cores) and the Jacobian columns ∂x_t/∂r_k^β (ln|D|'s Laplacian is
-// Σ F·∂²x + Σ v v T − tr((G·v)²)).
+// log|det M'| are kept pending and committed on acceptance.  The moves run
+// in their own launch (sweep3_kernel, the moves' smaller shared-memory
+// layout); the refresh that follows (refresh3_kernel) rebuilds x from the
+// positions and every particle's ∇ and per-dimension ∂² ln|D| from the
+// committed A and F: T = Aᵀ∂∂φ, G^a = Aᵀ∂_aφ (three N×N×N products on the
+// FP64 tensor cores) and the Jacobian columns ∂x_t/∂r_k^β (ln|D|'s
+// Laplacian is Σ F·∂²x + Σ v v T − tr((G·v)²)), then the local energy.
 //
 // Record of a 3-D walker (doubles): positions, Jastrow ∇/∂², two zero planes
 // (the k-space planes of the 2-D layout, read by the download), determinant
 // ∇/∂², the scalars, then per determinant x (3N), A (N²), F (3N) and
-// (log|det|, sign).  All of it is hot: it is staged in shared memory for the
-// whole sweep, in and out as one bulk copy each.
+// (log|det|, sign).  All of it is hot: each launch stages it in shared
+// memory, in and out as one bulk copy each.
 #include "alea_warp.cuh"
 
 namespace alea_gpu {
@@ -689,7 +691,10 @@ __device__ __forceinline__ void jastrow_pair_change(const DevSys& s, const V3& v
 // and 1 invert, warps 2 and 3 form the Jastrow ratio and p's new Jastrow
 // gradient into misc (with fewer warps ratio3 forms them first).  The ∇φ
 // rows are not kept (the moves' layout fits four walkers per SM): F'
-// evaluates them again, two lanes per row.
+// evaluates them again, two lanes per row.  Move work area per determinant:
+// the Gauss-Jordan multipliers (N) and row exchanges (N ints).  (Keeping the
+// new orbital values for F', a plane wave's gradient being its partner's
+// value times ±k, ran no faster in 12 KB more per walker.)
 template <int NT>
 __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool grad) {
     const int np = s.np, nb = s.nbf, W = s.maxN;
