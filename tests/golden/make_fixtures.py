@@ -73,6 +73,9 @@ SYSTEMS = {
     # open 3-D cell, the reference's own 3-D backflow test shape: Gaussian
     # orbitals, two backflow channels, a Padé Jastrow and open Coulomb
     "gauss3d": dict(system="gauss3d"),
+    # the 14-electron gas with its backflow determinant alone, for the
+    # statistical DMC comparison (kinetic energy only: stable weights)
+    "heg14bf3dp": dict(system="heg3d", nu=7, nd=7, rs=5, jastrow=0),
 }
 VMC = {
     "exciton": dict(nw=6, seed=11, eq=1, acc=2, steps=3, substeps=2, tau=0.05),
@@ -142,6 +145,7 @@ VMC_STAT = {
 DMC_STAT = {
     "heg10": dict(nw=1024, seed=424242, eq=10, acc=50, steps=10, substeps=1, tau=0.5, threads=8),
     "heg42": dict(nw=1024, seed=424243, eq=10, acc=40, steps=10, substeps=1, tau=0.5, threads=8),
+    "heg14bf3dp": dict(nw=1024, seed=424244, eq=10, acc=40, steps=10, substeps=1, tau=0.5, threads=8),
 }
 
 
@@ -213,7 +217,7 @@ def chain_fixtures(only=None):
 
 
 # systems that serve only DMC fixtures (no evaluation fixture)
-NO_EVAL = {"heg14bf3ds", "heg54bf3ds"}
+NO_EVAL = {"heg14bf3ds", "heg54bf3ds", "heg14bf3dp"}
 
 
 def main(only=None):

@@ -330,3 +330,26 @@ def test_served_3d_job_equals_its_own_run():
     assert r is not None and r.status == 0
     assert r.result.energy == own.energy and r.result.n_moves == own.n_moves
     srv.close()
+
+
+@pytest.mark.gpu
+def test_dmc_energy_agrees_with_reference_statistically():
+    """The 14-electron 3-D gas with its backflow determinant alone (kinetic
+    energy only): the device's DMC energy from an independent start and seed
+    against a long DMC::run of the compiled reference (1024 walkers, 40
+    blocks of 10 steps, tau = 0.5), within 2 combined standard errors."""
+    from alea_b200 import setup as S
+    ref = golden("dmcstat_heg14bf3dp.json")
+    p = ref["params"]
+    st = S.heg3d(7, 7, 5.0)
+    start = st.positions(4244, p["nw"])
+    st.close()
+    g = walkers(golden("setup_heg14bf3dp.json"), 2 * p["nw"] + 2)
+    g.upload(start)
+    res, blocks = g.dmc_run(p["eq"], p["acc"], p["steps"], p["substeps"], p["tau"], p["threads"],
+                            seed=4245, target=p["nw"], generations=10.0)
+    assert len(blocks) == p["acc"] and np.all(np.isfinite(blocks))
+    sigma = float(np.hypot(res.energy_error, ref["energy_error"]))
+    assert res.energy_error > 0 and abs(res.energy - ref["energy"]) < 2.0 * sigma, \
+        (res.energy, res.energy_error, ref["energy"], ref["energy_error"])
+    g.close()
