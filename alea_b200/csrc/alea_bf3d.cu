@@ -153,6 +153,34 @@ __device__ __forceinline__ double bf3_hess(const DevSys& s, const DevBF& D, int 
 
 __device__ __forceinline__ bool in_sources(const DevBFCh& C, int k) { return k >= C.sf && k < C.sl; }
 
+// Plane-wave orbitals m and m + 1 are the cosine and the sine of one k.
+__device__ __forceinline__ bool pw_pair(const DevBF& D, int m) {
+    if (m < 0 || m + 1 >= D.n || D.is_sin[m] != 0.0 || D.is_sin[m + 1] == 0.0) return false;
+    const double* k = D.k + m * 3;
+    return k[0] == k[3] && k[1] == k[4] && k[2] == k[5];
+}
+
+// The orbital units of a determinant, for a move's new matrices: units[d][u]
+// is the orbital index of unit u (with kUnitPair: it and the next orbital
+// are a plane wave's cosine and sine), units[d][32] the number of units.
+// Built by the first warp; the caller's barrier publishes it.
+constexpr unsigned char kUnitPair = 0x40;
+
+__device__ void build_units(const DevSys& s, unsigned char (*units)[33]) {
+    if (threadIdx.x >= 32) return;
+    const int m = threadIdx.x;
+    for (int d = 0; d < s.nbf; ++d) {
+        const DevBF& D = s.bf[d];
+        const bool pw = D.type == 0;
+        const bool first = m < D.n && !(pw && pw_pair(D, m - 1));
+        const unsigned mask = __ballot_sync(0xffffffffu, first);
+        if (first)
+            units[d][__popc(mask & ((1u << m) - 1u))] =
+                static_cast<unsigned char>(m | (pw && pw_pair(D, m) ? kUnitPair : 0));
+        if (m == 0) units[d][32] = static_cast<unsigned char>(__popc(mask));
+    }
+}
+
 // In-place pivoted Gauss-Jordan of the N×N matrix A (N <= 32, row-major in
 // shared memory) by the calling warp: A becomes A⁻¹; out[0] = log|det A|,
 // out[1] = its sign, out[2] = 1 when every pivot is finite and nonzero.
@@ -696,7 +724,8 @@ __device__ __forceinline__ void jastrow_pair_change(const DevSys& s, const V3& v
 // new orbital values for F', a plane wave's gradient being its partner's
 // value times ±k, ran no faster in 12 KB more per walker.)
 template <int NT>
-__device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool grad) {
+__device__ void propose3(const DevSys& s, const V3& v, double* sm, const unsigned char (*units)[33], int p,
+                         bool grad) {
     const int np = s.np, nb = s.nbf, W = s.maxN;
     const long mstride = (2L * W + 3) & ~3L;
     bool touched[2] = {false, false};
@@ -760,15 +789,28 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
             px[2] = xt[2];
         }
     __syncthreads();
-    // the new matrices (values into A's pending storage, inverted there) and ∇φ rows
-    for (int e = threadIdx.x; e < nb * W * W; e += NT) {
-        const int d = e / (W * W), tm = e % (W * W), t = tm / W, m = tm % W;
+    // the new matrices (values into A's pending storage, inverted there), one
+    // work item per orbital unit of a row (units: a plane wave's cosine and
+    // sine of one k take one sincos)
+    const int U = max(static_cast<int>(units[0][32]), nb > 1 ? static_cast<int>(units[1][32]) : 0);
+    for (int e = threadIdx.x; e < nb * W * U; e += NT) {
+        const int d = e / (W * U), tu = e % (W * U), t = tu / U, u = tu % U;
         const DevBF& D = s.bf[d];
-        if (!touched[d] || t >= D.n || m >= D.n) continue;
-        const int N = D.n;
-        double val, g[3];
-        bf3_orbital(s, D, m, sm + D.pX + t * 3, val, g);
-        sm[D.pA + t * N + m] = val;
+        if (!touched[d] || t >= D.n || u >= units[d][32]) continue;
+        const int N = D.n, mu = units[d][u], m = mu & 31;
+        const double* xt = sm + D.pX + t * 3;
+        double* row = sm + D.pA + t * N;
+        if (D.type == 0) {
+            const double* k = D.k + m * 3;
+            double sn, c;
+            sincos(fma(k[2], xt[2], fma(k[1], xt[1], k[0] * xt[0])), &sn, &c);
+            row[m] = D.is_sin[m] != 0.0 ? sn : c;
+            if (mu & kUnitPair) row[m + 1] = sn;
+        } else {
+            double val, g[3];
+            bf3_orbital(s, D, m, xt, val, g);
+            row[m] = val;
+        }
     }
     __syncthreads();
     if (warp < nb && touched[warp]) {
@@ -846,9 +888,11 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, int p, bool g
 }
 
 // log ψ(R')/ψ(R), its sign and (with grad) p's new gradient, for the
-// proposal in v.newpos.
+// proposal in v.newpos, in thread 0's misc slots: the caller's next barrier
+// publishes them.  Called after a barrier.
 template <int NT>
-__device__ void ratio3(const DevSys& s, const V3& v, double* sm, int p, bool grad) {
+__device__ void ratio3(const DevSys& s, const V3& v, double* sm, const unsigned char (*units)[33], int p,
+                       bool grad) {
     if (threadIdx.x == 0) {
         v.misc[T_SIGN] = 1.0;
         v.misc[T_BAD] = 0.0;
@@ -865,9 +909,10 @@ __device__ void ratio3(const DevSys& s, const V3& v, double* sm, int p, bool gra
                 v.misc[T_JL + d] = acc[4 + d];
             }
         }
+        __syncthreads();
     }
-    __syncthreads();
-    propose3<NT>(s, v, sm, p, grad);
+    // (T_SIGN and T_BAD are thread 0's alone until the caller's next barrier)
+    propose3<NT>(s, v, sm, units, p, grad);
     if (threadIdx.x == 0)
         for (int d = 0; d < s.nbf; ++d) {
             const DevBF& D = s.bf[d];
@@ -881,13 +926,15 @@ __device__ void ratio3(const DevSys& s, const V3& v, double* sm, int p, bool gra
                 v.misc[T_SIGN] *= pm[1] * ls[1];
             }
         }
-    __syncthreads();
 }
 
 // Accepted move of p: position (wrapped), pending determinants, the Jastrow
-// planes of p and its partners.
+// planes of p and its partners.  p's new position is thread 0's store after
+// the last barrier; with sync_pos a barrier publishes it (the drift moves'
+// refresh of the next particle reads every position), else the caller's
+// next barrier does.
 template <int NT>
-__device__ void commit3(const DevSys& s, const V3& v, double* sm, int p) {
+__device__ void commit3(const DevSys& s, const V3& v, double* sm, int p, bool sync_pos) {
     const int np = s.np;
     for (int j = threadIdx.x; j < np; j += NT) {
         if (j == p) continue;
@@ -946,7 +993,7 @@ __device__ void commit3(const DevSys& s, const V3& v, double* sm, int p) {
         v.pos[p * 3 + 1] = r[1];
         v.pos[p * 3 + 2] = r[2];
     }
-    __syncthreads();
+    if (sync_pos) __syncthreads();
 }
 
 // The determinant part of p's gradient at the committed state into sg
@@ -1083,6 +1130,8 @@ __global__ void __launch_bounds__(NT, 4) sweep3_kernel(DevSys s, double* records
         }
     }
     if (threadIdx.x == 0) v.misc[T_ERR] = 0.0;
+    __shared__ unsigned char units[2][33];
+    build_units(s, units);
     __syncthreads();
     for (int sub = 0; sub < prm.n_sub; ++sub) {
         const double* rnd = randoms + static_cast<long>(sub) * np * 4 * stride;
@@ -1111,7 +1160,7 @@ __global__ void __launch_bounds__(NT, 4) sweep3_kernel(DevSys s, double* records
                 v.misc[T_U] = g[3 * stride + w];
             }
             __syncthreads();
-            ratio3<NT>(s, v, sm, p, drift);
+            ratio3<NT>(s, v, sm, units, p, drift);
             if (threadIdx.x == 0) {
                 const double logr = v.misc[T_LOGR];
                 const double u = v.misc[T_U];
@@ -1161,7 +1210,7 @@ __global__ void __launch_bounds__(NT, 4) sweep3_kernel(DevSys s, double* records
                 if (acc) v.scal[S_NACC] += 1.0;
             }
             __syncthreads();
-            if (v.misc[T_ACC] != 0.0) commit3<NT>(s, v, sm, p);
+            if (v.misc[T_ACC] != 0.0) commit3<NT>(s, v, sm, p, drift);
         }
     }
     if (threadIdx.x == 0 && v.misc[T_ERR] != 0.0) v.scal[S_ERR] = 1.0;
