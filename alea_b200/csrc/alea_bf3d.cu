@@ -201,6 +201,7 @@ __device__ void gj_warp_signed(double* A, int N, double* mult, int* perm, double
     __syncwarp();
     double sign = 1.0, my_pivot = 1.0;   // lane k keeps pivot k: one log per lane at the end
     bool bad = false;
+    const bool vec = (reinterpret_cast<uintptr_t>(mult) & 15u) == 0;
     for (int k = 0; k < N; ++k) {
         const double x = lane < N ? A[lane * N + k] : 0.0;   // column k, row = lane
         unsigned long long key = 0ull;
@@ -240,11 +241,23 @@ __device__ void gj_warp_signed(double* A, int N, double* mult, int* perm, double
         if (lane < N)
             for (int r0 = 0; r0 < N; r0 += 8) {   // eight rows' loads in flight, then their updates
                 double f[8], y[8];
+                if (vec && r0 + 8 <= N) {   // a whole block: its multipliers as four 16-byte loads
+                    const double2* m2 = reinterpret_cast<const double2*>(mult + r0);
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const bool on = r0 + u < N;
-                    f[u] = on ? mult[r0 + u] : 0.0;
-                    y[u] = on ? A[(r0 + u) * N + lane] : 0.0;
+                    for (int u = 0; u < 4; ++u) {
+                        const double2 q = m2[u];
+                        f[2 * u] = q.x;
+                        f[2 * u + 1] = q.y;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) y[u] = A[(r0 + u) * N + lane];
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const bool on = r0 + u < N;
+                        f[u] = on ? mult[r0 + u] : 0.0;
+                        y[u] = on ? A[(r0 + u) * N + lane] : 0.0;
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < 8; ++u)
@@ -841,8 +854,9 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, const unsigne
         }
     }
     // F'_t = Σ_m A'[m][t] ∇φ_m(x'_t)
-    // lanes 2i and 2i + 1 take the even and odd orbitals of one row; every
-    // lane of the warp takes part in the pair's shuffle
+    // lanes 2i and 2i + 1 take the even and odd orbital units (plane waves) or
+    // orbitals of one row; every lane of the warp takes part in the pair's
+    // shuffle
     for (int base = 0; base < nb * W * 2; base += NT) {
         const int e = base + threadIdx.x, h = e & 1, dt = e >> 1, d = dt / W, t = dt % W;
         const DevBF* Dp = d < nb ? &s.bf[d] : nullptr;
@@ -853,13 +867,31 @@ __device__ void propose3(const DevSys& s, const V3& v, double* sm, const unsigne
             const int N = D.n;
             const double* pa = sm + D.pA;
             const double* xt = sm + D.pX + t * 3;
-            for (int m = h; m < N; m += 2) {
-                double val, g[3];
-                bf3_orbital(s, D, m, xt, val, g);
-                const double am = pa[m * N + t];
-                acc[0] = fma(am, g[0], acc[0]);
-                acc[1] = fma(am, g[1], acc[1]);
-                acc[2] = fma(am, g[2], acc[2]);
+            if (D.type == 0) {   // by orbital units: one sincos per cosine-sine pair
+                for (int u = h; u < units[d][32]; u += 2) {
+                    const int mu = units[d][u], m = mu & 31;
+                    const double* k = D.k + m * 3;
+                    double sn, c;
+                    sincos(fma(k[2], xt[2], fma(k[1], xt[1], k[0] * xt[0])), &sn, &c);
+                    const double dv = D.is_sin[m] != 0.0 ? c : -sn;
+                    const double am = pa[m * N + t];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) acc[a] = fma(am, k[a] * dv, acc[a]);
+                    if (mu & kUnitPair) {
+                        const double an = pa[(m + 1) * N + t];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) acc[a] = fma(an, k[a] * c, acc[a]);
+                    }
+                }
+            } else {
+                for (int m = h; m < N; m += 2) {
+                    double val, g[3];
+                    bf3_orbital(s, D, m, xt, val, g);
+                    const double am = pa[m * N + t];
+                    acc[0] = fma(am, g[0], acc[0]);
+                    acc[1] = fma(am, g[1], acc[1]);
+                    acc[2] = fma(am, g[2], acc[2]);
+                }
             }
         }
 #pragma unroll
