@@ -181,6 +181,25 @@ __device__ void build_units(const DevSys& s, unsigned char (*units)[33]) {
     }
 }
 
+// Rows r0 .. r0 + B - 1 of A lose their multiple mult[r] of the pivot row's
+// entry pk in this lane's column: B rows' loads in flight, then their
+// updates, the multipliers as 16-byte loads (mult + r0 16-byte aligned).
+template <int B>
+__device__ __forceinline__ void gj_rows(double* A, const double* mult, int N, int r0, int lane, double pk) {
+    double f[B], y[B];
+    const double2* m2 = reinterpret_cast<const double2*>(mult + r0);
+#pragma unroll
+    for (int u = 0; u < B / 2; ++u) {
+        const double2 q = m2[u];
+        f[2 * u] = q.x;
+        f[2 * u + 1] = q.y;
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u) y[u] = A[(r0 + u) * N + lane];
+#pragma unroll
+    for (int u = 0; u < B; ++u) A[(r0 + u) * N + lane] = fma(-f[u], pk, y[u]);
+}
+
 // In-place pivoted Gauss-Jordan of the N×N matrix A (N <= 32, row-major in
 // shared memory) by the calling warp: A becomes A⁻¹; out[0] = log|det A|,
 // out[1] = its sign, out[2] = 1 when every pivot is finite and nonzero.
@@ -238,31 +257,34 @@ __device__ void gj_warp_signed(double* A, int N, double* mult, int* perm, double
         }
         if (lane == 0) perm[k] = piv;
         __syncwarp();
-        if (lane < N)
-            for (int r0 = 0; r0 < N; r0 += 8) {   // eight rows' loads in flight, then their updates
-                double f[8], y[8];
-                if (vec && r0 + 8 <= N) {   // a whole block: its multipliers as four 16-byte loads
-                    const double2* m2 = reinterpret_cast<const double2*>(mult + r0);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const double2 q = m2[u];
-                        f[2 * u] = q.x;
-                        f[2 * u + 1] = q.y;
-                    }
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) y[u] = A[(r0 + u) * N + lane];
-                } else {
+        if (lane < N) {
+            if (vec) {   // whole blocks of 8, then 4, 2 and 1 rows, multipliers in 16-byte loads
+                int r0 = 0;
+                for (; r0 + 8 <= N; r0 += 8) gj_rows<8>(A, mult, N, r0, lane, pk);
+                if (r0 + 4 <= N) {
+                    gj_rows<4>(A, mult, N, r0, lane, pk);
+                    r0 += 4;
+                }
+                if (r0 + 2 <= N) {
+                    gj_rows<2>(A, mult, N, r0, lane, pk);
+                    r0 += 2;
+                }
+                if (r0 < N) A[r0 * N + lane] = fma(-mult[r0], pk, A[r0 * N + lane]);
+            } else {
+                for (int r0 = 0; r0 < N; r0 += 8) {   // eight rows' loads in flight, then their updates
+                    double f[8], y[8];
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const bool on = r0 + u < N;
                         f[u] = on ? mult[r0 + u] : 0.0;
                         y[u] = on ? A[(r0 + u) * N + lane] : 0.0;
                     }
-                }
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (r0 + u < N) A[(r0 + u) * N + lane] = fma(-f[u], pk, y[u]);
+                    for (int u = 0; u < 8; ++u)
+                        if (r0 + u < N) A[(r0 + u) * N + lane] = fma(-f[u], pk, y[u]);
+                }
             }
+        }
         __syncwarp();
     }
     for (int k = N - 1; k >= 0; --k) {
