@@ -564,9 +564,13 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
             for (int q = 0; q < 12; ++q) own[q] = warp_sum(own[q]);
         }
         // Jacobian columns Jw[β][t·3 + a] = ∂x_t^a/∂r_k^β and F_t·∂²x_t/∂(r_k^β)², lane = row
+        // (N <= 32); nz: row t's column is nonzero (k's own row, or t within a
+        // backflow cutoff of k)
+        bool nz = false;
         for (int t = lane; t < N; t += 32) {
             double vj[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, fs[3] = {0, 0, 0};
             const double* Ft = F + t * 3;
+            nz = t == tk;
             if (t == tk) {
 #pragma unroll
                 for (int q = 0; q < 9; ++q) vj[q] = own[q] + (q % 4 == 0 ? 1.0 : 0.0);   // [β·3 + a]
@@ -579,6 +583,7 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
                     if (!in_sources(D.ch[c], k)) continue;
                     double unused[3] = {0, 0, 0}, B[9], S[9];
                     if (!bf3_pair(s, D.ch[c], v.pos + P * 3, rk, 1.0, unused, B, S)) continue;
+                    nz = true;
 #pragma unroll
                     for (int b = 0; b < 3; ++b)
 #pragma unroll
@@ -611,16 +616,29 @@ __device__ void bf3_refresh(const DevSys& s, const V3& v, double* sm, int d, boo
             acc[b] += gg;
             acc[3 + b] += tt + FSw[b * N + t];
         }
-        for (int e = lane; e < 3 * N * N; e += 32) {
-            const int b = e / (N * N), jr = e % (N * N), j = jr / N, r = jr % N;
-            const double* vb = Jw + b * 3 * N;
-            double u1 = 0.0, u2 = 0.0;
+        // U_jr vanishes with row r's column and U_rj with row j's: the pairs of
+        // nonzero rows only, srow on lane i the i-th of them
+        const unsigned smask = __ballot_sync(0xffffffffu, nz);
+        const int ns = __popc(smask), n2 = ns * ns;
+        const unsigned spos = __fns(smask, 0, lane + 1);
+        const int srow = spos < 32u ? static_cast<int>(spos) : 0;
+        for (int base = 0; base < 3 * n2; base += 32) {   // every lane takes part in the shuffles
+            const int e = base + lane;
+            const bool on = e < 3 * n2;
+            const int ee = on ? e : 0;
+            const int b = ee / n2, jr = ee % n2;
+            const int j = __shfl_sync(0xffffffffu, srow, jr / ns);
+            const int r = __shfl_sync(0xffffffffu, srow, jr % ns);
+            if (on) {
+                const double* vb = Jw + b * 3 * N;
+                double u1 = 0.0, u2 = 0.0;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                u1 += vb[r * 3 + a] * G[a * N * N + j * N + r];
-                u2 += vb[j * 3 + a] * G[a * N * N + r * N + j];
+                for (int a = 0; a < 3; ++a) {
+                    u1 += vb[r * 3 + a] * G[a * N * N + j * N + r];
+                    u2 += vb[j * 3 + a] * G[a * N * N + r * N + j];
+                }
+                acc[3 + b] -= u1 * u2;
             }
-            acc[3 + b] -= u1 * u2;
         }
 #pragma unroll
         for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
